@@ -1,0 +1,244 @@
+/*
+ * ising_gpu.h -- C-ABI of libisinggpu.so, the B200 (sm_100a) Heisenberg Monte Carlo path.
+ *
+ * Drop-in boundary for the Fortran drivers of SamuelJosephs/ISING (src/PT.f90,
+ * src/ISING.f90).  Every entry point replaces one reference routine or inline block;
+ * the replaced interface is cited beside each declaration (paths within the reference
+ * project).  A Fortran `bind(C)` module over these symbols lets the drivers switch by
+ * changing `use` lines.
+ *
+ * Conventions
+ *  - Plain C types only; no CUDA or framework types cross this boundary.
+ *  - Every call returns an int status (ISING_OK = 0) and never aborts; on failure
+ *    ising_last_error() gives a message (thread-local).
+ *  - Host spin arrays are FP64 column-major (numAtoms, 3), the layout of
+ *    ChainMesh_t%atomSpins (src/chainMesh.f90:20).  Atom order is the reference's:
+ *    atom = cell*n_sub + i, cell = (ix*ny + iy)*nz + iz (src/chainMesh.f90:684,878).
+ *  - Indices at this boundary are 0-based unless a name ends in _1based.
+ *  - The library owns device memory (FP32 SoA spins, FP64 accumulators, lattice tables)
+ *    behind opaque handles; one CUDA stream per handle; one host thread per handle.
+ *  - Energy sign convention is the reference's: E = +J S_i.S_j (src/energyMin.f90:139),
+ *    so a ferromagnet has J < 0.
+ */
+#ifndef ISING_GPU_H
+#define ISING_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+#define ISING_OK 0
+#define ISING_ERR_ARG 1          /* bad argument (the reference calls error stop / MPI_Abort) */
+#define ISING_ERR_NAN 2          /* NaN in spins or proposals (src/energyMin.f90:330-331) */
+#define ISING_ERR_BOUNDS 3       /* index out of range (e.g. Z_index, rsp:334) */
+#define ISING_ERR_TIMEOUT 4      /* a bounded device-side wait gave up */
+#define ISING_ERR_UNSUPPORTED 5  /* e.g. demag=.true. (out of scope) */
+#define ISING_ERR_CUDA 6         /* CUDA runtime error or no usable device */
+#define ISING_ERR_ALLOC 7        /* device or host allocation failed */
+#define ISING_ERR_LATTICE 8      /* derivative list incomplete ("Unable to locate atoms",
+                                    src/chainMesh.f90:1028) */
+
+const char* ising_status_string(int status);
+const char* ising_last_error(void);
+/* Library version, e.g. "isinggpu 0.1 sm_100a". */
+const char* ising_version(void);
+
+/* ---------------------------------------------------------------- unit cells */
+#define ISING_CELL_SC 0            /* simple cubic, one atom at the origin (no reference cell) */
+#define ISING_CELL_BCC 1           /* bcc_unit_cell, src/unit_cells.f90:7-30 */
+#define ISING_CELL_HYPER_KAGOME 2  /* hyper_kagome_unit_cell, src/unit_cells.f90:32-77 */
+
+/* Fills the Bravais parameters and fractional atom coordinates of a unit cell.
+ * frac_xyz receives n_atoms x 3 floats (row-major), at most 12 atoms.
+ * Replaces bcc_unit_cell / hyper_kagome_unit_cell (src/unit_cells.f90:7,32). */
+int ising_unit_cell(int kind, double* a, double* b, double* c, double* ab_deg,
+                    double* bc_deg, double* ca_deg, float* frac_xyz, int* n_atoms);
+
+/* ---------------------------------------------------------------- lattice + state */
+typedef struct ising_mesh ising_mesh;
+
+typedef struct {
+    int64_t num_atoms;       /* ChainMesh_t%numAtoms */
+    int64_t num_cells;       /* ChainMesh_t%numChainMeshCells */
+    int nx, ny, nz, n_sub;   /* numCellsX/Y/Z, atoms per unit cell */
+    int n_shells;            /* neighbour shells built (default 2) */
+    int n_replicas;          /* replica spin buffers held on the device */
+    int shell_size[2];       /* entries per atom in shells 1 and 2 (sublattice 0) */
+    int checkerboard;        /* 1 if the SC 2-colour fast path applies */
+    double a_vec[3], b_vec[3], c_vec[3];
+} ising_mesh_info;
+
+/* Builds the lattice and allocates n_replicas spin buffers on `device`.
+ * Replaces makeChainMesh(numCellsX, numCellsY, numCellsZ, AtomsInUnitCell, a, b, c,
+ * ab_deg, bc_deg, ca_deg [, distance_threshold, numShells]) (src/chainMesh.f90:729-732).
+ * shell_tol <= 0 selects 0.1*a (:783); n_shells <= 0 selects 2 (:784).
+ * Requires nx, ny, nz >= 3 (smaller meshes stop the reference at :1028).
+ * device = -1 builds the lattice tables only (no GPU state); calls that need spins then
+ * return ISING_ERR_ARG. */
+int ising_mesh_create(const float* frac_xyz, int n_atoms_cell, int nx, int ny, int nz,
+                      double a, double b, double c, double ab_deg, double bc_deg,
+                      double ca_deg, double shell_tol, int n_shells, int n_replicas,
+                      int device, ising_mesh** out);
+/* Replaces deallocateChainMesh (src/chainMesh.f90:914-929). */
+int ising_mesh_destroy(ising_mesh* mesh);
+int ising_mesh_get_info(const ising_mesh* mesh, ising_mesh_info* info);
+/* Issue the handle's device work on an external CUDA stream (a cudaStream_t passed as an
+ * opaque pointer); NULL restores the handle's own stream.  No reference counterpart. */
+int ising_mesh_set_stream(ising_mesh* mesh, void* cuda_stream);
+/* Atom positions, real(4) like Atom_t%x,y,z (src/atom.f90:5): xyz is num_atoms x 3 row-major. */
+int ising_mesh_positions(const ising_mesh* mesh, float* xyz);
+/* Neighbour list of one atom, expanded from the lattice tables:
+ * shell 0/1 = atomShells(atom, 1/2)%NNList (src/chainMesh.f90:41,495-591);
+ * shell -1 = the legacy atoms(atom)%NeighborList (src/atom.f90:9, chainMesh.f90:280-405).
+ * Writes up to cap entries, returns the count in *n. */
+int ising_mesh_neighbours(const ising_mesh* mesh, int64_t atom, int shell, int64_t* out,
+                          int cap, int* n);
+/* derivativeList(atom, d, side) (src/chainMesh.f90:23,931-1031), 0-based atoms,
+ * out is num_atoms x 3 x 2 row-major (side 0 = lower, 1 = higher). */
+int ising_mesh_derivative_list(const ising_mesh* mesh, int64_t* out);
+
+/* Spins of one replica from / to a host FP64 column-major (num_atoms, 3) array
+ * (ChainMesh_t%atomSpins, src/chainMesh.f90:20).  set rejects NaN or zero vectors. */
+int ising_spins_set(ising_mesh* mesh, int replica, const double* col_major_n3);
+int ising_spins_get(const ising_mesh* mesh, int replica, double* col_major_n3);
+/* Uniform unit vectors on every replica from Philox(seed; site, 0, replica, ensemble|1).
+ * The reference leaves PT spins uninitialised (src/chainMesh.f90:889-890). */
+int ising_spins_init_uniform(ising_mesh* mesh, uint64_t seed, uint32_t ensemble);
+
+/* ---------------------------------------------------------------- Hamiltonian */
+#define ISING_DMI_INTERFACIAL 0   /* D_ij = Dz * n x r_ij, n = dmi_axis (src/energyMin.f90:114,137) */
+#define ISING_DMI_BULK 1          /* D_ij = Dz * r_ij, the commented form (src/energyMin.f90:138) */
+
+typedef struct {
+    /* the reference's argument list (src/energyMin.f90:86-87, 234-235, 499) */
+    double J, J_prime, Dz, Dz_prime, B;
+    /* uniaxial anisotropy -K (S.e)^2: an extension with no reference counterpart */
+    double K;
+    double K_axis[3];
+    /* Zeeman prefactor: 1 in calculateHeisenbergEnergy (:161), g*mu_B = 2 in
+     * TotalHeisenbergEnergy (:222, src/constants.f90:11,14) */
+    double zeeman_factor;
+    int include_Jp;      /* 1: add the J' shell-2 sum (local routine); 0: total routine */
+    int dmi_mode;        /* ISING_DMI_INTERFACIAL or ISING_DMI_BULK */
+    double dmi_axis[3];  /* interfacial axis; all zero selects c_vec/|c_vec| (:114) */
+    int legacy_neighbours; /* 1: sum over the legacy NeighborList (TotalHeisenbergEnergy) */
+    int demag;           /* must be 0: demag=.true. returns ISING_ERR_UNSUPPORTED */
+} ising_params;
+
+/* Fills p with the conventions of one reference routine:
+ * which = 0: calculateHeisenbergEnergy / Metropolis_mcs (zeeman 1, J' on, axis c_hat)
+ * which = 1: TotalHeisenbergEnergy (zeeman g*mu_B = 2, J' off, axis z, legacy list). */
+int ising_params_reference(int which, double J, double J_prime, double Dz, double Dz_prime,
+                           double B, ising_params* p);
+
+/* Colour class of every atom as the sweep uses it for the Hamiltonian p: the checkerboard
+ * (x+y+z)&1 on even simple-cubic meshes without J', a verified greedy colouring of the active
+ * shells otherwise.  No reference counterpart: Metropolis_mcs draws random parity cells
+ * instead (src/energyMin.f90:288-316). */
+int ising_mesh_colouring(ising_mesh* mesh, const ising_params* p, int* colour_of, int* n_colours);
+
+/* ---------------------------------------------------------------- energies */
+/* Replaces calculateHeisenbergEnergy(chainMesh, atomIndex, J, J', Dz, Dz', B, lockArray,
+ * S_proposed, oldEnergy, newEnergy, demag_array, demag) (src/energyMin.f90:86-171).
+ * FP32 local field on the device, results widened to FP64. */
+int ising_local_energy(const ising_mesh* mesh, int replica, int atom_index_1based,
+                       const ising_params* p, const double s_prop[3], double* old_e,
+                       double* new_e);
+/* Batched form of the above for n sites (0-based), s_prop n x 3 row-major. */
+int ising_local_energy_batch(const ising_mesh* mesh, int replica, int n, const int64_t* atoms,
+                             const double* s_prop, const ising_params* p, double* old_e,
+                             double* new_e);
+/* Replaces TotalHeisenbergEnergy(chainMesh, J, J', Dz, Dz', B, lockArray, totalEnergy,
+ * demag) (src/energyMin.f90:499-528): FP32 terms, FP64 block sums. */
+int ising_total_energy(const ising_mesh* mesh, int replica, const ising_params* p, double* e);
+/* Energy and magnetisation vector of every replica in one pass: e[R], m[R*3]. */
+int ising_observables(const ising_mesh* mesh, const ising_params* p, double* e, double* m);
+
+/* ---------------------------------------------------------------- sweeps */
+#define ISING_MOVE_UNIFORM 0   /* fresh uniform unit vector */
+#define ISING_MOVE_BALL 1      /* S' = norm(S + r*ball), UniformRandomInSphere (src/energyMin.f90:49-68) */
+
+/* Replaces Metropolis_mcs(chainMesh, beta, numMCSSweeps, J, J', Dz, Dz', B, r, lockArray,
+ * demag) (src/energyMin.f90:234-374).  A sweep visits every atom once through colour
+ * classes (checkerboard on even simple-cubic meshes, greedy colouring otherwise) with
+ * Philox keyed by (seed, ensemble 0, replica, sweep, atom); the per-replica sweep counter
+ * lives in the handle so successive calls continue the stream.  r > 0 selects the ball
+ * move of radius r, r <= 0 the uniform move.  lockArray has no counterpart (no locks). */
+int ising_metropolis_mcs(ising_mesh* mesh, int replica, double beta, int n_sweeps,
+                         const ising_params* p, double r, uint64_t seed);
+
+/* ---------------------------------------------------------------- winding number */
+/* Replaces calculate_winding_number2(chainMesh, Z_index) (rsp:320-364). FP64 on device. */
+int ising_winding_number(const ising_mesh* mesh, int replica, int z_1based, double* q);
+/* All nz slices of one replica (the loop of src/PT-Utils.f90:49-51). */
+int ising_winding_all_slices(const ising_mesh* mesh, int replica, double* q_per_slice);
+/* Replaces chainMesh_statistics (src/PT-Utils.f90:33-66) except the skyrmion count. */
+int ising_statistics(const ising_mesh* mesh, int replica, double* wnd_mid, double* wnd_spread,
+                     double m[3]);
+/* Replaces calculate_winding_number_density (rsp:438-500): nx x ny column-major. */
+int ising_winding_density(const ising_mesh* mesh, int replica, int z_1based, double* density);
+
+/* ---------------------------------------------------------------- parallel tempering */
+typedef struct ising_pt ising_pt;
+
+#define ISING_PT_EVEN_ODD 0     /* deterministic alternating neighbour pairs, correct criterion */
+#define ISING_PT_RANDOM_PAIRS 1 /* n random neighbour pairs per round (src/PT.f90:236-244),
+                                   correct criterion */
+
+typedef struct {
+    uint64_t seed;
+    uint32_t ensemble;        /* Philox key component; distinct per ensemble */
+    int move;                 /* ISING_MOVE_UNIFORM or ISING_MOVE_BALL */
+    double r;                 /* ball radius (src/PT.f90:230 uses 0.2) */
+    int scheme;               /* ISING_PT_EVEN_ODD or ISING_PT_RANDOM_PAIRS */
+    int resync_every;         /* rounds between FP64 energy resyncs (0 = never) */
+    int record;               /* 1: record E, |M|, Q per sweep into a device series */
+    int record_capacity;      /* sweeps to keep per replica when record = 1 */
+} ising_pt_options;
+
+/* Replaces the PT state of src/PT.f90:193-204 (TemperatureMeshArray, TemperatureArray):
+ * replicas 0..n_temps-1 of `mesh` start at temperature slots 0..n_temps-1 with inverse
+ * temperatures betas[t]. */
+int ising_pt_create(ising_mesh* mesh, int n_temps, const double* betas, const ising_params* p,
+                    const ising_pt_options* opt, ising_pt** out);
+int ising_pt_destroy(ising_pt* pt);
+/* rounds x [sweeps_per_swap sweeps of every replica, then one exchange], replacing the
+ * iteration loop of src/PT.f90:219-273; replayed from a CUDA graph. */
+int ising_pt_run(ising_pt* pt, int sweeps_per_swap, int rounds);
+/* n_sweeps sweeps of every replica at its current temperature without exchange: the
+ * "relax each domain" loop of src/PT.f90:276-287. */
+int ising_pt_relax(ising_pt* pt, int n_sweeps);
+/* temperature slot -> replica (TemperatureMeshArray(i, :), src/PT.f90:58) */
+int ising_pt_permutation(const ising_pt* pt, int* temp_to_replica);
+/* running FP64 energies and magnetisation vectors by replica */
+int ising_pt_energies(const ising_pt* pt, double* e_per_replica, double* m_per_replica);
+/* recompute the running accumulators from the spins (periodic FP64 resync) */
+int ising_pt_resync(ising_pt* pt);
+/* attempts and accepts per neighbour pair (t, t+1), n_temps-1 entries each */
+int ising_pt_swap_stats(const ising_pt* pt, uint64_t* attempts, uint64_t* accepts);
+/* Recorded series by temperature slot (the replica holding slot t at each recorded
+ * sweep): E, |M| = |sum S|/N, Q_mid (slice nz/2) and Q_mean (mean over slices).
+ * out is n_temps x record_capacity x 4; *n_recorded gives the filled length. */
+int ising_pt_series(const ising_pt* pt, double* out, int* n_recorded);
+
+/* ---------------------------------------------------------------- CSV outputs */
+/* write_spins_to_file(chainMesh, filename, append, include_header, frame_index)
+ * (src/LLG.f90:93-172): "x,y,z,Sx,Sy,Sz" with ES22.14; frame_index < 0 means absent. */
+int ising_write_spins_csv(const ising_mesh* mesh, int replica, const char* path, int append,
+                          int include_header, int frame_index);
+/* The data_<J>_<D>_<B>_<T>.csv record of src/PT.f90:318-362 (header, F0.4/F0.10 and
+ * F0.4/I0.4/F0.2 formats) and its file name (PT.f90:337-341). */
+int ising_write_pt_data_csv(const char* path, double J, double D, double B, double T,
+                            double wnd_mid, int sk_mid, double wnd_spread, const double m[3]);
+int ising_pt_file_tag(char* buf, size_t cap, double J, double D, double B, double T);
+/* write_winding_number_density (rsp:544-580): "x,y,z,Winding_Density" with F0.8. */
+int ising_write_winding_density_csv(const ising_mesh* mesh, int replica, const char* path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ISING_GPU_H */

@@ -1,0 +1,378 @@
+"""Python host mirror of the reference's driver-facing routines over libisinggpu.
+
+Names, argument meaning and error behaviour follow the Fortran routines of
+SamuelJosephs/ISING (citations per function).  Where the reference calls ``error stop``
+these raise :class:`IsingError`.  All compute runs in the CUDA library; nothing here
+computes physics on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import (CELL_BCC, CELL_HYPER_KAGOME, CELL_SC, DMI_BULK, DMI_INTERFACIAL, MOVE_BALL,
+                   MOVE_UNIFORM, PT_EVEN_ODD, PT_RANDOM_PAIRS, IsingError, MeshInfo, Params, PTOptions)
+
+_P = C.POINTER
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_P(C.c_double))
+
+
+# ---------------------------------------------------------------- unit cells
+def unit_cell(kind: int):
+    """(a, b, c, ab, bc, ca, frac) of ISING_CELL_SC / _BCC (src/unit_cells.f90:7-30) /
+    _HYPER_KAGOME (src/unit_cells.f90:32-77)."""
+    a, b, c, ab, bc, ca = (C.c_double() for _ in range(6))
+    frac = (C.c_float * 36)()
+    n = C.c_int()
+    _lib.call("ising_unit_cell", kind, C.byref(a), C.byref(b), C.byref(c), C.byref(ab), C.byref(bc),
+              C.byref(ca), frac, C.byref(n))
+    f = np.array(frac[: 3 * n.value], dtype=np.float32).reshape(n.value, 3)
+    return a.value, b.value, c.value, ab.value, bc.value, ca.value, f
+
+
+def bcc_unit_cell():
+    return unit_cell(CELL_BCC)
+
+
+def hyper_kagome_unit_cell():
+    return unit_cell(CELL_HYPER_KAGOME)
+
+
+def sc_unit_cell():
+    return unit_cell(CELL_SC)
+
+
+# ---------------------------------------------------------------- Hamiltonian
+def params(J=0.0, J_prime=0.0, Dz=0.0, Dz_prime=0.0, B=0.0, K=0.0, K_axis=(0.0, 0.0, 1.0),
+           zeeman_factor=1.0, include_Jp=True, dmi="interfacial", dmi_axis=None,
+           legacy_neighbours=False, demag=False) -> Params:
+    """Hamiltonian block.  Defaults follow calculateHeisenbergEnergy / Metropolis_mcs
+    (src/energyMin.f90:86-171): Zeeman factor 1, J' on, interfacial DMI about c_hat.
+    Sign convention E = +J S.S' (src/energyMin.f90:139): a ferromagnet has J < 0."""
+    p = Params()
+    p.J, p.J_prime, p.Dz, p.Dz_prime, p.B, p.K = J, J_prime, Dz, Dz_prime, B, K
+    p.K_axis[:] = list(K_axis)
+    p.zeeman_factor = zeeman_factor
+    p.include_Jp = int(bool(include_Jp))
+    p.dmi_mode = DMI_BULK if dmi == "bulk" else DMI_INTERFACIAL
+    p.dmi_axis[:] = list(dmi_axis) if dmi_axis is not None else [0.0, 0.0, 0.0]
+    p.legacy_neighbours = int(bool(legacy_neighbours))
+    p.demag = int(bool(demag))
+    return p
+
+
+def reference_params(which: str, J, J_prime, Dz, Dz_prime, B) -> Params:
+    """Conventions of one reference routine: 'local' (calculateHeisenbergEnergy,
+    Metropolis_mcs) or 'total' (TotalHeisenbergEnergy: g*mu_B*B, no J', D axis z)."""
+    p = Params()
+    _lib.call("ising_params_reference", 0 if which == "local" else 1, J, J_prime, Dz, Dz_prime, B, C.byref(p))
+    return p
+
+
+# ---------------------------------------------------------------- lattice
+class ChainMesh:
+    """makeChainMesh (src/chainMesh.f90:729-911) on the device, with n_replicas spin buffers."""
+
+    def __init__(self, numCellsX: int, numCellsY: int, numCellsZ: int, atoms_in_unit_cell,
+                 a: float, b: float, c: float, ab_deg: float = 90.0, bc_deg: float = 90.0,
+                 ca_deg: float = 90.0, distance_threshold: Optional[float] = None,
+                 numShells: Optional[int] = None, n_replicas: int = 1, device: int = 0):
+        frac = np.ascontiguousarray(atoms_in_unit_cell, dtype=np.float32).reshape(-1, 3)
+        h = C.c_void_p()
+        _lib.call("ising_mesh_create", frac.ctypes.data_as(_P(C.c_float)), frac.shape[0], numCellsX,
+                  numCellsY, numCellsZ, a, b, c, ab_deg, bc_deg, ca_deg,
+                  distance_threshold if distance_threshold else 0.0, numShells if numShells else 0,
+                  n_replicas, device, C.byref(h))
+        self._h = h
+        info = MeshInfo()
+        _lib.call("ising_mesh_get_info", h, C.byref(info))
+        self.info = info
+        self.numAtoms = int(info.num_atoms)
+        self.numCellsX, self.numCellsY, self.numCellsZ = info.nx, info.ny, info.nz
+        self.n_sub = info.n_sub
+        self.n_replicas = info.n_replicas
+        self.checkerboard = bool(info.checkerboard)
+        self.a_vec = np.array(info.a_vec[:])
+        self.b_vec = np.array(info.b_vec[:])
+        self.c_vec = np.array(info.c_vec[:])
+
+    @classmethod
+    def simple_cubic(cls, L: int, ny: Optional[int] = None, nz: Optional[int] = None, a: float = 1.0,
+                     **kw) -> "ChainMesh":
+        return cls(L, ny or L, nz or L, np.zeros((1, 3), np.float32), a, a, a, **kw)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.load().ising_mesh_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # spins ---------------------------------------------------------------
+    def get_spins(self, replica: int = 0) -> np.ndarray:
+        """atomSpins(numAtoms, 3) of one replica (FP64, widened from the device FP32)."""
+        out = np.empty((3, self.numAtoms), dtype=np.float64)
+        _lib.call("ising_spins_get", self._h, replica, _dp(out))
+        return out.T
+
+    def set_spins(self, spins, replica: int = 0):
+        s = np.asarray(spins, dtype=np.float64).reshape(self.numAtoms, 3)
+        col = np.ascontiguousarray(s.T)
+        _lib.call("ising_spins_set", self._h, replica, _dp(col))
+
+    @property
+    def atomSpins(self) -> np.ndarray:
+        return self.get_spins(0)
+
+    @atomSpins.setter
+    def atomSpins(self, v):
+        self.set_spins(v, 0)
+
+    def set_stream(self, cuda_stream: Optional[int]):
+        """Issue this mesh's device work on an external stream (e.g. a torch stream's
+        .cuda_stream); None restores the mesh's own stream."""
+        _lib.call("ising_mesh_set_stream", self._h, C.c_void_p(cuda_stream) if cuda_stream else None)
+
+    def init_uniform(self, seed: int, ensemble: int = 0):
+        _lib.call("ising_spins_init_uniform", self._h, seed, ensemble)
+
+    # geometry ------------------------------------------------------------
+    def positions(self) -> np.ndarray:
+        out = np.empty((self.numAtoms, 3), dtype=np.float32)
+        _lib.call("ising_mesh_positions", self._h, out.ctypes.data_as(_P(C.c_float)))
+        return out
+
+    def neighbours(self, atom: int, shell: int) -> np.ndarray:
+        """0-based neighbour atoms: shell 0/1 = atomShells(atom+1, 1/2)%NNList, -1 = NeighborList."""
+        cap = 256
+        out = np.empty(cap, dtype=np.int64)
+        n = C.c_int()
+        _lib.call("ising_mesh_neighbours", self._h, atom, shell, out.ctypes.data_as(_P(C.c_int64)), cap, C.byref(n))
+        return out[: n.value].copy()
+
+    def colouring(self, p: Params):
+        """(colour per atom, number of classes) the sweep uses for Hamiltonian p."""
+        out = np.empty(self.numAtoms, dtype=np.int32)
+        n = C.c_int()
+        _lib.call("ising_mesh_colouring", self._h, C.byref(p), out.ctypes.data_as(_P(C.c_int)), C.byref(n))
+        return out, n.value
+
+    def derivative_list(self) -> np.ndarray:
+        out = np.empty((self.numAtoms, 3, 2), dtype=np.int64)
+        _lib.call("ising_mesh_derivative_list", self._h, out.ctypes.data_as(_P(C.c_int64)))
+        return out
+
+
+def make_chain_mesh(numCellsX, numCellsY, numCellsZ, atoms_in_unit_cell, a, b, c, ab_deg, bc_deg, ca_deg,
+                    distance_threshold=None, numShells=None, n_replicas=1, device=0) -> ChainMesh:
+    return ChainMesh(numCellsX, numCellsY, numCellsZ, atoms_in_unit_cell, a, b, c, ab_deg, bc_deg, ca_deg,
+                     distance_threshold, numShells, n_replicas, device)
+
+
+# ---------------------------------------------------------------- energies
+def calculate_heisenberg_energy(mesh: ChainMesh, atomIndex: int, J, J_prime, Dz, Dz_prime, B,
+                                S_proposed, demag: bool = False, replica: int = 0,
+                                p: Optional[Params] = None):
+    """calculateHeisenbergEnergy (src/energyMin.f90:86-171): (oldEnergy, newEnergy) of the
+    1-based atomIndex for the current spin and S_proposed."""
+    if p is None:
+        p = reference_params("local", J, J_prime, Dz, Dz_prime, B)
+        p.demag = int(bool(demag))
+    sp = np.ascontiguousarray(S_proposed, dtype=np.float64)
+    o, n = C.c_double(), C.c_double()
+    _lib.call("ising_local_energy", mesh.handle, replica, atomIndex, C.byref(p), _dp(sp), C.byref(o), C.byref(n))
+    return o.value, n.value
+
+
+def local_energy_batch(mesh: ChainMesh, atoms, s_prop, p: Params, replica: int = 0):
+    atoms = np.ascontiguousarray(atoms, dtype=np.int64)
+    sp = np.ascontiguousarray(s_prop, dtype=np.float64).reshape(-1, 3)
+    n = atoms.shape[0]
+    old, new = np.empty(n), np.empty(n)
+    _lib.call("ising_local_energy_batch", mesh.handle, replica, n, atoms.ctypes.data_as(_P(C.c_int64)), _dp(sp),
+              C.byref(p), _dp(old), _dp(new))
+    return old, new
+
+
+def total_heisenberg_energy(mesh: ChainMesh, J, J_prime, Dz, Dz_prime, B, demag: bool = False,
+                            replica: int = 0, p: Optional[Params] = None) -> float:
+    """TotalHeisenbergEnergy (src/energyMin.f90:499-528)."""
+    if p is None:
+        p = reference_params("total", J, J_prime, Dz, Dz_prime, B)
+        p.demag = int(bool(demag))
+    e = C.c_double()
+    _lib.call("ising_total_energy", mesh.handle, replica, C.byref(p), C.byref(e))
+    return e.value
+
+
+def observables(mesh: ChainMesh, p: Params):
+    """(E[R], M[R,3]) of every replica in one device pass."""
+    R = mesh.n_replicas
+    e, m = np.empty(R), np.empty((R, 3))
+    _lib.call("ising_observables", mesh.handle, C.byref(p), _dp(e), _dp(m))
+    return e, m
+
+
+# ---------------------------------------------------------------- sweeps
+def metropolis_mcs(mesh: ChainMesh, beta: float, numMCSSweeps: int, J, J_prime, Dz, Dz_prime, B, r,
+                   lockArray=None, demag: bool = False, replica: int = 0, seed: int = 0x15196,
+                   p: Optional[Params] = None):
+    """Metropolis_mcs (src/energyMin.f90:234-374) as an exact colour-class sweep on the GPU.
+    r > 0 selects the ball move of radius r; lockArray is accepted and ignored."""
+    if p is None:
+        p = reference_params("local", J, J_prime, Dz, Dz_prime, B)
+        p.demag = int(bool(demag))
+    _lib.call("ising_metropolis_mcs", mesh.handle, replica, beta, numMCSSweeps, C.byref(p), r, seed)
+
+
+# ---------------------------------------------------------------- winding number
+def calculate_winding_number2(mesh: ChainMesh, Z_index: int, replica: int = 0) -> float:
+    """calculate_winding_number2 (src/reciprocalSpaceProcesses.f90:320-364), 1-based Z_index."""
+    q = C.c_double()
+    _lib.call("ising_winding_number", mesh.handle, replica, Z_index, C.byref(q))
+    return q.value
+
+
+def winding_all_slices(mesh: ChainMesh, replica: int = 0) -> np.ndarray:
+    out = np.empty(mesh.numCellsZ)
+    _lib.call("ising_winding_all_slices", mesh.handle, replica, _dp(out))
+    return out
+
+
+def calculate_winding_number_density(mesh: ChainMesh, Z_index: int, replica: int = 0) -> np.ndarray:
+    """calculate_winding_number_density (rsp:438-500): (numCellsX, numCellsY) array."""
+    out = np.empty(mesh.numCellsX * mesh.numCellsY)
+    _lib.call("ising_winding_density", mesh.handle, replica, Z_index, _dp(out))
+    return out.reshape(mesh.numCellsY, mesh.numCellsX).T
+
+
+def chain_mesh_statistics(mesh: ChainMesh, replica: int = 0):
+    """chainMesh_statistics (src/PT-Utils.f90:33-66) without the skyrmion count:
+    (winding_number_middle, winding_number_spread, magnetisation[3])."""
+    wm, ws = C.c_double(), C.c_double()
+    m = np.empty(3)
+    _lib.call("ising_statistics", mesh.handle, replica, C.byref(wm), C.byref(ws), _dp(m))
+    return wm.value, ws.value, m
+
+
+# ---------------------------------------------------------------- CSV outputs
+def write_spins_to_file(mesh: ChainMesh, filename: str, append: bool = False, include_header: bool = True,
+                        frame_index: Optional[int] = None, replica: int = 0):
+    """write_spins_to_file (src/LLG.f90:93-172)."""
+    _lib.call("ising_write_spins_csv", mesh.handle, replica, filename.encode(), int(append), int(include_header),
+              -1 if frame_index is None else int(frame_index))
+
+
+def write_winding_number_density(mesh: ChainMesh, filepath: str, replica: int = 0):
+    """write_winding_number_density (rsp:544-580)."""
+    _lib.call("ising_write_winding_density_csv", mesh.handle, replica, filepath.encode())
+
+
+def pt_file_tag(J, D, B, T) -> str:
+    """The (F0.4,"_",F0.4,"_",F0.4,"_",e0.4) tag of src/PT.f90:337-338."""
+    buf = C.create_string_buffer(256)
+    _lib.call("ising_pt_file_tag", buf, 256, J, D, B, T)
+    return buf.value.decode()
+
+
+def write_pt_data_csv(path: str, J, D, B, T, winding_number_middle, skyrmion_number_middle,
+                      winding_number_spread, magnetisation: Sequence[float]):
+    """The data_<tag>.csv record of src/PT.f90:318-362."""
+    m = np.ascontiguousarray(magnetisation, dtype=np.float64)
+    _lib.call("ising_write_pt_data_csv", path.encode(), J, D, B, T, winding_number_middle,
+              int(skyrmion_number_middle), winding_number_spread, _dp(m))
+
+
+# ---------------------------------------------------------------- parallel tempering
+def temperature_ladder(Tmin: float, Tmax: float, n: int) -> np.ndarray:
+    """Geometric ladder T_j = Tmin (Tmax/Tmin)^((j-1)/(n-1)) (src/PT.f90:202)."""
+    if n == 1:
+        return np.array([Tmin])
+    j = np.arange(n)
+    return Tmin * (Tmax / Tmin) ** (j / (n - 1))
+
+
+class ParallelTempering:
+    """The PT block of src/PT.f90:193-272 on the device: replicas 0..n-1 of `mesh` start at
+    temperature slots 0..n-1; exchange relabels slots (TemperatureMeshArray)."""
+
+    def __init__(self, mesh: ChainMesh, betas, p: Params, seed: int = 0x15196, ensemble: int = 0,
+                 move: int = MOVE_BALL, r: float = 0.2, scheme: int = PT_EVEN_ODD, resync_every: int = 0,
+                 record: bool = False, record_capacity: int = 0):
+        self.mesh = mesh
+        self.betas = np.ascontiguousarray(betas, dtype=np.float64)
+        self.n = len(self.betas)
+        self.p = p
+        o = PTOptions()
+        o.seed, o.ensemble, o.move, o.r, o.scheme = seed, ensemble, move, r, scheme
+        o.resync_every, o.record, o.record_capacity = resync_every, int(record), record_capacity
+        self.opt = o
+        h = C.c_void_p()
+        _lib.call("ising_pt_create", mesh.handle, self.n, _dp(self.betas), C.byref(p), C.byref(o), C.byref(h))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.load().ising_pt_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, sweeps_per_swap: int, rounds: int):
+        _lib.call("ising_pt_run", self._h, sweeps_per_swap, rounds)
+
+    def relax(self, n_sweeps: int):
+        """Sweeps without exchange (the relax loop of src/PT.f90:276-287)."""
+        _lib.call("ising_pt_relax", self._h, n_sweeps)
+
+    def permutation(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.int32)
+        _lib.call("ising_pt_permutation", self._h, out.ctypes.data_as(_P(C.c_int)))
+        return out
+
+    def energies(self):
+        e, m = np.empty(self.n), np.empty((self.n, 3))
+        _lib.call("ising_pt_energies", self._h, _dp(e), _dp(m))
+        return e, m
+
+    def resync(self):
+        _lib.call("ising_pt_resync", self._h)
+
+    def swap_stats(self):
+        att = np.zeros(max(self.n - 1, 1), dtype=np.uint64)
+        acc = np.zeros(max(self.n - 1, 1), dtype=np.uint64)
+        _lib.call("ising_pt_swap_stats", self._h, att.ctypes.data_as(_P(C.c_uint64)),
+                  acc.ctypes.data_as(_P(C.c_uint64)))
+        return att[: self.n - 1], acc[: self.n - 1]
+
+    def series(self) -> np.ndarray:
+        """(n_temps, n_recorded, 4): E, |M|, Q_mid, Q_mean per recorded sweep."""
+        cap = self.opt.record_capacity
+        out = np.empty((self.n, cap, 4))
+        n = C.c_int()
+        _lib.call("ising_pt_series", self._h, _dp(out), C.byref(n))
+        return out[:, : n.value, :]

@@ -1,0 +1,997 @@
+// capi.cu -- the extern "C" entry points of libisinggpu (declared in include/ising_gpu.h).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+// ======================================================================= errors
+namespace isg {
+static thread_local std::string g_err;
+void set_error(const std::string& m) { g_err = m; }
+int fail(int status, const std::string& m) { g_err = m; return status; }
+int cuda_fail(cudaError_t e, const char* what) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return ISING_ERR_CUDA;
+}
+}  // namespace isg
+
+using namespace isg;
+
+#define ISG_TRY(expr)                  \
+    do {                               \
+        int st_ = (expr);              \
+        if (st_ != ISING_OK) return st_; \
+    } while (0)
+
+extern "C" const char* ising_last_error(void) { return isg::g_err.c_str(); }
+
+extern "C" const char* ising_status_string(int s) {
+    switch (s) {
+        case ISING_OK: return "ok";
+        case ISING_ERR_ARG: return "invalid argument";
+        case ISING_ERR_NAN: return "NaN encountered";
+        case ISING_ERR_BOUNDS: return "index out of bounds";
+        case ISING_ERR_TIMEOUT: return "device wait timed out";
+        case ISING_ERR_UNSUPPORTED: return "unsupported option";
+        case ISING_ERR_CUDA: return "CUDA error";
+        case ISING_ERR_ALLOC: return "allocation failed";
+        case ISING_ERR_LATTICE: return "lattice error";
+        default: return "unknown status";
+    }
+}
+
+extern "C" const char* ising_version(void) { return "isinggpu 0.1 sm_100a"; }
+
+// ======================================================================= helpers
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+template <typename T>
+int dev_alloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e != cudaSuccess) return fail(ISING_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return ISING_OK;
+}
+
+// status word -> error code; clears it
+int check_status(ising_mesh* m) {
+    ISG_CUDA(cudaMemcpyAsync(m->h_pinned, m->d_status, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+    ISG_CUDA(cudaStreamSynchronize(m->stream));
+    int st;
+    std::memcpy(&st, m->h_pinned, sizeof(int));
+    if (st) {
+        ISG_CUDA(cudaMemsetAsync(m->d_status, 0, sizeof(int), m->stream));
+        if (st & kStatNan) return fail(ISING_ERR_NAN, "NaN in spins or proposals");
+        if (st & kStatTimeout) return fail(ISING_ERR_TIMEOUT, "device wait timed out");
+        if (st & kStatBounds) return fail(ISING_ERR_BOUNDS, "device index out of bounds");
+    }
+    return ISING_OK;
+}
+
+int validate_params(const ising_params* p) {
+    if (!p) return fail(ISING_ERR_ARG, "params is NULL");
+    if (p->demag) return fail(ISING_ERR_UNSUPPORTED, "demag=.true. is out of scope (demagnetising field not built)");
+    const double v[] = {p->J, p->J_prime, p->Dz, p->Dz_prime, p->B, p->K, p->zeeman_factor};
+    for (double x : v) if (!std::isfinite(x)) return fail(ISING_ERR_NAN, "non-finite Hamiltonian parameter");
+    if (p->dmi_mode != ISING_DMI_INTERFACIAL && p->dmi_mode != ISING_DMI_BULK)
+        return fail(ISING_ERR_ARG, "dmi_mode must be ISING_DMI_INTERFACIAL or ISING_DMI_BULK");
+    return ISING_OK;
+}
+
+// DMI vector of a bond with min-image r = r_j - r_i, reference orientation r_hat = -r/|r|
+// (src/energyMin.f90:135-138).
+void bond_dmi(const Lattice& L, const ising_params& p, const double r[3], double D[3]) {
+    const double n = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    const double rh[3] = {-r[0] / n, -r[1] / n, -r[2] / n};
+    if (p.dmi_mode == ISING_DMI_BULK) {
+        for (int k = 0; k < 3; ++k) D[k] = p.Dz * rh[k];
+        return;
+    }
+    double ax[3] = {p.dmi_axis[0], p.dmi_axis[1], p.dmi_axis[2]};
+    if (ax[0] == 0.0 && ax[1] == 0.0 && ax[2] == 0.0) {
+        const double cn = std::sqrt(L.cv[0] * L.cv[0] + L.cv[1] * L.cv[1] + L.cv[2] * L.cv[2]);
+        for (int k = 0; k < 3; ++k) ax[k] = L.cv[k] / cn;
+    }
+    const double t[3] = {p.Dz * ax[0], p.Dz * ax[1], p.Dz * ax[2]};
+    D[0] = t[1] * rh[2] - t[2] * rh[1];
+    D[1] = t[2] * rh[0] - t[0] * rh[2];
+    D[2] = t[0] * rh[1] - t[1] * rh[0];
+}
+
+HamDev make_ham(const ising_params& p) {
+    HamDev h{};
+    h.J = (float)p.J;
+    h.Jp = (float)p.J_prime;
+    h.Bz = (float)(p.zeeman_factor * p.B);
+    h.K = (float)p.K;
+    h.kx = (float)p.K_axis[0]; h.ky = (float)p.K_axis[1]; h.kz = (float)p.K_axis[2];
+    return h;
+}
+
+bool uses_shell2(const Lattice& L, const ising_params& p) {
+    return p.include_Jp && p.J_prime != 0.0 && L.nshells > 1;
+}
+
+// Fill the device stencil of `m` for the given Hamiltonian.  legacy: the legacy list with
+// (J, D); otherwise shell 1 with (J, D) and shell 2 with J' when active.
+int upload_stencil(ising_mesh* m, const ising_params& p, bool legacy, Slot* dst_slots, int* dst_count) {
+    const Lattice& L = m->lat;
+    std::vector<Slot> slots((size_t)kMaxSub * kMaxSlots);
+    std::vector<int> cnt(kMaxSub, 0);
+    for (int s = 0; s < L.nsub; ++s) {
+        int c = 0;
+        auto add = [&](const NbrSlot& q, float w, bool dmi) -> int {
+            if (c >= kMaxSlots) return fail(ISING_ERR_ARG, "stencil exceeds 64 slots");
+            Slot e{};
+            e.dx = (int8_t)q.dx; e.dy = (int8_t)q.dy; e.dz = (int8_t)q.dz; e.sub = (uint8_t)q.sub;
+            e.w = w;
+            if (dmi && p.Dz != 0.0) {
+                double D[3];
+                bond_dmi(L, p, q.r, D);
+                e.Dx = (float)D[0]; e.Dy = (float)D[1]; e.Dz = (float)D[2];
+            }
+            slots[(size_t)s * kMaxSlots + c++] = e;
+            return ISING_OK;
+        };
+        if (legacy) {
+            for (const auto& q : L.legacy[s]) ISG_TRY(add(q, (float)p.J, true));
+        } else {
+            for (const auto& q : L.shell[0][s]) ISG_TRY(add(q, (float)p.J, true));
+            if (uses_shell2(L, p))
+                for (const auto& q : L.shell[1][s]) ISG_TRY(add(q, (float)p.J_prime, false));
+        }
+        cnt[s] = c;
+    }
+    ISG_CUDA(cudaMemcpyAsync(dst_slots, slots.data(), slots.size() * sizeof(Slot), cudaMemcpyHostToDevice, m->stream));
+    ISG_CUDA(cudaMemcpyAsync(dst_count, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice, m->stream));
+    // the host vectors die at return: make the copies complete first
+    ISG_CUDA(cudaStreamSynchronize(m->stream));
+    return ISING_OK;
+}
+
+// the mesh's query stencil (local energies, reductions); sweeps of a PT own theirs
+int upload_query_stencil(ising_mesh* m, const ising_params& p, bool legacy) {
+    return upload_stencil(m, p, legacy, m->d_slots, m->d_slot_count);
+}
+StencilDev stencil_of(const ising_mesh* m) { return StencilDev{m->d_slots, m->d_slot_count, m->lat.nsub}; }
+
+// SC fast path: D vectors per direction (+x,-x,+y,-y,+z,-z) and the specialisation kind.
+int sc_dmi(const ising_mesh* m, const ising_params& p, HamDev* h, int* kind) {
+    const Lattice& L = m->lat;
+    for (const auto& q : L.shell[0][0]) {
+        int k = q.dx == 1 ? 0 : q.dx == -1 ? 1 : q.dy == 1 ? 2 : q.dy == -1 ? 3 : q.dz == 1 ? 4 : 5;
+        double D[3] = {0, 0, 0};
+        if (p.Dz != 0.0) bond_dmi(L, p, q.r, D);
+        for (int c = 0; c < 3; ++c) h->D[k][c] = (float)D[c];
+    }
+    if (p.Dz == 0.0) { *kind = 0; return ISING_OK; }
+    const float d = (float)p.Dz;
+    auto eq = [](const float* a, float x, float y, float z) { return a[0] == x && a[1] == y && a[2] == z; };
+    const bool bulk = eq(h->D[0], -d, 0, 0) && eq(h->D[1], d, 0, 0) && eq(h->D[2], 0, -d, 0) &&
+                      eq(h->D[3], 0, d, 0) && eq(h->D[4], 0, 0, -d) && eq(h->D[5], 0, 0, d);
+    const bool intz = eq(h->D[0], 0, -d, 0) && eq(h->D[1], 0, d, 0) && eq(h->D[2], d, 0, 0) &&
+                      eq(h->D[3], -d, 0, 0) && eq(h->D[4], 0, 0, 0) && eq(h->D[5], 0, 0, 0);
+    // eq() compares exact floats; -0.0f == 0.0f holds, so sign-of-zero does not matter
+    *kind = bulk ? 1 : intz ? 2 : 3;
+    return ISING_OK;
+}
+
+int ensure_colouring(ising_mesh* m, bool shell2, Colouring** out) {
+    Colouring& c = m->colour[shell2 ? 1 : 0];
+    if (c.d_sites) { *out = &c; return ISING_OK; }
+    if (c.host_colour.empty()) {
+        int ncol = 0;
+        ISG_TRY(greedy_colouring(m->lat, shell2, &c.host_colour, &ncol));
+        c.ncol = ncol;
+    }
+    c.class_start.assign(c.ncol + 1, 0);
+    for (int v : c.host_colour) c.class_start[v + 1]++;
+    for (int k = 0; k < c.ncol; ++k) c.class_start[k + 1] += c.class_start[k];
+    std::vector<int> sites(m->lat.natoms);
+    std::vector<int> pos(c.class_start.begin(), c.class_start.end() - 1);
+    for (int64_t a = 0; a < m->lat.natoms; ++a) sites[pos[c.host_colour[a]]++] = (int)a;
+    ISG_TRY(dev_alloc(&c.d_sites, sites.size()));
+    ISG_CUDA(cudaMemcpy(c.d_sites, sites.data(), sites.size() * sizeof(int), cudaMemcpyHostToDevice));
+    *out = &c;
+    return ISING_OK;
+}
+
+// One sweep plan: which kernels to launch for a set of replicas.
+struct SweepPlan {
+    bool sc = false;
+    int dmi_kind = 0;
+    HamDev ham{};
+    Colouring* col = nullptr;
+    int slots_per_rep = 0;
+    Slot* d_slots = nullptr;   // general path: stencil buffers this plan reads
+    int* d_count = nullptr;
+};
+
+// Fills plan for Hamiltonian p; the general path uploads its stencil into (slots, count).
+int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots, int* count) {
+    plan->ham = make_ham(p);
+    const bool sh2 = uses_shell2(m->lat, p);
+    if (m->checkerboard && !sh2) {
+        plan->sc = true;
+        ISG_TRY(sc_dmi(m, p, &plan->ham, &plan->dmi_kind));
+        plan->slots_per_rep = sc_slots_per_rep(m->lat.nx, m->lat.ny, m->lat.nz);
+        return ISING_OK;
+    }
+    plan->sc = false;
+    plan->d_slots = slots;
+    plan->d_count = count;
+    ISG_TRY(upload_stencil(m, p, false, slots, count));
+    ISG_TRY(ensure_colouring(m, sh2, &plan->col));
+    int tot = 0;
+    for (int k = 0; k < plan->col->ncol; ++k)
+        tot += general_slots_for(plan->col->class_start[k + 1] - plan->col->class_start[k]);
+    plan->slots_per_rep = tot;
+    return ISING_OK;
+}
+
+// Enqueue one sweep (all colour classes) for replicas [rep_first, rep_first + n_rep).
+int enqueue_sweep(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_rep,
+                  const double* d_beta_rep, uint32_t sweep_offset, uint64_t seed, uint32_t ensemble,
+                  int move, double r, double* partials) {
+    const Lattice& L = m->lat;
+    float* base = m->d_spins + (int64_t)rep_first * 3 * L.natoms;
+    if (plan.sc) {
+        SweepLaunch a{};
+        a.spins = base; a.natoms = L.natoms; a.nx = L.nx; a.ny = L.ny; a.nz = L.nz;
+        a.n_rep = n_rep; a.rep_first = rep_first; a.beta_rep = d_beta_rep; a.sweep_ctr = m->d_sweep;
+        a.sweep_offset = sweep_offset; a.seed = seed; a.ensemble = ensemble; a.move = move;
+        a.r = (float)r; a.ham = plan.ham; a.dmi_kind = plan.dmi_kind; a.partials = partials;
+        a.slots_per_rep = plan.slots_per_rep; a.status = m->d_status;
+        for (int c = 0; c < 2; ++c) ISG_TRY(launch_sc_colour(a, c, m->stream));
+        return ISING_OK;
+    }
+    GeneralLaunch g{};
+    g.spins = base; g.natoms = L.natoms; g.nx = L.nx; g.ny = L.ny; g.nz = L.nz; g.nsub = L.nsub;
+    g.n_rep = n_rep; g.rep_first = rep_first; g.beta_rep = d_beta_rep; g.sweep_ctr = m->d_sweep;
+    g.sweep_offset = sweep_offset; g.seed = seed; g.ensemble = ensemble; g.move = move; g.r = (float)r;
+    g.ham = plan.ham; g.st = StencilDev{plan.d_slots, plan.d_count, L.nsub}; g.partials = partials;
+    g.slots_per_rep = plan.slots_per_rep;
+    g.status = m->d_status;
+    int slot = 0;
+    for (int k = 0; k < plan.col->ncol; ++k) {
+        g.sites = plan.col->d_sites + plan.col->class_start[k];
+        g.n_sites = plan.col->class_start[k + 1] - plan.col->class_start[k];
+        g.slot_base = slot;
+        ISG_TRY(launch_general_colour(g, m->stream));
+        slot += general_slots_for(g.n_sites);
+    }
+    return ISING_OK;
+}
+
+int check_replica(const ising_mesh* m, int replica) {
+    if (!m) return fail(ISING_ERR_ARG, "mesh is NULL");
+    if (m->device < 0) return fail(ISING_ERR_ARG, "mesh was created without a device (device = -1)");
+    if (replica < 0 || replica >= m->n_replicas) return fail(ISING_ERR_BOUNDS, "replica index out of range");
+    return ISING_OK;
+}
+
+// energy + magnetisation of replicas [first, first+n) into d_out[n][4] (device)
+int enqueue_energy(ising_mesh* m, const ising_params& p, int first, int n, double* d_out, double* d_tmp) {
+    ISG_TRY(upload_query_stencil(m, p, p.legacy_neighbours != 0));
+    ReduceLaunch a{};
+    a.spins = m->d_spins + (int64_t)first * 3 * m->lat.natoms;
+    a.natoms = m->lat.natoms; a.nx = m->lat.nx; a.ny = m->lat.ny; a.nz = m->lat.nz; a.nsub = m->lat.nsub;
+    a.n_rep = n; a.ham = make_ham(p); a.st = stencil_of(m); a.out = d_out; a.block_tmp = d_tmp;
+    a.blocks_per_rep = energy_blocks_for(m->lat.natoms);
+    return launch_energy_mag(a, m->stream);
+}
+
+int energy_tmp_doubles(const ising_mesh* m, int n) { return energy_blocks_for(m->lat.natoms) * n * 4; }
+
+}  // namespace
+
+// ======================================================================= unit cells
+extern "C" int ising_unit_cell(int kind, double* a, double* b, double* c, double* ab, double* bc,
+                               double* ca, float* frac, int* n) {
+    if (!a || !b || !c || !ab || !bc || !ca || !frac || !n) return fail(ISING_ERR_ARG, "NULL argument");
+    *ab = *bc = *ca = 90.0;
+    if (kind == ISING_CELL_SC) {
+        *a = *b = *c = 1.0;
+        frac[0] = frac[1] = frac[2] = 0.f;
+        *n = 1;
+        return ISING_OK;
+    }
+    if (kind == ISING_CELL_BCC) {  // src/unit_cells.f90:21-28
+        *a = *b = *c = 2.0;
+        const float f[6] = {0.f, 0.f, 0.f, 0.5f, 0.5f, 0.5f};
+        std::memcpy(frac, f, sizeof f);
+        *n = 2;
+        return ISING_OK;
+    }
+    if (kind == ISING_CELL_HYPER_KAGOME) {  // src/unit_cells.f90:47-76
+        *a = *b = *c = 6.0;
+        const float f[36] = {-0.5f, 0.0f, 0.5f,   -0.25f, 0.75f, 0.5f,  -0.5f, 0.75f, 0.25f,
+                             -0.25f, 0.25f, 0.0f, -0.5f, 0.25f, 0.75f,  -0.25f, 0.5f, 0.75f,
+                             -0.75f, 0.5f, 0.25f, 0.0f, 0.5f, 0.5f,     0.0f, 0.25f, 0.25f,
+                             -0.75f, 0.75f, 0.0f, 0.0f, 0.0f, 0.0f,     -0.75f, 0.0f, 0.75f};
+        std::memcpy(frac, f, sizeof f);
+        *n = 12;
+        return ISING_OK;
+    }
+    return fail(ISING_ERR_ARG, "unknown unit cell kind");
+}
+
+// ======================================================================= mesh
+extern "C" int ising_mesh_create(const float* frac, int nsub, int nx, int ny, int nz, double a, double b,
+                                 double c, double ab, double bc, double ca, double shell_tol, int n_shells,
+                                 int n_replicas, int device, ising_mesh** out) {
+    if (!out) return fail(ISING_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (n_replicas < 1) return fail(ISING_ERR_ARG, "n_replicas must be >= 1");
+    std::unique_ptr<ising_mesh> m(new ising_mesh());
+    ISG_TRY(build_lattice(frac, nsub, nx, ny, nz, a, b, c, ab, bc, ca, shell_tol, n_shells, &m->lat));
+    m->checkerboard = is_checkerboard_sc(m->lat);
+    if (device == -1) {  // lattice tables only
+        m->device = -1;
+        m->n_replicas = n_replicas;
+        *out = m.release();
+        return ISING_OK;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(ISING_ERR_CUDA, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(ISING_ERR_ARG, "device index out of range");
+    DeviceGuard g(device);
+    m->device = device;
+    m->n_replicas = n_replicas;
+    m->checkerboard = is_checkerboard_sc(m->lat);
+    ISG_CUDA(cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking));
+    m->stream = m->own_stream;
+    const int64_t N = m->lat.natoms;
+    ISG_TRY(dev_alloc(&m->d_spins, (size_t)n_replicas * 3 * N));
+    ISG_TRY(dev_alloc(&m->d_sweep, n_replicas));
+    ISG_TRY(dev_alloc(&m->d_beta, n_replicas));
+    ISG_TRY(dev_alloc(&m->d_scratch, kScratchDoubles));
+    ISG_TRY(dev_alloc(&m->d_status, 1));
+    ISG_TRY(dev_alloc(&m->d_slots, (size_t)kMaxSub * kMaxSlots));
+    ISG_TRY(dev_alloc(&m->d_slot_count, kMaxSub));
+    ISG_TRY(dev_alloc(&m->d_plaq, 16));
+    ISG_TRY(dev_alloc(&m->d_winding_tmp, (size_t)n_replicas * nz));
+    ISG_CUDA(cudaMallocHost((void**)&m->h_pinned, kScratchDoubles * sizeof(double)));
+    ISG_CUDA(cudaMemset(m->d_spins, 0, (size_t)n_replicas * 3 * N * sizeof(float)));
+    ISG_CUDA(cudaMemset(m->d_sweep, 0, n_replicas * sizeof(uint32_t)));
+    ISG_CUDA(cudaMemset(m->d_status, 0, sizeof(int)));
+    m->h_sweep.assign(n_replicas, 0u);
+    // winding plaquette: s1 = first atom of the cell (last unit-cell atom, linked-list head,
+    // src/chainMesh.f90:663-671), s2 = +a of s1, s4 = +b of s2, s3 = +b of s1 (rsp:344-347)
+    {
+        const Lattice& L = m->lat;
+        const int s1 = L.nsub - 1;
+        const NbrSlot& a2 = L.deriv[s1 * 6 + 0 * 2 + 1];
+        const NbrSlot& a4 = L.deriv[a2.sub * 6 + 1 * 2 + 1];
+        const NbrSlot& a3 = L.deriv[s1 * 6 + 1 * 2 + 1];
+        const int plaq[16] = {0, 0, 0, s1,
+                              a2.dx, a2.dy, a2.dz, a2.sub,
+                              a2.dx + a4.dx, a2.dy + a4.dy, a2.dz + a4.dz, a4.sub,
+                              a3.dx, a3.dy, a3.dz, a3.sub};
+        ISG_CUDA(cudaMemcpy(m->d_plaq, plaq, sizeof plaq, cudaMemcpyHostToDevice));
+    }
+    *out = m.release();
+    return ISING_OK;
+}
+
+extern "C" int ising_mesh_destroy(ising_mesh* m) {
+    if (!m) return ISING_OK;
+    if (m->device < 0) { delete m; return ISING_OK; }
+    DeviceGuard g(m->device);
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    cudaFree(m->d_spins); cudaFree(m->d_sweep); cudaFree(m->d_scratch); cudaFree(m->d_status);
+    cudaFree(m->d_staging); cudaFree(m->d_beta); cudaFree(m->d_winding_tmp); cudaFree(m->d_slots); cudaFree(m->d_slot_count);
+    cudaFree(m->d_plaq);
+    for (auto& c : m->colour) cudaFree(c.d_sites);
+    if (m->h_pinned) cudaFreeHost(m->h_pinned);
+    if (m->own_stream) cudaStreamDestroy(m->own_stream);
+    delete m;
+    return ISING_OK;
+}
+
+extern "C" int ising_mesh_get_info(const ising_mesh* m, ising_mesh_info* info) {
+    if (!m || !info) return fail(ISING_ERR_ARG, "NULL argument");
+    const Lattice& L = m->lat;
+    std::memset(info, 0, sizeof *info);
+    info->num_atoms = L.natoms; info->num_cells = L.ncells;
+    info->nx = L.nx; info->ny = L.ny; info->nz = L.nz; info->n_sub = L.nsub;
+    info->n_shells = L.nshells; info->n_replicas = m->n_replicas;
+    info->shell_size[0] = (int)L.shell[0][0].size();
+    info->shell_size[1] = (int)L.shell[1][0].size();
+    info->checkerboard = m->checkerboard ? 1 : 0;
+    for (int k = 0; k < 3; ++k) { info->a_vec[k] = L.av[k]; info->b_vec[k] = L.bv[k]; info->c_vec[k] = L.cv[k]; }
+    return ISING_OK;
+}
+
+extern "C" int ising_mesh_set_stream(ising_mesh* m, void* stream) {
+    if (!m) return fail(ISING_ERR_ARG, "mesh is NULL");
+    if (m->device < 0) return fail(ISING_ERR_ARG, "mesh was created without a device (device = -1)");
+    DeviceGuard g(m->device);
+    // order the switch: work already issued on the old stream completes first
+    ISG_CUDA(cudaStreamSynchronize(m->stream));
+    m->stream = stream ? static_cast<cudaStream_t>(stream) : m->own_stream;
+    return ISING_OK;
+}
+
+extern "C" int ising_mesh_positions(const ising_mesh* m, float* xyz) {
+    if (!m || !xyz) return fail(ISING_ERR_ARG, "NULL argument");
+    for (int64_t a = 0; a < m->lat.natoms; ++a) m->lat.position(a, xyz + 3 * a);
+    return ISING_OK;
+}
+
+extern "C" int ising_mesh_neighbours(const ising_mesh* m, int64_t atom, int shell, int64_t* out, int cap, int* n) {
+    if (!m || !n) return fail(ISING_ERR_ARG, "NULL argument");
+    const Lattice& L = m->lat;
+    if (atom < 0 || atom >= L.natoms) return fail(ISING_ERR_BOUNDS, "atom index out of range");
+    if (shell < -1 || shell > 1) return fail(ISING_ERR_ARG, "shell must be -1, 0 or 1");
+    int ix, iy, iz, s;
+    L.cell_of(atom, &ix, &iy, &iz, &s);
+    const auto& lst = shell < 0 ? L.legacy[s] : L.shell[shell][s];
+    *n = (int)lst.size();
+    for (int q = 0; q < *n && q < cap; ++q) out[q] = L.neighbour_atom(atom, lst[q]);
+    return ISING_OK;
+}
+
+extern "C" int ising_mesh_derivative_list(const ising_mesh* m, int64_t* out) {
+    if (!m || !out) return fail(ISING_ERR_ARG, "NULL argument");
+    const Lattice& L = m->lat;
+    for (int64_t a = 0; a < L.natoms; ++a) {
+        int ix, iy, iz, s;
+        L.cell_of(a, &ix, &iy, &iz, &s);
+        for (int d = 0; d < 6; ++d) out[a * 6 + d] = L.neighbour_atom(a, L.deriv[s * 6 + d]);
+    }
+    return ISING_OK;
+}
+
+extern "C" int ising_mesh_colouring(ising_mesh* m, const ising_params* p, int* colour_of, int* n_colours) {
+    if (!m || !colour_of || !n_colours) return fail(ISING_ERR_ARG, "NULL argument");
+    ISG_TRY(validate_params(p));
+    const Lattice& L = m->lat;
+    const bool sh2 = uses_shell2(L, *p);
+    if (m->checkerboard && !sh2) {
+        for (int64_t a = 0; a < L.natoms; ++a) {
+            int ix, iy, iz, s;
+            L.cell_of(a, &ix, &iy, &iz, &s);
+            colour_of[a] = (ix + iy + iz) & 1;
+        }
+        *n_colours = 2;
+        return ISING_OK;
+    }
+    Colouring& c = m->colour[sh2 ? 1 : 0];
+    if (c.host_colour.empty()) {
+        int ncol = 0;
+        ISG_TRY(greedy_colouring(L, sh2, &c.host_colour, &ncol));
+        c.ncol = ncol;
+    }
+    std::memcpy(colour_of, c.host_colour.data(), L.natoms * sizeof(int));
+    *n_colours = c.ncol;
+    return ISING_OK;
+}
+
+// ======================================================================= spins
+namespace {
+int staging(ising_mesh* m, double** d) {
+    // FP64 staging for 3N doubles, allocated on first use
+    const size_t need = (size_t)3 * m->lat.natoms;
+    if (m->staging_size < need) {
+        cudaFree(m->d_staging);
+        m->d_staging = nullptr;
+        m->staging_size = 0;
+        ISG_TRY(dev_alloc(&m->d_staging, need));
+        m->staging_size = need;
+    }
+    *d = m->d_staging;
+    return ISING_OK;
+}
+}  // namespace
+
+extern "C" int ising_spins_set(ising_mesh* m, int replica, const double* s) {
+    ISG_TRY(check_replica(m, replica));
+    if (!s) return fail(ISING_ERR_ARG, "spins array is NULL");
+    DeviceGuard g(m->device);
+    double* d;
+    ISG_TRY(staging(m, &d));
+    const int64_t N = m->lat.natoms;
+    ISG_CUDA(cudaMemcpyAsync(d, s, (size_t)3 * N * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+    ISG_TRY(launch_spins_from_f64(d, m->d_spins + (int64_t)replica * 3 * N, N, m->d_status, m->stream));
+    return check_status(m);
+}
+
+extern "C" int ising_spins_get(const ising_mesh* mc, int replica, double* s) {
+    ising_mesh* m = const_cast<ising_mesh*>(mc);
+    ISG_TRY(check_replica(m, replica));
+    if (!s) return fail(ISING_ERR_ARG, "spins array is NULL");
+    DeviceGuard g(m->device);
+    double* d;
+    ISG_TRY(staging(m, &d));
+    const int64_t N = m->lat.natoms;
+    ISG_TRY(launch_spins_to_f64(m->d_spins + (int64_t)replica * 3 * N, d, N, m->stream));
+    ISG_CUDA(cudaMemcpyAsync(s, d, (size_t)3 * N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    ISG_CUDA(cudaStreamSynchronize(m->stream));
+    return ISING_OK;
+}
+
+extern "C" int ising_spins_init_uniform(ising_mesh* m, uint64_t seed, uint32_t ensemble) {
+    ISG_TRY(check_replica(m, 0));
+    if (ensemble >= (1u << 24)) return fail(ISING_ERR_ARG, "ensemble id must be < 2^24");
+    DeviceGuard g(m->device);
+    ISG_TRY(launch_init_uniform(m->d_spins, m->lat.natoms, m->n_replicas, seed, ensemble, m->stream));
+    ISG_CUDA(cudaStreamSynchronize(m->stream));
+    return ISING_OK;
+}
+
+// ======================================================================= params
+extern "C" int ising_params_reference(int which, double J, double Jp, double Dz, double Dzp, double B,
+                                      ising_params* p) {
+    if (!p) return fail(ISING_ERR_ARG, "params is NULL");
+    std::memset(p, 0, sizeof *p);
+    p->J = J; p->J_prime = Jp; p->Dz = Dz; p->Dz_prime = Dzp; p->B = B;
+    p->K_axis[2] = 1.0;
+    p->dmi_mode = ISING_DMI_INTERFACIAL;
+    if (which == 0) {           // calculateHeisenbergEnergy / Metropolis_mcs
+        p->zeeman_factor = 1.0;
+        p->include_Jp = 1;
+    } else if (which == 1) {    // TotalHeisenbergEnergy
+        p->zeeman_factor = 2.0; // g * mu_B (src/constants.f90:11,14)
+        p->include_Jp = 0;
+        p->dmi_axis[2] = 1.0;   // [0, 0, Dz] (src/energyMin.f90:198)
+        p->legacy_neighbours = 1;
+    } else {
+        return fail(ISING_ERR_ARG, "which must be 0 or 1");
+    }
+    return ISING_OK;
+}
+
+// ======================================================================= energies
+extern "C" int ising_local_energy_batch(const ising_mesh* mc, int replica, int n, const int64_t* atoms,
+                                        const double* sprop, const ising_params* p, double* old_e, double* new_e) {
+    ising_mesh* m = const_cast<ising_mesh*>(mc);
+    ISG_TRY(check_replica(m, replica));
+    ISG_TRY(validate_params(p));
+    if (n < 0 || (n > 0 && (!atoms || !sprop || !old_e || !new_e))) return fail(ISING_ERR_ARG, "bad batch arguments");
+    for (int i = 0; i < n; ++i) {
+        if (atoms[i] < 0 || atoms[i] >= m->lat.natoms) return fail(ISING_ERR_BOUNDS, "atom index out of range");
+        for (int k = 0; k < 3; ++k)
+            if (!std::isfinite(sprop[3 * i + k])) return fail(ISING_ERR_NAN, "NaN in proposed spin");
+    }
+    if (n == 0) return ISING_OK;
+    DeviceGuard g(m->device);
+    // scratch layout: atoms (n int64 as doubles), sprop (3n), old (n), new (n)
+    const int chunk = kScratchDoubles / 6;
+    ISG_TRY(upload_query_stencil(m, *p, false));
+    for (int off = 0; off < n; off += chunk) {
+        const int k = std::min(chunk, n - off);
+        int64_t* d_atoms = reinterpret_cast<int64_t*>(m->d_scratch);
+        double* d_sp = m->d_scratch + k;
+        double* d_old = d_sp + 3 * k;
+        double* d_new = d_old + k;
+        std::memcpy(m->h_pinned, atoms + off, k * sizeof(int64_t));
+        std::memcpy(m->h_pinned + k, sprop + 3 * off, 3 * k * sizeof(double));
+        ISG_CUDA(cudaMemcpyAsync(m->d_scratch, m->h_pinned, 4 * k * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+        LocalLaunch a{};
+        a.spins = m->d_spins + (int64_t)replica * 3 * m->lat.natoms;
+        a.natoms = m->lat.natoms; a.nx = m->lat.nx; a.ny = m->lat.ny; a.nz = m->lat.nz; a.nsub = m->lat.nsub;
+        a.ham = make_ham(*p); a.st = stencil_of(m); a.atoms = d_atoms; a.sprop = d_sp; a.old_e = d_old; a.new_e = d_new; a.n = k;
+        ISG_TRY(launch_local_energy(a, m->stream));
+        ISG_CUDA(cudaMemcpyAsync(m->h_pinned + 4 * k, d_old, 2 * k * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+        ISG_CUDA(cudaStreamSynchronize(m->stream));
+        std::memcpy(old_e + off, m->h_pinned + 4 * k, k * sizeof(double));
+        std::memcpy(new_e + off, m->h_pinned + 5 * k, k * sizeof(double));
+    }
+    return ISING_OK;
+}
+
+extern "C" int ising_local_energy(const ising_mesh* m, int replica, int atom_1based, const ising_params* p,
+                                  const double s_prop[3], double* old_e, double* new_e) {
+    if (!m) return fail(ISING_ERR_ARG, "mesh is NULL");
+    if (!s_prop || !old_e || !new_e) return fail(ISING_ERR_ARG, "NULL argument");
+    if (atom_1based < 1 || atom_1based > m->lat.natoms) return fail(ISING_ERR_BOUNDS, "atomIndex out of range");
+    const int64_t a = atom_1based - 1;
+    return ising_local_energy_batch(m, replica, 1, &a, s_prop, p, old_e, new_e);
+}
+
+extern "C" int ising_observables(const ising_mesh* mc, const ising_params* p, double* e, double* mv) {
+    ising_mesh* m = const_cast<ising_mesh*>(mc);
+    ISG_TRY(check_replica(m, 0));
+    ISG_TRY(validate_params(p));
+    DeviceGuard g(m->device);
+    const int R = m->n_replicas;
+    const int tmp = energy_tmp_doubles(m, R);
+    double* d_tmp = nullptr;
+    ISG_TRY(dev_alloc(&d_tmp, (size_t)tmp + 4 * R));
+    int st = enqueue_energy(m, *p, 0, R, d_tmp + tmp, d_tmp);
+    std::vector<double> h(4 * R);
+    if (st == ISING_OK) {
+        cudaError_t ce = cudaMemcpyAsync(h.data(), d_tmp + tmp, 4 * R * sizeof(double), cudaMemcpyDeviceToHost, m->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(m->stream);
+        if (ce != cudaSuccess) st = cuda_fail(ce, "observables copy");
+    }
+    cudaFree(d_tmp);
+    if (st != ISING_OK) return st;
+    for (int r = 0; r < R; ++r) {
+        if (e) e[r] = h[4 * r];
+        if (mv) for (int k = 0; k < 3; ++k) mv[3 * r + k] = h[4 * r + 1 + k];
+    }
+    return ISING_OK;
+}
+
+extern "C" int ising_total_energy(const ising_mesh* mc, int replica, const ising_params* p, double* e) {
+    ising_mesh* m = const_cast<ising_mesh*>(mc);
+    ISG_TRY(check_replica(m, replica));
+    ISG_TRY(validate_params(p));
+    if (!e) return fail(ISING_ERR_ARG, "e is NULL");
+    DeviceGuard g(m->device);
+    const int tmp = energy_tmp_doubles(m, 1);
+    double* d_tmp = nullptr;
+    ISG_TRY(dev_alloc(&d_tmp, (size_t)tmp + 4));
+    int st = enqueue_energy(m, *p, replica, 1, d_tmp + tmp, d_tmp);
+    double h[4] = {0, 0, 0, 0};
+    if (st == ISING_OK) {
+        cudaError_t ce = cudaMemcpyAsync(h, d_tmp + tmp, 4 * sizeof(double), cudaMemcpyDeviceToHost, m->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(m->stream);
+        if (ce != cudaSuccess) st = cuda_fail(ce, "energy copy");
+    }
+    cudaFree(d_tmp);
+    if (st != ISING_OK) return st;
+    *e = h[0];
+    return ISING_OK;
+}
+
+// ======================================================================= sweeps
+extern "C" int ising_metropolis_mcs(ising_mesh* m, int replica, double beta, int n_sweeps, const ising_params* p,
+                                    double r, uint64_t seed) {
+    ISG_TRY(check_replica(m, replica));
+    ISG_TRY(validate_params(p));
+    if (n_sweeps < 0) return fail(ISING_ERR_ARG, "numMCSSweeps must be >= 0");
+    if (!std::isfinite(beta) || !std::isfinite(r)) return fail(ISING_ERR_NAN, "non-finite beta or r");
+    if (n_sweeps == 0) return ISING_OK;
+    DeviceGuard g(m->device);
+    SweepPlan plan;
+    ISG_TRY(make_plan(m, *p, &plan, m->d_slots, m->d_slot_count));
+    const int move = r > 0.0 ? 1 : 0;
+    m->h_pinned[0] = beta;
+    ISG_CUDA(cudaMemcpyAsync(m->d_beta + replica, m->h_pinned, sizeof(double), cudaMemcpyHostToDevice, m->stream));
+    for (int sw = 0; sw < n_sweeps; ++sw)
+        ISG_TRY(enqueue_sweep(m, plan, replica, 1, m->d_beta, (uint32_t)sw, seed, 0u, move, r, nullptr));
+    ISG_TRY(launch_advance(m->d_sweep + replica, 1, (uint32_t)n_sweeps, m->stream));
+    m->h_sweep[replica] += (uint32_t)n_sweeps;
+    return check_status(m);
+}
+
+// ======================================================================= winding
+extern "C" int ising_winding_all_slices(const ising_mesh* mc, int replica, double* q) {
+    ising_mesh* m = const_cast<ising_mesh*>(mc);
+    ISG_TRY(check_replica(m, replica));
+    if (!q) return fail(ISING_ERR_ARG, "q is NULL");
+    DeviceGuard g(m->device);
+    const Lattice& L = m->lat;
+    WindingLaunch w{};
+    w.spins = m->d_spins + (int64_t)replica * 3 * L.natoms;
+    w.natoms = L.natoms; w.nx = L.nx; w.ny = L.ny; w.nz = L.nz; w.nsub = L.nsub; w.n_rep = 1;
+    w.plaq = m->d_plaq; w.out = m->d_winding_tmp; w.fp64 = 1;
+    ISG_TRY(launch_winding(w, m->stream));
+    ISG_CUDA(cudaMemcpyAsync(q, m->d_winding_tmp, L.nz * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    ISG_CUDA(cudaStreamSynchronize(m->stream));
+    return ISING_OK;
+}
+
+extern "C" int ising_winding_number(const ising_mesh* m, int replica, int z1, double* q) {
+    if (!m) return fail(ISING_ERR_ARG, "mesh is NULL");
+    if (z1 < 1 || z1 > m->lat.nz) return fail(ISING_ERR_BOUNDS, "Z_index out of bounds");
+    if (!q) return fail(ISING_ERR_ARG, "q is NULL");
+    std::vector<double> all(m->lat.nz);
+    ISG_TRY(ising_winding_all_slices(m, replica, all.data()));
+    *q = all[z1 - 1];
+    return ISING_OK;
+}
+
+extern "C" int ising_statistics(const ising_mesh* m, int replica, double* wnd_mid, double* wnd_spread, double mv[3]) {
+    ISG_TRY(check_replica(m, replica));
+    if (m->lat.nz < 2) return fail(ISING_ERR_BOUNDS, "numCellsZ/2 is 0");
+    std::vector<double> all(m->lat.nz);
+    ISG_TRY(ising_winding_all_slices(m, replica, all.data()));
+    const double mx = *std::max_element(all.begin(), all.end());
+    const double mn = *std::min_element(all.begin(), all.end());
+    if (wnd_spread) *wnd_spread = std::fabs(mx - mn);
+    if (wnd_mid) *wnd_mid = all[m->lat.nz / 2 - 1];
+    if (mv) {
+        ising_params p{};
+        p.zeeman_factor = 1.0;
+        std::vector<double> e(m->n_replicas), mm(3 * m->n_replicas);
+        ISG_TRY(ising_observables(m, &p, e.data(), mm.data()));
+        for (int k = 0; k < 3; ++k) mv[k] = mm[3 * replica + k] / (double)m->lat.natoms;
+    }
+    return ISING_OK;
+}
+
+// plaquette density (rsp:438-500) computed on the host from downloaded spins
+extern "C" int ising_winding_density(const ising_mesh* m, int replica, int z1, double* dens) {
+    ISG_TRY(check_replica(m, replica));
+    if (z1 < 1 || z1 > m->lat.nz) return fail(ISING_ERR_BOUNDS, "Z_index out of bounds");
+    if (!dens) return fail(ISING_ERR_ARG, "density is NULL");
+    const Lattice& L = m->lat;
+    std::vector<double> s((size_t)3 * L.natoms);
+    ISG_TRY(ising_spins_get(m, replica, s.data()));
+    const int64_t N = L.natoms;
+    auto unit = [&](int64_t j, double* o) {
+        const double x = s[j], y = s[N + j], z = s[2 * N + j];
+        const double n = std::sqrt(x * x + y * y + z * z);
+        o[0] = x / n; o[1] = y / n; o[2] = z / n;
+    };
+    auto arc = [](const double* s1, const double* s2, const double* s3) {
+        const double d12 = s1[0] * s2[0] + s1[1] * s2[1] + s1[2] * s2[2];
+        const double d23 = s2[0] * s3[0] + s2[1] * s3[1] + s2[2] * s3[2];
+        const double d31 = s3[0] * s1[0] + s3[1] * s1[1] + s3[2] * s1[2];
+        const double cx = s2[1] * s3[2] - s2[2] * s3[1], cy = s2[2] * s3[0] - s2[0] * s3[2],
+                     cz = s2[0] * s3[1] - s2[1] * s3[0];
+        double re = 1.0 + d12 + d23 + d31, im = s1[0] * cx + s1[1] * cy + s1[2] * cz;
+        const double nrm = std::sqrt(2.0 * (1.0 + d12) * (1.0 + d23) * (1.0 + d31));
+        re /= nrm; im /= nrm;
+        return 2.0 * std::atan2(im, re);
+    };
+    const int s1sub = L.nsub - 1;
+    const NbrSlot& a2 = L.deriv[s1sub * 6 + 1];
+    const NbrSlot& a4 = L.deriv[a2.sub * 6 + 3];
+    const NbrSlot& a3 = L.deriv[s1sub * 6 + 3];
+    const double four_pi = 4.0 * (double)3.14159265358979323846f;
+    for (int i = 0; i < L.nx; ++i)
+        for (int j = 0; j < L.ny; ++j) {
+            const int64_t b1 = L.atom_of(i, j, z1 - 1, s1sub);
+            const int64_t b2 = L.neighbour_atom(b1, a2);
+            const int64_t b4 = L.neighbour_atom(b2, a4);
+            const int64_t b3 = L.neighbour_atom(b1, a3);
+            double v1[3], v2[3], v3[3], v4[3];
+            unit(b1, v1); unit(b2, v2); unit(b3, v3); unit(b4, v4);
+            dens[i + (int64_t)j * L.nx] = (arc(v1, v2, v4) + arc(v1, v4, v3)) / four_pi;
+        }
+    return ISING_OK;
+}
+
+// ======================================================================= parallel tempering
+struct ising_pt {
+    ising_mesh* mesh = nullptr;
+    int n = 0;
+    ising_params p{};
+    ising_pt_options opt{};
+    SweepPlan plan;
+    double* d_beta_t = nullptr;
+    double* d_beta_rep = nullptr;
+    int* d_t2r = nullptr;
+    int* d_r2t = nullptr;
+    Acc4* d_acc = nullptr;
+    double* d_partials = nullptr;
+    unsigned long long* d_stats = nullptr;
+    uint32_t* d_round = nullptr;
+    double* d_series = nullptr;
+    int* d_count = nullptr;
+    double* d_q = nullptr;
+    double* d_energy_tmp = nullptr;
+    double* d_energy_out = nullptr;
+    Slot* d_plan_slots = nullptr;
+    int* d_plan_count = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_k = -1;
+    int rounds_done = 0;
+};
+
+namespace {
+void pt_free(ising_pt* pt) {
+    if (pt->graph) cudaGraphExecDestroy(pt->graph);
+    cudaFree(pt->d_beta_t); cudaFree(pt->d_beta_rep); cudaFree(pt->d_t2r); cudaFree(pt->d_r2t);
+    cudaFree(pt->d_acc); cudaFree(pt->d_partials); cudaFree(pt->d_stats); cudaFree(pt->d_round);
+    cudaFree(pt->d_series); cudaFree(pt->d_count); cudaFree(pt->d_q); cudaFree(pt->d_energy_tmp);
+    cudaFree(pt->d_energy_out); cudaFree(pt->d_plan_slots); cudaFree(pt->d_plan_count);
+}
+
+int pt_resync_enqueue(ising_pt* pt) {
+    ising_mesh* m = pt->mesh;
+    ISG_TRY(enqueue_energy(m, pt->p, 0, pt->n, pt->d_energy_out, pt->d_energy_tmp));
+    ISG_CUDA(cudaMemcpyAsync(pt->d_acc, pt->d_energy_out, (size_t)pt->n * 4 * sizeof(double),
+                             cudaMemcpyDeviceToDevice, m->stream));
+    return ISING_OK;
+}
+
+// Enqueue one PT round: k sweeps of replicas 0..n-1 (recording after each sweep when asked),
+// fold the per-block partial sums into the FP64 accumulators, exchange, advance counters.
+int pt_enqueue_round(ising_pt* pt, int k) {
+    ising_mesh* m = pt->mesh;
+    const int n = pt->n;
+    const int move = pt->opt.move;
+    for (int sw = 0; sw < k; ++sw) {
+        ISG_TRY(enqueue_sweep(m, pt->plan, 0, n, pt->d_beta_rep, (uint32_t)sw, pt->opt.seed, pt->opt.ensemble, move,
+                              pt->opt.r, pt->d_partials));
+        if (pt->opt.record) {
+            ISG_TRY(launch_fold_partials(pt->d_partials, pt->plan.slots_per_rep, n, pt->d_acc, m->stream));
+            WindingLaunch w{};
+            w.spins = m->d_spins; w.natoms = m->lat.natoms; w.nx = m->lat.nx; w.ny = m->lat.ny; w.nz = m->lat.nz;
+            w.nsub = m->lat.nsub; w.n_rep = n; w.plaq = m->d_plaq; w.out = pt->d_q; w.fp64 = 0;
+            ISG_TRY(launch_winding(w, m->stream));
+            RecordLaunch rl{};
+            rl.acc = pt->d_acc; rl.q = pt->d_q; rl.t2r = pt->d_t2r; rl.nz = m->lat.nz; rl.n_rep = n;
+            rl.natoms = m->lat.natoms; rl.series = pt->d_series; rl.cap = pt->opt.record_capacity; rl.count = pt->d_count;
+            ISG_TRY(launch_record(rl, m->stream));
+        }
+    }
+    if (!pt->opt.record)
+        ISG_TRY(launch_fold_partials(pt->d_partials, pt->plan.slots_per_rep, n, pt->d_acc, m->stream));
+    ExchangeLaunch ex{};
+    ex.n = n; ex.beta_t = pt->d_beta_t; ex.beta_rep = pt->d_beta_rep; ex.t2r = pt->d_t2r; ex.r2t = pt->d_r2t;
+    ex.acc = pt->d_acc; ex.stats = pt->d_stats; ex.round = pt->d_round; ex.seed = pt->opt.seed;
+    ex.ensemble = pt->opt.ensemble; ex.scheme = pt->opt.scheme;
+    ISG_TRY(launch_exchange(ex, m->stream));
+    ISG_TRY(launch_advance(m->d_sweep, n, (uint32_t)k, m->stream));
+    return ISING_OK;
+}
+}  // namespace
+
+extern "C" int ising_pt_create(ising_mesh* m, int n, const double* betas, const ising_params* p,
+                               const ising_pt_options* opt, ising_pt** out) {
+    if (!out) return fail(ISING_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!m || !betas || !opt) return fail(ISING_ERR_ARG, "NULL argument");
+    ISG_TRY(check_replica(m, 0));
+    ISG_TRY(validate_params(p));
+    if (n < 1 || n > m->n_replicas) return fail(ISING_ERR_ARG, "n_temps must be in 1..n_replicas");
+    for (int t = 0; t < n; ++t) if (!std::isfinite(betas[t])) return fail(ISING_ERR_NAN, "non-finite beta");
+    if (opt->move != ISING_MOVE_UNIFORM && opt->move != ISING_MOVE_BALL) return fail(ISING_ERR_ARG, "bad move");
+    if (opt->scheme != ISING_PT_EVEN_ODD && opt->scheme != ISING_PT_RANDOM_PAIRS) return fail(ISING_ERR_ARG, "bad scheme");
+    if (opt->ensemble >= (1u << 24)) return fail(ISING_ERR_ARG, "ensemble id must be < 2^24");
+    if (opt->record && opt->record_capacity < 1) return fail(ISING_ERR_ARG, "record_capacity must be >= 1");
+    DeviceGuard g(m->device);
+    std::unique_ptr<ising_pt> pt(new ising_pt());
+    pt->mesh = m; pt->n = n; pt->p = *p; pt->opt = *opt;
+    auto bail = [&](int s) { pt_free(pt.get()); return s; };
+    int st = ISING_OK;
+    if ((st = dev_alloc(&pt->d_plan_slots, (size_t)kMaxSub * kMaxSlots)) ||
+        (st = dev_alloc(&pt->d_plan_count, kMaxSub)))
+        return bail(st);
+    if ((st = make_plan(m, *p, &pt->plan, pt->d_plan_slots, pt->d_plan_count)) != ISING_OK) return bail(st);
+    const int tmp = energy_tmp_doubles(m, n);
+    if ((st = dev_alloc(&pt->d_beta_t, n)) || (st = dev_alloc(&pt->d_beta_rep, m->n_replicas)) ||
+        (st = dev_alloc(&pt->d_t2r, n)) || (st = dev_alloc(&pt->d_r2t, n)) || (st = dev_alloc(&pt->d_acc, n)) ||
+        (st = dev_alloc(&pt->d_partials, (size_t)n * pt->plan.slots_per_rep * 4)) ||
+        (st = dev_alloc(&pt->d_stats, 2 * (size_t)n)) || (st = dev_alloc(&pt->d_round, 1)) ||
+        (st = dev_alloc(&pt->d_count, 1)) || (st = dev_alloc(&pt->d_q, (size_t)n * m->lat.nz)) ||
+        (st = dev_alloc(&pt->d_energy_tmp, tmp)) || (st = dev_alloc(&pt->d_energy_out, 4 * (size_t)n)))
+        return bail(st);
+    if (opt->record && (st = dev_alloc(&pt->d_series, (size_t)n * opt->record_capacity * 4))) return bail(st);
+    std::vector<int> ident(n);
+    for (int t = 0; t < n; ++t) ident[t] = t;
+    cudaError_t ce = cudaMemcpy(pt->d_beta_t, betas, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaMemcpy(pt->d_beta_rep, betas, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaMemcpy(pt->d_t2r, ident.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaMemcpy(pt->d_r2t, ident.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaMemset(pt->d_partials, 0, (size_t)n * pt->plan.slots_per_rep * 4 * sizeof(double));
+    if (ce == cudaSuccess) ce = cudaMemset(pt->d_stats, 0, 2 * (size_t)n * sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = cudaMemset(pt->d_round, 0, sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = cudaMemset(pt->d_count, 0, sizeof(int));
+    if (ce != cudaSuccess) return bail(cuda_fail(ce, "pt init"));
+    if ((st = pt_resync_enqueue(pt.get())) != ISING_OK) return bail(st);
+    if ((ce = cudaStreamSynchronize(m->stream)) != cudaSuccess) return bail(cuda_fail(ce, "pt init sync"));
+    *out = pt.release();
+    return ISING_OK;
+}
+
+extern "C" int ising_pt_destroy(ising_pt* pt) {
+    if (!pt) return ISING_OK;
+    DeviceGuard g(pt->mesh->device);
+    cudaStreamSynchronize(pt->mesh->stream);
+    pt_free(pt);
+    delete pt;
+    return ISING_OK;
+}
+
+extern "C" int ising_pt_run(ising_pt* pt, int k, int rounds) {
+    if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
+    if (k < 1 || rounds < 0) return fail(ISING_ERR_ARG, "sweeps_per_swap must be >= 1 and rounds >= 0");
+    ising_mesh* m = pt->mesh;
+    DeviceGuard g(m->device);
+    if (pt->graph_k != k) {
+        if (pt->graph) { cudaGraphExecDestroy(pt->graph); pt->graph = nullptr; }
+        cudaGraph_t graph;
+        ISG_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+        int st = pt_enqueue_round(pt, k);
+        cudaError_t ce = cudaStreamEndCapture(m->stream, &graph);
+        if (st != ISING_OK) { if (ce == cudaSuccess) cudaGraphDestroy(graph); return st; }
+        ISG_CUDA(ce);
+        ce = cudaGraphInstantiate(&pt->graph, graph, 0);
+        cudaGraphDestroy(graph);
+        ISG_CUDA(ce);
+        pt->graph_k = k;
+    }
+    for (int r = 0; r < rounds; ++r) {
+        ISG_CUDA(cudaGraphLaunch(pt->graph, m->stream));
+        ++pt->rounds_done;
+        if (pt->opt.resync_every > 0 && pt->rounds_done % pt->opt.resync_every == 0) ISG_TRY(pt_resync_enqueue(pt));
+    }
+    return check_status(m);
+}
+
+extern "C" int ising_pt_relax(ising_pt* pt, int n_sweeps) {
+    if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
+    if (n_sweeps < 0) return fail(ISING_ERR_ARG, "n_sweeps must be >= 0");
+    ising_mesh* m = pt->mesh;
+    DeviceGuard g(m->device);
+    for (int sw = 0; sw < n_sweeps; ++sw)
+        ISG_TRY(enqueue_sweep(m, pt->plan, 0, pt->n, pt->d_beta_rep, (uint32_t)sw, pt->opt.seed, pt->opt.ensemble,
+                              pt->opt.move, pt->opt.r, pt->d_partials));
+    ISG_TRY(launch_fold_partials(pt->d_partials, pt->plan.slots_per_rep, pt->n, pt->d_acc, m->stream));
+    ISG_TRY(launch_advance(m->d_sweep, pt->n, (uint32_t)n_sweeps, m->stream));
+    return check_status(m);
+}
+
+extern "C" int ising_pt_permutation(const ising_pt* pt, int* t2r) {
+    if (!pt || !t2r) return fail(ISING_ERR_ARG, "NULL argument");
+    DeviceGuard g(pt->mesh->device);
+    ISG_CUDA(cudaMemcpyAsync(t2r, pt->d_t2r, pt->n * sizeof(int), cudaMemcpyDeviceToHost, pt->mesh->stream));
+    ISG_CUDA(cudaStreamSynchronize(pt->mesh->stream));
+    return ISING_OK;
+}
+
+extern "C" int ising_pt_energies(const ising_pt* pt, double* e, double* mv) {
+    if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
+    DeviceGuard g(pt->mesh->device);
+    std::vector<Acc4> h(pt->n);
+    ISG_CUDA(cudaMemcpyAsync(h.data(), pt->d_acc, pt->n * sizeof(Acc4), cudaMemcpyDeviceToHost, pt->mesh->stream));
+    ISG_CUDA(cudaStreamSynchronize(pt->mesh->stream));
+    for (int r = 0; r < pt->n; ++r) {
+        if (e) e[r] = h[r].e;
+        if (mv) { mv[3 * r] = h[r].mx; mv[3 * r + 1] = h[r].my; mv[3 * r + 2] = h[r].mz; }
+    }
+    return ISING_OK;
+}
+
+extern "C" int ising_pt_resync(ising_pt* pt) {
+    if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
+    DeviceGuard g(pt->mesh->device);
+    ISG_TRY(pt_resync_enqueue(pt));
+    ISG_CUDA(cudaStreamSynchronize(pt->mesh->stream));
+    return ISING_OK;
+}
+
+extern "C" int ising_pt_swap_stats(const ising_pt* pt, uint64_t* att, uint64_t* acc) {
+    if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
+    DeviceGuard g(pt->mesh->device);
+    std::vector<unsigned long long> h(2 * (size_t)pt->n);
+    ISG_CUDA(cudaMemcpyAsync(h.data(), pt->d_stats, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             pt->mesh->stream));
+    ISG_CUDA(cudaStreamSynchronize(pt->mesh->stream));
+    for (int t = 0; t + 1 < pt->n; ++t) {
+        if (att) att[t] = h[t];
+        if (acc) acc[t] = h[(pt->n - 1) + t];
+    }
+    return ISING_OK;
+}
+
+extern "C" int ising_pt_series(const ising_pt* pt, double* out, int* n_rec) {
+    if (!pt || !n_rec) return fail(ISING_ERR_ARG, "NULL argument");
+    if (!pt->opt.record) return fail(ISING_ERR_ARG, "recording was not enabled");
+    DeviceGuard g(pt->mesh->device);
+    int c = 0;
+    ISG_CUDA(cudaMemcpyAsync(&c, pt->d_count, sizeof(int), cudaMemcpyDeviceToHost, pt->mesh->stream));
+    ISG_CUDA(cudaStreamSynchronize(pt->mesh->stream));
+    *n_rec = c;
+    if (out)
+        ISG_CUDA(cudaMemcpy(out, pt->d_series, (size_t)pt->n * pt->opt.record_capacity * 4 * sizeof(double),
+                            cudaMemcpyDeviceToHost));
+    return ISING_OK;
+}

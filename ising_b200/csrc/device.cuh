@@ -1,0 +1,126 @@
+// device.cuh -- device helpers shared by the sm_100a kernels of libisinggpu.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace isg {
+
+// ---------------------------------------------------------------- Philox4x32
+// Counter-based generator of Salmon, Moraes, Dror and Shaw, "Parallel random numbers:
+// as easy as 1, 2, 3" (SC'11).  Each round: two 32x32->64 products of the even counter
+// words with the published multipliers, an S-box style exchange with the odd words and
+// the key, and a Weyl increment of the key.
+constexpr uint32_t kPhiloxM0 = 0xD2511F53u;
+constexpr uint32_t kPhiloxM1 = 0xCD9E8D57u;
+constexpr uint32_t kPhiloxW0 = 0x9E3779B9u;
+constexpr uint32_t kPhiloxW1 = 0xBB67AE85u;
+
+// Stream tags in the top counter word (low 8 bits); the ensemble id fills the rest.
+enum : uint32_t { kTagSweep = 0, kTagInit = 1, kTagExchange = 2, kTagPatch = 3 };
+
+template <int ROUNDS = 10>
+__host__ __device__ __forceinline__ uint4 philox4x32(uint4 c, uint2 k) {
+#pragma unroll
+    for (int i = 0; i < ROUNDS; ++i) {
+#ifdef __CUDA_ARCH__
+        const uint32_t hi0 = __umulhi(kPhiloxM0, c.x), lo0 = kPhiloxM0 * c.x;
+        const uint32_t hi1 = __umulhi(kPhiloxM1, c.z), lo1 = kPhiloxM1 * c.z;
+#else
+        const uint64_t p0 = (uint64_t)kPhiloxM0 * c.x, p1 = (uint64_t)kPhiloxM1 * c.z;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += kPhiloxW0;
+        k.y += kPhiloxW1;
+    }
+    return c;
+}
+
+#if defined(__CUDACC__)
+// (0,1) uniform with 23 random bits: (2*(x>>9)+1) * 2^-24, formed exactly as
+// (1 + m*2^-23) - (1 - 2^-24) (Sterbenz: the subtraction is exact).
+__device__ __forceinline__ float u01(uint32_t x) {
+    return __uint_as_float((x >> 9) | 0x3f800000u) - 0.99999994f;
+}
+
+#endif  // __CUDACC__
+__host__ __device__ __forceinline__ uint2 philox_key(uint64_t seed) {
+    return make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+// ---------------------------------------------------------------- small vector helpers
+struct f3 { float x, y, z; };
+#if defined(__CUDACC__)
+__device__ __forceinline__ f3 mk(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ float dot(f3 a, f3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// Trial spin from four uniforms (u0: cos theta, u1: azimuth, u2: ball radius).
+// MOVE 0: fresh uniform unit vector.  MOVE 1: S' = norm(S + r*cbrt(u2)*v), the ball move
+// of UniformRandomInSphere (reference src/energyMin.f90:49-68).
+template <int MOVE>
+__device__ __forceinline__ f3 propose(f3 s, float u0, float u1, float u2, float r) {
+    const float cz = fmaf(2.0f, u0, -1.0f);                       // exact
+    const float q = (1.0f - cz) * (1.0f + cz);
+    const float st = q * rsqrtf(q);
+    float sn, cs;
+    __sincosf(3.14159265f * (2.0f * (u1 - 0.5f)), &sn, &cs);      // azimuth in (-pi, pi)
+    f3 v = {st * cs, st * sn, cz};
+    if (MOVE == 1) {
+        const float rho = r * __expf(0.33333334f * __logf(u2));   // r * cbrt(u2)
+        v = {fmaf(rho, v.x, s.x), fmaf(rho, v.y, s.y), fmaf(rho, v.z, s.z)};
+    }
+    const float rn = rsqrtf(dot(v, v));
+    return {v.x * rn, v.y * rn, v.z * rn};
+}
+#endif  // __CUDACC__
+
+// ---------------------------------------------------------------- kernel-facing structs
+// FP32 Hamiltonian as the kernels consume it.
+struct HamDev {
+    float J, Jp;      // shell-1 exchange, shell-2 exchange
+    float Bz;         // zeeman_factor * B (field along +z)
+    float K;          // anisotropy -K (S.e)^2
+    float kx, ky, kz; // anisotropy axis
+    float D[6][3];    // simple cubic: D vector per bond direction (+x,-x,+y,-y,+z,-z)
+};
+
+// One neighbour slot of a sublattice in a general crystal.
+struct Slot {
+    int8_t dx, dy, dz;   // cell offset (any sign, wraps periodically)
+    uint8_t sub;         // neighbour sublattice
+    float w;             // exchange weight (J for shell 1, J' for shell 2)
+    float Dx, Dy, Dz;    // DMI vector (zero on shell 2)
+};
+
+constexpr int kMaxSub = 16;
+constexpr int kMaxSlots = 64;
+
+struct StencilDev {
+    const Slot* slots;   // n_sub * kMaxSlots, slot s of sublattice i at [i*kMaxSlots + s]
+    const int* count;    // per sublattice
+    int nsub;
+};
+
+// Per-replica running accumulators: E, Mx, My, Mz.
+struct Acc4 { double e, mx, my, mz; };
+
+// Device status word bits.
+enum : int { kStatNan = 1, kStatBounds = 2, kStatTimeout = 4 };
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+__device__ __forceinline__ int wrap_any(int v, int n) { v %= n; return v < 0 ? v + n : v; }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+#endif  // __CUDACC__
+
+}  // namespace isg

@@ -1,0 +1,233 @@
+// internal.h -- host-side structures of libisinggpu (not part of the C-ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ising_gpu.h"
+#include "device.cuh"
+
+namespace isg {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+#define ISG_CUDA(call)                                              \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return ::isg::cuda_fail(e_, #call);  \
+    } while (0)
+
+// ---------------------------------------------------------------- lattice compiler
+// A neighbour of sublattice i expressed as a cell offset plus target sublattice, with the
+// minimum-image bond vector r_j - r_i.  Because the periodic mesh is translation
+// invariant, one list per sublattice (built at cell 0) describes every atom.
+struct NbrSlot {
+    int dx, dy, dz, sub;
+    double r[3];
+};
+
+struct Lattice {
+    int nx = 0, ny = 0, nz = 0, nsub = 0, nshells = 2;
+    int64_t ncells = 0, natoms = 0;
+    double a = 0, b = 0, c = 0;
+    double av[3], bv[3], cv[3], ar[3], br[3], cr[3];
+    std::vector<float> frac;                      // nsub x 3
+    std::vector<std::vector<NbrSlot>> shell[2];   // per sublattice, shells 1 and 2
+    std::vector<std::vector<NbrSlot>> legacy;     // per sublattice, legacy NeighborList
+    std::vector<NbrSlot> deriv;                   // [sub*6 + d*2 + side]
+    bool deriv_ok = true;
+
+    // position of atom (cell, sub) as real(4), as makeChainMesh stores it
+    void position(int64_t atom, float out[3]) const;
+    int64_t atom_of(int ix, int iy, int iz, int sub) const {
+        return (((int64_t)ix * ny + iy) * nz + iz) * nsub + sub;
+    }
+    void cell_of(int64_t atom, int* ix, int* iy, int* iz, int* sub) const;
+    int64_t neighbour_atom(int64_t atom, const NbrSlot& s) const;
+};
+
+// Builds a Lattice; returns ISING_OK or an error status (message set).
+int build_lattice(const float* frac, int nsub, int nx, int ny, int nz, double a, double b,
+                  double c, double ab_deg, double bc_deg, double ca_deg, double shell_tol,
+                  int n_shells, Lattice* out);
+
+// Greedy colouring of the bond graph of the active shells (shell 1 always, shell 2 when
+// use_shell2).  Returns colour per atom and the number of colours; verifies that every
+// class is an independent set.
+int greedy_colouring(const Lattice& L, bool use_shell2, std::vector<int>* colour, int* ncol);
+
+// True if the mesh is simple cubic with the six axis neighbours as shell 1 and even
+// extents, so the 2-colour checkerboard fast path applies.
+bool is_checkerboard_sc(const Lattice& L);
+
+// ---------------------------------------------------------------- device-side handle
+struct Colouring {
+    int ncol = 0;
+    std::vector<int> host_colour;
+    std::vector<int> class_start;   // ncol + 1
+    int* d_sites = nullptr;         // atoms grouped by class
+};
+
+struct DeviceStencil {
+    Slot* d_slots = nullptr;        // kMaxSub * kMaxSlots
+    int* d_count = nullptr;         // kMaxSub
+    bool built = false;
+};
+
+}  // namespace isg
+
+struct ising_mesh {
+    isg::Lattice lat;
+    int device = 0;
+    int n_replicas = 0;
+    cudaStream_t stream = nullptr;       // stream all work is issued on
+    cudaStream_t own_stream = nullptr;   // the handle's own stream
+    float* d_spins = nullptr;            // [R][3][natoms] FP32 SoA planes
+    uint32_t* d_sweep = nullptr;         // per-replica sweep counters
+    std::vector<uint32_t> h_sweep;       // host mirror of d_sweep
+    double* d_scratch = nullptr;         // small per-call device buffer (kScratchDoubles)
+    double* h_pinned = nullptr;          // pinned host mirror of d_scratch
+    int* d_status = nullptr;             // device status word
+    double* d_beta = nullptr;            // per-replica beta for single-replica sweeps
+    double* d_staging = nullptr;         // 3N doubles for host-layout spin transfers
+    size_t staging_size = 0;
+    double* d_winding_tmp = nullptr;     // per-slice winding results
+    bool checkerboard = false;
+    isg::Colouring colour[2];            // [0]: shell 1 bonds, [1]: shells 1+2
+    // cached device stencils keyed by the Hamiltonian that filled their weights
+    isg::Slot* d_slots = nullptr;
+    int* d_slot_count = nullptr;
+    int* d_plaq = nullptr;               // winding plaquette offsets (4 x {dx,dy,sub})
+};
+
+namespace isg {
+constexpr int kScratchDoubles = 1 << 16;
+
+// Kernel launchers (kernels.cu).
+struct SweepLaunch {
+    float* spins;          // replica block base
+    int64_t natoms;
+    int nx, ny, nz;
+    int n_rep;             // replicas in this launch (blockIdx.z)
+    int rep_first;         // first replica index (into beta/sweep/partials arrays)
+    const double* beta_rep;   // per replica (indexed by replica id)
+    const uint32_t* sweep_ctr; // per replica (indexed by replica id)
+    uint32_t sweep_offset;
+    uint64_t seed;
+    uint32_t ensemble;
+    int move;
+    float r;
+    HamDev ham;
+    int dmi_kind;          // 0 none, 1 bulk, 2 interfacial z, 3 generic
+    double* partials;      // [rep][slot][4]
+    int slots_per_rep;
+    int* status;
+};
+int launch_sc_colour(const SweepLaunch& a, int colour, cudaStream_t s);
+int sc_slots_per_rep(int nx, int ny, int nz);
+
+struct GeneralLaunch {
+    float* spins;
+    int64_t natoms;
+    int nx, ny, nz, nsub;
+    int n_rep, rep_first;
+    const double* beta_rep;
+    const uint32_t* sweep_ctr;
+    uint32_t sweep_offset;
+    uint64_t seed;
+    uint32_t ensemble;
+    int move;
+    float r;
+    HamDev ham;
+    StencilDev st;
+    const int* sites;      // atoms of this colour class
+    int n_sites;
+    double* partials;
+    int slots_per_rep;
+    int slot_base;         // class offset into the slot range
+    int* status;
+};
+int launch_general_colour(const GeneralLaunch& a, cudaStream_t s);
+int general_slots_for(int n_sites);
+
+struct ReduceLaunch {
+    const float* spins;
+    int64_t natoms;
+    int nx, ny, nz, nsub;
+    int n_rep;
+    HamDev ham;            // Bz already multiplied by the zeeman factor
+    StencilDev st;         // slots used for the energy (weights 0.5 applied in kernel)
+    double* out;           // [rep][4]: E, Mx, My, Mz
+    double* block_tmp;     // [rep][blocks][4]
+    int blocks_per_rep;
+};
+int launch_energy_mag(const ReduceLaunch& a, cudaStream_t s);
+int energy_blocks_for(int64_t natoms);
+
+int launch_fold_partials(double* partials, int slots_per_rep, int n_rep, Acc4* acc,
+                         cudaStream_t s);
+
+struct WindingLaunch {
+    const float* spins;
+    int64_t natoms;
+    int nx, ny, nz, nsub;
+    int n_rep;
+    const int* plaq;       // 4 entries of (dx, dy, dz, sub) relative to sublattice nsub-1
+    double* out;           // [rep][nz]
+    int fp64;
+};
+int launch_winding(const WindingLaunch& a, cudaStream_t s);
+
+struct LocalLaunch {
+    const float* spins;    // one replica
+    int64_t natoms;
+    int nx, ny, nz, nsub;
+    HamDev ham;
+    StencilDev st;
+    const int64_t* atoms;
+    const double* sprop;   // n x 3
+    double* old_e;
+    double* new_e;
+    int n;
+};
+int launch_local_energy(const LocalLaunch& a, cudaStream_t s);
+
+int launch_init_uniform(float* spins, int64_t natoms, int n_rep, uint64_t seed,
+                        uint32_t ensemble, cudaStream_t s);
+int launch_advance(uint32_t* ctr, int n, uint32_t by, cudaStream_t s);
+int launch_spins_from_f64(const double* in, float* out, int64_t natoms, int* status, cudaStream_t s);
+int launch_spins_to_f64(const float* in, double* out, int64_t natoms, cudaStream_t s);
+
+struct ExchangeLaunch {
+    int n;                       // temperature slots
+    const double* beta_t;        // per slot
+    double* beta_rep;            // per replica (updated)
+    int* t2r;
+    int* r2t;
+    const Acc4* acc;             // per replica
+    unsigned long long* stats;   // [2][n-1]: attempts, accepts
+    uint32_t* round;             // device round counter (advanced)
+    uint64_t seed;
+    uint32_t ensemble;
+    int scheme;
+};
+int launch_exchange(const ExchangeLaunch& a, cudaStream_t s);
+
+struct RecordLaunch {
+    const Acc4* acc;
+    const double* q;     // [rep][nz] winding per slice
+    const int* t2r;      // temperature slot -> replica
+    int nz;
+    int n_rep;
+    int64_t natoms;
+    double* series;      // [slot][cap][4]
+    int cap;
+    int* count;          // device count (advanced)
+};
+int launch_record(const RecordLaunch& a, cudaStream_t s);
+
+}  // namespace isg

@@ -1,0 +1,620 @@
+// kernels.cu -- sm_100a kernels of libisinggpu (grid-launched forms).
+//
+// Layout in HBM: per replica three FP32 planes (Sx[N], Sy[N], Sz[N]) in the reference's atom
+// order (z fastest for one atom per cell); replicas follow each other.  FP64 is used only in
+// per-replica accumulators and in the parity reductions.
+#include <cstdio>
+
+#include "internal.h"
+
+namespace isg {
+
+// ================================================================= checkerboard sweep (SC)
+// One colour class of the simple cubic checkerboard.  Thread (k, y) of block (yb, x, rep)
+// owns the site z = 2k + ((x+y+colour)&1) of row (x, y).  Local field from the six axis
+// neighbours:  h = J sum S_j + sum_k S_k x D_k - Bz z_hat  (D.(S x S_j) = S.(S_j x D)),
+// dE = (S'-S).h - K[(S'.e)^2 - (S.e)^2]  (reference calculateHeisenbergEnergy,
+// src/energyMin.f90:86-171, rewritten in local-field form).
+constexpr int kScThreads = 256;
+
+struct ScGeom { int tx, ty, zb, yb; };
+static ScGeom sc_geom(int nx, int ny, int nz) {
+    ScGeom g;
+    const int half = nz / 2;
+    g.tx = half < 128 ? half : 128;
+    g.ty = kScThreads / g.tx;
+    if (g.ty < 1) g.ty = 1;
+    g.zb = (half + g.tx - 1) / g.tx;
+    g.yb = (ny + g.ty - 1) / g.ty;
+    (void)nx;
+    return g;
+}
+int sc_slots_per_rep(int nx, int ny, int nz) {
+    ScGeom g = sc_geom(nx, ny, nz);
+    return g.zb * g.yb * nx;
+}
+
+template <typename T>
+__device__ __forceinline__ void block_sum4(T v0, T v1, T v2, T v3, T* out /* smem 4 */) {
+    __shared__ T red[4][32];
+    v0 = warp_sum(v0); v1 = warp_sum(v1); v2 = warp_sum(v2); v3 = warp_sum(v3);
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = tid & 31, wid = tid >> 5;
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if (lane == 0) { red[0][wid] = v0; red[1][wid] = v1; red[2][wid] = v2; red[3][wid] = v3; }
+    __syncthreads();
+    if (wid == 0) {
+        T a = lane < nw ? red[0][lane] : T(0), b = lane < nw ? red[1][lane] : T(0);
+        T c = lane < nw ? red[2][lane] : T(0), d = lane < nw ? red[3][lane] : T(0);
+        a = warp_sum(a); b = warp_sum(b); c = warp_sum(c); d = warp_sum(d);
+        if (lane == 0) { out[0] = a; out[1] = b; out[2] = c; out[3] = d; }
+    }
+}
+
+template <int MOVE, int DMI, bool HAS_K>
+__global__ void __launch_bounds__(kScThreads) k_sc_colour(SweepLaunch a, int colour, int zb) {
+    const int bx = blockIdx.x;
+    const int k = (bx % zb) * blockDim.x + threadIdx.x;
+    const int y = (bx / zb) * blockDim.y + threadIdx.y;
+    const int x = blockIdx.y;
+    const int rl = blockIdx.z;
+    const int rep = a.rep_first + rl;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
+    if (y < ny && k < (nz >> 1)) {
+        const int64_t N = a.natoms;
+        float* __restrict__ sx = a.spins + (int64_t)rl * 3 * N;
+        float* __restrict__ sy = sx + N;
+        float* __restrict__ sz = sy + N;
+        const int z = 2 * k + ((x + y + colour) & 1);
+        const int64_t row = (int64_t)x * ny + y;
+        const int64_t i = row * nz + z;
+        const int xp = x + 1 == nx ? 0 : x + 1, xm = x == 0 ? nx - 1 : x - 1;
+        const int yp = y + 1 == ny ? 0 : y + 1, ym = y == 0 ? ny - 1 : y - 1;
+        const int zp = z + 1 == nz ? 0 : z + 1, zm = z == 0 ? nz - 1 : z - 1;
+        const int64_t ixp = ((int64_t)xp * ny + y) * nz + z, ixm = ((int64_t)xm * ny + y) * nz + z;
+        const int64_t iyp = ((int64_t)x * ny + yp) * nz + z, iym = ((int64_t)x * ny + ym) * nz + z;
+        const int64_t izp = row * nz + zp, izm = row * nz + zm;
+        const f3 s = {sx[i], sy[i], sz[i]};
+        const f3 px = {sx[ixp], sy[ixp], sz[ixp]}, mx = {sx[ixm], sy[ixm], sz[ixm]};
+        const f3 py = {sx[iyp], sy[iyp], sz[iyp]}, my = {sx[iym], sy[iym], sz[iym]};
+        const f3 pz = {sx[izp], sy[izp], sz[izp]}, mz = {sx[izm], sy[izm], sz[izm]};
+        const HamDev& H = a.ham;
+        f3 h = {(px.x + mx.x) + (py.x + my.x) + (pz.x + mz.x),
+                (px.y + mx.y) + (py.y + my.y) + (pz.y + mz.y),
+                (px.z + mx.z) + (py.z + my.z) + (pz.z + mz.z)};
+        h.x *= H.J; h.y *= H.J; h.z *= H.J;
+        if (DMI == 1) {
+            // bulk: D_{+a} = -D a_hat, D_{-a} = +D a_hat  ->  D (S_{-a} - S_{+a}) x a_hat
+            const float D = H.D[1][0];
+            const f3 dx = {mx.x - px.x, mx.y - px.y, mx.z - px.z};
+            const f3 dy = {my.x - py.x, my.y - py.y, my.z - py.z};
+            const f3 dz = {mz.x - pz.x, mz.y - pz.y, mz.z - pz.z};
+            h.x = fmaf(D, dz.y - dy.z, h.x);
+            h.y = fmaf(D, dx.z - dz.x, h.y);
+            h.z = fmaf(D, dy.x - dx.y, h.z);
+        } else if (DMI == 2) {
+            // interfacial along z: D_{+x} = -D y, D_{-x} = +D y, D_{+y} = +D x, D_{-y} = -D x
+            const float D = H.D[2][0];
+            const f3 ax = {mx.x - px.x, mx.y - px.y, mx.z - px.z};  // (S_{-x}-S_{+x}) x y_hat
+            const f3 ay = {py.x - my.x, py.y - my.y, py.z - my.z};  // (S_{+y}-S_{-y}) x x_hat
+            h.x = fmaf(D, -ax.z, h.x);
+            h.y = fmaf(D, ay.z, h.y);
+            h.z = fmaf(D, ax.x - ay.y, h.z);
+        } else if (DMI == 3) {
+            const f3 nb[6] = {px, mx, py, my, pz, mz};
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const f3 D = {H.D[q][0], H.D[q][1], H.D[q][2]};
+                const f3 c = cross(nb[q], D);
+                h.x += c.x; h.y += c.y; h.z += c.z;
+            }
+        }
+        h.z -= H.Bz;
+        const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
+        const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)i, sweep, (uint32_t)rep,
+                                                   (a.ensemble << 8) | kTagSweep),
+                                        philox_key(a.seed));
+        const f3 sp = propose<MOVE>(s, u01(r4.x), u01(r4.y), u01(r4.z), a.r);
+        float dE = (sp.x - s.x) * h.x + (sp.y - s.y) * h.y + (sp.z - s.z) * h.z;
+        if (HAS_K) {
+            const float e1 = sp.x * H.kx + sp.y * H.ky + sp.z * H.kz;
+            const float e0 = s.x * H.kx + s.y * H.ky + s.z * H.kz;
+            dE -= H.K * (e1 * e1 - e0 * e0);
+        }
+        const float beta = (float)a.beta_rep[rep];
+        if (!(dE == dE)) atomicOr(a.status, kStatNan);
+        const bool acc = (dE <= 0.f) || (u01(r4.w) < __expf(-beta * dE));
+        if (acc) {
+            sx[i] = sp.x; sy[i] = sp.y; sz[i] = sp.z;
+            de = dE; dmx = sp.x - s.x; dmy = sp.y - s.y; dmz = sp.z - s.z;
+        }
+    }
+    if (a.partials) {
+        __shared__ double tot[4];
+        block_sum4<double>(de, dmx, dmy, dmz, tot);
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            const int slot = bx + gridDim.x * x;
+            double* p = a.partials + ((int64_t)rep * a.slots_per_rep + slot) * 4;
+            p[0] += tot[0]; p[1] += tot[1]; p[2] += tot[2]; p[3] += tot[3];
+        }
+    }
+}
+
+template <int MOVE, int DMI>
+static void sc_dispatch_k(const SweepLaunch& a, int colour, dim3 g, dim3 b, int zb, bool hk,
+                          cudaStream_t s) {
+    if (hk) k_sc_colour<MOVE, DMI, true><<<g, b, 0, s>>>(a, colour, zb);
+    else k_sc_colour<MOVE, DMI, false><<<g, b, 0, s>>>(a, colour, zb);
+}
+
+int launch_sc_colour(const SweepLaunch& a, int colour, cudaStream_t s) {
+    ScGeom gg = sc_geom(a.nx, a.ny, a.nz);
+    dim3 b(gg.tx, gg.ty), g(gg.zb * gg.yb, a.nx, a.n_rep);
+    const bool hk = a.ham.K != 0.f;
+#define ISG_SC(M, D) sc_dispatch_k<M, D>(a, colour, g, b, gg.zb, hk, s)
+    if (a.move == 0) {
+        switch (a.dmi_kind) { case 0: ISG_SC(0, 0); break; case 1: ISG_SC(0, 1); break;
+                              case 2: ISG_SC(0, 2); break; default: ISG_SC(0, 3); }
+    } else {
+        switch (a.dmi_kind) { case 0: ISG_SC(1, 0); break; case 1: ISG_SC(1, 1); break;
+                              case 2: ISG_SC(1, 2); break; default: ISG_SC(1, 3); }
+    }
+#undef ISG_SC
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+// ================================================================= general crystal sweep
+// One colour class of a greedy colouring over an arbitrary unit cell: the site list of the
+// class is read, each site's neighbours come from its sublattice stencil (cell offset plus
+// sublattice) held in shared memory.
+constexpr int kGenThreads = 256;
+constexpr int kGenSitesPerThread = 4;
+
+int general_slots_for(int n_sites) {
+    int per = kGenThreads * kGenSitesPerThread;
+    return (n_sites + per - 1) / per;
+}
+
+__device__ __forceinline__ void decode_atom(int64_t at, int nsub, int ny, int nz, int* ix, int* iy,
+                                            int* iz, int* sub) {
+    *sub = (int)(at % nsub);
+    const int64_t cell = at / nsub;
+    *iz = (int)(cell % nz);
+    const int64_t r = cell / nz;
+    *iy = (int)(r % ny);
+    *ix = (int)(r / ny);
+}
+
+// local field of atom (ix,iy,iz,sub) from its stencil in shared memory
+__device__ __forceinline__ f3 stencil_field(const float* sx, const float* sy, const float* sz,
+                                            const Slot* sl, int cnt, int ix, int iy, int iz,
+                                            int nx, int ny, int nz, int nsub) {
+    f3 h = {0.f, 0.f, 0.f};
+    for (int q = 0; q < cnt; ++q) {
+        const Slot e = sl[q];
+        const int jx = wrap_any(ix + e.dx, nx), jy = wrap_any(iy + e.dy, ny), jz = wrap_any(iz + e.dz, nz);
+        const int64_t j = (((int64_t)jx * ny + jy) * nz + jz) * nsub + e.sub;
+        const f3 sj = {sx[j], sy[j], sz[j]};
+        const f3 c = cross(sj, mk(e.Dx, e.Dy, e.Dz));
+        h.x += fmaf(e.w, sj.x, c.x);
+        h.y += fmaf(e.w, sj.y, c.y);
+        h.z += fmaf(e.w, sj.z, c.z);
+    }
+    return h;
+}
+
+template <int MOVE>
+__global__ void __launch_bounds__(kGenThreads) k_general_colour(GeneralLaunch a) {
+    extern __shared__ unsigned char smem_raw[];
+    Slot* sl = reinterpret_cast<Slot*>(smem_raw);
+    int* cnt = reinterpret_cast<int*>(sl + a.st.nsub * kMaxSlots);
+    for (int q = threadIdx.x; q < a.st.nsub * kMaxSlots; q += blockDim.x) sl[q] = a.st.slots[q];
+    for (int q = threadIdx.x; q < a.st.nsub; q += blockDim.x) cnt[q] = a.st.count[q];
+    __syncthreads();
+    const int rl = blockIdx.y;
+    const int rep = a.rep_first + rl;
+    const int64_t N = a.natoms;
+    float* __restrict__ sx = a.spins + (int64_t)rl * 3 * N;
+    float* __restrict__ sy = sx + N;
+    float* __restrict__ sz = sy + N;
+    const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
+    const float beta = (float)a.beta_rep[rep];
+    const HamDev& H = a.ham;
+    float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
+    const int base = blockIdx.x * blockDim.x * kGenSitesPerThread;
+    for (int it = 0; it < kGenSitesPerThread; ++it) {
+        const int t = base + it * blockDim.x + threadIdx.x;
+        if (t >= a.n_sites) break;
+        const int64_t at = a.sites[t];
+        int ix, iy, iz, sub;
+        decode_atom(at, a.nsub, a.ny, a.nz, &ix, &iy, &iz, &sub);
+        f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.nx, a.ny, a.nz, a.nsub);
+        h.z -= H.Bz;
+        const f3 s = {sx[at], sy[at], sz[at]};
+        const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)at, sweep, (uint32_t)rep,
+                                                   (a.ensemble << 8) | kTagSweep),
+                                        philox_key(a.seed));
+        const f3 sp = propose<MOVE>(s, u01(r4.x), u01(r4.y), u01(r4.z), a.r);
+        float dE = (sp.x - s.x) * h.x + (sp.y - s.y) * h.y + (sp.z - s.z) * h.z;
+        if (H.K != 0.f) {
+            const float e1 = sp.x * H.kx + sp.y * H.ky + sp.z * H.kz;
+            const float e0 = s.x * H.kx + s.y * H.ky + s.z * H.kz;
+            dE -= H.K * (e1 * e1 - e0 * e0);
+        }
+        if (!(dE == dE)) atomicOr(a.status, kStatNan);
+        if ((dE <= 0.f) || (u01(r4.w) < __expf(-beta * dE))) {
+            sx[at] = sp.x; sy[at] = sp.y; sz[at] = sp.z;
+            de += dE; dmx += sp.x - s.x; dmy += sp.y - s.y; dmz += sp.z - s.z;
+        }
+    }
+    if (a.partials) {
+        __shared__ double tot[4];
+        block_sum4<double>(de, dmx, dmy, dmz, tot);
+        if (threadIdx.x == 0) {
+            double* p = a.partials + ((int64_t)rep * a.slots_per_rep + a.slot_base + blockIdx.x) * 4;
+            p[0] += tot[0]; p[1] += tot[1]; p[2] += tot[2]; p[3] += tot[3];
+        }
+    }
+}
+
+int launch_general_colour(const GeneralLaunch& a, cudaStream_t s) {
+    if (a.n_sites <= 0) return ISING_OK;
+    dim3 g(general_slots_for(a.n_sites), a.n_rep), b(kGenThreads);
+    size_t sm = (size_t)a.st.nsub * kMaxSlots * sizeof(Slot) + kMaxSub * sizeof(int);
+    if (a.move == 0) k_general_colour<0><<<g, b, sm, s>>>(a);
+    else k_general_colour<1><<<g, b, sm, s>>>(a);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+// ================================================================= energy + magnetisation
+// e_i = 1/2 S.(sum_j w S_j + S_j x D_ij) - Bz S_z - K (S.e)^2, summed per replica:
+// TotalHeisenbergEnergy (src/energyMin.f90:499-528) with FP32 terms and FP64 block sums.
+constexpr int kRedThreads = 256;
+constexpr int kRedSitesPerBlock = 4096;
+
+int energy_blocks_for(int64_t natoms) {
+    return (int)((natoms + kRedSitesPerBlock - 1) / kRedSitesPerBlock);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_energy_mag(ReduceLaunch a) {
+    extern __shared__ unsigned char smem_raw[];
+    Slot* sl = reinterpret_cast<Slot*>(smem_raw);
+    int* cnt = reinterpret_cast<int*>(sl + a.st.nsub * kMaxSlots);
+    for (int q = threadIdx.x; q < a.st.nsub * kMaxSlots; q += blockDim.x) sl[q] = a.st.slots[q];
+    for (int q = threadIdx.x; q < a.st.nsub; q += blockDim.x) cnt[q] = a.st.count[q];
+    __syncthreads();
+    const int rep = blockIdx.y;
+    const int64_t N = a.natoms;
+    const float* sx = a.spins + (int64_t)rep * 3 * N;
+    const float* sy = sx + N;
+    const float* sz = sy + N;
+    const HamDev& H = a.ham;
+    double e = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+    const int64_t i0 = (int64_t)blockIdx.x * kRedSitesPerBlock;
+    int64_t i1 = i0 + kRedSitesPerBlock;
+    if (i1 > N) i1 = N;
+    for (int64_t at = i0 + threadIdx.x; at < i1; at += blockDim.x) {
+        int ix, iy, iz, sub;
+        decode_atom(at, a.nsub, a.ny, a.nz, &ix, &iy, &iz, &sub);
+        const f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.nx, a.ny, a.nz, a.nsub);
+        const f3 s = {sx[at], sy[at], sz[at]};
+        float ei = 0.5f * dot(s, h) - H.Bz * s.z;
+        if (H.K != 0.f) {
+            const float ea = s.x * H.kx + s.y * H.ky + s.z * H.kz;
+            ei -= H.K * ea * ea;
+        }
+        e += (double)ei;
+        mx += (double)s.x; my += (double)s.y; mz += (double)s.z;
+    }
+    __shared__ double tot[4];
+    block_sum4<double>(e, mx, my, mz, tot);
+    if (threadIdx.x == 0) {
+        double* p = a.block_tmp + ((int64_t)rep * a.blocks_per_rep + blockIdx.x) * 4;
+        p[0] = tot[0]; p[1] = tot[1]; p[2] = tot[2]; p[3] = tot[3];
+    }
+}
+
+// Deterministic per-replica sum of block partials: out[rep] = sum_b in[rep][b]; optionally
+// accumulate into acc and zero the inputs.
+__global__ void k_sum_blocks(double* in, int nb, double* out, Acc4* acc, int zero_in) {
+    const int rep = blockIdx.x;
+    double v[4] = {0, 0, 0, 0};
+    double* p = in + (int64_t)rep * nb * 4;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        for (int q = 0; q < 4; ++q) v[q] += p[(int64_t)b * 4 + q];
+        if (zero_in) for (int q = 0; q < 4; ++q) p[(int64_t)b * 4 + q] = 0.0;
+    }
+    __shared__ double tot[4];
+    block_sum4<double>(v[0], v[1], v[2], v[3], tot);
+    if (threadIdx.x == 0) {
+        if (out) for (int q = 0; q < 4; ++q) out[rep * 4 + q] = tot[q];
+        if (acc) { acc[rep].e += tot[0]; acc[rep].mx += tot[1]; acc[rep].my += tot[2]; acc[rep].mz += tot[3]; }
+    }
+}
+
+int launch_energy_mag(const ReduceLaunch& a, cudaStream_t s) {
+    dim3 g(a.blocks_per_rep, a.n_rep);
+    size_t sm = (size_t)a.st.nsub * kMaxSlots * sizeof(Slot) + kMaxSub * sizeof(int);
+    k_energy_mag<<<g, kRedThreads, sm, s>>>(a);
+    ISG_CUDA(cudaGetLastError());
+    k_sum_blocks<<<a.n_rep, 256, 0, s>>>(a.block_tmp, a.blocks_per_rep, a.out, nullptr, 0);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+int launch_fold_partials(double* partials, int slots_per_rep, int n_rep, Acc4* acc, cudaStream_t s) {
+    k_sum_blocks<<<n_rep, 256, 0, s>>>(partials, slots_per_rep, nullptr, acc, 1);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+// ================================================================= winding number
+// Per z-slice Berg-Luscher topological charge (calculate_winding_number2, rsp:320-364 with
+// arc_winding rsp:284-318): plaquette (s1, s1+a, s1+b, s1+a+b) from the derivative list,
+// triangles (s1,s2,s4) and (s1,s4,s3), divided by 4*pi (pi as the reference's
+// default-real literal).
+template <typename T>
+__device__ __forceinline__ T arc_winding_t(const T* s1, const T* s2, const T* s3) {
+    const T d12 = s1[0] * s2[0] + s1[1] * s2[1] + s1[2] * s2[2];
+    const T d23 = s2[0] * s3[0] + s2[1] * s3[1] + s2[2] * s3[2];
+    const T d31 = s3[0] * s1[0] + s3[1] * s1[1] + s3[2] * s1[2];
+    const T cx = s2[1] * s3[2] - s2[2] * s3[1];
+    const T cy = s2[2] * s3[0] - s2[0] * s3[2];
+    const T cz = s2[0] * s3[1] - s2[1] * s3[0];
+    T re = T(1) + d12 + d23 + d31;
+    T im = s1[0] * cx + s1[1] * cy + s1[2] * cz;
+    const T nrm = sqrt(T(2) * (T(1) + d12) * (T(1) + d23) * (T(1) + d31));
+    re = re / nrm;
+    im = im / nrm;
+    return T(2) * atan2(im, re);
+}
+
+template <typename T>
+__device__ __forceinline__ void load_unit(const float* sx, const float* sy, const float* sz, int64_t j, T* o) {
+    const T x = (T)sx[j], y = (T)sy[j], z = (T)sz[j];
+    const T n = sqrt(x * x + y * y + z * z);
+    o[0] = x / n; o[1] = y / n; o[2] = z / n;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_winding(WindingLaunch a) {
+    const int zc = blockIdx.x;
+    const int rep = blockIdx.y;
+    const int64_t N = a.natoms;
+    const float* sx = a.spins + (int64_t)rep * 3 * N;
+    const float* sy = sx + N;
+    const float* sz = sy + N;
+    const int nsub = a.nsub;
+    const int* P = a.plaq;  // 4 x (dx, dy, dz, sub): s1, s2, s4, s3
+    T w = T(0);
+    const int np = a.nx * a.ny;
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        const int i = p / a.ny, j = p % a.ny;
+        int64_t at[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int jx = wrap_any(i + P[4 * q], a.nx), jy = wrap_any(j + P[4 * q + 1], a.ny);
+            const int jz = wrap_any(zc + P[4 * q + 2], a.nz);
+            at[q] = (((int64_t)jx * a.ny + jy) * a.nz + jz) * nsub + P[4 * q + 3];
+        }
+        T s1[3], s2[3], s4[3], s3[3];
+        load_unit<T>(sx, sy, sz, at[0], s1);
+        load_unit<T>(sx, sy, sz, at[1], s2);
+        load_unit<T>(sx, sy, sz, at[2], s4);
+        load_unit<T>(sx, sy, sz, at[3], s3);
+        w += arc_winding_t<T>(s1, s2, s4) + arc_winding_t<T>(s1, s4, s3);
+    }
+    __shared__ double tot[4];
+    block_sum4<double>((double)w, 0.0, 0.0, 0.0, tot);
+    if (threadIdx.x == 0) {
+        const double four_pi = 4.0 * (double)3.14159265358979323846f;
+        a.out[(int64_t)rep * a.nz + zc] = tot[0] / four_pi;
+    }
+}
+
+int launch_winding(const WindingLaunch& a, cudaStream_t s) {
+    dim3 g(a.nz, a.n_rep);
+    if (a.fp64) k_winding<double><<<g, 256, 0, s>>>(a);
+    else k_winding<float><<<g, 256, 0, s>>>(a);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+// ================================================================= local energy queries
+// calculateHeisenbergEnergy (src/energyMin.f90:86-171) for a batch of (atom, S') pairs:
+// E(S) = S.h - K (S.e)^2 with h the FP32 local field.
+__global__ void k_local_energy(LocalLaunch a) {
+    extern __shared__ unsigned char smem_raw[];
+    Slot* sl = reinterpret_cast<Slot*>(smem_raw);
+    int* cnt = reinterpret_cast<int*>(sl + a.st.nsub * kMaxSlots);
+    for (int q = threadIdx.x; q < a.st.nsub * kMaxSlots; q += blockDim.x) sl[q] = a.st.slots[q];
+    for (int q = threadIdx.x; q < a.st.nsub; q += blockDim.x) cnt[q] = a.st.count[q];
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const int64_t N = a.natoms;
+    const float* sx = a.spins;
+    const float* sy = sx + N;
+    const float* sz = sy + N;
+    const int64_t at = a.atoms[t];
+    int ix, iy, iz, sub;
+    decode_atom(at, a.nsub, a.ny, a.nz, &ix, &iy, &iz, &sub);
+    f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.nx, a.ny, a.nz, a.nsub);
+    h.z -= a.ham.Bz;
+    const f3 s = {sx[at], sy[at], sz[at]};
+    const f3 sp = {(float)a.sprop[3 * t], (float)a.sprop[3 * t + 1], (float)a.sprop[3 * t + 2]};
+    float e0 = dot(s, h), e1 = dot(sp, h);
+    if (a.ham.K != 0.f) {
+        const float q0 = s.x * a.ham.kx + s.y * a.ham.ky + s.z * a.ham.kz;
+        const float q1 = sp.x * a.ham.kx + sp.y * a.ham.ky + sp.z * a.ham.kz;
+        e0 -= a.ham.K * q0 * q0;
+        e1 -= a.ham.K * q1 * q1;
+    }
+    a.old_e[t] = (double)e0;
+    a.new_e[t] = (double)e1;
+}
+
+int launch_local_energy(const LocalLaunch& a, cudaStream_t s) {
+    if (a.n <= 0) return ISING_OK;
+    size_t sm = (size_t)a.st.nsub * kMaxSlots * sizeof(Slot) + kMaxSub * sizeof(int);
+    k_local_energy<<<(a.n + 127) / 128, 128, sm, s>>>(a);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+// ================================================================= initial spins
+__global__ void k_init_uniform(float* spins, int64_t N, uint64_t seed, uint32_t ensemble) {
+    const int rep = blockIdx.y;
+    float* sx = spins + (int64_t)rep * 3 * N;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)i, 0u, (uint32_t)rep, (ensemble << 8) | kTagInit),
+                                        philox_key(seed));
+        const f3 v = propose<0>(mk(0.f, 0.f, 1.f), u01(r4.x), u01(r4.y), 0.5f, 0.f);
+        sx[i] = v.x; sx[N + i] = v.y; sx[2 * N + i] = v.z;
+    }
+}
+
+int launch_init_uniform(float* spins, int64_t natoms, int n_rep, uint64_t seed, uint32_t ensemble,
+                        cudaStream_t s) {
+    int blocks = (int)((natoms + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    dim3 g(blocks, n_rep);
+    k_init_uniform<<<g, 256, 0, s>>>(spins, natoms, seed, ensemble);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+__global__ void k_advance(uint32_t* ctr, int n, uint32_t by) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) ctr[i] += by;
+}
+
+int launch_advance(uint32_t* ctr, int n, uint32_t by, cudaStream_t s) {
+    k_advance<<<(n + 255) / 256, 256, 0, s>>>(ctr, n, by);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+// ================================================================= replica exchange
+// Swap of temperature labels between neighbouring slots (the reference relabels
+// TemperatureMeshArray and never moves spins, src/PT.f90:264-268).  Criterion
+// min(1, exp((b_t - b_{t+1})(E_t - E_{t+1}))) with FP64 running energies.
+// EVEN_ODD: all pairs (t, t+1) with t = round parity, in parallel (disjoint pairs).
+// RANDOM_PAIRS: n sequential attempts at Index1 = nint(u (n-1)) (src/PT.f90:236-244).
+__global__ void k_exchange(ExchangeLaunch a) {
+    const int n = a.n;
+    const uint32_t round = *a.round;
+    const uint2 key = philox_key(a.seed);
+    const uint32_t tagw = (a.ensemble << 8) | kTagExchange;
+    if (a.scheme == 0) {
+        for (int t = (int)(round & 1u) + 2 * threadIdx.x; t + 1 < n; t += 2 * blockDim.x) {
+            const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)t, round, 0u, tagw), key);
+            const int ra = a.t2r[t], rb = a.t2r[t + 1];
+            const double d = (a.beta_t[t] - a.beta_t[t + 1]) * (a.acc[ra].e - a.acc[rb].e);
+            const double u = (double)(2u * (r4.x >> 9) + 1u) * (1.0 / 16777216.0);
+            a.stats[t] += 1ull;
+            if (d >= 0.0 || u < exp(d)) {
+                a.t2r[t] = rb; a.t2r[t + 1] = ra;
+                a.stats[(n - 1) + t] += 1ull;
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        for (int q = 0; q < n; ++q) {
+            const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)q, round, 1u, tagw), key);
+            const double u0 = (double)(2u * (r4.x >> 9) + 1u) * (1.0 / 16777216.0);
+            const double u1 = (double)(2u * (r4.y >> 9) + 1u) * (1.0 / 16777216.0);
+            const double xv = u0 * (double)(n - 1);
+            const int i1 = (int)(xv >= 0.0 ? floor(xv + 0.5) : -floor(-xv + 0.5));
+            const int i2 = i1 == 0 ? 1 : (i1 == n - 1 ? n - 2 : i1 + 1);
+            const int t = i1 < i2 ? i1 : i2;
+            const int ra = a.t2r[t], rb = a.t2r[t + 1];
+            const double d = (a.beta_t[t] - a.beta_t[t + 1]) * (a.acc[ra].e - a.acc[rb].e);
+            a.stats[t] += 1ull;
+            if (d >= 0.0 || u1 < exp(d)) {
+                a.t2r[t] = rb; a.t2r[t + 1] = ra;
+                a.stats[(n - 1) + t] += 1ull;
+            }
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int r = a.t2r[t];
+        a.r2t[r] = t;
+        a.beta_rep[r] = a.beta_t[t];
+    }
+    if (threadIdx.x == 0) *a.round = round + 1u;
+}
+
+int launch_exchange(const ExchangeLaunch& a, cudaStream_t s) {
+    if (a.n < 2) return ISING_OK;
+    k_exchange<<<1, 256, 0, s>>>(a);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+// ================================================================= per-sweep record
+// One row per temperature slot t: observables of the replica that holds slot t now.
+__global__ void k_record(RecordLaunch a) {
+    const int c = *a.count;
+    if (c < a.cap) {
+        for (int t = threadIdx.x; t < a.n_rep; t += blockDim.x) {
+            const int rep = a.t2r[t];
+            const Acc4 v = a.acc[rep];
+            double* o = a.series + ((int64_t)t * a.cap + c) * 4;
+            const double m = sqrt(v.mx * v.mx + v.my * v.my + v.mz * v.mz) / (double)a.natoms;
+            double qs = 0.0;
+            for (int z = 0; z < a.nz; ++z) qs += a.q[(int64_t)rep * a.nz + z];
+            const int zmid = a.nz / 2 - 1 >= 0 ? a.nz / 2 - 1 : 0;  // winding_array(numCellsZ/2)
+            o[0] = v.e;
+            o[1] = m;
+            o[2] = a.q[(int64_t)rep * a.nz + zmid];
+            o[3] = qs / (double)a.nz;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && c < a.cap) *a.count = c + 1;
+}
+
+int launch_record(const RecordLaunch& a, cudaStream_t s) {
+    k_record<<<1, 256, 0, s>>>(a);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+// ================================================================= host-layout conversion
+// atomSpins(numAtoms,3) column-major FP64 is the planes layout already; only the width
+// changes.  Zero or non-finite vectors raise the NaN status (src/energyMin.f90:330-331).
+__global__ void k_spins_from_f64(const double* in, float* out, int64_t N, int* status) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = in[i], y = in[N + i], z = in[2 * N + i];
+        const double n2 = x * x + y * y + z * z;
+        if (!(n2 > 0.0) || !isfinite(n2)) atomicOr(status, kStatNan);
+        out[i] = (float)x; out[N + i] = (float)y; out[2 * N + i] = (float)z;
+    }
+}
+
+__global__ void k_spins_to_f64(const float* in, double* out, int64_t N) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 3 * N; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (double)in[i];
+}
+
+int launch_spins_from_f64(const double* in, float* out, int64_t natoms, int* status, cudaStream_t s) {
+    int blocks = (int)((natoms + 255) / 256);
+    if (blocks > 8192) blocks = 8192;
+    k_spins_from_f64<<<blocks, 256, 0, s>>>(in, out, natoms, status);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+int launch_spins_to_f64(const float* in, double* out, int64_t natoms, cudaStream_t s) {
+    int blocks = (int)((3 * natoms + 255) / 256);
+    if (blocks > 8192) blocks = 8192;
+    k_spins_to_f64<<<blocks, 256, 0, s>>>(in, out, natoms);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
+}  // namespace isg

@@ -1,0 +1,81 @@
+"""CPU tests of the product's host lattice compiler (meshes built with device = -1) against
+the oracle's per-atom restatement of makeChainMesh / initAtomShells / assignNearestNeighbors /
+DerivativeList (src/chainMesh.f90)."""
+import numpy as np
+import pytest
+
+CASES = [
+    ("sc3", "SC", (3, 3, 3)), ("sc4", "SC", (4, 4, 4)), ("sc5", "SC", (5, 5, 5)),
+    ("sc_rect", "SC", (4, 6, 8)), ("sc_odd", "SC", (5, 3, 7)),
+    ("bcc4", "BCC", (4, 4, 4)), ("bcc3", "BCC", (3, 4, 3)),
+    ("hk3", "HK", (3, 3, 3)), ("hk4", "HK", (4, 4, 4)),
+]
+
+
+def _cell(oracle, kind):
+    if kind == "SC":
+        return oracle.SC_CELL
+    if kind == "BCC":
+        return oracle.BCC_CELL
+    return oracle.HYPER_KAGOME_CELL
+
+
+@pytest.mark.parametrize("name,kind,dims", CASES, ids=[c[0] for c in CASES])
+def test_lattice_tables_match_oracle(oracle, ib, name, kind, dims):
+    frac, (a, b, c, ab, bc, ca) = _cell(oracle, kind)
+    om = oracle.Mesh(frac, *dims, a, b, c, ab, bc, ca)
+    pm = ib.ChainMesh(*dims, frac, a, b, c, ab, bc, ca, device=-1)
+    assert pm.numAtoms == om.natoms
+    assert np.array_equal(pm.positions(), om.positions())
+    # shells as ordered lists (positions are exact here, so the order is identical)
+    for atom in range(om.natoms):
+        for s in (0, 1):
+            assert np.array_equal(pm.neighbours(atom, s), om.shell(atom, s)), (atom, s)
+        assert np.array_equal(pm.neighbours(atom, -1), om.neighbor_list(atom)), atom
+    assert np.array_equal(pm.derivative_list(), om.derivative_table())
+    v = om.vectors()
+    assert np.allclose(pm.a_vec, v[0]) and np.allclose(pm.b_vec, v[1]) and np.allclose(pm.c_vec, v[2])
+
+
+def test_non_orthogonal_cell_sets(oracle, ib):
+    # monoclinic cell with an inexact lattice constant: neighbour SETS must agree
+    frac = np.array([[0.0, 0.0, 0.0], [0.5, 0.5, 0.0]], np.float32)
+    args = (5, 5, 4, frac, 2.8, 3.1, 2.9, 90.0, 90.0, 100.0)
+    om = oracle.Mesh(frac, 5, 5, 4, 2.8, 3.1, 2.9, 90.0, 90.0, 100.0)
+    pm = ib.ChainMesh(*args, device=-1)
+    for atom in range(0, om.natoms, 7):
+        for s in (0, 1):
+            assert sorted(pm.neighbours(atom, s)) == sorted(om.shell(atom, s))
+        assert sorted(pm.neighbours(atom, -1)) == sorted(om.neighbor_list(atom))
+
+
+def test_colouring_is_independent(oracle, ib):
+    for kind, dims in (("SC", (6, 6, 6)), ("SC", (5, 5, 5)), ("BCC", (4, 4, 4)), ("HK", (4, 4, 4))):
+        frac, (a, b, c, ab, bc, ca) = _cell(oracle, kind)
+        pm = ib.ChainMesh(*dims, frac, a, b, c, ab, bc, ca, device=-1)
+        for Jp in (0.0, 0.2):
+            col, n = pm.colouring(ib.params(J=-1.0, J_prime=Jp))
+            shells = (0, 1) if Jp else (0,)
+            for atom in range(pm.numAtoms):
+                for s in shells:
+                    nb = pm.neighbours(atom, s)
+                    assert np.all(col[nb] != col[atom])
+            if kind == "SC" and dims[0] % 2 == 0 and Jp == 0.0:
+                assert n == 2 and pm.checkerboard
+            deg = sum(len(pm.neighbours(0, s)) for s in shells)
+            assert n <= deg + 1  # greedy bound
+
+
+def test_mesh_argument_errors(ib):
+    with pytest.raises(ib.IsingError) as e:
+        ib.ChainMesh.simple_cubic(2, device=-1)
+    assert e.value.status == 1
+    with pytest.raises(ib.IsingError):
+        ib.ChainMesh(4, 4, 4, np.zeros((17, 3), np.float32), 1, 1, 1, device=-1)
+    with pytest.raises(ib.IsingError) as e:
+        ib.ChainMesh(4, 4, 4, np.array([[np.nan, 0, 0]], np.float32), 1, 1, 1, device=-1)
+    assert e.value.status == 2
+    m = ib.ChainMesh.simple_cubic(4, device=-1)
+    with pytest.raises(ib.IsingError) as e:
+        m.get_spins(0)  # no device state on a lattice-only mesh
+    assert e.value.status == 1
