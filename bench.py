@@ -64,8 +64,8 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, bus_id=None):
-        self.bus_id = (bus_id or "").lower()
+    def __init__(self, bus=None):
+        self.bus = bus if isinstance(bus, int) else None  # PCI bus number of the timed GPU
         self.proc = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
 
@@ -93,7 +93,11 @@ class ClockSampler:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
-            if self.bus_id and not parts[0].lower().endswith(self.bus_id[-12:]):
+            try:
+                bus = int(parts[0].split(":")[1], 16)
+            except (IndexError, ValueError):
+                bus = None
+            if self.bus is not None and bus is not None and bus != self.bus:
                 continue
             rows.append(parts)
         if not rows:
@@ -206,8 +210,11 @@ def run_gpu(args, w):
     updates_per_step = R * N * k
     value = world * updates_per_step * args.steps / (ms / 1e3)
 
-    # dominant kernel: the colour-class sweep, timed alone on the same stream
+    # dominant kernel: the colour-pass kernel, timed alone on the same stream over n_relax
+    # sweeps (the relax call issues only colour-pass launches plus one fold and one advance)
+    group, per_round, kern_id = pt.schedule(k)
     n_relax = max(4, min(40, args.steps * k // 2))
+    launches = pt.schedule(n_relax)[1]
     pt.relax(2)
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -216,8 +223,8 @@ def run_gpu(args, w):
     e1.record(stream)
     barrier()
     sweep_ms = e0.elapsed_time(e1) / n_relax
-    launch_ms = sweep_ms / 2.0  # two colour classes per sweep
-    bytes_per_launch = BYTES_PER_UPDATE * R * N / 2
+    launch_ms = e0.elapsed_time(e1) / launches
+    bytes_per_launch = BYTES_PER_UPDATE * R * N * n_relax / launches
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -281,9 +288,9 @@ def run_gpu(args, w):
         rate, sample = cpu_reference_rate(w, 2, 1, threads, L_sample=min(L, 64))
         cpu = {"value": rate, "unit": "spin-updates/s", "cores": threads, "kind": "port", "sample": sample}
 
-    # launches of this library inside the timed region: 2 colour kernels per sweep plus
-    # fold + exchange + counter advance per round
-    launches = args.steps * (2 * k + 3)
+    # launches of this library inside the timed region: the paired colour passes of a round
+    # (G*k + 1, or 2k with one group) plus fold + exchange + counter advance
+    launches = args.steps * (per_round + 3)
     if rank == 0:
         line = {
             "metric": "spin-updates/s", "value": value, "unit": "spin-updates/s", "n_gpus": world,
@@ -295,12 +302,15 @@ def run_gpu(args, w):
                        "l2": "state larger than L2 (no flush)" if R * N * 12 > 126e6 else "state fits L2; no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
-                         "kernel": "k_sc_colour", "launch_ms": launch_ms,
-                         "bytes_per_launch": bytes_per_launch},
+                         "kernel": "k_cb_sweep", "launch_ms": launch_ms,
+                         "bytes_per_launch": bytes_per_launch, "sweep_ms": sweep_ms,
+                         "basis": "24 B per attempted update (one FP32 x,y,z read + write per site per sweep)"},
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
+            "schedule": {"l2_group_replicas": group, "colour_pass_launches_per_round": per_round,
+                         "kernel": {0: "stencil", 1: "k_cb_sweep", 2: "k_cb_tma"}[kern_id]},
         }
         print(json.dumps(line), flush=True)
     pt.close()

@@ -68,7 +68,7 @@ typedef struct {
     int n_shells;            /* neighbour shells built (default 2) */
     int n_replicas;          /* replica spin buffers held on the device */
     int shell_size[2];       /* entries per atom in shells 1 and 2 (sublattice 0) */
-    int checkerboard;        /* 1 if the SC 2-colour fast path applies */
+    int checkerboard;        /* 1 if the SC 2-colour fast path applies (even nx, ny; nz % 4 == 0) */
     double a_vec[3], b_vec[3], c_vec[3];
 } ising_mesh_info;
 
@@ -136,8 +136,8 @@ int ising_params_reference(int which, double J, double J_prime, double Dz, doubl
                            double B, ising_params* p);
 
 /* Colour class of every atom as the sweep uses it for the Hamiltonian p: the checkerboard
- * (x+y+z)&1 on even simple-cubic meshes without J', a verified greedy colouring of the active
- * shells otherwise.  No reference counterpart: Metropolis_mcs draws random parity cells
+ * (x+y+z)&1 on simple-cubic meshes with even nx, ny, nz % 4 == 0 and no J', a verified greedy
+ * colouring of the active shells otherwise.  No reference counterpart: Metropolis_mcs draws random parity cells
  * instead (src/energyMin.f90:288-316). */
 int ising_mesh_colouring(ising_mesh* mesh, const ising_params* p, int* colour_of, int* n_colours);
 
@@ -198,6 +198,8 @@ typedef struct {
     int resync_every;         /* rounds between FP64 energy resyncs (0 = never) */
     int record;               /* 1: record E, |M|, Q per sweep into a device series */
     int record_capacity;      /* sweeps to keep per replica when record = 1 */
+    int l2_group;             /* replicas per group of the L2-paired sweep schedule (0 = auto) */
+    int sweep_kernel;         /* checkerboard meshes: 0 auto, 1 register kernel, 2 TMA-staged kernel */
 } ising_pt_options;
 
 /* Replaces the PT state of src/PT.f90:193-204 (TemperatureMeshArray, TemperatureArray):
@@ -212,6 +214,11 @@ int ising_pt_run(ising_pt* pt, int sweeps_per_swap, int rounds);
 /* n_sweeps sweeps of every replica at its current temperature without exchange: the
  * "relax each domain" loop of src/PT.f90:276-287. */
 int ising_pt_relax(ising_pt* pt, int n_sweeps);
+/* Launch schedule of a round: replicas per L2 group, colour-pass launches per round of
+ * sweeps_per_swap sweeps, and which colour-pass kernel runs (1 register, 2 TMA-staged,
+ * 0 the greedy-colouring stencil kernel).  No reference counterpart. */
+int ising_pt_schedule(const ising_pt* pt, int sweeps_per_swap, int* l2_group, int* pass_launches,
+                      int* kernel);
 /* temperature slot -> replica (TemperatureMeshArray(i, :), src/PT.f90:58) */
 int ising_pt_permutation(const ising_pt* pt, int* temp_to_replica);
 /* running FP64 energies and magnetisation vectors by replica */

@@ -48,7 +48,7 @@ class Params(C.Structure):
 class PTOptions(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("ensemble", C.c_uint32), ("move", C.c_int), ("r", C.c_double),
                 ("scheme", C.c_int), ("resync_every", C.c_int), ("record", C.c_int),
-                ("record_capacity", C.c_int)]
+                ("record_capacity", C.c_int), ("l2_group", C.c_int), ("sweep_kernel", C.c_int)]
 
 
 _P = C.POINTER
@@ -84,6 +84,7 @@ _SIGS = {
     "ising_pt_destroy": (_i, [_vp]),
     "ising_pt_run": (_i, [_vp, _i, _i]),
     "ising_pt_relax": (_i, [_vp, _i]),
+    "ising_pt_schedule": (_i, [_vp, _i, _P(_i), _P(_i), _P(_i)]),
     "ising_pt_permutation": (_i, [_vp, _P(_i)]),
     "ising_pt_energies": (_i, [_vp, _P(_d), _P(_d)]),
     "ising_pt_resync": (_i, [_vp]),

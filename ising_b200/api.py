@@ -318,7 +318,7 @@ class ParallelTempering:
 
     def __init__(self, mesh: ChainMesh, betas, p: Params, seed: int = 0x15196, ensemble: int = 0,
                  move: int = MOVE_BALL, r: float = 0.2, scheme: int = PT_EVEN_ODD, resync_every: int = 0,
-                 record: bool = False, record_capacity: int = 0):
+                 record: bool = False, record_capacity: int = 0, l2_group: int = 0, sweep_kernel: int = 0):
         self.mesh = mesh
         self.betas = np.ascontiguousarray(betas, dtype=np.float64)
         self.n = len(self.betas)
@@ -326,6 +326,8 @@ class ParallelTempering:
         o = PTOptions()
         o.seed, o.ensemble, o.move, o.r, o.scheme = seed, ensemble, move, r, scheme
         o.resync_every, o.record, o.record_capacity = resync_every, int(record), record_capacity
+        o.l2_group = l2_group
+        o.sweep_kernel = sweep_kernel
         self.opt = o
         h = C.c_void_p()
         _lib.call("ising_pt_create", mesh.handle, self.n, _dp(self.betas), C.byref(p), C.byref(o), C.byref(h))
@@ -348,6 +350,12 @@ class ParallelTempering:
     def relax(self, n_sweeps: int):
         """Sweeps without exchange (the relax loop of src/PT.f90:276-287)."""
         _lib.call("ising_pt_relax", self._h, n_sweeps)
+
+    def schedule(self, sweeps_per_swap: int):
+        """(replicas per L2 group, colour-pass launches per round, kernel id)."""
+        g, n, k = C.c_int(), C.c_int(), C.c_int()
+        _lib.call("ising_pt_schedule", self._h, sweeps_per_swap, C.byref(g), C.byref(n), C.byref(k))
+        return g.value, n.value, k.value
 
     def permutation(self) -> np.ndarray:
         out = np.empty(self.n, dtype=np.int32)

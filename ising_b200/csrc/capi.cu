@@ -140,7 +140,7 @@ int upload_stencil(ising_mesh* m, const ising_params& p, bool legacy, Slot* dst_
     for (int s = 0; s < L.nsub; ++s) {
         int c = 0;
         auto add = [&](const NbrSlot& q, float w, bool dmi) -> int {
-            if (c >= kMaxSlots) return fail(ISING_ERR_ARG, "stencil exceeds 64 slots");
+            if (c >= kMaxSlots) return fail(ISING_ERR_ARG, "stencil exceeds 128 slots");
             Slot e{};
             e.dx = (int8_t)q.dx; e.dy = (int8_t)q.dy; e.dz = (int8_t)q.dz; e.sub = (uint8_t)q.sub;
             e.w = w;
@@ -218,6 +218,8 @@ int ensure_colouring(ising_mesh* m, bool shell2, Colouring** out) {
 // One sweep plan: which kernels to launch for a set of replicas.
 struct SweepPlan {
     bool sc = false;
+    bool tma = false;          // TMA-staged colour pass (nz % 8 == 0)
+    int group = 1;             // replicas per L2 group in the paired schedule
     int dmi_kind = 0;
     HamDev ham{};
     Colouring* col = nullptr;
@@ -230,10 +232,16 @@ struct SweepPlan {
 int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots, int* count) {
     plan->ham = make_ham(p);
     const bool sh2 = uses_shell2(m->lat, p);
-    if (m->checkerboard && !sh2) {
+    if (m->layout.cb && !sh2) {
         plan->sc = true;
         ISG_TRY(sc_dmi(m, p, &plan->ham, &plan->dmi_kind));
-        plan->slots_per_rep = sc_slots_per_rep(m->lat.nx, m->lat.ny, m->lat.nz);
+        const Lattice& Lt = m->lat;
+        plan->tma = false;   // the register kernel measures faster; the TMA pass is opt-in
+        (void)Lt;
+        plan->slots_per_rep = std::max(cb_slots_per_rep(), plan->tma ? cb_tma_slots_per_rep(Lt.nx, Lt.ny, Lt.nz) : 0);
+        // replicas per group: the two groups of a paired launch stay well inside the 126 MB L2
+        const double rep_bytes = 12.0 * (double)m->lat.natoms;
+        plan->group = std::max(1, (int)(kL2GroupBytes / rep_bytes));
         return ISING_OK;
     }
     plan->sc = false;
@@ -248,38 +256,85 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
     return ISING_OK;
 }
 
-// Enqueue one sweep (all colour classes) for replicas [rep_first, rep_first + n_rep).
-int enqueue_sweep(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_rep,
-                  const double* d_beta_rep, uint32_t sweep_offset, uint64_t seed, uint32_t ensemble,
-                  int move, double r, double* partials) {
+// Checkerboard schedule for n_sweeps sweeps of replicas [rep_first, rep_first + n_rep):
+// replica groups g = 0..G-1, first-colour units R_0..R_{M-1} and second-colour units
+// B_0..B_{M-1} in (sweep, group) order.  With G >= 2: launch 0 = {R_0}, launch j = {B_{j-1},
+// R_j}, launch M = {B_{M-1}}; R_j needs B_{j-G} (same group, previous sweep), finished by
+// launch j-G+1 < j, and B_j needs R_j, finished by launch j.  With one group the units run
+// one per launch.
+int enqueue_cb(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_rep, const double* d_beta_rep,
+               uint32_t sw0, int n_sweeps, uint64_t seed, uint32_t ensemble, int move, double r,
+               double* partials) {
     const Lattice& L = m->lat;
-    float* base = m->d_spins + (int64_t)rep_first * 3 * L.natoms;
-    if (plan.sc) {
-        SweepLaunch a{};
-        a.spins = base; a.natoms = L.natoms; a.nx = L.nx; a.ny = L.ny; a.nz = L.nz;
-        a.n_rep = n_rep; a.rep_first = rep_first; a.beta_rep = d_beta_rep; a.sweep_ctr = m->d_sweep;
-        a.sweep_offset = sweep_offset; a.seed = seed; a.ensemble = ensemble; a.move = move;
-        a.r = (float)r; a.ham = plan.ham; a.dmi_kind = plan.dmi_kind; a.partials = partials;
-        a.slots_per_rep = plan.slots_per_rep; a.status = m->d_status;
-        for (int c = 0; c < 2; ++c) ISG_TRY(launch_sc_colour(a, c, m->stream));
+    CbLaunch a{};
+    a.spins = m->d_spins; a.natoms = L.natoms; a.nx = L.nx; a.ny = L.ny; a.nz = L.nz;
+    a.beta_rep = d_beta_rep; a.sweep_ctr = m->d_sweep; a.seed = seed; a.ensemble = ensemble; a.r = (float)r;
+    a.ham = plan.ham; a.partials = partials; a.slots_per_rep = plan.slots_per_rep; a.status = m->d_status;
+    const int G = (n_rep + plan.group - 1) / plan.group;
+    auto unit = [&](int j, int colour) {
+        const int sw = j / G, g = j % G;
+        CbSeg sgm;
+        sgm.rep_first = rep_first + g * plan.group;
+        sgm.n_rep = std::min(plan.group, rep_first + n_rep - sgm.rep_first);
+        sgm.colour = colour;
+        sgm.sweep_offset = sw0 + (uint32_t)sw;
+        return sgm;
+    };
+    const int M = G * n_sweeps;
+    if (G == 1) {
+        for (int j = 0; j < M; ++j)
+            for (int c = 0; c < 2; ++c) {
+                a.seg[0] = unit(j, c);
+                a.seg[1] = CbSeg{0, 0, 0, 0};
+                a.n_seg = 1;
+                ISG_TRY(plan.tma ? launch_cb_tma(a, move, plan.dmi_kind, m->stream)
+                                 : launch_cb_sweep(a, move, plan.dmi_kind, m->stream));
+            }
         return ISING_OK;
     }
-    GeneralLaunch g{};
-    g.spins = base; g.natoms = L.natoms; g.nx = L.nx; g.ny = L.ny; g.nz = L.nz; g.nsub = L.nsub;
-    g.n_rep = n_rep; g.rep_first = rep_first; g.beta_rep = d_beta_rep; g.sweep_ctr = m->d_sweep;
-    g.sweep_offset = sweep_offset; g.seed = seed; g.ensemble = ensemble; g.move = move; g.r = (float)r;
-    g.ham = plan.ham; g.st = StencilDev{plan.d_slots, plan.d_count, L.nsub}; g.partials = partials;
-    g.slots_per_rep = plan.slots_per_rep;
-    g.status = m->d_status;
-    int slot = 0;
-    for (int k = 0; k < plan.col->ncol; ++k) {
-        g.sites = plan.col->d_sites + plan.col->class_start[k];
-        g.n_sites = plan.col->class_start[k + 1] - plan.col->class_start[k];
-        g.slot_base = slot;
-        ISG_TRY(launch_general_colour(g, m->stream));
-        slot += general_slots_for(g.n_sites);
+    for (int j = 0; j <= M; ++j) {
+        a.n_seg = 0;
+        if (j >= 1) a.seg[a.n_seg++] = unit(j - 1, 1);
+        if (j < M) a.seg[a.n_seg++] = unit(j, 0);
+        if (a.n_seg == 1) a.seg[1] = CbSeg{0, 0, 0, 0};
+        ISG_TRY(plan.tma ? launch_cb_tma(a, move, plan.dmi_kind, m->stream)
+                         : launch_cb_sweep(a, move, plan.dmi_kind, m->stream));
     }
     return ISING_OK;
+}
+
+// n_sweeps consecutive sweeps (sweep offsets sw0 .. sw0+n_sweeps-1) of replicas
+// [rep_first, rep_first + n_rep), all colour classes.
+int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_rep, const double* d_beta_rep,
+                   uint32_t sw0, int n_sweeps, uint64_t seed, uint32_t ensemble, int move, double r,
+                   double* partials) {
+    if (plan.sc)
+        return enqueue_cb(m, plan, rep_first, n_rep, d_beta_rep, sw0, n_sweeps, seed, ensemble, move, r, partials);
+    const Lattice& L = m->lat;
+    GeneralLaunch g{};
+    g.spins = m->d_spins + (int64_t)rep_first * 3 * L.natoms;
+    g.natoms = L.natoms; g.nx = L.nx; g.ny = L.ny; g.nz = L.nz; g.nsub = L.nsub;
+    g.n_rep = n_rep; g.rep_first = rep_first; g.beta_rep = d_beta_rep; g.sweep_ctr = m->d_sweep;
+    g.seed = seed; g.ensemble = ensemble; g.move = move; g.r = (float)r;
+    g.ham = plan.ham; g.st = StencilDev{plan.d_slots, plan.d_count, L.nsub}; g.layout = m->layout;
+    g.partials = partials; g.slots_per_rep = plan.slots_per_rep; g.status = m->d_status;
+    for (int sw = 0; sw < n_sweeps; ++sw) {
+        g.sweep_offset = sw0 + (uint32_t)sw;
+        int slot = 0;
+        for (int k = 0; k < plan.col->ncol; ++k) {
+            g.sites = plan.col->d_sites + plan.col->class_start[k];
+            g.n_sites = plan.col->class_start[k + 1] - plan.col->class_start[k];
+            g.slot_base = slot;
+            ISG_TRY(launch_general_colour(g, m->stream));
+            slot += general_slots_for(g.n_sites);
+        }
+    }
+    return ISING_OK;
+}
+
+int enqueue_sweep(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_rep, const double* d_beta_rep,
+                  uint32_t sweep_offset, uint64_t seed, uint32_t ensemble, int move, double r, double* partials) {
+    return enqueue_sweeps(m, plan, rep_first, n_rep, d_beta_rep, sweep_offset, 1, seed, ensemble, move, r, partials);
 }
 
 int check_replica(const ising_mesh* m, int replica) {
@@ -295,7 +350,7 @@ int enqueue_energy(ising_mesh* m, const ising_params& p, int first, int n, doubl
     ReduceLaunch a{};
     a.spins = m->d_spins + (int64_t)first * 3 * m->lat.natoms;
     a.natoms = m->lat.natoms; a.nx = m->lat.nx; a.ny = m->lat.ny; a.nz = m->lat.nz; a.nsub = m->lat.nsub;
-    a.n_rep = n; a.ham = make_ham(p); a.st = stencil_of(m); a.out = d_out; a.block_tmp = d_tmp;
+    a.n_rep = n; a.ham = make_ham(p); a.st = stencil_of(m); a.layout = m->layout; a.out = d_out; a.block_tmp = d_tmp;
     a.blocks_per_rep = energy_blocks_for(m->lat.natoms);
     return launch_energy_mag(a, m->stream);
 }
@@ -345,6 +400,10 @@ extern "C" int ising_mesh_create(const float* frac, int nsub, int nx, int ny, in
     std::unique_ptr<ising_mesh> m(new ising_mesh());
     ISG_TRY(build_lattice(frac, nsub, nx, ny, nz, a, b, c, ab, bc, ca, shell_tol, n_shells, &m->lat));
     m->checkerboard = is_checkerboard_sc(m->lat);
+    {
+        const Lattice& L = m->lat;
+        m->layout = Layout{m->checkerboard && L.nz % 4 == 0 ? 1 : 0, L.nx, L.ny, L.nz, L.nsub, L.natoms / 2};
+    }
     if (device == -1) {  // lattice tables only
         m->device = -1;
         m->n_replicas = n_replicas;
@@ -357,7 +416,6 @@ extern "C" int ising_mesh_create(const float* frac, int nsub, int nx, int ny, in
     DeviceGuard g(device);
     m->device = device;
     m->n_replicas = n_replicas;
-    m->checkerboard = is_checkerboard_sc(m->lat);
     ISG_CUDA(cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking));
     m->stream = m->own_stream;
     const int64_t N = m->lat.natoms;
@@ -417,7 +475,7 @@ extern "C" int ising_mesh_get_info(const ising_mesh* m, ising_mesh_info* info) {
     info->n_shells = L.nshells; info->n_replicas = m->n_replicas;
     info->shell_size[0] = (int)L.shell[0][0].size();
     info->shell_size[1] = (int)L.shell[1][0].size();
-    info->checkerboard = m->checkerboard ? 1 : 0;
+    info->checkerboard = m->layout.cb;
     for (int k = 0; k < 3; ++k) { info->a_vec[k] = L.av[k]; info->b_vec[k] = L.bv[k]; info->c_vec[k] = L.cv[k]; }
     return ISING_OK;
 }
@@ -467,7 +525,7 @@ extern "C" int ising_mesh_colouring(ising_mesh* m, const ising_params* p, int* c
     ISG_TRY(validate_params(p));
     const Lattice& L = m->lat;
     const bool sh2 = uses_shell2(L, *p);
-    if (m->checkerboard && !sh2) {
+    if (m->layout.cb && !sh2) {
         for (int64_t a = 0; a < L.natoms; ++a) {
             int ix, iy, iz, s;
             L.cell_of(a, &ix, &iy, &iz, &s);
@@ -512,7 +570,7 @@ extern "C" int ising_spins_set(ising_mesh* m, int replica, const double* s) {
     ISG_TRY(staging(m, &d));
     const int64_t N = m->lat.natoms;
     ISG_CUDA(cudaMemcpyAsync(d, s, (size_t)3 * N * sizeof(double), cudaMemcpyHostToDevice, m->stream));
-    ISG_TRY(launch_spins_from_f64(d, m->d_spins + (int64_t)replica * 3 * N, N, m->d_status, m->stream));
+    ISG_TRY(launch_spins_from_f64(d, m->d_spins + (int64_t)replica * 3 * N, N, m->layout, m->d_status, m->stream));
     return check_status(m);
 }
 
@@ -524,7 +582,7 @@ extern "C" int ising_spins_get(const ising_mesh* mc, int replica, double* s) {
     double* d;
     ISG_TRY(staging(m, &d));
     const int64_t N = m->lat.natoms;
-    ISG_TRY(launch_spins_to_f64(m->d_spins + (int64_t)replica * 3 * N, d, N, m->stream));
+    ISG_TRY(launch_spins_to_f64(m->d_spins + (int64_t)replica * 3 * N, d, N, m->layout, m->stream));
     ISG_CUDA(cudaMemcpyAsync(s, d, (size_t)3 * N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
     ISG_CUDA(cudaStreamSynchronize(m->stream));
     return ISING_OK;
@@ -534,7 +592,7 @@ extern "C" int ising_spins_init_uniform(ising_mesh* m, uint64_t seed, uint32_t e
     ISG_TRY(check_replica(m, 0));
     if (ensemble >= (1u << 24)) return fail(ISING_ERR_ARG, "ensemble id must be < 2^24");
     DeviceGuard g(m->device);
-    ISG_TRY(launch_init_uniform(m->d_spins, m->lat.natoms, m->n_replicas, seed, ensemble, m->stream));
+    ISG_TRY(launch_init_uniform(m->d_spins, m->lat.natoms, m->layout, m->n_replicas, seed, ensemble, m->stream));
     ISG_CUDA(cudaStreamSynchronize(m->stream));
     return ISING_OK;
 }
@@ -590,7 +648,7 @@ extern "C" int ising_local_energy_batch(const ising_mesh* mc, int replica, int n
         LocalLaunch a{};
         a.spins = m->d_spins + (int64_t)replica * 3 * m->lat.natoms;
         a.natoms = m->lat.natoms; a.nx = m->lat.nx; a.ny = m->lat.ny; a.nz = m->lat.nz; a.nsub = m->lat.nsub;
-        a.ham = make_ham(*p); a.st = stencil_of(m); a.atoms = d_atoms; a.sprop = d_sp; a.old_e = d_old; a.new_e = d_new; a.n = k;
+        a.ham = make_ham(*p); a.st = stencil_of(m); a.layout = m->layout; a.atoms = d_atoms; a.sprop = d_sp; a.old_e = d_old; a.new_e = d_new; a.n = k;
         ISG_TRY(launch_local_energy(a, m->stream));
         ISG_CUDA(cudaMemcpyAsync(m->h_pinned + 4 * k, d_old, 2 * k * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
         ISG_CUDA(cudaStreamSynchronize(m->stream));
@@ -670,8 +728,7 @@ extern "C" int ising_metropolis_mcs(ising_mesh* m, int replica, double beta, int
     const int move = r > 0.0 ? 1 : 0;
     m->h_pinned[0] = beta;
     ISG_CUDA(cudaMemcpyAsync(m->d_beta + replica, m->h_pinned, sizeof(double), cudaMemcpyHostToDevice, m->stream));
-    for (int sw = 0; sw < n_sweeps; ++sw)
-        ISG_TRY(enqueue_sweep(m, plan, replica, 1, m->d_beta, (uint32_t)sw, seed, 0u, move, r, nullptr));
+    ISG_TRY(enqueue_sweeps(m, plan, replica, 1, m->d_beta, 0u, n_sweeps, seed, 0u, move, r, nullptr));
     ISG_TRY(launch_advance(m->d_sweep + replica, 1, (uint32_t)n_sweeps, m->stream));
     m->h_sweep[replica] += (uint32_t)n_sweeps;
     return check_status(m);
@@ -687,7 +744,7 @@ extern "C" int ising_winding_all_slices(const ising_mesh* mc, int replica, doubl
     WindingLaunch w{};
     w.spins = m->d_spins + (int64_t)replica * 3 * L.natoms;
     w.natoms = L.natoms; w.nx = L.nx; w.ny = L.ny; w.nz = L.nz; w.nsub = L.nsub; w.n_rep = 1;
-    w.plaq = m->d_plaq; w.out = m->d_winding_tmp; w.fp64 = 1;
+    w.plaq = m->d_plaq; w.layout = m->layout; w.out = m->d_winding_tmp; w.fp64 = 1;
     ISG_TRY(launch_winding(w, m->stream));
     ISG_CUDA(cudaMemcpyAsync(q, m->d_winding_tmp, L.nz * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
     ISG_CUDA(cudaStreamSynchronize(m->stream));
@@ -816,14 +873,17 @@ int pt_enqueue_round(ising_pt* pt, int k) {
     ising_mesh* m = pt->mesh;
     const int n = pt->n;
     const int move = pt->opt.move;
-    for (int sw = 0; sw < k; ++sw) {
+    if (!pt->opt.record)
+        ISG_TRY(enqueue_sweeps(m, pt->plan, 0, n, pt->d_beta_rep, 0u, k, pt->opt.seed, pt->opt.ensemble, move,
+                               pt->opt.r, pt->d_partials));
+    for (int sw = 0; sw < k && pt->opt.record; ++sw) {
         ISG_TRY(enqueue_sweep(m, pt->plan, 0, n, pt->d_beta_rep, (uint32_t)sw, pt->opt.seed, pt->opt.ensemble, move,
                               pt->opt.r, pt->d_partials));
-        if (pt->opt.record) {
+        {
             ISG_TRY(launch_fold_partials(pt->d_partials, pt->plan.slots_per_rep, n, pt->d_acc, m->stream));
             WindingLaunch w{};
             w.spins = m->d_spins; w.natoms = m->lat.natoms; w.nx = m->lat.nx; w.ny = m->lat.ny; w.nz = m->lat.nz;
-            w.nsub = m->lat.nsub; w.n_rep = n; w.plaq = m->d_plaq; w.out = pt->d_q; w.fp64 = 0;
+            w.nsub = m->lat.nsub; w.n_rep = n; w.plaq = m->d_plaq; w.layout = m->layout; w.out = pt->d_q; w.fp64 = 0;
             ISG_TRY(launch_winding(w, m->stream));
             RecordLaunch rl{};
             rl.acc = pt->d_acc; rl.q = pt->d_q; rl.t2r = pt->d_t2r; rl.nz = m->lat.nz; rl.n_rep = n;
@@ -865,6 +925,16 @@ extern "C" int ising_pt_create(ising_mesh* m, int n, const double* betas, const 
         (st = dev_alloc(&pt->d_plan_count, kMaxSub)))
         return bail(st);
     if ((st = make_plan(m, *p, &pt->plan, pt->d_plan_slots, pt->d_plan_count)) != ISING_OK) return bail(st);
+    if (opt->l2_group < 0) return bail(fail(ISING_ERR_ARG, "l2_group must be >= 0"));
+    if (opt->l2_group > 0) pt->plan.group = opt->l2_group;
+    if (opt->sweep_kernel < 0 || opt->sweep_kernel > 2) return bail(fail(ISING_ERR_ARG, "sweep_kernel must be 0, 1 or 2"));
+    if (opt->sweep_kernel == 2) {
+        const Lattice& Lt = m->lat;
+        if (!pt->plan.sc || !cb_tma_supported(Lt.nx, Lt.ny, Lt.nz))
+            return bail(fail(ISING_ERR_ARG, "the TMA-staged kernel needs a checkerboard mesh with nz % 8 == 0"));
+        pt->plan.tma = true;
+        pt->plan.slots_per_rep = std::max(pt->plan.slots_per_rep, cb_tma_slots_per_rep(Lt.nx, Lt.ny, Lt.nz));
+    }
     const int tmp = energy_tmp_doubles(m, n);
     if ((st = dev_alloc(&pt->d_beta_t, n)) || (st = dev_alloc(&pt->d_beta_rep, m->n_replicas)) ||
         (st = dev_alloc(&pt->d_t2r, n)) || (st = dev_alloc(&pt->d_r2t, n)) || (st = dev_alloc(&pt->d_acc, n)) ||
@@ -931,12 +1001,26 @@ extern "C" int ising_pt_relax(ising_pt* pt, int n_sweeps) {
     if (n_sweeps < 0) return fail(ISING_ERR_ARG, "n_sweeps must be >= 0");
     ising_mesh* m = pt->mesh;
     DeviceGuard g(m->device);
-    for (int sw = 0; sw < n_sweeps; ++sw)
-        ISG_TRY(enqueue_sweep(m, pt->plan, 0, pt->n, pt->d_beta_rep, (uint32_t)sw, pt->opt.seed, pt->opt.ensemble,
-                              pt->opt.move, pt->opt.r, pt->d_partials));
+    ISG_TRY(enqueue_sweeps(m, pt->plan, 0, pt->n, pt->d_beta_rep, 0u, n_sweeps, pt->opt.seed, pt->opt.ensemble,
+                           pt->opt.move, pt->opt.r, pt->d_partials));
     ISG_TRY(launch_fold_partials(pt->d_partials, pt->plan.slots_per_rep, pt->n, pt->d_acc, m->stream));
     ISG_TRY(launch_advance(m->d_sweep, pt->n, (uint32_t)n_sweeps, m->stream));
     return check_status(m);
+}
+
+extern "C" int ising_pt_schedule(const ising_pt* pt, int k, int* group, int* launches, int* kernel) {
+    if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
+    if (k < 1) return fail(ISING_ERR_ARG, "sweeps_per_swap must be >= 1");
+    const SweepPlan& P = pt->plan;
+    int grp = P.sc ? P.group : pt->n;
+    int G = (pt->n + grp - 1) / grp;
+    int L = 0;
+    if (P.sc) L = G > 1 ? G * k + 1 : 2 * k;
+    else L = k * P.col->ncol;
+    if (group) *group = grp;
+    if (launches) *launches = L;
+    if (kernel) *kernel = P.sc ? (P.tma ? 2 : 1) : 0;
+    return ISING_OK;
 }
 
 extern "C" int ising_pt_permutation(const ising_pt* pt, int* t2r) {

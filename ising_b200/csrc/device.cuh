@@ -58,23 +58,33 @@ __device__ __forceinline__ f3 cross(f3 a, f3 b) {
     return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
 
-// Trial spin from four uniforms (u0: cos theta, u1: azimuth, u2: ball radius).
-// MOVE 0: fresh uniform unit vector.  MOVE 1: S' = norm(S + r*cbrt(u2)*v), the ball move
-// of UniformRandomInSphere (reference src/energyMin.f90:49-68).
+// Hardware approximations (PTX ISA: sin/cos/ex2/lg2/sqrt/rsqrt .approx).  Their error
+// (about 2^-21 relative, 2^-20.5 absolute for sin/cos on [-pi, pi]) is below the FP32 spin
+// resolution; the proposals stay symmetric because they depend only on fresh uniforms.
+__device__ __forceinline__ float ax_sin(float x) { float y; asm("sin.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+__device__ __forceinline__ float ax_cos(float x) { float y; asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+__device__ __forceinline__ float ax_ex2(float x) { float y; asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+__device__ __forceinline__ float ax_lg2(float x) { float y; asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+__device__ __forceinline__ float ax_sqrt(float x) { float y; asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+__device__ __forceinline__ float ax_rsqrt(float x) { float y; asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+
+// Trial spin from uniforms (u0: cos theta, u1: azimuth, u2: ball radius).
+// MOVE 0: fresh uniform unit vector (|v| = 1 to the sin/cos accuracy; not renormalised).
+// MOVE 1: S' = norm(S + r*cbrt(u2)*v), the ball move of UniformRandomInSphere
+// (reference src/energyMin.f90:49-68).
 template <int MOVE>
 __device__ __forceinline__ f3 propose(f3 s, float u0, float u1, float u2, float r) {
     const float cz = fmaf(2.0f, u0, -1.0f);                       // exact
-    const float q = (1.0f - cz) * (1.0f + cz);
-    const float st = q * rsqrtf(q);
-    float sn, cs;
-    __sincosf(3.14159265f * (2.0f * (u1 - 0.5f)), &sn, &cs);      // azimuth in (-pi, pi)
-    f3 v = {st * cs, st * sn, cz};
+    const float st = ax_sqrt(fmaf(-cz, cz, 1.0f));
+    const float ph = 6.28318531f * (u1 - 0.5f);                    // azimuth in (-pi, pi)
+    f3 v = {st * ax_cos(ph), st * ax_sin(ph), cz};
     if (MOVE == 1) {
-        const float rho = r * __expf(0.33333334f * __logf(u2));   // r * cbrt(u2)
+        const float rho = r * ax_ex2(0.33333334f * ax_lg2(u2));   // r * cbrt(u2)
         v = {fmaf(rho, v.x, s.x), fmaf(rho, v.y, s.y), fmaf(rho, v.z, s.z)};
+        const float rn = ax_rsqrt(dot(v, v));
+        v = {v.x * rn, v.y * rn, v.z * rn};
     }
-    const float rn = rsqrtf(dot(v, v));
-    return {v.x * rn, v.y * rn, v.z * rn};
+    return v;
 }
 #endif  // __CUDACC__
 
@@ -97,13 +107,38 @@ struct Slot {
 };
 
 constexpr int kMaxSub = 16;
-constexpr int kMaxSlots = 64;
+constexpr int kMaxSlots = 128;
 
 struct StencilDev {
     const Slot* slots;   // n_sub * kMaxSlots, slot s of sublattice i at [i*kMaxSlots + s]
     const int* count;    // per sublattice
     int nsub;
 };
+
+// Storage order of a replica's three spin planes.  cb = 0: the reference atom order.
+// cb = 1 (simple-cubic meshes with even extents): colour-separated -- the sites with
+// (x+y+z)&1 == 0 first, then colour 1; inside a colour, row order (x, y) with the packed
+// z index z>>1, so a colour pass reads and writes whole sectors of its own colour.
+struct Layout {
+    int cb;
+    int nx, ny, nz, nsub;
+    int64_t half;   // sites per colour (cb = 1)
+};
+
+__host__ __device__ __forceinline__ int64_t sidx(const Layout& L, int ix, int iy, int iz, int sub) {
+    if (!L.cb) return (((int64_t)ix * L.ny + iy) * L.nz + iz) * L.nsub + sub;
+    const int c = (ix + iy + iz) & 1;
+    return c * L.half + ((int64_t)ix * L.ny + iy) * (L.nz >> 1) + (iz >> 1);
+}
+
+// storage index of a reference-order atom index
+__host__ __device__ __forceinline__ int64_t sidx_atom(const Layout& L, int64_t atom) {
+    if (!L.cb) return atom;
+    const int iz = (int)(atom % L.nz);
+    const int64_t row = atom / L.nz;
+    const int iy = (int)(row % L.ny), ix = (int)(row / L.ny);
+    return sidx(L, ix, iy, iz, 0);
+}
 
 // Per-replica running accumulators: E, Mx, My, Mz.
 struct Acc4 { double e, mx, my, mz; };

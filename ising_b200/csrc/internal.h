@@ -97,6 +97,7 @@ struct ising_mesh {
     size_t staging_size = 0;
     double* d_winding_tmp = nullptr;     // per-slice winding results
     bool checkerboard = false;
+    isg::Layout layout{};                // storage order of the spin planes
     isg::Colouring colour[2];            // [0]: shell 1 bonds, [1]: shells 1+2
     // cached device stencils keyed by the Hamiltonian that filled their weights
     isg::Slot* d_slots = nullptr;
@@ -106,29 +107,37 @@ struct ising_mesh {
 
 namespace isg {
 constexpr int kScratchDoubles = 1 << 16;
+constexpr double kL2GroupBytes = 64.0e6;   // replica group size of the paired colour schedule
 
-// Kernel launchers (kernels.cu).
-struct SweepLaunch {
-    float* spins;          // replica block base
+// Kernel launchers.
+// Colour-separated checkerboard sweep (sweep_cb.cu): up to two segments per launch, each a
+// replica range, a colour and a sweep offset.
+struct CbSeg {
+    int rep_first, n_rep, colour;
+    uint32_t sweep_offset;
+};
+struct CbLaunch {
+    float* spins;          // replica 0 of the mesh
     int64_t natoms;
     int nx, ny, nz;
-    int n_rep;             // replicas in this launch (blockIdx.z)
-    int rep_first;         // first replica index (into beta/sweep/partials arrays)
-    const double* beta_rep;   // per replica (indexed by replica id)
-    const uint32_t* sweep_ctr; // per replica (indexed by replica id)
-    uint32_t sweep_offset;
+    CbSeg seg[2];
+    int n_seg;
+    const double* beta_rep;
+    const uint32_t* sweep_ctr;
     uint64_t seed;
     uint32_t ensemble;
-    int move;
     float r;
     HamDev ham;
-    int dmi_kind;          // 0 none, 1 bulk, 2 interfacial z, 3 generic
-    double* partials;      // [rep][slot][4]
+    double* partials;
     int slots_per_rep;
     int* status;
 };
-int launch_sc_colour(const SweepLaunch& a, int colour, cudaStream_t s);
-int sc_slots_per_rep(int nx, int ny, int nz);
+int cb_slots_per_rep();
+int launch_cb_sweep(const CbLaunch& a, int move, int dmi_kind, cudaStream_t s);
+// TMA-staged variant (sweep_tma.cu): nz % 8 == 0
+bool cb_tma_supported(int nx, int ny, int nz);
+int cb_tma_slots_per_rep(int nx, int ny, int nz);
+int launch_cb_tma(const CbLaunch& a, int move, int dmi_kind, cudaStream_t s);
 
 struct GeneralLaunch {
     float* spins;
@@ -144,6 +153,7 @@ struct GeneralLaunch {
     float r;
     HamDev ham;
     StencilDev st;
+    Layout layout;
     const int* sites;      // atoms of this colour class
     int n_sites;
     double* partials;
@@ -161,6 +171,7 @@ struct ReduceLaunch {
     int n_rep;
     HamDev ham;            // Bz already multiplied by the zeeman factor
     StencilDev st;         // slots used for the energy (weights 0.5 applied in kernel)
+    Layout layout;
     double* out;           // [rep][4]: E, Mx, My, Mz
     double* block_tmp;     // [rep][blocks][4]
     int blocks_per_rep;
@@ -177,6 +188,7 @@ struct WindingLaunch {
     int nx, ny, nz, nsub;
     int n_rep;
     const int* plaq;       // 4 entries of (dx, dy, dz, sub) relative to sublattice nsub-1
+    Layout layout;
     double* out;           // [rep][nz]
     int fp64;
 };
@@ -188,6 +200,7 @@ struct LocalLaunch {
     int nx, ny, nz, nsub;
     HamDev ham;
     StencilDev st;
+    Layout layout;
     const int64_t* atoms;
     const double* sprop;   // n x 3
     double* old_e;
@@ -196,11 +209,12 @@ struct LocalLaunch {
 };
 int launch_local_energy(const LocalLaunch& a, cudaStream_t s);
 
-int launch_init_uniform(float* spins, int64_t natoms, int n_rep, uint64_t seed,
+int launch_init_uniform(float* spins, int64_t natoms, const Layout& L, int n_rep, uint64_t seed,
                         uint32_t ensemble, cudaStream_t s);
 int launch_advance(uint32_t* ctr, int n, uint32_t by, cudaStream_t s);
-int launch_spins_from_f64(const double* in, float* out, int64_t natoms, int* status, cudaStream_t s);
-int launch_spins_to_f64(const float* in, double* out, int64_t natoms, cudaStream_t s);
+int launch_spins_from_f64(const double* in, float* out, int64_t natoms, const Layout& L, int* status,
+                          cudaStream_t s);
+int launch_spins_to_f64(const float* in, double* out, int64_t natoms, const Layout& L, cudaStream_t s);
 
 struct ExchangeLaunch {
     int n;                       // temperature slots

@@ -9,31 +9,7 @@
 
 namespace isg {
 
-// ================================================================= checkerboard sweep (SC)
-// One colour class of the simple cubic checkerboard.  Thread (k, y) of block (yb, x, rep)
-// owns the site z = 2k + ((x+y+colour)&1) of row (x, y).  Local field from the six axis
-// neighbours:  h = J sum S_j + sum_k S_k x D_k - Bz z_hat  (D.(S x S_j) = S.(S_j x D)),
-// dE = (S'-S).h - K[(S'.e)^2 - (S.e)^2]  (reference calculateHeisenbergEnergy,
-// src/energyMin.f90:86-171, rewritten in local-field form).
-constexpr int kScThreads = 256;
-
-struct ScGeom { int tx, ty, zb, yb; };
-static ScGeom sc_geom(int nx, int ny, int nz) {
-    ScGeom g;
-    const int half = nz / 2;
-    g.tx = half < 128 ? half : 128;
-    g.ty = kScThreads / g.tx;
-    if (g.ty < 1) g.ty = 1;
-    g.zb = (half + g.tx - 1) / g.tx;
-    g.yb = (ny + g.ty - 1) / g.ty;
-    (void)nx;
-    return g;
-}
-int sc_slots_per_rep(int nx, int ny, int nz) {
-    ScGeom g = sc_geom(nx, ny, nz);
-    return g.zb * g.yb * nx;
-}
-
+// ================================================================= helpers
 template <typename T>
 __device__ __forceinline__ void block_sum4(T v0, T v1, T v2, T v3, T* out /* smem 4 */) {
     __shared__ T red[4][32];
@@ -49,120 +25,6 @@ __device__ __forceinline__ void block_sum4(T v0, T v1, T v2, T v3, T* out /* sme
         a = warp_sum(a); b = warp_sum(b); c = warp_sum(c); d = warp_sum(d);
         if (lane == 0) { out[0] = a; out[1] = b; out[2] = c; out[3] = d; }
     }
-}
-
-template <int MOVE, int DMI, bool HAS_K>
-__global__ void __launch_bounds__(kScThreads) k_sc_colour(SweepLaunch a, int colour, int zb) {
-    const int bx = blockIdx.x;
-    const int k = (bx % zb) * blockDim.x + threadIdx.x;
-    const int y = (bx / zb) * blockDim.y + threadIdx.y;
-    const int x = blockIdx.y;
-    const int rl = blockIdx.z;
-    const int rep = a.rep_first + rl;
-    const int nx = a.nx, ny = a.ny, nz = a.nz;
-    float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
-    if (y < ny && k < (nz >> 1)) {
-        const int64_t N = a.natoms;
-        float* __restrict__ sx = a.spins + (int64_t)rl * 3 * N;
-        float* __restrict__ sy = sx + N;
-        float* __restrict__ sz = sy + N;
-        const int z = 2 * k + ((x + y + colour) & 1);
-        const int64_t row = (int64_t)x * ny + y;
-        const int64_t i = row * nz + z;
-        const int xp = x + 1 == nx ? 0 : x + 1, xm = x == 0 ? nx - 1 : x - 1;
-        const int yp = y + 1 == ny ? 0 : y + 1, ym = y == 0 ? ny - 1 : y - 1;
-        const int zp = z + 1 == nz ? 0 : z + 1, zm = z == 0 ? nz - 1 : z - 1;
-        const int64_t ixp = ((int64_t)xp * ny + y) * nz + z, ixm = ((int64_t)xm * ny + y) * nz + z;
-        const int64_t iyp = ((int64_t)x * ny + yp) * nz + z, iym = ((int64_t)x * ny + ym) * nz + z;
-        const int64_t izp = row * nz + zp, izm = row * nz + zm;
-        const f3 s = {sx[i], sy[i], sz[i]};
-        const f3 px = {sx[ixp], sy[ixp], sz[ixp]}, mx = {sx[ixm], sy[ixm], sz[ixm]};
-        const f3 py = {sx[iyp], sy[iyp], sz[iyp]}, my = {sx[iym], sy[iym], sz[iym]};
-        const f3 pz = {sx[izp], sy[izp], sz[izp]}, mz = {sx[izm], sy[izm], sz[izm]};
-        const HamDev& H = a.ham;
-        f3 h = {(px.x + mx.x) + (py.x + my.x) + (pz.x + mz.x),
-                (px.y + mx.y) + (py.y + my.y) + (pz.y + mz.y),
-                (px.z + mx.z) + (py.z + my.z) + (pz.z + mz.z)};
-        h.x *= H.J; h.y *= H.J; h.z *= H.J;
-        if (DMI == 1) {
-            // bulk: D_{+a} = -D a_hat, D_{-a} = +D a_hat  ->  D (S_{-a} - S_{+a}) x a_hat
-            const float D = H.D[1][0];
-            const f3 dx = {mx.x - px.x, mx.y - px.y, mx.z - px.z};
-            const f3 dy = {my.x - py.x, my.y - py.y, my.z - py.z};
-            const f3 dz = {mz.x - pz.x, mz.y - pz.y, mz.z - pz.z};
-            h.x = fmaf(D, dz.y - dy.z, h.x);
-            h.y = fmaf(D, dx.z - dz.x, h.y);
-            h.z = fmaf(D, dy.x - dx.y, h.z);
-        } else if (DMI == 2) {
-            // interfacial along z: D_{+x} = -D y, D_{-x} = +D y, D_{+y} = +D x, D_{-y} = -D x
-            const float D = H.D[2][0];
-            const f3 ax = {mx.x - px.x, mx.y - px.y, mx.z - px.z};  // (S_{-x}-S_{+x}) x y_hat
-            const f3 ay = {py.x - my.x, py.y - my.y, py.z - my.z};  // (S_{+y}-S_{-y}) x x_hat
-            h.x = fmaf(D, -ax.z, h.x);
-            h.y = fmaf(D, ay.z, h.y);
-            h.z = fmaf(D, ax.x - ay.y, h.z);
-        } else if (DMI == 3) {
-            const f3 nb[6] = {px, mx, py, my, pz, mz};
-#pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                const f3 D = {H.D[q][0], H.D[q][1], H.D[q][2]};
-                const f3 c = cross(nb[q], D);
-                h.x += c.x; h.y += c.y; h.z += c.z;
-            }
-        }
-        h.z -= H.Bz;
-        const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
-        const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)i, sweep, (uint32_t)rep,
-                                                   (a.ensemble << 8) | kTagSweep),
-                                        philox_key(a.seed));
-        const f3 sp = propose<MOVE>(s, u01(r4.x), u01(r4.y), u01(r4.z), a.r);
-        float dE = (sp.x - s.x) * h.x + (sp.y - s.y) * h.y + (sp.z - s.z) * h.z;
-        if (HAS_K) {
-            const float e1 = sp.x * H.kx + sp.y * H.ky + sp.z * H.kz;
-            const float e0 = s.x * H.kx + s.y * H.ky + s.z * H.kz;
-            dE -= H.K * (e1 * e1 - e0 * e0);
-        }
-        const float beta = (float)a.beta_rep[rep];
-        if (!(dE == dE)) atomicOr(a.status, kStatNan);
-        const bool acc = (dE <= 0.f) || (u01(r4.w) < __expf(-beta * dE));
-        if (acc) {
-            sx[i] = sp.x; sy[i] = sp.y; sz[i] = sp.z;
-            de = dE; dmx = sp.x - s.x; dmy = sp.y - s.y; dmz = sp.z - s.z;
-        }
-    }
-    if (a.partials) {
-        __shared__ double tot[4];
-        block_sum4<double>(de, dmx, dmy, dmz, tot);
-        if (threadIdx.x == 0 && threadIdx.y == 0) {
-            const int slot = bx + gridDim.x * x;
-            double* p = a.partials + ((int64_t)rep * a.slots_per_rep + slot) * 4;
-            p[0] += tot[0]; p[1] += tot[1]; p[2] += tot[2]; p[3] += tot[3];
-        }
-    }
-}
-
-template <int MOVE, int DMI>
-static void sc_dispatch_k(const SweepLaunch& a, int colour, dim3 g, dim3 b, int zb, bool hk,
-                          cudaStream_t s) {
-    if (hk) k_sc_colour<MOVE, DMI, true><<<g, b, 0, s>>>(a, colour, zb);
-    else k_sc_colour<MOVE, DMI, false><<<g, b, 0, s>>>(a, colour, zb);
-}
-
-int launch_sc_colour(const SweepLaunch& a, int colour, cudaStream_t s) {
-    ScGeom gg = sc_geom(a.nx, a.ny, a.nz);
-    dim3 b(gg.tx, gg.ty), g(gg.zb * gg.yb, a.nx, a.n_rep);
-    const bool hk = a.ham.K != 0.f;
-#define ISG_SC(M, D) sc_dispatch_k<M, D>(a, colour, g, b, gg.zb, hk, s)
-    if (a.move == 0) {
-        switch (a.dmi_kind) { case 0: ISG_SC(0, 0); break; case 1: ISG_SC(0, 1); break;
-                              case 2: ISG_SC(0, 2); break; default: ISG_SC(0, 3); }
-    } else {
-        switch (a.dmi_kind) { case 0: ISG_SC(1, 0); break; case 1: ISG_SC(1, 1); break;
-                              case 2: ISG_SC(1, 2); break; default: ISG_SC(1, 3); }
-    }
-#undef ISG_SC
-    ISG_CUDA(cudaGetLastError());
-    return ISING_OK;
 }
 
 // ================================================================= general crystal sweep
@@ -190,12 +52,12 @@ __device__ __forceinline__ void decode_atom(int64_t at, int nsub, int ny, int nz
 // local field of atom (ix,iy,iz,sub) from its stencil in shared memory
 __device__ __forceinline__ f3 stencil_field(const float* sx, const float* sy, const float* sz,
                                             const Slot* sl, int cnt, int ix, int iy, int iz,
-                                            int nx, int ny, int nz, int nsub) {
+                                            const Layout& L) {
     f3 h = {0.f, 0.f, 0.f};
     for (int q = 0; q < cnt; ++q) {
         const Slot e = sl[q];
-        const int jx = wrap_any(ix + e.dx, nx), jy = wrap_any(iy + e.dy, ny), jz = wrap_any(iz + e.dz, nz);
-        const int64_t j = (((int64_t)jx * ny + jy) * nz + jz) * nsub + e.sub;
+        const int jx = wrap_any(ix + e.dx, L.nx), jy = wrap_any(iy + e.dy, L.ny), jz = wrap_any(iz + e.dz, L.nz);
+        const int64_t j = sidx(L, jx, jy, jz, e.sub);
         const f3 sj = {sx[j], sy[j], sz[j]};
         const f3 c = cross(sj, mk(e.Dx, e.Dy, e.Dz));
         h.x += fmaf(e.w, sj.x, c.x);
@@ -230,9 +92,10 @@ __global__ void __launch_bounds__(kGenThreads) k_general_colour(GeneralLaunch a)
         const int64_t at = a.sites[t];
         int ix, iy, iz, sub;
         decode_atom(at, a.nsub, a.ny, a.nz, &ix, &iy, &iz, &sub);
-        f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.nx, a.ny, a.nz, a.nsub);
+        f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.layout);
         h.z -= H.Bz;
-        const f3 s = {sx[at], sy[at], sz[at]};
+        const int64_t si = sidx(a.layout, ix, iy, iz, sub);
+        const f3 s = {sx[si], sy[si], sz[si]};
         const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)at, sweep, (uint32_t)rep,
                                                    (a.ensemble << 8) | kTagSweep),
                                         philox_key(a.seed));
@@ -245,7 +108,7 @@ __global__ void __launch_bounds__(kGenThreads) k_general_colour(GeneralLaunch a)
         }
         if (!(dE == dE)) atomicOr(a.status, kStatNan);
         if ((dE <= 0.f) || (u01(r4.w) < __expf(-beta * dE))) {
-            sx[at] = sp.x; sy[at] = sp.y; sz[at] = sp.z;
+            sx[si] = sp.x; sy[si] = sp.y; sz[si] = sp.z;
             de += dE; dmx += sp.x - s.x; dmy += sp.y - s.y; dmz += sp.z - s.z;
         }
     }
@@ -299,8 +162,9 @@ __global__ void __launch_bounds__(kRedThreads) k_energy_mag(ReduceLaunch a) {
     for (int64_t at = i0 + threadIdx.x; at < i1; at += blockDim.x) {
         int ix, iy, iz, sub;
         decode_atom(at, a.nsub, a.ny, a.nz, &ix, &iy, &iz, &sub);
-        const f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.nx, a.ny, a.nz, a.nsub);
-        const f3 s = {sx[at], sy[at], sz[at]};
+        const f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.layout);
+        const int64_t si = sidx(a.layout, ix, iy, iz, sub);
+        const f3 s = {sx[si], sy[si], sz[si]};
         float ei = 0.5f * dot(s, h) - H.Bz * s.z;
         if (H.K != 0.f) {
             const float ea = s.x * H.kx + s.y * H.ky + s.z * H.kz;
@@ -387,7 +251,6 @@ __global__ void __launch_bounds__(256) k_winding(WindingLaunch a) {
     const float* sx = a.spins + (int64_t)rep * 3 * N;
     const float* sy = sx + N;
     const float* sz = sy + N;
-    const int nsub = a.nsub;
     const int* P = a.plaq;  // 4 x (dx, dy, dz, sub): s1, s2, s4, s3
     T w = T(0);
     const int np = a.nx * a.ny;
@@ -398,7 +261,7 @@ __global__ void __launch_bounds__(256) k_winding(WindingLaunch a) {
         for (int q = 0; q < 4; ++q) {
             const int jx = wrap_any(i + P[4 * q], a.nx), jy = wrap_any(j + P[4 * q + 1], a.ny);
             const int jz = wrap_any(zc + P[4 * q + 2], a.nz);
-            at[q] = (((int64_t)jx * a.ny + jy) * a.nz + jz) * nsub + P[4 * q + 3];
+            at[q] = sidx(a.layout, jx, jy, jz, P[4 * q + 3]);
         }
         T s1[3], s2[3], s4[3], s3[3];
         load_unit<T>(sx, sy, sz, at[0], s1);
@@ -442,9 +305,10 @@ __global__ void k_local_energy(LocalLaunch a) {
     const int64_t at = a.atoms[t];
     int ix, iy, iz, sub;
     decode_atom(at, a.nsub, a.ny, a.nz, &ix, &iy, &iz, &sub);
-    f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.nx, a.ny, a.nz, a.nsub);
+    f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.layout);
     h.z -= a.ham.Bz;
-    const f3 s = {sx[at], sy[at], sz[at]};
+    const int64_t si = sidx(a.layout, ix, iy, iz, sub);
+    const f3 s = {sx[si], sy[si], sz[si]};
     const f3 sp = {(float)a.sprop[3 * t], (float)a.sprop[3 * t + 1], (float)a.sprop[3 * t + 2]};
     float e0 = dot(s, h), e1 = dot(sp, h);
     if (a.ham.K != 0.f) {
@@ -466,23 +330,30 @@ int launch_local_energy(const LocalLaunch& a, cudaStream_t s) {
 }
 
 // ================================================================= initial spins
-__global__ void k_init_uniform(float* spins, int64_t N, uint64_t seed, uint32_t ensemble) {
+__global__ void k_init_uniform(float* spins, int64_t N, Layout L, uint64_t seed, uint32_t ensemble) {
     const int rep = blockIdx.y;
     float* sx = spins + (int64_t)rep * 3 * N;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
         const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)i, 0u, (uint32_t)rep, (ensemble << 8) | kTagInit),
                                         philox_key(seed));
-        const f3 v = propose<0>(mk(0.f, 0.f, 1.f), u01(r4.x), u01(r4.y), 0.5f, 0.f);
-        sx[i] = v.x; sx[N + i] = v.y; sx[2 * N + i] = v.z;
+        // uniform unit vector: cos theta = 2u-1, azimuth 2 pi (u - 1/2), normalised
+        const float cz = fmaf(2.0f, u01(r4.x), -1.0f);
+        const float st = sqrtf(fmaf(-cz, cz, 1.0f));
+        float sn, cs;
+        sincospif(2.0f * (u01(r4.y) - 0.5f), &sn, &cs);
+        f3 v = {st * cs, st * sn, cz};
+        const float rn = rsqrtf(dot(v, v));
+        const int64_t j = sidx_atom(L, i);
+        sx[j] = v.x * rn; sx[N + j] = v.y * rn; sx[2 * N + j] = v.z * rn;
     }
 }
 
-int launch_init_uniform(float* spins, int64_t natoms, int n_rep, uint64_t seed, uint32_t ensemble,
-                        cudaStream_t s) {
+int launch_init_uniform(float* spins, int64_t natoms, const Layout& L, int n_rep, uint64_t seed,
+                        uint32_t ensemble, cudaStream_t s) {
     int blocks = (int)((natoms + 255) / 256);
     if (blocks > 4096) blocks = 4096;
     dim3 g(blocks, n_rep);
-    k_init_uniform<<<g, 256, 0, s>>>(spins, natoms, seed, ensemble);
+    k_init_uniform<<<g, 256, 0, s>>>(spins, natoms, L, seed, ensemble);
     ISG_CUDA(cudaGetLastError());
     return ISING_OK;
 }
@@ -587,32 +458,36 @@ int launch_record(const RecordLaunch& a, cudaStream_t s) {
 // ================================================================= host-layout conversion
 // atomSpins(numAtoms,3) column-major FP64 is the planes layout already; only the width
 // changes.  Zero or non-finite vectors raise the NaN status (src/energyMin.f90:330-331).
-__global__ void k_spins_from_f64(const double* in, float* out, int64_t N, int* status) {
+__global__ void k_spins_from_f64(const double* in, float* out, int64_t N, Layout L, int* status) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
         const double x = in[i], y = in[N + i], z = in[2 * N + i];
         const double n2 = x * x + y * y + z * z;
         if (!(n2 > 0.0) || !isfinite(n2)) atomicOr(status, kStatNan);
-        out[i] = (float)x; out[N + i] = (float)y; out[2 * N + i] = (float)z;
+        const int64_t j = sidx_atom(L, i);
+        out[j] = (float)x; out[N + j] = (float)y; out[2 * N + j] = (float)z;
     }
 }
 
-__global__ void k_spins_to_f64(const float* in, double* out, int64_t N) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 3 * N; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = (double)in[i];
+__global__ void k_spins_to_f64(const float* in, double* out, int64_t N, Layout L) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = sidx_atom(L, i);
+        out[i] = (double)in[j]; out[N + i] = (double)in[N + j]; out[2 * N + i] = (double)in[2 * N + j];
+    }
 }
 
-int launch_spins_from_f64(const double* in, float* out, int64_t natoms, int* status, cudaStream_t s) {
+int launch_spins_from_f64(const double* in, float* out, int64_t natoms, const Layout& L, int* status,
+                          cudaStream_t s) {
     int blocks = (int)((natoms + 255) / 256);
     if (blocks > 8192) blocks = 8192;
-    k_spins_from_f64<<<blocks, 256, 0, s>>>(in, out, natoms, status);
+    k_spins_from_f64<<<blocks, 256, 0, s>>>(in, out, natoms, L, status);
     ISG_CUDA(cudaGetLastError());
     return ISING_OK;
 }
 
-int launch_spins_to_f64(const float* in, double* out, int64_t natoms, cudaStream_t s) {
-    int blocks = (int)((3 * natoms + 255) / 256);
+int launch_spins_to_f64(const float* in, double* out, int64_t natoms, const Layout& L, cudaStream_t s) {
+    int blocks = (int)((natoms + 255) / 256);
     if (blocks > 8192) blocks = 8192;
-    k_spins_to_f64<<<blocks, 256, 0, s>>>(in, out, natoms);
+    k_spins_to_f64<<<blocks, 256, 0, s>>>(in, out, natoms, L);
     ISG_CUDA(cudaGetLastError());
     return ISING_OK;
 }

@@ -226,7 +226,7 @@ int build_lattice(const float* frac, int nsub, int nx, int ny, int nz, double a,
             push(idx[q], shell);
         }
         if ((int)L.shell[0][i].size() > kMaxSlots || (int)L.shell[1][i].size() > kMaxSlots)
-            return fail(ISING_ERR_ARG, "neighbour shell larger than the 64-slot stencil limit");
+            return fail(ISING_ERR_ARG, "neighbour shell larger than the 128-slot stencil limit");
 
         // ---- legacy NeighborList: 27 cells (getNeighboringCells :85-131), dedup by atom,
         // |d - d_min| < a/100 in single precision (:299-357)
@@ -263,7 +263,7 @@ int build_lattice(const float* frac, int nsub, int nx, int ny, int nz, double a,
             }
         }
         if ((int)L.legacy[i].size() > kMaxSlots)
-            return fail(ISING_ERR_ARG, "legacy neighbour list larger than 64 slots");
+            return fail(ISING_ERR_ARG, "legacy neighbour list larger than 128 slots");
 
         // ---- derivative list (:956-1031): other cells only, the two other Bravais
         // coefficients within 1e-4, nearest below / above along d, ties to the later atom

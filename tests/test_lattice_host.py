@@ -60,7 +60,7 @@ def test_colouring_is_independent(oracle, ib):
                 for s in shells:
                     nb = pm.neighbours(atom, s)
                     assert np.all(col[nb] != col[atom])
-            if kind == "SC" and dims[0] % 2 == 0 and Jp == 0.0:
+            if kind == "SC" and dims[0] % 4 == 0 and Jp == 0.0:
                 assert n == 2 and pm.checkerboard
             deg = sum(len(pm.neighbours(0, s)) for s in shells)
             assert n <= deg + 1  # greedy bound
