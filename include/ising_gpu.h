@@ -155,6 +155,15 @@ int ising_local_energy_batch(const ising_mesh* mesh, int replica, int n, const i
 /* Replaces TotalHeisenbergEnergy(chainMesh, J, J', Dz, Dz', B, lockArray, totalEnergy,
  * demag) (src/energyMin.f90:499-528): FP32 terms, FP64 block sums. */
 int ising_total_energy(const ising_mesh* mesh, int replica, const ising_params* p, double* e);
+/* Same result as ising_total_energy, but allocates no device memory: the per-block partial
+ * sums live in a fixed array inside the library (128 KiB per device, held until exit), so
+ * callers that cannot call cudaMalloc -- loops that must not stall other streams, work
+ * issued while another thread captures a graph, applications that reserve device memory up
+ * front -- can still evaluate energies.  Replicas are limited to 16,777,216 atoms (larger
+ * ones return ISING_ERR_ARG).  All calls on a device share that array: calls that overlap
+ * on the GPU race, so issue them one after another.  The first call on a device looks up
+ * the array's address; make it before any stream capture.  No counterpart in the reference. */
+int ising_total_energy_noalloc(const ising_mesh* mesh, int replica, const ising_params* p, double* e);
 /* Energy and magnetisation vector of every replica in one pass: e[R], m[R*3]. */
 int ising_observables(const ising_mesh* mesh, const ising_params* p, double* e, double* m);
 

@@ -74,6 +74,7 @@ _SIGS = {
     "ising_local_energy": (_i, [_vp, _i, _i, _P(Params), _P(_d), _P(_d), _P(_d)]),
     "ising_local_energy_batch": (_i, [_vp, _i, _i, _P(_i64), _P(_d), _P(Params), _P(_d), _P(_d)]),
     "ising_total_energy": (_i, [_vp, _i, _P(Params), _P(_d)]),
+    "ising_total_energy_noalloc": (_i, [_vp, _i, _P(Params), _P(_d)]),
     "ising_observables": (_i, [_vp, _P(Params), _P(_d), _P(_d)]),
     "ising_metropolis_mcs": (_i, [_vp, _i, _d, _i, _P(Params), _d, _u64]),
     "ising_winding_number": (_i, [_vp, _i, _i, _P(_d)]),

@@ -1079,3 +1079,39 @@ extern "C" int ising_pt_series(const ising_pt* pt, double* out, int* n_rec) {
                             cudaMemcpyDeviceToHost));
     return ISING_OK;
 }
+
+// ======================================================================= helpers for noalloc.cu
+namespace isg {
+// Shell or legacy stencil of p written into caller-provided host memory (no allocation).
+int fill_query_stencil_host(const ising_mesh* m, const ising_params& p, bool legacy, Slot* slots, int* cnt) {
+    const Lattice& L = m->lat;
+    for (int s = 0; s < kMaxSub; ++s) cnt[s] = 0;
+    for (int s = 0; s < L.nsub; ++s) {
+        int c = 0;
+        auto add = [&](const NbrSlot& q, float w, bool dmi) -> int {
+            if (c >= kMaxSlots) return fail(ISING_ERR_ARG, "stencil exceeds 128 slots");
+            Slot e{};
+            e.dx = (int8_t)q.dx; e.dy = (int8_t)q.dy; e.dz = (int8_t)q.dz; e.sub = (uint8_t)q.sub;
+            e.w = w;
+            if (dmi && p.Dz != 0.0) {
+                double D[3];
+                bond_dmi(L, p, q.r, D);
+                e.Dx = (float)D[0]; e.Dy = (float)D[1]; e.Dz = (float)D[2];
+            }
+            slots[(size_t)s * kMaxSlots + c++] = e;
+            return ISING_OK;
+        };
+        if (legacy) {
+            for (const auto& q : L.legacy[s]) ISG_TRY(add(q, (float)p.J, true));
+        } else {
+            for (const auto& q : L.shell[0][s]) ISG_TRY(add(q, (float)p.J, true));
+            if (uses_shell2(L, p))
+                for (const auto& q : L.shell[1][s]) ISG_TRY(add(q, (float)p.J_prime, false));
+        }
+        cnt[s] = c;
+    }
+    return ISING_OK;
+}
+HamDev ham_of(const ising_params& p) { return make_ham(p); }
+int check_params(const ising_params* p) { return validate_params(p); }
+}  // namespace isg

@@ -244,4 +244,9 @@ struct RecordLaunch {
 };
 int launch_record(const RecordLaunch& a, cudaStream_t s);
 
+// host helpers shared with the allocation-free entry point (capi.cu)
+int fill_query_stencil_host(const ising_mesh* m, const ising_params& p, bool legacy, Slot* slots, int* cnt);
+HamDev ham_of(const ising_params& p);
+int check_params(const ising_params* p);
+
 }  // namespace isg
