@@ -216,6 +216,7 @@ typedef struct {
  * temperatures betas[t]. */
 int ising_pt_create(ising_mesh* mesh, int n_temps, const double* betas, const ising_params* p,
                     const ising_pt_options* opt, ising_pt** out);
+/* destroy a PT object before its mesh */
 int ising_pt_destroy(ising_pt* pt);
 /* rounds x [sweeps_per_swap sweeps of every replica, then one exchange], replacing the
  * iteration loop of src/PT.f90:219-273; replayed from a CUDA graph. */
@@ -240,6 +241,75 @@ int ising_pt_swap_stats(const ising_pt* pt, uint64_t* attempts, uint64_t* accept
  * sweep): E, |M| = |sum S|/N, Q_mid (slice nz/2) and Q_mean (mean over slices).
  * out is n_temps x record_capacity x 4; *n_recorded gives the filled length. */
 int ising_pt_series(const ising_pt* pt, double* out, int* n_recorded);
+
+/* ---------------------------------------------------------------- batched ensembles
+ * Many independent PT ensembles (one per parameter slot of src/PT.f90:147-176, which the
+ * reference runs one after another per MPI rank) of uneven lattice sizes and Hamiltonians,
+ * all replicas advanced by ONE persistent kernel per launch: sweeps, running-sum folds and
+ * exchanges of every ensemble, replayed from a CUDA graph.  Each ensemble is a
+ * colour-separated simple-cubic mesh (even nx, ny; nz % 4 == 0; shell 1 only).  The per-site
+ * updates, Philox keys and exchange decisions are those of ising_pt_* on the same mesh,
+ * seed and ensemble id.  The engine issues all work on its own stream (or the one
+ * ising_ensembles_set_stream gives); the meshes must not be used elsewhere meanwhile and
+ * must outlive the engine (destroy the engine first). */
+typedef struct ising_ensembles ising_ensembles;
+
+typedef struct {
+    ising_mesh* mesh;
+    int n_temps;              /* replicas 0..n_temps-1 of mesh take part */
+    const double* betas;      /* n_temps inverse temperatures by slot */
+    ising_params params;
+    uint32_t ensemble;        /* Philox key component (< 2^24), distinct per ensemble */
+} ising_ensemble_desc;
+
+#define ISING_ENS_ORDER_PHASE 0   /* queue by colour pass: every ensemble's pass p, then p+1 */
+#define ISING_ENS_ORDER_GROUPS 1  /* replica groups of ~group_bytes run a whole round in turn
+                                     (the group's spins stay resident in L2) */
+
+typedef struct {
+    uint64_t seed;
+    int move;                 /* ISING_MOVE_UNIFORM or ISING_MOVE_BALL, all ensembles */
+    double r;
+    int scheme;               /* ISING_PT_EVEN_ODD or ISING_PT_RANDOM_PAIRS */
+    int resync_every;         /* rounds between FP64 energy resyncs (0 = never) */
+    int wait_timeout_ms;      /* bound of every in-kernel wait (0 = 2000) */
+} ising_ensembles_options;
+
+/* One schedule: block size, target site pairs per task, queue order and group size. */
+typedef struct {
+    int block_threads;        /* 64..256, whole warps */
+    int chunk_pairs;          /* site pairs of one colour per task (whole x-planes) */
+    int order;                /* ISING_ENS_ORDER_* */
+    int64_t group_bytes;      /* ISING_ENS_ORDER_GROUPS: spin bytes per replica group */
+    double ms_per_round;      /* autotuner output: measured time per round */
+} ising_ensembles_schedule_t;
+
+/* No reference counterpart (the reference has no batched form). */
+int ising_ensembles_create(int n_ensembles, const ising_ensemble_desc* desc,
+                           const ising_ensembles_options* opt, ising_ensembles** out);
+int ising_ensembles_destroy(ising_ensembles* s);
+int ising_ensembles_set_stream(ising_ensembles* s, void* cuda_stream);
+/* rounds x [sweeps_per_swap sweeps of every replica of every ensemble, then each
+ * ensemble's exchange]: the iteration loop of src/PT.f90:219-273 for all slots at once. */
+int ising_ensembles_run(ising_ensembles* s, int sweeps_per_swap, int rounds);
+int ising_ensembles_set_schedule(ising_ensembles* s, const ising_ensembles_schedule_t* sched);
+/* current schedule, persistent grid size and tasks per colour pass (all replicas) */
+int ising_ensembles_get_schedule(const ising_ensembles* s, ising_ensembles_schedule_t* sched,
+                                 int* grid_blocks, int64_t* tasks_per_pass);
+/* Times candidate schedules (each trial runs warm-up and rounds_per_trial ordinary rounds
+ * of the chain) and keeps the fastest; trials may be NULL. */
+int ising_ensembles_autotune(ising_ensembles* s, int sweeps_per_swap, int rounds_per_trial,
+                             ising_ensembles_schedule_t* trials, int max_trials, int* n_trials);
+int ising_ensembles_permutation(const ising_ensembles* s, int ensemble_index, int* temp_to_replica);
+int ising_ensembles_energies(const ising_ensembles* s, int ensemble_index, double* e_per_replica,
+                             double* m_per_replica);
+int ising_ensembles_swap_stats(const ising_ensembles* s, int ensemble_index, uint64_t* attempts,
+                               uint64_t* accepts);
+int ising_ensembles_resync(ising_ensembles* s);
+/* Test hook for the bounded waits: in the next run, rounds >= 1 of ensemble_index wait for
+ * a flag that nothing sets, so that run returns ISING_ERR_TIMEOUT after wait_timeout_ms;
+ * the engine then resynchronises its accumulators and stays usable. */
+int ising_ensembles_inject_stall(ising_ensembles* s, int ensemble_index);
 
 /* ---------------------------------------------------------------- CSV outputs */
 /* write_spins_to_file(chainMesh, filename, append, include_header, frame_index)

@@ -51,6 +51,23 @@ class PTOptions(C.Structure):
                 ("record_capacity", C.c_int), ("l2_group", C.c_int), ("sweep_kernel", C.c_int)]
 
 
+class EnsembleDesc(C.Structure):
+    _fields_ = [("mesh", C.c_void_p), ("n_temps", C.c_int), ("betas", C.POINTER(C.c_double)),
+                ("params", Params), ("ensemble", C.c_uint32)]
+
+
+class EnsemblesOptions(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("move", C.c_int), ("r", C.c_double), ("scheme", C.c_int),
+                ("resync_every", C.c_int), ("wait_timeout_ms", C.c_int)]
+
+
+class EnsSchedule(C.Structure):
+    _fields_ = [("block_threads", C.c_int), ("chunk_pairs", C.c_int), ("order", C.c_int),
+                ("group_bytes", C.c_int64), ("ms_per_round", C.c_double)]
+
+
+ENS_ORDER_PHASE, ENS_ORDER_GROUPS = 0, 1
+
 _P = C.POINTER
 _d, _i, _i64, _u32, _u64, _vp = C.c_double, C.c_int, C.c_int64, C.c_uint32, C.c_uint64, C.c_void_p
 
@@ -91,6 +108,18 @@ _SIGS = {
     "ising_pt_resync": (_i, [_vp]),
     "ising_pt_swap_stats": (_i, [_vp, _P(_u64), _P(_u64)]),
     "ising_pt_series": (_i, [_vp, _P(_d), _P(_i)]),
+    "ising_ensembles_create": (_i, [_i, _P(EnsembleDesc), _P(EnsemblesOptions), _P(_vp)]),
+    "ising_ensembles_destroy": (_i, [_vp]),
+    "ising_ensembles_set_stream": (_i, [_vp, _vp]),
+    "ising_ensembles_run": (_i, [_vp, _i, _i]),
+    "ising_ensembles_set_schedule": (_i, [_vp, _P(EnsSchedule)]),
+    "ising_ensembles_get_schedule": (_i, [_vp, _P(EnsSchedule), _P(_i), _P(_i64)]),
+    "ising_ensembles_autotune": (_i, [_vp, _i, _i, _P(EnsSchedule), _i, _P(_i)]),
+    "ising_ensembles_permutation": (_i, [_vp, _i, _P(_i)]),
+    "ising_ensembles_energies": (_i, [_vp, _i, _P(_d), _P(_d)]),
+    "ising_ensembles_swap_stats": (_i, [_vp, _i, _P(_u64), _P(_u64)]),
+    "ising_ensembles_resync": (_i, [_vp]),
+    "ising_ensembles_inject_stall": (_i, [_vp, _i]),
     "ising_write_spins_csv": (_i, [_vp, _i, C.c_char_p, _i, _i, _i]),
     "ising_write_pt_data_csv": (_i, [C.c_char_p, _d, _d, _d, _d, _d, _i, _d, _P(_d)]),
     "ising_pt_file_tag": (_i, [C.c_char_p, C.c_size_t, _d, _d, _d, _d]),

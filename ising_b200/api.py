@@ -8,13 +8,15 @@ computes physics on the CPU.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from typing import Optional, Sequence
 
 import numpy as np
 
 from . import _lib
 from ._lib import (CELL_BCC, CELL_HYPER_KAGOME, CELL_SC, DMI_BULK, DMI_INTERFACIAL, MOVE_BALL,
-                   MOVE_UNIFORM, PT_EVEN_ODD, PT_RANDOM_PAIRS, IsingError, MeshInfo, Params, PTOptions)
+                   MOVE_UNIFORM, PT_EVEN_ODD, PT_RANDOM_PAIRS, ENS_ORDER_GROUPS, ENS_ORDER_PHASE, EnsembleDesc,
+                   EnsSchedule, EnsemblesOptions, IsingError, MeshInfo, Params, PTOptions)
 
 _P = C.POINTER
 
@@ -111,7 +113,15 @@ class ChainMesh:
     def handle(self):
         return self._h
 
+    def _depend(self, obj):
+        """Register a PT object or engine that must be destroyed before this mesh."""
+        if not hasattr(self, "_dependents"):
+            self._dependents = weakref.WeakSet()
+        self._dependents.add(obj)
+
     def close(self):
+        for d in list(getattr(self, "_dependents", ())):
+            d.close()
         if getattr(self, "_h", None) and self._h.value:
             _lib.load().ising_mesh_destroy(self._h)
             self._h = C.c_void_p()
@@ -332,6 +342,7 @@ class ParallelTempering:
         h = C.c_void_p()
         _lib.call("ising_pt_create", mesh.handle, self.n, _dp(self.betas), C.byref(p), C.byref(o), C.byref(h))
         self._h = h
+        mesh._depend(self)
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
@@ -384,3 +395,93 @@ class ParallelTempering:
         n = C.c_int()
         _lib.call("ising_pt_series", self._h, _dp(out), C.byref(n))
         return out[:, : n.value, :]
+
+
+class Ensembles:
+    """Many PT ensembles (parameter slots of src/PT.f90:147-176) advanced together by one
+    persistent kernel per launch.  `members` is a sequence of (mesh, betas, params,
+    ensemble_id); each mesh must be a colour-separated simple-cubic mesh of its own."""
+
+    def __init__(self, members, seed: int = 0x15196, move: int = MOVE_BALL, r: float = 0.2,
+                 scheme: int = PT_EVEN_ODD, resync_every: int = 0, wait_timeout_ms: int = 0):
+        self.members = list(members)
+        self._betas = [np.ascontiguousarray(b, dtype=np.float64) for _, b, _, _ in self.members]
+        descs = (EnsembleDesc * len(self.members))()
+        for i, (mesh, _, p, ens) in enumerate(self.members):
+            descs[i].mesh = mesh.handle
+            descs[i].n_temps = len(self._betas[i])
+            descs[i].betas = _dp(self._betas[i])
+            descs[i].params = p
+            descs[i].ensemble = ens
+        o = EnsemblesOptions()
+        o.seed, o.move, o.r, o.scheme, o.resync_every, o.wait_timeout_ms = seed, move, r, scheme, resync_every, wait_timeout_ms
+        self.opt = o
+        h = C.c_void_p()
+        _lib.call("ising_ensembles_create", len(self.members), descs, C.byref(o), C.byref(h))
+        self._h = h
+        for mesh, *_ in self.members:
+            mesh._depend(self)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.load().ising_ensembles_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        _lib.call("ising_ensembles_set_stream", self._h, C.c_void_p(stream_ptr or 0))
+
+    def run(self, sweeps_per_swap: int, rounds: int):
+        _lib.call("ising_ensembles_run", self._h, sweeps_per_swap, rounds)
+
+    def set_schedule(self, block_threads: int = 256, chunk_pairs: int = 4096, order: int = ENS_ORDER_PHASE,
+                     group_bytes: int = 48_000_000):
+        c = EnsSchedule(block_threads, chunk_pairs, order, group_bytes, 0.0)
+        _lib.call("ising_ensembles_set_schedule", self._h, C.byref(c))
+
+    def schedule(self) -> dict:
+        c, g, t = EnsSchedule(), C.c_int(), C.c_int64()
+        _lib.call("ising_ensembles_get_schedule", self._h, C.byref(c), C.byref(g), C.byref(t))
+        return {"block_threads": c.block_threads, "chunk_pairs": c.chunk_pairs,
+                "order": "groups" if c.order == ENS_ORDER_GROUPS else "phase", "group_bytes": c.group_bytes,
+                "ms_per_round": c.ms_per_round, "grid_blocks": g.value, "tasks_per_pass": t.value}
+
+    def autotune(self, sweeps_per_swap: int, rounds_per_trial: int = 1):
+        """Times the candidate schedules and keeps the fastest; returns the trials."""
+        trials = (EnsSchedule * 64)()
+        n = C.c_int()
+        _lib.call("ising_ensembles_autotune", self._h, sweeps_per_swap, rounds_per_trial, trials, 64, C.byref(n))
+        return [{"block_threads": t.block_threads, "chunk_pairs": t.chunk_pairs,
+                 "order": "groups" if t.order == ENS_ORDER_GROUPS else "phase", "group_bytes": t.group_bytes,
+                 "ms_per_round": t.ms_per_round} for t in trials[: n.value]]
+
+    def permutation(self, e: int) -> np.ndarray:
+        out = np.empty(len(self._betas[e]), dtype=np.int32)
+        _lib.call("ising_ensembles_permutation", self._h, e, out.ctypes.data_as(_P(C.c_int)))
+        return out
+
+    def energies(self, e: int):
+        n = len(self._betas[e])
+        en, m = np.empty(n), np.empty((n, 3))
+        _lib.call("ising_ensembles_energies", self._h, e, _dp(en), _dp(m))
+        return en, m
+
+    def swap_stats(self, e: int):
+        n = len(self._betas[e])
+        att = np.zeros(max(n - 1, 1), dtype=np.uint64)
+        acc = np.zeros(max(n - 1, 1), dtype=np.uint64)
+        _lib.call("ising_ensembles_swap_stats", self._h, e, att.ctypes.data_as(_P(C.c_uint64)),
+                  acc.ctypes.data_as(_P(C.c_uint64)))
+        return att[: n - 1], acc[: n - 1]
+
+    def resync(self):
+        _lib.call("ising_ensembles_resync", self._h)
+
+    def inject_stall(self, e: int):
+        """Test hook: the next run's rounds >= 1 of ensemble e wait for a flag nothing sets."""
+        _lib.call("ising_ensembles_inject_stall", self._h, e)

@@ -42,12 +42,38 @@ def needs_build() -> bool:
     return any(os.path.getmtime(f) > t for f in sources() + headers())
 
 
+BUILD_DIR = os.path.join(HERE, "_build")
+
+
+def _compile(src: str, obj: str, extra) -> None:
+    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-c",
+           "-ccbin", shutil.which("g++") or "g++",
+           "-I", os.path.join(HERE, "..", "include"), *extra, "-o", obj + ".tmp", src]
+    subprocess.run(cmd, check=True)
+    os.replace(obj + ".tmp", obj)
+
+
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
+    """Compile every source to an object in _build/ (in parallel; a source is recompiled
+    when it or any header is newer than its object), then link libisinggpu.so."""
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
-           "-ccbin", shutil.which("g++") or "g++",
-           "-I", os.path.join(HERE, "..", "include"), *extra, "-o", LIB + ".tmp", *sources()]
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    newest_header = max((os.path.getmtime(h) for h in headers()), default=0.0)
+    jobs = []
+    objs = []
+    for src in sources():
+        obj = os.path.join(BUILD_DIR, os.path.basename(src) + ".o")
+        objs.append(obj)
+        if force or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src), newest_header):
+            jobs.append((src, obj))
+    if verbose:
+        print(f"compiling {len(jobs)} of {len(objs)} sources", file=sys.stderr)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_compile, src, obj, list(extra)) for src, obj in jobs]:
+            f.result()
+    cmd = [nvcc(), *ARCH, "-shared", "-ccbin", shutil.which("g++") or "g++", "-o", LIB + ".tmp", *objs]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "ensembles.h"
 
 // ======================================================================= errors
 namespace isg {
@@ -1081,6 +1082,564 @@ extern "C" int ising_pt_series(const ising_pt* pt, double* out, int* n_rec) {
 }
 
 // ======================================================================= helpers for noalloc.cu
+// ======================================================================= batched ensembles
+namespace {
+
+struct EnsHost {
+    ising_mesh* mesh = nullptr;
+    int n = 0;
+    ising_params p{};
+    uint32_t ensemble = 0;
+    HamDev ham{};
+    int dmi_kind = 0;
+    double* d_beta_t = nullptr;
+    double* d_beta_rep = nullptr;
+    int* d_t2r = nullptr;
+    int* d_r2t = nullptr;
+    Acc4* d_acc = nullptr;
+    unsigned long long* d_stats = nullptr;
+    uint32_t* d_round = nullptr;
+    double* d_energy_tmp = nullptr;
+    double* d_energy_out = nullptr;
+    uint32_t P = 1, nch = 1;        // x-planes per chunk, chunks per replica
+    size_t part_off = 0, done_off = 0;
+};
+
+// sync words, zeroed before every launch: head, abort, where, (pad), ready[kMaxEnsembles],
+// fin[kMaxEnsembles] (64-bit), then the done counters of every replica's chunks
+constexpr size_t kSyncReady = 4;
+constexpr size_t kSyncFin = kSyncReady + kMaxEnsembles;   // word offset, 8-byte aligned
+constexpr size_t kSyncDone = kSyncFin + 2 * kMaxEnsembles;
+
+}  // namespace
+
+struct ising_ensembles {
+    std::vector<EnsHost> ens;
+    ising_ensembles_options opt{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;   // the engine's own stream (never a mesh's)
+    int move = 1, dmi = 0;
+    bool has_k = false;
+    ising_ensembles_schedule_t sched{256, 4096, ISING_ENS_ORDER_PHASE, 48000000, 0.0};
+    int grid = 0;
+    std::vector<uint2> table;
+    int table_k = -1;
+    uint2* d_table = nullptr;
+    size_t table_cap = 0;
+    double* d_partials = nullptr;
+    size_t partials_cap = 0;
+    uint32_t* d_sync = nullptr;
+    size_t sync_cap = 0, sync_words = 0;
+    int* d_status = nullptr;
+    uint32_t* h_words = nullptr;    // pinned: status, where
+    cudaGraphExec_t graph = nullptr;
+    int graph_k = -1, graph_rounds = -1;
+    int64_t rounds_done = 0;
+    int stall_next = -1;
+};
+
+namespace {
+
+void ens_free(ising_ensembles* s) {
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    for (auto& h : s->ens) {
+        cudaFree(h.d_beta_t); cudaFree(h.d_beta_rep); cudaFree(h.d_t2r); cudaFree(h.d_r2t); cudaFree(h.d_acc);
+        cudaFree(h.d_stats); cudaFree(h.d_round); cudaFree(h.d_energy_tmp); cudaFree(h.d_energy_out);
+    }
+    cudaFree(s->d_table); cudaFree(s->d_partials); cudaFree(s->d_sync); cudaFree(s->d_status);
+    if (s->h_words) cudaFreeHost(s->h_words);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+}
+
+void ens_drop_graph(ising_ensembles* s) {
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    s->graph_k = s->graph_rounds = -1;
+}
+
+// Chunking, grid and buffers for schedule `c`.
+int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) {
+    if (c.block_threads < 64 || c.block_threads > kEnsMaxThreads || c.block_threads % 32)
+        return fail(ISING_ERR_ARG, "block_threads must be 64..256 in whole warps");
+    if (c.chunk_pairs < 1) return fail(ISING_ERR_ARG, "chunk_pairs must be >= 1");
+    if (c.order != ISING_ENS_ORDER_PHASE && c.order != ISING_ENS_ORDER_GROUPS)
+        return fail(ISING_ERR_ARG, "order must be ISING_ENS_ORDER_PHASE or ISING_ENS_ORDER_GROUPS");
+    if (c.order == ISING_ENS_ORDER_GROUPS && c.group_bytes < 1) return fail(ISING_ERR_ARG, "group_bytes must be >= 1");
+    size_t part = 0, done = 0;
+    for (auto& h : s->ens) {
+        const Lattice& L = h.mesh->lat;
+        const int lanes = L.nz / 4;   // W / 2
+        if (lanes > c.block_threads) return fail(ISING_ERR_ARG, "block_threads smaller than nz / 4 of an ensemble");
+        const double plane_pairs = (double)L.ny * lanes;
+        int P = (int)std::lround((double)c.chunk_pairs / plane_pairs);
+        P = std::max(1, std::min(P, L.nx));
+        h.P = (uint32_t)P;
+        h.nch = (uint32_t)((L.nx + P - 1) / P);
+        h.part_off = part;
+        h.done_off = done;
+        part += (size_t)h.n * h.nch * 4;
+        done += (size_t)h.n * h.nch;
+    }
+    int per_sm = 0;
+    ISG_TRY(ensembles_blocks_per_sm(s->move, s->dmi, s->has_k, c.block_threads, &per_sm));
+    if (per_sm < 1) return fail(ISING_ERR_CUDA, "persistent engine kernel cannot be resident");
+    int sms = 0;
+    ISG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    ISG_CUDA(cudaStreamSynchronize(s->stream));
+    if (part > s->partials_cap) {
+        cudaFree(s->d_partials);
+        s->d_partials = nullptr;
+        s->partials_cap = 0;
+        ISG_TRY(dev_alloc(&s->d_partials, part));
+        s->partials_cap = part;
+    }
+    // partial sums are zero between rounds; a new layout starts from zero as well
+    ISG_CUDA(cudaMemsetAsync(s->d_partials, 0, s->partials_cap * sizeof(double), s->stream));
+    const size_t words = kSyncDone + done;
+    if (words > s->sync_cap) {
+        cudaFree(s->d_sync);
+        s->d_sync = nullptr;
+        s->sync_cap = 0;
+        ISG_TRY(dev_alloc(&s->d_sync, words));
+        s->sync_cap = words;
+    }
+    s->sync_words = words;
+    s->grid = per_sm * sms;
+    s->sched = c;
+    s->sched.ms_per_round = 0.0;
+    s->table_k = -1;
+    ens_drop_graph(s);
+    return ISING_OK;
+}
+
+// Task table of one round: groups of replicas (all replicas in PHASE order), each running
+// its 2k colour passes in turn; within a pass, replica by replica, chunk by chunk.
+int ens_build_table(ising_ensembles* s, int k) {
+    if (s->table_k == k) return ISING_OK;
+    struct Unit { int e, r; double bytes; };
+    std::vector<Unit> units;
+    for (int e = 0; e < (int)s->ens.size(); ++e)
+        for (int r = 0; r < s->ens[e].n; ++r) units.push_back({e, r, 12.0 * (double)s->ens[e].mesh->lat.natoms});
+    std::vector<std::pair<size_t, size_t>> groups;   // [begin, end) into units
+    if (s->sched.order == ISING_ENS_ORDER_PHASE) {
+        groups.push_back({0, units.size()});
+    } else {
+        size_t b = 0;
+        double acc = 0.0;
+        for (size_t i = 0; i < units.size(); ++i) {
+            if (i > b && acc + units[i].bytes > (double)s->sched.group_bytes) {
+                groups.push_back({b, i});
+                b = i;
+                acc = 0.0;
+            }
+            acc += units[i].bytes;
+        }
+        groups.push_back({b, units.size()});
+    }
+    s->table.clear();
+    for (const auto& g : groups)
+        for (int ph = 0; ph < 2 * k; ++ph)
+            for (size_t u = g.first; u < g.second; ++u) {
+                const EnsHost& h = s->ens[units[u].e];
+                for (uint32_t ch = 0; ch < h.nch; ++ch)
+                    s->table.push_back(make_uint2(((uint32_t)units[u].e << 24) | (uint32_t)units[u].r,
+                                                  ((uint32_t)ph << 16) | ch));
+            }
+    if (s->table.size() >= (1u << 30)) return fail(ISING_ERR_ARG, "task table too large");
+    ISG_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->table.size() > s->table_cap) {
+        cudaFree(s->d_table);
+        s->d_table = nullptr;
+        s->table_cap = 0;
+        ISG_TRY(dev_alloc(&s->d_table, s->table.size()));
+        s->table_cap = s->table.size();
+    }
+    ISG_CUDA(cudaMemcpy(s->d_table, s->table.data(), s->table.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    s->table_k = k;
+    ens_drop_graph(s);
+    return ISING_OK;
+}
+
+void ens_params(const ising_ensembles* s, int k, int rounds, int stall, EnsParams* P) {
+    std::memset(P, 0, sizeof(*P));
+    for (size_t i = 0; i < s->ens.size(); ++i) {
+        const EnsHost& h = s->ens[i];
+        const Lattice& L = h.mesh->lat;
+        EnsDev& d = P->e[i];
+        d.g.ham = h.ham;
+        d.g.nx = L.nx; d.g.ny = L.ny; d.g.nz = L.nz;
+        d.g.W = (uint32_t)(L.nz / 2);
+        d.g.half = (uint32_t)(L.natoms / 2);
+        d.g.row_stride_x = d.g.W * (uint32_t)L.ny;
+        d.g.ensemble = h.ensemble;
+        d.g.r = (float)s->opt.r;
+        d.spins = h.mesh->d_spins;
+        d.N = (uint32_t)L.natoms;
+        d.divNY = make_div((uint32_t)L.ny);
+        d.divTX = make_div(d.g.W / 2u);
+        d.P = h.P;
+        d.nch = h.nch;
+        d.rb = (uint32_t)s->sched.block_threads / (d.g.W / 2u);
+        d.step_x = d.rb / (uint32_t)L.ny;
+        d.step_y = d.rb % (uint32_t)L.ny;
+        d.n_rep = h.n;
+        d.beta_rep = h.d_beta_rep;
+        d.sweep_ctr = h.mesh->d_sweep;
+        d.partials = s->d_partials + h.part_off;
+        d.done = s->d_sync + kSyncDone + h.done_off;
+        d.ready = s->d_sync + kSyncReady + i;
+        d.fin = reinterpret_cast<unsigned long long*>(s->d_sync + kSyncFin) + i;
+        d.acc = h.d_acc; d.beta_t = h.d_beta_t; d.t2r = h.d_t2r; d.r2t = h.d_r2t;
+        d.stats = h.d_stats; d.round_ctr = h.d_round;
+    }
+    P->n_ens = (int)s->ens.size();
+    P->table = s->d_table;
+    P->tasks_per_round = (uint32_t)s->table.size();
+    P->rounds = (uint32_t)rounds;
+    P->k = (uint32_t)k;
+    P->head = s->d_sync;
+    P->abort = s->d_sync + 1;
+    P->where = s->d_sync + 2;
+    P->status = s->d_status;
+    P->wait_ns = (uint64_t)(s->opt.wait_timeout_ms > 0 ? s->opt.wait_timeout_ms : 2000) * 1000000ull;
+    P->scheme = s->opt.scheme;
+    P->stall_ens = stall;
+    P->seed = s->opt.seed;
+    uint32_t k0 = (uint32_t)s->opt.seed, k1 = (uint32_t)(s->opt.seed >> 32);
+    for (int i = 0; i < 10; ++i) { P->rk[2 * i] = k0; P->rk[2 * i + 1] = k1; k0 += kPhiloxW0; k1 += kPhiloxW1; }
+}
+
+int ens_enqueue_launch(ising_ensembles* s, int k, int rounds, int stall) {
+    EnsParams P;
+    ens_params(s, k, rounds, stall, &P);
+    ISG_CUDA(cudaMemsetAsync(s->d_sync, 0, s->sync_words * sizeof(uint32_t), s->stream));
+    return launch_ensembles(P, s->move, s->dmi, s->has_k, s->sched.block_threads, s->grid, s->stream);
+}
+
+int ens_resync_enqueue(ising_ensembles* s) {
+    for (auto& h : s->ens) {
+        ising_mesh* m = h.mesh;
+        cudaStream_t keep = m->stream;
+        m->stream = s->stream;
+        const int st = enqueue_energy(m, h.p, 0, h.n, h.d_energy_out, h.d_energy_tmp);
+        m->stream = keep;
+        ISG_TRY(st);
+        ISG_CUDA(cudaMemcpyAsync(h.d_acc, h.d_energy_out, (size_t)h.n * 4 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                 s->stream));
+    }
+    return ISING_OK;
+}
+
+// engine status -> error code; after a timeout the partial sums are cleared and the
+// accumulators recomputed so that the engine stays usable
+int ens_check(ising_ensembles* s) {
+    ISG_CUDA(cudaMemcpyAsync(s->h_words, s->d_status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    ISG_CUDA(cudaMemcpyAsync(s->h_words + 1, s->d_sync + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    ISG_CUDA(cudaStreamSynchronize(s->stream));
+    const int st = (int)s->h_words[0];
+    if (!st) return ISING_OK;
+    const uint32_t where = s->h_words[1];
+    ISG_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
+    if (st & kStatTimeout) {
+        ISG_CUDA(cudaMemsetAsync(s->d_partials, 0, s->partials_cap * sizeof(double), s->stream));
+        ISG_TRY(ens_resync_enqueue(s));
+        ISG_CUDA(cudaStreamSynchronize(s->stream));
+        char msg[160];
+        std::snprintf(msg, sizeof msg, "device wait timed out at task %u of the round table", where ? where - 1 : 0u);
+        return fail(ISING_ERR_TIMEOUT, msg);
+    }
+    if (st & kStatNan) return fail(ISING_ERR_NAN, "NaN in spins or proposals");
+    return fail(ISING_ERR_BOUNDS, "device index out of bounds");
+}
+
+int ens_run(ising_ensembles* s, int k, int rounds) {
+    ISG_TRY(ens_build_table(s, k));
+    const int64_t tpr = (int64_t)s->table.size();
+    const int max_r = (int)std::max<int64_t>(1, ((int64_t)1 << 31) / std::max<int64_t>(tpr, 1) - 1);
+    while (rounds > 0) {
+        int R = std::min(rounds, max_r);
+        if (s->opt.resync_every > 0)
+            R = std::min<int64_t>(R, s->opt.resync_every - s->rounds_done % s->opt.resync_every);
+        if (s->stall_next >= 0) {
+            const int stall = s->stall_next;
+            s->stall_next = -1;
+            ISG_TRY(ens_enqueue_launch(s, k, R, stall));
+        } else {
+            if (!s->graph || s->graph_k != k || s->graph_rounds != R) {
+                ens_drop_graph(s);
+                cudaGraph_t g;
+                ISG_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+                const int st = ens_enqueue_launch(s, k, R, -1);
+                cudaError_t ce = cudaStreamEndCapture(s->stream, &g);
+                if (st != ISING_OK) { if (ce == cudaSuccess) cudaGraphDestroy(g); return st; }
+                ISG_CUDA(ce);
+                ce = cudaGraphInstantiate(&s->graph, g, 0);
+                cudaGraphDestroy(g);
+                ISG_CUDA(ce);
+                s->graph_k = k;
+                s->graph_rounds = R;
+            }
+            ISG_CUDA(cudaGraphLaunch(s->graph, s->stream));
+        }
+        s->rounds_done += R;
+        rounds -= R;
+        if (s->opt.resync_every > 0 && s->rounds_done % s->opt.resync_every == 0) ISG_TRY(ens_resync_enqueue(s));
+    }
+    return ens_check(s);
+}
+
+int ens_index(const ising_ensembles* s, int e) {
+    if (!s) return fail(ISING_ERR_ARG, "engine is NULL");
+    if (e < 0 || e >= (int)s->ens.size()) return fail(ISING_ERR_BOUNDS, "ensemble index out of range");
+    return ISING_OK;
+}
+
+}  // namespace
+
+extern "C" int ising_ensembles_create(int n, const ising_ensemble_desc* desc, const ising_ensembles_options* opt,
+                                      ising_ensembles** out) {
+    if (!out) return fail(ISING_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!desc || !opt) return fail(ISING_ERR_ARG, "NULL argument");
+    if (n < 1 || n > kMaxEnsembles) return fail(ISING_ERR_ARG, "n_ensembles must be 1..16");
+    if (opt->move != ISING_MOVE_UNIFORM && opt->move != ISING_MOVE_BALL) return fail(ISING_ERR_ARG, "bad move");
+    if (opt->scheme != ISING_PT_EVEN_ODD && opt->scheme != ISING_PT_RANDOM_PAIRS) return fail(ISING_ERR_ARG, "bad scheme");
+    if (opt->resync_every < 0 || opt->wait_timeout_ms < 0) return fail(ISING_ERR_ARG, "negative option");
+    if (!std::isfinite(opt->r)) return fail(ISING_ERR_NAN, "non-finite r");
+    const int dev = desc[0].mesh ? desc[0].mesh->device : -1;
+    std::vector<int> kinds;
+    for (int e = 0; e < n; ++e) {
+        const ising_ensemble_desc& d = desc[e];
+        ISG_TRY(check_replica(d.mesh, 0));
+        if (d.mesh->device != dev) return fail(ISING_ERR_ARG, "all meshes must be on one device");
+        for (int f = 0; f < e; ++f)
+            if (desc[f].mesh == d.mesh) return fail(ISING_ERR_ARG, "each ensemble needs its own mesh");
+        ISG_TRY(validate_params(&d.params));
+        const Lattice& L = d.mesh->lat;
+        if (!d.mesh->layout.cb || uses_shell2(L, d.params))
+            return fail(ISING_ERR_UNSUPPORTED, "the batched engine needs colour-separated simple-cubic meshes "
+                                               "(even nx, ny; nz % 4 == 0) and shell-1 couplings");
+        if (L.nx > 65535 || L.natoms >= (int64_t)1 << 31) return fail(ISING_ERR_ARG, "mesh too large for the engine");
+        if (d.n_temps < 1 || d.n_temps > d.mesh->n_replicas) return fail(ISING_ERR_ARG, "n_temps must be in 1..n_replicas");
+        if (d.ensemble >= (1u << 24)) return fail(ISING_ERR_ARG, "ensemble id must be < 2^24");
+        if (!d.betas) return fail(ISING_ERR_ARG, "betas is NULL");
+        for (int t = 0; t < d.n_temps; ++t) if (!std::isfinite(d.betas[t])) return fail(ISING_ERR_NAN, "non-finite beta");
+    }
+    DeviceGuard g(dev);
+    std::unique_ptr<ising_ensembles> s(new ising_ensembles());
+    s->opt = *opt;
+    s->device = dev;
+    s->move = opt->move;
+    auto bail = [&](int st) { ens_free(s.get()); return st; };
+    int st = ISING_OK;
+    if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(cuda_fail(cudaGetLastError(), "cudaStreamCreateWithFlags"));
+    s->stream = s->own_stream;
+    std::vector<int> dk;
+    for (int e = 0; e < n; ++e) {
+        const ising_ensemble_desc& d = desc[e];
+        EnsHost h;
+        h.mesh = d.mesh; h.n = d.n_temps; h.p = d.params; h.ensemble = d.ensemble;
+        h.ham = make_ham(d.params);
+        if ((st = sc_dmi(d.mesh, d.params, &h.ham, &h.dmi_kind)) != ISING_OK) return bail(st);
+        if (h.ham.K != 0.f) s->has_k = true;
+        dk.push_back(h.dmi_kind);
+        s->ens.push_back(h);
+    }
+    // one kernel variant for all: the common DMI form, else the tabulated one (kind 0 is
+    // kind 1 with D = 0)
+    {
+        int kind = 0;
+        for (int k : dk) {
+            if (k == 0) continue;
+            if (kind == 0) kind = k;
+            else if (kind != k) kind = 3;
+        }
+        s->dmi = kind;
+    }
+    for (int e = 0; e < n; ++e) {
+        EnsHost& h = s->ens[e];
+        ising_mesh* m = h.mesh;
+        if ((st = cudaStreamSynchronize(m->stream)) != cudaSuccess) return bail(cuda_fail((cudaError_t)st, "mesh sync"));
+        const int tmp = energy_tmp_doubles(m, h.n);
+        if ((st = dev_alloc(&h.d_beta_t, h.n)) || (st = dev_alloc(&h.d_beta_rep, h.n)) ||
+            (st = dev_alloc(&h.d_t2r, h.n)) || (st = dev_alloc(&h.d_r2t, h.n)) || (st = dev_alloc(&h.d_acc, h.n)) ||
+            (st = dev_alloc(&h.d_stats, 2 * (size_t)h.n)) || (st = dev_alloc(&h.d_round, 1)) ||
+            (st = dev_alloc(&h.d_energy_tmp, tmp)) || (st = dev_alloc(&h.d_energy_out, 4 * (size_t)h.n)))
+            return bail(st);
+        std::vector<int> ident(h.n);
+        for (int t = 0; t < h.n; ++t) ident[t] = t;
+        cudaError_t ce = cudaMemcpy(h.d_beta_t, desc[e].betas, h.n * sizeof(double), cudaMemcpyHostToDevice);
+        if (ce == cudaSuccess) ce = cudaMemcpy(h.d_beta_rep, desc[e].betas, h.n * sizeof(double), cudaMemcpyHostToDevice);
+        if (ce == cudaSuccess) ce = cudaMemcpy(h.d_t2r, ident.data(), h.n * sizeof(int), cudaMemcpyHostToDevice);
+        if (ce == cudaSuccess) ce = cudaMemcpy(h.d_r2t, ident.data(), h.n * sizeof(int), cudaMemcpyHostToDevice);
+        if (ce == cudaSuccess) ce = cudaMemset(h.d_stats, 0, 2 * (size_t)h.n * sizeof(unsigned long long));
+        if (ce == cudaSuccess) ce = cudaMemset(h.d_round, 0, sizeof(uint32_t));
+        if (ce != cudaSuccess) return bail(cuda_fail(ce, "ensemble init"));
+    }
+    if ((st = dev_alloc(&s->d_status, 1)) != ISING_OK) return bail(st);
+    if (cudaMemset(s->d_status, 0, sizeof(int)) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "status init"));
+    if (cudaMallocHost((void**)&s->h_words, 4 * sizeof(uint32_t)) != cudaSuccess) {
+        s->h_words = nullptr;
+        return bail(fail(ISING_ERR_ALLOC, "cudaMallocHost failed"));
+    }
+    ising_ensembles_schedule_t c = s->sched;
+    int max_lanes = 0;
+    for (auto& h : s->ens) max_lanes = std::max(max_lanes, h.mesh->lat.nz / 4);
+    if (max_lanes > c.block_threads) return bail(fail(ISING_ERR_ARG, "nz too large for the engine (nz <= 1024)"));
+    if ((st = ens_apply_schedule(s.get(), c)) != ISING_OK) return bail(st);
+    if ((st = ens_resync_enqueue(s.get())) != ISING_OK) return bail(st);
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "engine init sync"));
+    *out = s.release();
+    return ISING_OK;
+}
+
+extern "C" int ising_ensembles_destroy(ising_ensembles* s) {
+    if (!s) return ISING_OK;
+    DeviceGuard g(s->device);
+    cudaStreamSynchronize(s->stream);
+    ens_free(s);
+    delete s;
+    return ISING_OK;
+}
+
+extern "C" int ising_ensembles_set_stream(ising_ensembles* s, void* stream) {
+    if (!s) return fail(ISING_ERR_ARG, "engine is NULL");
+    DeviceGuard g(s->device);
+    ISG_CUDA(cudaStreamSynchronize(s->stream));
+    s->stream = stream ? static_cast<cudaStream_t>(stream) : s->own_stream;
+    ens_drop_graph(s);
+    return ISING_OK;
+}
+
+extern "C" int ising_ensembles_run(ising_ensembles* s, int k, int rounds) {
+    if (!s) return fail(ISING_ERR_ARG, "engine is NULL");
+    if (k < 1 || k > 32767 || rounds < 0) return fail(ISING_ERR_ARG, "sweeps_per_swap must be 1..32767 and rounds >= 0");
+    DeviceGuard g(s->device);
+    return ens_run(s, k, rounds);
+}
+
+extern "C" int ising_ensembles_set_schedule(ising_ensembles* s, const ising_ensembles_schedule_t* c) {
+    if (!s || !c) return fail(ISING_ERR_ARG, "NULL argument");
+    DeviceGuard g(s->device);
+    return ens_apply_schedule(s, *c);
+}
+
+extern "C" int ising_ensembles_get_schedule(const ising_ensembles* s, ising_ensembles_schedule_t* c, int* grid,
+                                            int64_t* tasks_per_pass) {
+    if (!s) return fail(ISING_ERR_ARG, "engine is NULL");
+    if (c) *c = s->sched;
+    if (grid) *grid = s->grid;
+    if (tasks_per_pass) {
+        int64_t t = 0;
+        for (const auto& h : s->ens) t += (int64_t)h.n * h.nch;
+        *tasks_per_pass = t;
+    }
+    return ISING_OK;
+}
+
+extern "C" int ising_ensembles_autotune(ising_ensembles* s, int k, int rounds_per_trial,
+                                        ising_ensembles_schedule_t* trials, int max_trials, int* n_trials) {
+    if (!s) return fail(ISING_ERR_ARG, "engine is NULL");
+    if (k < 1 || rounds_per_trial < 1) return fail(ISING_ERR_ARG, "sweeps_per_swap and rounds_per_trial must be >= 1");
+    DeviceGuard g(s->device);
+    std::vector<ising_ensembles_schedule_t> cand;
+    int max_lanes = 0;
+    for (auto& h : s->ens) max_lanes = std::max(max_lanes, h.mesh->lat.nz / 4);
+    const int threads[] = {256, 128};
+    const int chunks[] = {2048, 4096, 8192};
+    for (int t : threads) {
+        if (t < max_lanes) continue;
+        for (int c : chunks) {
+            cand.push_back({t, c, ISING_ENS_ORDER_PHASE, 0, 0.0});
+            cand.push_back({t, c, ISING_ENS_ORDER_GROUPS, 32000000, 0.0});
+            cand.push_back({t, c, ISING_ENS_ORDER_GROUPS, 64000000, 0.0});
+        }
+    }
+    cudaEvent_t e0, e1;
+    ISG_CUDA(cudaEventCreate(&e0));
+    ISG_CUDA(cudaEventCreate(&e1));
+    int best = -1, n = 0;
+    int st = ISING_OK;
+    for (size_t i = 0; i < cand.size() && st == ISING_OK; ++i) {
+        if ((st = ens_apply_schedule(s, cand[i])) != ISING_OK) break;
+        if ((st = ens_run(s, k, rounds_per_trial)) != ISING_OK) break;   // warm-up: table, graph
+        cudaEventRecord(e0, s->stream);
+        if ((st = ens_run(s, k, rounds_per_trial)) != ISING_OK) break;
+        cudaEventRecord(e1, s->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cand[i].ms_per_round = ms / rounds_per_trial;
+        if (trials && n < max_trials) trials[n] = cand[i];
+        ++n;
+        if (best < 0 || cand[i].ms_per_round < cand[best].ms_per_round) best = (int)i;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (n_trials) *n_trials = n;
+    if (st != ISING_OK) return st;
+    if (best < 0) return fail(ISING_ERR_ARG, "no candidate schedule fits these ensembles");
+    const double ms = cand[best].ms_per_round;
+    ISG_TRY(ens_apply_schedule(s, cand[best]));
+    s->sched.ms_per_round = ms;
+    return ISING_OK;
+}
+
+extern "C" int ising_ensembles_permutation(const ising_ensembles* s, int e, int* t2r) {
+    ISG_TRY(ens_index(s, e));
+    if (!t2r) return fail(ISING_ERR_ARG, "NULL argument");
+    DeviceGuard g(s->device);
+    const EnsHost& h = s->ens[e];
+    ISG_CUDA(cudaMemcpyAsync(t2r, h.d_t2r, h.n * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    ISG_CUDA(cudaStreamSynchronize(s->stream));
+    return ISING_OK;
+}
+
+extern "C" int ising_ensembles_energies(const ising_ensembles* s, int e, double* E, double* M) {
+    ISG_TRY(ens_index(s, e));
+    DeviceGuard g(s->device);
+    const EnsHost& h = s->ens[e];
+    std::vector<Acc4> a(h.n);
+    ISG_CUDA(cudaMemcpyAsync(a.data(), h.d_acc, h.n * sizeof(Acc4), cudaMemcpyDeviceToHost, s->stream));
+    ISG_CUDA(cudaStreamSynchronize(s->stream));
+    for (int r = 0; r < h.n; ++r) {
+        if (E) E[r] = a[r].e;
+        if (M) { M[3 * r] = a[r].mx; M[3 * r + 1] = a[r].my; M[3 * r + 2] = a[r].mz; }
+    }
+    return ISING_OK;
+}
+
+extern "C" int ising_ensembles_swap_stats(const ising_ensembles* s, int e, uint64_t* att, uint64_t* acc) {
+    ISG_TRY(ens_index(s, e));
+    DeviceGuard g(s->device);
+    const EnsHost& h = s->ens[e];
+    std::vector<unsigned long long> v(2 * (size_t)h.n);
+    ISG_CUDA(cudaMemcpyAsync(v.data(), h.d_stats, v.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             s->stream));
+    ISG_CUDA(cudaStreamSynchronize(s->stream));
+    for (int t = 0; t + 1 < h.n; ++t) {
+        if (att) att[t] = v[t];
+        if (acc) acc[t] = v[(h.n - 1) + t];
+    }
+    return ISING_OK;
+}
+
+extern "C" int ising_ensembles_resync(ising_ensembles* s) {
+    if (!s) return fail(ISING_ERR_ARG, "engine is NULL");
+    DeviceGuard g(s->device);
+    ISG_TRY(ens_resync_enqueue(s));
+    ISG_CUDA(cudaStreamSynchronize(s->stream));
+    return ISING_OK;
+}
+
+extern "C" int ising_ensembles_inject_stall(ising_ensembles* s, int e) {
+    ISG_TRY(ens_index(s, e));
+    s->stall_next = e;
+    return ISING_OK;
+}
+
 namespace isg {
 // Shell or legacy stencil of p written into caller-provided host memory (no allocation).
 int fill_query_stencil_host(const ising_mesh* m, const ising_params& p, bool legacy, Slot* slots, int* cnt) {

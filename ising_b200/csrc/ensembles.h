@@ -1,0 +1,70 @@
+// ensembles.h -- device-side description of the persistent multi-ensemble PT engine.
+//
+// Work is a queue of tasks, one per (ensemble e, replica r, phase, chunk): a phase is one
+// colour pass (phase p of a round is colour p & 1 of sweep p >> 1), a chunk is P consecutive
+// x-planes of the colour-separated layout.  A task may start when its own chunk and the two
+// x-neighbour chunks (cyclic) have finished the previous phase, and, for the first phase of
+// a round, when ensemble e has finished the previous round's exchange.  The queue order
+// (host-built table) puts every task after all tasks it waits for, so a block only ever waits
+// for tasks that running blocks hold and the kernel needs no co-residency guarantee.  The
+// last task of a round of ensemble e folds the partial sums and runs the exchange in-kernel.
+#pragma once
+#include "sweep_cb.cuh"
+
+namespace isg {
+
+constexpr int kMaxEnsembles = 16;   // compile-time slots of the kernel's ensemble switch
+constexpr int kEnsMaxThreads = 256;
+
+struct EnsDev {
+    CbGeom g;                    // geometry and Hamiltonian for the pair update
+    float* spins;                // replica 0 of the mesh
+    uint32_t N;                  // atoms per replica
+    FastDiv divNY;
+    FastDiv divTX;               // W / 2 lanes per packed row
+    uint32_t P;                  // x-planes per chunk
+    uint32_t nch;                // chunks per replica
+    uint32_t rb;                 // rows per block pass: threads / (W / 2)
+    uint32_t step_x, step_y;     // rb = step_x * ny + step_y
+    int n_rep;                   // replicas 0..n_rep-1 (= temperature slots)
+    double* beta_rep;
+    uint32_t* sweep_ctr;         // the mesh's per-replica sweep counters
+    double* partials;            // [n_rep][nch][4]: dE, dMx, dMy, dMz of the running round
+    uint32_t* done;              // [n_rep][nch]: phases finished in this launch
+    uint32_t* ready;             // rounds of this launch whose exchange is finished
+    unsigned long long* fin;     // final-phase tasks finished in this launch
+    Acc4* acc;
+    const double* beta_t;
+    int* t2r;
+    int* r2t;
+    unsigned long long* stats;
+    uint32_t* round_ctr;
+};
+
+struct EnsParams {
+    EnsDev e[kMaxEnsembles];
+    int n_ens;
+    const uint2* table;          // one round: x = e << 24 | r, y = phase << 16 | chunk
+    uint32_t tasks_per_round;
+    uint32_t rounds;
+    uint32_t k;                  // sweeps per round
+    uint32_t* head;              // queue position
+    uint32_t* abort;             // set when a wait gives up; every block then stops
+    uint32_t* where;             // 1 + task id of the first wait that gave up
+    int* status;
+    uint64_t wait_ns;            // bound of every wait
+    int scheme;
+    int stall_ens;               // test hook: round >= 1 of this ensemble waits for a flag nothing sets
+    uint64_t seed;
+    uint32_t rk[20];             // Philox round keys of seed
+};
+static_assert(sizeof(EnsParams) < 32000, "kernel parameter block too large");
+
+int launch_ensembles(const EnsParams& P, int move, int dmi, bool has_k, int threads, int grid, cudaStream_t s);
+// kernel instantiations, one translation unit per move kind (dmi in 1..3: 1 bulk,
+// 2 interfacial about z, 3 tabulated per bond direction)
+const void* ensembles_kernel_uniform(int dmi, bool has_k);
+const void* ensembles_kernel_ball(int dmi, bool has_k);
+int ensembles_blocks_per_sm(int move, int dmi, bool has_k, int threads, int* out);
+
+}  // namespace isg

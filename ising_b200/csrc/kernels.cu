@@ -6,6 +6,7 @@
 #include <cstdio>
 
 #include "internal.h"
+#include "exchange.cuh"
 
 namespace isg {
 
@@ -370,54 +371,8 @@ int launch_advance(uint32_t* ctr, int n, uint32_t by, cudaStream_t s) {
 }
 
 // ================================================================= replica exchange
-// Swap of temperature labels between neighbouring slots (the reference relabels
-// TemperatureMeshArray and never moves spins, src/PT.f90:264-268).  Criterion
-// min(1, exp((b_t - b_{t+1})(E_t - E_{t+1}))) with FP64 running energies.
-// EVEN_ODD: all pairs (t, t+1) with t = round parity, in parallel (disjoint pairs).
-// RANDOM_PAIRS: n sequential attempts at Index1 = nint(u (n-1)) (src/PT.f90:236-244).
-__global__ void k_exchange(ExchangeLaunch a) {
-    const int n = a.n;
-    const uint32_t round = *a.round;
-    const uint2 key = philox_key(a.seed);
-    const uint32_t tagw = (a.ensemble << 8) | kTagExchange;
-    if (a.scheme == 0) {
-        for (int t = (int)(round & 1u) + 2 * threadIdx.x; t + 1 < n; t += 2 * blockDim.x) {
-            const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)t, round, 0u, tagw), key);
-            const int ra = a.t2r[t], rb = a.t2r[t + 1];
-            const double d = (a.beta_t[t] - a.beta_t[t + 1]) * (a.acc[ra].e - a.acc[rb].e);
-            const double u = (double)(2u * (r4.x >> 9) + 1u) * (1.0 / 16777216.0);
-            a.stats[t] += 1ull;
-            if (d >= 0.0 || u < exp(d)) {
-                a.t2r[t] = rb; a.t2r[t + 1] = ra;
-                a.stats[(n - 1) + t] += 1ull;
-            }
-        }
-    } else if (threadIdx.x == 0) {
-        for (int q = 0; q < n; ++q) {
-            const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)q, round, 1u, tagw), key);
-            const double u0 = (double)(2u * (r4.x >> 9) + 1u) * (1.0 / 16777216.0);
-            const double u1 = (double)(2u * (r4.y >> 9) + 1u) * (1.0 / 16777216.0);
-            const double xv = u0 * (double)(n - 1);
-            const int i1 = (int)(xv >= 0.0 ? floor(xv + 0.5) : -floor(-xv + 0.5));
-            const int i2 = i1 == 0 ? 1 : (i1 == n - 1 ? n - 2 : i1 + 1);
-            const int t = i1 < i2 ? i1 : i2;
-            const int ra = a.t2r[t], rb = a.t2r[t + 1];
-            const double d = (a.beta_t[t] - a.beta_t[t + 1]) * (a.acc[ra].e - a.acc[rb].e);
-            a.stats[t] += 1ull;
-            if (d >= 0.0 || u1 < exp(d)) {
-                a.t2r[t] = rb; a.t2r[t + 1] = ra;
-                a.stats[(n - 1) + t] += 1ull;
-            }
-        }
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < n; t += blockDim.x) {
-        const int r = a.t2r[t];
-        a.r2t[r] = t;
-        a.beta_rep[r] = a.beta_t[t];
-    }
-    if (threadIdx.x == 0) *a.round = round + 1u;
-}
+// One exchange round (exchange.cuh) as its own single-block launch.
+__global__ void k_exchange(ExchangeLaunch a) { exchange_round(a); }
 
 int launch_exchange(const ExchangeLaunch& a, cudaStream_t s) {
     if (a.n < 2) return ISING_OK;
