@@ -2,13 +2,18 @@
 """Benchmark of the Heisenberg Metropolis / parallel-tempering hot path on B200.
 
 One step = one parallel-tempering round of the workload: `sweeps_per_swap` colour-class
-sweeps of every replica followed by one replica exchange, replayed from a CUDA graph.
+sweeps of every replica of every ensemble, then each ensemble's replica exchange.  The
+whole timed region is one launch of the persistent multi-ensemble kernel (ising_ensembles_*,
+replayed from a CUDA graph); its schedule is picked by the library's autotuner during
+warm-up.  `--engine pt` times the per-colour-pass launch path (ising_pt_*) instead.
 metric: spin-updates/s = attempted single-site updates (N per replica per sweep) / s.
 
 Default workload (N=1): simple cubic L=128, 16 replicas, T geometric 0.1-1.5, J=1
 (ferromagnetic, passed as J=-1 in the reference sign convention), bulk DMI D=0.7,
 B=0.3 along z, K=0.05 along z, ball move r=0.2, swaps every 10 sweeps.  Spin state is
-384 MiB (> 126 MB L2), so no L2 flush is needed between steps.
+384 MiB (> 126 MB L2), so no L2 flush is needed between steps.  Workload c4: 12 ensembles
+L in {16,24,32,48,64,96} (two each), (D,B) on the grid {0.3,0.5,0.7} x {0.1,0.3},
+16-64 replicas each, T geometric 0.1-2.0 (148,160,512 sites, 1.78 GB of spins).
 
 Under torchrun each rank runs its own copy of the workload on its GPU (independent
 ensembles, weak scaling, no collective on the data path); the timed region is bracketed
@@ -39,6 +44,12 @@ WORKLOADS = {
                desc="SC L=32 x 32 PT replicas, T 0.2-2.0, J=1, bulk D=0.5, B=0.2 z"),
     "c5": dict(L=96, R=48, tmin=0.1, tmax=1.5, J=-1.0, D=0.5, B=0.25, K=0.0, move="ball", r=0.2, k=10,
                desc="SC L=96 x 48 PT replicas, T 0.1-1.5, J=1, bulk D=0.5, B=0.25 z"),
+    "c4": dict(L=96, R=64, tmin=0.1, tmax=2.0, J=-1.0, D=0.5, B=0.1, K=0.0, move="ball", r=0.2, k=10,
+               desc="12 SC PT ensembles, L in {16,24,32,48,64,96} x2, (D,B) in {0.3,0.5,0.7}x{0.1,0.3}, "
+                    "16-64 replicas, T 0.1-2.0, J=1, bulk DMI, B z",
+               ensembles=[(L, {16: 16, 24: 16, 32: 32, 48: 32, 64: 48, 96: 64}[L],
+                           [(0.3, 0.1), (0.3, 0.3), (0.5, 0.1), (0.5, 0.3), (0.7, 0.1), (0.7, 0.3)][i % 6])
+                          for i, L in enumerate([16, 16, 24, 24, 32, 32, 48, 48, 64, 64, 96, 96])]),
 }
 BYTES_PER_UPDATE = 24  # algorithmic: one FP32 x,y,z read and write per site per sweep
 
@@ -155,6 +166,13 @@ def run_reference(args, w):
 
 
 # ---------------------------------------------------------------- GPU arm
+def ensembles_of(args, w):
+    """[(L, replicas, D, B)] of the workload."""
+    if "ensembles" in w:
+        return [(L, R, D, B) for L, R, (D, B) in w["ensembles"]]
+    return [(args.L or w["L"], args.replicas or w["R"], w["D"], w["B"])]
+
+
 def run_gpu(args, w):
     import numpy as np
     import torch
@@ -169,17 +187,19 @@ def run_gpu(args, w):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     dev = torch.cuda.current_device()
     stream = torch.cuda.current_stream()
-    L, R = args.L or w["L"], args.replicas or w["R"]
     k = w["k"]
-    N = L ** 3
-    mesh = ib.ChainMesh.simple_cubic(L, n_replicas=R, device=dev)
-    mesh.set_stream(stream.cuda_stream)
-    mesh.init_uniform(0x15196, ensemble=rank)
-    p = ib.params(J=w["J"], Dz=w["D"], B=w["B"], K=w["K"], dmi="bulk")
-    T = ib.temperature_ladder(w["tmin"], w["tmax"], R)
-    betas = 1.0 / T
     move = _lib.MOVE_BALL if w["move"] == "ball" else _lib.MOVE_UNIFORM
-    pt = ib.ParallelTempering(mesh, betas, p, seed=0x15196, ensemble=rank, move=move, r=w["r"])
+    spec = ensembles_of(args, w)
+    members = []
+    for i, (L, R, D, B) in enumerate(spec):
+        ens_id = rank * len(spec) + i            # distinct Philox streams per rank and ensemble
+        m = ib.ChainMesh.simple_cubic(L, n_replicas=R, device=dev)
+        m.set_stream(stream.cuda_stream)
+        m.init_uniform(0x15196, ensemble=ens_id)
+        p = ib.params(J=w["J"], Dz=D, B=B, K=w["K"], dmi="bulk")
+        members.append((m, 1.0 / ib.temperature_ladder(w["tmin"], w["tmax"], R), p, ens_id))
+    sites = sum(L ** 3 * R for L, R, _, _ in spec)
+    updates_per_step = sites * k
 
     def barrier():
         if world > 1:
@@ -193,8 +213,37 @@ def run_gpu(args, w):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # warm-up (also builds the CUDA graph)
-    pt.run(k, max(args.warmup, 1) if args.warmup > 0 else 1)
+    sched_info = {}
+    if args.engine == "ensembles":
+        eng = ib.Ensembles(members, seed=0x15196, move=move, r=w["r"])
+        eng.set_stream(stream.cuda_stream)
+        trials = eng.autotune(k, 1) if not args.no_autotune else []
+        eng.run(k, max(args.warmup, 1))
+        run = lambda n: eng.run(k, n)
+        energies = lambda: [eng.energies(i) for i in range(len(members))]
+        sched_info = eng.schedule()
+        sched_info["autotune_trials"] = len(trials)
+        if trials:
+            best = min(trials, key=lambda t: t["ms_per_round"])
+            worst = max(trials, key=lambda t: t["ms_per_round"])
+            sched_info["autotune_spread_ms"] = [best["ms_per_round"], worst["ms_per_round"]]
+        kernel_name = "k_ensembles"
+        launches_timed = 1                       # one persistent launch (plus a memset node)
+        closers = [eng]
+    else:
+        if len(members) != 1:
+            raise SystemExit("--engine pt runs single-ensemble workloads only")
+        m, betas, p, ens_id = members[0]
+        pt = ib.ParallelTempering(m, betas, p, seed=0x15196, ensemble=ens_id, move=move, r=w["r"])
+        pt.run(k, max(args.warmup, 1))
+        run = lambda n: pt.run(k, n)
+        energies = lambda: [pt.energies()]
+        group, per_round, kern_id = pt.schedule(k)
+        sched_info = {"l2_group_replicas": group, "colour_pass_launches_per_round": per_round,
+                      "kernel": {0: "stencil", 1: "k_cb_sweep", 2: "k_cb_tma"}[kern_id]}
+        kernel_name = sched_info["kernel"]
+        launches_timed = args.steps * (per_round + 3)   # colour passes + fold + exchange + advance
+        closers = [pt]
     barrier()
 
     clocks = ClockSampler(getattr(torch.cuda.get_device_properties(dev), "pci_bus_id", None))
@@ -202,29 +251,32 @@ def run_gpu(args, w):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     ev0.record(stream)
-    pt.run(k, args.steps)
+    run(args.steps)
     ev1.record(stream)
     barrier()
-    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    ms_local = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms_local)
     clk = clocks.stop()
-    updates_per_step = R * N * k
     value = world * updates_per_step * args.steps / (ms / 1e3)
 
-    # dominant kernel: the colour-pass kernel, timed alone on the same stream over n_relax
-    # sweeps (the relax call issues only colour-pass launches plus one fold and one advance)
-    group, per_round, kern_id = pt.schedule(k)
-    n_relax = max(4, min(40, args.steps * k // 2))
-    launches = pt.schedule(n_relax)[1]
-    pt.relax(2)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    pt.relax(n_relax)
-    e1.record(stream)
-    barrier()
-    sweep_ms = e0.elapsed_time(e1) / n_relax
-    launch_ms = e0.elapsed_time(e1) / launches
-    bytes_per_launch = BYTES_PER_UPDATE * R * N * n_relax / launches
+    # dominant kernel: with the engine the timed region is one launch of k_ensembles, so its
+    # launch duration is the event time of the region; with --engine pt the colour-pass
+    # kernel is timed alone over relax sweeps (colour-pass launches plus one fold/advance)
+    if args.engine == "ensembles":
+        launch_ms = ms_local
+        bytes_per_launch = BYTES_PER_UPDATE * updates_per_step * args.steps
+    else:
+        n_relax = max(4, min(40, args.steps * k // 2))
+        launches = pt.schedule(n_relax)[1]
+        pt.relax(2)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pt.relax(n_relax)
+        e1.record(stream)
+        barrier()
+        launch_ms = e0.elapsed_time(e1) / launches
+        bytes_per_launch = BYTES_PER_UPDATE * sites * n_relax / launches
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -238,9 +290,9 @@ def run_gpu(args, w):
     tfile = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     if os.path.exists(tfile):
         try:
-            t = json.load(open(tfile))
-            if t.get("workload") == args.workload and t.get("bytes_per_update"):
-                traffic = t["bytes_per_update"] * R * N / 2
+            for t in json.load(open(tfile)).get("kernels", []):
+                if t.get("kernel") == kernel_name and t.get("bytes_per_update"):
+                    traffic = t["bytes_per_update"] * bytes_per_launch / BYTES_PER_UPDATE
         except Exception:
             traffic = None
 
@@ -250,22 +302,23 @@ def run_gpu(args, w):
     e2e = None
     if not args.no_e2e:
         L_ = _lib.load()
-        host = [torch.empty(3 * N, dtype=torch.float64, pin_memory=True) for _ in range(R)]
-        for r in range(R):
-            _lib.check(L_.ising_spins_get(mesh.handle, r, C.cast(host[r].data_ptr(), C.POINTER(C.c_double))), "get")
-        e_host = np.empty(R)
-        m_host = np.empty((R, 3))
+        host = [[torch.empty(3 * mm.numAtoms, dtype=torch.float64, pin_memory=True) for _ in range(len(b))]
+                for mm, b, _, _ in members]
+        dp = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_double))
+        for (mm, b, _, _), hs in zip(members, host):
+            for r in range(len(b)):
+                _lib.check(L_.ising_spins_get(mm.handle, r, dp(hs[r])), "get")
         e2e_steps = max(1, min(args.steps, 5))
 
         def e2e_step():
-            for r in range(R):
-                _lib.check(L_.ising_spins_set(mesh.handle, r, C.cast(host[r].data_ptr(), C.POINTER(C.c_double))), "set")
-            pt.run(k, 1)
-            for r in range(R):
-                _lib.check(L_.ising_spins_get(mesh.handle, r, C.cast(host[r].data_ptr(), C.POINTER(C.c_double))), "get")
-            e_, m_ = pt.energies()
-            e_host[:] = e_
-            m_host[:] = m_
+            for (mm, b, _, _), hs in zip(members, host):
+                for r in range(len(b)):
+                    _lib.check(L_.ising_spins_set(mm.handle, r, dp(hs[r])), "set")
+            run(1)
+            for (mm, b, _, _), hs in zip(members, host):
+                for r in range(len(b)):
+                    _lib.check(L_.ising_spins_get(mm.handle, r, dp(hs[r])), "get")
+            return energies()
 
         e2e_step()
         barrier()
@@ -278,43 +331,44 @@ def run_gpu(args, w):
         barrier()
         wall = time.perf_counter() - t0
         e_ms = max_over_ranks(max(a0.elapsed_time(a1), wall * 1e3))
+        n_rep = sum(len(b) for _, b, _, _ in members)
         e2e = {"value": world * updates_per_step * e2e_steps / (e_ms / 1e3), "unit": "spin-updates/s",
-               "h2d_bytes_per_step": R * 3 * N * 8, "d2h_bytes_per_step": R * 3 * N * 8 + R * 32,
-               "steps": e2e_steps, "path": "ising_spins_set x R -> ising_pt_run -> ising_spins_get x R + energies"}
+               "h2d_bytes_per_step": sites * 3 * 8, "d2h_bytes_per_step": sites * 3 * 8 + n_rep * 32,
+               "steps": e2e_steps,
+               "path": "ising_spins_set per replica -> one round -> ising_spins_get per replica + energies"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = host_cores()
-        rate, sample = cpu_reference_rate(w, 2, 1, threads, L_sample=min(L, 64))
+        rate, sample = cpu_reference_rate(w, 2, 1, threads, L_sample=min(max(L for L, _, _, _ in spec), 64))
         cpu = {"value": rate, "unit": "spin-updates/s", "cores": threads, "kind": "port", "sample": sample}
 
-    # launches of this library inside the timed region: the paired colour passes of a round
-    # (G*k + 1, or 2k with one group) plus fold + exchange + counter advance
-    launches = args.steps * (per_round + 3)
     if rank == 0:
         line = {
             "metric": "spin-updates/s", "value": value, "unit": "spin-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (uniform random initial spins from Philox, seed 0x15196)",
-            "config": {"workload": args.workload, "desc": w["desc"], "L": L, "replicas": R,
-                       "sweeps_per_step": k, "sites": R * N, "parallelism": f"replicas x{world} (independent ensembles)",
-                       "l2": "state larger than L2 (no flush)" if R * N * 12 > 126e6 else "state fits L2; no flush"},
+            "config": {"workload": args.workload, "desc": w["desc"], "ensembles": len(spec),
+                       "lattices": sorted({L for L, _, _, _ in spec}), "replicas": sum(R for _, R, _, _ in spec),
+                       "sweeps_per_step": k, "sites": sites, "engine": args.engine,
+                       "parallelism": f"replicas x{world} (independent ensembles)",
+                       "l2": "state larger than L2 (no flush)" if sites * 12 > 126e6 else "state fits L2; no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
-                         "kernel": "k_cb_sweep", "launch_ms": launch_ms,
-                         "bytes_per_launch": bytes_per_launch, "sweep_ms": sweep_ms,
+                         "kernel": kernel_name, "launch_ms": launch_ms, "bytes_per_launch": bytes_per_launch,
                          "basis": "24 B per attempted update (one FP32 x,y,z read + write per site per sweep)"},
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "gpu_launches": launches,
-            "schedule": {"l2_group_replicas": group, "colour_pass_launches_per_round": per_round,
-                         "kernel": {0: "stencil", 1: "k_cb_sweep", 2: "k_cb_tma"}[kern_id]},
+            "gpu_launches": launches_timed,
+            "schedule": sched_info,
         }
         print(json.dumps(line), flush=True)
-    pt.close()
-    mesh.close()
+    for c in closers:
+        c.close()
+    for mm, *_ in members:
+        mm.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -328,6 +382,8 @@ def main():
     ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--L", type=int, default=0, help="override lattice size (profiling)")
     ap.add_argument("--replicas", type=int, default=0, help="override replica count (profiling)")
+    ap.add_argument("--engine", default="ensembles", choices=["ensembles", "pt"])
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
