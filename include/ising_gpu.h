@@ -324,6 +324,15 @@ int ising_pt_file_tag(char* buf, size_t cap, double J, double D, double B, doubl
 /* write_winding_number_density (rsp:544-580): "x,y,z,Winding_Density" with F0.8. */
 int ising_write_winding_density_csv(const ising_mesh* mesh, int replica, const char* path);
 
+/* ---------------------------------------------------------------- learned patch proposal */
+/* Tensor-core GEMM on device buffers (no reference counterpart): c / o_bf16 (M x N) =
+ * a (M x K, BF16, K contiguous) * b (N x K, BF16)^T (+ bias[N]); o_bf16 gets GELU(tanh form)
+ * of the sum when gelu = 1.  N multiple of 16 up to 256, K multiple of 16, row pitches
+ * multiples of 8; a must hold ceil(M/128)*128 readable rows.  stream is a cudaStream_t
+ * (NULL = legacy default stream); the call synchronises it. */
+int ising_bf16_gemm(const void* a, int lda, const void* b, int ldb, int M, int N, int K, const float* bias,
+                    float* c, int ldc, void* o_bf16, int ldo, int gelu, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -120,6 +120,7 @@ _SIGS = {
     "ising_ensembles_swap_stats": (_i, [_vp, _i, _P(_u64), _P(_u64)]),
     "ising_ensembles_resync": (_i, [_vp]),
     "ising_ensembles_inject_stall": (_i, [_vp, _i]),
+    "ising_bf16_gemm": (_i, [_vp, _i, _vp, _i, _i, _i, _i, _P(C.c_float), _P(C.c_float), _i, _vp, _i, _i, _vp]),
     "ising_write_spins_csv": (_i, [_vp, _i, C.c_char_p, _i, _i, _i]),
     "ising_write_pt_data_csv": (_i, [C.c_char_p, _d, _d, _d, _d, _d, _i, _d, _P(_d)]),
     "ising_pt_file_tag": (_i, [C.c_char_p, C.c_size_t, _d, _d, _d, _d]),
