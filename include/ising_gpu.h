@@ -333,6 +333,27 @@ int ising_write_winding_density_csv(const ising_mesh* mesh, int replica, const c
 int ising_bf16_gemm(const void* a, int lda, const void* b, int ldb, int M, int N, int K, const float* bias,
                     float* c, int ldc, void* o_bf16, int ldo, int gelu, void* stream);
 
+/* The proposal network (no reference counterpart; the reference proposes single-spin moves
+ * only, src/energyMin.f90:49-68).  Input windows are FP32 device arrays [n][3][8][8][8]
+ * (component, then window site (i, j, k) = lattice site (px-2+i, py-2+j, pz-2+k) of a patch
+ * with lowest corner (px, py, pz)); output [n][64][4] = (mu_x, mu_y, mu_z, log sigma) per
+ * patch site (i, j, k of the 4^3 patch, k fastest).  Parameters are FP32 in PyTorch conv3d
+ * order: W1[32][3][3][3][3], b1[32], W2[32][32][3][3][3], b2, W3, b3, Wh[4][32], bh[4]. */
+typedef struct ising_net ising_net;
+int ising_net_create(int device, int max_batch, uint64_t seed, ising_net** out);
+int ising_net_destroy(ising_net* net);
+int ising_net_param_count(void);
+int ising_net_set_params(ising_net* net, const float* host_params);
+int ising_net_get_params(const ising_net* net, float* host_params);
+int ising_net_forward(ising_net* net, const float* d_windows, int n, float* d_out);
+/* mean Gaussian NLL of target patch spins d_targets [n][64][3] (tangent rotation from the
+ * window's patch spins) and its gradient (host_grads may be NULL) */
+int ising_net_loss_grad(ising_net* net, const float* d_windows, const float* d_targets, int n, double* loss,
+                        float* host_grads);
+/* one Adam step on that loss */
+int ising_net_train_step(ising_net* net, const float* d_windows, const float* d_targets, int n, double lr,
+                         double* loss);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,14 +7,14 @@ there is no CPU fallback.
 """
 from . import _lib
 from ._lib import IsingError, Params, load
-from .api import (ChainMesh, Ensembles, ParallelTempering, bcc_unit_cell, calculate_heisenberg_energy,
+from .api import (ChainMesh, Ensembles, ParallelTempering, ProposalNet, bcc_unit_cell, calculate_heisenberg_energy,
                   calculate_winding_number2, calculate_winding_number_density, chain_mesh_statistics,
                   hyper_kagome_unit_cell, local_energy_batch, make_chain_mesh, metropolis_mcs, observables,
                   params, pt_file_tag, reference_params, sc_unit_cell, temperature_ladder,
                   total_heisenberg_energy, unit_cell, winding_all_slices, write_pt_data_csv,
                   write_spins_to_file, write_winding_number_density)
 
-__all__ = ["ChainMesh", "Ensembles", "ParallelTempering", "IsingError", "Params", "load", "bcc_unit_cell",
+__all__ = ["ChainMesh", "Ensembles", "ParallelTempering", "ProposalNet", "IsingError", "Params", "load", "bcc_unit_cell",
            "calculate_heisenberg_energy", "calculate_winding_number2", "calculate_winding_number_density",
            "chain_mesh_statistics", "hyper_kagome_unit_cell", "local_energy_batch", "make_chain_mesh",
            "metropolis_mcs", "observables", "params", "pt_file_tag", "reference_params", "sc_unit_cell",

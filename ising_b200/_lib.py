@@ -121,6 +121,14 @@ _SIGS = {
     "ising_ensembles_resync": (_i, [_vp]),
     "ising_ensembles_inject_stall": (_i, [_vp, _i]),
     "ising_bf16_gemm": (_i, [_vp, _i, _vp, _i, _i, _i, _i, _P(C.c_float), _P(C.c_float), _i, _vp, _i, _i, _vp]),
+    "ising_net_create": (_i, [_i, _i, _u64, _P(_vp)]),
+    "ising_net_destroy": (_i, [_vp]),
+    "ising_net_param_count": (_i, []),
+    "ising_net_set_params": (_i, [_vp, _P(C.c_float)]),
+    "ising_net_get_params": (_i, [_vp, _P(C.c_float)]),
+    "ising_net_forward": (_i, [_vp, _P(C.c_float), _i, _P(C.c_float)]),
+    "ising_net_loss_grad": (_i, [_vp, _P(C.c_float), _P(C.c_float), _i, _P(_d), _P(C.c_float)]),
+    "ising_net_train_step": (_i, [_vp, _P(C.c_float), _P(C.c_float), _i, _d, _P(_d)]),
     "ising_write_spins_csv": (_i, [_vp, _i, C.c_char_p, _i, _i, _i]),
     "ising_write_pt_data_csv": (_i, [C.c_char_p, _d, _d, _d, _d, _d, _i, _d, _P(_d)]),
     "ising_pt_file_tag": (_i, [C.c_char_p, C.c_size_t, _d, _d, _d, _d]),

@@ -485,3 +485,65 @@ class Ensembles:
     def inject_stall(self, e: int):
         """Test hook: the next run's rounds >= 1 of ensemble e wait for a flag nothing sets."""
         _lib.call("ising_ensembles_inject_stall", self._h, e)
+
+
+class ProposalNet:
+    """The learned patch proposal's network on one GPU (tensor-core forward, backward and
+    Adam).  Windows are float32 CUDA tensors [n, 3, 8, 8, 8]; outputs [n, 64, 4]."""
+
+    def __init__(self, device: int = 0, max_batch: int = 1024, seed: int = 1):
+        h = C.c_void_p()
+        _lib.call("ising_net_create", device, max_batch, seed, C.byref(h))
+        self._h = h
+        self.max_batch = max_batch
+        self.n_params = _lib.load().ising_net_param_count()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.load().ising_net_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.n_params, dtype=np.float32)
+        _lib.call("ising_net_get_params", self._h, out.ctypes.data_as(_P(C.c_float)))
+        return out
+
+    def set_params(self, flat):
+        a = np.ascontiguousarray(flat, dtype=np.float32)
+        assert a.size == self.n_params
+        _lib.call("ising_net_set_params", self._h, a.ctypes.data_as(_P(C.c_float)))
+
+    @staticmethod
+    def _fp(t):
+        return C.cast(t.data_ptr(), _P(C.c_float))
+
+    def forward(self, windows):
+        import torch
+        w = windows.contiguous()
+        out = torch.empty((w.shape[0], 64, 4), dtype=torch.float32, device=w.device)
+        _lib.call("ising_net_forward", self._h, self._fp(w), w.shape[0], self._fp(out))
+        return out
+
+    def loss_grad(self, windows, targets):
+        w, t = windows.contiguous(), targets.contiguous()
+        loss = C.c_double()
+        g = np.empty(self.n_params, dtype=np.float32)
+        _lib.call("ising_net_loss_grad", self._h, self._fp(w), self._fp(t), w.shape[0], C.byref(loss),
+                  g.ctypes.data_as(_P(C.c_float)))
+        return loss.value, g
+
+    def train_step(self, windows, targets, lr: float = 1e-3) -> float:
+        w, t = windows.contiguous(), targets.contiguous()
+        loss = C.c_double()
+        _lib.call("ising_net_train_step", self._h, self._fp(w), self._fp(t), w.shape[0], lr, C.byref(loss))
+        return loss.value

@@ -38,3 +38,71 @@ def test_tcgen05_gemm_matches_fp32_matmul(ib, cuda_ok, M, N, K):
     assert err <= 1e-4 * np.sqrt(K) * ref.abs().max().item() + 1e-4, err
     gel = torch.nn.functional.gelu(ref, approximate="tanh")
     assert (O.double() - gel).abs().max().item() <= 1e-2 * gel.abs().max().item() + 1e-2
+
+
+def _rand_windows(n, seed):
+    import torch
+    g = torch.Generator().manual_seed(seed)
+    w = torch.randn((n, 3, 8, 8, 8), generator=g, dtype=torch.float64)
+    w[:, 2] += 1.5                                   # partly ordered along +z
+    return w / w.norm(dim=1, keepdim=True)
+
+
+def _targets(windows, seed, amp=0.3):
+    import torch
+    from oracle import learned_ref as R
+    g = torch.Generator().manual_seed(seed)
+    s = R.patch_spins(windows)
+    om = amp * torch.randn(s.shape[:-1] + (2,), generator=g, dtype=torch.float64)
+    return R.exp_map(s, om)
+
+
+def test_network_forward_matches_oracle(ib, cuda_ok):
+    import torch
+    from oracle import learned_ref as R
+    net = ib.ProposalNet(max_batch=8, seed=3)
+    p = R.unflatten(net.get_params())
+    p["bh"][:3] = torch.tensor([0.1, -0.2, 0.05], dtype=torch.float64)
+    net.set_params(R.flatten(p).numpy())
+    w = _rand_windows(6, 1)
+    out = net.forward(w.float().cuda()).double().cpu()
+    # the oracle sees the same FP32-rounded windows and BF16 weights / activations
+    ref = R.forward(R.unflatten(net.get_params()), w.float().double(), round_bf16=True)
+    err = (out - ref).abs().max().item()
+    assert err <= 2e-2 * ref.abs().max().item() + 2e-3, err
+
+
+def test_network_gradients_match_oracle(ib, cuda_ok):
+    import torch
+    from oracle import learned_ref as R
+    net = ib.ProposalNet(max_batch=8, seed=5)
+    w = _rand_windows(8, 2)
+    t = _targets(w, 3)
+    loss, g = net.loss_grad(w.float().cuda(), t.float().cuda())
+    p = R.unflatten(net.get_params())
+    lref, gref = R.grads(p, w.float().double(), t.float().double(), round_bf16=True)
+    assert abs(loss - lref) <= 1e-2 * abs(lref) + 1e-3, (loss, lref)
+    G = R.unflatten(g)
+    for name, _ in R.PARAM_SHAPES:
+        a, b = G[name].reshape(-1), gref[name].reshape(-1)
+        rel = (a - b).norm() / b.norm().clamp_min(1e-12)
+        assert rel < 5e-2, (name, float(rel))
+
+
+def test_training_reduces_the_loss(ib, cuda_ok):
+    import torch
+    from oracle import learned_ref as R
+    net = ib.ProposalNet(max_batch=64, seed=7)
+    w = _rand_windows(64, 4)
+    s = R.patch_spins(w)
+    # a learnable target: rotate every patch spin by 0.4 rad toward +z in its tangent frame
+    e1, e2 = R.frame(s)
+    ez = torch.tensor([0.0, 0.0, 1.0], dtype=torch.float64)
+    om = torch.stack([(ez * e1).sum(-1), (ez * e2).sum(-1)], -1)
+    om = 0.4 * om / om.norm(dim=-1, keepdim=True).clamp_min(1e-9)
+    t = R.exp_map(s, om)
+    wc, tc = w.float().cuda(), t.float().cuda()
+    l0 = net.train_step(wc, tc, lr=3e-3)
+    for _ in range(150):
+        l1 = net.train_step(wc, tc, lr=3e-3)
+    assert np.isfinite(l1) and l1 < l0 - 1.0, (l0, l1)
