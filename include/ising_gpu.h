@@ -354,6 +354,26 @@ int ising_net_loss_grad(ising_net* net, const float* d_windows, const float* d_t
 int ising_net_train_step(ising_net* net, const float* d_windows, const float* d_targets, int n, double lr,
                          double* loss);
 
+/* The learned patch move on a PT object (simple-cubic mesh, nx, ny, nz divisible by 8; no
+ * reference counterpart): one class `colour` (0..7) of the 2x2x2 colouring of 4^3 blocks,
+ * shifted by (offx, offy, offz), on the replicas holding temperature slots 0..slots-1
+ * (slots = 0: all).  Each patch gets a network proposal and an exact Metropolis-Hastings
+ * accept; the running FP64 energies and magnetisations follow the accepted patches. */
+int ising_pt_patch_step(ising_pt* pt, ising_net* net, int colour, int offx, int offy, int offz, int slots);
+/* windows per patch step (slots x (nx/8)(ny/8)(nz/8)) */
+int ising_pt_patch_count(const ising_pt* pt, int slots, int64_t* n_windows);
+/* Training samples from the current PT state: the windows of one colour class (device
+ * [n][3][8][8][8]) and, as targets (device [n][64][3]), their patches after n_local
+ * Metropolis sweeps of the patch with the halo fixed at the replica's temperature. */
+int ising_pt_patch_samples(ising_pt* pt, int colour, int offx, int offy, int offz, int slots, int n_local,
+                           float* d_windows, float* d_targets);
+/* Inspection of the last patch step's first n windows (its first batch): windows x and x'
+ * ([n][3][8][8][8]), log q(x'|x) per window, and, for the first n windows of the step, the
+ * energy change and the accept flag.  Any pointer may be NULL. */
+int ising_pt_patch_last(const ising_pt* pt, int n, float* win, float* winp, double* lqf, double* dE, int* accepted);
+/* patch moves proposed and accepted per temperature slot since creation */
+int ising_pt_patch_stats(const ising_pt* pt, uint64_t* proposed, uint64_t* accepted);
+
 #ifdef __cplusplus
 }
 #endif

@@ -388,6 +388,33 @@ class ParallelTempering:
                   acc.ctypes.data_as(_P(C.c_uint64)))
         return att[: self.n - 1], acc[: self.n - 1]
 
+    # learned patch move ------------------------------------------------------
+    def patch_step(self, net: "ProposalNet", colour: int, offset=(0, 0, 0), slots: int = 0):
+        """One class of the 2x2x2 colouring of 4^3 blocks, shifted by offset, on the
+        replicas holding temperature slots 0..slots-1 (0: all)."""
+        _lib.call("ising_pt_patch_step", self._h, net.handle, colour, offset[0], offset[1], offset[2], slots)
+
+    def patch_count(self, slots: int = 0) -> int:
+        n = C.c_int64()
+        _lib.call("ising_pt_patch_count", self._h, slots, C.byref(n))
+        return n.value
+
+    def patch_samples(self, colour: int, offset=(0, 0, 0), slots: int = 0, n_local: int = 20):
+        """(windows [n,3,8,8,8], targets [n,64,3]) as float32 CUDA tensors."""
+        import torch
+        n = self.patch_count(slots)
+        w = torch.empty((n, 3, 8, 8, 8), dtype=torch.float32, device="cuda")
+        t = torch.empty((n, 64, 3), dtype=torch.float32, device="cuda")
+        fp = lambda x: C.cast(x.data_ptr(), _P(C.c_float))
+        _lib.call("ising_pt_patch_samples", self._h, colour, offset[0], offset[1], offset[2], slots, n_local, fp(w), fp(t))
+        return w, t
+
+    def patch_stats(self):
+        p = np.zeros(self.n, dtype=np.uint64)
+        a = np.zeros(self.n, dtype=np.uint64)
+        _lib.call("ising_pt_patch_stats", self._h, p.ctypes.data_as(_P(C.c_uint64)), a.ctypes.data_as(_P(C.c_uint64)))
+        return p, a
+
     def series(self) -> np.ndarray:
         """(n_temps, n_recorded, 4): E, |M|, Q_mid, Q_mean per recorded sweep."""
         cap = self.opt.record_capacity

@@ -9,6 +9,7 @@
 
 #include "internal.h"
 #include "ensembles.h"
+#include "learned.h"
 
 // ======================================================================= errors
 namespace isg {
@@ -849,6 +850,14 @@ struct ising_pt {
     cudaGraphExec_t graph = nullptr;
     int graph_k = -1;
     int rounds_done = 0;
+    // learned patch move workspace (allocated by the first patch call)
+    float *pw_win = nullptr, *pw_winp = nullptr, *pw_prop = nullptr;
+    double *pw_lqf = nullptr, *pw_dE = nullptr, *pw_dM = nullptr;
+    int *pw_rej = nullptr, *pw_acc = nullptr;
+    unsigned long long* pw_stats = nullptr;
+    int pw_batch = 0;
+    int64_t pw_windows = 0;
+    uint32_t patch_round = 0;
 };
 
 namespace {
@@ -858,6 +867,8 @@ void pt_free(ising_pt* pt) {
     cudaFree(pt->d_acc); cudaFree(pt->d_partials); cudaFree(pt->d_stats); cudaFree(pt->d_round);
     cudaFree(pt->d_series); cudaFree(pt->d_count); cudaFree(pt->d_q); cudaFree(pt->d_energy_tmp);
     cudaFree(pt->d_energy_out); cudaFree(pt->d_plan_slots); cudaFree(pt->d_plan_count);
+    cudaFree(pt->pw_win); cudaFree(pt->pw_winp); cudaFree(pt->pw_prop); cudaFree(pt->pw_lqf); cudaFree(pt->pw_dE);
+    cudaFree(pt->pw_dM); cudaFree(pt->pw_rej); cudaFree(pt->pw_acc); cudaFree(pt->pw_stats);
 }
 
 int pt_resync_enqueue(ising_pt* pt) {
@@ -1082,6 +1093,148 @@ extern "C" int ising_pt_series(const ising_pt* pt, double* out, int* n_rec) {
 }
 
 // ======================================================================= helpers for noalloc.cu
+
+// ======================================================================= learned patch move
+namespace {
+
+int patch_setup(ising_pt* pt, int colour, int offx, int offy, int offz, int slots, PatchStep* P, int* n_slots) {
+    ising_mesh* m = pt->mesh;
+    const Lattice& L = m->lat;
+    if (!pt->plan.sc || L.nsub != 1) return fail(ISING_ERR_UNSUPPORTED, "the patch move needs a simple-cubic mesh with shell-1 couplings");
+    if (L.nx % 8 || L.ny % 8 || L.nz % 8) return fail(ISING_ERR_ARG, "the patch move needs nx, ny, nz divisible by 8");
+    if (colour < 0 || colour > 7) return fail(ISING_ERR_ARG, "colour must be 0..7");
+    if (offx < 0 || offx > 7 || offy < 0 || offy > 7 || offz < 0 || offz > 7) return fail(ISING_ERR_ARG, "offsets must be 0..7");
+    if (slots < 0 || slots > pt->n) return fail(ISING_ERR_ARG, "slots must be 0..n_temps");
+    *n_slots = slots ? slots : pt->n;
+    PatchStep& Q = *P;
+    Q = PatchStep{};
+    Q.spins = m->d_spins; Q.natoms = L.natoms; Q.nx = L.nx; Q.ny = L.ny; Q.nz = L.nz; Q.layout = m->layout;
+    Q.colour = colour; Q.offx = offx; Q.offy = offy; Q.offz = offz;
+    Q.per_slot = (L.nx / 8) * (L.ny / 8) * (L.nz / 8);
+    Q.t2r = pt->d_t2r; Q.beta_rep = pt->d_beta_rep; Q.ham = pt->plan.ham;
+    Q.seed = pt->opt.seed; Q.ensemble = pt->opt.ensemble; Q.status = m->d_status;
+    return ISING_OK;
+}
+
+int patch_workspace(ising_pt* pt, int batch) {
+    ising_mesh* m = pt->mesh;
+    const int64_t windows = (int64_t)pt->n * (m->lat.nx / 8) * (m->lat.ny / 8) * (m->lat.nz / 8);
+    if (pt->pw_batch >= batch && pt->pw_windows >= windows) return ISING_OK;
+    cudaFree(pt->pw_win); cudaFree(pt->pw_winp); cudaFree(pt->pw_prop); cudaFree(pt->pw_lqf); cudaFree(pt->pw_dE);
+    cudaFree(pt->pw_dM); cudaFree(pt->pw_rej); cudaFree(pt->pw_acc);
+    pt->pw_win = pt->pw_winp = pt->pw_prop = nullptr;
+    pt->pw_lqf = pt->pw_dE = pt->pw_dM = nullptr;
+    pt->pw_rej = pt->pw_acc = nullptr;
+    pt->pw_batch = 0;
+    pt->pw_windows = 0;
+    ISG_TRY(dev_alloc(&pt->pw_win, (size_t)batch * 1536));
+    ISG_TRY(dev_alloc(&pt->pw_winp, (size_t)batch * 1536));
+    ISG_TRY(dev_alloc(&pt->pw_prop, (size_t)batch * 192));
+    ISG_TRY(dev_alloc(&pt->pw_lqf, batch));
+    ISG_TRY(dev_alloc(&pt->pw_rej, batch));
+    ISG_TRY(dev_alloc(&pt->pw_dE, windows));
+    ISG_TRY(dev_alloc(&pt->pw_dM, 3 * windows));
+    ISG_TRY(dev_alloc(&pt->pw_acc, windows));
+    if (!pt->pw_stats) {
+        ISG_TRY(dev_alloc(&pt->pw_stats, 2 * (size_t)pt->n));
+        ISG_CUDA(cudaMemset(pt->pw_stats, 0, 2 * (size_t)pt->n * sizeof(unsigned long long)));
+    }
+    pt->pw_batch = batch;
+    pt->pw_windows = windows;
+    return ISING_OK;
+}
+
+}  // namespace
+
+extern "C" int ising_pt_patch_count(const ising_pt* pt, int slots, int64_t* n_windows) {
+    if (!pt || !n_windows) return fail(ISING_ERR_ARG, "NULL argument");
+    const Lattice& L = pt->mesh->lat;
+    if (slots < 0 || slots > pt->n) return fail(ISING_ERR_ARG, "slots must be 0..n_temps");
+    *n_windows = (int64_t)(slots ? slots : pt->n) * (L.nx / 8) * (L.ny / 8) * (L.nz / 8);
+    return ISING_OK;
+}
+
+extern "C" int ising_pt_patch_step(ising_pt* pt, ising_net* net, int colour, int offx, int offy, int offz, int slots) {
+    if (!pt || !net) return fail(ISING_ERR_ARG, "NULL argument");
+    ising_mesh* m = pt->mesh;
+    if (net_device(net) != m->device) return fail(ISING_ERR_ARG, "network and mesh are on different devices");
+    DeviceGuard g(m->device);
+    PatchStep P;
+    int ns = 0;
+    ISG_TRY(patch_setup(pt, colour, offx, offy, offz, slots, &P, &ns));
+    const int batch = net_max_batch(net);
+    ISG_TRY(patch_workspace(pt, batch));
+    P.round = pt->patch_round++;
+    const int64_t total = (int64_t)ns * P.per_slot;
+    cudaStream_t s = m->stream;
+    for (int64_t w0 = 0; w0 < total; w0 += batch) {
+        const int nb = (int)std::min<int64_t>(batch, total - w0);
+        const float* out = nullptr;
+        ISG_TRY(launch_patch_gather(P, w0, nb, nullptr, pt->pw_win, s));
+        ISG_TRY(net_forward_on(net, pt->pw_win, nb, s, &out));
+        ISG_TRY(launch_patch_propose(P, w0, nb, pt->pw_win, out, pt->pw_prop, pt->pw_lqf, pt->pw_rej, s));
+        ISG_TRY(launch_patch_gather(P, w0, nb, pt->pw_prop, pt->pw_winp, s));
+        ISG_TRY(net_forward_on(net, pt->pw_winp, nb, s, &out));
+        ISG_TRY(launch_patch_accept(P, w0, nb, pt->pw_win, pt->pw_winp, out, pt->pw_prop, pt->pw_lqf, pt->pw_rej,
+                                    pt->pw_dE, pt->pw_dM, pt->pw_acc, s));
+    }
+    ISG_TRY(launch_patch_fold(P, ns, total, pt->pw_dE, pt->pw_dM, pt->pw_acc, pt->d_acc, pt->pw_stats, s));
+    ISG_TRY(net_status_on(net, s));
+    return check_status(m);
+}
+
+extern "C" int ising_pt_patch_samples(ising_pt* pt, int colour, int offx, int offy, int offz, int slots, int n_local,
+                                      float* d_windows, float* d_targets) {
+    if (!pt || !d_windows || !d_targets) return fail(ISING_ERR_ARG, "NULL argument");
+    if (n_local < 0) return fail(ISING_ERR_ARG, "n_local must be >= 0");
+    ising_mesh* m = pt->mesh;
+    DeviceGuard g(m->device);
+    PatchStep P;
+    int ns = 0;
+    ISG_TRY(patch_setup(pt, colour, offx, offy, offz, slots, &P, &ns));
+    P.round = pt->patch_round++;
+    const int64_t total = (int64_t)ns * P.per_slot;
+    const int chunk = 1 << 16;
+    for (int64_t w0 = 0; w0 < total; w0 += chunk) {
+        const int nb = (int)std::min<int64_t>(chunk, total - w0);
+        ISG_TRY(launch_patch_gather(P, w0, nb, nullptr, d_windows + w0 * 1536, m->stream));
+        ISG_TRY(launch_patch_equilibrate(P, w0, nb, d_windows + w0 * 1536, n_local, pt->opt.move, (float)pt->opt.r,
+                                         d_targets + w0 * 192, m->stream));
+    }
+    return check_status(m);
+}
+
+extern "C" int ising_pt_patch_last(const ising_pt* pt, int n, float* win, float* winp, double* lqf, double* dE,
+                                   int* accepted) {
+    if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
+    if (n < 0 || n > pt->pw_batch || n > pt->pw_windows) return fail(ISING_ERR_ARG, "n exceeds the last patch batch");
+    DeviceGuard g(pt->mesh->device);
+    cudaStream_t s = pt->mesh->stream;
+    if (win) ISG_CUDA(cudaMemcpyAsync(win, pt->pw_win, (size_t)n * 1536 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (winp) ISG_CUDA(cudaMemcpyAsync(winp, pt->pw_winp, (size_t)n * 1536 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (lqf) ISG_CUDA(cudaMemcpyAsync(lqf, pt->pw_lqf, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (dE) ISG_CUDA(cudaMemcpyAsync(dE, pt->pw_dE, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (accepted) ISG_CUDA(cudaMemcpyAsync(accepted, pt->pw_acc, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, s));
+    ISG_CUDA(cudaStreamSynchronize(s));
+    return ISING_OK;
+}
+
+extern "C" int ising_pt_patch_stats(const ising_pt* pt, uint64_t* proposed, uint64_t* accepted) {
+    if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
+    DeviceGuard g(pt->mesh->device);
+    std::vector<unsigned long long> h(2 * (size_t)pt->n, 0ull);
+    if (pt->pw_stats) {
+        ISG_CUDA(cudaMemcpyAsync(h.data(), pt->pw_stats, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 pt->mesh->stream));
+        ISG_CUDA(cudaStreamSynchronize(pt->mesh->stream));
+    }
+    for (int t = 0; t < pt->n; ++t) {
+        if (proposed) proposed[t] = h[2 * t];
+        if (accepted) accepted[t] = h[2 * t + 1];
+    }
+    return ISING_OK;
+}
+
 // ======================================================================= batched ensembles
 namespace {
 

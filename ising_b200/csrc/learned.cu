@@ -518,3 +518,30 @@ extern "C" int ising_net_train_step(ising_net* n, const float* d_windows, const 
     if (loss) *loss = l / (double)((int64_t)nb * 64);
     return ISING_OK;
 }
+
+namespace isg {
+
+int net_forward_on(ising_net* n, const float* d_windows, int nb, cudaStream_t s, const float** out) {
+    if (nb < 1 || nb > n->max_batch) return fail(ISING_ERR_ARG, "window batch exceeds the network's max_batch");
+    cudaStream_t keep = n->stream;
+    n->stream = s;
+    k_windows_to_rows<<<grid_for((int64_t)nb * 1536), 256, 0, s>>>(d_windows, nb, n->X0);
+    const int st = net_forward_rows(n, nb);
+    n->stream = keep;
+    *out = n->out;
+    return st;
+}
+int net_max_batch(const ising_net* n) { return n->max_batch; }
+int net_status_on(ising_net* n, cudaStream_t s) {
+    int h = 0;
+    ISG_CUDA(cudaMemcpyAsync(&h, n->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ISG_CUDA(cudaStreamSynchronize(s));
+    if (h) {
+        cudaMemsetAsync(n->status, 0, sizeof(int), s);
+        return fail(h & kStatTimeout ? ISING_ERR_TIMEOUT : ISING_ERR_NAN, "proposal network failed on the device");
+    }
+    return ISING_OK;
+}
+int net_device(const ising_net* n) { return n->device; }
+
+}  // namespace isg

@@ -7,6 +7,8 @@
 
 #include "internal.h"
 
+struct ising_net;
+
 namespace isg {
 
 // C/O[M x N] = epilogue(A[M x K] * B[N x K]^T + bias)
@@ -27,5 +29,40 @@ struct GemmArgs {
     uint32_t tmem_cols;     // set by the launcher
 };
 int launch_gemm_bf16(GemmArgs g, cudaStream_t s);
+
+// forward of nb windows ([nb][3][8][8][8] FP32, device) on stream s; *out = [nb*64][4]
+int net_forward_on(ising_net* n, const float* d_windows, int nb, cudaStream_t s, const float** out);
+int net_max_batch(const ising_net* n);
+int net_device(const ising_net* n);
+// reads and clears the network status word after the work queued on s (synchronises s)
+int net_status_on(ising_net* n, cudaStream_t s);
+
+// One class of the 2x2x2 colouring of 4^3 blocks (shifted by (offx, offy, offz)) on the
+// replicas that hold temperature slots 0..n_slots-1: window w belongs to slot w / per_slot.
+struct PatchStep {
+    float* spins;
+    int64_t natoms;
+    int nx, ny, nz;
+    Layout layout;
+    int colour, offx, offy, offz;
+    int per_slot;
+    const int* t2r;            // slot -> replica
+    const double* beta_rep;
+    HamDev ham;
+    uint64_t seed;
+    uint32_t ensemble;
+    uint32_t round;
+    int* status;
+};
+int launch_patch_gather(const PatchStep& P, int64_t w0, int nb, const float* prop, float* win, cudaStream_t s);
+int launch_patch_propose(const PatchStep& P, int64_t w0, int nb, const float* win, const float* out, float* prop,
+                         double* lqf, int* rej, cudaStream_t s);
+int launch_patch_accept(const PatchStep& P, int64_t w0, int nb, const float* win, const float* winp, const float* outp,
+                        const float* prop, const double* lqf, const int* rej, double* dE, double* dM, int* acc,
+                        cudaStream_t s);
+int launch_patch_fold(const PatchStep& P, int n_slots, int64_t n_windows, const double* dE, const double* dM,
+                      const int* accepted, Acc4* acc, unsigned long long* stats, cudaStream_t s);
+int launch_patch_equilibrate(const PatchStep& P, int64_t w0, int nb, const float* win, int n_local, int move, float r,
+                             float* tgt, cudaStream_t s);
 
 }  // namespace isg

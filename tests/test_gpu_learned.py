@@ -106,3 +106,129 @@ def test_training_reduces_the_loss(ib, cuda_ok):
     for _ in range(150):
         l1 = net.train_step(wc, tc, lr=3e-3)
     assert np.isfinite(l1) and l1 < l0 - 1.0, (l0, l1)
+
+
+# ---------------------------------------------------------------- the patch move
+def _pt_setup(ib, L=8, betas=(0.1, 0.3, 1.0, 3.0), J=-1.0, D=0.5, B=0.25, K=0.0, seed=11, record=0):
+    m = ib.ChainMesh.simple_cubic(L, n_replicas=len(betas))
+    m.init_uniform(seed, 0)
+    p = ib.params(J=J, Dz=D, B=B, K=K, dmi="bulk", include_Jp=False)
+    pt = ib.ParallelTempering(m, np.array(betas), p, seed=seed, ensemble=0, record=bool(record), record_capacity=record)
+    return m, p, pt
+
+
+def _window(spins, L, origin):
+    """[3, 8, 8, 8] window of a (3, L^3) spin array (reference atom order, z fastest)."""
+    S = spins.reshape(3, L, L, L)
+    idx = [(np.arange(8) + o - 2) % L for o in origin]
+    return S[:, idx[0]][:, :, idx[1]][:, :, :, idx[2]]
+
+
+def test_patch_move_matches_oracle(ib, cuda_ok):
+    import torch
+    from oracle import learned_ref as R
+    L, betas = 8, (0.1, 0.3, 1.0, 3.0)
+    m, p, pt = _pt_setup(ib, L, betas)
+    net = ib.ProposalNet(max_batch=16, seed=9)
+    params = R.unflatten(net.get_params())
+    colour, off = 5, (1, 2, 3)
+    t2r = pt.permutation()
+    pre = [m.get_spins(r).T.copy() for r in range(len(betas))]          # (3, N)
+    pt.patch_step(net, colour, off)
+    post = [m.get_spins(r).T.copy() for r in range(len(betas))]
+    n = len(betas)
+    win = np.empty((n, 3, 8, 8, 8), np.float32)
+    winp = np.empty((n, 3, 8, 8, 8), np.float32)
+    lqf = np.empty(n)
+    dE = np.empty(n)
+    acc = np.empty(n, np.int32)
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    ib._lib.call("ising_pt_patch_last", pt._h, n, fp(win), fp(winp), dp(lqf), dp(dE), acc.ctypes.data_as(C.POINTER(C.c_int)))
+    origin = ((4 * (colour & 1) + off[0]) % L, (4 * ((colour >> 1) & 1) + off[1]) % L, (4 * ((colour >> 2) & 1) + off[2]) % L)
+    n_acc = 0
+    for t in range(n):
+        r = t2r[t]
+        x = torch.tensor(win[t], dtype=torch.float64)
+        xp = torch.tensor(winp[t], dtype=torch.float64)
+        np.testing.assert_array_equal(win[t], _window(pre[r], L, origin).astype(np.float32))
+        halo = np.ones((8, 8, 8), bool)
+        halo[2:6, 2:6, 2:6] = False
+        np.testing.assert_array_equal(winp[t][:, halo], win[t][:, halo])
+        s, sp = R.patch_spins(x), R.patch_spins(xp)
+        assert torch.allclose(sp.norm(dim=-1), torch.ones(64, dtype=torch.float64), atol=1e-5)
+        out = R.forward(params, x[None], round_bf16=True)[0]
+        outp = R.forward(params, xp[None], round_bf16=True)[0]
+        om, th = R.log_map(s, sp)
+        ls = out[:, 3].clamp(-6.0, 1.5)
+        eps = (om - R.tangent_mean(out, s)) / torch.exp(ls)[:, None]
+        lq_f = float((-0.5 * (eps * eps).sum(-1) - 2.0 * ls + R.log_jac(th)).sum())
+        outp_c = outp.clone()
+        outp_c[:, 3] = outp_c[:, 3].clamp(-6.0, 1.5)
+        lq_r = float(R.log_q_reverse(outp_c, sp, s)) + 64 * np.log(2 * np.pi)
+        de = float(R.patch_energy(xp, -1.0, 0.5, 0.25) - R.patch_energy(x, -1.0, 0.5, 0.25))
+        assert abs(lq_f - lqf[t]) < 0.5, (lq_f, lqf[t])
+        assert abs(de - dE[t]) < 1e-3 * max(1.0, abs(de)) or not acc[t], (de, dE[t])
+        la = -betas[t] * de + lq_r - lq_f
+        if la > 3.0 and float(th.max()) < np.pi - 1e-3:
+            assert acc[t] == 1, (t, la)
+        if la < -30.0:
+            assert acc[t] == 0, (t, la)
+        # spins after the step: the patch is x' when accepted, x otherwise; nothing else moved
+        expect = pre[r].copy().reshape(3, L, L, L)
+        if acc[t]:
+            n_acc += 1
+            idx = [(np.arange(2, 6) + o - 2) % L for o in origin]
+            expect[np.ix_(range(3), idx[0], idx[1], idx[2])] = winp[t][:, 2:6, 2:6, 2:6]
+        np.testing.assert_allclose(post[r].reshape(3, L, L, L), expect, atol=0, rtol=0)
+    proposed, accepted = pt.patch_stats()
+    assert proposed.sum() == n and accepted.sum() == n_acc
+
+
+def test_patch_steps_keep_the_running_energies(ib, cuda_ok):
+    m, p, pt = _pt_setup(ib, 16, (0.2, 0.5, 1.0), K=0.05)
+    net = ib.ProposalNet(max_batch=64, seed=2)
+    rng = np.random.default_rng(0)
+    for i in range(12):
+        pt.run(1, 1)
+        pt.patch_step(net, i % 8, tuple(int(v) for v in rng.integers(0, 4, 3)))
+    e_run, m_run = pt.energies()
+    pt.resync()
+    e_new, m_new = pt.energies()
+    assert np.max(np.abs(e_run - e_new)) < 1e-6 * 16 ** 3
+    assert np.max(np.abs(m_run - m_new)) < 1e-6 * 16 ** 3
+    assert pt.patch_stats()[0].sum() == 12 * 3 * 8
+
+
+def test_patch_samples(ib, cuda_ok):
+    import torch
+    m, p, pt = _pt_setup(ib, 8, (0.5, 2.0))
+    w, t = pt.patch_samples(2, (0, 1, 2), n_local=0)
+    assert w.shape == (2, 3, 8, 8, 8) and t.shape == (2, 64, 3)
+    from oracle import learned_ref as R
+    np.testing.assert_array_equal(R.patch_spins(w.double().cpu()).numpy(), t.double().cpu().numpy())
+    w2, t2 = pt.patch_samples(2, (0, 1, 2), n_local=30)
+    np.testing.assert_array_equal(w2.cpu().numpy(), w.cpu().numpy())        # the state is not changed
+    assert torch.allclose(t2.norm(dim=-1), torch.ones_like(t2[..., 0]), atol=1e-5)
+    assert (t2 - t).abs().max().item() > 0.1
+
+
+def test_patch_moves_leave_the_energy_distribution_unchanged(ib, cuda_ok):
+    """Plain Metropolis vs Metropolis alternating with patch moves on a small lattice: the
+    mean energy agrees within four binning standard errors."""
+    from ising_b200.analysis import binning_error
+    means = []
+    for learned in (False, True):
+        m, p, pt = _pt_setup(ib, 8, (0.8,), D=0.3, B=0.1, seed=21 + learned, record=3000)
+        net = ib.ProposalNet(max_batch=16, seed=4)
+        rng = np.random.default_rng(1)
+        for i in range(3000):
+            pt.run(1, 1)
+            if learned:
+                pt.patch_step(net, int(rng.integers(0, 8)), tuple(int(v) for v in rng.integers(0, 8, 3)))
+        e = pt.series()[0, 500:, 0]
+        means.append((e.mean(), binning_error(e)))
+        if learned:
+            assert pt.patch_stats()[1].sum() > 0
+    (a, ea), (b, eb) = means
+    assert abs(a - b) < 4.0 * np.hypot(ea, eb), means
