@@ -373,6 +373,164 @@ def run_gpu(args, w):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- C5: learned vs plain
+def run_c5(args, w):
+    """Learned patch proposal against plain Metropolis on the C5 ensemble (SC L=96, 48 PT
+    replicas): train the network on PT windows, then run both samplers from the same
+    equilibrated chain with the same exchange schedule (one exchange per sweep) and compare
+    the topological charge's integrated autocorrelation time and effective samples per
+    second, and the observables per temperature slot (within 2 binning standard errors)."""
+    import numpy as np
+    import torch
+
+    import ising_b200 as ib
+    from ising_b200 import _lib
+    from ising_b200 import analysis as A
+
+    L, R, k = w["L"], w["R"], 1
+    N = L ** 3
+    n_plain, n_learned = args.c5_plain, args.c5_learned
+    stream = torch.cuda.current_stream()
+    mesh = ib.ChainMesh.simple_cubic(L, n_replicas=R)
+    mesh.set_stream(stream.cuda_stream)
+    mesh.init_uniform(0x15196, ensemble=0)
+    p = ib.params(J=w["J"], Dz=w["D"], B=w["B"], K=w["K"], dmi="bulk", include_Jp=False)
+    betas = 1.0 / ib.temperature_ladder(w["tmin"], w["tmax"], R)
+    pt = ib.ParallelTempering(mesh, betas, p, seed=0x15196, ensemble=0, move=_lib.MOVE_BALL, r=w["r"],
+                              record=True, record_capacity=n_plain + n_learned + 8)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        t0 = time.perf_counter()
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3) / 1e3
+
+    pt.relax(args.c5_therm)
+    # kernel-level plain throughput (sweeps without exchange or recording)
+    t_relax = timed(lambda: pt.relax(40))
+    value = 40 * R * N / t_relax
+    rng = np.random.default_rng(7)
+    net = ib.ProposalNet(max_batch=args.c5_batch, seed=1)
+
+    def jump_stats(steps=8):
+        """per slot: acceptance and squared spin displacement per site per proposal (ESJD)
+        over `steps` patch steps at the current step scales"""
+        p0, a0 = pt.patch_stats()
+        j0 = pt.patch_jump()
+        for i in range(steps):
+            pt.patch_step(net, i % 8, tuple(int(v) for v in rng.integers(0, 8, 3)))
+        p1, a1 = pt.patch_stats()
+        j1 = pt.patch_jump()
+        n = np.maximum(p1 - p0, 1).astype(float)
+        return (a1 - a0) / n, (j1 - j0) / n / 64.0
+
+    # the network as initialised (mu ~ 0, sigma = 0.3 everywhere) with its own tuned step scale
+    scale_untrained = pt.patch_tune_scale(net, target=0.25, iters=args.c5_tune, seed=1, drift=1.0)
+    acc_untrained, esjd_untrained = jump_stats()
+    # training set: windows of plain-PT states, targets from local equilibration of the patch
+    ws, ts = [], []
+    n_have = 0
+    while n_have < args.c5_train:
+        pt.relax(20)
+        wi, ti = pt.patch_samples(int(rng.integers(0, 8)), tuple(int(v) for v in rng.integers(0, 8, 3)),
+                                  n_local=args.c5_nlocal)
+        ws.append(wi)
+        ts.append(ti)
+        n_have += wi.shape[0]
+    W = torch.cat(ws)[: args.c5_train]
+    T = torch.cat(ts)[: args.c5_train]
+    del ws, ts
+    losses = []
+
+    def train():
+        bs = 512
+        for ep in range(args.c5_epochs):
+            perm = torch.randperm(W.shape[0], device=W.device)
+            for b0 in range(0, W.shape[0] - bs + 1, bs):
+                j = perm[b0:b0 + bs]
+                losses.append(net.train_step(W[j], T[j], lr=1e-3))
+
+    t_train = timed(train)
+    # the trained network at three drift weights, each with its own tuned step scale; the
+    # measurement run uses the one with the largest mean ESJD
+    trained = {}
+    for lam in (0.0, 0.25, 1.0):
+        sc = pt.patch_tune_scale(net, target=0.25, iters=args.c5_tune, seed=2, drift=lam)
+        acc, ej = jump_stats()
+        trained[lam] = (sc, acc, ej)
+    best_lam = max(trained, key=lambda l: float(np.mean(trained[l][2])))
+    scale_trained, acc_trained, esjd_trained = trained[best_lam]
+    pt.patch_set_scale(scale_trained, best_lam)
+    # measurement: plain, then learned (1:1 alternation), from the same chain
+    c0 = pt.series().shape[1]
+    t_plain = timed(lambda: pt.run(k, n_plain))
+    c1 = pt.series().shape[1]
+
+    def learned_run():
+        for i in range(n_learned):
+            pt.run(k, 1)
+            pt.patch_step(net, i % 8, tuple(int(v) for v in rng.integers(0, 8, 3)), slots=args.c5_slots)
+
+    t_learned = timed(learned_run)
+    ser = pt.series()
+    sp, sl = ser[:, c0:c1], ser[:, c1:]
+
+    def arm(x, secs):
+        out = []
+        for t in range(R):
+            q, e = x[t, :, 3], x[t, :, 0]
+            tq, te = A.tau_int(q), A.tau_int(e)
+            out.append({"tau_Q": tq, "tau_E": te, "ess_Q_per_s": len(q) / (2 * tq) / secs, "ess_E_per_s": len(e) / (2 * te) / secs})
+        return out
+
+    ap, al = arm(sp, t_plain), arm(sl, t_learned)
+    within = {}
+    for name, col in (("E", 0), ("absM", 1), ("Q", 3)):
+        ok = 0
+        for t in range(R):
+            a, b = sp[t, :, col], sl[t, :, col]
+            err = np.hypot(A.binning_error(a), A.binning_error(b))
+            ok += int(abs(a.mean() - b.mean()) <= 2 * err + 1e-12)
+        within[name] = ok
+    qp = float(np.mean([x["ess_Q_per_s"] for x in ap]))
+    ql = float(np.mean([x["ess_Q_per_s"] for x in al]))
+    line = {
+        "metric": "spin-updates/s", "value": value, "unit": "spin-updates/s", "n_gpus": 1, "steps": n_plain,
+        "warmup": args.c5_therm, "ms_per_step": 1e3 * t_plain / n_plain, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (uniform random initial spins from Philox, seed 0x15196)",
+        "config": {"workload": "c5", "desc": w["desc"], "L": L, "replicas": R, "exchange_every": 1,
+                   "patch_slots": args.c5_slots or R, "train_windows": int(W.shape[0]), "epochs": args.c5_epochs},
+        "q_ess": {"metric": "Q-ESS/s (mean over temperature slots)", "plain": qp, "learned": ql,
+                  "learned_over_plain": ql / qp if qp > 0 else None,
+                  "plain_sweeps": n_plain, "learned_steps": n_learned,
+                  "plain_s": t_plain, "learned_s": t_learned,
+                  "tau_Q_plain": [round(x["tau_Q"], 2) for x in ap], "tau_Q_learned": [round(x["tau_Q"], 2) for x in al],
+                  "E_ess_per_s": {"plain": float(np.mean([x["ess_E_per_s"] for x in ap])),
+                                  "learned": float(np.mean([x["ess_E_per_s"] for x in al]))},
+                  "slots_within_2sigma": within, "slots": R},
+        "training": {"seconds": t_train, "steps": len(losses), "loss_first": losses[0] if losses else None,
+                     "loss_last": losses[-1] if losses else None,
+                     "untrained": {"step_scale": [round(float(x), 4) for x in scale_untrained],
+                                   "acceptance": [round(float(x), 4) for x in acc_untrained],
+                                   "esjd_per_site": [float("%.3g" % x) for x in esjd_untrained]},
+                     "trained": {str(l): {"step_scale": [round(float(x), 4) for x in v[0]],
+                                          "acceptance": [round(float(x), 4) for x in v[1]],
+                                          "esjd_per_site": [float("%.3g" % x) for x in v[2]],
+                                          "esjd_mean": float(np.mean(v[2]))} for l, v in trained.items()},
+                     "drift_used": best_lam, "n_local": args.c5_nlocal,
+                     "esjd_trained_over_untrained_mean": float(np.mean(esjd_trained) / max(np.mean(esjd_untrained), 1e-30))},
+        "roofline": None, "e2e": None, "cpu_baseline": None, "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+    net.close()
+    pt.close()
+    mesh.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -385,11 +543,23 @@ def main():
     ap.add_argument("--engine", default="ensembles", choices=["ensembles", "pt"])
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--learned", action="store_true", help="c5: learned patch proposal vs plain Metropolis")
+    ap.add_argument("--c5-plain", type=int, default=3000)
+    ap.add_argument("--c5-learned", type=int, default=600)
+    ap.add_argument("--c5-therm", type=int, default=5000)
+    ap.add_argument("--c5-tune", type=int, default=10)
+    ap.add_argument("--c5-nlocal", type=int, default=20)
+    ap.add_argument("--c5-train", type=int, default=100000)
+    ap.add_argument("--c5-epochs", type=int, default=3)
+    ap.add_argument("--c5-batch", type=int, default=8192)
+    ap.add_argument("--c5-slots", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, w)
+    elif args.learned:
+        run_c5(args, WORKLOADS["c5"])
     else:
         run_gpu(args, w)
 

@@ -360,6 +360,10 @@ int ising_net_train_step(ising_net* net, const float* d_windows, const float* d_
  * (slots = 0: all).  Each patch gets a network proposal and an exact Metropolis-Hastings
  * accept; the running FP64 energies and magnetisations follow the accepted patches. */
 int ising_pt_patch_step(ising_pt* pt, ising_net* net, int colour, int offx, int offy, int offz, int slots);
+/* Per-slot step scale a and drift weight l of the patch move: the tangent move becomes
+ * a * (l P_s(mu) + sigma eps), still an exact MH proposal.  scale_per_slot holds n_temps
+ * positive values, or NULL for a = 1; l = 1 uses the mean rotation as predicted. */
+int ising_pt_patch_set_scale(ising_pt* pt, const float* scale_per_slot, float drift);
 /* windows per patch step (slots x (nx/8)(ny/8)(nz/8)) */
 int ising_pt_patch_count(const ising_pt* pt, int slots, int64_t* n_windows);
 /* Training samples from the current PT state: the windows of one colour class (device
@@ -371,6 +375,9 @@ int ising_pt_patch_samples(ising_pt* pt, int colour, int offx, int offy, int off
  * ([n][3][8][8][8]), log q(x'|x) per window, and, for the first n windows of the step, the
  * energy change and the accept flag.  Any pointer may be NULL. */
 int ising_pt_patch_last(const ising_pt* pt, int n, float* win, float* winp, double* lqf, double* dE, int* accepted);
+/* per temperature slot: sum over accepted patch moves of sum_i |s_i' - s_i|^2 since creation
+ * (the expected squared jump distance is this over the proposals) */
+int ising_pt_patch_jump(const ising_pt* pt, double* sq_jump_per_slot);
 /* patch moves proposed and accepted per temperature slot since creation */
 int ising_pt_patch_stats(const ising_pt* pt, uint64_t* proposed, uint64_t* accepted);
 

@@ -131,8 +131,10 @@ _SIGS = {
     "ising_net_train_step": (_i, [_vp, _P(C.c_float), _P(C.c_float), _i, _d, _P(_d)]),
     "ising_pt_patch_step": (_i, [_vp, _vp, _i, _i, _i, _i, _i]),
     "ising_pt_patch_count": (_i, [_vp, _i, _P(_i64)]),
+    "ising_pt_patch_set_scale": (_i, [_vp, _P(C.c_float), C.c_float]),
     "ising_pt_patch_samples": (_i, [_vp, _i, _i, _i, _i, _i, _i, _P(C.c_float), _P(C.c_float)]),
     "ising_pt_patch_stats": (_i, [_vp, _P(_u64), _P(_u64)]),
+    "ising_pt_patch_jump": (_i, [_vp, _P(_d)]),
     "ising_pt_patch_last": (_i, [_vp, _i, _P(C.c_float), _P(C.c_float), _P(_d), _P(_d), _P(_i)]),
     "ising_write_spins_csv": (_i, [_vp, _i, C.c_char_p, _i, _i, _i]),
     "ising_write_pt_data_csv": (_i, [C.c_char_p, _d, _d, _d, _d, _d, _i, _d, _P(_d)]),

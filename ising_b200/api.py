@@ -394,6 +394,33 @@ class ParallelTempering:
         replicas holding temperature slots 0..slots-1 (0: all)."""
         _lib.call("ising_pt_patch_step", self._h, net.handle, colour, offset[0], offset[1], offset[2], slots)
 
+    def patch_set_scale(self, scale, drift: float = 1.0):
+        """Per-slot step scale (None restores 1) and drift weight of the patch move."""
+        self._drift = drift
+        if scale is None:
+            _lib.call("ising_pt_patch_set_scale", self._h, None, drift)
+            return
+        a = np.ascontiguousarray(scale, dtype=np.float32)
+        assert a.size == self.n
+        _lib.call("ising_pt_patch_set_scale", self._h, a.ctypes.data_as(_P(C.c_float)), drift)
+
+    def patch_tune_scale(self, net: "ProposalNet", target: float = 0.25, iters: int = 12, init: float = 0.3,
+                         seed: int = 0, drift: float = 1.0):
+        """Robbins-Monro tuning of the per-slot step scale toward a target acceptance (each
+        iteration is an ordinary patch step of all eight colour classes)."""
+        rng = np.random.default_rng(seed)
+        a = np.full(self.n, init)
+        for it in range(iters):
+            self.patch_set_scale(a, drift)
+            p0, c0 = self.patch_stats()
+            for c in range(8):
+                self.patch_step(net, c, tuple(int(v) for v in rng.integers(0, 8, 3)))
+            p1, c1 = self.patch_stats()
+            acc = (c1 - c0) / np.maximum(p1 - p0, 1)
+            a = np.clip(a * np.exp(2.0 * (acc - target) / np.sqrt(it + 1.0)), 1e-3, 2.0)
+        self.patch_set_scale(a, drift)
+        return a
+
     def patch_count(self, slots: int = 0) -> int:
         n = C.c_int64()
         _lib.call("ising_pt_patch_count", self._h, slots, C.byref(n))
@@ -408,6 +435,12 @@ class ParallelTempering:
         fp = lambda x: C.cast(x.data_ptr(), _P(C.c_float))
         _lib.call("ising_pt_patch_samples", self._h, colour, offset[0], offset[1], offset[2], slots, n_local, fp(w), fp(t))
         return w, t
+
+    def patch_jump(self) -> np.ndarray:
+        """Per slot: summed squared spin displacement of the accepted patch moves."""
+        out = np.zeros(self.n)
+        _lib.call("ising_pt_patch_jump", self._h, _dp(out))
+        return out
 
     def patch_stats(self):
         p = np.zeros(self.n, dtype=np.uint64)

@@ -855,6 +855,9 @@ struct ising_pt {
     double *pw_lqf = nullptr, *pw_dE = nullptr, *pw_dM = nullptr;
     int *pw_rej = nullptr, *pw_acc = nullptr;
     unsigned long long* pw_stats = nullptr;
+    float* pw_scale = nullptr;          // per-slot step scale (null: 1)
+    double* pw_jump = nullptr;          // per-slot sum of squared spin displacements of accepted patches
+    float pw_drift = 1.f;               // weight of the network's mean rotation
     int pw_batch = 0;
     int64_t pw_windows = 0;
     uint32_t patch_round = 0;
@@ -868,7 +871,8 @@ void pt_free(ising_pt* pt) {
     cudaFree(pt->d_series); cudaFree(pt->d_count); cudaFree(pt->d_q); cudaFree(pt->d_energy_tmp);
     cudaFree(pt->d_energy_out); cudaFree(pt->d_plan_slots); cudaFree(pt->d_plan_count);
     cudaFree(pt->pw_win); cudaFree(pt->pw_winp); cudaFree(pt->pw_prop); cudaFree(pt->pw_lqf); cudaFree(pt->pw_dE);
-    cudaFree(pt->pw_dM); cudaFree(pt->pw_rej); cudaFree(pt->pw_acc); cudaFree(pt->pw_stats);
+    cudaFree(pt->pw_dM); cudaFree(pt->pw_rej); cudaFree(pt->pw_acc); cudaFree(pt->pw_stats); cudaFree(pt->pw_scale);
+    cudaFree(pt->pw_jump);
 }
 
 int pt_resync_enqueue(ising_pt* pt) {
@@ -1111,7 +1115,7 @@ int patch_setup(ising_pt* pt, int colour, int offx, int offy, int offz, int slot
     Q.spins = m->d_spins; Q.natoms = L.natoms; Q.nx = L.nx; Q.ny = L.ny; Q.nz = L.nz; Q.layout = m->layout;
     Q.colour = colour; Q.offx = offx; Q.offy = offy; Q.offz = offz;
     Q.per_slot = (L.nx / 8) * (L.ny / 8) * (L.nz / 8);
-    Q.t2r = pt->d_t2r; Q.beta_rep = pt->d_beta_rep; Q.ham = pt->plan.ham;
+    Q.t2r = pt->d_t2r; Q.beta_rep = pt->d_beta_rep; Q.ham = pt->plan.ham; Q.step_scale = pt->pw_scale; Q.drift = pt->pw_drift;
     Q.seed = pt->opt.seed; Q.ensemble = pt->opt.ensemble; Q.status = m->d_status;
     return ISING_OK;
 }
@@ -1133,11 +1137,13 @@ int patch_workspace(ising_pt* pt, int batch) {
     ISG_TRY(dev_alloc(&pt->pw_lqf, batch));
     ISG_TRY(dev_alloc(&pt->pw_rej, batch));
     ISG_TRY(dev_alloc(&pt->pw_dE, windows));
-    ISG_TRY(dev_alloc(&pt->pw_dM, 3 * windows));
+    ISG_TRY(dev_alloc(&pt->pw_dM, 4 * windows));
     ISG_TRY(dev_alloc(&pt->pw_acc, windows));
     if (!pt->pw_stats) {
         ISG_TRY(dev_alloc(&pt->pw_stats, 2 * (size_t)pt->n));
         ISG_CUDA(cudaMemset(pt->pw_stats, 0, 2 * (size_t)pt->n * sizeof(unsigned long long)));
+        ISG_TRY(dev_alloc(&pt->pw_jump, pt->n));
+        ISG_CUDA(cudaMemset(pt->pw_jump, 0, (size_t)pt->n * sizeof(double)));
     }
     pt->pw_batch = batch;
     pt->pw_windows = windows;
@@ -1145,6 +1151,24 @@ int patch_workspace(ising_pt* pt, int batch) {
 }
 
 }  // namespace
+
+extern "C" int ising_pt_patch_set_scale(ising_pt* pt, const float* scale_per_slot, float drift) {
+    if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
+    if (!(drift >= 0.f) || !std::isfinite(drift)) return fail(ISING_ERR_ARG, "drift must be >= 0");
+    DeviceGuard g(pt->mesh->device);
+    pt->pw_drift = drift;
+    if (!scale_per_slot) {
+        cudaFree(pt->pw_scale);
+        pt->pw_scale = nullptr;
+        return ISING_OK;
+    }
+    for (int t = 0; t < pt->n; ++t)
+        if (!(scale_per_slot[t] > 0.f) || !std::isfinite(scale_per_slot[t])) return fail(ISING_ERR_ARG, "step scales must be positive");
+    if (!pt->pw_scale) ISG_TRY(dev_alloc(&pt->pw_scale, pt->n));
+    ISG_CUDA(cudaMemcpyAsync(pt->pw_scale, scale_per_slot, pt->n * sizeof(float), cudaMemcpyHostToDevice, pt->mesh->stream));
+    ISG_CUDA(cudaStreamSynchronize(pt->mesh->stream));
+    return ISING_OK;
+}
 
 extern "C" int ising_pt_patch_count(const ising_pt* pt, int slots, int64_t* n_windows) {
     if (!pt || !n_windows) return fail(ISING_ERR_ARG, "NULL argument");
@@ -1178,7 +1202,7 @@ extern "C" int ising_pt_patch_step(ising_pt* pt, ising_net* net, int colour, int
         ISG_TRY(launch_patch_accept(P, w0, nb, pt->pw_win, pt->pw_winp, out, pt->pw_prop, pt->pw_lqf, pt->pw_rej,
                                     pt->pw_dE, pt->pw_dM, pt->pw_acc, s));
     }
-    ISG_TRY(launch_patch_fold(P, ns, total, pt->pw_dE, pt->pw_dM, pt->pw_acc, pt->d_acc, pt->pw_stats, s));
+    ISG_TRY(launch_patch_fold(P, ns, total, pt->pw_dE, pt->pw_dM, pt->pw_acc, pt->d_acc, pt->pw_stats, pt->pw_jump, s));
     ISG_TRY(net_status_on(net, s));
     return check_status(m);
 }
@@ -1216,6 +1240,17 @@ extern "C" int ising_pt_patch_last(const ising_pt* pt, int n, float* win, float*
     if (dE) ISG_CUDA(cudaMemcpyAsync(dE, pt->pw_dE, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (accepted) ISG_CUDA(cudaMemcpyAsync(accepted, pt->pw_acc, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, s));
     ISG_CUDA(cudaStreamSynchronize(s));
+    return ISING_OK;
+}
+
+extern "C" int ising_pt_patch_jump(const ising_pt* pt, double* sq_jump) {
+    if (!pt || !sq_jump) return fail(ISING_ERR_ARG, "NULL argument");
+    DeviceGuard g(pt->mesh->device);
+    for (int t = 0; t < pt->n; ++t) sq_jump[t] = 0.0;
+    if (pt->pw_jump) {
+        ISG_CUDA(cudaMemcpyAsync(sq_jump, pt->pw_jump, pt->n * sizeof(double), cudaMemcpyDeviceToHost, pt->mesh->stream));
+        ISG_CUDA(cudaStreamSynchronize(pt->mesh->stream));
+    }
     return ISING_OK;
 }
 

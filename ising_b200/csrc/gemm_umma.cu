@@ -4,7 +4,8 @@
 //
 // A is M x K, B is N x K, both BF16 with K contiguous (row pitches lda, ldb, multiples of
 // 8 elements), K a multiple of 16, N a multiple of 16 up to 256; A holds ceil(M/128)*128
-// readable rows.  One block of 128 threads computes a 128-row tile for all N columns:
+// readable rows.  For a 32-channel 3^3 convolution A is not stored: the loader gathers its
+// 16-byte pieces from the channel-last input grid (implicit GEMM), zero outside the grid.  One block of 128 threads computes a 128-row tile for all N columns:
 // chunks of 64 values of K are staged by all threads into a two-stage ring in the canonical
 // no-swizzle layout (umma.cuh), thread 0 issues the MMAs and commits them to the stage's
 // mbarrier, and the block refills a stage once that mbarrier reports its MMAs done.  The
@@ -60,7 +61,24 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const GemmArgs g) {
         const int q8 = kw >> 3;
         for (int i = tid; i < 128 * q8; i += kGemmThreads) {
             const int r = i / q8, q = i - r * q8;
-            const uint4 v = *reinterpret_cast<const uint4*>(g.A + (size_t)(m0 + r) * g.lda + kc0 + 8 * q);
+            const int row = m0 + r, k = kc0 + 8 * q;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (g.conv_in) {
+                // implicit convolution: the 8 values are channels ch..ch+7 of kernel offset o
+                const int C = g.conv_C, Go = g.conv_Go, Gi = g.conv_Gi;
+                const int o = k / C, ch = k - o * C;
+                if (row < g.M && o < 27) {
+                    const int Go3 = Go * Go * Go;
+                    const int b = row / Go3, u = row - b * Go3;
+                    const int x = u / (Go * Go) + o / 9 - g.conv_pad;
+                    const int y = (u / Go) % Go + (o / 3) % 3 - g.conv_pad;
+                    const int z = u % Go + o % 3 - g.conv_pad;
+                    if (x >= 0 && x < Gi && y >= 0 && y < Gi && z >= 0 && z < Gi)
+                        v = *reinterpret_cast<const uint4*>(g.conv_in + ((((int64_t)b * Gi + x) * Gi + y) * Gi + z) * C + ch);
+                }
+            } else {
+                v = *reinterpret_cast<const uint4*>(g.A + (size_t)row * g.lda + k);
+            }
             *reinterpret_cast<uint4*>(sA + umma_off(128, r, 8 * q)) = v;
         }
         for (int i = tid; i < N * q8; i += kGemmThreads) {
@@ -106,16 +124,22 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const GemmArgs g) {
     if (warp == 0) tmem_dealloc(taddr, ncols);
 }
 
-// at least 72 KB: keeps a few resident blocks per SM and every descriptor-addressed range
-// well inside the allocation
-static int gemm_smem_bytes(int N) { return max(72 * 1024, 2 * (128 * kGemmKC * 2 + N * kGemmKC * 2) + 64); }
+static int gemm_smem_bytes(int N) { return 2 * (128 * kGemmKC * 2 + N * kGemmKC * 2) + 64; }
 
 int launch_gemm_bf16(GemmArgs g, cudaStream_t s) {
     if (g.N < 16 || g.N > 256 || g.N % 16) return fail(ISING_ERR_ARG, "GEMM N must be a multiple of 16 in 16..256");
     if (g.K < 16 || g.K % 16) return fail(ISING_ERR_ARG, "GEMM K must be a positive multiple of 16");
     if (g.M < 1) return ISING_OK;
-    if (g.lda % 8 || g.ldb % 8 || g.lda < g.K || g.ldb < g.K) return fail(ISING_ERR_ARG, "GEMM row pitch must be >= K and a multiple of 8");
-    if ((reinterpret_cast<uintptr_t>(g.A) | reinterpret_cast<uintptr_t>(g.B)) & 15) return fail(ISING_ERR_ARG, "GEMM operands must be 16-byte aligned");
+    if (g.conv_in) {
+        if (g.conv_C % 8 || g.K != 27 * g.conv_C || g.conv_Gi < 1 || g.conv_Go < 1)
+            return fail(ISING_ERR_ARG, "implicit convolution needs C % 8 == 0 and K = 27 C");
+        if (reinterpret_cast<uintptr_t>(g.conv_in) & 15) return fail(ISING_ERR_ARG, "GEMM operands must be 16-byte aligned");
+    } else {
+        if (g.lda % 8 || g.lda < g.K) return fail(ISING_ERR_ARG, "GEMM row pitch must be >= K and a multiple of 8");
+        if (reinterpret_cast<uintptr_t>(g.A) & 15) return fail(ISING_ERR_ARG, "GEMM operands must be 16-byte aligned");
+    }
+    if (g.ldb % 8 || g.ldb < g.K) return fail(ISING_ERR_ARG, "GEMM row pitch must be >= K and a multiple of 8");
+    if (reinterpret_cast<uintptr_t>(g.B) & 15) return fail(ISING_ERR_ARG, "GEMM operands must be 16-byte aligned");
     g.tmem_cols = g.N <= 32 ? 32 : g.N <= 64 ? 64 : g.N <= 128 ? 128 : 256;
     // resident blocks per SM x TMEM columns must fit the SM's 512 columns: a block whose
     // allocation cannot be met would stall until another block frees its columns

@@ -6,6 +6,8 @@
 // after each, then a 1^3 head 32 -> 4 giving mu (3) and log sigma per patch site.
 // Activations are channel-last BF16 rows (one row per window voxel); each convolution is
 //     out[rows x 32] = im2col(in)[rows x 27*Cin] * Wf[32 x 27*Cin]^T + b      (tensor cores)
+// where the 32-channel layers gather im2col(in) inside the GEMM's loader (implicit GEMM) and
+// the 3-channel input layer and the weight gradients use materialised im2col matrices.
 // with column k = o * Cin + c, o = (dx*3 + dy)*3 + dz.  Backward: the data gradient of a
 // convolution is a convolution of the output gradient with the flipped, transposed kernel
 // (same im2col, weights WfT[ci][o'*32 + co] = W[co][ci][26 - o']); the weight gradient is
@@ -90,6 +92,33 @@ __global__ void k_im2col(const __nv_bfloat16* __restrict__ in, int C, int Gi, in
                 v = in[((b * Gi + x) * Gi + y) * (int64_t)Gi * C + (int64_t)z * C + c];
         }
         out[i] = v;
+    }
+}
+
+// im2col of the 3-channel input grid (8^3 -> 6^3, Kp = 96): one thread per row, the 81
+// values gathered into registers and stored as twelve 16-byte vectors
+__global__ void k_im2col_c3(const __nv_bfloat16* __restrict__ in, int64_t n_rows, __nv_bfloat16* __restrict__ out) {
+    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n_rows; row += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = row / 216;
+        const int u = (int)(row - b * 216);
+        const int x = u / 36, y = (u / 6) % 6, z = u % 6;
+        const __nv_bfloat16* base = in + (((b * 8 + x) * 8 + y) * 8 + z) * 3;
+        uint32_t w[48];
+#pragma unroll
+        for (int q = 0; q < 48; ++q) w[q] = 0u;
+#pragma unroll
+        for (int o = 0; o < 27; ++o) {
+            const int off = ((o / 9) * 64 + ((o / 3) % 3) * 8 + (o % 3)) * 3;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const int k = o * 3 + c;
+                const uint32_t h = __bfloat16_as_ushort(base[off + c]);
+                w[k >> 1] |= (k & 1) ? (h << 16) : h;
+            }
+        }
+        uint4* dst = reinterpret_cast<uint4*>(out + row * kK1);
+#pragma unroll
+        for (int q = 0; q < 12; ++q) dst[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
     }
 }
 
@@ -261,10 +290,10 @@ struct ising_net {
     float *P = nullptr, *G = nullptr, *M = nullptr, *V = nullptr;
     int adam_t = 0;
     __nv_bfloat16 *Wf1 = nullptr, *Wf2 = nullptr, *Wf3 = nullptr, *W2fT = nullptr, *W3fT = nullptr;
-    __nv_bfloat16 *X0 = nullptr, *A1 = nullptr, *H1 = nullptr, *A2 = nullptr, *H2 = nullptr, *A3 = nullptr, *H3 = nullptr;
+    __nv_bfloat16 *X0 = nullptr, *A1 = nullptr, *H1 = nullptr, *H2 = nullptr, *H3 = nullptr;
     float *pre1 = nullptr, *pre2 = nullptr, *pre3 = nullptr, *out = nullptr;
     float *dout = nullptr, *dh = nullptr, *Cw = nullptr;
-    __nv_bfloat16 *dp = nullptr, *dpt = nullptr, *AT = nullptr, *Abig = nullptr;
+    __nv_bfloat16 *dp = nullptr, *dpt = nullptr, *AT = nullptr;
     double* loss = nullptr;
     int* status = nullptr;
 };
@@ -288,9 +317,9 @@ int nalloc(T** p, size_t n) {
 }
 
 void net_free(ising_net* n) {
-    void* ptrs[] = {n->P, n->G, n->M, n->V, n->Wf1, n->Wf2, n->Wf3, n->W2fT, n->W3fT, n->X0, n->A1, n->H1, n->A2,
-                    n->H2, n->A3, n->H3, n->pre1, n->pre2, n->pre3, n->out, n->dout, n->dh, n->Cw, n->dp, n->dpt,
-                    n->AT, n->Abig, n->loss, n->status};
+    void* ptrs[] = {n->P, n->G, n->M, n->V, n->Wf1, n->Wf2, n->Wf3, n->W2fT, n->W3fT, n->X0, n->A1, n->H1,
+                    n->H2, n->H3, n->pre1, n->pre2, n->pre3, n->out, n->dout, n->dh, n->Cw, n->dp, n->dpt,
+                    n->AT, n->loss, n->status};
     for (void* p : ptrs) cudaFree(p);
     if (n->stream) cudaStreamDestroy(n->stream);
 }
@@ -314,20 +343,27 @@ GemmArgs gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, 
     return g;
 }
 
+// a 32-channel 3^3 convolution as an implicit GEMM: rows over the Go^3 output grid of every
+// window, A gathered from the channel-last input grid by the GEMM's loader
+GemmArgs conv_gemm(const __nv_bfloat16* in, int Gi, int Go, int pad, const __nv_bfloat16* W, int rows, int* st) {
+    GemmArgs g{};
+    g.B = W; g.ldb = kK2; g.M = rows; g.N = kCh; g.K = kK2; g.status = st;
+    g.conv_in = in; g.conv_C = kCh; g.conv_Gi = Gi; g.conv_Go = Go; g.conv_pad = pad;
+    return g;
+}
+
 // forward of nb windows already in X0; keeps pre-activations (for backward) and out
 int net_forward_rows(ising_net* n, int nb) {
     cudaStream_t s = n->stream;
     const int64_t R1 = (int64_t)nb * 216, R2 = (int64_t)nb * 64;
-    k_im2col<<<grid_for(R1 * kK1), 256, 0, s>>>(n->X0, 3, 8, 6, 0, R1, n->A1, kK1, 0, 0, 0);
+    k_im2col_c3<<<grid_for(R1, 128), 128, 0, s>>>(n->X0, R1, n->A1);
     GemmArgs g = gemm(n->A1, kK1, n->Wf1, kK1, (int)R1, kCh, kK1, n->status);
     g.bias = n->P + kOffB1; g.C = n->pre1; g.ldc = kCh; g.O = n->H1; g.ldo = kCh; g.gelu = 1;
     ISG_TRY_N(launch_gemm_bf16(g, s));
-    k_im2col<<<grid_for(R2 * kK2), 256, 0, s>>>(n->H1, kCh, 6, 4, 0, R2, n->A2, kK2, 0, 0, 0);
-    g = gemm(n->A2, kK2, n->Wf2, kK2, (int)R2, kCh, kK2, n->status);
+    g = conv_gemm(n->H1, 6, 4, 0, n->Wf2, (int)R2, n->status);
     g.bias = n->P + kOffB2; g.C = n->pre2; g.ldc = kCh; g.O = n->H2; g.ldo = kCh; g.gelu = 1;
     ISG_TRY_N(launch_gemm_bf16(g, s));
-    k_im2col<<<grid_for(R2 * kK2), 256, 0, s>>>(n->H2, kCh, 4, 4, 1, R2, n->A3, kK2, 0, 0, 0);
-    g = gemm(n->A3, kK2, n->Wf3, kK2, (int)R2, kCh, kK2, n->status);
+    g = conv_gemm(n->H2, 4, 4, 1, n->Wf3, (int)R2, n->status);
     g.bias = n->P + kOffB3; g.C = n->pre3; g.ldc = kCh; g.O = n->H3; g.ldo = kCh; g.gelu = 1;
     ISG_TRY_N(launch_gemm_bf16(g, s));
     k_head_fwd<<<(int)((R2 + 127) / 128), 128, 0, s>>>(n->H3, R2, n->P, n->out);
@@ -351,8 +387,7 @@ int net_backward(ising_net* n, const float* win, const float* tgt, int nb) {
     g.C = n->Cw; g.ldc = kCh;
     ISG_TRY_N(launch_gemm_bf16(g, s));
     k_scatter_wgrad<<<(27 * kCh * kCh + 255) / 256, 256, 0, s>>>(n->Cw, kCh, kOffW3, n->G);
-    k_im2col<<<grid_for(R2 * kK2), 256, 0, s>>>(n->dp, kCh, 4, 4, 1, R2, n->A3, kK2, 0, 0, 0);
-    g = gemm(n->A3, kK2, n->W3fT, kK2, (int)R2, kCh, kK2, n->status);
+    g = conv_gemm(n->dp, 4, 4, 1, n->W3fT, (int)R2, n->status);
     g.C = n->dh; g.ldc = kCh;
     ISG_TRY_N(launch_gemm_bf16(g, s));
     // conv2
@@ -362,8 +397,7 @@ int net_backward(ising_net* n, const float* win, const float* tgt, int nb) {
     g.C = n->Cw; g.ldc = kCh;
     ISG_TRY_N(launch_gemm_bf16(g, s));
     k_scatter_wgrad<<<(27 * kCh * kCh + 255) / 256, 256, 0, s>>>(n->Cw, kCh, kOffW2, n->G);
-    k_im2col<<<grid_for(R1 * kK2), 256, 0, s>>>(n->dp, kCh, 4, 6, 2, R1, n->Abig, kK2, 0, 0, 0);
-    g = gemm(n->Abig, kK2, n->W2fT, kK2, (int)R1, kCh, kK2, n->status);
+    g = conv_gemm(n->dp, 4, 6, 2, n->W2fT, (int)R1, n->status);
     g.C = n->dh; g.ldc = kCh;
     ISG_TRY_N(launch_gemm_bf16(g, s));
     // conv1
@@ -403,25 +437,22 @@ extern "C" int ising_net_create(int device, int max_batch, uint64_t seed, ising_
     if (cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(cuda_fail(cudaGetLastError(), "cudaStreamCreateWithFlags"));
     const size_t B = (size_t)max_batch, R1 = B * 216, R2 = B * 64;
-    const size_t R1p = pad128(R1), R2p = pad128(R2), L1 = pad32(R1);
+    const size_t R1p = pad128(R1), L1 = pad32(R1);
     int st = ISING_OK;
     if ((st = nalloc(&n->P, kNParams)) || (st = nalloc(&n->G, kNParams)) || (st = nalloc(&n->M, kNParams)) ||
         (st = nalloc(&n->V, kNParams)) || (st = nalloc(&n->Wf1, kCh * kK1)) || (st = nalloc(&n->Wf2, kCh * kK2)) ||
         (st = nalloc(&n->Wf3, kCh * kK2)) || (st = nalloc(&n->W2fT, kCh * kK2)) || (st = nalloc(&n->W3fT, kCh * kK2)) ||
         (st = nalloc(&n->X0, B * 512 * 3)) || (st = nalloc(&n->A1, R1p * kK1)) || (st = nalloc(&n->H1, R1 * kCh)) ||
-        (st = nalloc(&n->A2, R2p * kK2)) || (st = nalloc(&n->H2, R2 * kCh)) || (st = nalloc(&n->A3, R2p * kK2)) ||
+        (st = nalloc(&n->H2, R2 * kCh)) ||
         (st = nalloc(&n->H3, R2 * kCh)) || (st = nalloc(&n->pre1, R1 * kCh)) || (st = nalloc(&n->pre2, R2 * kCh)) ||
         (st = nalloc(&n->pre3, R2 * kCh)) || (st = nalloc(&n->out, R2 * 4)) || (st = nalloc(&n->dout, R2 * 4)) ||
         (st = nalloc(&n->dh, R1 * kCh)) || (st = nalloc(&n->Cw, (size_t)kK2Pad * kCh)) ||
         (st = nalloc(&n->dp, R1 * kCh)) || (st = nalloc(&n->dpt, (size_t)kCh * L1)) ||
         (st = nalloc(&n->AT, std::max((size_t)kK2Pad * pad32(R2), (size_t)128 * L1))) ||
-        (st = nalloc(&n->Abig, R1p * kK2)) || (st = nalloc(&n->loss, 1)) || (st = nalloc(&n->status, 1)))
+        (st = nalloc(&n->loss, 1)) || (st = nalloc(&n->status, 1)))
         return bail(st);
     // padding rows of the GEMM A operands stay zero
     cudaMemset(n->A1, 0, R1p * kK1 * sizeof(__nv_bfloat16));
-    cudaMemset(n->A2, 0, R2p * kK2 * sizeof(__nv_bfloat16));
-    cudaMemset(n->A3, 0, R2p * kK2 * sizeof(__nv_bfloat16));
-    cudaMemset(n->Abig, 0, R1p * kK2 * sizeof(__nv_bfloat16));
     cudaMemset(n->M, 0, kNParams * sizeof(float));
     cudaMemset(n->V, 0, kNParams * sizeof(float));
     cudaMemset(n->status, 0, sizeof(int));

@@ -26,6 +26,11 @@ struct GemmArgs {
     int ldo;
     int gelu;
     int* status;
+    // implicit convolution: when conv_in is set, A is not read; A(row, k) = conv_in[b][u + o -
+    // conv_pad][c] for row = b*Go^3 + u, k = o*C + c (C % 8 == 0), zero outside the grid or
+    // for row >= M
+    const __nv_bfloat16* conv_in;
+    int conv_C, conv_Gi, conv_Go, conv_pad;
     uint32_t tmem_cols;     // set by the launcher
 };
 int launch_gemm_bf16(GemmArgs g, cudaStream_t s);
@@ -48,6 +53,8 @@ struct PatchStep {
     int per_slot;
     const int* t2r;            // slot -> replica
     const double* beta_rep;
+    const float* step_scale;   // per slot: the tangent move is scale * (drift P_s(mu) + sigma eps); null = 1
+    float drift;               // weight of the network's mean rotation (1 = the mean as predicted)
     HamDev ham;
     uint64_t seed;
     uint32_t ensemble;
@@ -58,10 +65,10 @@ int launch_patch_gather(const PatchStep& P, int64_t w0, int nb, const float* pro
 int launch_patch_propose(const PatchStep& P, int64_t w0, int nb, const float* win, const float* out, float* prop,
                          double* lqf, int* rej, cudaStream_t s);
 int launch_patch_accept(const PatchStep& P, int64_t w0, int nb, const float* win, const float* winp, const float* outp,
-                        const float* prop, const double* lqf, const int* rej, double* dE, double* dM, int* acc,
+                        const float* prop, const double* lqf, const int* rej, double* dE, double* dM4, int* acc,
                         cudaStream_t s);
 int launch_patch_fold(const PatchStep& P, int n_slots, int64_t n_windows, const double* dE, const double* dM,
-                      const int* accepted, Acc4* acc, unsigned long long* stats, cudaStream_t s);
+                      const int* accepted, Acc4* acc, unsigned long long* stats, double* jump, cudaStream_t s);
 int launch_patch_equilibrate(const PatchStep& P, int64_t w0, int nb, const float* win, int n_local, int move, float r,
                              float* tgt, cudaStream_t s);
 

@@ -10,7 +10,9 @@
 // log_{s'}(s); accept with min(1, exp(-beta dE) q(x|x') / q(x'|x)).  dE counts every bond of
 // the patch once (patch-halo bonds whole, patch-patch bonds half from each end) plus the
 // Zeeman and anisotropy terms of the patch sites.  The Jacobian |omega|/sin|omega| of the
-// exponential map enters both densities.
+// exponential map enters both densities.  A per-slot step scale a and a drift weight l shape
+// the tangent move, omega ~ N(a l mu, a^2 sigma^2); both are fixed during a step, so the
+// forward and reverse densities use the same a and l.
 #include "learned.h"
 
 namespace isg {
@@ -89,11 +91,12 @@ __global__ void __launch_bounds__(64) k_patch_propose(PatchStep P, int64_t w0, c
     const int v = (a * 8 + bb) * 8 + c;
     const V3 s = v3(win[((int64_t)b * 3) * 512 + v], win[((int64_t)b * 3 + 1) * 512 + v], win[((int64_t)b * 3 + 2) * 512 + v]);
     const float* o = out + ((int64_t)b * 64 + i) * 4;
-    const float ls = fminf(kLogSigMax, fmaxf(kLogSigMin, o[3]));
+    const float sc_ = P.step_scale ? P.step_scale[(int)(w / P.per_slot)] : 1.f;
+    const float ls = fminf(kLogSigMax, fmaxf(kLogSigMin, o[3])) + logf(sc_);
     const float sig = expf(ls);
     V3 e1, e2;
     pframe(s, e1, e2);
-    const V3 mu = v3(o[0], o[1], o[2]);
+    const V3 mu = vscale(sc_ * P.drift, v3(o[0], o[1], o[2]));
     const uint4 r = philox4x32<10>(make_uint4((uint32_t)(w * 64 + i), P.round, 0u, (P.ensemble << 8) | kTagPatch),
                                    philox_key(P.seed));
     const float u1 = 1.f - u01(r.x), u2 = u01(r.y);
@@ -138,7 +141,8 @@ __global__ void __launch_bounds__(64) k_patch_accept(PatchStep P, int64_t w0, co
     const V3 sp = v3(pp[0], pp[1], pp[2]);
     // reverse proposal density, network output at x'
     const float* o = outp + ((int64_t)b * 64 + i) * 4;
-    const float ls = fminf(kLogSigMax, fmaxf(kLogSigMin, o[3]));
+    const float sc_ = P.step_scale ? P.step_scale[(int)(w / P.per_slot)] : 1.f;
+    const float ls = fminf(kLogSigMax, fmaxf(kLogSigMin, o[3])) + logf(sc_);
     V3 e1, e2;
     pframe(sp, e1, e2);
     const float cth = fminf(1.f, fmaxf(-1.f, vdot(sp, s)));
@@ -146,7 +150,7 @@ __global__ void __launch_bounds__(64) k_patch_accept(PatchStep P, int64_t w0, co
     const V3 vv = vaxpy(-cth, sp, s);
     const float nv = sqrtf(vdot(vv, vv));
     const float sc = nv > 1e-12f ? th / nv : 0.f;
-    const V3 mu = v3(o[0], o[1], o[2]);
+    const V3 mu = vscale(sc_ * P.drift, v3(o[0], o[1], o[2]));
     const float r1 = sc * vdot(vv, e1) - vdot(mu, e1), r2 = sc * vdot(vv, e2) - vdot(mu, e2);
     const double lq = (double)(-0.5f * (r1 * r1 + r2 * r2) * expf(-2.f * ls) - 2.f * ls + log_jac(th));
     // energy of site i in x' minus in x; neighbours inside the patch count half
@@ -194,9 +198,10 @@ __global__ void __launch_bounds__(64) k_patch_accept(PatchStep P, int64_t w0, co
         dm = v3(sp.x - s.x, sp.y - s.y, sp.z - s.z);
     }
     const double mx = block_sum64((double)dm.x, sd), my = block_sum64((double)dm.y, sd), mz = block_sum64((double)dm.z, sd);
+    const double j2 = block_sum64((double)vdot(dm, dm), sd);
     if (i == 0) {
         dE[w] = ok ? dE_tot : 0.0;
-        dM[3 * w] = mx; dM[3 * w + 1] = my; dM[3 * w + 2] = mz;
+        dM[4 * w] = mx; dM[4 * w + 1] = my; dM[4 * w + 2] = mz; dM[4 * w + 3] = j2;
         accepted[w] = ok;
     }
 }
@@ -204,30 +209,31 @@ __global__ void __launch_bounds__(64) k_patch_accept(PatchStep P, int64_t w0, co
 // per temperature slot: fold the windows' dE, dM into the replica's accumulators
 __global__ void k_patch_fold(PatchStep P, int64_t n_windows, const double* __restrict__ dE, const double* __restrict__ dM,
                              const int* __restrict__ accepted, Acc4* __restrict__ acc,
-                             unsigned long long* __restrict__ stats) {
-    __shared__ double sm[4][8];
+                             unsigned long long* __restrict__ stats, double* __restrict__ jump) {
+    __shared__ double sm[5][8];
     __shared__ long long sa[8];
     const int t = blockIdx.x;
     const int64_t b0 = (int64_t)t * P.per_slot;
-    double v[4] = {0, 0, 0, 0};
+    double v[5] = {0, 0, 0, 0, 0};
     long long na = 0;
     for (int64_t w = b0 + threadIdx.x; w < b0 + P.per_slot && w < n_windows; w += blockDim.x) {
-        v[0] += dE[w]; v[1] += dM[3 * w]; v[2] += dM[3 * w + 1]; v[3] += dM[3 * w + 2];
+        v[0] += dE[w]; v[1] += dM[4 * w]; v[2] += dM[4 * w + 1]; v[3] += dM[4 * w + 2]; v[4] += dM[4 * w + 3];
         na += accepted[w];
     }
-    for (int q = 0; q < 4; ++q) v[q] = warp_sum(v[q]);
+    for (int q = 0; q < 5; ++q) v[q] = warp_sum(v[q]);
     na = warp_sum(na);
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-    if (lane == 0) { for (int q = 0; q < 4; ++q) sm[q][wp] = v[q]; sa[wp] = na; }
+    if (lane == 0) { for (int q = 0; q < 5; ++q) sm[q][wp] = v[q]; sa[wp] = na; }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double tot[4] = {0, 0, 0, 0};
+        double tot[5] = {0, 0, 0, 0, 0};
         long long ta = 0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { for (int q = 0; q < 4; ++q) tot[q] += sm[q][k]; ta += sa[k]; }
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { for (int q = 0; q < 5; ++q) tot[q] += sm[q][k]; ta += sa[k]; }
         const int rep = P.t2r ? P.t2r[t] : t;
         acc[rep].e += tot[0]; acc[rep].mx += tot[1]; acc[rep].my += tot[2]; acc[rep].mz += tot[3];
         stats[2 * t] += (unsigned long long)P.per_slot;
         stats[2 * t + 1] += (unsigned long long)ta;
+        jump[t] += tot[4];
     }
 }
 
@@ -300,8 +306,8 @@ int launch_patch_accept(const PatchStep& P, int64_t w0, int nb, const float* win
     return ISING_OK;
 }
 int launch_patch_fold(const PatchStep& P, int n_slots, int64_t n_windows, const double* dE, const double* dM,
-                      const int* accepted, Acc4* acc, unsigned long long* stats, cudaStream_t s) {
-    k_patch_fold<<<n_slots, 256, 0, s>>>(P, n_windows, dE, dM, accepted, acc, stats);
+                      const int* accepted, Acc4* acc, unsigned long long* stats, double* jump, cudaStream_t s) {
+    k_patch_fold<<<n_slots, 256, 0, s>>>(P, n_windows, dE, dM, accepted, acc, stats, jump);
     ISG_CUDA(cudaGetLastError());
     return ISING_OK;
 }

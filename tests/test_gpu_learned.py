@@ -132,6 +132,9 @@ def test_patch_move_matches_oracle(ib, cuda_ok):
     net = ib.ProposalNet(max_batch=16, seed=9)
     params = R.unflatten(net.get_params())
     colour, off = 5, (1, 2, 3)
+    scale = np.array([0.5, 1.0, 0.25, 0.1], np.float32)
+    drift = 0.7
+    pt.patch_set_scale(scale, drift)
     t2r = pt.permutation()
     pre = [m.get_spins(r).T.copy() for r in range(len(betas))]          # (3, N)
     pt.patch_step(net, colour, off)
@@ -160,11 +163,13 @@ def test_patch_move_matches_oracle(ib, cuda_ok):
         out = R.forward(params, x[None], round_bf16=True)[0]
         outp = R.forward(params, xp[None], round_bf16=True)[0]
         om, th = R.log_map(s, sp)
-        ls = out[:, 3].clamp(-6.0, 1.5)
-        eps = (om - R.tangent_mean(out, s)) / torch.exp(ls)[:, None]
+        a = float(scale[t])
+        ls = out[:, 3].clamp(-6.0, 1.5) + np.log(a)
+        eps = (om - a * drift * R.tangent_mean(out, s)) / torch.exp(ls)[:, None]
         lq_f = float((-0.5 * (eps * eps).sum(-1) - 2.0 * ls + R.log_jac(th)).sum())
         outp_c = outp.clone()
-        outp_c[:, 3] = outp_c[:, 3].clamp(-6.0, 1.5)
+        outp_c[:, :3] *= a * drift
+        outp_c[:, 3] = outp_c[:, 3].clamp(-6.0, 1.5) + np.log(a)
         lq_r = float(R.log_q_reverse(outp_c, sp, s)) + 64 * np.log(2 * np.pi)
         de = float(R.patch_energy(xp, -1.0, 0.5, 0.25) - R.patch_energy(x, -1.0, 0.5, 0.25))
         assert abs(lq_f - lqf[t]) < 0.5, (lq_f, lqf[t])
