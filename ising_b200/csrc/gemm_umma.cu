@@ -4,8 +4,9 @@
 //
 // A is M x K, B is N x K, both BF16 with K contiguous (row pitches lda, ldb, multiples of
 // 8 elements), K a multiple of 16, N a multiple of 16 up to 256; A holds ceil(M/128)*128
-// readable rows.  For a 32-channel 3^3 convolution A is not stored: the loader gathers its
-// 16-byte pieces from the channel-last input grid (implicit GEMM), zero outside the grid.  One block of 128 threads computes a 128-row tile for all N columns:
+// readable rows.  For a 3^3 convolution over an 8- or 32-channel grid A is not stored: the
+// loader gathers its 16-byte pieces from the channel-last input grid (implicit GEMM), zero
+// outside the grid; each thread owns one output row, decomposed once before the K loop.  One block of 128 threads computes a 128-row tile for all N columns:
 // chunks of 64 values of K are staged by all threads into a two-stage ring in the canonical
 // no-swizzle layout (umma.cuh), thread 0 issues the MMAs and commits them to the stage's
 // mbarrier, and the block refills a stage once that mbarrier reports its MMAs done.  The
@@ -49,47 +50,87 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const GemmArgs g) {
     const uint32_t taddr = *slot;
     const uint32_t idesc = umma_idesc_bf16(128, N);
     const int nk = (g.K + kGemmKC - 1) / kGemmKC;
+    // implicit convolution: this thread's row is fixed for the whole K loop
+    const __nv_bfloat16* cbase = nullptr;
+    int cx = 0, cy = 0, cz = 0;
+    bool crow_ok = false;
+    if (g.conv_in) {
+        const int row = m0 + tid, Go = g.conv_Go, Gi = g.conv_Gi;
+        const int Go3 = Go * Go * Go;
+        crow_ok = row < g.M;
+        const int b = crow_ok ? row / Go3 : 0, u = crow_ok ? row - b * Go3 : 0;
+        cx = u / (Go * Go) - g.conv_pad;
+        cy = (u / Go) % Go - g.conv_pad;
+        cz = u % Go - g.conv_pad;
+        cbase = g.conv_in + (int64_t)b * Gi * Gi * Gi * g.conv_C;
+    }
+    const bool C32 = g.conv_C == 32;
+    // Register-staged pipeline: the loads of chunk c+1 are issued right after chunk c is
+    // stored to shared memory, so they are in flight while chunk c's MMAs are issued and
+    // the next stage is awaited.  A: this thread's row, 8 values per piece, q8 <= 8 pieces;
+    // B: N x q8 pieces spread over the block (<= 16 per thread).
+    uint4 va[8], vb[16];
+    auto load_chunk = [&](int c) {
+        const int kc0 = c * kGemmKC;
+        const int q8 = min(kGemmKC, g.K - kc0) >> 3;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            va[j] = make_uint4(0u, 0u, 0u, 0u);
+            if (j < q8) {
+                const int k = kc0 + 8 * j;
+                if (g.conv_in) {
+                    // implicit convolution: channels ch..ch+7 of kernel offset o of this
+                    // thread's output voxel (C = 32: four pieces per offset; C = 8: one)
+                    const int o = C32 ? (k >> 5) : (k >> 3), ch = C32 ? (k & 31) : 0;
+                    if (crow_ok && o < 27) {
+                        const int x = cx + o / 9, y = cy + (o / 3) % 3, z = cz + o % 3;
+                        const int Gi = g.conv_Gi;
+                        if ((unsigned)x < (unsigned)Gi && (unsigned)y < (unsigned)Gi && (unsigned)z < (unsigned)Gi)
+                            va[j] = *reinterpret_cast<const uint4*>(cbase + (((int64_t)x * Gi + y) * Gi + z) * g.conv_C + ch);
+                    }
+                } else {
+                    va[j] = *reinterpret_cast<const uint4*>(g.A + (size_t)(m0 + tid) * g.lda + k);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int i = tid + j * kGemmThreads;
+            if (i < N * q8) {
+                const int r = i / q8, q = i - r * q8;
+                vb[j] = *reinterpret_cast<const uint4*>(g.B + (size_t)r * g.ldb + kc0 + 8 * q);
+            }
+        }
+    };
+    auto store_chunk = [&](int c, unsigned char* sA, unsigned char* sB) {
+        const int q8 = min(kGemmKC, g.K - c * kGemmKC) >> 3;
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j < q8) *reinterpret_cast<uint4*>(sA + umma_off(128, tid, 8 * j)) = va[j];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int i = tid + j * kGemmThreads;
+            if (i < N * q8) {
+                const int r = i / q8, q = i - r * q8;
+                *reinterpret_cast<uint4*>(sB + umma_off(N, r, 8 * q)) = vb[j];
+            }
+        }
+    };
     bool ok = true;
+    load_chunk(0);
     for (int c = 0; c < nk && ok; ++c) {
         const int s = c & 1;
         if (c >= 2) ok = mbar_wait(&bar[s], (uint32_t)(((c - 2) >> 1) & 1), kGemmWaitPolls);
         if (!__syncthreads_and(ok)) { ok = false; break; }
         unsigned char* sA = smem + s * stage_bytes;
         unsigned char* sB = sA + a_bytes;
-        const int kc0 = c * kGemmKC;
-        const int kw = min(kGemmKC, g.K - kc0);   // multiple of 16
-        const int q8 = kw >> 3;
-        for (int i = tid; i < 128 * q8; i += kGemmThreads) {
-            const int r = i / q8, q = i - r * q8;
-            const int row = m0 + r, k = kc0 + 8 * q;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (g.conv_in) {
-                // implicit convolution: the 8 values are channels ch..ch+7 of kernel offset o
-                const int C = g.conv_C, Go = g.conv_Go, Gi = g.conv_Gi;
-                const int o = k / C, ch = k - o * C;
-                if (row < g.M && o < 27) {
-                    const int Go3 = Go * Go * Go;
-                    const int b = row / Go3, u = row - b * Go3;
-                    const int x = u / (Go * Go) + o / 9 - g.conv_pad;
-                    const int y = (u / Go) % Go + (o / 3) % 3 - g.conv_pad;
-                    const int z = u % Go + o % 3 - g.conv_pad;
-                    if (x >= 0 && x < Gi && y >= 0 && y < Gi && z >= 0 && z < Gi)
-                        v = *reinterpret_cast<const uint4*>(g.conv_in + ((((int64_t)b * Gi + x) * Gi + y) * Gi + z) * C + ch);
-                }
-            } else {
-                v = *reinterpret_cast<const uint4*>(g.A + (size_t)row * g.lda + k);
-            }
-            *reinterpret_cast<uint4*>(sA + umma_off(128, r, 8 * q)) = v;
-        }
-        for (int i = tid; i < N * q8; i += kGemmThreads) {
-            const int r = i / q8, q = i - r * q8;
-            const uint4 v = *reinterpret_cast<const uint4*>(g.B + (size_t)r * g.ldb + kc0 + 8 * q);
-            *reinterpret_cast<uint4*>(sB + umma_off(N, r, 8 * q)) = v;
-        }
+        store_chunk(c, sA, sB);
+        if (c + 1 < nk) load_chunk(c + 1);
         fence_async_smem();
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
+            const int kw = min(kGemmKC, g.K - c * kGemmKC);
             const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
             for (int j = 0; j < (kw >> 4); ++j) {
                 const uint64_t ad = umma_smem_desc(a0 + (uint32_t)(2 * j) * (128u * 16u), 128u * 16u, 128u);
@@ -105,16 +146,45 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const GemmArgs g) {
     if (!ok) {
         if (tid == 0) atomicOr(g.status, kStatTimeout);
     } else {
+        // epilogue: each thread owns one output row; 16-byte stores (ldc % 4 == 0, ldo % 8 == 0)
         const int row = m0 + warp * 32 + lane;
         for (int cb = 0; cb < N; cb += 32) {
             float v[32];
             tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
             if (row < g.M) {
-                const int nc = min(32, N - cb);
-                for (int i = 0; i < nc; ++i) {
-                    float x = v[i] + (g.bias ? g.bias[cb + i] : 0.f);
-                    if (g.C) g.C[(size_t)row * g.ldc + cb + i] = g.accumulate ? g.C[(size_t)row * g.ldc + cb + i] + x : x;
-                    if (g.O) g.O[(size_t)row * g.ldo + cb + i] = __float2bfloat16_rn(g.gelu ? gelu_tanh(x) : x);
+                const int nc = min(32, N - cb);   // 16 or 32
+#pragma unroll
+                for (int i = 0; i < 32; ++i) v[i] += (g.bias && i < nc) ? g.bias[cb + i] : 0.f;
+                if (g.C) {
+                    float4* cp = reinterpret_cast<float4*>(g.C + (size_t)row * g.ldc + cb);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        if (4 * q < nc) {
+                            float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                            if (g.accumulate) {
+                                const float4 o = cp[q];
+                                x.x += o.x; x.y += o.y; x.z += o.z; x.w += o.w;
+                            }
+                            cp[q] = x;
+                        }
+                    }
+                }
+                if (g.O) {
+                    uint4* op = reinterpret_cast<uint4*>(g.O + (size_t)row * g.ldo + cb);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (8 * q < nc) {
+                            uint32_t w[4];
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                const float a = g.gelu ? gelu_tanh(v[8 * q + 2 * e]) : v[8 * q + 2 * e];
+                                const float b = g.gelu ? gelu_tanh(v[8 * q + 2 * e + 1]) : v[8 * q + 2 * e + 1];
+                                const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
+                                w[e] = *reinterpret_cast<const uint32_t*>(&h2);
+                            }
+                            op[q] = make_uint4(w[0], w[1], w[2], w[3]);
+                        }
+                    }
                 }
             }
         }
@@ -131,8 +201,9 @@ int launch_gemm_bf16(GemmArgs g, cudaStream_t s) {
     if (g.K < 16 || g.K % 16) return fail(ISING_ERR_ARG, "GEMM K must be a positive multiple of 16");
     if (g.M < 1) return ISING_OK;
     if (g.conv_in) {
-        if (g.conv_C % 8 || g.K != 27 * g.conv_C || g.conv_Gi < 1 || g.conv_Go < 1)
-            return fail(ISING_ERR_ARG, "implicit convolution needs C % 8 == 0 and K = 27 C");
+        if ((g.conv_C != 8 && g.conv_C != 32) || g.K < 27 * g.conv_C || g.K > 27 * g.conv_C + 15 || g.conv_Gi < 1 ||
+            g.conv_Go < 1)
+            return fail(ISING_ERR_ARG, "implicit convolution needs C = 8 or 32 and K = 27 C rounded up to 16");
         if (reinterpret_cast<uintptr_t>(g.conv_in) & 15) return fail(ISING_ERR_ARG, "GEMM operands must be 16-byte aligned");
     } else {
         if (g.lda % 8 || g.lda < g.K) return fail(ISING_ERR_ARG, "GEMM row pitch must be >= K and a multiple of 8");
@@ -140,6 +211,10 @@ int launch_gemm_bf16(GemmArgs g, cudaStream_t s) {
     }
     if (g.ldb % 8 || g.ldb < g.K) return fail(ISING_ERR_ARG, "GEMM row pitch must be >= K and a multiple of 8");
     if (reinterpret_cast<uintptr_t>(g.B) & 15) return fail(ISING_ERR_ARG, "GEMM operands must be 16-byte aligned");
+    if (g.C && (g.ldc % 4 || g.ldc < g.N || (reinterpret_cast<uintptr_t>(g.C) & 15)))
+        return fail(ISING_ERR_ARG, "GEMM FP32 output needs a 16-byte aligned base and ldc % 4 == 0");
+    if (g.O && (g.ldo % 8 || g.ldo < g.N || (reinterpret_cast<uintptr_t>(g.O) & 15)))
+        return fail(ISING_ERR_ARG, "GEMM BF16 output needs a 16-byte aligned base and ldo % 8 == 0");
     g.tmem_cols = g.N <= 32 ? 32 : g.N <= 64 ? 64 : g.N <= 128 ? 128 : 256;
     // resident blocks per SM x TMEM columns must fit the SM's 512 columns: a block whose
     // allocation cannot be met would stall until another block frees its columns

@@ -6,8 +6,9 @@
 // after each, then a 1^3 head 32 -> 4 giving mu (3) and log sigma per patch site.
 // Activations are channel-last BF16 rows (one row per window voxel); each convolution is
 //     out[rows x 32] = im2col(in)[rows x 27*Cin] * Wf[32 x 27*Cin]^T + b      (tensor cores)
-// where the 32-channel layers gather im2col(in) inside the GEMM's loader (implicit GEMM) and
-// the 3-channel input layer and the weight gradients use materialised im2col matrices.
+// where im2col(in) is gathered inside the GEMM's loader (implicit GEMM; the 3 input channels
+// are padded to 8, one 16-byte piece per voxel) and only the weight gradients use
+// materialised (transposed) im2col matrices.
 // with column k = o * Cin + c, o = (dx*3 + dy)*3 + dz.  Backward: the data gradient of a
 // convolution is a convolution of the output gradient with the flipped, transposed kernel
 // (same im2col, weights WfT[ci][o'*32 + co] = W[co][ci][26 - o']); the weight gradient is
@@ -35,13 +36,13 @@
 namespace isg {
 
 constexpr int kCh = 32;
-constexpr int kK1 = 96;           // 27 * 3 = 81 padded to a multiple of 16
+constexpr int kC0 = 8;            // input channels padded to 8 (one 16-byte piece per voxel)
+constexpr int kK1 = 224;          // 27 * 8 = 216 padded to a multiple of 16
 constexpr int kK2 = 27 * kCh;     // 864
 constexpr int kK2Pad = 896;       // rows of the transposed im2col for weight gradients
 constexpr int kOffW1 = 0, kOffB1 = 2592, kOffW2 = 2624, kOffB2 = 30272, kOffW3 = 30304, kOffB3 = 57952,
               kOffWh = 57984, kOffBh = 58112, kNParams = 58116;
 
-static inline size_t pad128(size_t n) { return (n + 127) / 128 * 128; }
 static inline size_t pad32(size_t n) { return (n + 31) / 32 * 32; }
 
 __device__ __forceinline__ float gelu_f(float x) {
@@ -55,15 +56,18 @@ __device__ __forceinline__ float gelu_d(float x) {
 }
 
 // ---------------------------------------------------------------- layout kernels
-// windows [B][3][8][8][8] FP32 -> X0 rows [B*512][3] BF16
+// windows [B][3][8][8][8] FP32 -> X0 rows [B*512][8] BF16 (channels 3..7 zero)
 __global__ void k_windows_to_rows(const float* __restrict__ w, int nb, __nv_bfloat16* __restrict__ x0) {
-    const int64_t n = (int64_t)nb * 512 * 3;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t row = i / 3;
-        const int c = (int)(i - row * 3);
+    const int64_t n = (int64_t)nb * 512;
+    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x) {
         const int64_t b = row / 512;
         const int v = (int)(row - b * 512);
-        x0[i] = __float2bfloat16_rn(w[(b * 3 + c) * 512 + v]);
+        __nv_bfloat162 h[4];
+        h[0] = __floats2bfloat162_rn(w[(b * 3 + 0) * 512 + v], w[(b * 3 + 1) * 512 + v]);
+        h[1] = __floats2bfloat162_rn(w[(b * 3 + 2) * 512 + v], 0.f);
+        h[2] = __floats2bfloat162_rn(0.f, 0.f);
+        h[3] = h[2];
+        *reinterpret_cast<uint4*>(x0 + row * kC0) = *reinterpret_cast<const uint4*>(h);
     }
 }
 
@@ -95,33 +99,6 @@ __global__ void k_im2col(const __nv_bfloat16* __restrict__ in, int C, int Gi, in
     }
 }
 
-// im2col of the 3-channel input grid (8^3 -> 6^3, Kp = 96): one thread per row, the 81
-// values gathered into registers and stored as twelve 16-byte vectors
-__global__ void k_im2col_c3(const __nv_bfloat16* __restrict__ in, int64_t n_rows, __nv_bfloat16* __restrict__ out) {
-    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n_rows; row += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t b = row / 216;
-        const int u = (int)(row - b * 216);
-        const int x = u / 36, y = (u / 6) % 6, z = u % 6;
-        const __nv_bfloat16* base = in + (((b * 8 + x) * 8 + y) * 8 + z) * 3;
-        uint32_t w[48];
-#pragma unroll
-        for (int q = 0; q < 48; ++q) w[q] = 0u;
-#pragma unroll
-        for (int o = 0; o < 27; ++o) {
-            const int off = ((o / 9) * 64 + ((o / 3) % 3) * 8 + (o % 3)) * 3;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const int k = o * 3 + c;
-                const uint32_t h = __bfloat16_as_ushort(base[off + c]);
-                w[k >> 1] |= (k & 1) ? (h << 16) : h;
-            }
-        }
-        uint4* dst = reinterpret_cast<uint4*>(out + row * kK1);
-#pragma unroll
-        for (int q = 0; q < 12; ++q) dst[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
-    }
-}
-
 // BF16 operand matrices from the FP32 parameters
 __global__ void k_pack(const float* __restrict__ P, __nv_bfloat16* Wf1, __nv_bfloat16* Wf2, __nv_bfloat16* Wf3,
                        __nv_bfloat16* W2fT, __nv_bfloat16* W3fT) {
@@ -129,7 +106,8 @@ __global__ void k_pack(const float* __restrict__ P, __nv_bfloat16* Wf1, __nv_bfl
     if (i < kCh * kK1) {
         const int co = i / kK1, k = i % kK1;
         float v = 0.f;
-        if (k < 81) { const int o = k / 3, c = k % 3; v = P[kOffW1 + (co * 3 + c) * 27 + o]; }
+        const int o = k / kC0, c = k % kC0;
+        if (o < 27 && c < 3) v = P[kOffW1 + (co * 3 + c) * 27 + o];
         Wf1[i] = __float2bfloat16_rn(v);
     }
     if (i < kCh * kK2) {
@@ -258,12 +236,12 @@ __global__ void k_gelu_bwd(const float* __restrict__ dh, const float* __restrict
     }
 }
 
-// weight gradient rows C[k][co] (k = o*Cin + ci) -> G[W][co][ci][o]
-__global__ void k_scatter_wgrad(const float* __restrict__ Cm, int Cin, int off, float* __restrict__ G) {
+// weight gradient rows C[k][co] (k = o*stride + ci, ci < Cin) -> G[W][co][ci][o]
+__global__ void k_scatter_wgrad(const float* __restrict__ Cm, int Cin, int stride, int off, float* __restrict__ G) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 27 * Cin * kCh) return;
-    const int k = i / kCh, co = i % kCh, o = k / Cin, ci = k % Cin;
-    G[off + (co * Cin + ci) * 27 + o] += Cm[i];
+    const int co = i % kCh, j = i / kCh, o = j / Cin, ci = j % Cin;
+    G[off + (co * Cin + ci) * 27 + o] += Cm[(o * stride + ci) * kCh + co];
 }
 
 __global__ void k_adam(float* __restrict__ P, const float* __restrict__ G, float* __restrict__ m, float* __restrict__ v,
@@ -290,7 +268,7 @@ struct ising_net {
     float *P = nullptr, *G = nullptr, *M = nullptr, *V = nullptr;
     int adam_t = 0;
     __nv_bfloat16 *Wf1 = nullptr, *Wf2 = nullptr, *Wf3 = nullptr, *W2fT = nullptr, *W3fT = nullptr;
-    __nv_bfloat16 *X0 = nullptr, *A1 = nullptr, *H1 = nullptr, *H2 = nullptr, *H3 = nullptr;
+    __nv_bfloat16 *X0 = nullptr, *H1 = nullptr, *H2 = nullptr, *H3 = nullptr;
     float *pre1 = nullptr, *pre2 = nullptr, *pre3 = nullptr, *out = nullptr;
     float *dout = nullptr, *dh = nullptr, *Cw = nullptr;
     __nv_bfloat16 *dp = nullptr, *dpt = nullptr, *AT = nullptr;
@@ -317,7 +295,7 @@ int nalloc(T** p, size_t n) {
 }
 
 void net_free(ising_net* n) {
-    void* ptrs[] = {n->P, n->G, n->M, n->V, n->Wf1, n->Wf2, n->Wf3, n->W2fT, n->W3fT, n->X0, n->A1, n->H1,
+    void* ptrs[] = {n->P, n->G, n->M, n->V, n->Wf1, n->Wf2, n->Wf3, n->W2fT, n->W3fT, n->X0, n->H1,
                     n->H2, n->H3, n->pre1, n->pre2, n->pre3, n->out, n->dout, n->dh, n->Cw, n->dp, n->dpt,
                     n->AT, n->loss, n->status};
     for (void* p : ptrs) cudaFree(p);
@@ -343,28 +321,30 @@ GemmArgs gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, 
     return g;
 }
 
-// a 32-channel 3^3 convolution as an implicit GEMM: rows over the Go^3 output grid of every
-// window, A gathered from the channel-last input grid by the GEMM's loader
-GemmArgs conv_gemm(const __nv_bfloat16* in, int Gi, int Go, int pad, const __nv_bfloat16* W, int rows, int* st) {
+// a 3^3 convolution over C-channel (8 or 32) channel-last grids as an implicit GEMM: rows
+// over the Go^3 output grid of every window, A gathered by the GEMM's loader; K = 27 C
+// rounded up to a multiple of 16 (the extra columns are zero)
+GemmArgs conv_gemm(const __nv_bfloat16* in, int C, int Gi, int Go, int pad, const __nv_bfloat16* W, int K, int rows,
+                   int* st) {
     GemmArgs g{};
-    g.B = W; g.ldb = kK2; g.M = rows; g.N = kCh; g.K = kK2; g.status = st;
-    g.conv_in = in; g.conv_C = kCh; g.conv_Gi = Gi; g.conv_Go = Go; g.conv_pad = pad;
+    g.B = W; g.ldb = K; g.M = rows; g.N = kCh; g.K = K; g.status = st;
+    g.conv_in = in; g.conv_C = C; g.conv_Gi = Gi; g.conv_Go = Go; g.conv_pad = pad;
     return g;
 }
 
-// forward of nb windows already in X0; keeps pre-activations (for backward) and out
-int net_forward_rows(ising_net* n, int nb) {
+// forward of nb windows already in X0 into out; keep_pre also stores the FP32 pre-activations
+// that the backward pass needs
+int net_forward_rows(ising_net* n, int nb, bool keep_pre) {
     cudaStream_t s = n->stream;
     const int64_t R1 = (int64_t)nb * 216, R2 = (int64_t)nb * 64;
-    k_im2col_c3<<<grid_for(R1, 128), 128, 0, s>>>(n->X0, R1, n->A1);
-    GemmArgs g = gemm(n->A1, kK1, n->Wf1, kK1, (int)R1, kCh, kK1, n->status);
-    g.bias = n->P + kOffB1; g.C = n->pre1; g.ldc = kCh; g.O = n->H1; g.ldo = kCh; g.gelu = 1;
+    GemmArgs g = conv_gemm(n->X0, kC0, 8, 6, 0, n->Wf1, kK1, (int)R1, n->status);
+    g.bias = n->P + kOffB1; g.C = keep_pre ? n->pre1 : nullptr; g.ldc = kCh; g.O = n->H1; g.ldo = kCh; g.gelu = 1;
     ISG_TRY_N(launch_gemm_bf16(g, s));
-    g = conv_gemm(n->H1, 6, 4, 0, n->Wf2, (int)R2, n->status);
-    g.bias = n->P + kOffB2; g.C = n->pre2; g.ldc = kCh; g.O = n->H2; g.ldo = kCh; g.gelu = 1;
+    g = conv_gemm(n->H1, kCh, 6, 4, 0, n->Wf2, kK2, (int)R2, n->status);
+    g.bias = n->P + kOffB2; g.C = keep_pre ? n->pre2 : nullptr; g.ldc = kCh; g.O = n->H2; g.ldo = kCh; g.gelu = 1;
     ISG_TRY_N(launch_gemm_bf16(g, s));
-    g = conv_gemm(n->H2, 4, 4, 1, n->Wf3, (int)R2, n->status);
-    g.bias = n->P + kOffB3; g.C = n->pre3; g.ldc = kCh; g.O = n->H3; g.ldo = kCh; g.gelu = 1;
+    g = conv_gemm(n->H2, kCh, 4, 4, 1, n->Wf3, kK2, (int)R2, n->status);
+    g.bias = n->P + kOffB3; g.C = keep_pre ? n->pre3 : nullptr; g.ldc = kCh; g.O = n->H3; g.ldo = kCh; g.gelu = 1;
     ISG_TRY_N(launch_gemm_bf16(g, s));
     k_head_fwd<<<(int)((R2 + 127) / 128), 128, 0, s>>>(n->H3, R2, n->P, n->out);
     if (cudaGetLastError() != cudaSuccess) return cuda_fail(cudaGetLastError(), "network forward");
@@ -386,8 +366,8 @@ int net_backward(ising_net* n, const float* win, const float* tgt, int nb) {
     GemmArgs g = gemm(n->AT, (int)L2, n->dpt, (int)L2, kK2, kCh, (int)L2, n->status);
     g.C = n->Cw; g.ldc = kCh;
     ISG_TRY_N(launch_gemm_bf16(g, s));
-    k_scatter_wgrad<<<(27 * kCh * kCh + 255) / 256, 256, 0, s>>>(n->Cw, kCh, kOffW3, n->G);
-    g = conv_gemm(n->dp, 4, 4, 1, n->W3fT, (int)R2, n->status);
+    k_scatter_wgrad<<<(27 * kCh * kCh + 255) / 256, 256, 0, s>>>(n->Cw, kCh, kCh, kOffW3, n->G);
+    g = conv_gemm(n->dp, kCh, 4, 4, 1, n->W3fT, kK2, (int)R2, n->status);
     g.C = n->dh; g.ldc = kCh;
     ISG_TRY_N(launch_gemm_bf16(g, s));
     // conv2
@@ -396,17 +376,17 @@ int net_backward(ising_net* n, const float* win, const float* tgt, int nb) {
     g = gemm(n->AT, (int)L2, n->dpt, (int)L2, kK2, kCh, (int)L2, n->status);
     g.C = n->Cw; g.ldc = kCh;
     ISG_TRY_N(launch_gemm_bf16(g, s));
-    k_scatter_wgrad<<<(27 * kCh * kCh + 255) / 256, 256, 0, s>>>(n->Cw, kCh, kOffW2, n->G);
-    g = conv_gemm(n->dp, 4, 6, 2, n->W2fT, (int)R1, n->status);
+    k_scatter_wgrad<<<(27 * kCh * kCh + 255) / 256, 256, 0, s>>>(n->Cw, kCh, kCh, kOffW2, n->G);
+    g = conv_gemm(n->dp, kCh, 4, 6, 2, n->W2fT, kK2, (int)R1, n->status);
     g.C = n->dh; g.ldc = kCh;
     ISG_TRY_N(launch_gemm_bf16(g, s));
     // conv1
     k_gelu_bwd<<<grid_for(kCh * L1), 256, 0, s>>>(n->dh, n->pre1, R1, L1, n->dp, n->dpt, n->G + kOffB1);
-    k_im2col<<<grid_for((int64_t)128 * L1), 256, 0, s>>>(n->X0, 3, 8, 6, 0, R1, n->AT, kK1, 1, L1, 128);
-    g = gemm(n->AT, (int)L1, n->dpt, (int)L1, 81, kCh, (int)L1, n->status);
-    g.M = 81; g.C = n->Cw; g.ldc = kCh;
+    k_im2col<<<grid_for((int64_t)256 * L1), 256, 0, s>>>(n->X0, kC0, 8, 6, 0, R1, n->AT, kK1, 1, L1, 256);
+    g = gemm(n->AT, (int)L1, n->dpt, (int)L1, 27 * kC0, kCh, (int)L1, n->status);
+    g.C = n->Cw; g.ldc = kCh;
     ISG_TRY_N(launch_gemm_bf16(g, s));
-    k_scatter_wgrad<<<(27 * 3 * kCh + 255) / 256, 256, 0, s>>>(n->Cw, 3, kOffW1, n->G);
+    k_scatter_wgrad<<<(27 * 3 * kCh + 255) / 256, 256, 0, s>>>(n->Cw, 3, kC0, kOffW1, n->G);
     if (cudaGetLastError() != cudaSuccess) return cuda_fail(cudaGetLastError(), "network backward");
     return ISING_OK;
 }
@@ -437,22 +417,21 @@ extern "C" int ising_net_create(int device, int max_batch, uint64_t seed, ising_
     if (cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(cuda_fail(cudaGetLastError(), "cudaStreamCreateWithFlags"));
     const size_t B = (size_t)max_batch, R1 = B * 216, R2 = B * 64;
-    const size_t R1p = pad128(R1), L1 = pad32(R1);
+    const size_t L1 = pad32(R1);
     int st = ISING_OK;
     if ((st = nalloc(&n->P, kNParams)) || (st = nalloc(&n->G, kNParams)) || (st = nalloc(&n->M, kNParams)) ||
         (st = nalloc(&n->V, kNParams)) || (st = nalloc(&n->Wf1, kCh * kK1)) || (st = nalloc(&n->Wf2, kCh * kK2)) ||
         (st = nalloc(&n->Wf3, kCh * kK2)) || (st = nalloc(&n->W2fT, kCh * kK2)) || (st = nalloc(&n->W3fT, kCh * kK2)) ||
-        (st = nalloc(&n->X0, B * 512 * 3)) || (st = nalloc(&n->A1, R1p * kK1)) || (st = nalloc(&n->H1, R1 * kCh)) ||
+        (st = nalloc(&n->X0, B * 512 * kC0)) || (st = nalloc(&n->H1, R1 * kCh)) ||
         (st = nalloc(&n->H2, R2 * kCh)) ||
         (st = nalloc(&n->H3, R2 * kCh)) || (st = nalloc(&n->pre1, R1 * kCh)) || (st = nalloc(&n->pre2, R2 * kCh)) ||
         (st = nalloc(&n->pre3, R2 * kCh)) || (st = nalloc(&n->out, R2 * 4)) || (st = nalloc(&n->dout, R2 * 4)) ||
         (st = nalloc(&n->dh, R1 * kCh)) || (st = nalloc(&n->Cw, (size_t)kK2Pad * kCh)) ||
         (st = nalloc(&n->dp, R1 * kCh)) || (st = nalloc(&n->dpt, (size_t)kCh * L1)) ||
-        (st = nalloc(&n->AT, std::max((size_t)kK2Pad * pad32(R2), (size_t)128 * L1))) ||
+        (st = nalloc(&n->AT, std::max((size_t)kK2Pad * pad32(R2), (size_t)256 * L1))) ||
         (st = nalloc(&n->loss, 1)) || (st = nalloc(&n->status, 1)))
         return bail(st);
     // padding rows of the GEMM A operands stay zero
-    cudaMemset(n->A1, 0, R1p * kK1 * sizeof(__nv_bfloat16));
     cudaMemset(n->M, 0, kNParams * sizeof(float));
     cudaMemset(n->V, 0, kNParams * sizeof(float));
     cudaMemset(n->status, 0, sizeof(int));
@@ -508,8 +487,8 @@ extern "C" int ising_net_forward(ising_net* n, const float* d_windows, int nb, f
     if (!n || !d_windows || !d_out) return fail(ISING_ERR_ARG, "NULL argument");
     ISG_TRY(net_check_batch(n, nb));
     NetGuard guard(n->device);
-    k_windows_to_rows<<<grid_for((int64_t)nb * 1536), 256, 0, n->stream>>>(d_windows, nb, n->X0);
-    ISG_TRY(net_forward_rows(n, nb));
+    k_windows_to_rows<<<grid_for((int64_t)nb * 512), 256, 0, n->stream>>>(d_windows, nb, n->X0);
+    ISG_TRY(net_forward_rows(n, nb, false));
     ISG_CUDA(cudaMemcpyAsync(d_out, n->out, (size_t)nb * 64 * 4 * sizeof(float), cudaMemcpyDeviceToDevice, n->stream));
     return net_check(n);
 }
@@ -519,8 +498,8 @@ extern "C" int ising_net_loss_grad(ising_net* n, const float* d_windows, const f
     if (!n || !d_windows || !d_targets) return fail(ISING_ERR_ARG, "NULL argument");
     ISG_TRY(net_check_batch(n, nb));
     NetGuard guard(n->device);
-    k_windows_to_rows<<<grid_for((int64_t)nb * 1536), 256, 0, n->stream>>>(d_windows, nb, n->X0);
-    ISG_TRY(net_forward_rows(n, nb));
+    k_windows_to_rows<<<grid_for((int64_t)nb * 512), 256, 0, n->stream>>>(d_windows, nb, n->X0);
+    ISG_TRY(net_forward_rows(n, nb, true));
     ISG_TRY(net_backward(n, d_windows, d_targets, nb));
     double l = 0.0;
     ISG_CUDA(cudaMemcpyAsync(&l, n->loss, sizeof(double), cudaMemcpyDeviceToHost, n->stream));
@@ -536,8 +515,8 @@ extern "C" int ising_net_train_step(ising_net* n, const float* d_windows, const 
     ISG_TRY(net_check_batch(n, nb));
     if (!(lr > 0.0) || !std::isfinite(lr)) return fail(ISING_ERR_ARG, "learning rate must be positive");
     NetGuard guard(n->device);
-    k_windows_to_rows<<<grid_for((int64_t)nb * 1536), 256, 0, n->stream>>>(d_windows, nb, n->X0);
-    ISG_TRY(net_forward_rows(n, nb));
+    k_windows_to_rows<<<grid_for((int64_t)nb * 512), 256, 0, n->stream>>>(d_windows, nb, n->X0);
+    ISG_TRY(net_forward_rows(n, nb, true));
     ISG_TRY(net_backward(n, d_windows, d_targets, nb));
     ++n->adam_t;
     const float b1t = (float)std::pow(0.9, n->adam_t), b2t = (float)std::pow(0.999, n->adam_t);
@@ -556,8 +535,8 @@ int net_forward_on(ising_net* n, const float* d_windows, int nb, cudaStream_t s,
     if (nb < 1 || nb > n->max_batch) return fail(ISING_ERR_ARG, "window batch exceeds the network's max_batch");
     cudaStream_t keep = n->stream;
     n->stream = s;
-    k_windows_to_rows<<<grid_for((int64_t)nb * 1536), 256, 0, s>>>(d_windows, nb, n->X0);
-    const int st = net_forward_rows(n, nb);
+    k_windows_to_rows<<<grid_for((int64_t)nb * 512), 256, 0, s>>>(d_windows, nb, n->X0);
+    const int st = net_forward_rows(n, nb, false);
     n->stream = keep;
     *out = n->out;
     return st;

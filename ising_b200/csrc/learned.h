@@ -27,8 +27,8 @@ struct GemmArgs {
     int gelu;
     int* status;
     // implicit convolution: when conv_in is set, A is not read; A(row, k) = conv_in[b][u + o -
-    // conv_pad][c] for row = b*Go^3 + u, k = o*C + c (C % 8 == 0), zero outside the grid or
-    // for row >= M
+    // conv_pad][c] for row = b*Go^3 + u, k = o*C + c (C = 8 or 32), zero outside the grid, for
+    // o >= 27 or for row >= M
     const __nv_bfloat16* conv_in;
     int conv_C, conv_Gi, conv_Go, conv_pad;
     uint32_t tmem_cols;     // set by the launcher
