@@ -118,7 +118,7 @@ __device__ __forceinline__ void run_chunk(const EnsParams& P, uint32_t rep, uint
 }
 
 template <int MOVE, int DMI, bool HAS_K>
-__global__ void __launch_bounds__(kEnsMaxThreads, 3) k_ensembles(const __grid_constant__ EnsParams P) {
+__global__ void __launch_bounds__(kEnsMaxThreads, 4) k_ensembles(const __grid_constant__ EnsParams P) {
     __shared__ uint32_t s_task[5];
     __shared__ int s_go, s_fin;
     __shared__ float red[4][kEnsMaxThreads / 32];
