@@ -1469,8 +1469,9 @@ void ens_params(const ising_ensembles* s, int k, int rounds, int stall, EnsParam
         d.P = h.P;
         d.nch = h.nch;
         d.rb = (uint32_t)s->sched.block_threads / (d.g.W / 2u);
-        d.step_x = d.rb / (uint32_t)L.ny;
-        d.step_y = d.rb % (uint32_t)L.ny;
+        d.nseg = std::max(1u, std::min((uint32_t)L.ny, (d.rb + h.P - 1) / h.P));
+        d.seg_len = ((uint32_t)L.ny + d.nseg - 1) / d.nseg;
+        d.divSeg = make_div(d.nseg);
         d.n_rep = h.n;
         d.beta_rep = h.d_beta_rep;
         d.sweep_ctr = h.mesh->d_sweep;

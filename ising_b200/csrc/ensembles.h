@@ -24,8 +24,9 @@ struct EnsDev {
     FastDiv divTX;               // W / 2 lanes per packed row
     uint32_t P;                  // x-planes per chunk
     uint32_t nch;                // chunks per replica
-    uint32_t rb;                 // rows per block pass: threads / (W / 2)
-    uint32_t step_x, step_y;     // rb = step_x * ny + step_y
+    uint32_t rb;                 // thread rows per block: threads / (W / 2)
+    uint32_t nseg, seg_len;      // y-segments per plane in a task, rows per segment
+    FastDiv divSeg;              // by nseg
     int n_rep;                   // replicas 0..n_rep-1 (= temperature slots)
     double* beta_rep;
     uint32_t* sweep_ctr;         // the mesh's per-replica sweep counters

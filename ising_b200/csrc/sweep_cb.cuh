@@ -110,35 +110,20 @@ __device__ __forceinline__ void propose2(const float2* s, uint4 ra, uint4 rb, fl
     sp[0] = vx; sp[1] = vy; sp[2] = vz;
 }
 
+// Update of one site pair from its loaded neighbourhood: own pair s at entries (j, j+1) of
+// packed row `row` (parity p), the other colour's pairs px, mx (x +- 1), py, my (y +- 1) and
+// oz (same row) at entries (j, j+1), and the edge entry (ex, ey, ez) of that row.  The pair
+// is written back at own_off when either site accepts.
 template <int MOVE, int DMI, bool HAS_K>
-__device__ __forceinline__ void pair_update(const CbGeom& P, const uint32_t* rk, int* status,
-                                            float* __restrict__ sx, float* __restrict__ sy,
-                                            float* __restrict__ sz, uint32_t row, uint32_t x, uint32_t y,
-                                            uint32_t j, int colour, uint32_t sweep, uint32_t rep, float beta2,
-                                            v2& de, v2& dmx, v2& dmy, v2& dmz) {
+__device__ __forceinline__ void pair_compute(const CbGeom& P, const uint32_t* rk, int* status,
+                                             float* __restrict__ sx, float* __restrict__ sy,
+                                             float* __restrict__ sz, uint32_t own_off, uint32_t row,
+                                             uint32_t j, uint32_t p, const v23& s, const v23& px, const v23& mx,
+                                             const v23& py, const v23& my, const v23& oz, float ex, float ey,
+                                             float ez, uint32_t sweep, uint32_t rep, float beta2,
+                                             v2& de, v2& dmx, v2& dmy, v2& dmz) {
     const CbGeom& a = P;
     const HamDev& H = P.ham;
-    const uint32_t p = (x + y + (uint32_t)colour) & 1u;
-    const uint32_t own = (uint32_t)colour * P.half;
-    const uint32_t oth = (uint32_t)(colour ^ 1) * P.half;
-    const uint32_t rowW = row * P.W;
-    // neighbour rows of the other colour
-    const uint32_t xs = P.row_stride_x;
-    const uint32_t r_xp = x + 1 == (uint32_t)a.nx ? rowW - x * xs : rowW + xs;
-    const uint32_t r_xm = x == 0 ? rowW + ((uint32_t)a.nx - 1) * xs : rowW - xs;
-    const uint32_t r_yp = y + 1 == (uint32_t)a.ny ? rowW - y * P.W : rowW + P.W;
-    const uint32_t r_ym = y == 0 ? rowW + ((uint32_t)a.ny - 1) * P.W : rowW - P.W;
-
-    v23 s = ld3(sx, sy, sz, own + rowW + j);
-    const v23 px = ld3(sx, sy, sz, oth + r_xp + j);
-    const v23 mx = ld3(sx, sy, sz, oth + r_xm + j);
-    const v23 py = ld3(sx, sy, sz, oth + r_yp + j);
-    const v23 my = ld3(sx, sy, sz, oth + r_ym + j);
-    const v23 oz = ld3(sx, sy, sz, oth + rowW + j);
-    // edge entry of the other colour's row: j-1 (p = 0) or j+2 (p = 1), periodic in the row
-    const uint32_t je = p ? (j + 2 == P.W ? 0u : j + 2) : (j == 0 ? P.W - 1 : j - 1);
-    const uint32_t oe = oth + rowW + je;
-    const float ex = sx[oe], ey = sy[oe], ez = sz[oe];
     v23 zp, zm;
     if (p) {   // site z = 2j+1(+2): z+1 -> j+1 (j+2), z-1 -> j (j+1)
         zp = {make_float2(oz.x.y, ex), make_float2(oz.y.y, ey), make_float2(oz.z.y, ez)};
@@ -211,11 +196,44 @@ __device__ __forceinline__ void pair_update(const CbGeom& P, const uint32_t* rk,
     const v2 ny_ = make_float2(acc0 ? sp.y.x : s.y.x, acc1 ? sp.y.y : s.y.y);
     const v2 nz_ = make_float2(acc0 ? sp.z.x : s.z.x, acc1 ? sp.z.y : s.z.y);
     if (acc0 | acc1) {
-        const uint32_t o = own + rowW + j;
+        const uint32_t o = own_off;
         *reinterpret_cast<v2*>(sx + o) = nx_;
         *reinterpret_cast<v2*>(sy + o) = ny_;
         *reinterpret_cast<v2*>(sz + o) = nz_;
     }
+}
+
+template <int MOVE, int DMI, bool HAS_K>
+__device__ __forceinline__ void pair_update(const CbGeom& P, const uint32_t* rk, int* status,
+                                            float* __restrict__ sx, float* __restrict__ sy,
+                                            float* __restrict__ sz, uint32_t row, uint32_t x, uint32_t y,
+                                            uint32_t j, int colour, uint32_t sweep, uint32_t rep, float beta2,
+                                            v2& de, v2& dmx, v2& dmy, v2& dmz) {
+    const CbGeom& a = P;
+    const HamDev& H = P.ham;
+    const uint32_t p = (x + y + (uint32_t)colour) & 1u;
+    const uint32_t own = (uint32_t)colour * P.half;
+    const uint32_t oth = (uint32_t)(colour ^ 1) * P.half;
+    const uint32_t rowW = row * P.W;
+    // neighbour rows of the other colour
+    const uint32_t xs = P.row_stride_x;
+    const uint32_t r_xp = x + 1 == (uint32_t)a.nx ? rowW - x * xs : rowW + xs;
+    const uint32_t r_xm = x == 0 ? rowW + ((uint32_t)a.nx - 1) * xs : rowW - xs;
+    const uint32_t r_yp = y + 1 == (uint32_t)a.ny ? rowW - y * P.W : rowW + P.W;
+    const uint32_t r_ym = y == 0 ? rowW + ((uint32_t)a.ny - 1) * P.W : rowW - P.W;
+
+    v23 s = ld3(sx, sy, sz, own + rowW + j);
+    const v23 px = ld3(sx, sy, sz, oth + r_xp + j);
+    const v23 mx = ld3(sx, sy, sz, oth + r_xm + j);
+    const v23 py = ld3(sx, sy, sz, oth + r_yp + j);
+    const v23 my = ld3(sx, sy, sz, oth + r_ym + j);
+    const v23 oz = ld3(sx, sy, sz, oth + rowW + j);
+    // edge entry of the other colour's row: j-1 (p = 0) or j+2 (p = 1), periodic in the row
+    const uint32_t je = p ? (j + 2 == P.W ? 0u : j + 2) : (j == 0 ? P.W - 1 : j - 1);
+    const uint32_t oe = oth + rowW + je;
+    const float ex = sx[oe], ey = sy[oe], ez = sz[oe];
+    pair_compute<MOVE, DMI, HAS_K>(P, rk, status, sx, sy, sz, own + rowW + j, row, j, p, s, px, mx, py, my, oz,
+                                   ex, ey, ez, sweep, rep, beta2, de, dmx, dmy, dmz);
 }
 
 }  // namespace isg
