@@ -44,6 +44,8 @@ WORKLOADS = {
                desc="SC L=32 x 32 PT replicas, T 0.2-2.0, J=1, bulk D=0.5, B=0.2 z"),
     "c5": dict(L=96, R=48, tmin=0.1, tmax=1.5, J=-1.0, D=0.5, B=0.25, K=0.0, move="ball", r=0.2, k=10,
                desc="SC L=96 x 48 PT replicas, T 0.1-1.5, J=1, bulk D=0.5, B=0.25 z"),
+    "c1": dict(L=16, R=1, tmin=0.5, tmax=0.5, J=-1.0, D=0.3, B=0.1, K=0.0, move="uniform", r=0.0, k=1,
+               desc="SC L=16, T=0.5, J=1, bulk D=0.3, B=0.1, uniform unit-vector moves"),
     "c4": dict(L=96, R=64, tmin=0.1, tmax=2.0, J=-1.0, D=0.5, B=0.1, K=0.0, move="ball", r=0.2, k=10,
                desc="12 SC PT ensembles, L in {16,24,32,48,64,96} x2, (D,B) in {0.3,0.5,0.7}x{0.1,0.3}, "
                     "16-64 replicas, T 0.1-2.0, J=1, bulk DMI, B z",
@@ -373,6 +375,106 @@ def run_gpu(args, w):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- C1: GPU vs the CPU reference chain
+def run_c1(args):
+    """The reference's CPU-runnable configuration: SC L=16, T=0.5, J=1, bulk D=0.3, B=0.1,
+    K=0, fresh uniform unit-vector proposals, 1000 thermalisation + 5000 measurement sweeps
+    with E, |M| and Q (middle slice) sampled every `c1_every` sweeps.  At T=0.5 single chains
+    freeze into different metastable skyrmion states, so the comparison is between ensembles
+    of independent chains from uniform random spins: GPU (c1_gpu_chains replicas of one mesh,
+    FP32 sweeps) and the FP64 CPU restatement of the reference's sweep (oracle, c1_cpu_chains
+    chains).  Per chain: time averages of E/N, |M|, Q, C_v and chi; the ensemble means are
+    compared within 2 standard errors of the mean over chains."""
+    import numpy as np
+    import torch
+
+    import ising_b200 as ib
+    from ising_b200 import _lib
+    from oracle import oracle as O
+
+    L, beta, n_th, n_me, every = 16, 2.0, args.c1_therm, args.c1_meas, args.c1_every
+    N = L ** 3
+    R, RC = args.c1_gpu_chains, args.c1_cpu_chains
+    mesh = ib.ChainMesh.simple_cubic(L, n_replicas=R)
+    stream = torch.cuda.current_stream()
+    mesh.set_stream(stream.cuda_stream)
+    mesh.init_uniform(0x15196)
+    p = ib.params(J=-1.0, Dz=0.3, B=0.1, dmi="bulk", include_Jp=False)
+    pt = ib.ParallelTempering(mesh, np.full(R, beta), p, seed=0x15196, move=_lib.MOVE_UNIFORM)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    pt.relax(n_th)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_gpu = e0.elapsed_time(e1) / 1e3
+    gs = {"E": [], "M": [], "Q": []}
+    q = C.c_double()
+    for it in range(n_me // every):
+        pt.relax(every)
+        e, m = pt.energies()
+        gs["E"].append(e / N)
+        gs["M"].append(np.linalg.norm(m, axis=1) / N)
+        qq = []
+        for r in range(R):
+            _lib.call("ising_winding_number", mesh.handle, r, L // 2, C.byref(q))
+            qq.append(q.value)
+        gs["Q"].append(np.array(qq))
+    g = {k: np.array(v).T for k, v in gs.items()}             # [chain][sample]
+
+    O.build()
+    op = O.Params(J=-1.0, Dz=0.3, B=0.1, dmi_bulk=True)
+    col = O.checkerboard(L, L, L)
+    cs = {"E": [], "M": [], "Q": []}
+    t_cpu = 0.0
+    for ch in range(RC):
+        om = O.Mesh.sc(L)
+        om.init_uniform(0x15196 + 1 + ch)
+        key = O.SweepKey(seed=0x5EED + ch, ensemble=0, replica=0, move=0, r=0.0, philox_rounds=10)
+        E, M, Q = [], [], []
+        for sw in range(n_th + n_me):
+            ts = time.perf_counter()
+            om.colour_pass(col, 0, sw, beta, op, key)
+            om.colour_pass(col, 1, sw, beta, op, key)
+            t_cpu += time.perf_counter() - ts
+            if sw >= n_th and (sw - n_th + 1) % every == 0:
+                E.append(om.canonical_energy(op) / N)
+                M.append(float(np.linalg.norm(om.spins.sum(axis=0))) / N)
+                Q.append(om.winding_number(L // 2))
+        cs["E"].append(E); cs["M"].append(M); cs["Q"].append(Q)
+    c = {k: np.array(v) for k, v in cs.items()}
+
+    def per_chain(x):
+        return {"E": x["E"].mean(1), "M": x["M"].mean(1), "Q": x["Q"].mean(1),
+                "C_v": beta * beta * N * x["E"].var(1), "chi": beta * N * x["M"].var(1)}
+
+    pg, pc = per_chain(g), per_chain(c)
+    obs = {}
+    for name in ("E", "M", "Q", "C_v", "chi"):
+        a, b = pg[name], pc[name]
+        err = float(np.hypot(a.std(ddof=1) / np.sqrt(len(a)), b.std(ddof=1) / np.sqrt(len(b))))
+        obs[name] = {"gpu": float(a.mean()), "cpu": float(b.mean()), "err": err,
+                     "within_2sigma": bool(abs(a.mean() - b.mean()) <= 2 * err + 1e-12)}
+    value = n_th * N * R / t_gpu
+    cpu_rate = (n_th + n_me) * N * RC / t_cpu
+    line = {
+        "metric": "spin-updates/s", "value": value, "unit": "spin-updates/s", "n_gpus": 1, "steps": n_th,
+        "warmup": 0, "ms_per_step": 1e3 * t_gpu / n_th, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (uniform random initial spins)",
+        "config": {"workload": "c1", "desc": "SC L=16, T=0.5, J=1, bulk D=0.3, B=0.1, uniform unit-vector moves, "
+                   "1000 + 5000 sweeps", "gpu_chains": R, "cpu_chains": RC, "sample_every": every,
+                   "note": "value = GPU sweeps of all chains during thermalisation (launch-bound size)"},
+        "observables_vs_cpu_reference": obs,
+        "all_within_2sigma": all(v["within_2sigma"] for v in obs.values()),
+        "cpu_baseline": {"value": cpu_rate, "unit": "spin-updates/s", "cores": 1, "kind": "port",
+                         "sample": f"{RC} chains x {n_th + n_me} colour-class sweeps of SC L=16 in FP64 (oracle)"},
+        "roofline": None, "e2e": None, "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+    pt.close()
+    mesh.close()
+
+
 # ---------------------------------------------------------------- C5: learned vs plain
 def run_c5(args, w):
     """Learned patch proposal against plain Metropolis on the C5 ensemble (SC L=96, 48 PT
@@ -549,6 +651,11 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--learned", action="store_true", help="c5: learned patch proposal vs plain Metropolis")
+    ap.add_argument("--c1-therm", type=int, default=1000)
+    ap.add_argument("--c1-meas", type=int, default=5000)
+    ap.add_argument("--c1-every", type=int, default=10)
+    ap.add_argument("--c1-gpu-chains", type=int, default=32)
+    ap.add_argument("--c1-cpu-chains", type=int, default=8)
     ap.add_argument("--c5-plain", type=int, default=3000)
     ap.add_argument("--c5-learned", type=int, default=600)
     ap.add_argument("--c5-therm", type=int, default=5000)
@@ -565,6 +672,8 @@ def main():
         run_reference(args, w)
     elif args.learned:
         run_c5(args, WORKLOADS["c5"])
+    elif args.workload == "c1":
+        run_c1(args)
     else:
         run_gpu(args, w)
 
