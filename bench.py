@@ -475,6 +475,37 @@ def run_c1(args):
     mesh.close()
 
 
+# ---------------------------------------------------------------- patch-step timing
+def run_patch_probe(args, w):
+    """Times learned patch steps (one colour class on every replica) on an SC PT object of
+    the C5 Hamiltonian; --L / --replicas shrink it for profiling."""
+    import numpy as np
+    import torch
+
+    import ising_b200 as ib
+
+    L, R = args.L or w["L"], args.replicas or w["R"]
+    mesh = ib.ChainMesh.simple_cubic(L, n_replicas=R)
+    mesh.init_uniform(0x15196, 0)
+    p = ib.params(J=w["J"], Dz=w["D"], B=w["B"], dmi="bulk", include_Jp=False)
+    pt = ib.ParallelTempering(mesh, 1.0 / ib.temperature_ladder(w["tmin"], w["tmax"], R), p, seed=1)
+    net = ib.ProposalNet(max_batch=min(args.c5_batch, pt.patch_count()), seed=1)
+    pt.patch_set_scale(np.full(R, 0.3, np.float32), 0.25)
+    pt.patch_step(net, 0, (0, 0, 0))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    n = max(1, args.steps)
+    for i in range(n):
+        pt.patch_step(net, i % 8, (i % 4, 0, 0))
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / n
+    print(json.dumps({"metric": "patch-step time", "value": dt * 1e3, "unit": "ms", "windows": pt.patch_count(),
+                      "L": L, "replicas": R, "steps": n}), flush=True)
+    net.close()
+    pt.close()
+    mesh.close()
+
+
 # ---------------------------------------------------------------- C5: learned vs plain
 def run_c5(args, w):
     """Learned patch proposal against plain Metropolis on the C5 ensemble (SC L=96, 48 PT
@@ -651,6 +682,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--learned", action="store_true", help="c5: learned patch proposal vs plain Metropolis")
+    ap.add_argument("--patch-probe", action="store_true", help="time learned patch steps (C5 Hamiltonian)")
     ap.add_argument("--c1-therm", type=int, default=1000)
     ap.add_argument("--c1-meas", type=int, default=5000)
     ap.add_argument("--c1-every", type=int, default=10)
@@ -670,6 +702,8 @@ def main():
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, w)
+    elif args.patch_probe:
+        run_patch_probe(args, WORKLOADS["c5"])
     elif args.learned:
         run_c5(args, WORKLOADS["c5"])
     elif args.workload == "c1":
