@@ -229,3 +229,27 @@ def test_fortran_formats_match_consumer_rule(oracle):
     for T in (400.0, 612.3, 1234.5678, 20000.0):
         e = math.floor(math.log10(T)) + 1
         assert oracle.fmt_E0(T, 4) == f"{round(T / 10 ** e, 4):.4f}E+{e}"
+
+
+def test_philox_stream_statistics(oracle):
+    """The device's keyed Philox4x32-10 stream (same algorithm as the oracle's, replayed
+    decision for decision by the GPU parity tests): uniformity of the (0,1) floats over 64
+    bins, no lag-1 correlation along sites, independence of neighbouring keys (seeds) and of
+    the four words of one call."""
+    L = oracle.lib()
+    n = 40000
+    w = np.array([oracle.philox([i, 7, 3, (5 << 8) | 0], [0x15196, 0]) for i in range(n)], dtype=np.uint64)
+    w2 = np.array([oracle.philox([i, 7, 3, (5 << 8) | 0], [0x15197, 0]) for i in range(n)], dtype=np.uint64)
+    u = np.array([L.ora_u01(int(x)) for x in w[:, 0]])
+    h, _ = np.histogram(u, bins=64, range=(0.0, 1.0))
+    chi2 = ((h - n / 64) ** 2 / (n / 64)).sum()
+    assert chi2 < 120, chi2                       # 63 dof: mean 63, sd 11
+    lim = 5.0 / np.sqrt(n)
+    uf = (w.astype(np.float64) + 0.5) / 2.0 ** 32
+    uf2 = (w2.astype(np.float64) + 0.5) / 2.0 ** 32
+    assert abs(np.corrcoef(uf[:-1, 0], uf[1:, 0])[0, 1]) < lim
+    assert abs(np.corrcoef(uf[:, 0], uf2[:, 0])[0, 1]) < lim
+    for a in range(4):
+        for b in range(a + 1, 4):
+            assert abs(np.corrcoef(uf[:, a], uf[:, b])[0, 1]) < lim
+    assert abs(uf.mean() - 0.5) < 5 * np.sqrt(1 / 12 / (4 * n))
