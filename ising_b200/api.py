@@ -7,6 +7,7 @@ computes physics on the CPU.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import weakref
 from typing import Optional, Sequence
@@ -19,6 +20,23 @@ from ._lib import (CELL_BCC, CELL_HYPER_KAGOME, CELL_SC, DMI_BULK, DMI_INTERFACI
                    EnsSchedule, EnsemblesOptions, IsingError, MeshInfo, Params, PTOptions)
 
 _P = C.POINTER
+
+# Live native handles, closed in dependency order (networks and engines, PT objects, then
+# meshes) when the interpreter exits: finalisers that run later, in arbitrary order and after
+# the CUDA runtime has begun to shut down, must find nothing left to free.
+_LIVE = {"net": weakref.WeakSet(), "eng": weakref.WeakSet(), "pt": weakref.WeakSet(), "mesh": weakref.WeakSet()}
+
+
+def _close_all():
+    for kind in ("net", "eng", "pt", "mesh"):
+        for obj in list(_LIVE[kind]):
+            try:
+                obj.close()
+            except Exception:
+                pass
+
+
+atexit.register(_close_all)
 
 
 def _dp(a: np.ndarray):
@@ -92,6 +110,7 @@ class ChainMesh:
                   distance_threshold if distance_threshold else 0.0, numShells if numShells else 0,
                   n_replicas, device, C.byref(h))
         self._h = h
+        _LIVE["mesh"].add(self)
         info = MeshInfo()
         _lib.call("ising_mesh_get_info", h, C.byref(info))
         self.info = info
@@ -343,6 +362,7 @@ class ParallelTempering:
         _lib.call("ising_pt_create", mesh.handle, self.n, _dp(self.betas), C.byref(p), C.byref(o), C.byref(h))
         self._h = h
         mesh._depend(self)
+        _LIVE["pt"].add(self)
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
@@ -481,6 +501,7 @@ class Ensembles:
         self._h = h
         for mesh, *_ in self.members:
             mesh._depend(self)
+        _LIVE["eng"].add(self)
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
@@ -555,6 +576,7 @@ class ProposalNet:
         h = C.c_void_p()
         _lib.call("ising_net_create", device, max_batch, seed, C.byref(h))
         self._h = h
+        _LIVE["net"].add(self)
         self.max_batch = max_batch
         self.n_params = _lib.load().ising_net_param_count()
 
