@@ -219,7 +219,7 @@ def run_gpu(args, w):
     if args.engine == "ensembles":
         eng = ib.Ensembles(members, seed=0x15196, move=move, r=w["r"])
         eng.set_stream(stream.cuda_stream)
-        trials = eng.autotune(k, 1) if not args.no_autotune else []
+        trials = eng.autotune(k, 2) if not args.no_autotune else []
         eng.run(k, max(args.warmup, 1))
         run = lambda n: eng.run(k, n)
         energies = lambda: [eng.energies(i) for i in range(len(members))]

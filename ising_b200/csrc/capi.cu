@@ -1737,14 +1737,12 @@ extern "C" int ising_ensembles_autotune(ising_ensembles* s, int k, int rounds_pe
     int max_lanes = 0;
     for (auto& h : s->ens) max_lanes = std::max(max_lanes, h.mesh->lat.nz / 4);
     const int threads[] = {256, 128};
-    const int chunks[] = {2048, 4096, 8192};
+    const int chunks[] = {2048, 4096, 8192, 16384, 32768};
     for (int t : threads) {
         if (t < max_lanes) continue;
-        for (int c : chunks) {
-            cand.push_back({t, c, ISING_ENS_ORDER_PHASE, 0, 0.0});
-            cand.push_back({t, c, ISING_ENS_ORDER_GROUPS, 32000000, 0.0});
-            cand.push_back({t, c, ISING_ENS_ORDER_GROUPS, 64000000, 0.0});
-        }
+        for (int c : chunks) cand.push_back({t, c, ISING_ENS_ORDER_PHASE, 0, 0.0});
+        // replica groups of ~64 MB (one L2-resident group per round); slower so far, kept as a candidate
+        cand.push_back({t, 8192, ISING_ENS_ORDER_GROUPS, 64000000, 0.0});
     }
     cudaEvent_t e0, e1;
     ISG_CUDA(cudaEventCreate(&e0));

@@ -138,7 +138,7 @@ def test_autotune_picks_a_timed_schedule(ib, cuda_ok):
         spec.append((m, _betas(ib, n), _p(ib, D, B), ens))
     eng = ib.Ensembles(spec, seed=SEED)
     trials = eng.autotune(2, 1)
-    assert len(trials) >= 12
+    assert len(trials) >= 10
     assert all(t["ms_per_round"] > 0 for t in trials)
     best = min(trials, key=lambda t: t["ms_per_round"])
     s = eng.schedule()
