@@ -88,12 +88,8 @@ static __device__ __forceinline__ void finish_round(const EnsParams& P, const En
     for (int r = threadIdx.x; r < E.n_rep; r += blockDim.x) __stcg(E.sweep_ctr + r, __ldcg(E.sweep_ctr + r) + P.k);
 }
 
-// One task's colour pass over x-planes [x0, x1).  Each thread owns a pair of packed entries
-// (j, j+1) in a column of rows (x fixed) and marches along y over a segment of it: the
-// other colour's row (x, y+1) loaded for row y is also the z-neighbour row of y+1 and the
-// (y-1)-row of y+2, so a pair costs 15 loads (own, y+1 row, x +- 1 rows, one edge entry)
-// instead of 21.  Columns are (plane, y-segment), nseg segments per plane so that every
-// thread row is busy.
+// One task's colour pass over x-planes [x0, x1): columns (plane, y-segment), nseg segments
+// per plane so that every thread row is busy, each marched along y (march_column).
 template <int MOVE, int DMI, bool HAS_K, int EI>
 __device__ __forceinline__ void run_chunk(const EnsParams& P, uint32_t rep, uint32_t ph, uint32_t ch,
                                           v2& de, v2& dmx, v2& dmy, v2& dmz) {
@@ -105,40 +101,20 @@ __device__ __forceinline__ void run_chunk(const EnsParams& P, uint32_t rep, uint
     float* __restrict__ sx = E.spins + (size_t)rep * 3 * E.N;
     float* __restrict__ sy = sx + E.N;
     float* __restrict__ sz = sy + E.N;
-    const uint32_t ny = (uint32_t)G.ny, nx = (uint32_t)G.nx, W = G.W, xs = G.row_stride_x;
+    const uint32_t ny = (uint32_t)G.ny, nx = (uint32_t)G.nx;
     const uint32_t x0 = ch * E.P;
     const uint32_t np = min(x0 + E.P, nx) - x0;
     const uint32_t ty = fdiv(threadIdx.x, E.divTX);
     const uint32_t j = 2u * (threadIdx.x - ty * E.divTX.d);
     if (ty >= E.rb) return;
-    const uint32_t own = (uint32_t)colour * G.half, oth = (uint32_t)(colour ^ 1) * G.half;
 #pragma unroll 1
     for (uint32_t col = ty; col < np * E.nseg; col += E.rb) {
         const uint32_t xo = fdiv(col, E.divSeg), seg = col - xo * E.nseg;
         const uint32_t x = x0 + xo;
         const uint32_t ya = seg * E.seg_len, yb = min(ya + E.seg_len, ny);
         if (ya >= yb) continue;
-        const uint32_t pl = x * xs;
-        const uint32_t plp = x + 1 == nx ? 0u : pl + xs;
-        const uint32_t plm = x == 0 ? (nx - 1) * xs : pl - xs;
-        v23 prev = ld3(sx, sy, sz, oth + pl + (ya == 0 ? ny - 1 : ya - 1) * W + j);
-        v23 cur = ld3(sx, sy, sz, oth + pl + ya * W + j);
-#pragma unroll 1
-        for (uint32_t y = ya; y < yb; ++y) {
-            const uint32_t rw = y * W;
-            const v23 next = ld3(sx, sy, sz, oth + pl + (y + 1 == ny ? 0u : rw + W) + j);
-            const v23 s = ld3(sx, sy, sz, own + pl + rw + j);
-            const v23 px = ld3(sx, sy, sz, oth + plp + rw + j);
-            const v23 mx = ld3(sx, sy, sz, oth + plm + rw + j);
-            const uint32_t p = (x + y + (uint32_t)colour) & 1u;
-            const uint32_t je = p ? (j + 2 == W ? 0u : j + 2) : (j == 0 ? W - 1 : j - 1);
-            const uint32_t oe = oth + pl + rw + je;
-            const float ex = sx[oe], ey = sy[oe], ez = sz[oe];
-            pair_compute<MOVE, DMI, HAS_K>(G, P.rk, P.status, sx, sy, sz, own + pl + rw + j, x * ny + y, j, p, s, px,
-                                           mx, next, prev, cur, ex, ey, ez, sweep, rep, beta2, de, dmx, dmy, dmz);
-            prev = cur;
-            cur = next;
-        }
+        march_column<MOVE, DMI, HAS_K>(G, P.rk, P.status, sx, sy, sz, x, ya, yb, j, colour, sweep, rep, beta2, de, dmx,
+                                       dmy, dmz);
     }
 }
 

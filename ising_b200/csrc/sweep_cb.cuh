@@ -236,4 +236,40 @@ __device__ __forceinline__ void pair_update(const CbGeom& P, const uint32_t* rk,
                                    ex, ey, ez, sweep, rep, beta2, de, dmx, dmy, dmz);
 }
 
+
+// One thread's march along y over rows [ya, yb) of x-plane x at entry pair (j, j+1): the
+// other colour's row (x, y+1) loaded for row y is also the z-neighbour row of y+1 and the
+// (y-1)-row of y+2, so a pair costs 15 loads (own pair, y+1 row, x +- 1 rows, one edge entry)
+// instead of 21.
+template <int MOVE, int DMI, bool HAS_K>
+__device__ __forceinline__ void march_column(const CbGeom& G, const uint32_t* rk, int* status,
+                                             float* __restrict__ sx, float* __restrict__ sy,
+                                             float* __restrict__ sz, uint32_t x, uint32_t ya, uint32_t yb,
+                                             uint32_t j, int colour, uint32_t sweep, uint32_t rep, float beta2,
+                                             v2& de, v2& dmx, v2& dmy, v2& dmz) {
+    const uint32_t ny = (uint32_t)G.ny, nx = (uint32_t)G.nx, W = G.W, xs = G.row_stride_x;
+    const uint32_t own = (uint32_t)colour * G.half, oth = (uint32_t)(colour ^ 1) * G.half;
+    const uint32_t pl = x * xs;
+    const uint32_t plp = x + 1 == nx ? 0u : pl + xs;
+    const uint32_t plm = x == 0 ? (nx - 1) * xs : pl - xs;
+    v23 prev = ld3(sx, sy, sz, oth + pl + (ya == 0 ? ny - 1 : ya - 1) * W + j);
+    v23 cur = ld3(sx, sy, sz, oth + pl + ya * W + j);
+#pragma unroll 1
+    for (uint32_t y = ya; y < yb; ++y) {
+        const uint32_t rw = y * W;
+        const v23 next = ld3(sx, sy, sz, oth + pl + (y + 1 == ny ? 0u : rw + W) + j);
+        const v23 s = ld3(sx, sy, sz, own + pl + rw + j);
+        const v23 px = ld3(sx, sy, sz, oth + plp + rw + j);
+        const v23 mx = ld3(sx, sy, sz, oth + plm + rw + j);
+        const uint32_t p = (x + y + (uint32_t)colour) & 1u;
+        const uint32_t je = p ? (j + 2 == W ? 0u : j + 2) : (j == 0 ? W - 1 : j - 1);
+        const uint32_t oe = oth + pl + rw + je;
+        const float ex = sx[oe], ey = sy[oe], ez = sz[oe];
+        pair_compute<MOVE, DMI, HAS_K>(G, rk, status, sx, sy, sz, own + pl + rw + j, x * ny + y, j, p, s, px, mx,
+                                       next, prev, cur, ex, ey, ez, sweep, rep, beta2, de, dmx, dmy, dmz);
+        prev = cur;
+        cur = next;
+    }
+}
+
 }  // namespace isg
