@@ -6,7 +6,10 @@
 // 8 elements), K a multiple of 16, N a multiple of 16 up to 256; A holds ceil(M/128)*128
 // readable rows.  For a 3^3 convolution over an 8- or 32-channel grid A is not stored: the
 // loader gathers its 16-byte pieces from the channel-last input grid (implicit GEMM), zero
-// outside the grid; each thread owns one output row, decomposed once before the K loop.  One block of 128 threads computes a 128-row tile for all N columns:
+// outside the grid.  Blocks have 256 threads: two per tile row (each loads half of the row's
+// pieces of a K chunk, prefetched one chunk ahead in registers; the row is decomposed once
+// before the K loop), and in the epilogue the two warps of a TMEM lane quadrant split each
+// 32-column block.  One block computes a 128-row tile for all N columns:
 // chunks of 64 values of K are staged by all threads into a two-stage ring in the canonical
 // no-swizzle layout (umma.cuh), thread 0 issues the MMAs and commits them to the stage's
 // mbarrier, and the block refills a stage once that mbarrier reports its MMAs done.  The
@@ -21,7 +24,7 @@
 
 namespace isg {
 
-constexpr int kGemmThreads = 128;
+constexpr int kGemmThreads = 256;   // two threads per row of the 128-row tile
 constexpr int kGemmKC = 64;
 constexpr uint32_t kGemmWaitPolls = 1u << 22;
 
@@ -30,7 +33,7 @@ __device__ __forceinline__ float gelu_tanh(float x) {
     return 0.5f * x * (1.f + tanhf(u));
 }
 
-__global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const GemmArgs g) {
+__global__ void __launch_bounds__(kGemmThreads, 4) k_gemm_bf16(const GemmArgs g) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int N = g.N;
     const uint32_t a_bytes = 128u * kGemmKC * 2u;
@@ -55,7 +58,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const GemmArgs g) {
     int cx = 0, cy = 0, cz = 0;
     bool crow_ok = false;
     if (g.conv_in) {
-        const int row = m0 + tid, Go = g.conv_Go, Gi = g.conv_Gi;
+        const int row = m0 + (tid & 127), Go = g.conv_Go, Gi = g.conv_Gi;
         const int Go3 = Go * Go * Go;
         crow_ok = row < g.M;
         const int b = crow_ok ? row / Go3 : 0, u = crow_ok ? row - b * Go3 : 0;
@@ -69,50 +72,53 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const GemmArgs g) {
     // stored to shared memory, so they are in flight while chunk c's MMAs are issued and
     // the next stage is awaited.  A: this thread's row, 8 values per piece, q8 <= 8 pieces;
     // B: N x q8 pieces spread over the block (<= 16 per thread).
-    uint4 va[8], vb[16];
+    uint4 va[4], vb[8];
+    const int arow = tid & 127, ahalf = tid >> 7;   // this thread's A row and half of the pieces
     auto load_chunk = [&](int c) {
         const int kc0 = c * kGemmKC;
         const int q8 = min(kGemmKC, g.K - kc0) >> 3;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            va[j] = make_uint4(0u, 0u, 0u, 0u);
+        for (int i = 0; i < 4; ++i) {
+            const int j = ahalf + 2 * i;
+            va[i] = make_uint4(0u, 0u, 0u, 0u);
             if (j < q8) {
                 const int k = kc0 + 8 * j;
                 if (g.conv_in) {
-                    // implicit convolution: channels ch..ch+7 of kernel offset o of this
-                    // thread's output voxel (C = 32: four pieces per offset; C = 8: one)
+                    // implicit convolution: channels ch..ch+7 of kernel offset o of this row's voxel
                     const int o = C32 ? (k >> 5) : (k >> 3), ch = C32 ? (k & 31) : 0;
                     if (crow_ok && o < 27) {
                         const int x = cx + o / 9, y = cy + (o / 3) % 3, z = cz + o % 3;
                         const int Gi = g.conv_Gi;
                         if ((unsigned)x < (unsigned)Gi && (unsigned)y < (unsigned)Gi && (unsigned)z < (unsigned)Gi)
-                            va[j] = *reinterpret_cast<const uint4*>(cbase + (((int64_t)x * Gi + y) * Gi + z) * g.conv_C + ch);
+                            va[i] = *reinterpret_cast<const uint4*>(cbase + (((int64_t)x * Gi + y) * Gi + z) * g.conv_C + ch);
                     }
                 } else {
-                    va[j] = *reinterpret_cast<const uint4*>(g.A + (size_t)(m0 + tid) * g.lda + k);
+                    va[i] = *reinterpret_cast<const uint4*>(g.A + (size_t)(m0 + arow) * g.lda + k);
                 }
             }
         }
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int i = tid + j * kGemmThreads;
+        for (int jj = 0; jj < 8; ++jj) {
+            const int i = tid + jj * kGemmThreads;
             if (i < N * q8) {
                 const int r = i / q8, q = i - r * q8;
-                vb[j] = *reinterpret_cast<const uint4*>(g.B + (size_t)r * g.ldb + kc0 + 8 * q);
+                vb[jj] = *reinterpret_cast<const uint4*>(g.B + (size_t)r * g.ldb + kc0 + 8 * q);
             }
         }
     };
     auto store_chunk = [&](int c, unsigned char* sA, unsigned char* sB) {
         const int q8 = min(kGemmKC, g.K - c * kGemmKC) >> 3;
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-            if (j < q8) *reinterpret_cast<uint4*>(sA + umma_off(128, tid, 8 * j)) = va[j];
+        for (int i = 0; i < 4; ++i) {
+            const int j = ahalf + 2 * i;
+            if (j < q8) *reinterpret_cast<uint4*>(sA + umma_off(128, arow, 8 * j)) = va[i];
+        }
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int i = tid + j * kGemmThreads;
+        for (int jj = 0; jj < 8; ++jj) {
+            const int i = tid + jj * kGemmThreads;
             if (i < N * q8) {
                 const int r = i / q8, q = i - r * q8;
-                *reinterpret_cast<uint4*>(sB + umma_off(N, r, 8 * q)) = vb[j];
+                *reinterpret_cast<uint4*>(sB + umma_off(N, r, 8 * q)) = vb[jj];
             }
         }
     };
@@ -146,44 +152,41 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const GemmArgs g) {
     if (!ok) {
         if (tid == 0) atomicOr(g.status, kStatTimeout);
     } else {
-        // epilogue: each thread owns one output row; 16-byte stores (ldc % 4 == 0, ldo % 8 == 0)
-        const int row = m0 + warp * 32 + lane;
-        for (int cb = 0; cb < N; cb += 32) {
-            float v[32];
-            tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (one output row per thread) and the
+        // 16-column half w / 4 of every 32-column block; 16-byte stores (ldc % 4 == 0, ldo % 8 == 0)
+        const int quad = warp & 3, hcol = (warp >> 2) * 16;
+        const int row = m0 + quad * 32 + lane;
+        for (int cb = hcol; cb < N; cb += 32) {
+            float v[16];
+            tmem_ld16(taddr + ((uint32_t)(quad * 32) << 16) + (uint32_t)cb, v);
             if (row < g.M) {
-                const int nc = min(32, N - cb);   // 16 or 32
 #pragma unroll
-                for (int i = 0; i < 32; ++i) v[i] += (g.bias && i < nc) ? g.bias[cb + i] : 0.f;
+                for (int i = 0; i < 16; ++i) v[i] += g.bias ? g.bias[cb + i] : 0.f;
                 if (g.C) {
                     float4* cp = reinterpret_cast<float4*>(g.C + (size_t)row * g.ldc + cb);
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        if (4 * q < nc) {
-                            float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-                            if (g.accumulate) {
-                                const float4 o = cp[q];
-                                x.x += o.x; x.y += o.y; x.z += o.z; x.w += o.w;
-                            }
-                            cp[q] = x;
+                    for (int q = 0; q < 4; ++q) {
+                        float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                        if (g.accumulate) {
+                            const float4 o = cp[q];
+                            x.x += o.x; x.y += o.y; x.z += o.z; x.w += o.w;
                         }
+                        cp[q] = x;
                     }
                 }
                 if (g.O) {
                     uint4* op = reinterpret_cast<uint4*>(g.O + (size_t)row * g.ldo + cb);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        if (8 * q < nc) {
-                            uint32_t w[4];
+                    for (int q = 0; q < 2; ++q) {
+                        uint32_t w[4];
 #pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                const float a = g.gelu ? gelu_tanh(v[8 * q + 2 * e]) : v[8 * q + 2 * e];
-                                const float b = g.gelu ? gelu_tanh(v[8 * q + 2 * e + 1]) : v[8 * q + 2 * e + 1];
-                                const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
-                                w[e] = *reinterpret_cast<const uint32_t*>(&h2);
-                            }
-                            op[q] = make_uint4(w[0], w[1], w[2], w[3]);
+                        for (int e = 0; e < 4; ++e) {
+                            const float a = g.gelu ? gelu_tanh(v[8 * q + 2 * e]) : v[8 * q + 2 * e];
+                            const float b = g.gelu ? gelu_tanh(v[8 * q + 2 * e + 1]) : v[8 * q + 2 * e + 1];
+                            const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
+                            w[e] = *reinterpret_cast<const uint32_t*>(&h2);
                         }
+                        op[q] = make_uint4(w[0], w[1], w[2], w[3]);
                     }
                 }
             }
