@@ -41,6 +41,8 @@ extern "C" {
 #define ISING_ERR_ALLOC 7        /* device or host allocation failed */
 #define ISING_ERR_LATTICE 8      /* derivative list incomplete ("Unable to locate atoms",
                                     src/chainMesh.f90:1028) */
+#define ISING_ERR_CAPACITY 9     /* region-growth stack of 10000 rows full ("Stack array
+                                    capacity exceeded", rsp:611) */
 
 const char* ising_status_string(int status);
 const char* ising_last_error(void);
@@ -188,8 +190,43 @@ int ising_winding_all_slices(const ising_mesh* mesh, int replica, double* q_per_
 /* Replaces chainMesh_statistics (src/PT-Utils.f90:33-66) except the skyrmion count. */
 int ising_statistics(const ising_mesh* mesh, int replica, double* wnd_mid, double* wnd_spread,
                      double m[3]);
-/* Replaces calculate_winding_number_density (rsp:438-500): nx x ny column-major. */
+/* Replaces calculate_winding_number_density (rsp:438-500): nx x ny column-major, computed
+ * by the winding kernel in FP64 on the device. */
 int ising_winding_density(const ising_mesh* mesh, int replica, int z_1based, double* density);
+/* The densities of all nz slices in one launch and one download: nz consecutive nx x ny
+ * column-major slices (the loop of write_winding_number_density, rsp:560-571). */
+int ising_winding_density_all(const ising_mesh* mesh, int replica, double* density);
+
+/* ---------------------------------------------------------------- skyrmion counting */
+/* Fine-grid scale factors of makeChainMesh's sclx, scly (src/chainMesh.f90:745-773; default
+ * 10, each >= 2 or ISING_ERR_ARG). */
+int ising_mesh_set_interpolation_scale(ising_mesh* mesh, int sclx, int scly);
+int ising_mesh_interpolation_scale(const ising_mesh* mesh, int* sclx, int* scly);
+/* Replaces calculate_winding_density_interpolated (rsp:366-436): (sclx*nx) x (scly*ny)
+ * column-major density of slice z on the band-limited interpolation of the slice's
+ * first-atom spins (the reference's FFTW layout is not reproducible; see DESIGN). */
+int ising_winding_density_interpolated(const ising_mesh* mesh, int replica, int z_1based,
+                                       double* density);
+/* Replaces calculate_skyrmion_number(chainMesh, Z_index, q_threshold, particle_number,
+ * sigma) (rsp:627-812).  ISING_ERR_CAPACITY where the reference stops on a full stack. */
+int ising_skyrmion_number(const ising_mesh* mesh, int replica, int z_1based, double q_threshold,
+                          int particle_number, double sigma, int* skyrmion_number);
+/* Replaces compute_skyrmion_distribution(chainMesh, N, winding_array, min_threshold,
+ * max_threshold, num_thresholds, Z_index) (rsp:930-983): winding_array[N]. */
+int ising_skyrmion_distribution(const ising_mesh* mesh, int replica, int N, double min_threshold,
+                                double max_threshold, int num_thresholds, int z_1based,
+                                int* winding_array);
+/* Replaces chainMesh_statistics (src/PT-Utils.f90:33-66) including skyrmion_number_middle. */
+int ising_chain_mesh_statistics(const ising_mesh* mesh, int replica, int* skyrmion_number_middle,
+                                double* wnd_mid, double* wnd_spread, double m[3]);
+/* Replaces Gaussian_filter_2d(array, sigma) (rsp:814-859) on a host nx x ny column-major
+ * array (nx, ny >= 5), computed on the current device. */
+int ising_gaussian_filter_2d(double* array, int nx, int ny, double sigma);
+/* calculate_skyrmion_number after its interpolation step, on a caller-supplied fx x fy fine
+ * density; nx, ny are the coarse cell counts the reference wraps with. */
+int ising_skyrmion_number_density(const double* density, int fx, int fy, int nx, int ny,
+                                  double q_threshold, int particle_number, double sigma,
+                                  int* skyrmion_number);
 
 /* ---------------------------------------------------------------- parallel tempering */
 typedef struct ising_pt ising_pt;
@@ -321,7 +358,8 @@ int ising_write_spins_csv(const ising_mesh* mesh, int replica, const char* path,
 int ising_write_pt_data_csv(const char* path, double J, double D, double B, double T,
                             double wnd_mid, int sk_mid, double wnd_spread, const double m[3]);
 int ising_pt_file_tag(char* buf, size_t cap, double J, double D, double B, double T);
-/* write_winding_number_density (rsp:544-580): "x,y,z,Winding_Density" with F0.8. */
+/* write_winding_number_density (rsp:544-580): "x,y,z,Winding_Density" with F0.8; the
+ * densities come from one device pass, the records are formatted on all host threads. */
 int ising_write_winding_density_csv(const ising_mesh* mesh, int replica, const char* path);
 
 /* ---------------------------------------------------------------- learned patch proposal */

@@ -8,17 +8,23 @@ there is no CPU fallback.
 from . import _lib
 from ._lib import IsingError, Params, load
 from .api import (ChainMesh, Ensembles, ParallelTempering, ProposalNet, bcc_unit_cell, calculate_heisenberg_energy,
-                  calculate_winding_number2, calculate_winding_number_density, chain_mesh_statistics,
+                  calculate_skyrmion_number, calculate_winding_density_interpolated, calculate_winding_number2,
+                  calculate_winding_number_density, chain_mesh_statistics, chain_mesh_statistics_full,
+                  compute_skyrmion_distribution, gaussian_filter_2d, interpolation_scale, set_interpolation_scale,
+                  skyrmion_number_from_density,
                   hyper_kagome_unit_cell, local_energy_batch, make_chain_mesh, metropolis_mcs, observables,
                   params, pt_file_tag, reference_params, sc_unit_cell, temperature_ladder,
-                  total_heisenberg_energy, unit_cell, winding_all_slices, write_pt_data_csv,
-                  write_spins_to_file, write_winding_number_density)
+                  total_heisenberg_energy, unit_cell, winding_all_slices, winding_density_all_slices,
+                  write_pt_data_csv, write_spins_to_file, write_winding_number_density)
 
 __all__ = ["ChainMesh", "Ensembles", "ParallelTempering", "ProposalNet", "IsingError", "Params", "load", "bcc_unit_cell",
+           "calculate_skyrmion_number", "calculate_winding_density_interpolated", "chain_mesh_statistics_full",
+           "compute_skyrmion_distribution", "gaussian_filter_2d", "interpolation_scale", "set_interpolation_scale",
+           "skyrmion_number_from_density",
            "calculate_heisenberg_energy", "calculate_winding_number2", "calculate_winding_number_density",
            "chain_mesh_statistics", "hyper_kagome_unit_cell", "local_energy_batch", "make_chain_mesh",
            "metropolis_mcs", "observables", "params", "pt_file_tag", "reference_params", "sc_unit_cell",
            "temperature_ladder", "total_heisenberg_energy", "unit_cell", "winding_all_slices",
-           "write_pt_data_csv", "write_spins_to_file", "write_winding_number_density"]
+           "winding_density_all_slices", "write_pt_data_csv", "write_spins_to_file", "write_winding_number_density"]
 
 load()

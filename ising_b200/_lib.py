@@ -15,7 +15,8 @@ HEADER = os.path.join(HERE, "..", "include", "ising_gpu.h")
 
 ISING_OK = 0
 STATUS = {1: "ISING_ERR_ARG", 2: "ISING_ERR_NAN", 3: "ISING_ERR_BOUNDS", 4: "ISING_ERR_TIMEOUT",
-          5: "ISING_ERR_UNSUPPORTED", 6: "ISING_ERR_CUDA", 7: "ISING_ERR_ALLOC", 8: "ISING_ERR_LATTICE"}
+          5: "ISING_ERR_UNSUPPORTED", 6: "ISING_ERR_CUDA", 7: "ISING_ERR_ALLOC", 8: "ISING_ERR_LATTICE",
+          9: "ISING_ERR_CAPACITY"}
 
 CELL_SC, CELL_BCC, CELL_HYPER_KAGOME = 0, 1, 2
 DMI_INTERFACIAL, DMI_BULK = 0, 1
@@ -98,6 +99,15 @@ _SIGS = {
     "ising_winding_all_slices": (_i, [_vp, _i, _P(_d)]),
     "ising_statistics": (_i, [_vp, _i, _P(_d), _P(_d), _P(_d)]),
     "ising_winding_density": (_i, [_vp, _i, _i, _P(_d)]),
+    "ising_winding_density_all": (_i, [_vp, _i, _P(_d)]),
+    "ising_mesh_set_interpolation_scale": (_i, [_vp, _i, _i]),
+    "ising_mesh_interpolation_scale": (_i, [_vp, _P(_i), _P(_i)]),
+    "ising_winding_density_interpolated": (_i, [_vp, _i, _i, _P(_d)]),
+    "ising_skyrmion_number": (_i, [_vp, _i, _i, _d, _i, _d, _P(_i)]),
+    "ising_skyrmion_distribution": (_i, [_vp, _i, _i, _d, _d, _i, _i, _P(_i)]),
+    "ising_chain_mesh_statistics": (_i, [_vp, _i, _P(_i), _P(_d), _P(_d), _P(_d)]),
+    "ising_gaussian_filter_2d": (_i, [_P(_d), _i, _i, _d]),
+    "ising_skyrmion_number_density": (_i, [_P(_d), _i, _i, _i, _i, _d, _i, _d, _P(_i)]),
     "ising_pt_create": (_i, [_vp, _i, _P(_d), _P(Params), _P(PTOptions), _P(_vp)]),
     "ising_pt_destroy": (_i, [_vp]),
     "ising_pt_run": (_i, [_vp, _i, _i]),

@@ -295,6 +295,80 @@ def calculate_winding_number_density(mesh: ChainMesh, Z_index: int, replica: int
     return out.reshape(mesh.numCellsY, mesh.numCellsX).T
 
 
+def winding_density_all_slices(mesh: ChainMesh, replica: int = 0) -> np.ndarray:
+    """The densities of every z slice in one launch: (numCellsX, numCellsY, numCellsZ) array,
+    slice z-1 equal to calculate_winding_number_density(mesh, z)."""
+    out = np.empty(mesh.numCellsX * mesh.numCellsY * mesh.numCellsZ)
+    _lib.call("ising_winding_density_all", mesh.handle, replica, _dp(out))
+    return out.reshape(mesh.numCellsZ, mesh.numCellsY, mesh.numCellsX).transpose(2, 1, 0)
+
+
+def set_interpolation_scale(mesh: ChainMesh, sclx: int = 10, scly: int = 10):
+    """makeChainMesh's sclx, scly (src/chainMesh.f90:745-773): fine grid = (sclx*nx, scly*ny)."""
+    _lib.call("ising_mesh_set_interpolation_scale", mesh.handle, int(sclx), int(scly))
+
+
+def interpolation_scale(mesh: ChainMesh):
+    sx, sy = C.c_int(0), C.c_int(0)
+    _lib.call("ising_mesh_interpolation_scale", mesh.handle, C.byref(sx), C.byref(sy))
+    return sx.value, sy.value
+
+
+def calculate_winding_density_interpolated(mesh: ChainMesh, z_index: int, replica: int = 0) -> np.ndarray:
+    """calculate_winding_density_interpolated (rsp:366-436): (sclx*numCellsX, scly*numCellsY)."""
+    sx, sy = interpolation_scale(mesh)
+    fx, fy = sx * mesh.numCellsX, sy * mesh.numCellsY
+    out = np.empty(fx * fy)
+    _lib.call("ising_winding_density_interpolated", mesh.handle, replica, z_index, _dp(out))
+    return out.reshape(fy, fx).T
+
+
+def calculate_skyrmion_number(mesh: ChainMesh, Z_index: int, q_threshold: float, particle_number: int,
+                              sigma: float, replica: int = 0) -> int:
+    """calculate_skyrmion_number (rsp:627-812)."""
+    out = C.c_int(0)
+    _lib.call("ising_skyrmion_number", mesh.handle, replica, Z_index, float(q_threshold), int(particle_number),
+              float(sigma), C.byref(out))
+    return out.value
+
+
+def compute_skyrmion_distribution(mesh: ChainMesh, N: int, min_threshold: float, max_threshold: float,
+                                  num_thresholds: int, Z_index: int, replica: int = 0) -> np.ndarray:
+    """compute_skyrmion_distribution (rsp:930-983): counts of particles with charge 1..N."""
+    out = np.zeros(N, dtype=np.int32)
+    _lib.call("ising_skyrmion_distribution", mesh.handle, replica, int(N), float(min_threshold),
+              float(max_threshold), int(num_thresholds), int(Z_index), out.ctypes.data_as(C.POINTER(C.c_int)))
+    return out
+
+
+def gaussian_filter_2d(array: np.ndarray, sigma: float) -> np.ndarray:
+    """Gaussian_filter_2d (rsp:814-859) of a 2-D array (returns the filtered copy)."""
+    a = np.asfortranarray(np.array(array, dtype=np.float64))
+    _lib.call("ising_gaussian_filter_2d", a.ctypes.data_as(C.POINTER(C.c_double)), a.shape[0], a.shape[1],
+              float(sigma))
+    return a
+
+
+def skyrmion_number_from_density(density: np.ndarray, numCellsX: int, numCellsY: int, q_threshold: float,
+                                 particle_number: int, sigma: float) -> int:
+    """calculate_skyrmion_number after its interpolation step, on a given fine density."""
+    a = np.asfortranarray(np.asarray(density, dtype=np.float64))
+    out = C.c_int(0)
+    _lib.call("ising_skyrmion_number_density", a.ctypes.data_as(C.POINTER(C.c_double)), a.shape[0], a.shape[1],
+              int(numCellsX), int(numCellsY), float(q_threshold), int(particle_number), float(sigma), C.byref(out))
+    return out.value
+
+
+def chain_mesh_statistics_full(mesh: ChainMesh, replica: int = 0):
+    """chainMesh_statistics (src/PT-Utils.f90:33-66): (skyrmion_number_middle,
+    winding_number_middle, winding_number_spread, magnetisation[3])."""
+    sk = C.c_int(0)
+    wm, ws = C.c_double(0), C.c_double(0)
+    m = np.zeros(3)
+    _lib.call("ising_chain_mesh_statistics", mesh.handle, replica, C.byref(sk), C.byref(wm), C.byref(ws), _dp(m))
+    return sk.value, wm.value, ws.value, m
+
+
 def chain_mesh_statistics(mesh: ChainMesh, replica: int = 0):
     """chainMesh_statistics (src/PT-Utils.f90:33-66) without the skyrmion count:
     (winding_number_middle, winding_number_spread, magnetisation[3])."""

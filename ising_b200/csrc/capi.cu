@@ -43,6 +43,7 @@ extern "C" const char* ising_status_string(int s) {
         case ISING_ERR_CUDA: return "CUDA error";
         case ISING_ERR_ALLOC: return "allocation failed";
         case ISING_ERR_LATTICE: return "lattice error";
+        case ISING_ERR_CAPACITY: return "stack capacity exceeded";
         default: return "unknown status";
     }
 }
@@ -461,6 +462,7 @@ extern "C" int ising_mesh_destroy(ising_mesh* m) {
     cudaFree(m->d_spins); cudaFree(m->d_sweep); cudaFree(m->d_scratch); cudaFree(m->d_status);
     cudaFree(m->d_staging); cudaFree(m->d_beta); cudaFree(m->d_winding_tmp); cudaFree(m->d_slots); cudaFree(m->d_slot_count);
     cudaFree(m->d_plaq);
+    isg::skyrmion_release(m);
     for (auto& c : m->colour) cudaFree(c.d_sites);
     if (m->h_pinned) cudaFreeHost(m->h_pinned);
     if (m->own_stream) cudaStreamDestroy(m->own_stream);
@@ -782,47 +784,40 @@ extern "C" int ising_statistics(const ising_mesh* m, int replica, double* wnd_mi
     return ISING_OK;
 }
 
-// plaquette density (rsp:438-500) computed on the host from downloaded spins
-extern "C" int ising_winding_density(const ising_mesh* m, int replica, int z1, double* dens) {
+// plaquette densities (rsp:438-500) of slices z0 .. z0+nzc-1 from k_winding in FP64, written
+// column-major per slice (x fastest) into the staging buffer (cells <= atoms < 3N doubles) and
+// downloaded once
+namespace {
+int winding_density_range(const ising_mesh* mc, int replica, int z0, int nzc, double* dens) {
+    ising_mesh* m = const_cast<ising_mesh*>(mc);
     ISG_TRY(check_replica(m, replica));
-    if (z1 < 1 || z1 > m->lat.nz) return fail(ISING_ERR_BOUNDS, "Z_index out of bounds");
     if (!dens) return fail(ISING_ERR_ARG, "density is NULL");
+    DeviceGuard g(m->device);
     const Lattice& L = m->lat;
-    std::vector<double> s((size_t)3 * L.natoms);
-    ISG_TRY(ising_spins_get(m, replica, s.data()));
-    const int64_t N = L.natoms;
-    auto unit = [&](int64_t j, double* o) {
-        const double x = s[j], y = s[N + j], z = s[2 * N + j];
-        const double n = std::sqrt(x * x + y * y + z * z);
-        o[0] = x / n; o[1] = y / n; o[2] = z / n;
-    };
-    auto arc = [](const double* s1, const double* s2, const double* s3) {
-        const double d12 = s1[0] * s2[0] + s1[1] * s2[1] + s1[2] * s2[2];
-        const double d23 = s2[0] * s3[0] + s2[1] * s3[1] + s2[2] * s3[2];
-        const double d31 = s3[0] * s1[0] + s3[1] * s1[1] + s3[2] * s1[2];
-        const double cx = s2[1] * s3[2] - s2[2] * s3[1], cy = s2[2] * s3[0] - s2[0] * s3[2],
-                     cz = s2[0] * s3[1] - s2[1] * s3[0];
-        double re = 1.0 + d12 + d23 + d31, im = s1[0] * cx + s1[1] * cy + s1[2] * cz;
-        const double nrm = std::sqrt(2.0 * (1.0 + d12) * (1.0 + d23) * (1.0 + d31));
-        re /= nrm; im /= nrm;
-        return 2.0 * std::atan2(im, re);
-    };
-    const int s1sub = L.nsub - 1;
-    const NbrSlot& a2 = L.deriv[s1sub * 6 + 1];
-    const NbrSlot& a4 = L.deriv[a2.sub * 6 + 3];
-    const NbrSlot& a3 = L.deriv[s1sub * 6 + 3];
-    const double four_pi = 4.0 * (double)3.14159265358979323846f;
-    for (int i = 0; i < L.nx; ++i)
-        for (int j = 0; j < L.ny; ++j) {
-            const int64_t b1 = L.atom_of(i, j, z1 - 1, s1sub);
-            const int64_t b2 = L.neighbour_atom(b1, a2);
-            const int64_t b4 = L.neighbour_atom(b2, a4);
-            const int64_t b3 = L.neighbour_atom(b1, a3);
-            double v1[3], v2[3], v3[3], v4[3];
-            unit(b1, v1); unit(b2, v2); unit(b3, v3); unit(b4, v4);
-            dens[i + (int64_t)j * L.nx] = (arc(v1, v2, v4) + arc(v1, v4, v3)) / four_pi;
-        }
+    double* d = nullptr;
+    ISG_TRY(staging(m, &d));
+    WindingLaunch w{};
+    w.spins = m->d_spins + (int64_t)replica * 3 * L.natoms;
+    w.natoms = L.natoms; w.nx = L.nx; w.ny = L.ny; w.nz = L.nz; w.nsub = L.nsub; w.n_rep = 1;
+    w.plaq = m->d_plaq; w.layout = m->layout; w.out = m->d_winding_tmp; w.fp64 = 1;
+    w.dens = d; w.z0 = z0; w.nzc = nzc;
+    ISG_TRY(launch_winding(w, m->stream));
+    const size_t n = (size_t)L.nx * L.ny * nzc;
+    ISG_CUDA(cudaMemcpyAsync(dens, d, n * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    ISG_CUDA(cudaStreamSynchronize(m->stream));
     return ISING_OK;
+}
+}  // namespace
+
+extern "C" int ising_winding_density(const ising_mesh* m, int replica, int z1, double* dens) {
+    if (!m) return fail(ISING_ERR_ARG, "mesh is NULL");
+    if (z1 < 1 || z1 > m->lat.nz) return fail(ISING_ERR_BOUNDS, "Z_index out of bounds");
+    return winding_density_range(m, replica, z1 - 1, 1, dens);
+}
+
+extern "C" int ising_winding_density_all(const ising_mesh* m, int replica, double* dens) {
+    if (!m) return fail(ISING_ERR_ARG, "mesh is NULL");
+    return winding_density_range(m, replica, 0, m->lat.nz, dens);
 }
 
 // ======================================================================= parallel tempering

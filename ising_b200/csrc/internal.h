@@ -103,7 +103,14 @@ struct ising_mesh {
     isg::Slot* d_slots = nullptr;
     int* d_slot_count = nullptr;
     int* d_plaq = nullptr;               // winding plaquette offsets (4 x {dx,dy,sub})
+    int sclx = 10, scly = 10;            // fine-grid scale factors (makeChainMesh defaults)
+    void* sky = nullptr;                 // skyrmion-counting workspace, made on first use
 };
+
+namespace isg {
+// Frees the skyrmion-counting workspace of a mesh (called by ising_mesh_destroy).
+void skyrmion_release(ising_mesh* m);
+}  // namespace isg
 
 namespace isg {
 constexpr int kScratchDoubles = 1 << 16;
@@ -191,6 +198,8 @@ struct WindingLaunch {
     Layout layout;
     double* out;           // [rep][nz]
     int fp64;
+    double* dens;          // optional plaquette densities [rep][slice][ny][nx] (nx fastest), or NULL
+    int z0, nzc;           // slices z0 .. z0+nzc-1 (nzc == 0: all nz slices)
 };
 int launch_winding(const WindingLaunch& a, cudaStream_t s);
 

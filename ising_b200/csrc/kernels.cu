@@ -7,6 +7,7 @@
 
 #include "internal.h"
 #include "exchange.cuh"
+#include "winding.cuh"
 
 namespace isg {
 
@@ -221,32 +222,12 @@ int launch_fold_partials(double* partials, int slots_per_rep, int n_rep, Acc4* a
 // arc_winding rsp:284-318): plaquette (s1, s1+a, s1+b, s1+a+b) from the derivative list,
 // triangles (s1,s2,s4) and (s1,s4,s3), divided by 4*pi (pi as the reference's
 // default-real literal).
-template <typename T>
-__device__ __forceinline__ T arc_winding_t(const T* s1, const T* s2, const T* s3) {
-    const T d12 = s1[0] * s2[0] + s1[1] * s2[1] + s1[2] * s2[2];
-    const T d23 = s2[0] * s3[0] + s2[1] * s3[1] + s2[2] * s3[2];
-    const T d31 = s3[0] * s1[0] + s3[1] * s1[1] + s3[2] * s1[2];
-    const T cx = s2[1] * s3[2] - s2[2] * s3[1];
-    const T cy = s2[2] * s3[0] - s2[0] * s3[2];
-    const T cz = s2[0] * s3[1] - s2[1] * s3[0];
-    T re = T(1) + d12 + d23 + d31;
-    T im = s1[0] * cx + s1[1] * cy + s1[2] * cz;
-    const T nrm = sqrt(T(2) * (T(1) + d12) * (T(1) + d23) * (T(1) + d31));
-    re = re / nrm;
-    im = im / nrm;
-    return T(2) * atan2(im, re);
-}
-
-template <typename T>
-__device__ __forceinline__ void load_unit(const float* sx, const float* sy, const float* sz, int64_t j, T* o) {
-    const T x = (T)sx[j], y = (T)sy[j], z = (T)sz[j];
-    const T n = sqrt(x * x + y * y + z * z);
-    o[0] = x / n; o[1] = y / n; o[2] = z / n;
-}
-
+// One block per (slice, replica). With a.dens set, every plaquette also stores its density
+// (calculate_winding_number_density, rsp:438-500): density_matrix(i,j) column-major per slice,
+// which the x-fastest plaquette order writes coalesced.
 template <typename T>
 __global__ void __launch_bounds__(256) k_winding(WindingLaunch a) {
-    const int zc = blockIdx.x;
+    const int zc = a.z0 + blockIdx.x;
     const int rep = blockIdx.y;
     const int64_t N = a.natoms;
     const float* sx = a.spins + (int64_t)rep * 3 * N;
@@ -255,8 +236,9 @@ __global__ void __launch_bounds__(256) k_winding(WindingLaunch a) {
     const int* P = a.plaq;  // 4 x (dx, dy, dz, sub): s1, s2, s4, s3
     T w = T(0);
     const int np = a.nx * a.ny;
+    double* dn = a.dens ? a.dens + ((int64_t)rep * gridDim.x + blockIdx.x) * np : nullptr;
     for (int p = threadIdx.x; p < np; p += blockDim.x) {
-        const int i = p / a.ny, j = p % a.ny;
+        const int i = p % a.nx, j = p / a.nx;
         int64_t at[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -269,7 +251,9 @@ __global__ void __launch_bounds__(256) k_winding(WindingLaunch a) {
         load_unit<T>(sx, sy, sz, at[1], s2);
         load_unit<T>(sx, sy, sz, at[2], s4);
         load_unit<T>(sx, sy, sz, at[3], s3);
-        w += arc_winding_t<T>(s1, s2, s4) + arc_winding_t<T>(s1, s4, s3);
+        const T pl = arc_winding_t<T>(s1, s2, s4) + arc_winding_t<T>(s1, s4, s3);
+        w += pl;
+        if (dn) dn[p] = (double)pl / (4.0 * (double)3.14159265358979323846f);
     }
     __shared__ double tot[4];
     block_sum4<double>((double)w, 0.0, 0.0, 0.0, tot);
@@ -280,7 +264,9 @@ __global__ void __launch_bounds__(256) k_winding(WindingLaunch a) {
 }
 
 int launch_winding(const WindingLaunch& a, cudaStream_t s) {
-    dim3 g(a.nz, a.n_rep);
+    const int nzc = a.nzc > 0 ? a.nzc : a.nz;
+    if (a.z0 < 0 || a.z0 + nzc > a.nz) return fail(ISING_ERR_BOUNDS, "winding slice range out of bounds");
+    dim3 g(nzc, a.n_rep);
     if (a.fp64) k_winding<double><<<g, 256, 0, s>>>(a);
     else k_winding<float><<<g, 256, 0, s>>>(a);
     ISG_CUDA(cudaGetLastError());

@@ -688,6 +688,217 @@ void ora_statistics(const ora_mesh* m, double* wnd_mid, double* wnd_spread, doub
     for (int d = 0; d < 3; ++d) mag[d] = s[d] / (double)m->natoms;
 }
 
+/* ======================= skyrmion counting ======================= */
+/* Fine-grid arrays are column-major (first index fastest), 1-based in the comments as in the
+ * reference.  The summations below are written without fused multiply-adds so that their
+ * rounding is defined by the order alone. */
+#define IDX2(a, i, j, ld) (a)[((long)(i) - 1) + ((long)(j) - 1) * (long)(ld)]
+
+/* Gaussian_filter_2d (rsp:814-859): 5x5 kernel exp(-(di^2+dj^2)/(2 sigma^2)) normalised by
+ * its sum; buffer(i,j) = sum_{l,m=1..5} array(i-l, j-m) G(l,m) with periodic indices
+ * (index 0 -> Nx, -k -> Nx-k), l outer and m inner.  The output is shifted by 3 cells
+ * against a centred filter, as in the reference.  Requires nx, ny >= 5. */
+__attribute__((optimize("fp-contract=off")))
+void ora_gaussian_kernel(double sigma, double G[25])
+{
+    const int k = 2;
+    double acc = 0.0;
+    for (int i = 1; i <= 2 * k + 1; ++i)
+        for (int j = 1; j <= 2 * k + 1; ++j) {
+            const int num = (i - k - 1) * (i - k - 1) + (j - k - 1) * (j - k - 1);
+            const double g = exp((double)(-num) / (2.0 * (sigma * sigma)));
+            G[(i - 1) * 5 + (j - 1)] = g;
+            acc = acc + g;
+        }
+    for (int q = 0; q < 25; ++q) G[q] = G[q] / acc;
+}
+
+__attribute__((optimize("fp-contract=off")))
+int ora_gaussian_filter_2d(double* a, int nx, int ny, double sigma)
+{
+    if (nx < 5 || ny < 5) return 1;
+    double G[25];
+    ora_gaussian_kernel(sigma, G);
+    double* buf = (double*)calloc((size_t)nx * ny, sizeof(double));
+    if (!buf) return 2;
+    for (int i = 1; i <= nx; ++i)
+        for (int j = 1; j <= ny; ++j) {
+            double acc = 0.0;
+            for (int l = 1; l <= 5; ++l)
+                for (int m = 1; m <= 5; ++m) {
+                    int ii = i - l, jj = j - m;
+                    if (ii > nx) ii -= nx;
+                    if (ii < 1) ii = nx - abs(ii);
+                    if (jj > ny) jj -= ny;
+                    if (jj < 1) jj = ny - abs(jj);
+                    const double t = IDX2(a, ii, jj, nx) * G[(l - 1) * 5 + (m - 1)];
+                    acc = acc + t;
+                }
+            IDX2(buf, i, j, nx) = acc;
+        }
+    memcpy(a, buf, sizeof(double) * (size_t)nx * ny);
+    free(buf);
+    return 0;
+}
+
+/* add_neighbors_to_stack (rsp:582-622): the 3x3 neighbourhood of (i,j) wrapped with the
+ * COARSE cell counts ncx, ncy (index < 1 -> ncx, index > ncx -> 1); an unvisited, masked,
+ * not-yet-stacked, downhill neighbour is pushed.  Returns 1 when the 10000-row stack would
+ * overflow ("Stack array capacity exceeded"). */
+static int sk_push_neighbours(int i, int j, int ncx, int ncy, int fx, int* stack, int* sp,
+                              const unsigned char* visited, const unsigned char* mask,
+                              unsigned char* in_stack, const double* d)
+{
+    const double dij = fabs(IDX2(d, i, j, fx));
+    for (int di = -1; di <= 1; ++di)
+        for (int dj = -1; dj <= 1; ++dj) {
+            int it = i + di, jt = j + dj;
+            if (it < 1) it = ncx;
+            if (it > ncx) it = 1;
+            if (jt < 1) jt = ncy;
+            if (jt > ncy) jt = 1;
+            if (IDX2(in_stack, it, jt, fx)) continue;
+            const int downhill = dij >= fabs(IDX2(d, it, jt, fx)) - 1e-10;
+            if (!IDX2(visited, it, jt, fx) && IDX2(mask, it, jt, fx) && downhill) {
+                if (*sp + 1 > 10000) return 1;
+                stack[2 * (*sp - 1)] = it;
+                stack[2 * (*sp - 1) + 1] = jt;
+                *sp += 1;
+                IDX2(in_stack, it, jt, fx) = 1;
+            }
+        }
+    return 0;
+}
+
+/* calculate_skyrmion_number (rsp:627-812) after its interpolation step: dens is the fx x fy
+ * fine-grid density (overwritten by its Gaussian-filtered copy), ncx x ncy the coarse cell
+ * counts that the reference uses for every periodic wrap.  Status 0, 1 on a q_threshold
+ * outside [0,1], 2 on stack overflow, 3 on a fine grid below 5x5, 4 on allocation failure. */
+__attribute__((optimize("fp-contract=off")))
+int ora_skyrmion_number(double* d, int fx, int fy, int ncx, int ncy, double q_threshold,
+                        int particle_number, double sigma, int* out)
+{
+    const double skThreshold = 0.05;
+    if (fabs(q_threshold) > 1.0 || q_threshold < 0.0) return 1;
+    if (ora_gaussian_filter_2d(d, fx, fy, sigma)) return 3;
+    const long n = (long)fx * fy;
+    double mx = 0.0;
+    for (long q = 0; q < n; ++q) if (fabs(d[q]) > mx) mx = fabs(d[q]);
+    unsigned char* mask = (unsigned char*)malloc(n);
+    unsigned char* visited = (unsigned char*)calloc(n, 1);
+    unsigned char* in_stack = (unsigned char*)calloc(n, 1);
+    int* region = (int*)calloc(n, sizeof(int));
+    int* stack = (int*)malloc(sizeof(int) * 2 * 10000);
+    long cap = 64, nreg = 0;
+    double* accs = (double*)malloc(sizeof(double) * cap);
+    unsigned char* merged = (unsigned char*)malloc(cap);
+    int status = 0;
+    if (!mask || !visited || !in_stack || !region || !stack || !accs || !merged) { status = 4; goto done; }
+    for (long q = 0; q < n; ++q) mask[q] = fabs(d[q]) > q_threshold * mx;
+    for (int i = 1; i <= fx && !status; ++i)
+        for (int j = 1; j <= fy && !status; ++j) {
+            int is_max = 1;
+            for (int di = -1; di <= 1; ++di)
+                for (int dj = -1; dj <= 1; ++dj) {
+                    const int x = (int)f_modulo(i + di - 1, ncx) + 1, y = (int)f_modulo(j + dj - 1, ncy) + 1;
+                    if (di == 0 && dj == 0) continue;
+                    if (fabs(IDX2(d, i, j, fx)) < fabs(IDX2(d, x, y, fx))) is_max = 0;
+                }
+            if (!(IDX2(mask, i, j, fx) && !IDX2(visited, i, j, fx) && is_max)) continue;
+            IDX2(visited, i, j, fx) = 1;
+            if (nreg == cap) {
+                cap *= 2;
+                accs = (double*)realloc(accs, sizeof(double) * cap);
+                merged = (unsigned char*)realloc(merged, cap);
+            }
+            accs[nreg] = IDX2(d, i, j, fx);
+            merged[nreg] = 0;
+            nreg += 1;
+            IDX2(region, i, j, fx) = (int)nreg;
+            int sp = 1;
+            memset(in_stack, 0, n);
+            if (sk_push_neighbours(i, j, ncx, ncy, fx, stack, &sp, visited, mask, in_stack, d)) { status = 2; break; }
+            while (sp - 1 != 0) {
+                const int it = stack[2 * (sp - 2)], jt = stack[2 * (sp - 2) + 1];
+                sp -= 1;
+                if (!IDX2(visited, it, jt, fx)) {
+                    accs[nreg - 1] = accs[nreg - 1] + IDX2(d, it, jt, fx);
+                    IDX2(visited, it, jt, fx) = 1;
+                    if (sk_push_neighbours(it, jt, ncx, ncy, fx, stack, &sp, visited, mask, in_stack, d)) {
+                        status = 2;
+                        break;
+                    }
+                    IDX2(region, it, jt, fx) = (int)nreg;
+                }
+            }
+        }
+    if (status) goto done;
+    {
+        int sk = 0;
+        for (int i = 1; i <= fx; ++i)
+            for (int j = 1; j <= fy; ++j) {
+                const int id1 = IDX2(region, i, j, fx);
+                if (id1 == 0) continue;
+                if (merged[id1 - 1]) continue;
+                const double acc = accs[id1 - 1];
+                if (fabs(fabs(acc) - particle_number) < skThreshold) {
+                    sk += (int)f_nint(copysign(1.0, acc));
+                    continue;
+                }
+                for (int di = -1; di <= 1; ++di)
+                    for (int dj = -1; dj <= 1; ++dj) {
+                        const int x = (int)f_modulo(i + di - 1, ncx) + 1, y = (int)f_modulo(j + dj - 1, ncy) + 1;
+                        if (di == 0 && dj == 0) continue;
+                        const int id2 = IDX2(region, x, y, fx);
+                        if (id2 == 0) continue;
+                        if (merged[id2 - 1]) continue;
+                        if (fabs(fabs(accs[id1 - 1] + accs[id2 - 1]) - particle_number) < skThreshold) {
+                            merged[id1 - 1] = 1;
+                            merged[id2 - 1] = 1;
+                        }
+                    }
+            }
+        *out = sk;
+    }
+done:
+    free(mask); free(visited); free(in_stack); free(region); free(stack); free(accs); free(merged);
+    return status;
+}
+
+/* compute_skyrmion_distribution (rsp:930-983) on a fixed fine density: thresholds
+ * max - (i/num)(max - min) outer, sigma = 1 - (s/20)(1 - 1e-5) inner; per pair the counts of
+ * particles 1..N, kept when their charge sum rounds closer to nint(total_charge) than the
+ * best so far; returns early when the sum is within 0.1 of total_charge. */
+int ora_skyrmion_distribution(const double* dens, int fx, int fy, int ncx, int ncy, double total_charge,
+                              int N, double min_t, double max_t, int num_thresholds, int* winding)
+{
+    if (max_t < min_t) return 5;
+    int* closest = (int*)calloc(N, sizeof(int));
+    double* work = (double*)malloc(sizeof(double) * (size_t)fx * fy);
+    if (!closest || !work) { free(closest); free(work); return 4; }
+    for (int j = 0; j < N; ++j) winding[j] = 0;
+    for (int i = 1; i <= num_thresholds; ++i)
+        for (int si = 1; si <= 20; ++si) {
+            const double sigma = 1.0 - ((double)si / 20.0) * (1.0 - 0.00001);
+            const double thr = max_t - ((double)i / (double)num_thresholds) * (max_t - min_t);
+            double w = 0.0;
+            long cur = 0;
+            for (int j = 1; j <= N; ++j) {
+                memcpy(work, dens, sizeof(double) * (size_t)fx * fy);
+                int st = ora_skyrmion_number(work, fx, fy, ncx, ncy, thr, j, sigma, &winding[j - 1]);
+                if (st) { free(closest); free(work); return st; }
+                w = w + (double)(j * winding[j - 1]);
+                cur = cur + (long)j * closest[j - 1];
+            }
+            if (labs(f_nint(w) - f_nint(total_charge)) < labs(cur - f_nint(total_charge)))
+                memcpy(closest, winding, sizeof(int) * N);
+            if (fabs(w - total_charge) < 0.1) { free(closest); free(work); return 0; }
+        }
+    memcpy(winding, closest, sizeof(int) * N);
+    free(closest); free(work);
+    return 0;
+}
+
 /* ======================= reference sweep ======================= */
 /* UniformRandomInSphere (energyMin.f90:49-68); its pi is the float-rounded literal. */
 static void uniform_in_ball(ora_random* rng, double R, double v[3])

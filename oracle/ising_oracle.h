@@ -91,6 +91,13 @@ double ora_canonical_energy(const ora_mesh* m, const ora_params* p);
 double ora_arc_winding(const double s1[3], const double s2[3], const double s3[3]);
 double ora_winding_number(const ora_mesh* m, int z_1based);
 void   ora_winding_density(const ora_mesh* m, int z_1based, double* dens /* nx*ny col-major */);
+/* ---------------- skyrmion counting (reciprocalSpaceProcesses.f90:582-983) ---------------- */
+void ora_gaussian_kernel(double sigma, double G[25]);
+int ora_gaussian_filter_2d(double* a, int nx, int ny, double sigma);
+int ora_skyrmion_number(double* dens, int fx, int fy, int ncx, int ncy, double q_threshold,
+                        int particle_number, double sigma, int* out);
+int ora_skyrmion_distribution(const double* dens, int fx, int fy, int ncx, int ncy, double total_charge,
+                              int N, double min_t, double max_t, int num_thresholds, int* winding);
 /* chainMesh_statistics (src/PT-Utils.f90:33-66) without the skyrmion count */
 void   ora_statistics(const ora_mesh* m, double* wnd_mid, double* wnd_spread, double mag[3]);
 

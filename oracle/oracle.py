@@ -72,6 +72,13 @@ def lib():
         L.ora_winding_number.argtypes = [C.c_void_p, i]
         L.ora_winding_density.argtypes = [C.c_void_p, i, P(d)]
         L.ora_statistics.argtypes = [C.c_void_p, P(d), P(d), P(d)]
+        L.ora_gaussian_kernel.argtypes = [d, P(d)]
+        L.ora_gaussian_filter_2d.restype = i
+        L.ora_gaussian_filter_2d.argtypes = [P(d), i, i, d]
+        L.ora_skyrmion_number.restype = i
+        L.ora_skyrmion_number.argtypes = [P(d), i, i, i, i, d, i, d, P(i)]
+        L.ora_skyrmion_distribution.restype = i
+        L.ora_skyrmion_distribution.argtypes = [P(d), i, i, i, i, d, i, d, d, i, P(i)]
         L.ora_metropolis_mcs_ref.argtypes = [C.c_void_p, d, i, C.c_void_p, d]
         L.ora_metropolis_mcs_omp.argtypes = [C.c_void_p, d, i, C.c_void_p, d, i, i]
         L.ora_colour_pass.restype = l
@@ -364,3 +371,111 @@ def fmt_I0m(v, m):
     b = C.create_string_buffer(64)
     lib().ora_fmt_I0m(b, v, m)
     return b.value.decode()
+
+
+# ---------------------------------------------------------------- skyrmion counting
+def gaussian_kernel(sigma):
+    """The normalised 5x5 kernel of Gaussian_filter_2d (rsp:814-834), G[l-1, m-1]."""
+    G = np.zeros(25)
+    lib().ora_gaussian_kernel(sigma, _dp(G))
+    return G.reshape(5, 5)
+
+
+def gaussian_filter_2d(a, sigma):
+    """Gaussian_filter_2d (rsp:814-859) on a copy of the (nx, ny) array a."""
+    b = np.asfortranarray(np.array(a, dtype=np.float64))
+    st = lib().ora_gaussian_filter_2d(b.ctypes.data_as(C.POINTER(C.c_double)), b.shape[0], b.shape[1], sigma)
+    if st:
+        raise ValueError(f"gaussian_filter_2d status {st}")
+    return b
+
+
+def skyrmion_number(dens, ncx, ncy, q_threshold, particle_number, sigma):
+    """calculate_skyrmion_number (rsp:627-812) after its interpolation step, on the (fx, fy)
+    fine density; returns (status, count)."""
+    b = np.asfortranarray(np.array(dens, dtype=np.float64))
+    out = C.c_int(0)
+    st = lib().ora_skyrmion_number(b.ctypes.data_as(C.POINTER(C.c_double)), b.shape[0], b.shape[1], ncx, ncy,
+                                   q_threshold, particle_number, sigma, C.byref(out))
+    return st, out.value
+
+
+def skyrmion_distribution(dens, ncx, ncy, total_charge, N, min_t, max_t, num_thresholds):
+    """compute_skyrmion_distribution (rsp:930-983) on a fixed fine density; returns
+    (status, counts of particles 1..N)."""
+    b = np.asfortranarray(np.array(dens, dtype=np.float64))
+    out = (C.c_int * N)()
+    st = lib().ora_skyrmion_distribution(b.ctypes.data_as(C.POINTER(C.c_double)), b.shape[0], b.shape[1], ncx, ncy,
+                                         total_charge, N, min_t, max_t, num_thresholds, out)
+    return st, list(out)
+
+
+def spectral_upsample(f, sclx, scly):
+    """Band-limited periodic interpolation of the (nx, ny, 3) grid f onto (sclx*nx, scly*ny):
+    the 2-D DFT zero-padded in the middle of each axis, an even axis's Nyquist bin split
+    between +N/2 and -N/2, scaled so that the fine grid passes through the coarse samples.
+    This is the operation spectral_interpolate_to_fine (rsp:12-70) names; the reference's own
+    FFTW plans (src/fft.f90:80-84,128-155) take the padded row length 2(nx/2+1) as the
+    transform length and write rows of nx/2+2 bins at a pitch of nx/2+1, so its values are
+    not reproducible and this restatement follows the stated intent."""
+    f = np.asarray(f, dtype=np.float64)
+    nx, ny = f.shape[:2]
+    Mx, My = sclx * nx, scly * ny
+
+    def pad(F, n, M, axis):
+        F = np.moveaxis(F, axis, 0)
+        G = np.zeros((M,) + F.shape[1:], dtype=complex)
+        h = n // 2
+        if n % 2 == 0:
+            G[:h] = F[:h]
+            if h > 0:
+                G[M - h + 1:] = F[h + 1:]
+            G[h] += F[h] / 2
+            G[M - h] += F[h] / 2
+        else:
+            G[:h + 1] = F[:h + 1]
+            if h > 0:
+                G[M - h:] = F[h + 1:]
+        return np.moveaxis(G, 0, axis)
+
+    F = np.fft.fft2(f, axes=(0, 1))
+    G = pad(pad(F, nx, Mx, 0), ny, My, 1)
+    return np.real(np.fft.ifft2(G, axes=(0, 1))) * (Mx * My) / (nx * ny)
+
+
+def fine_winding_density(g):
+    """The density loop of calculate_winding_density_interpolated (rsp:409-434) on the
+    (fx, fy, 3) fine grid: triangles (s1,s2,s3) and (s1,s3,s4) of the periodic plaquette
+    (i,j), (i+1,j), (i+1,j+1), (i,j+1), normalised spins, divided by 4 pi (float pi)."""
+    s1 = g / np.linalg.norm(g, axis=2, keepdims=True)
+    s2 = np.roll(s1, -1, axis=0)
+    s3 = np.roll(s2, -1, axis=1)
+    s4 = np.roll(s1, -1, axis=1)
+
+    def arc(a, b, c):
+        d12 = (a * b).sum(2)
+        d23 = (b * c).sum(2)
+        d31 = (c * a).sum(2)
+        im = (a * np.cross(b, c)).sum(2)
+        re = 1.0 + d12 + d23 + d31
+        nrm = np.sqrt(2.0 * (1.0 + d12) * (1.0 + d23) * (1.0 + d31))
+        return 2.0 * np.arctan2(im / nrm, re / nrm)
+
+    return (arc(s1, s2, s3) + arc(s1, s3, s4)) / (4.0 * float(np.float32(np.pi)))
+
+
+def std_grid(mesh, z1):
+    """map_spins_to_std_grid (src/chainMesh.f90:54-83): the spin of the first atom (the
+    linked-list head) of every cell of slice z1, as an (nx, ny, 3) array."""
+    out = np.zeros((mesh.nx, mesh.ny, 3))
+    s = mesh.spins
+    for i in range(mesh.nx):
+        for j in range(mesh.ny):
+            out[i, j] = s[mesh.first_atom((i * mesh.ny + j) * mesh.nz + (z1 - 1))]
+    return out
+
+
+def winding_density_interpolated(mesh, z1, sclx=10, scly=10):
+    """calculate_winding_density_interpolated (rsp:366-436) with the band-limited
+    interpolation of spectral_upsample."""
+    return fine_winding_density(spectral_upsample(std_grid(mesh, z1), sclx, scly))

@@ -119,6 +119,46 @@ def test_winding_parity(oracle, ib, cuda_ok, kind, dims):
     assert np.allclose(d, om.winding_density(2), atol=1e-12)
 
 
+@pytest.mark.parametrize("kind,dims", [("SC", (8, 6, 5)), ("BCC", (4, 5, 3)), ("HK", (3, 3, 4))])
+def test_winding_density_all_slices(oracle, ib, cuda_ok, kind, dims):
+    """All slices in one launch equal the oracle's per-slice density (rsp:438-500), and each
+    slice sums to that slice's winding number."""
+    om, pm = _pair(oracle, ib, kind, dims)
+    s = _random_spins(om.natoms, 33)
+    om.set_spins(s)
+    pm.set_spins(s)
+    d = ib.winding_density_all_slices(pm)
+    assert d.shape == dims
+    q = ib.winding_all_slices(pm)
+    for z in range(1, dims[2] + 1):
+        assert np.allclose(d[:, :, z - 1], om.winding_density(z), rtol=0, atol=1e-12)
+        assert np.array_equal(d[:, :, z - 1], ib.calculate_winding_number_density(pm, z))
+        assert abs(d[:, :, z - 1].sum() - q[z - 1]) <= 1e-9
+
+
+def test_winding_density_csv_bytes(oracle, ib, cuda_ok, tmp_path):
+    """write_winding_number_density (rsp:544-580): header, "x,y,z,d" records in F0.8 with the
+    record's own new_line plus the trimmed buffer's, in (z, x, y) order, and a terminator."""
+    dims = (5, 4, 3)
+    om, pm = _pair(oracle, ib, "BCC", dims)
+    s = _random_spins(om.natoms, 4)
+    om.set_spins(s)
+    pm.set_spins(s)
+    path = tmp_path / "density.csv"
+    ib.write_winding_number_density(pm, str(path))
+    av, bv, cv = om.vectors()[:3]
+    out = ["x,y,z,Winding_Density\n"]
+    for i in range(1, dims[2] + 1):
+        dens = om.winding_density(i)
+        for j in range(1, dims[0] + 1):
+            for k in range(1, dims[1] + 1):
+                pos = (j * av + k * bv) + i * cv
+                f = [oracle.fmt_F0(float(v), 8) for v in (*pos, dens[j - 1, k - 1])]
+                out.append(",".join(f) + "\n\n")
+    out.append("\n")
+    assert path.read_text() == "".join(out)
+
+
 def test_skyrmion_winding_rounds_exactly(oracle, ib, cuda_ok):
     om, pm = _pair(oracle, ib, "SC", (16, 16, 4))
     om.init_skyrmion(8.0, 8.0, 3.0, 1.56, 1)
@@ -231,6 +271,23 @@ def test_spins_csv_bytes(oracle, ib, cuda_ok, tmp_path):
     assert path.read_text() == "\n".join(lines) + "\n"
     ib.write_spins_to_file(pm, str(path), append=True, include_header=False)
     assert path.read_text().count("\n") == 2 + 2 * om.natoms
+
+
+def test_spins_csv_bytes_threaded(oracle, ib, cuda_ok, tmp_path):
+    """A mesh large enough for the writer to split its records over several host threads:
+    the file is still the sequential ES22.14 text."""
+    om, pm = _pair(oracle, ib, "SC", (24, 24, 24))
+    s = _random_spins(om.natoms, 12)
+    pm.set_spins(s)
+    path = tmp_path / "spins.csv"
+    ib.write_spins_to_file(pm, str(path))
+    g = pm.get_spins(0)
+    pos = om.positions()
+    lines = ["x,y,z,Sx,Sy,Sz"]
+    for i in range(om.natoms):
+        vals = [float(pos[i, 0]), float(pos[i, 1]), float(pos[i, 2]), g[i, 0], g[i, 1], g[i, 2]]
+        lines.append(",".join(oracle.fmt_ES(v, 22, 14) for v in vals))
+    assert path.read_text() == "\n".join(lines) + "\n"
 
 
 def test_observables_match_oracle_statistically(oracle, ib, cuda_ok):

@@ -1,0 +1,175 @@
+"""GPU parity of skyrmion counting (rsp:366-436,582-983) through the C-ABI against the oracle.
+
+Tolerances: the interpolated density within 1e-10 of the oracle's FFT-based interpolation
+(two independent FP64 routes to the same band-limited interpolant); the Gaussian filter
+bit-exact (same order, no fused multiply-adds); skyrmion counts and distributions exactly
+equal when both sides count on the same fine density."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _cell(oracle, kind):
+    return {"SC": oracle.SC_CELL, "BCC": oracle.BCC_CELL, "HK": oracle.HYPER_KAGOME_CELL}[kind]
+
+
+def _pair(oracle, ib, kind, dims):
+    frac, (a, b, c, ab, bc, ca) = _cell(oracle, kind)
+    return oracle.Mesh(frac, *dims, a, b, c, ab, bc, ca), ib.ChainMesh(*dims, frac, a, b, c, ab, bc, ca)
+
+
+def _random_spins(n, seed):
+    rng = np.random.default_rng(seed)
+    s = rng.normal(size=(n, 3))
+    s /= np.linalg.norm(s, axis=1, keepdims=True)
+    return s.astype(np.float32).astype(np.float64)
+
+
+def _skyrmion_pair(oracle, ib, L=12, nz=4, scale=None):
+    om = oracle.Mesh.sc(L, L, nz)
+    om.init_skyrmion(L / 2, L / 2, L / 4, 1.56, 1)
+    pm = ib.ChainMesh.simple_cubic(L, L, nz)
+    pm.set_spins(om.spins.copy())
+    om.set_spins(pm.get_spins(0))
+    if scale:
+        ib.set_interpolation_scale(pm, *scale)
+    return om, pm
+
+
+@pytest.mark.parametrize("kind,dims,scale", [("SC", (8, 6, 4), (3, 2)), ("BCC", (4, 5, 3), (4, 3)),
+                                             ("SC", (6, 6, 4), (10, 10))])
+def test_interpolated_density_matches_oracle(oracle, ib, cuda_ok, kind, dims, scale):
+    om, pm = _pair(oracle, ib, kind, dims)
+    s = _random_spins(om.natoms, 5)
+    om.set_spins(s)
+    pm.set_spins(s)
+    ib.set_interpolation_scale(pm, *scale)
+    assert ib.interpolation_scale(pm) == scale
+    for z in range(1, dims[2] + 1):
+        g = ib.calculate_winding_density_interpolated(pm, z)
+        o = oracle.winding_density_interpolated(om, z, *scale)
+        assert g.shape == o.shape == (dims[0] * scale[0], dims[1] * scale[1])
+        assert np.abs(g - o).max() <= 1e-10
+
+
+def test_interpolated_density_keeps_the_charge(oracle, ib, cuda_ok):
+    om, pm = _skyrmion_pair(oracle, ib, L=16, scale=(4, 4))
+    pi_ratio = float(np.float32(np.pi)) / np.pi
+    for z in (1, 2):
+        t = ib.calculate_winding_density_interpolated(pm, z).sum() * pi_ratio
+        assert abs(t - round(t)) < 1e-9 and round(t) == round(ib.calculate_winding_number2(pm, z))
+        assert abs(round(t)) == 1
+
+
+@pytest.mark.parametrize("shape", [(5, 5), (5, 9), (37, 23), (64, 40)])
+def test_gaussian_filter_bit_exact(oracle, ib, cuda_ok, shape):
+    rng = np.random.default_rng(shape[0] * 100 + shape[1])
+    a = rng.normal(size=shape)
+    for sigma in (1.0, 0.55, 0.05, 1e-5):
+        assert np.array_equal(ib.gaussian_filter_2d(a, sigma), oracle.gaussian_filter_2d(a, sigma))
+    with pytest.raises(ib.IsingError):
+        ib.gaussian_filter_2d(np.zeros((4, 8)), 0.5)
+
+
+def _densities():
+    rng = np.random.default_rng(17)
+    out = []
+    # noise, smooth bumps of both signs, a bump outside the first coarse block, plateaus
+    out.append((rng.normal(size=(30, 24)), 10, 8))
+    x, y = np.meshgrid(np.arange(40), np.arange(36), indexing="ij")
+    bump = lambda cx, cy, w: np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * w * w))
+    d = bump(4, 5, 1.5) / bump(4, 5, 1.5).sum() - bump(25, 20, 2.0) / bump(25, 20, 2.0).sum()
+    out.append((d, 8, 9))
+    d = 0.02 * rng.normal(size=(40, 36)) + bump(3, 3, 1.0) / bump(3, 3, 1.0).sum()
+    out.append((d, 20, 18))
+    d = np.zeros((20, 20))
+    d[2:5, 2:5] = 1.0 / 9.0
+    out.append((d, 10, 10))
+    return out
+
+
+def test_skyrmion_number_on_given_densities(oracle, ib, cuda_ok):
+    n_nonzero = 0
+    for d, ncx, ncy in _densities():
+        for q in (0.0, 1e-5, 0.1, 0.3, 0.6, 0.95, 1.0):
+            for sigma in (1.0, 0.5, 0.05, 1e-5):
+                for pn in (1, 2):
+                    st, want = oracle.skyrmion_number(d, ncx, ncy, q, pn, sigma)
+                    assert st == 0
+                    got = ib.skyrmion_number_from_density(d, ncx, ncy, q, pn, sigma)
+                    assert got == want, (d.shape, ncx, ncy, q, sigma, pn)
+                    n_nonzero += want != 0
+    assert n_nonzero > 0
+    with pytest.raises(ib.IsingError) as e:
+        ib.skyrmion_number_from_density(np.zeros((20, 20)), 10, 10, 1.5, 1, 0.5)
+    assert e.value.status == 1
+
+
+def test_stack_capacity_matches_reference_stop(oracle, ib, cuda_ok):
+    """Plateaus over 160 x 160 and 150 x 150 coarse blocks: every cell is downhill of its
+    neighbours and the region-growth stack passes the reference's 10000 rows ("Stack array
+    capacity exceeded", rsp:611) on both sides; a 100 x 100 block stays below it."""
+    rng = np.random.default_rng(0)
+    for n, d in ((160, np.full((166, 166), 1e-3)), (150, 1e-3 + 1e-12 * rng.random((156, 156)))):
+        st, _ = oracle.skyrmion_number(d, n, n, 0.5, 1, 1e-5)
+        assert st == 2
+        with pytest.raises(ib.IsingError) as e:
+            ib.skyrmion_number_from_density(d, n, n, 0.5, 1, 1e-5)
+        assert e.value.status == 9
+    d = 1e-3 + 1e-12 * rng.random((106, 106))
+    assert oracle.skyrmion_number(d, 100, 100, 0.5, 1, 1e-5) == (0, ib.skyrmion_number_from_density(d, 100, 100, 0.5, 1, 1e-5))
+
+
+@pytest.mark.parametrize("state", ["skyrmion", "random", "uniform"])
+def test_skyrmion_number_on_mesh(oracle, ib, cuda_ok, state):
+    om, pm = _skyrmion_pair(oracle, ib, L=12, scale=(3, 3))
+    if state == "random":
+        pm.set_spins(_random_spins(om.natoms, 9))
+    elif state == "uniform":
+        pm.set_spins(np.tile([0.0, 0.0, 1.0], (om.natoms, 1)))
+    for z in (1, 3):
+        dens = ib.calculate_winding_density_interpolated(pm, z)
+        for q, pn, sigma in ((0.3, 1, 0.5), (0.05, 1, 1e-5), (0.9, 2, 1.0), (0.0, 1, 0.25)):
+            want = oracle.skyrmion_number(dens, 12, 12, q, pn, sigma)
+            assert want[0] == 0
+            assert ib.calculate_skyrmion_number(pm, z, q, pn, sigma) == want[1]
+
+
+@pytest.mark.parametrize("state,N", [("skyrmion", 1), ("skyrmion", 2), ("random", 1), ("random", 3),
+                                     ("uniform", 1)])
+def test_skyrmion_distribution_on_mesh(oracle, ib, cuda_ok, state, N):
+    om, pm = _skyrmion_pair(oracle, ib, L=10, scale=(3, 3))
+    if state == "random":
+        pm.set_spins(_random_spins(om.natoms, 4))
+    elif state == "uniform":
+        pm.set_spins(np.tile([0.0, 0.0, 1.0], (om.natoms, 1)))
+    z = 2
+    dens = ib.calculate_winding_density_interpolated(pm, z)
+    total = ib.calculate_winding_number2(pm, z)
+    for (lo, hi, n) in ((1e-5, 0.95, 60), (0.2, 0.8, 7)):
+        st, want = oracle.skyrmion_distribution(dens, 10, 10, total, N, lo, hi, n)
+        assert st == 0
+        got = ib.compute_skyrmion_distribution(pm, N, lo, hi, n, z)
+        assert list(got) == want, (state, N, lo, hi, n)
+
+
+def test_chain_mesh_statistics_full(oracle, ib, cuda_ok):
+    om, pm = _skyrmion_pair(oracle, ib, L=10, nz=4, scale=(2, 2))
+    sk, wm, ws, mag = ib.chain_mesh_statistics_full(pm)
+    wm0, ws0, mag0 = ib.chain_mesh_statistics(pm)
+    assert (wm, ws) == (wm0, ws0) and np.array_equal(mag, mag0)
+    z = 4 // 2
+    dens = ib.calculate_winding_density_interpolated(pm, z)
+    st, want = oracle.skyrmion_distribution(dens, 10, 10, ib.calculate_winding_number2(pm, z), 1, 1e-5, 0.95, 60)
+    assert st == 0 and sk == want[0]
+
+
+def test_interpolation_scale_checks(ib, cuda_ok):
+    pm = ib.ChainMesh.simple_cubic(4, 4, 4)
+    assert ib.interpolation_scale(pm) == (10, 10)
+    with pytest.raises(ib.IsingError):
+        ib.set_interpolation_scale(pm, 1, 4)
+    with pytest.raises(ib.IsingError):
+        ib.calculate_skyrmion_number(pm, 5, 0.3, 1, 0.5)
+    pm.close()
