@@ -53,6 +53,9 @@ WORKLOADS = {
                            [(0.3, 0.1), (0.3, 0.3), (0.5, 0.1), (0.5, 0.3), (0.7, 0.1), (0.7, 0.3)][i % 6])
                           for i, L in enumerate([16, 16, 24, 24, 32, 32, 48, 48, 64, 64, 96, 96])]),
 }
+WORKLOADS["stats"] = dict(L=96, nz=96, scale=10, J=-1.0, D=0.5, B=0.25, K=0.0, move="ball", r=0.2, tmin=0.1,
+                          desc="chainMesh_statistics on SC L=96 (96 slices): winding per slice, magnetisation and "
+                               "the 60 x 20 skyrmion search on the middle slice's 960 x 960 interpolated density")
 BYTES_PER_UPDATE = 24  # algorithmic: one FP32 x,y,z read and write per site per sweep
 
 
@@ -151,6 +154,18 @@ def cpu_reference_rate(w, steps, warmup, threads, L_sample=None):
 def run_reference(args, w):
     rank, world, _ = dist_env()
     if rank != 0:
+        return
+    if args.workload == "stats":
+        L, nz = args.L or w["L"], w["nz"]
+        cpu = stats_cpu_baseline(w, L, nz, skyrmion_texture(L, nz, L / 6, [(L / 4, L / 4), (3 * L / 4, L / 3),
+                                                                           (L / 2, 3 * L / 4)], 0x15196))
+        line = {"metric": "statistics calls/s", "value": cpu["value"], "unit": cpu["unit"], "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / cpu["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": "stats", "desc": w["desc"]},
+                "cpu_baseline": cpu,
+                "e2e": {"value": cpu["value"], "unit": cpu["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return
     threads = host_cores()
     rate, sample = cpu_reference_rate(w, max(args.steps, 1), max(args.warmup, 0), threads)
@@ -373,6 +388,119 @@ def run_gpu(args, w):
         mm.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- post-processing: chainMesh_statistics
+def skyrmion_texture(L, nz, R, centres, seed):
+    """A z-uniform texture of Bloch skyrmions of radius R at the given (x, y) centres on a
+    core-down background, plus small seeded noise: (L*L*nz, 3) unit vectors in atom order."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    x, y = np.meshgrid(np.arange(L, dtype=np.float64), np.arange(L, dtype=np.float64), indexing="ij")
+    theta = np.zeros((L, L))
+    phi = np.zeros((L, L))
+    for cx, cy in centres:
+        dx = (x - cx + L / 2) % L - L / 2
+        dy = (y - cy + L / 2) % L - L / 2
+        r = np.hypot(dx, dy)
+        inside = r < R
+        theta = np.where(inside, np.pi * (1.0 - r / R), theta)
+        phi = np.where(inside, np.arctan2(dy, dx) + np.pi / 2, phi)
+    s = np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), -np.cos(theta)], axis=-1)
+    s = np.repeat(s[:, :, None, :], nz, axis=2).reshape(-1, 3) + 0.05 * rng.normal(size=(L * L * nz, 3))
+    return s / np.linalg.norm(s, axis=1, keepdims=True)
+
+
+def stats_cpu_baseline(w, L, nz, spins, n_sample=4):
+    """chainMesh_statistics on the oracle (one host thread): the nz slice winding numbers and
+    magnetisation, the FFT interpolation of the middle slice, and n_sample pairs of the
+    60 x 20 threshold/sigma search through the literal calculate_skyrmion_number restatement,
+    scaled to the 1200 pairs a search without an early exit evaluates."""
+    from oracle import oracle as O
+    O.build()
+    om = O.Mesh.sc(L, L, nz)
+    om.set_spins(spins)
+    t0 = time.perf_counter()
+    for z in range(1, nz + 1):
+        om.winding_number(z)
+    om.statistics()
+    dens = O.winding_density_interpolated(om, nz // 2, w["scale"], w["scale"])
+    t_fixed = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for k in range(n_sample):      # the first pairs of the search: threshold index 1, sigma index 1..n
+        thr = 0.95 - (1 / 60) * (0.95 - 1e-5)
+        O.skyrmion_number(dens, L, L, thr, 1, 1.0 - ((k + 1) / 20.0) * (1.0 - 0.00001))
+    t_pair = (time.perf_counter() - t0) / n_sample
+    pairs = 1200
+    t_call = t_fixed + pairs * t_pair
+    fx = L * w["scale"]
+    return {"value": 1.0 / t_call, "unit": "statistics calls/s", "cores": 1, "kind": "port",
+            "sample": f"{n_sample} of the {pairs} (threshold, sigma) pairs through the literal "
+                      f"calculate_skyrmion_number restatement on the {fx}x{fx} density ({t_pair*1e3:.1f} ms each, "
+                      f"scaled to {pairs}) plus the {nz} slice winding numbers, magnetisation and one FFT "
+                      f"interpolation ({t_fixed*1e3:.1f} ms); the reference redoes the interpolation per pair"}
+
+
+def run_stats(args, w):
+    """One step = one chainMesh_statistics call (src/PT-Utils.f90:33-66) through the C-ABI on a
+    resident replica; e2e adds the upload of the spins from pinned host memory."""
+    import numpy as np
+    import torch
+    import ising_b200 as ib
+    rank, world, local = dist_env()
+    L, nz = args.L or w["L"], w["nz"]
+    torch.cuda.set_device(local)
+    mesh = ib.ChainMesh.simple_cubic(L, L, nz, device=local)
+    ib.set_interpolation_scale(mesh, w["scale"], w["scale"])
+    spins = skyrmion_texture(L, nz, L / 6, [(L / 4, L / 4), (3 * L / 4, L / 3), (L / 2, 3 * L / 4)], 0x15196)
+    host = torch.from_numpy(np.ascontiguousarray(spins)).pin_memory()
+    mesh.set_spins(host.numpy())
+    for _ in range(args.warmup):
+        res = ib.chain_mesh_statistics_full(mesh)
+    clk = ClockSampler(getattr(torch.cuda.get_device_properties(local), "pci_bus_id", None))
+    clk.start()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        res = ib.chain_mesh_statistics_full(mesh)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    clocks = clk.stop()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        mesh.set_spins(host.numpy())
+        res = ib.chain_mesh_statistics_full(mesh)
+    torch.cuda.synchronize()
+    e2e_dt = (time.perf_counter() - t0) / max(1, args.steps // 2)
+    sk, wmid, wspread, mag = res
+    zmid = nz // 2
+    total = ib.calculate_winding_number2(mesh, zmid)
+    early = abs(sk - total) < 0.1      # the search stops at the first pair that matches Q
+    fx, fy = L * w["scale"], L * w["scale"]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = stats_cpu_baseline(w, L, nz, mesh.get_spins(0))
+    if rank == 0:
+        line = {
+            "metric": "statistics calls/s", "value": args.steps / dt, "unit": "statistics calls/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (three Bloch skyrmions of radius L/6, z-uniform, 5% seeded noise)",
+            "config": {"workload": "stats", "desc": w["desc"], "L": L, "nz": nz, "fine_grid": [fx, fy],
+                       "pairs_searched": 1200 if not early else "early exit",
+                       "timer": "host wall clock around synchronous C-ABI calls (device and host stages)"},
+            "result": {"skyrmion_number_middle": sk, "winding_number_middle": wmid,
+                       "winding_number_spread": wspread, "magnetisation": list(map(float, mag))},
+            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "e2e": {"value": 1.0 / e2e_dt, "unit": "statistics calls/s", "h2d_bytes_per_step": int(spins.size * 8),
+                    "d2h_bytes_per_step": int(20 * L * L * 8 + 2 * nz * 8 + 20 * 12),
+                    "path": "ising_spins_set (host doubles) -> ising_chain_mesh_statistics; d2h excludes the "
+                            "local-maximum lists (12 B per listed cell)"},
+            "cpu_baseline": cpu,
+            "gpu_launches": args.steps * 10,
+        }
+        print(json.dumps(line), flush=True)
+    mesh.close()
 
 
 # ---------------------------------------------------------------- C1: GPU vs the CPU reference chain
@@ -708,6 +836,8 @@ def main():
         run_c5(args, WORKLOADS["c5"])
     elif args.workload == "c1":
         run_c1(args)
+    elif args.workload == "stats":
+        run_stats(args, w)
     else:
         run_gpu(args, w)
 
