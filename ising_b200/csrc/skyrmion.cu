@@ -242,10 +242,34 @@ __global__ void k_sky_localmax(const double* __restrict__ filt, const unsigned l
 }
 
 // ------------------------------------------------------------------ host side
+// Runs fn(k, t) for k in [a, b) on up to hardware_concurrency threads, t the thread's index
+// (0 .. threads-1), k interleaved over the threads.
+int host_threads() { return (int)std::max(1u, std::thread::hardware_concurrency()); }
+
+template <typename Fn>
+void parallel_for(int a, int b, const Fn& fn) {
+    const int n = b - a;
+    const int nt = std::max(1, std::min(n, host_threads()));
+    std::vector<std::thread> pool;
+    auto work = [&](int t) {
+        for (int k = a + t; k < b; k += nt) fn(k, t);
+    };
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+}
+
+// A cell that passed the local-maximum test: 0-based fine coordinates, its coordinates
+// wrapped with the coarse counts (the reference's modulo(i+di-1, nx)+1 before adding di), and
+// its filtered value.  Sorted by the reference's loop order, i outer and j inner.
+struct Cand {
+    int I, J, xm, ym;
+    double v;
+};
+
 struct SigmaData {
     double max = 0.0;
-    std::vector<long long> cp;   // sorted fine indices (i-1)*fy + (j-1)
-    std::vector<double> cv;
+    std::vector<Cand> c;
     std::vector<double> win;     // filtered values of the first nx x ny cells, x fastest
 };
 
@@ -254,72 +278,90 @@ struct Grid {
 };
 
 // Region growth (rsp:694-765) for one (threshold, sigma): per region its charge sum, per
-// window cell its region, and the starting cells outside the window with their region.
-// Returns ISING_ERR_CAPACITY without setting the error message (it runs on worker threads).
+// window cell its region, and the starting cells outside the window with their region.  The
+// vectors are kept between calls of one host thread.  Returns ISING_ERR_CAPACITY without
+// setting the error message (it runs on worker threads).
 struct Regions {
     std::vector<double> accs;
-    std::vector<int> region;                               // nx*ny, 0 = none
-    std::vector<std::pair<long long, int>> outside;        // (fine index, region)
+    std::vector<int> region;                        // nx*ny, 0 = none
+    std::vector<std::pair<int, int>> outside;       // (candidate index, region)
+    std::vector<unsigned char> mask, visited, merged;
+    std::vector<int> in_stack, stack;
 };
 
 int grow_regions(const SigmaData& S, const Grid& g, double thr, Regions* R) {
     const int nx = g.nx, ny = g.ny;
     const size_t nw = (size_t)nx * ny;
     const double cut = thr * S.max;
-    std::vector<unsigned char> mask(nw), visited(nw, 0);
-    std::vector<int> in_stack(nw, 0), stack(kStackRows);
     R->accs.clear();
     R->outside.clear();
     R->region.assign(nw, 0);
-    for (size_t q = 0; q < nw; ++q) mask[q] = std::fabs(S.win[q]) > cut;
+    R->visited.assign(nw, 0);
+    R->in_stack.assign(nw, 0);
+    R->mask.resize(nw);
+    R->stack.resize(kStackRows);
+    unsigned char* mask = R->mask.data();
+    unsigned char* visited = R->visited.data();
+    int* in_stack = R->in_stack.data();
+    int* stack = R->stack.data();
+    int* region = R->region.data();
+    const double* win = S.win.data();
+    for (size_t q = 0; q < nw; ++q) mask[q] = std::fabs(win[q]) > cut;
     int rc = 0, sp = 1;
-    // add_neighbors_to_stack (rsp:582-622) around fine cell (i,j), 1-based
-    auto push = [&](int i, int j, double absd) -> bool {
-        for (int di = -1; di <= 1; ++di)
-            for (int dj = -1; dj <= 1; ++dj) {
-                int it = i + di, jt = j + dj;
-                if (it < 1) it = nx;
-                if (it > nx) it = 1;
-                if (jt < 1) jt = ny;
-                if (jt > ny) jt = 1;
-                const int q = (it - 1) + (jt - 1) * nx;
-                if (in_stack[q] == rc) continue;
-                const bool downhill = absd >= std::fabs(S.win[q]) - 1e-10;
-                if (!visited[q] && mask[q] && downhill) {
-                    if (sp + 1 > kStackRows) return false;
-                    stack[sp - 1] = q;
-                    sp += 1;
-                    in_stack[q] = rc;
-                }
-            }
+    // one neighbour of add_neighbors_to_stack (rsp:600-616), window index q
+    auto consider = [&](int q, double absd) -> bool {
+        if (in_stack[q] == rc) return true;
+        const bool downhill = absd >= std::fabs(win[q]) - 1e-10;
+        if (!visited[q] && mask[q] && downhill) {
+            if (sp + 1 > kStackRows) return false;
+            stack[sp - 1] = q;
+            sp += 1;
+            in_stack[q] = rc;
+        }
         return true;
     };
-    for (size_t k = 0; k < S.cp.size(); ++k) {
-        const double v = S.cv[k];
-        if (!(std::fabs(v) > cut)) continue;
-        const long long p = S.cp[k];
-        const int i = (int)(p / g.fy) + 1, j = (int)(p % g.fy) + 1;
-        const bool inwin = i <= nx && j <= ny;
-        const int qw = inwin ? (i - 1) + (j - 1) * nx : -1;
+    // add_neighbors_to_stack (rsp:582-622) around 0-based fine cell (I, J): indices wrap with the
+    // coarse counts (index < 1 -> nx, index > nx -> 1)
+    auto push = [&](int I, int J, double absd) -> bool {
+        if (I > nx && J > ny) return consider(0, absd);   // all nine map to the window's (1,1)
+        for (int di = -1; di <= 1; ++di) {
+            int it = I + 1 + di;
+            if (it < 1) it = nx;
+            if (it > nx) it = 1;
+            for (int dj = -1; dj <= 1; ++dj) {
+                int jt = J + 1 + dj;
+                if (jt < 1) jt = ny;
+                if (jt > ny) jt = 1;
+                if (!consider((it - 1) + (jt - 1) * nx, absd)) return false;
+            }
+        }
+        return true;
+    };
+    const int nc = (int)S.c.size();
+    for (int k = 0; k < nc; ++k) {
+        const Cand& c = S.c[k];
+        if (!(std::fabs(c.v) > cut)) continue;
+        const bool inwin = c.I < nx && c.J < ny;
+        const int qw = inwin ? c.I + c.J * nx : -1;
         if (inwin && visited[qw]) continue;
-        R->accs.push_back(v);
+        R->accs.push_back(c.v);
         rc = (int)R->accs.size();
         if (inwin) {
             visited[qw] = 1;
-            R->region[qw] = rc;
+            region[qw] = rc;
         } else {
-            R->outside.emplace_back(p, rc);
+            R->outside.emplace_back(k, rc);
         }
         sp = 1;
-        if (!push(i, j, std::fabs(v))) return ISING_ERR_CAPACITY;
+        if (!push(c.I, c.J, std::fabs(c.v))) return ISING_ERR_CAPACITY;
         while (sp - 1 != 0) {
             const int q = stack[sp - 2];
             sp -= 1;
             if (!visited[q]) {
-                R->accs[rc - 1] = R->accs[rc - 1] + S.win[q];
+                R->accs[rc - 1] = R->accs[rc - 1] + win[q];
                 visited[q] = 1;
-                if (!push(q % nx + 1, q / nx + 1, std::fabs(S.win[q]))) return ISING_ERR_CAPACITY;
-                R->region[q] = rc;
+                if (!push(q % nx, q / nx, std::fabs(win[q]))) return ISING_ERR_CAPACITY;
+                region[q] = rc;
             }
         }
     }
@@ -329,41 +371,57 @@ int grow_regions(const SigmaData& S, const Grid& g, double thr, Regions* R) {
 // The merge loop (rsp:772-805): fine cells with a region in (i, j) order.  A cell of an unmerged
 // region whose sum is within 0.05 of particle_number adds sign(sum); otherwise regions whose
 // joint sum is within 0.05 are marked merged.
-int count_regions(const Regions& R, const Grid& g, int particle_number) {
+int count_regions(Regions& R, const SigmaData& S, const Grid& g, int particle_number) {
     const int nx = g.nx, ny = g.ny;
-    std::vector<unsigned char> merged(R.accs.size(), 0);
+    R.merged.assign(R.accs.size(), 0);
+    unsigned char* merged = R.merged.data();
+    const double* accs = R.accs.data();
+    const int* region = R.region.data();
     const double pn = (double)particle_number;
     int sk = 0;
-    auto cell = [&](long long p, int id1) {
+    auto cell = [&](int xm, int ym, int id1) {
         if (merged[id1 - 1]) return;
-        const double acc = R.accs[id1 - 1];
+        const double acc = accs[id1 - 1];
         if (std::fabs(std::fabs(acc) - pn) < kSkThreshold) {
             sk += std::signbit(acc) ? -1 : 1;
             return;
         }
-        const int I = (int)(p / g.fy), J = (int)(p % g.fy);
-        for (int di = -1; di <= 1; ++di)
+        for (int di = -1; di <= 1; ++di) {
+            int x = xm + di;
+            if (x < 0) x += nx;
+            if (x >= nx) x -= nx;
             for (int dj = -1; dj <= 1; ++dj) {
                 if (di == 0 && dj == 0) continue;
-                const int x = ((I + di) % nx + nx) % nx, y = ((J + dj) % ny + ny) % ny;
-                const int id2 = R.region[x + y * nx];
+                int y = ym + dj;
+                if (y < 0) y += ny;
+                if (y >= ny) y -= ny;
+                const int id2 = region[x + y * nx];
                 if (id2 == 0) continue;
                 if (merged[id2 - 1]) continue;
-                if (std::fabs(std::fabs(R.accs[id1 - 1] + R.accs[id2 - 1]) - pn) < kSkThreshold) {
+                if (std::fabs(std::fabs(accs[id1 - 1] + accs[id2 - 1]) - pn) < kSkThreshold) {
                     merged[id1 - 1] = 1;
                     merged[id2 - 1] = 1;
                 }
             }
+        }
     };
     size_t o = 0;
+    const size_t no = R.outside.size();
     for (int i = 0; i < nx; ++i)
         for (int j = 0; j < ny; ++j) {
             const long long p = (long long)i * g.fy + j;
-            while (o < R.outside.size() && R.outside[o].first < p) { cell(R.outside[o].first, R.outside[o].second); ++o; }
-            const int id = R.region[i + j * nx];
-            if (id) cell(p, id);
+            for (; o < no; ++o) {
+                const Cand& c = S.c[R.outside[o].first];
+                if ((long long)c.I * g.fy + c.J >= p) break;
+                cell(c.xm, c.ym, R.outside[o].second);
+            }
+            const int id = region[i + j * nx];
+            if (id) cell(i, j, id);
         }
-    for (; o < R.outside.size(); ++o) cell(R.outside[o].first, R.outside[o].second);
+    for (; o < no; ++o) {
+        const Cand& c = S.c[R.outside[o].first];
+        cell(c.xm, c.ym, R.outside[o].second);
+    }
     return sk;
 }
 
@@ -410,18 +468,19 @@ int filter_and_collect(SkyWork* w, const std::vector<double>& sigmas, double tmi
                                    w->fx * sizeof(double), w->nx * sizeof(double), w->ny, cudaMemcpyDeviceToHost, st));
     }
     ISG_CUDA(cudaStreamSynchronize(st));
-    for (int s = 0; s < ns; ++s) {
+    const int nx = w->nx, ny = w->ny, fy = w->fy;
+    parallel_for(0, ns, [&](int s, int) {
         SigmaData& S = (*out)[s];
         std::vector<size_t> ord(cp[s].size());
         for (size_t k = 0; k < ord.size(); ++k) ord[k] = k;
         std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return cp[s][a] < cp[s][b]; });
-        S.cp.resize(ord.size());
-        S.cv.resize(ord.size());
+        S.c.resize(ord.size());
         for (size_t k = 0; k < ord.size(); ++k) {
-            S.cp[k] = cp[s][ord[k]];
-            S.cv[k] = cv[s][ord[k]];
+            const long long p = cp[s][ord[k]];
+            const int I = (int)(p / fy), J = (int)(p % fy);
+            S.c[k] = Cand{I, J, I % nx, J % ny, cv[s][ord[k]]};
         }
-    }
+    });
     return ISING_OK;
 }
 
@@ -496,20 +555,6 @@ int fine_density(ising_mesh* m, int replica, int z1, int n_sigma, SkyWork** out)
     return ISING_OK;
 }
 
-// Runs fn(k) for k in [a, b) on up to hardware_concurrency threads.
-template <typename Fn>
-void parallel_for(int a, int b, const Fn& fn) {
-    const int n = b - a;
-    const int nt = std::max(1, std::min<int>(n, (int)std::max(1u, std::thread::hardware_concurrency())));
-    std::vector<std::thread> pool;
-    auto work = [&](int t) {
-        for (int k = a + t; k < b; k += nt) fn(k);
-    };
-    for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
-    work(0);
-    for (auto& th : pool) th.join();
-}
-
 // compute_skyrmion_distribution's search (rsp:957-981) over prepared sigma data: results are
 // taken in the reference's order; pairs are evaluated speculatively in batches on host threads.
 int distribution(const std::vector<SigmaData>& S, const Grid& g, double total_charge, int N, double min_t,
@@ -517,23 +562,24 @@ int distribution(const std::vector<SigmaData>& S, const Grid& g, double total_ch
     std::vector<int> closest(N, 0);
     const long nq = std::lround(total_charge);   // nint for |x| below 2^31
     const int n_pairs = num_thresholds * kSigmas;
-    const int batch = std::max(1, (int)std::thread::hardware_concurrency());
+    const int batch = 4 * host_threads();
     std::vector<std::vector<int>> res(batch, std::vector<int>(N));
     std::vector<int> status(batch);
+    std::vector<Regions> scratch(host_threads());
     for (int j = 0; j < N; ++j) winding[j] = 0;
     for (int base = 0; base < n_pairs; base += batch) {
         const int hi = std::min(n_pairs, base + batch);
-        parallel_for(base, hi, [&](int k) {
+        parallel_for(base, hi, [&](int k, int t) {
             const int i = k / kSigmas + 1, si = k % kSigmas + 1;
             const double thr = max_t - ((double)i / (double)num_thresholds) * (max_t - min_t);
             if (std::fabs(thr) > 1.0 || thr < 0.0) {   // the q_threshold check of rsp:689
                 status[k - base] = ISING_ERR_ARG;
                 return;
             }
-            Regions R;
+            Regions& R = scratch[t];
             status[k - base] = grow_regions(S[si - 1], g, thr, &R);
             if (status[k - base] == ISING_OK)
-                for (int j = 1; j <= N; ++j) res[k - base][j - 1] = count_regions(R, g, j);
+                for (int j = 1; j <= N; ++j) res[k - base][j - 1] = count_regions(R, S[si - 1], g, j);
         });
         for (int k = base; k < hi; ++k) {
             if (status[k - base] == ISING_ERR_ARG) return fail(ISING_ERR_ARG, "q_threshold must be between 0 and 1");
@@ -612,7 +658,7 @@ extern "C" int ising_skyrmion_number(const ising_mesh* mc, int replica, int z1, 
     const Grid g{w->nx, w->ny, w->fx, w->fy};
     Regions R;
     if (grow_regions(S[0], g, q_threshold, &R) != ISING_OK) return fail(ISING_ERR_CAPACITY, "Stack array capacity exceeded");
-    *skyrmion_number = count_regions(R, g, particle_number);
+    *skyrmion_number = count_regions(R, S[0], g, particle_number);
     return ISING_OK;
 }
 
@@ -700,6 +746,6 @@ extern "C" int ising_skyrmion_number_density(const double* density, int fx, int 
     const Grid g{nx, ny, fx, fy};
     Regions R;
     if (grow_regions(S[0], g, q_threshold, &R) != ISING_OK) return fail(ISING_ERR_CAPACITY, "Stack array capacity exceeded");
-    *skyrmion_number = count_regions(R, g, particle_number);
+    *skyrmion_number = count_regions(R, S[0], g, particle_number);
     return ISING_OK;
 }
