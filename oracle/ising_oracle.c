@@ -1069,6 +1069,99 @@ long ora_colour_sweeps_omp(ora_mesh* m, const int* colour_of, int n_colours, uin
     return nacc;
 }
 
+/* ======================= optimised CPU checkerboard (baseline only) ======================= */
+/* The fastest CPU form of the sweep, for the CPU baseline: simple cubic, FP32 SoA planes in
+ * reference atom order (z fastest), colour (x+y+z)&1, the local-field form of
+ * calculateHeisenbergEnergy (energyMin.f90:86-171) with shell-1 exchange, bulk or
+ * interfacial DMI about z, Zeeman along z and the -K (S.e)^2 extension, ball or uniform
+ * proposals (energyMin.f90:49-68) and Philox4x32-10 draws keyed (site, sweep, replica,
+ * ensemble<<8) like the device sweep; OpenMP over (x, y) rows.  Returns accepted trials. */
+static inline float cb_u01f(uint32_t x) { return (float)(2u * (x >> 9) + 1u) * (1.0f / 16777216.0f); }
+
+long ora_cb_sweeps_f32(float* sx, float* sy, float* sz, int L, int n_sweeps, uint32_t sweep0,
+                       double beta, const ora_params* p, const ora_sweep_key* key, int n_threads)
+{
+    const int n = L;
+    const float J = (float)p->J, D = (float)p->Dz, B = (float)p->B, K = (float)p->K;
+    const float ex = (float)p->K_axis[0], ey = (float)p->K_axis[1], ez = (float)p->K_axis[2];
+    const float fb = (float)beta, r = (float)key->r;
+    const int bulk = p->dmi_bulk, move = key->move;
+    const uint32_t k0 = (uint32_t)key->seed, k1 = (uint32_t)(key->seed >> 32);
+    const uint32_t cw = (key->ensemble << 8);
+    long nacc = 0;
+    if (n_threads < 1) n_threads = 1;
+    for (int sw = 0; sw < n_sweeps; ++sw)
+        for (int colour = 0; colour < 2; ++colour) {
+            long acc = 0;
+#pragma omp parallel for num_threads(n_threads) reduction(+:acc) schedule(static) collapse(2)
+            for (int x = 0; x < n; ++x)
+                for (int y = 0; y < n; ++y) {
+                    const long row = ((long)x * n + y) * n;
+                    const long rxp = ((long)(x + 1 == n ? 0 : x + 1) * n + y) * n;
+                    const long rxm = ((long)(x == 0 ? n - 1 : x - 1) * n + y) * n;
+                    const long ryp = ((long)x * n + (y + 1 == n ? 0 : y + 1)) * n;
+                    const long rym = ((long)x * n + (y == 0 ? n - 1 : y - 1)) * n;
+                    for (int z = (x + y + colour) & 1; z < n; z += 2) {
+                        const int zp = z + 1 == n ? 0 : z + 1, zm = z == 0 ? n - 1 : z - 1;
+                        const long at = row + z;
+                        const float pxx = sx[rxp + z], pxy = sy[rxp + z], pxz = sz[rxp + z];
+                        const float mxx = sx[rxm + z], mxy = sy[rxm + z], mxz = sz[rxm + z];
+                        const float pyx = sx[ryp + z], pyy = sy[ryp + z], pyz = sz[ryp + z];
+                        const float myx = sx[rym + z], myy = sy[rym + z], myz = sz[rym + z];
+                        const float pzx = sx[row + zp], pzy = sy[row + zp], pzz = sz[row + zp];
+                        const float mzx = sx[row + zm], mzy = sy[row + zm], mzz = sz[row + zm];
+                        float hx = J * (pxx + mxx + pyx + myx + pzx + mzx);
+                        float hy = J * (pxy + mxy + pyy + myy + pzy + mzy);
+                        float hz = J * (pxz + mxz + pyz + myz + pzz + mzz);
+                        if (bulk) {
+                            hx += D * ((mzy - pzy) - (myz - pyz));
+                            hy += D * ((mxz - pxz) - (mzx - pzx));
+                            hz += D * ((myx - pyx) - (mxy - pxy));
+                        } else {
+                            hx += D * (pxz - mxz);
+                            hy += D * (pyz - myz);
+                            hz += D * ((mxx - pxx) - (pyy - myy));
+                        }
+                        hz -= B;
+                        /* Philox4x32-10, counter (site, sweep, replica, ensemble<<8) */
+                        uint32_t c0 = (uint32_t)at, c1 = sweep0 + (uint32_t)sw, c2 = key->replica, c3 = cw;
+                        uint32_t q0 = k0, q1 = k1;
+                        for (int i = 0; i < 10; ++i) {
+                            const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+                            c0 = (uint32_t)(p1 >> 32) ^ c1 ^ q0;
+                            c1 = (uint32_t)p1;
+                            c2 = (uint32_t)(p0 >> 32) ^ c3 ^ q1;
+                            c3 = (uint32_t)p0;
+                            q0 += 0x9E3779B9u;
+                            q1 += 0xBB67AE85u;
+                        }
+                        const float sxo = sx[at], syo = sy[at], szo = sz[at];
+                        const float cz = 2.0f * cb_u01f(c0) - 1.0f;
+                        const float st = sqrtf((1.0f - cz) * (1.0f + cz));
+                        const float ph = 6.28318531f * (cb_u01f(c1) - 0.5f);
+                        float vx = st * cosf(ph), vy = st * sinf(ph), vz = cz;
+                        if (move == 1) {
+                            const float rho = r * cbrtf(cb_u01f(c2));
+                            vx = sxo + rho * vx; vy = syo + rho * vy; vz = szo + rho * vz;
+                            const float in = 1.0f / sqrtf(vx * vx + vy * vy + vz * vz);
+                            vx *= in; vy *= in; vz *= in;
+                        }
+                        float dE = (vx - sxo) * hx + (vy - syo) * hy + (vz - szo) * hz;
+                        if (K != 0.0f) {
+                            const float e1 = vx * ex + vy * ey + vz * ez, e0 = sxo * ex + syo * ey + szo * ez;
+                            dE -= K * (e1 * e1 - e0 * e0);
+                        }
+                        if (dE <= 0.0f || cb_u01f(c3) < expf(-fb * dE)) {
+                            sx[at] = vx; sy[at] = vy; sz[at] = vz;
+                            ++acc;
+                        }
+                    }
+                }
+            nacc += acc;
+        }
+    return nacc;
+}
+
 void ora_init_uniform(ora_mesh* m, uint64_t seed, uint32_t ensemble, uint32_t replica)
 {
     for (long at = 0; at < m->natoms; ++at) {

@@ -124,6 +124,10 @@ typedef struct {
     double r;
     int philox_rounds;
 } ora_sweep_key;
+/* Optimised FP32 checkerboard sweep of a simple cubic L^3 mesh (CPU baseline only): SoA planes
+ * in reference atom order, OpenMP over rows; returns accepted trials. */
+long ora_cb_sweeps_f32(float* sx, float* sy, float* sz, int L, int n_sweeps, uint32_t sweep0,
+                       double beta, const ora_params* p, const ora_sweep_key* key, int n_threads);
 long ora_colour_pass(ora_mesh* m, const int* colour_of, int colour, uint32_t sweep,
                      double beta, const ora_params* p, const ora_sweep_key* key,
                      double* de_sum, uint8_t* accepted /* natoms or NULL */,

@@ -72,6 +72,9 @@ def lib():
         L.ora_winding_number.argtypes = [C.c_void_p, i]
         L.ora_winding_density.argtypes = [C.c_void_p, i, P(d)]
         L.ora_statistics.argtypes = [C.c_void_p, P(d), P(d), P(d)]
+        L.ora_cb_sweeps_f32.restype = l
+        L.ora_cb_sweeps_f32.argtypes = [P(C.c_float), P(C.c_float), P(C.c_float), i, i, C.c_uint32, d,
+                                        C.c_void_p, C.c_void_p, i]
         L.ora_gaussian_kernel.argtypes = [d, P(d)]
         L.ora_gaussian_filter_2d.restype = i
         L.ora_gaussian_filter_2d.argtypes = [P(d), i, i, d]
@@ -479,3 +482,13 @@ def winding_density_interpolated(mesh, z1, sclx=10, scly=10):
     """calculate_winding_density_interpolated (rsp:366-436) with the band-limited
     interpolation of spectral_upsample."""
     return fine_winding_density(spectral_upsample(std_grid(mesh, z1), sclx, scly))
+
+
+def cb_sweeps_f32(planes, L, n_sweeps, sweep0, beta, params, key, n_threads=1):
+    """The optimised FP32 checkerboard sweep (CPU baseline) on planes = float32 array (3, L^3)
+    in reference atom order, updated in place; returns the accepted count."""
+    assert planes.dtype == np.float32 and planes.flags["C_CONTIGUOUS"] and planes.shape == (3, L ** 3)
+    f = C.POINTER(C.c_float)
+    return lib().ora_cb_sweeps_f32(planes[0].ctypes.data_as(f), planes[1].ctypes.data_as(f),
+                                   planes[2].ctypes.data_as(f), L, n_sweeps, sweep0, beta,
+                                   C.byref(params), C.byref(key), n_threads)

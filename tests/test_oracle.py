@@ -253,3 +253,24 @@ def test_philox_stream_statistics(oracle):
         for b in range(a + 1, 4):
             assert abs(np.corrcoef(uf[:, a], uf[:, b])[0, 1]) < lim
     assert abs(uf.mean() - 0.5) < 5 * np.sqrt(1 / 12 / (4 * n))
+
+
+@pytest.mark.parametrize("bulk,move", [(True, 1), (True, 0), (False, 1), (False, 0)])
+def test_fast_cpu_checkerboard_replays_colour_pass(oracle, bulk, move):
+    """The optimised FP32 CPU sweep (the fastest CPU baseline) takes the same decisions as the
+    FP64 colour-class sweep with the same Philox keys: spins equal to FP32 rounding."""
+    L = 8
+    om = oracle.Mesh.sc(L)
+    om.init_uniform(5)
+    s0 = om.spins.copy()
+    p = oracle.Params(J=-1.0, Dz=0.7, B=0.3, K=0.05, dmi_bulk=bulk)
+    key = oracle.SweepKey(seed=0x15196, ensemble=0, replica=0, move=move, r=0.2, philox_rounds=10)
+    col = oracle.checkerboard(L, L, L)
+    for sw in range(2):
+        om.colour_pass(col, 0, sw, 2.0, p, key)
+        om.colour_pass(col, 1, sw, 2.0, p, key)
+    planes = np.ascontiguousarray(s0.T.astype(np.float32))
+    acc = oracle.cb_sweeps_f32(planes, L, 2, 0, 2.0, p, key, 2)
+    assert acc > 0
+    d = np.abs(planes.T.astype(np.float64) - om.spins).max(axis=1)
+    assert (d > 1e-4).sum() <= 2 and np.median(d) < 1e-6
