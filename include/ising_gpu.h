@@ -358,6 +358,12 @@ int ising_write_spins_csv(const ising_mesh* mesh, int replica, const char* path,
 int ising_write_pt_data_csv(const char* path, double J, double D, double B, double T,
                             double wnd_mid, int sk_mid, double wnd_spread, const double m[3]);
 int ising_pt_file_tag(char* buf, size_t cap, double J, double D, double B, double T);
+/* frame file name of the annealing driver: trim(output_dir)//"/frame_"//I5.5//".csv"
+ * (src/ISING.f90:218). */
+int ising_frame_filename(char* buf, size_t cap, const char* output_dir, int index);
+/* info.txt of the annealing driver (src/ISING.f90:232-237): frame count, then numCellsX and
+ * the lattice parameter, blank-separated as the visualisation scripts parse it. */
+int ising_write_frame_info(const char* path, int num_frames, int num_cells_x, float lattice_param);
 /* write_winding_number_density (rsp:544-580): "x,y,z,Winding_Density" with F0.8; the
  * densities come from one device pass, the records are formatted on all host threads. */
 int ising_write_winding_density_csv(const ising_mesh* mesh, int replica, const char* path);

@@ -150,6 +150,8 @@ _SIGS = {
     "ising_write_pt_data_csv": (_i, [C.c_char_p, _d, _d, _d, _d, _d, _i, _d, _P(_d)]),
     "ising_pt_file_tag": (_i, [C.c_char_p, C.c_size_t, _d, _d, _d, _d]),
     "ising_write_winding_density_csv": (_i, [_vp, _i, C.c_char_p]),
+    "ising_frame_filename": (_i, [C.c_char_p, C.c_size_t, C.c_char_p, _i]),
+    "ising_write_frame_info": (_i, [C.c_char_p, _i, _i, C.c_float]),
 }
 
 _lib = None

@@ -398,6 +398,18 @@ def pt_file_tag(J, D, B, T) -> str:
     return buf.value.decode()
 
 
+def frame_filename(output_dir: str, index: int) -> str:
+    """trim(output_dir)//"/frame_"//I5.5//".csv" of src/ISING.f90:218."""
+    buf = C.create_string_buffer(len(output_dir) + 64)
+    _lib.call("ising_frame_filename", buf, len(buf), output_dir.encode(), int(index))
+    return buf.value.decode()
+
+
+def write_frame_info(path: str, num_frames: int, numCellsX: int, latticeParam: float):
+    """info.txt of the annealing driver (src/ISING.f90:232-237)."""
+    _lib.call("ising_write_frame_info", path.encode(), int(num_frames), int(numCellsX), float(latticeParam))
+
+
 def write_pt_data_csv(path: str, J, D, B, T, winding_number_middle, skyrmion_number_middle,
                       winding_number_spread, magnetisation: Sequence[float]):
     """The data_<tag>.csv record of src/PT.f90:318-362."""

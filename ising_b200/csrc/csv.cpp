@@ -171,6 +171,37 @@ extern "C" int ising_write_pt_data_csv(const char* path, double J, double D, dou
     return write_all(path, out, false);
 }
 
+// write(frame_filename, '(A,A,I5.5,A)') trim(output_dir), "/frame_", index, ".csv"
+// (src/ISING.f90:218): five digits with leading zeros, ***** when the value does not fit.
+extern "C" int ising_frame_filename(char* buf, size_t cap, const char* output_dir, int index) {
+    if (!buf || !output_dir) return fail(ISING_ERR_ARG, "NULL argument");
+    std::string dir(output_dir);
+    while (!dir.empty() && dir.back() == ' ') dir.pop_back();   // trim()
+    // I5.5 needs five digits, so a negative value (which also needs its sign) does not fit
+    const std::string num = (index < 0 || index > 99999) ? std::string("*****") : fmt::I0m(index, 5);
+    const std::string s = dir + "/frame_" + num + ".csv";
+    if (s.size() + 1 > cap) return fail(ISING_ERR_ARG, "buffer too small");
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return ISING_OK;
+}
+
+// info.txt of the annealing driver (src/ISING.f90:232-237): the frame count, then numCellsX and
+// the default-real lattice parameter, list-directed: blank-separated, integers right-aligned in
+// 12 columns and the real with 9 significant digits.  The visualisation scripts read the two
+// lines with strip() and split() (skyrmion_evolution_simple.py:86-91, visualise_skyrmion.py:15-20).
+extern "C" int ising_write_frame_info(const char* path, int num_frames, int num_cells_x, float lattice_param) {
+    if (!path) return fail(ISING_ERR_ARG, "NULL argument");
+    char a[64], b[96];
+    std::snprintf(a, sizeof a, "%12d\n", num_frames);
+    const double v = (double)lattice_param;
+    const double av = std::fabs(v);
+    char r[48];
+    if (av != 0.0 && (av < 0.1 || av >= 1e8)) std::snprintf(r, sizeof r, "%.8E", v);
+    else std::snprintf(r, sizeof r, "%.*f", av == 0.0 ? 8 : 8 - (int)std::floor(std::log10(av)), v);
+    std::snprintf(b, sizeof b, "%12d   %s\n", num_cells_x, r);
+    return write_all(path, std::string(a) + b, false);
+}
+
 // (F0.4,"_",F0.4,"_",F0.4,"_",e0.4) of src/PT.f90:337-338
 extern "C" int ising_pt_file_tag(char* buf, size_t cap, double J, double D, double B, double T) {
     if (!buf) return fail(ISING_ERR_ARG, "NULL buffer");

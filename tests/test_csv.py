@@ -43,3 +43,22 @@ def test_formatters_agree_on_many_values(oracle, ib):
     for v in np.concatenate([rng.normal(size=200) * 10, [0.0, -0.0, 1e-9, -1e-9, 0.99995, -0.99995]]):
         tag = ib.pt_file_tag(float(v), 0.0, 0.0, 1.0)
         assert tag.split("_")[0] == oracle.fmt_F0(float(v), 4)
+
+
+def test_frame_filename_and_info(ib, tmp_path):
+    """Frame names as write(frame_filename, '(A,A,I5.5,A)') forms them (src/ISING.f90:218), and
+    info.txt read back the way the visualisation scripts parse it
+    (skyrmion_evolution_simple.py:86-91, visualise_skyrmion.py:15-20)."""
+    assert ib.frame_filename("./out   ", 7) == "./out/frame_00007.csv"
+    assert ib.frame_filename("o", 99999) == "o/frame_99999.csv"
+    assert ib.frame_filename("o", 100000) == "o/frame_*****.csv"
+    assert ib.frame_filename("o", -1) == "o/frame_*****.csv"
+    path = tmp_path / "info.txt"
+    for frames, cells, a in ((41, 16, 2.8), (1, 128, 1.0), (3, 96, 0.05), (0, 8, 3.5e9)):
+        ib.write_frame_info(str(path), frames, cells, a)
+        lines = path.read_text().splitlines(True)
+        assert len(lines) == 2
+        assert int(lines[0].strip()) == frames
+        mesh_params = lines[1].strip().split()
+        assert int(mesh_params[0]) == cells
+        assert float(mesh_params[1]) == pytest.approx(float(np.float32(a)), rel=1e-8)
