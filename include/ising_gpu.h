@@ -358,6 +358,9 @@ int ising_write_spins_csv(const ising_mesh* mesh, int replica, const char* path,
 int ising_write_pt_data_csv(const char* path, double J, double D, double B, double T,
                             double wnd_mid, int sk_mid, double wnd_spread, const double m[3]);
 int ising_pt_file_tag(char* buf, size_t cap, double J, double D, double B, double T);
+/* write_winding_number_density_interpolated (rsp:502-540): the density file of the fine grid
+ * of every slice (positions from the fine indices, as in the reference). */
+int ising_write_winding_density_interpolated_csv(const ising_mesh* mesh, int replica, const char* path);
 /* frame file name of the annealing driver: trim(output_dir)//"/frame_"//I5.5//".csv"
  * (src/ISING.f90:218). */
 int ising_frame_filename(char* buf, size_t cap, const char* output_dir, int index);

@@ -151,6 +151,7 @@ _SIGS = {
     "ising_pt_file_tag": (_i, [C.c_char_p, C.c_size_t, _d, _d, _d, _d]),
     "ising_write_winding_density_csv": (_i, [_vp, _i, C.c_char_p]),
     "ising_frame_filename": (_i, [C.c_char_p, C.c_size_t, C.c_char_p, _i]),
+    "ising_write_winding_density_interpolated_csv": (_i, [_vp, _i, C.c_char_p]),
     "ising_write_frame_info": (_i, [C.c_char_p, _i, _i, C.c_float]),
 }
 

@@ -398,6 +398,11 @@ def pt_file_tag(J, D, B, T) -> str:
     return buf.value.decode()
 
 
+def write_winding_number_density_interpolated(mesh: ChainMesh, filepath: str, replica: int = 0):
+    """write_winding_number_density_interpolated (rsp:502-540)."""
+    _lib.call("ising_write_winding_density_interpolated_csv", mesh.handle, replica, filepath.encode())
+
+
 def frame_filename(output_dir: str, index: int) -> str:
     """trim(output_dir)//"/frame_"//I5.5//".csv" of src/ISING.f90:218."""
     buf = C.create_string_buffer(len(output_dir) + 64)

@@ -238,3 +238,37 @@ extern "C" int ising_write_winding_density_csv(const ising_mesh* m, int replica,
     parts.push_back("\n");
     return write_parts(path, parts, false);
 }
+
+// write_winding_number_density_interpolated (rsp:502-540): the same records as
+// write_winding_number_density over the (sclx nx) x (scly ny) fine grid of every slice; the
+// position of record (j, k) of slice i is j a + k b + i c with the FINE indices j, k, as in the
+// reference.
+extern "C" int ising_write_winding_density_interpolated_csv(const ising_mesh* m, int replica, const char* path) {
+    if (!m || !path) return fail(ISING_ERR_ARG, "NULL argument");
+    const Lattice& L = m->lat;
+    int sx = 0, sy = 0;
+    int st = ising_mesh_interpolation_scale(m, &sx, &sy);
+    if (st != ISING_OK) return st;
+    const int fx = L.nx * sx, fy = L.ny * sy;
+    const int64_t plane = (int64_t)fx * fy;
+    std::vector<double> dens((size_t)plane);
+    std::vector<std::string> parts;
+    parts.emplace_back("x,y,z,Winding_Density\n");
+    for (int i = 1; i <= L.nz; ++i) {
+        st = ising_winding_density_interpolated(m, replica, i, dens.data());
+        if (st != ISING_OK) return st;
+        std::vector<std::string> slice = format_records(plane, 4 * 14, [&](int64_t r, std::string& o) {
+            const int j = (int)(r / fy) + 1, k = (int)(r % fy) + 1;
+            double pos[3];
+            for (int c = 0; c < 3; ++c) pos[c] = ((double)j * L.av[c] + (double)k * L.bv[c]) + (double)i * L.cv[c];
+            fmt::F0_app(o, pos[0], 8); o += ',';
+            fmt::F0_app(o, pos[1], 8); o += ',';
+            fmt::F0_app(o, pos[2], 8); o += ',';
+            fmt::F0_app(o, dens[(size_t)((j - 1) + (int64_t)(k - 1) * fx)], 8);
+            o += "\n\n";
+        });
+        for (auto& x : slice) parts.push_back(std::move(x));
+    }
+    parts.push_back("\n");
+    return write_parts(path, parts, false);
+}

@@ -173,3 +173,22 @@ def test_interpolation_scale_checks(ib, cuda_ok):
     with pytest.raises(ib.IsingError):
         ib.calculate_skyrmion_number(pm, 5, 0.3, 1, 0.5)
     pm.close()
+
+
+def test_interpolated_density_csv_bytes(oracle, ib, cuda_ok, tmp_path):
+    """write_winding_number_density_interpolated (rsp:502-540): F0.8 records over the fine grid
+    of every slice, positions j a + k b + i c from the fine indices, byte-equal to the oracle's
+    formats on the device densities."""
+    om, pm = _skyrmion_pair(oracle, ib, L=6, nz=4, scale=(2, 3))
+    path = tmp_path / "density_interp.csv"
+    ib.write_winding_number_density_interpolated(pm, str(path))
+    av, bv, cv = om.vectors()[:3]
+    out = ["x,y,z,Winding_Density\n"]
+    for i in range(1, 5):
+        dens = ib.calculate_winding_density_interpolated(pm, i)
+        for j in range(1, 13):
+            for k in range(1, 19):
+                pos = (j * av + k * bv) + i * cv
+                out.append(",".join(oracle.fmt_F0(float(v), 8) for v in (*pos, dens[j - 1, k - 1])) + "\n\n")
+    out.append("\n")
+    assert path.read_text() == "".join(out)
