@@ -76,16 +76,58 @@ def host_cores():
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock and clock-event reasons of the timed GPU while the timed region runs.
+
+    NVML is polled from a background thread every 5 ms (read-only queries), so even a timed
+    region of a few tens of milliseconds holds several samples; without NVML an
+    `nvidia-smi -lms 200` subprocess is the fallback."""
     FIELDS = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_S = 0.005
 
     def __init__(self, bus=None):
         self.bus = bus if isinstance(bus, int) else None  # PCI bus number of the timed GPU
         self.proc = None
+        self.thread = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
 
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        self.nv = pynvml
+        n = pynvml.nvmlDeviceGetCount()
+        for i in range(n):
+            h = pynvml.nvmlDeviceGetHandleByIndex(i)
+            if self.bus is None or pynvml.nvmlDeviceGetPciInfo(h).bus == self.bus:
+                return h
+        return None
+
     def start(self):
+        import threading
+        try:
+            h = self._nvml_handle()
+        except Exception:
+            h = None
+        if h is not None:
+            nv = self.nv
+            self.samples = []
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.stop_evt = threading.Event()
+
+            def poll():
+                while True:
+                    try:
+                        self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                             nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                    except Exception:
+                        pass
+                    if self.stop_evt.wait(self.PERIOD_S):
+                        break
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
@@ -96,6 +138,23 @@ class ClockSampler:
 
     def stop(self):
         out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.thread is not None:
+            self.stop_evt.set()
+            self.thread.join(timeout=5)
+            nv = self.nv
+            flags = [("hw_slowdown", nv.nvmlClocksEventReasonHwSlowdown),
+                     ("hw_thermal_slowdown", nv.nvmlClocksEventReasonHwThermalSlowdown),
+                     ("sw_thermal_slowdown", nv.nvmlClocksEventReasonSwThermalSlowdown),
+                     ("sw_power_cap", nv.nvmlClocksEventReasonSwPowerCap)]
+            if self.samples:
+                out.update(sm_mhz=statistics.median(c for c, _ in self.samples), sm_max_mhz=self.max_mhz,
+                           reasons=sorted({n for _, r in self.samples for n, bit in flags if r & bit}),
+                           samples=len(self.samples), source="nvml")
+            try:
+                nv.nvmlShutdown()
+            except Exception:
+                pass
+            return out
         if self.proc is None:
             return out
         self.proc.terminate()
@@ -125,7 +184,8 @@ class ClockSampler:
             return out
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() in ("active", "1")})
-        out.update(sm_mhz=statistics.median(sm), sm_max_mhz=mx, reasons=reasons, samples=len(rows))
+        out.update(sm_mhz=statistics.median(sm), sm_max_mhz=mx, reasons=reasons, samples=len(rows),
+                   source="nvidia-smi")
         return out
 
 
@@ -399,7 +459,8 @@ def run_gpu(args, w):
                          "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
                          "kernel": kernel_name, "launch_ms": launch_ms, "bytes_per_launch": bytes_per_launch,
                          "basis": "24 B per attempted update (one FP32 x,y,z read + write per site per sweep)"},
-            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                       "samples": clk["samples"]},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "cpu_fastest": cpu_fast,
@@ -516,7 +577,8 @@ def run_stats(args, w):
                        "timer": "host wall clock around synchronous C-ABI calls (device and host stages)"},
             "result": {"skyrmion_number_middle": sk, "winding_number_middle": wmid,
                        "winding_number_spread": wspread, "magnetisation": list(map(float, mag))},
-            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
+                       "samples": clocks["samples"]},
             "e2e": {"value": 1.0 / e2e_dt, "unit": "statistics calls/s", "h2d_bytes_per_step": int(spins.size * 8),
                     "d2h_bytes_per_step": int(20 * L * L * 8 + 2 * nz * 8 + 20 * 12),
                     "path": "ising_spins_set (host doubles) -> ising_chain_mesh_statistics; d2h excludes the "
