@@ -75,96 +75,113 @@ def host_cores():
 
 
 # ---------------------------------------------------------------- clocks
+_NVML_POLLER = r"""
+import sys, time
+import pynvml as nv
+nv.nvmlInit()
+bus = int(sys.argv[1])
+h = None
+for i in range(nv.nvmlDeviceGetCount()):
+    d = nv.nvmlDeviceGetHandleByIndex(i)
+    if bus < 0 or nv.nvmlDeviceGetPciInfo(d).bus == bus:
+        h = d
+        break
+mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+print("max", mx, flush=True)
+while True:
+    print(time.time_ns(), nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), nv.nvmlDeviceGetCurrentClocksEventReasons(h),
+          flush=True)
+    time.sleep(0.002)
+"""
+
+
 class ClockSampler:
     """SM clock and clock-event reasons of the timed GPU while the timed region runs.
 
-    NVML is polled from a background thread every 5 ms (read-only queries), so even a timed
-    region of a few tens of milliseconds holds several samples; without NVML an
-    `nvidia-smi -lms 200` subprocess is the fallback."""
+    A separate process polls NVML (read-only queries) every ~2 ms and timestamps each sample;
+    mark() / stop() bracket the timed region and only samples inside it are kept.  (An
+    in-process NVML poller waits behind the CUDA driver call that blocks on the stream.)
+    Without NVML an `nvidia-smi -lms 200` subprocess is the fallback."""
     FIELDS = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-    PERIOD_S = 0.005
+    # NVML clock-event reason bits (nvmlClocksEventReason*)
+    REASONS = (("sw_power_cap", 0x4), ("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20),
+               ("hw_thermal_slowdown", 0x40))
 
     def __init__(self, bus=None):
         self.bus = bus if isinstance(bus, int) else None  # PCI bus number of the timed GPU
         self.proc = None
-        self.thread = None
+        self.kind = None
+        self.t0 = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
 
-    def _nvml_handle(self):
-        import pynvml
-        pynvml.nvmlInit()
-        self.nv = pynvml
-        n = pynvml.nvmlDeviceGetCount()
-        for i in range(n):
-            h = pynvml.nvmlDeviceGetHandleByIndex(i)
-            if self.bus is None or pynvml.nvmlDeviceGetPciInfo(h).bus == self.bus:
-                return h
-        return None
-
     def start(self):
-        import threading
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        self.f = open(self.path, "w")
         try:
-            h = self._nvml_handle()
-        except Exception:
-            h = None
-        if h is not None:
-            nv = self.nv
-            self.samples = []
-            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-            self.stop_evt = threading.Event()
-
-            def poll():
-                while True:
-                    try:
-                        self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
-                                             nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
-                    except Exception:
-                        pass
-                    if self.stop_evt.wait(self.PERIOD_S):
-                        break
-
-            self.thread = threading.Thread(target=poll, daemon=True)
-            self.thread.start()
-            return
-        try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml  # noqa: F401
+            self.proc = subprocess.Popen([sys.executable, "-c", _NVML_POLLER, str(-1 if self.bus is None else self.bus)],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+            self.kind = "nvml"
+            deadline = time.time() + 10.0
+            while time.time() < deadline and self.proc.poll() is None:   # wait for the first sample
+                if sum(1 for _ in open(self.path)) >= 2:
+                    break
+                time.sleep(0.01)
+            if self.proc.poll() is None:
+                self.t0 = time.time_ns()
+                return
+            self.proc = None
         except Exception:
             self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            self.kind = "nvidia-smi"
+        except Exception:
+            self.proc = None
+        self.t0 = time.time_ns()
+
+    def mark(self):
+        """Start of the timed region (after warm-up work queued since start())."""
+        self.t0 = time.time_ns()
 
     def stop(self):
+        t1 = time.time_ns()
         out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        if self.thread is not None:
-            self.stop_evt.set()
-            self.thread.join(timeout=5)
-            nv = self.nv
-            flags = [("hw_slowdown", nv.nvmlClocksEventReasonHwSlowdown),
-                     ("hw_thermal_slowdown", nv.nvmlClocksEventReasonHwThermalSlowdown),
-                     ("sw_thermal_slowdown", nv.nvmlClocksEventReasonSwThermalSlowdown),
-                     ("sw_power_cap", nv.nvmlClocksEventReasonSwPowerCap)]
-            if self.samples:
-                out.update(sm_mhz=statistics.median(c for c, _ in self.samples), sm_max_mhz=self.max_mhz,
-                           reasons=sorted({n for _, r in self.samples for n, bit in flags if r & bit}),
-                           samples=len(self.samples), source="nvml")
-            try:
-                nv.nvmlShutdown()
-            except Exception:
-                pass
-            return out
         if self.proc is None:
             return out
+        if self.kind == "nvml":
+            time.sleep(0.01)   # one more sample after the region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
         self.f.close()
+        lines = open(self.path).read().split("\n")
+        if self.kind == "nvml":
+            mx, rows = None, []
+            for line in lines:
+                parts = line.split()
+                if len(parts) == 2 and parts[0] == "max":
+                    mx = int(parts[1])
+                elif len(parts) == 3:
+                    try:
+                        rows.append((int(parts[0]), int(parts[1]), int(parts[2])))
+                    except ValueError:
+                        pass
+            inside = [r for r in rows if self.t0 <= r[0] <= t1]
+            if not inside and rows:   # region shorter than the poll period: the nearest samples
+                inside = sorted(rows, key=lambda r: min(abs(r[0] - self.t0), abs(r[0] - t1)))[:2]
+            if inside:
+                out.update(sm_mhz=statistics.median(r[1] for r in inside), sm_max_mhz=mx,
+                           reasons=sorted({n for r in inside for n, bit in self.REASONS if r[2] & bit}),
+                           samples=len(inside), source="nvml")
+            return out
         rows = []
-        for line in open(self.path):
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -348,6 +365,7 @@ def run_gpu(args, w):
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
+    clocks.mark()
     ev0.record(stream)
     run(args.steps)
     ev1.record(stream)
@@ -546,6 +564,7 @@ def run_stats(args, w):
     clk = ClockSampler(getattr(torch.cuda.get_device_properties(local), "pci_bus_id", None))
     clk.start()
     torch.cuda.synchronize()
+    clk.mark()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         res = ib.chain_mesh_statistics_full(mesh)
