@@ -372,6 +372,15 @@ int ising_write_frame_info(const char* path, int num_frames, int num_cells_x, fl
 int ising_write_winding_density_csv(const ising_mesh* mesh, int replica, const char* path);
 
 /* ---------------------------------------------------------------- learned patch proposal */
+/* 3^3 convolution of a channel-last BF16 grid (nwin windows of Gi^3 cells x C channels, C = 8
+ * or 32) onto Go^3 output cells with zero padding pad, as an implicit GEMM on the tensor cores:
+ * out(row, n) = bias[n] + sum_{o, ch} in[window][cell(row) + offset(o) - pad][ch] w[n][o C + ch]
+ * with K = 27 C rounded up to 16, rows = nwin Go^3 (FP32 rows in c and/or GELU'd BF16 rows in
+ * o_bf16).  loader: 0 = automatic, 1 = register-staged operands, 2 = TMA copies (C = 32,
+ * Go = 4 only).  No reference counterpart (the learned proposal's network). */
+int ising_conv3_bf16(const void* in, int C, int Gi, int Go, int pad, int nwin, const void* w, int ldb, int N,
+                     const float* bias, float* c, int ldc, void* o_bf16, int ldo, int gelu, int loader,
+                     void* stream);
 /* Tensor-core GEMM on device buffers (no reference counterpart): c / o_bf16 (M x N) =
  * a (M x K, BF16, K contiguous) * b (N x K, BF16)^T (+ bias[N]); o_bf16 gets GELU(tanh form)
  * of the sum when gelu = 1.  N multiple of 16 up to 256, K multiple of 16, row pitches

@@ -218,6 +218,7 @@ int launch_gemm_bf16(GemmArgs g, cudaStream_t s) {
         return fail(ISING_ERR_ARG, "GEMM FP32 output needs a 16-byte aligned base and ldc % 4 == 0");
     if (g.O && (g.ldo % 8 || g.ldo < g.N || (reinterpret_cast<uintptr_t>(g.O) & 15)))
         return fail(ISING_ERR_ARG, "GEMM BF16 output needs a 16-byte aligned base and ldo % 8 == 0");
+    if (g.loader == 2 || (g.loader == 0 && conv_tma_applies(g))) return launch_conv_tma(g, s);
     g.tmem_cols = g.N <= 32 ? 32 : g.N <= 64 ? 64 : g.N <= 128 ? 128 : 256;
     // resident blocks per SM x TMEM columns must fit the SM's 512 columns: a block whose
     // allocation cannot be met would stall until another block frees its columns
@@ -244,6 +245,30 @@ static __device__ int g_gemm_status;
 }  // namespace isg
 
 using namespace isg;
+
+extern "C" int ising_conv3_bf16(const void* in, int C, int Gi, int Go, int pad, int nwin, const void* w, int ldb, int N,
+                                const float* bias, float* c, int ldc, void* o_bf16, int ldo, int gelu, int loader,
+                                void* stream) {
+    if (!in || !w || (!c && !o_bf16)) return fail(ISING_ERR_ARG, "NULL operand");
+    if (nwin < 1 || loader < 0 || loader > 2) return fail(ISING_ERR_ARG, "bad window count or loader");
+    int* st = nullptr;
+    ISG_CUDA(cudaGetSymbolAddress((void**)&st, g_gemm_status));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    ISG_CUDA(cudaMemsetAsync(st, 0, sizeof(int), s));
+    GemmArgs g{};
+    g.B = static_cast<const __nv_bfloat16*>(w); g.ldb = ldb;
+    g.M = nwin * Go * Go * Go; g.N = N; g.K = (27 * C + 15) / 16 * 16; g.bias = bias; g.C = c; g.ldc = ldc;
+    g.O = static_cast<__nv_bfloat16*>(o_bf16); g.ldo = ldo; g.gelu = gelu; g.status = st;
+    g.conv_in = static_cast<const __nv_bfloat16*>(in); g.conv_C = C; g.conv_Gi = Gi; g.conv_Go = Go; g.conv_pad = pad;
+    g.loader = loader;
+    int r = launch_gemm_bf16(g, s);
+    if (r != ISING_OK) return r;
+    int h = 0;
+    ISG_CUDA(cudaMemcpyAsync(&h, st, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ISG_CUDA(cudaStreamSynchronize(s));
+    if (h & kStatTimeout) return fail(ISING_ERR_TIMEOUT, "tensor-core convolution: an mbarrier wait gave up");
+    return ISING_OK;
+}
 
 extern "C" int ising_bf16_gemm(const void* a, int lda, const void* b, int ldb, int M, int N, int K, const float* bias,
                                float* c, int ldc, void* o_bf16, int ldo, int gelu, void* stream) {

@@ -31,9 +31,16 @@ struct GemmArgs {
     // o >= 27 or for row >= M
     const __nv_bfloat16* conv_in;
     int conv_C, conv_Gi, conv_Go, conv_pad;
+    // operand path: 0 = TMA copies where the shape allows (conv_tma.cu), else registers;
+    // 1 = register-staged loader; 2 = TMA copies (an error where the shape does not allow)
+    int loader;
     uint32_t tmem_cols;     // set by the launcher
 };
 int launch_gemm_bf16(GemmArgs g, cudaStream_t s);
+// 3^3 convolution over 32 channels onto a 4^3 output grid (pad 0 from 6^3, pad 1 from 4^3)
+// with TMA-fed operands (conv_tma.cu)
+bool conv_tma_applies(const GemmArgs& g);
+int launch_conv_tma(const GemmArgs& g, cudaStream_t s);
 
 // forward of nb windows ([nb][3][8][8][8] FP32, device) on stream s; *out = [nb*64][4]
 int net_forward_on(ising_net* n, const float* d_windows, int nb, cudaStream_t s, const float** out);
