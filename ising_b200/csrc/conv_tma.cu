@@ -197,6 +197,156 @@ __global__ void __launch_bounds__(kCtThreads) k_conv_tma(const __grid_constant__
     if (warp == 0) tmem_dealloc(taddr, g.tmem_cols);
 }
 
+// First layer: 3^3 convolution over an 8-channel grid (8^3 cells) onto its 6^3 valid output
+// cells.  A block computes one window: its 216 rows sit in a 256-row tile covered by two
+// M = 128 MMAs with accumulators in TMEM columns [0, N) and [N, 2N).  Kernel offset t is one
+// 216 x 8 box (16-byte rows, no swizzle) copied densely into a 256-row buffer, which is the
+// canonical no-swizzle K-major layout with 8-row groups 128 bytes apart; the two offsets of
+// a K = 16 step sit in consecutive buffers (leading offset 4 KB), as do their N x 8 weight
+// slices.  Offset 27 pads K to 224: its box lies wholly outside the tensor (window index
+// nwin) and TMA fills it with zeros.  Rows 216..255 of a buffer are never written and feed
+// only the discarded accumulator rows.
+constexpr int kC8Stages = 4;
+constexpr int kC8Pairs = 14;                  // 28 offsets (27 + the zero pad), two per K step
+constexpr uint32_t kC8TapA = 256u * 16u;      // 256 rows x 8 BF16
+
+struct Conv8Args {
+    int M, N, nwin;
+    const float* bias;
+    float* C;
+    int ldc, accumulate;
+    __nv_bfloat16* O;
+    int ldo, gelu;
+    int* status;
+    uint32_t tmem_cols;
+};
+
+__global__ void __launch_bounds__(kCtThreads) k_conv8_tma(const __grid_constant__ CUtensorMap tA,
+                                                          const __grid_constant__ CUtensorMap tB,
+                                                          const Conv8Args g) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    const int N = g.N;
+    const uint32_t tapB = (uint32_t)N * 16u;
+    const uint32_t stage_bytes = 2u * kC8TapA + 2u * tapB;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kC8Stages * stage_bytes);
+    uint64_t* empty = full + kC8Stages;
+    uint64_t* done = empty + kC8Stages;
+    uint32_t* slot = reinterpret_cast<uint32_t*>(done + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int win = (int)blockIdx.x;
+
+    if (warp == 0) tmem_alloc(slot, g.tmem_cols);
+    if (tid == 0) {
+        for (int s = 0; s < kC8Stages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        mbar_init_fence();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t taddr = *slot;
+
+    bool ok = true;
+    if (tid == 0) {
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tA)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tB)) : "memory");
+        const uint32_t tx = 2u * (216u * 16u + tapB);
+        const uint32_t idesc = umma_idesc_bf16(128, N);
+        auto issue = [&](int p) {
+            const int s = p % kC8Stages;
+            unsigned char* st = smem + s * stage_bytes;
+            ct_expect_tx(&full[s], tx);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int t = 2 * p + h;
+                if (t < kCtTaps)
+                    tma_load_5d(st + h * kC8TapA, &tA, 0, t % 3, (t / 3) % 3, t / 9, win, &full[s]);
+                else   // the pad offset: a box outside the tensor reads as zeros
+                    tma_load_5d(st + h * kC8TapA, &tA, 0, 0, 0, 0, g.nwin, &full[s]);
+                tma_load_2d(st + 2u * kC8TapA + h * tapB, &tB, 8 * t, 0, &full[s]);
+            }
+        };
+        int issued = 0;
+        for (; issued < kC8Stages && issued < kC8Pairs; ++issued) issue(issued);
+        int p = 0;
+        for (; p < kC8Pairs && ok; ++p) {
+            const int s = p % kC8Stages;
+            ok = mbar_wait(&full[s], (uint32_t)((p / kC8Stages) & 1), kCtWaitPolls);
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(smem + s * stage_bytes), b0 = a0 + 2u * kC8TapA;
+            const uint64_t bd = umma_smem_desc(b0, tapB, 128u);
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                umma_bf16(taddr + (uint32_t)(h * N), umma_smem_desc(a0 + (uint32_t)h * 2048u, kC8TapA, 128u), bd, idesc,
+                          p > 0 ? 1u : 0u);
+            umma_commit(&empty[s]);
+            if (p >= 1 && issued < kC8Pairs) {
+                const int ps = (p - 1) % kC8Stages;
+                ok = mbar_wait(&empty[ps], (uint32_t)(((p - 1) / kC8Stages) & 1), kCtWaitPolls);
+                if (ok) issue(issued++);
+            }
+        }
+        if (!ok) {
+            for (int u = p; u < issued; ++u) mbar_wait(&full[u % kC8Stages], (uint32_t)((u / kC8Stages) & 1), 1u << 20);
+            atomicOr(g.status, kStatTimeout);
+        }
+        umma_commit(done);
+    }
+    ok = __syncthreads_and(ok);
+    const bool fin = mbar_wait(done, 0u, kCtWaitPolls);
+    tc_fence_after();
+    if (!fin && tid == 0) atomicOr(g.status, kStatTimeout);
+    if (ok && fin) {
+        for (int h = 0; h < 2; ++h) {
+            const int u = h * 128 + warp * 32 + lane;     // output cell of this window
+            const int row = win * 216 + u;
+            for (int cb = 0; cb < N; cb += 16) {
+                float v[16];
+                tmem_ld16(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * N + cb), v);
+                if (u < 216 && row < g.M) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) v[i] += g.bias ? g.bias[cb + i] : 0.f;
+                    if (g.C) {
+                        float4* cp = reinterpret_cast<float4*>(g.C + (size_t)row * g.ldc + cb);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                            if (g.accumulate) {
+                                const float4 o = cp[q];
+                                x.x += o.x; x.y += o.y; x.z += o.z; x.w += o.w;
+                            }
+                            cp[q] = x;
+                        }
+                    }
+                    if (g.O) {
+                        uint4* op = reinterpret_cast<uint4*>(g.O + (size_t)row * g.ldo + cb);
+#pragma unroll
+                        for (int q = 0; q < 2; ++q) {
+                            uint32_t w[4];
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                const float a = g.gelu ? ct_gelu(v[8 * q + 2 * e]) : v[8 * q + 2 * e];
+                                const float b = g.gelu ? ct_gelu(v[8 * q + 2 * e + 1]) : v[8 * q + 2 * e + 1];
+                                const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
+                                w[e] = *reinterpret_cast<const uint32_t*>(&h2);
+                            }
+                            op[q] = make_uint4(w[0], w[1], w[2], w[3]);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(taddr, g.tmem_cols);
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static bool tried = false;
@@ -211,25 +361,84 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
+bool conv8_shape(const GemmArgs& g) {
+    return g.conv_in && g.conv_C == 8 && g.conv_Gi == 8 && g.conv_Go == 6 && g.conv_pad == 0 && g.K == 224 &&
+           g.M % 216 == 0 && g.N % 16 == 0 && g.N <= 128;
+}
+
+bool conv32_shape(const GemmArgs& g) {
+    return g.conv_in && g.conv_C == 32 && g.conv_Go == 4 && g.K == 27 * 32 && (g.conv_pad == 0 || g.conv_pad == 1) &&
+           g.conv_Gi == 4 + 2 - 2 * g.conv_pad && g.M % 64 == 0 && g.N % 16 == 0 && g.N <= 256;
+}
+
+int launch_conv8_tma(const GemmArgs& g, cudaStream_t s) {
+    // tensor-map rules checked before any copy: 16-byte aligned bases, strides multiples of
+    // 16 bytes, 16-byte inner boxes, innermost coordinates 0 and 8 t (16 t bytes)
+    if ((reinterpret_cast<uintptr_t>(g.conv_in) & 15) || (reinterpret_cast<uintptr_t>(g.B) & 15) || g.ldb % 8 ||
+        g.ldb < g.K)
+        return fail(ISING_ERR_ARG, "TMA convolution: operands must be 16-byte aligned with ldb % 8 == 0");
+    const int nwin = g.M / 216;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+    CUtensorMap tA, tB;
+    {
+        const cuuint64_t dims[5] = {8, 8, 8, 8, (cuuint64_t)nwin};
+        const cuuint64_t strides[4] = {16, 128, 1024, 8192};
+        const cuuint32_t box[5] = {8, 6, 6, 6, 1};
+        const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+        if (enc(&tA, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(g.conv_in), dims, strides, box, es,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return fail(ISING_ERR_CUDA, "cuTensorMapEncodeTiled (first-layer windows) failed");
+    }
+    {
+        const cuuint64_t dims[2] = {(cuuint64_t)g.K, (cuuint64_t)g.N};
+        const cuuint64_t strides[1] = {(cuuint64_t)g.ldb * 2};
+        const cuuint32_t box[2] = {8, (cuuint32_t)g.N};
+        const cuuint32_t es[2] = {1, 1};
+        if (enc(&tB, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(g.B), dims, strides, box, es,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return fail(ISING_ERR_CUDA, "cuTensorMapEncodeTiled (first-layer weights) failed");
+    }
+    Conv8Args a{};
+    a.M = g.M; a.N = g.N; a.nwin = nwin; a.bias = g.bias; a.C = g.C; a.ldc = g.ldc; a.accumulate = g.accumulate;
+    a.O = g.O; a.ldo = g.ldo; a.gelu = g.gelu; a.status = g.status;
+    a.tmem_cols = 2 * g.N <= 32 ? 32 : 2 * g.N <= 64 ? 64 : 2 * g.N <= 128 ? 128 : 256;
+    int smem = 1024 + kC8Stages * (int)(2u * kC8TapA + 2u * (uint32_t)g.N * 16u) + (2 * kC8Stages + 1) * 8 + 16;
+    static bool attr_set = false;
+    if (!attr_set) {
+        ISG_CUDA(cudaFuncSetAttribute(k_conv8_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_set = true;
+    }
+    for (;;) {
+        int occ = 0;
+        ISG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv8_tma, kCtThreads, smem));
+        if (occ * (int)a.tmem_cols <= 512 || smem >= 200 * 1024) break;
+        smem += 8 * 1024;
+    }
+    k_conv8_tma<<<nwin, kCtThreads, smem, s>>>(tA, tB, a);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
 }  // namespace
 
 bool conv_tma_applies(const GemmArgs& g) {
-    return g.conv_in && g.conv_C == 32 && g.conv_Go == 4 && g.K == 27 * 32 && (g.conv_pad == 0 || g.conv_pad == 1) &&
-           g.conv_Gi == 4 + 2 - 2 * g.conv_pad && g.M % 64 == 0 && g.N % 16 == 0 && g.N <= 256 &&
-           encode_fn() != nullptr;
+    return (conv32_shape(g) || conv8_shape(g)) && encode_fn() != nullptr;
 }
 
 int launch_conv_tma(const GemmArgs& g, cudaStream_t s) {
     if (!conv_tma_applies(g)) return fail(ISING_ERR_ARG, "TMA convolution: unsupported shape");
+    if (g.C && (g.ldc % 4 || g.ldc < g.N || (reinterpret_cast<uintptr_t>(g.C) & 15)))
+        return fail(ISING_ERR_ARG, "GEMM FP32 output needs a 16-byte aligned base and ldc % 4 == 0");
+    if (g.O && (g.ldo % 8 || g.ldo < g.N || (reinterpret_cast<uintptr_t>(g.O) & 15)))
+        return fail(ISING_ERR_ARG, "GEMM BF16 output needs a 16-byte aligned base and ldo % 8 == 0");
+    if (conv8_shape(g)) return launch_conv8_tma(g, s);
     // the tensor-map rules, checked before any copy is issued: 16-byte aligned bases, strides
     // multiples of 16 bytes, a 64-byte inner box (<= the 64-byte swizzle span), boxes <= 256
     if ((reinterpret_cast<uintptr_t>(g.conv_in) & 15) || (reinterpret_cast<uintptr_t>(g.B) & 15) || g.ldb % 8 ||
         g.ldb < g.K)
         return fail(ISING_ERR_ARG, "TMA convolution: operands must be 16-byte aligned with ldb % 8 == 0");
-    if (g.C && (g.ldc % 4 || g.ldc < g.N || (reinterpret_cast<uintptr_t>(g.C) & 15)))
-        return fail(ISING_ERR_ARG, "GEMM FP32 output needs a 16-byte aligned base and ldc % 4 == 0");
-    if (g.O && (g.ldo % 8 || g.ldo < g.N || (reinterpret_cast<uintptr_t>(g.O) & 15)))
-        return fail(ISING_ERR_ARG, "GEMM BF16 output needs a 16-byte aligned base and ldo % 8 == 0");
     const int nwin = g.M / 64, Gi = g.conv_Gi;
     PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
     CUtensorMap tA, tB;
