@@ -868,6 +868,15 @@ def run_c5(args, w):
         within[name] = ok
     qp = float(np.mean([ap[t]["ess_Q_per_s"] for t in live])) if live else 0.0
     ql = float(np.mean([al[t]["ess_Q_per_s"] for t in live])) if live else 0.0
+    # per-slot ratios: the mean of ESS/s over slots is dominated by the slots with the shortest tau
+    ratios = [al[t]["ess_Q_per_s"] / ap[t]["ess_Q_per_s"] for t in live if ap[t]["ess_Q_per_s"] > 0]
+    per_slot = {"ratios": [round(r, 3) for r in ratios],
+                "median": float(np.median(ratios)) if ratios else None,
+                "geometric_mean": float(np.exp(np.mean(np.log(ratios)))) if ratios else None,
+                "slots_learned_better": sum(1 for r in ratios if r > 1.0)}
+    # a windowed tau estimate means something only for chains much longer than tau (N >= 50 tau)
+    reliable = {"plain": sum(1 for t in live if n_plain >= 50 * ap[t]["tau_Q"]),
+                "learned": sum(1 for t in live if n_learned >= 50 * al[t]["tau_Q"]), "of": len(live)}
     line = {
         "metric": "spin-updates/s", "value": value, "unit": "spin-updates/s", "n_gpus": 1, "steps": n_plain,
         "warmup": args.c5_therm, "ms_per_step": 1e3 * t_plain / n_plain, "higher_is_better": True, "scaling": "weak",
@@ -877,7 +886,9 @@ def run_c5(args, w):
         "q_ess": {"metric": "Q-ESS/s (mean over the temperature slots where Q fluctuates in both runs)",
                   "slots_used": live, "plain": qp, "learned": ql,
                   "learned_over_plain": ql / qp if qp > 0 else None,
+                  "learned_over_plain_per_slot": per_slot,
                   "plain_sweeps": n_plain, "learned_steps": n_learned,
+                  "slots_with_N_ge_50_tauQ": reliable,
                   "s_per_step": {"plain": t_plain / n_plain, "learned": t_learned / n_learned},
                   "plain_s": t_plain, "learned_s": t_learned,
                   "tau_Q_plain": [round(x["tau_Q"], 2) for x in ap], "tau_Q_learned": [round(x["tau_Q"], 2) for x in al],
@@ -923,7 +934,8 @@ def main():
     ap.add_argument("--c1-gpu-chains", type=int, default=32)
     ap.add_argument("--c1-cpu-chains", type=int, default=8)
     ap.add_argument("--c5-plain", type=int, default=3000)
-    ap.add_argument("--c5-learned", type=int, default=600)
+    ap.add_argument("--c5-learned", type=int, default=3000,
+                    help="learned steps; equal to --c5-plain so both tau estimates see chains of one length")
     ap.add_argument("--c5-therm", type=int, default=5000)
     ap.add_argument("--c5-tune", type=int, default=10)
     ap.add_argument("--c5-nlocal", type=int, default=20)

@@ -45,6 +45,9 @@ struct ConvTmaArgs {
     int ldo, gelu;
     int* status;
     uint32_t tmem_cols, b_stage;   // B bytes per stage, rounded up to 1024
+    const float* head_w;           // optional fused 1^3 head: head_w[4][N], head_b[4]
+    const float* head_b;
+    float* head_out;               // [M][4]
 };
 
 // K-major operand in the 64-byte swizzle layout: 64-byte rows, 8-row groups 512 bytes apart
@@ -156,6 +159,9 @@ __global__ void __launch_bounds__(kCtThreads) k_conv_tma(const __grid_constant__
     if (ok && fin) {
         // warp w reads TMEM lanes 32 w .. 32 w + 31: one output row per thread
         const int row = (int)blockIdx.x * 128 + warp * 32 + lane;
+        float hacc[4] = {0.f, 0.f, 0.f, 0.f};
+        if (g.head_out)
+            for (int o = 0; o < 4; ++o) hacc[o] = g.head_b[o];
         for (int cb = 0; cb < N; cb += 16) {
             float v[16];
             tmem_ld16(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
@@ -174,8 +180,7 @@ __global__ void __launch_bounds__(kCtThreads) k_conv_tma(const __grid_constant__
                         cp[q] = x;
                     }
                 }
-                if (g.O) {
-                    uint4* op = reinterpret_cast<uint4*>(g.O + (size_t)row * g.ldo + cb);
+                if (g.O || g.head_out) {
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
                         uint32_t w[4];
@@ -185,12 +190,23 @@ __global__ void __launch_bounds__(kCtThreads) k_conv_tma(const __grid_constant__
                             const float b = g.gelu ? ct_gelu(v[8 * q + 2 * e + 1]) : v[8 * q + 2 * e + 1];
                             const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
                             w[e] = *reinterpret_cast<const uint32_t*>(&h2);
+                            if (g.head_out) {   // the head reads the BF16-rounded channels, in order
+                                const int c = cb + 8 * q + 2 * e;
+                                const float ha = __low2float(h2), hb = __high2float(h2);
+#pragma unroll
+                                for (int o = 0; o < 4; ++o) hacc[o] = fmaf(ha, g.head_w[o * N + c], hacc[o]);
+#pragma unroll
+                                for (int o = 0; o < 4; ++o) hacc[o] = fmaf(hb, g.head_w[o * N + c + 1], hacc[o]);
+                            }
                         }
-                        op[q] = make_uint4(w[0], w[1], w[2], w[3]);
+                        if (g.O)
+                            reinterpret_cast<uint4*>(g.O + (size_t)row * g.ldo + cb)[q] = make_uint4(w[0], w[1], w[2], w[3]);
                     }
                 }
             }
         }
+        if (g.head_out && row < g.M)
+            *reinterpret_cast<float4*>(g.head_out + (size_t)row * 4) = make_float4(hacc[0], hacc[1], hacc[2], hacc[3]);
     }
     tc_fence_before();
     __syncthreads();
@@ -433,6 +449,8 @@ int launch_conv_tma(const GemmArgs& g, cudaStream_t s) {
         return fail(ISING_ERR_ARG, "GEMM FP32 output needs a 16-byte aligned base and ldc % 4 == 0");
     if (g.O && (g.ldo % 8 || g.ldo < g.N || (reinterpret_cast<uintptr_t>(g.O) & 15)))
         return fail(ISING_ERR_ARG, "GEMM BF16 output needs a 16-byte aligned base and ldo % 8 == 0");
+    if (g.head_out && ((reinterpret_cast<uintptr_t>(g.head_out) & 15) || !g.head_w || !g.head_b || conv8_shape(g)))
+        return fail(ISING_ERR_ARG, "fused head: 16-byte aligned output, weights and bias, 32-channel layers only");
     if (conv8_shape(g)) return launch_conv8_tma(g, s);
     // the tensor-map rules, checked before any copy is issued: 16-byte aligned bases, strides
     // multiples of 16 bytes, a 64-byte inner box (<= the 64-byte swizzle span), boxes <= 256
@@ -466,6 +484,7 @@ int launch_conv_tma(const GemmArgs& g, cudaStream_t s) {
     a.M = g.M; a.N = g.N; a.pad = g.conv_pad; a.bias = g.bias; a.C = g.C; a.ldc = g.ldc; a.accumulate = g.accumulate;
     a.O = g.O; a.ldo = g.ldo; a.gelu = g.gelu; a.status = g.status;
     a.tmem_cols = g.N <= 32 ? 32 : g.N <= 64 ? 64 : g.N <= 128 ? 128 : 256;
+    a.head_w = g.head_w; a.head_b = g.head_b; a.head_out = g.head_out;
     a.b_stage = ((uint32_t)g.N * 64u + 1023u) & ~1023u;
     int smem = 1024 + kCtStages * (int)(kCtA + a.b_stage) + (2 * kCtStages + 1) * 8 + 16;
     static bool attr_set = false;

@@ -219,6 +219,7 @@ int launch_gemm_bf16(GemmArgs g, cudaStream_t s) {
     if (g.O && (g.ldo % 8 || g.ldo < g.N || (reinterpret_cast<uintptr_t>(g.O) & 15)))
         return fail(ISING_ERR_ARG, "GEMM BF16 output needs a 16-byte aligned base and ldo % 8 == 0");
     if (g.loader == 2 || (g.loader == 0 && conv_tma_applies(g))) return launch_conv_tma(g, s);
+    if (g.head_out) return fail(ISING_ERR_ARG, "the fused head needs the TMA convolution path");
     g.tmem_cols = g.N <= 32 ? 32 : g.N <= 64 ? 64 : g.N <= 128 ? 128 : 256;
     // resident blocks per SM x TMEM columns must fit the SM's 512 columns: a block whose
     // allocation cannot be met would stall until another block frees its columns

@@ -345,8 +345,14 @@ int net_forward_rows(ising_net* n, int nb, bool keep_pre) {
     ISG_TRY_N(launch_gemm_bf16(g, s));
     g = conv_gemm(n->H2, kCh, 4, 4, 1, n->Wf3, kK2, (int)R2, n->status);
     g.bias = n->P + kOffB3; g.C = keep_pre ? n->pre3 : nullptr; g.ldc = kCh; g.O = n->H3; g.ldo = kCh; g.gelu = 1;
+    // the TMA path computes the head in its epilogue; H3 is then written only for training
+    const bool fused = conv_tma_applies(g);
+    if (fused) {
+        g.head_w = n->P + kOffWh; g.head_b = n->P + kOffBh; g.head_out = n->out;
+        if (!keep_pre) g.O = nullptr;
+    }
     ISG_TRY_N(launch_gemm_bf16(g, s));
-    k_head_fwd<<<(int)((R2 + 127) / 128), 128, 0, s>>>(n->H3, R2, n->P, n->out);
+    if (!fused) k_head_fwd<<<(int)((R2 + 127) / 128), 128, 0, s>>>(n->H3, R2, n->P, n->out);
     if (cudaGetLastError() != cudaSuccess) return cuda_fail(cudaGetLastError(), "network forward");
     return ISING_OK;
 }

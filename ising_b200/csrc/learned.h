@@ -34,6 +34,12 @@ struct GemmArgs {
     // operand path: 0 = TMA copies where the shape allows (conv_tma.cu), else registers;
     // 1 = register-staged loader; 2 = TMA copies (an error where the shape does not allow)
     int loader;
+    // optional 1^3 head fused into the TMA path's epilogue (32 -> 4 channels onto 4^3 grids):
+    // head_out[row][o] = head_b[o] + sum_c bf16(gelu(acc + bias))[row][c] head_w[o][c], the
+    // channels taken in order; the register path refuses it
+    const float* head_w;
+    const float* head_b;
+    float* head_out;
     uint32_t tmem_cols;     // set by the launcher
 };
 int launch_gemm_bf16(GemmArgs g, cudaStream_t s);
