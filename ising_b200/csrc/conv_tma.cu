@@ -214,8 +214,9 @@ __global__ void __launch_bounds__(kCtThreads) k_conv_tma(const __grid_constant__
 }
 
 // First layer: 3^3 convolution over an 8-channel grid (8^3 cells) onto its 6^3 valid output
-// cells.  A block computes one window: its 216 rows sit in a 256-row tile covered by two
-// M = 128 MMAs with accumulators in TMEM columns [0, N) and [N, 2N).  Kernel offset t is one
+// cells.  A block computes two windows: each window's 216 rows sit in a 256-row tile covered
+// by two M = 128 MMAs, the four accumulators N TMEM columns apart, and the two windows share
+// each step's weight slices.  Kernel offset t is one
 // 216 x 8 box (16-byte rows, no swizzle) copied densely into a 256-row buffer, which is the
 // canonical no-swizzle K-major layout with 8-row groups 128 bytes apart; the two offsets of
 // a K = 16 step sit in consecutive buffers (leading offset 4 KB), as do their N x 8 weight
@@ -223,6 +224,7 @@ __global__ void __launch_bounds__(kCtThreads) k_conv_tma(const __grid_constant__
 // nwin) and TMA fills it with zeros.  Rows 216..255 of a buffer are never written and feed
 // only the discarded accumulator rows.
 constexpr int kC8Stages = 4;
+constexpr int kC8Win = 2;                     // windows per block
 constexpr int kC8Pairs = 14;                  // 28 offsets (27 + the zero pad), two per K step
 constexpr uint32_t kC8TapA = 256u * 16u;      // 256 rows x 8 BF16
 
@@ -244,13 +246,13 @@ __global__ void __launch_bounds__(kCtThreads) k_conv8_tma(const __grid_constant_
     unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const int N = g.N;
     const uint32_t tapB = (uint32_t)N * 16u;
-    const uint32_t stage_bytes = 2u * kC8TapA + 2u * tapB;
+    const uint32_t stage_bytes = kC8Win * 2u * kC8TapA + 2u * tapB;   // [window][offset] A, then B
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + kC8Stages * stage_bytes);
     uint64_t* empty = full + kC8Stages;
     uint64_t* done = empty + kC8Stages;
     uint32_t* slot = reinterpret_cast<uint32_t*>(done + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int win = (int)blockIdx.x;
+    const int win0 = kC8Win * (int)blockIdx.x;
 
     if (warp == 0) tmem_alloc(slot, g.tmem_cols);
     if (tid == 0) {
@@ -270,7 +272,7 @@ __global__ void __launch_bounds__(kCtThreads) k_conv8_tma(const __grid_constant_
     if (tid == 0) {
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tA)) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tB)) : "memory");
-        const uint32_t tx = 2u * (216u * 16u + tapB);
+        const uint32_t tx = kC8Win * 2u * 216u * 16u + 2u * tapB;
         const uint32_t idesc = umma_idesc_bf16(128, N);
         auto issue = [&](int p) {
             const int s = p % kC8Stages;
@@ -279,11 +281,15 @@ __global__ void __launch_bounds__(kCtThreads) k_conv8_tma(const __grid_constant_
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int t = 2 * p + h;
-                if (t < kCtTaps)
-                    tma_load_5d(st + h * kC8TapA, &tA, 0, t % 3, (t / 3) % 3, t / 9, win, &full[s]);
-                else   // the pad offset: a box outside the tensor reads as zeros
-                    tma_load_5d(st + h * kC8TapA, &tA, 0, 0, 0, 0, g.nwin, &full[s]);
-                tma_load_2d(st + 2u * kC8TapA + h * tapB, &tB, 8 * t, 0, &full[s]);
+                // a window index at or past nwin (a block's missing second window, or the pad
+                // offset) lies outside the tensor and reads as zeros
+#pragma unroll
+                for (int w = 0; w < kC8Win; ++w) {
+                    unsigned char* dst = st + (uint32_t)(2 * w + h) * kC8TapA;
+                    if (t < kCtTaps) tma_load_5d(dst, &tA, 0, t % 3, (t / 3) % 3, t / 9, win0 + w, &full[s]);
+                    else tma_load_5d(dst, &tA, 0, 0, 0, 0, g.nwin, &full[s]);
+                }
+                tma_load_2d(st + kC8Win * 2u * kC8TapA + h * tapB, &tB, 8 * t, 0, &full[s]);
             }
         };
         int issued = 0;
@@ -294,12 +300,15 @@ __global__ void __launch_bounds__(kCtThreads) k_conv8_tma(const __grid_constant_
             ok = mbar_wait(&full[s], (uint32_t)((p / kC8Stages) & 1), kCtWaitPolls);
             if (!ok) break;
             tc_fence_after();
-            const uint32_t a0 = smem_u32(smem + s * stage_bytes), b0 = a0 + 2u * kC8TapA;
+            const uint32_t a0 = smem_u32(smem + s * stage_bytes), b0 = a0 + kC8Win * 2u * kC8TapA;
             const uint64_t bd = umma_smem_desc(b0, tapB, 128u);
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
-                umma_bf16(taddr + (uint32_t)(h * N), umma_smem_desc(a0 + (uint32_t)h * 2048u, kC8TapA, 128u), bd, idesc,
-                          p > 0 ? 1u : 0u);
+            for (int w = 0; w < kC8Win; ++w)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    umma_bf16(taddr + (uint32_t)((2 * w + h) * N),
+                              umma_smem_desc(a0 + (uint32_t)(2 * w) * kC8TapA + (uint32_t)h * 2048u, kC8TapA, 128u), bd,
+                              idesc, p > 0 ? 1u : 0u);
             umma_commit(&empty[s]);
             if (p >= 1 && issued < kC8Pairs) {
                 const int ps = (p - 1) % kC8Stages;
@@ -318,12 +327,12 @@ __global__ void __launch_bounds__(kCtThreads) k_conv8_tma(const __grid_constant_
     tc_fence_after();
     if (!fin && tid == 0) atomicOr(g.status, kStatTimeout);
     if (ok && fin) {
-        for (int h = 0; h < 2; ++h) {
-            const int u = h * 128 + warp * 32 + lane;     // output cell of this window
-            const int row = win * 216 + u;
+        for (int wh = 0; wh < 2 * kC8Win; ++wh) {
+            const int u = (wh & 1) * 128 + warp * 32 + lane;     // output cell of window win0 + wh / 2
+            const int row = (win0 + (wh >> 1)) * 216 + u;
             for (int cb = 0; cb < N; cb += 16) {
                 float v[16];
-                tmem_ld16(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * N + cb), v);
+                tmem_ld16(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)(wh * N + cb), v);
                 if (u < 216 && row < g.M) {
 #pragma unroll
                     for (int i = 0; i < 16; ++i) v[i] += g.bias ? g.bias[cb + i] : 0.f;
@@ -379,7 +388,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 bool conv8_shape(const GemmArgs& g) {
     return g.conv_in && g.conv_C == 8 && g.conv_Gi == 8 && g.conv_Go == 6 && g.conv_pad == 0 && g.K == 224 &&
-           g.M % 216 == 0 && g.N % 16 == 0 && g.N <= 128;
+           g.M % 216 == 0 && g.N % 16 == 0 && g.N <= 64;
 }
 
 bool conv32_shape(const GemmArgs& g) {
@@ -419,8 +428,9 @@ int launch_conv8_tma(const GemmArgs& g, cudaStream_t s) {
     Conv8Args a{};
     a.M = g.M; a.N = g.N; a.nwin = nwin; a.bias = g.bias; a.C = g.C; a.ldc = g.ldc; a.accumulate = g.accumulate;
     a.O = g.O; a.ldo = g.ldo; a.gelu = g.gelu; a.status = g.status;
-    a.tmem_cols = 2 * g.N <= 32 ? 32 : 2 * g.N <= 64 ? 64 : 2 * g.N <= 128 ? 128 : 256;
-    int smem = 1024 + kC8Stages * (int)(2u * kC8TapA + 2u * (uint32_t)g.N * 16u) + (2 * kC8Stages + 1) * 8 + 16;
+    const int cols = kC8Win * 2 * g.N;   // two 128-row halves per window
+    a.tmem_cols = cols <= 32 ? 32 : cols <= 64 ? 64 : cols <= 128 ? 128 : 256;
+    int smem = 1024 + kC8Stages * (int)(kC8Win * 2u * kC8TapA + 2u * (uint32_t)g.N * 16u) + (2 * kC8Stages + 1) * 8 + 16;
     static bool attr_set = false;
     if (!attr_set) {
         ISG_CUDA(cudaFuncSetAttribute(k_conv8_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -432,7 +442,7 @@ int launch_conv8_tma(const GemmArgs& g, cudaStream_t s) {
         if (occ * (int)a.tmem_cols <= 512 || smem >= 200 * 1024) break;
         smem += 8 * 1024;
     }
-    k_conv8_tma<<<nwin, kCtThreads, smem, s>>>(tA, tB, a);
+    k_conv8_tma<<<(nwin + kC8Win - 1) / kC8Win, kCtThreads, smem, s>>>(tA, tB, a);
     ISG_CUDA(cudaGetLastError());
     return ISING_OK;
 }
