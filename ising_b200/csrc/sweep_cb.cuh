@@ -210,7 +210,6 @@ __device__ __forceinline__ void pair_update(const CbGeom& P, const uint32_t* rk,
                                             uint32_t j, int colour, uint32_t sweep, uint32_t rep, float beta2,
                                             v2& de, v2& dmx, v2& dmy, v2& dmz) {
     const CbGeom& a = P;
-    const HamDev& H = P.ham;
     const uint32_t p = (x + y + (uint32_t)colour) & 1u;
     const uint32_t own = (uint32_t)colour * P.half;
     const uint32_t oth = (uint32_t)(colour ^ 1) * P.half;
