@@ -23,6 +23,8 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <atomic>
+
 #include "internal.h"
 #include "learned.h"
 #include "umma.cuh"
@@ -372,17 +374,16 @@ __global__ void __launch_bounds__(kCtThreads) k_conv8_tma(const __grid_constant_
     if (warp == 0) tmem_dealloc(taddr, g.tmem_cols);
 }
 
+// the driver's tensor-map encoder, looked up once (thread-safe static initialisation)
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        return nullptr;
+    }();
     return fn;
 }
 
@@ -431,10 +432,16 @@ int launch_conv8_tma(const GemmArgs& g, cudaStream_t s) {
     const int cols = kC8Win * 2 * g.N;   // two 128-row halves per window
     a.tmem_cols = cols <= 32 ? 32 : cols <= 64 ? 64 : cols <= 128 ? 128 : 256;
     int smem = 1024 + kC8Stages * (int)(kC8Win * 2u * kC8TapA + 2u * (uint32_t)g.N * 16u) + (2 * kC8Stages + 1) * 8 + 16;
-    static bool attr_set = false;
-    if (!attr_set) {
-        ISG_CUDA(cudaFuncSetAttribute(k_conv8_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr_set = true;
+    // the shared-memory limit is a per-device attribute of the kernel: raise it once per device
+    static std::atomic<unsigned long long> attr_set{0};
+    {
+        int dev = 0;
+        ISG_CUDA(cudaGetDevice(&dev));
+        const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+        if (!bit || !(attr_set.load() & bit)) {
+            ISG_CUDA(cudaFuncSetAttribute(k_conv8_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            attr_set.fetch_or(bit);
+        }
     }
     for (;;) {
         int occ = 0;
@@ -497,10 +504,16 @@ int launch_conv_tma(const GemmArgs& g, cudaStream_t s) {
     a.head_w = g.head_w; a.head_b = g.head_b; a.head_out = g.head_out;
     a.b_stage = ((uint32_t)g.N * 64u + 1023u) & ~1023u;
     int smem = 1024 + kCtStages * (int)(kCtA + a.b_stage) + (2 * kCtStages + 1) * 8 + 16;
-    static bool attr_set = false;
-    if (!attr_set) {
-        ISG_CUDA(cudaFuncSetAttribute(k_conv_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr_set = true;
+    // the shared-memory limit is a per-device attribute of the kernel: raise it once per device
+    static std::atomic<unsigned long long> attr_set{0};
+    {
+        int dev = 0;
+        ISG_CUDA(cudaGetDevice(&dev));
+        const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+        if (!bit || !(attr_set.load() & bit)) {
+            ISG_CUDA(cudaFuncSetAttribute(k_conv_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            attr_set.fetch_or(bit);
+        }
     }
     if (smem > 200 * 1024) return fail(ISING_ERR_ARG, "TMA convolution: N too large for the stage ring");
     // resident blocks x TMEM columns must fit the SM's 512 columns

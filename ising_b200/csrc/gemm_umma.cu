@@ -18,6 +18,8 @@
 // gives up sets kStatTimeout and skips the epilogue.
 #include <cuda_bf16.h>
 
+#include <atomic>
+
 #include "internal.h"
 #include "learned.h"
 #include "umma.cuh"
@@ -224,10 +226,16 @@ int launch_gemm_bf16(GemmArgs g, cudaStream_t s) {
     // resident blocks per SM x TMEM columns must fit the SM's 512 columns: a block whose
     // allocation cannot be met would stall until another block frees its columns
     int smem = gemm_smem_bytes(g.N);
-    static bool attr_set = false;
-    if (!attr_set) {
-        ISG_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr_set = true;
+    // the shared-memory limit is a per-device attribute of the kernel: raise it once per device
+    static std::atomic<unsigned long long> attr_set{0};
+    {
+        int dev = 0;
+        ISG_CUDA(cudaGetDevice(&dev));
+        const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+        if (!bit || !(attr_set.load() & bit)) {
+            ISG_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            attr_set.fetch_or(bit);
+        }
     }
     for (;;) {
         int occ = 0;
