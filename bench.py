@@ -764,7 +764,7 @@ def run_c5(args, w):
     p = ib.params(J=w["J"], Dz=w["D"], B=w["B"], K=w["K"], dmi="bulk", include_Jp=False)
     betas = 1.0 / ib.temperature_ladder(w["tmin"], w["tmax"], R)
     pt = ib.ParallelTempering(mesh, betas, p, seed=0x15196, ensemble=0, move=_lib.MOVE_BALL, r=w["r"],
-                              record=True, record_capacity=n_plain + n_learned + 8)
+                              record=True, record_capacity=2 * n_plain + n_learned + 8)
 
     def timed(fn):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -843,8 +843,12 @@ def run_c5(args, w):
             pt.patch_step(net, i % 8, tuple(int(v) for v in rng.integers(0, 8, 3)), slots=args.c5_slots)
 
     t_learned = timed(learned_run)
+    c2 = pt.series().shape[1]
+    # a second plain segment after the learned one: the first starts closer to thermalisation,
+    # so drift could inflate its tau; the plain arm is the segment with the larger Q-ESS
+    t_plain2 = timed(lambda: pt.run(k, n_plain))
     ser = pt.series()
-    sp, sl = ser[:, c0:c1], ser[:, c1:]
+    sp, sl, sp2 = ser[:, c0:c1], ser[:, c1:c2], ser[:, c2:]
 
     def arm(x, secs):
         out = []
@@ -855,14 +859,18 @@ def run_c5(args, w):
                         "ess_E_per_s": len(e) / (2 * te) / secs, "q_var": float(np.var(q))})
         return out
 
-    ap, al = arm(sp, t_plain), arm(sl, t_learned)
-    # Q-ESS over the slots where Q fluctuates in both runs (a frozen Q has no defined tau)
-    live = [t for t in range(R) if ap[t]["q_var"] > 1e-12 and al[t]["q_var"] > 1e-12]
+    ap1, al, ap2 = arm(sp, t_plain), arm(sl, t_learned), arm(sp2, t_plain2)
+    # Q-ESS over the slots where Q fluctuates in every segment (a frozen Q has no defined tau)
+    live = [t for t in range(R) if ap1[t]["q_var"] > 1e-12 and al[t]["q_var"] > 1e-12 and ap2[t]["q_var"] > 1e-12]
+    q1 = float(np.mean([ap1[t]["ess_Q_per_s"] for t in live])) if live else 0.0
+    q2 = float(np.mean([ap2[t]["ess_Q_per_s"] for t in live])) if live else 0.0
+    ap = ap2 if q2 > q1 else ap1
+    plain_segment = "after" if q2 > q1 else "before"
     within = {}
     for name, col in (("E", 0), ("absM", 1), ("Q", 3)):
         ok = 0
         for t in range(R):
-            a, b = sp[t, :, col], sl[t, :, col]
+            a, b = (sp2 if plain_segment == "after" else sp)[t, :, col], sl[t, :, col]
             err = np.hypot(A.binning_error(a), A.binning_error(b))
             ok += int(abs(a.mean() - b.mean()) <= 2 * err + 1e-12)
         within[name] = ok
@@ -887,6 +895,9 @@ def run_c5(args, w):
                   "slots_used": live, "plain": qp, "learned": ql,
                   "learned_over_plain": ql / qp if qp > 0 else None,
                   "learned_over_plain_per_slot": per_slot,
+                  "plain_segments": {"before_learned": q1, "after_learned": q2, "used": plain_segment,
+                                     "tau_Q_before": [round(ap1[t]["tau_Q"], 2) for t in live],
+                                     "tau_Q_after": [round(ap2[t]["tau_Q"], 2) for t in live]},
                   "plain_sweeps": n_plain, "learned_steps": n_learned,
                   "slots_with_N_ge_50_tauQ": reliable,
                   "s_per_step": {"plain": t_plain / n_plain, "learned": t_learned / n_learned},
