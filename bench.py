@@ -947,7 +947,7 @@ def main():
     ap.add_argument("--c5-plain", type=int, default=3000)
     ap.add_argument("--c5-learned", type=int, default=3000,
                     help="learned steps; equal to --c5-plain so both tau estimates see chains of one length")
-    ap.add_argument("--c5-therm", type=int, default=5000)
+    ap.add_argument("--c5-therm", type=int, default=20000)
     ap.add_argument("--c5-tune", type=int, default=10)
     ap.add_argument("--c5-nlocal", type=int, default=20)
     ap.add_argument("--c5-train", type=int, default=100000)
