@@ -1,8 +1,10 @@
-// conv_tma.cu -- 3^3 convolution over a 32-channel channel-last grid with a 4^3 output grid per
-// window, as an implicit GEMM on the sm_100a tensor cores with TMA-fed operands.
+// conv_tma.cu -- the proposal network's 3^3 convolutions as implicit GEMMs on the sm_100a
+// tensor cores with TMA-fed operands: k_conv_tma for 32-channel grids onto 4^3 output grids
+// (optionally with the 1^3 head fused into its epilogue), k_conv8_tma for the first layer
+// (8 padded channels, 8^3 -> 6^3; described above the kernel).
 //
-// Rows are (window, x, y, z) of the output grid, 64 per window; a block computes the 128 rows
-// of two windows for all N output channels.  K runs over the 27 kernel offsets (dx, dy, dz) x
+// k_conv_tma.  Rows are (window, x, y, z) of the output grid, 64 per window; a block
+// computes the 128 rows of two windows for all N output channels.  K runs over the 27 kernel offsets (dx, dy, dz) x
 // 32 channels.  For offset t the 128 x 32 A tile is one box of the 5-D tensor
 // (channel, z, y, x, window) of the input: channels 0..31, z, y, x from offset - pad over 4
 // cells each, windows w0, w0 + 1.  One tiled TMA copy moves it into shared memory with the
@@ -13,7 +15,8 @@
 // stage's transaction count, issues the two K = 16 MMAs of the offset (the second starting
 // 32 bytes into the swizzled rows) and commits them to the stage's "empty" barrier, which
 // releases the stage for the copies of offset t + 6.  The epilogue is the one of the
-// register-staged GEMM (gemm_umma.cu): bias, optional GELU, FP32 and/or BF16 rows.
+// register-staged GEMM (gemm_umma.cu): bias, optional GELU, FP32 and/or BF16 rows, and, when
+// asked, the head's four outputs per row from the BF16-rounded channels.
 //
 // The accumulation order (offset by offset, K = 16 steps in K order) is the register-staged
 // kernel's, so both produce identical sums.  Every mbarrier wait is bounded; after a wait
