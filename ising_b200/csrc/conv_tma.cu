@@ -4,8 +4,8 @@
 // (8 padded channels, 8^3 -> 6^3; described above the kernel).
 //
 // k_conv_tma.  Rows are (window, x, y, z) of the output grid, 64 per window; a block
-// computes the 128 rows of two windows for all N output channels.  K runs over the 27 kernel offsets (dx, dy, dz) x
-// 32 channels.  For offset t the 128 x 32 A tile is one box of the 5-D tensor
+// computes the 128 rows of two windows for all N output channels.  K runs over the 27 kernel
+// offsets (dx, dy, dz) x 32 channels.  For offset t the 128 x 32 A tile is one box of the 5-D tensor
 // (channel, z, y, x, window) of the input: channels 0..31, z, y, x from offset - pad over 4
 // cells each, windows w0, w0 + 1.  One tiled TMA copy moves it into shared memory with the
 // 64-byte swizzle (each 64-byte row holds the 32 channels of one output row), and coordinates
