@@ -1189,11 +1189,11 @@ extern "C" int ising_pt_patch_step(ising_pt* pt, ising_net* net, int colour, int
     for (int64_t w0 = 0; w0 < total; w0 += batch) {
         const int nb = (int)std::min<int64_t>(batch, total - w0);
         const float* out = nullptr;
-        ISG_TRY(launch_patch_gather(P, w0, nb, nullptr, pt->pw_win, s));
-        ISG_TRY(net_forward_on(net, pt->pw_win, nb, s, &out));
+        ISG_TRY(launch_patch_gather(P, w0, nb, nullptr, pt->pw_win, s, net_rows(net)));
+        ISG_TRY(net_forward_prepared(net, nb, s, &out));
         ISG_TRY(launch_patch_propose(P, w0, nb, pt->pw_win, out, pt->pw_prop, pt->pw_lqf, pt->pw_rej, s));
-        ISG_TRY(launch_patch_gather(P, w0, nb, pt->pw_prop, pt->pw_winp, s));
-        ISG_TRY(net_forward_on(net, pt->pw_winp, nb, s, &out));
+        ISG_TRY(launch_patch_gather(P, w0, nb, pt->pw_prop, pt->pw_winp, s, net_rows(net)));
+        ISG_TRY(net_forward_prepared(net, nb, s, &out));
         ISG_TRY(launch_patch_accept(P, w0, nb, pt->pw_win, pt->pw_winp, out, pt->pw_prop, pt->pw_lqf, pt->pw_rej,
                                     pt->pw_dE, pt->pw_dM, pt->pw_acc, s));
     }

@@ -537,11 +537,11 @@ extern "C" int ising_net_train_step(ising_net* n, const float* d_windows, const 
 
 namespace isg {
 
-int net_forward_on(ising_net* n, const float* d_windows, int nb, cudaStream_t s, const float** out) {
+__nv_bfloat16* net_rows(ising_net* n) { return n->X0; }
+int net_forward_prepared(ising_net* n, int nb, cudaStream_t s, const float** out) {
     if (nb < 1 || nb > n->max_batch) return fail(ISING_ERR_ARG, "window batch exceeds the network's max_batch");
     cudaStream_t keep = n->stream;
     n->stream = s;
-    k_windows_to_rows<<<grid_for((int64_t)nb * 512), 256, 0, s>>>(d_windows, nb, n->X0);
     const int st = net_forward_rows(n, nb, false);
     n->stream = keep;
     *out = n->out;

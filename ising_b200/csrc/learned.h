@@ -48,8 +48,10 @@ int launch_gemm_bf16(GemmArgs g, cudaStream_t s);
 bool conv_tma_applies(const GemmArgs& g);
 int launch_conv_tma(const GemmArgs& g, cudaStream_t s);
 
-// forward of nb windows ([nb][3][8][8][8] FP32, device) on stream s; *out = [nb*64][4]
-int net_forward_on(ising_net* n, const float* d_windows, int nb, cudaStream_t s, const float** out);
+// the network's input-row buffer ([max_batch*512][8] BF16) and a forward on stream s of the
+// nb windows already written there; *out = [nb*64][4]
+__nv_bfloat16* net_rows(ising_net* n);
+int net_forward_prepared(ising_net* n, int nb, cudaStream_t s, const float** out);
 int net_max_batch(const ising_net* n);
 int net_device(const ising_net* n);
 // reads and clears the network status word after the work queued on s (synchronises s)
@@ -74,7 +76,10 @@ struct PatchStep {
     uint32_t round;
     int* status;
 };
-int launch_patch_gather(const PatchStep& P, int64_t w0, int nb, const float* prop, float* win, cudaStream_t s);
+// windows w0 .. w0+nb-1 as FP32 [window][3][512] in win and, when x0 is given, as the
+// network's BF16 input rows (net_rows) for net_forward_prepared
+int launch_patch_gather(const PatchStep& P, int64_t w0, int nb, const float* prop, float* win, cudaStream_t s,
+                        __nv_bfloat16* x0 = nullptr);
 int launch_patch_propose(const PatchStep& P, int64_t w0, int nb, const float* win, const float* out, float* prop,
                          double* lqf, int* rej, cudaStream_t s);
 int launch_patch_accept(const PatchStep& P, int64_t w0, int nb, const float* win, const float* winp, const float* outp,

@@ -58,7 +58,8 @@ __device__ __forceinline__ void patch_origin(const PatchStep& P, int64_t w, int&
 }
 
 // windows [nb][3][8][8][8] of windows w0 .. w0+nb-1; patch voxels from prop when given
-__global__ void k_patch_gather(PatchStep P, int64_t w0, int nb, const float* __restrict__ prop, float* __restrict__ win) {
+__global__ void k_patch_gather(PatchStep P, int64_t w0, int nb, const float* __restrict__ prop, float* __restrict__ win,
+                               __nv_bfloat16* __restrict__ x0) {
     const int64_t n = (int64_t)nb * 512;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int b = (int)(i / 512), v = (int)(i % 512);
@@ -76,6 +77,14 @@ __global__ void k_patch_gather(PatchStep P, int64_t w0, int nb, const float* __r
             for (int q = 0; q < 3; ++q) s[q] = base[q * P.natoms + si];
         }
         for (int q = 0; q < 3; ++q) win[((int64_t)b * 3 + q) * 512 + v] = s[q];
+        if (x0) {   // the network's input row: 3 channels padded to 8, as k_windows_to_rows writes it
+            __nv_bfloat162 h[4];
+            h[0] = __floats2bfloat162_rn(s[0], s[1]);
+            h[1] = __floats2bfloat162_rn(s[2], 0.f);
+            h[2] = __floats2bfloat162_rn(0.f, 0.f);
+            h[3] = h[2];
+            *reinterpret_cast<uint4*>(x0 + i * 8) = *reinterpret_cast<const uint4*>(h);
+        }
     }
 }
 
@@ -286,9 +295,10 @@ __global__ void __launch_bounds__(64) k_patch_equilibrate(PatchStep P, int64_t w
     for (int q = 0; q < 3; ++q) tgt[((int64_t)b * 64 + i) * 3 + q] = S[q][v];
 }
 
-int launch_patch_gather(const PatchStep& P, int64_t w0, int nb, const float* prop, float* win, cudaStream_t s) {
+int launch_patch_gather(const PatchStep& P, int64_t w0, int nb, const float* prop, float* win, cudaStream_t s,
+                        __nv_bfloat16* x0) {
     const int64_t n = (int64_t)nb * 512;
-    k_patch_gather<<<(int)std::min<int64_t>((n + 255) / 256, 148 * 64), 256, 0, s>>>(P, w0, nb, prop, win);
+    k_patch_gather<<<(int)std::min<int64_t>((n + 255) / 256, 148 * 64), 256, 0, s>>>(P, w0, nb, prop, win, x0);
     ISG_CUDA(cudaGetLastError());
     return ISING_OK;
 }
