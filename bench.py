@@ -332,7 +332,10 @@ def run_gpu(args, w):
     if args.engine == "ensembles":
         eng = ib.Ensembles(members, seed=0x15196, move=move, r=w["r"])
         eng.set_stream(stream.cuda_stream)
-        trials = eng.autotune(k, 2) if not args.no_autotune else []
+        if args.schedule:   # threads,chunk_pairs,loader: a fixed schedule instead of the autotuner
+            bt, cp, ld = (int(v) for v in args.schedule.split(","))
+            eng.set_schedule(block_threads=bt, chunk_pairs=cp, loader=ld)
+        trials = eng.autotune(k, 2) if not (args.no_autotune or args.schedule) else []
         eng.run(k, max(args.warmup, 1))
         run = lambda n: eng.run(k, n)
         energies = lambda: [eng.energies(i) for i in range(len(members))]
@@ -936,6 +939,7 @@ def main():
     ap.add_argument("--replicas", type=int, default=0, help="override replica count (profiling)")
     ap.add_argument("--engine", default="ensembles", choices=["ensembles", "pt"])
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--schedule", default="", help="engine schedule 'threads,chunk_pairs,loader' (no autotuner)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--learned", action="store_true", help="c5: learned patch proposal vs plain Metropolis")
     ap.add_argument("--patch-probe", action="store_true", help="time learned patch steps (C5 Hamiltonian)")

@@ -312,13 +312,19 @@ typedef struct {
     int wait_timeout_ms;      /* bound of every in-kernel wait (0 = 2000) */
 } ising_ensembles_options;
 
-/* One schedule: block size, target site pairs per task, queue order and group size. */
+#define ISING_ENS_LOADER_REGISTERS 0   /* each thread loads its sites' neighbours from global memory */
+#define ISING_ENS_LOADER_STAGED 1      /* rows staged in shared memory by TMA copies (every ensemble
+                                          with nz = 128 and nx % 4 == 0; whole groups of 4 x-planes
+                                          per task; 256-thread blocks) */
+
+/* One schedule: block size, target site pairs per task, queue order, group size, loader. */
 typedef struct {
     int block_threads;        /* 64..256, whole warps */
     int chunk_pairs;          /* site pairs of one colour per task (whole x-planes) */
     int order;                /* ISING_ENS_ORDER_* */
     int64_t group_bytes;      /* ISING_ENS_ORDER_GROUPS: spin bytes per replica group */
     double ms_per_round;      /* autotuner output: measured time per round */
+    int loader;               /* ISING_ENS_LOADER_* */
 } ising_ensembles_schedule_t;
 
 /* No reference counterpart (the reference has no batched form). */

@@ -64,10 +64,11 @@ class EnsemblesOptions(C.Structure):
 
 class EnsSchedule(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("chunk_pairs", C.c_int), ("order", C.c_int),
-                ("group_bytes", C.c_int64), ("ms_per_round", C.c_double)]
+                ("group_bytes", C.c_int64), ("ms_per_round", C.c_double), ("loader", C.c_int)]
 
 
 ENS_ORDER_PHASE, ENS_ORDER_GROUPS = 0, 1
+ENS_LOADER_REGISTERS, ENS_LOADER_STAGED = 0, 1
 
 _P = C.POINTER
 _d, _i, _i64, _u32, _u64, _vp = C.c_double, C.c_int, C.c_int64, C.c_uint32, C.c_uint64, C.c_void_p

@@ -612,8 +612,10 @@ class Ensembles:
         _lib.call("ising_ensembles_run", self._h, sweeps_per_swap, rounds)
 
     def set_schedule(self, block_threads: int = 256, chunk_pairs: int = 4096, order: int = ENS_ORDER_PHASE,
-                     group_bytes: int = 48_000_000):
-        c = EnsSchedule(block_threads, chunk_pairs, order, group_bytes, 0.0)
+                     group_bytes: int = 48_000_000, loader: int = 0):
+        """loader 0: neighbours loaded per thread; 1: rows staged in shared memory by TMA
+        (nz = 128 and nx % 4 == 0 in every ensemble, 256-thread blocks)."""
+        c = EnsSchedule(block_threads, chunk_pairs, order, group_bytes, 0.0, loader)
         _lib.call("ising_ensembles_set_schedule", self._h, C.byref(c))
 
     def schedule(self) -> dict:
@@ -621,6 +623,7 @@ class Ensembles:
         _lib.call("ising_ensembles_get_schedule", self._h, C.byref(c), C.byref(g), C.byref(t))
         return {"block_threads": c.block_threads, "chunk_pairs": c.chunk_pairs,
                 "order": "groups" if c.order == ENS_ORDER_GROUPS else "phase", "group_bytes": c.group_bytes,
+                "loader": "staged" if c.loader == 1 else "registers",
                 "ms_per_round": c.ms_per_round, "grid_blocks": g.value, "tasks_per_pass": t.value}
 
     def autotune(self, sweeps_per_swap: int, rounds_per_trial: int = 1):
@@ -630,6 +633,7 @@ class Ensembles:
         _lib.call("ising_ensembles_autotune", self._h, sweeps_per_swap, rounds_per_trial, trials, 64, C.byref(n))
         return [{"block_threads": t.block_threads, "chunk_pairs": t.chunk_pairs,
                  "order": "groups" if t.order == ENS_ORDER_GROUPS else "phase", "group_bytes": t.group_bytes,
+                 "loader": "staged" if t.loader == 1 else "registers",
                  "ms_per_round": t.ms_per_round} for t in trials[: n.value]]
 
     def permutation(self, e: int) -> np.ndarray:

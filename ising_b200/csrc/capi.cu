@@ -1341,6 +1341,17 @@ void ens_drop_graph(ising_ensembles* s) {
     s->graph_k = s->graph_rounds = -1;
 }
 
+// Every ensemble suits the staged loader: packed rows of 64 entries (nz = 128), whole groups
+// of kStG x-planes, and the driver's tensor-map encoder is present.
+bool ens_staged_fits(const ising_ensembles* s) {
+    if (!tensor_map_encoder()) return false;
+    for (const auto& h : s->ens) {
+        const Lattice& L = h.mesh->lat;
+        if (L.nz != 128 || L.nx % kStG != 0) return false;
+    }
+    return true;
+}
+
 // Chunking, grid and buffers for schedule `c`.
 int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) {
     if (c.block_threads < 64 || c.block_threads > kEnsMaxThreads || c.block_threads % 32)
@@ -1349,6 +1360,13 @@ int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) 
     if (c.order != ISING_ENS_ORDER_PHASE && c.order != ISING_ENS_ORDER_GROUPS)
         return fail(ISING_ERR_ARG, "order must be ISING_ENS_ORDER_PHASE or ISING_ENS_ORDER_GROUPS");
     if (c.order == ISING_ENS_ORDER_GROUPS && c.group_bytes < 1) return fail(ISING_ERR_ARG, "group_bytes must be >= 1");
+    if (c.loader != ISING_ENS_LOADER_REGISTERS && c.loader != ISING_ENS_LOADER_STAGED)
+        return fail(ISING_ERR_ARG, "loader must be ISING_ENS_LOADER_REGISTERS or ISING_ENS_LOADER_STAGED");
+    const bool staged = c.loader == ISING_ENS_LOADER_STAGED;
+    if (staged) {
+        if (c.block_threads != kStSub * kStG * 32) return fail(ISING_ERR_ARG, "the staged loader runs 256-thread blocks");
+        if (!ens_staged_fits(s)) return fail(ISING_ERR_ARG, "the staged loader needs nz = 128 and nx % 4 == 0 in every ensemble");
+    }
     size_t part = 0, done = 0;
     for (auto& h : s->ens) {
         const Lattice& L = h.mesh->lat;
@@ -1357,6 +1375,7 @@ int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) 
         const double plane_pairs = (double)L.ny * lanes;
         int P = (int)std::lround((double)c.chunk_pairs / plane_pairs);
         P = std::max(1, std::min(P, L.nx));
+        if (staged) P = std::max(kStG, P / kStG * kStG);   // whole plane groups (nx % kStG == 0)
         h.P = (uint32_t)P;
         h.nch = (uint32_t)((L.nx + P - 1) / P);
         h.part_off = part;
@@ -1365,7 +1384,7 @@ int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) 
         done += (size_t)h.n * h.nch;
     }
     int per_sm = 0;
-    ISG_TRY(ensembles_blocks_per_sm(s->move, s->dmi, s->has_k, c.block_threads, &per_sm));
+    ISG_TRY(ensembles_blocks_per_sm(s->move, s->dmi, s->has_k, staged, c.block_threads, &per_sm));
     if (per_sm < 1) return fail(ISING_ERR_CUDA, "persistent engine kernel cannot be resident");
     int sms = 0;
     ISG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
@@ -1467,6 +1486,12 @@ void ens_params(const ising_ensembles* s, int k, int rounds, int stall, EnsParam
         d.nseg = std::max(1u, std::min((uint32_t)L.ny, (d.rb + h.P - 1) / h.P));
         d.seg_len = ((uint32_t)L.ny + d.nseg - 1) / d.nseg;
         d.divSeg = make_div(d.nseg);
+        if (s->sched.loader == ISING_ENS_LOADER_STAGED) {
+            // units of a task (plane groups x y-segments) come in pairs, one per sub-block
+            const uint32_t groups = h.P / (uint32_t)kStG;
+            d.st_nseg = std::min<uint32_t>((uint32_t)L.ny, groups % 2 ? 2u : 1u);
+            d.st_seg_len = ((uint32_t)L.ny + d.st_nseg - 1) / d.st_nseg;
+        }
         d.n_rep = h.n;
         d.beta_rep = h.d_beta_rep;
         d.sweep_ctr = h.mesh->d_sweep;
@@ -1497,8 +1522,16 @@ void ens_params(const ising_ensembles* s, int k, int rounds, int stall, EnsParam
 int ens_enqueue_launch(ising_ensembles* s, int k, int rounds, int stall) {
     EnsParams P;
     ens_params(s, k, rounds, stall, &P);
+    const bool staged = s->sched.loader == ISING_ENS_LOADER_STAGED;
+    if (staged)
+        for (size_t i = 0; i < s->ens.size(); ++i) {
+            const EnsHost& h = s->ens[i];
+            const Lattice& L = h.mesh->lat;
+            if (!ensembles_encode_maps(h.mesh->d_spins, L.nx, L.ny, h.n, &P.maps[i]))
+                return fail(ISING_ERR_CUDA, "cuTensorMapEncodeTiled (staged loader) failed");
+        }
     ISG_CUDA(cudaMemsetAsync(s->d_sync, 0, s->sync_words * sizeof(uint32_t), s->stream));
-    return launch_ensembles(P, s->move, s->dmi, s->has_k, s->sched.block_threads, s->grid, s->stream);
+    return launch_ensembles(P, s->move, s->dmi, s->has_k, staged, s->sched.block_threads, s->grid, s->stream);
 }
 
 int ens_resync_enqueue(ising_ensembles* s) {
@@ -1735,10 +1768,12 @@ extern "C" int ising_ensembles_autotune(ising_ensembles* s, int k, int rounds_pe
     const int chunks[] = {2048, 4096, 8192, 16384, 32768};
     for (int t : threads) {
         if (t < max_lanes) continue;
-        for (int c : chunks) cand.push_back({t, c, ISING_ENS_ORDER_PHASE, 0, 0.0});
+        for (int c : chunks) cand.push_back({t, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_REGISTERS});
         // replica groups of ~64 MB (one L2-resident group per round); slower so far, kept as a candidate
-        cand.push_back({t, 8192, ISING_ENS_ORDER_GROUPS, 64000000, 0.0});
+        cand.push_back({t, 8192, ISING_ENS_ORDER_GROUPS, 64000000, 0.0, ISING_ENS_LOADER_REGISTERS});
     }
+    if (ens_staged_fits(s))   // groups of 4, 8 and 16 x-planes per task at nz = 128
+        for (int c : {16384, 32768, 65536}) cand.push_back({256, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_STAGED});
     cudaEvent_t e0, e1;
     ISG_CUDA(cudaEventCreate(&e0));
     ISG_CUDA(cudaEventCreate(&e1));

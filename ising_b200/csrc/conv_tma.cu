@@ -377,17 +377,8 @@ __global__ void __launch_bounds__(kCtThreads) k_conv8_tma(const __grid_constant_
     if (warp == 0) tmem_dealloc(taddr, g.tmem_cols);
 }
 
-// the driver's tensor-map encoder, looked up once (thread-safe static initialisation)
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-        return nullptr;
-    }();
-    return fn;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
 }
 
 bool conv8_shape(const GemmArgs& g) {
@@ -458,6 +449,19 @@ int launch_conv8_tma(const GemmArgs& g, cudaStream_t s) {
 }
 
 }  // namespace
+
+// the driver's tensor-map encoder, looked up once (thread-safe static initialisation)
+void* tensor_map_encoder() {
+    static void* const fn = []() -> void* {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            return p;
+        return nullptr;
+    }();
+    return fn;
+}
 
 bool conv_tma_applies(const GemmArgs& g) {
     return (conv32_shape(g) || conv8_shape(g)) && encode_fn() != nullptr;

@@ -9,6 +9,8 @@
 // for tasks that running blocks hold and the kernel needs no co-residency guarantee.  The
 // last task of a round of ensemble e folds the partial sums and runs the exchange in-kernel.
 #pragma once
+#include <cuda.h>   // CUtensorMap
+
 #include "sweep_cb.cuh"
 
 namespace isg {
@@ -27,6 +29,7 @@ struct EnsDev {
     uint32_t rb;                 // thread rows per block: threads / (W / 2)
     uint32_t nseg, seg_len;      // y-segments per plane in a task, rows per segment
     FastDiv divSeg;              // by nseg
+    uint32_t st_nseg, st_seg_len;   // staged loader: y-segments per group of kStG planes, rows per segment
     int n_rep;                   // replicas 0..n_rep-1 (= temperature slots)
     double* beta_rep;
     uint32_t* sweep_ctr;         // the mesh's per-replica sweep counters
@@ -42,7 +45,29 @@ struct EnsDev {
     uint32_t* round_ctr;
 };
 
+// Staged loader (schedule loader 1; W = 64 only): a sub-block of kStG warps marches kStG
+// consecutive x-planes (one warp per plane) along y in lockstep.  For each row y a ring stage
+// receives, by two tiled TMA copies, the own colour's rows (planes x0 .. x0+kStG-1, all three
+// components) and the other colour's row y+1 of planes x0-1 .. x0+kStG; rows y-1 and y of
+// the other colour are the previous two stages.
+constexpr int kStG = 4;
+constexpr int kStSub = 2;                  // sub-blocks per 256-thread block
+constexpr int kStStages = 7;               // ring stages per sub-block
+constexpr int kStAhead = kStStages - 3;    // stages issued beyond the one being computed
+constexpr uint32_t kStNxtFloats = 3u * (kStG + 2) * 64u;   // [3][kStG+2][64]
+constexpr uint32_t kStOwnFloats = 3u * kStG * 64u;         // [3][kStG][64]
+constexpr uint32_t kStStageFloats = kStNxtFloats + kStOwnFloats;
+constexpr uint32_t kStSmemBytes = kStSub * kStStages * kStStageFloats * 4u + 2u * kStSub * kStStages * 8u + 128u;
+
+// Tensor maps of one ensemble's spins, dims (entry, y, x, colour, 3 replica + component):
+// next = box {64, 1, kStG+2, 1, 3}, own = {64, 1, kStG, 1, 3}, ctr = {64, 1, kStG, 1, 1},
+// halo = {64, 1, 1, 1, 1} (ctr and halo serve plane groups whose x-halo wraps around).
+struct alignas(64) EnsMaps {
+    CUtensorMap next, own, ctr, halo;
+};
+
 struct EnsParams {
+    EnsMaps maps[kMaxEnsembles];   // staged loader only
     EnsDev e[kMaxEnsembles];
     int n_ens;
     const uint2* table;          // one round: x = e << 24 | r, y = phase << 16 | chunk
@@ -61,11 +86,15 @@ struct EnsParams {
 };
 static_assert(sizeof(EnsParams) < 32000, "kernel parameter block too large");
 
-int launch_ensembles(const EnsParams& P, int move, int dmi, bool has_k, int threads, int grid, cudaStream_t s);
+int launch_ensembles(const EnsParams& P, int move, int dmi, bool has_k, bool staged, int threads, int grid,
+                     cudaStream_t s);
 // kernel instantiations, one translation unit per move kind (dmi in 1..3: 1 bulk,
 // 2 interfacial about z, 3 tabulated per bond direction)
-const void* ensembles_kernel_uniform(int dmi, bool has_k);
-const void* ensembles_kernel_ball(int dmi, bool has_k);
-int ensembles_blocks_per_sm(int move, int dmi, bool has_k, int threads, int* out);
+const void* ensembles_kernel_uniform(int dmi, bool has_k, bool staged);
+const void* ensembles_kernel_ball(int dmi, bool has_k, bool staged);
+int ensembles_blocks_per_sm(int move, int dmi, bool has_k, bool staged, int threads, int* out);
+// the staged loader's tensor maps for one ensemble (spins of n_rep replicas of an
+// nx x ny x 128 colour-separated mesh); false if the driver refuses one
+bool ensembles_encode_maps(float* spins, int nx, int ny, int n_rep, EnsMaps* m);
 
 }  // namespace isg

@@ -5,13 +5,16 @@
 namespace isg {
 
 template <int D, bool K>
-static const void* fn() { return reinterpret_cast<const void*>(&k_ensembles<0, D, K>); }
+static const void* fn(bool staged) {
+    return staged ? reinterpret_cast<const void*>(&k_ensembles<0, D, K, true>)
+                  : reinterpret_cast<const void*>(&k_ensembles<0, D, K, false>);
+}
 
-const void* ensembles_kernel_uniform(int dmi, bool has_k) {
+const void* ensembles_kernel_uniform(int dmi, bool has_k, bool staged) {
     switch (dmi) {
-        case 1: return has_k ? fn<1, true>() : fn<1, false>();
-        case 2: return has_k ? fn<2, true>() : fn<2, false>();
-        default: return has_k ? fn<3, true>() : fn<3, false>();
+        case 1: return has_k ? fn<1, true>(staged) : fn<1, false>(staged);
+        case 2: return has_k ? fn<2, true>(staged) : fn<2, false>(staged);
+        default: return has_k ? fn<3, true>(staged) : fn<3, false>(staged);
     }
 }
 

@@ -15,6 +15,8 @@ namespace isg {
 void set_error(const std::string& msg);
 int fail(int status, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
+// the driver's cuTensorMapEncodeTiled (nullptr if the driver has none), looked up once
+void* tensor_map_encoder();
 #define ISG_CUDA(call)                                              \
     do {                                                            \
         cudaError_t e_ = (call);                                    \

@@ -26,8 +26,9 @@ def _engine_and_refs(ib, members, k, rounds, scheme=0, move=1, sched=None, dmi="
     """Runs the engine on fresh meshes and one ParallelTempering per member on twin meshes."""
     emeshes, rmeshes, spec = [], [], []
     for L, n, D, B, K, ens in members:
-        em = ib.ChainMesh.simple_cubic(L, n_replicas=n)
-        rm = ib.ChainMesh.simple_cubic(L, n_replicas=n)
+        nx, ny, nz = L if isinstance(L, tuple) else (L, L, L)
+        em = ib.ChainMesh.simple_cubic(nx, ny=ny, nz=nz, n_replicas=n)
+        rm = ib.ChainMesh.simple_cubic(nx, ny=ny, nz=nz, n_replicas=n)
         em.init_uniform(SEED, ens)
         rm.init_uniform(SEED, ens)
         emeshes.append(em)
@@ -48,6 +49,7 @@ def _engine_and_refs(ib, members, k, rounds, scheme=0, move=1, sched=None, dmi="
 
 def _assert_same(members, eng, emeshes, rmeshes, refs):
     for i, (L, n, *_rest) in enumerate(members):
+        sites = int(np.prod(L)) if isinstance(L, tuple) else L ** 3
         for r in range(n):
             np.testing.assert_array_equal(emeshes[i].get_spins(r), rmeshes[i].get_spins(r),
                                           err_msg=f"ensemble {i} replica {r}")
@@ -56,8 +58,8 @@ def _assert_same(members, eng, emeshes, rmeshes, refs):
         e0, m0 = refs[i].energies()
         # the running sums add FP32 per-block partials; block shapes differ between the two
         # paths, so they agree to FP32 rounding of the per-round increments
-        np.testing.assert_allclose(e1, e0, rtol=1e-6, atol=1e-6 * n * L ** 3)
-        np.testing.assert_allclose(m1, m0, rtol=1e-6, atol=1e-6 * L ** 3)
+        np.testing.assert_allclose(e1, e0, rtol=1e-6, atol=1e-6 * n * sites)
+        np.testing.assert_allclose(m1, m0, rtol=1e-6, atol=1e-6 * sites)
         a1, c1 = eng.swap_stats(i)
         a0, c0 = refs[i].swap_stats()
         np.testing.assert_array_equal(a1, a0)
@@ -73,6 +75,69 @@ def _assert_same(members, eng, emeshes, rmeshes, refs):
 def test_engine_matches_single_ensemble_pt(ib, cuda_ok, sched):
     eng, em, rm, refs = _engine_and_refs(ib, MEMBERS, k=3, rounds=5, sched=sched)
     _assert_same(MEMBERS, eng, em, rm, refs)
+
+
+# nz = 128 meshes for the staged loader: plane groups that wrap in x (nx = 4: both halos),
+# interior groups (nx = 12, 16), short y columns (ny = 4), uneven chunk tails (P = 8 of 12)
+STAGED = [((12, 6, 128), 3, 0.5, 0.3, 0.05, 41), ((4, 4, 128), 2, 0.7, 0.1, 0.0, 42),
+          ((16, 8, 128), 4, 0.3, 0.2, 0.0, 43)]
+
+
+@pytest.mark.parametrize("chunk", [768, 1536, 2304, 100000])   # 4, 8, 12 planes, whole meshes
+@pytest.mark.parametrize("move", [1, 0])
+def test_staged_loader_matches_single_ensemble_pt(ib, cuda_ok, chunk, move):
+    sched = {"block_threads": 256, "chunk_pairs": chunk, "order": 0, "loader": 1}
+    eng, em, rm, refs = _engine_and_refs(ib, STAGED, k=3, rounds=4, move=move, sched=sched)
+    assert eng.schedule()["loader"] == "staged"
+    _assert_same(STAGED, eng, em, rm, refs)
+
+
+def test_staged_loader_at_l128(ib, cuda_ok):
+    members = [((128, 8, 128), 3, 0.7, 0.3, 0.05, 44)]
+    sched = {"block_threads": 256, "chunk_pairs": 16384, "order": 0, "loader": 1}
+    eng, em, rm, refs = _engine_and_refs(ib, members, k=2, rounds=3, sched=sched)
+    _assert_same(members, eng, em, rm, refs)
+
+
+def test_staged_loader_rejects_unsuited_meshes(ib, cuda_ok):
+    spec = []
+    for L, n, D, B, K, ens in MEMBERS[:2]:
+        m = ib.ChainMesh.simple_cubic(L, n_replicas=n)
+        m.init_uniform(SEED, ens)
+        spec.append((m, _betas(ib, n), _p(ib, D, B), ens))
+    eng = ib.Ensembles(spec, seed=SEED)
+    with pytest.raises(ib.IsingError):
+        eng.set_schedule(block_threads=256, chunk_pairs=4096, loader=1)      # nz != 128
+    spec2 = []
+    m = ib.ChainMesh.simple_cubic(12, ny=4, nz=128, n_replicas=2)
+    m.init_uniform(SEED, 45)
+    spec2.append((m, _betas(ib, 2), _p(ib, 0.5, 0.1), 45))
+    eng2 = ib.Ensembles(spec2, seed=SEED)
+    with pytest.raises(ib.IsingError):
+        eng2.set_schedule(block_threads=128, chunk_pairs=4096, loader=1)     # blocks of 256 only
+    eng2.set_schedule(block_threads=256, chunk_pairs=4096, loader=1)
+    eng2.run(2, 1)
+
+
+def test_staged_loader_timeout_and_recovery(ib, cuda_ok):
+    spec = []
+    for L, n, D, B, K, ens in STAGED[:2]:
+        m = ib.ChainMesh.simple_cubic(L[0], ny=L[1], nz=L[2], n_replicas=n)
+        m.init_uniform(SEED, ens)
+        spec.append((m, _betas(ib, n), _p(ib, D, B), ens))
+    eng = ib.Ensembles(spec, seed=SEED, wait_timeout_ms=50)
+    eng.set_schedule(block_threads=256, chunk_pairs=768, loader=1)
+    eng.inject_stall(1)
+    with pytest.raises(ib.IsingError) as ei:
+        eng.run(2, 3)
+    assert ei.value.status == 4          # ISING_ERR_TIMEOUT
+    eng.run(2, 2)
+    for i in range(2):
+        e_run, _ = eng.energies(i)
+        assert np.all(np.isfinite(e_run))
+        eng.resync()
+        e_new, _ = eng.energies(i)
+        assert np.max(np.abs(e_run - e_new)) / spec[i][0].numAtoms < 1e-5
 
 
 def test_engine_random_pairs_and_uniform_move(ib, cuda_ok):
