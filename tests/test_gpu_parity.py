@@ -101,6 +101,24 @@ def test_init_uniform_matches_oracle(oracle, ib, cuda_ok):
         assert np.allclose(np.linalg.norm(g, axis=1), 1.0, atol=1e-6)
 
 
+@pytest.mark.parametrize("kind", ["bulk", "interfacial"])
+def test_spin_spiral_energy_known_answer_at_l128(ib, cuda_ok, kind):
+    """The device energy of a commensurate spiral at L=128 equals the closed form
+    N (J cos q - Dz sin q + 2J) that pins the oracle's DMI convention (tests/test_oracle.py)."""
+    L = 128
+    pm = ib.ChainMesh.simple_cubic(L)
+    q = 2.0 * np.pi * 5 / L
+    x = np.rint(pm.positions()[:, 0]).astype(np.float64)
+    c, s_, z = np.cos(q * x), np.sin(q * x), np.zeros_like(x)
+    spins = np.stack([z, c, s_], axis=1) if kind == "bulk" else np.stack([s_, z, c], axis=1)
+    pm.set_spins(spins)
+    J, Dz, B = -1.0, 0.7, 0.3
+    e, _m = ib.observables(pm, ib.params(J=J, Dz=Dz, B=B, dmi=kind, include_Jp=False))
+    N = pm.numAtoms
+    want = N * (J * np.cos(q) - Dz * np.sin(q) + 2.0 * J)
+    assert abs(e[0] - want) <= 1e-6 * N * (6 * abs(J) + 6 * Dz + B)
+
+
 @pytest.mark.parametrize("kind,dims", [("SC", (8, 8, 6)), ("BCC", (4, 4, 4)), ("HK", (3, 3, 4))])
 def test_winding_parity(oracle, ib, cuda_ok, kind, dims):
     om, pm = _pair(oracle, ib, kind, dims)

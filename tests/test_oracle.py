@@ -105,6 +105,43 @@ def test_uniform_state_energies(oracle, J, B, Dz):
     assert n == pytest.approx(-6 * J + B, abs=1e-12)
 
 
+def _spiral(positions, q, kind):
+    """Commensurate spiral along x: a Bloch helix (0, cos qx, sin qx) for bulk DMI, a Neel
+    cycloid (sin qx, 0, cos qx) for interfacial DMI about z."""
+    x = np.rint(positions[:, 0]).astype(np.float64)
+    c, s = np.cos(q * x), np.sin(q * x)
+    z = np.zeros_like(x)
+    return np.stack([z, c, s], axis=1) if kind == "bulk" else np.stack([s, z, c], axis=1)
+
+
+@pytest.mark.parametrize("kind", ["bulk", "interfacial"])
+@pytest.mark.parametrize("m_q", [1, -1, 3])
+def test_spin_spiral_dmi_known_answers(oracle, kind, m_q):
+    """DMI sign and bond-vector convention pinned by a closed form.  With the bond vector
+    r = -(r_j - r_i)/|r_j - r_i| and D = Dz r (bulk) or Dz z x r (interfacial), both x-bonds of
+    a site of the spiral give D.(S_i x S_j) = -Dz sin q and J cos q, the y and z bonds J:
+    energy per site J cos q - Dz sin q + 2J (the Zeeman sum vanishes over whole periods), local
+    sum 2J cos q - 2 Dz sin q + 4J - B S_z."""
+    L = 8
+    m = oracle.Mesh.sc(L)
+    q = 2.0 * np.pi * m_q / L
+    m.set_spins(_spiral(m.positions(), q, kind))
+    J, Dz, B = -1.0, 0.7, 0.3
+    p = oracle.Params(J=J, Dz=Dz, B=B, dmi_bulk=(kind == "bulk"))
+    N = m.natoms
+    per_site = J * np.cos(q) - Dz * np.sin(q) + 2.0 * J
+    assert m.canonical_energy(p) == pytest.approx(N * per_site, abs=1e-9)
+    assert m.total_energy(p, 2.0) == pytest.approx(N * per_site, abs=1e-9)
+    for atom in (0, 9, 77, N - 1):
+        S = m.spins[atom].copy()
+        o, n = m.local_energy(atom, p, S)
+        want = 2.0 * J * np.cos(q) - 2.0 * Dz * np.sin(q) + 4.0 * J - B * S[2]
+        assert o == pytest.approx(want, abs=1e-12) and n == pytest.approx(want, abs=1e-12)
+    # the opposite chirality costs 2 Dz sin q more (or less) per site: DMI selects one hand
+    m.set_spins(_spiral(m.positions(), -q, kind))
+    assert m.canonical_energy(p) - N * per_site == pytest.approx(N * 2.0 * Dz * np.sin(q), abs=1e-9)
+
+
 def test_local_delta_equals_total_difference(oracle):
     m = oracle.Mesh.sc(6)
     m.init_uniform(0x15196)
