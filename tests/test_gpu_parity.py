@@ -274,6 +274,24 @@ def test_error_paths(ib, cuda_ok):
     assert e.value.status == 3
 
 
+def test_empty_and_null_inputs(ib, cuda_ok):
+    """Empty batches are no-ops; NULL buffers and out-of-range replicas are argument errors."""
+    from ising_b200 import _lib
+    pm = ib.ChainMesh.simple_cubic(6)
+    old, new = ib.local_energy_batch(pm, np.zeros(0, np.int64), np.zeros((0, 3)), ib.params(J=-1.0))
+    assert old.shape == (0,) and new.shape == (0,)
+    L = _lib.load()
+    assert L.ising_spins_set(pm.handle, 0, None) == 1
+    assert L.ising_spins_get(pm.handle, 0, None) == 1
+    assert L.ising_spins_set(pm.handle, 1, None) in (1, 3)
+    spec = [(pm, 1.0 / ib.temperature_ladder(0.5, 1.0, 1), ib.params(J=-1.0, Dz=0.3, dmi="bulk"), 1)]
+    before = pm.get_spins(0).copy()
+    eng = ib.Ensembles(spec, seed=7)
+    eng.run(2, 0)                       # zero rounds: nothing runs, nothing changes
+    np.testing.assert_array_equal(pm.get_spins(0), before)
+    eng.close()
+
+
 def test_spins_csv_bytes(oracle, ib, cuda_ok, tmp_path):
     om, pm = _pair(oracle, ib, "BCC", (3, 3, 3))
     s = _random_spins(om.natoms, 8)

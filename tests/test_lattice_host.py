@@ -79,3 +79,14 @@ def test_mesh_argument_errors(ib):
     with pytest.raises(ib.IsingError) as e:
         m.get_spins(0)  # no device state on a lattice-only mesh
     assert e.value.status == 1
+    # maximum size: 1300^3 > 2^31-1 atoms is refused before any table is allocated
+    with pytest.raises(ib.IsingError) as e:
+        ib.ChainMesh.simple_cubic(1300, device=-1)
+    assert e.value.status == 1 and "2^31" in str(e.value)
+    for kw in ({"n_replicas": 0}, {"numShells": 5}):
+        with pytest.raises(ib.IsingError) as e:
+            ib.ChainMesh.simple_cubic(4, device=-1, **kw)
+        assert e.value.status == 1
+    with pytest.raises(ib.IsingError) as e:
+        ib.ChainMesh.simple_cubic(4, a=0.0, device=-1)
+    assert e.value.status == 1
