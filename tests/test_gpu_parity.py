@@ -284,11 +284,13 @@ def test_empty_and_null_inputs(ib, cuda_ok):
     assert L.ising_spins_set(pm.handle, 0, None) == 1
     assert L.ising_spins_get(pm.handle, 0, None) == 1
     assert L.ising_spins_set(pm.handle, 1, None) in (1, 3)
-    spec = [(pm, 1.0 / ib.temperature_ladder(0.5, 1.0, 1), ib.params(J=-1.0, Dz=0.3, dmi="bulk"), 1)]
-    before = pm.get_spins(0).copy()
+    em = ib.ChainMesh.simple_cubic(8)           # the engine needs nz % 4 == 0
+    em.init_uniform(7, 1)
+    spec = [(em, 1.0 / ib.temperature_ladder(0.5, 1.0, 1), ib.params(J=-1.0, Dz=0.3, dmi="bulk", include_Jp=False), 1)]
+    before = em.get_spins(0).copy()
     eng = ib.Ensembles(spec, seed=7)
     eng.run(2, 0)                       # zero rounds: nothing runs, nothing changes
-    np.testing.assert_array_equal(pm.get_spins(0), before)
+    np.testing.assert_array_equal(em.get_spins(0), before)
     eng.close()
 
 
