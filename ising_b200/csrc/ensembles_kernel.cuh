@@ -145,12 +145,14 @@ __device__ __forceinline__ bool st_try_suspend(uint64_t* bar, uint32_t par) {
     return ok != 0;
 }
 // bounded wait for phase parity `par`; gives up when the block's abort flag is raised or
-// the wait passes the engine's bound (then raises the flags itself)
+// the wait passes the engine's bound (then raises the flags itself).  The poll count is a
+// second bound in case the timer does not advance: a poll lasts from tens of nanoseconds
+// to the 20 us suspend, so wait_ns / 4096 polls end within ~wait_ns / 100 .. 5 wait_ns.
 static __device__ __forceinline__ bool st_wait(const EnsParams& P, uint64_t* bar, uint32_t par,
                                                volatile int* s_abort) {
     if (st_try(bar, par)) return true;
     const uint64_t t0 = global_ns();
-    const uint64_t max_polls = P.wait_ns / 16u + 4096u;
+    const uint64_t max_polls = P.wait_ns / 4096u + 4096u;
     for (uint64_t it = 0; it < max_polls; ++it) {
         if (st_try_suspend(bar, par)) return true;
         if (*s_abort) return false;
