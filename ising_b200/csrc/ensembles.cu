@@ -26,7 +26,8 @@ int ensembles_blocks_per_sm(int move, int dmi, bool has_k, bool staged, int thre
     const int st = ens_smem_attr(fn, staged);
     if (st != ISING_OK) return st;
     int n = 0;
-    ISG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, staged ? (size_t)kStSmemBytes : 0));
+    ISG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, staged ? kStThreads : threads,
+                                                           staged ? (size_t)kStSmemBytes : 0));
     *out = n;
     return ISING_OK;
 }
@@ -39,7 +40,9 @@ int launch_ensembles(const EnsParams& P, int move, int dmi, bool has_k, bool sta
     if (P.n_ens < 1 || P.n_ens > kMaxEnsembles) return fail(ISING_ERR_ARG, "1..16 ensembles per engine");
     const void* fn = ens_kernel(move, dmi, has_k, staged);
     void* args[] = {const_cast<EnsParams*>(&P)};
-    ISG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, staged ? (size_t)kStSmemBytes : 0, s));
+    // staged: the schedule's 256 compute threads plus the copy warp
+    ISG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(staged ? kStThreads : threads), args,
+                              staged ? (size_t)kStSmemBytes : 0, s));
     return ISING_OK;
 }
 

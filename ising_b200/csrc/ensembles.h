@@ -49,11 +49,11 @@ struct EnsDev {
 // consecutive x-planes (one warp per plane) along y in lockstep.  For each row y a ring stage
 // receives, by two tiled TMA copies, the own colour's rows (planes x0 .. x0+kStG-1, all three
 // components) and the other colour's row y+1 of planes x0-1 .. x0+kStG; rows y-1 and y of
-// the other colour are the previous two stages.
+// the other colour are the previous two stages.  A separate copy warp issues the copies.
 constexpr int kStG = 4;
-constexpr int kStSub = 2;                  // sub-blocks per 256-thread block
+constexpr int kStSub = 2;                  // sub-blocks of compute warps per block
+constexpr int kStThreads = kStSub * kStG * 32 + 32;   // the compute warps and one copy warp
 constexpr int kStStages = 7;               // ring stages per sub-block
-constexpr int kStAhead = kStStages - 3;    // stages issued beyond the one being computed
 constexpr uint32_t kStNxtFloats = 3u * (kStG + 2) * 64u;   // [3][kStG+2][64]
 constexpr uint32_t kStOwnFloats = 3u * kStG * 64u;         // [3][kStG][64]
 constexpr uint32_t kStStageFloats = kStNxtFloats + kStOwnFloats;

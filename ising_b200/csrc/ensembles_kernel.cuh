@@ -208,42 +208,61 @@ static __device__ __forceinline__ void st_issue(const EnsMaps& M, const EnsDev& 
     if (t >= 2) st_tma5(st + kStNxtFloats, &M.own, (int)(U.ya + t - 2), x0, colour, c4, fb);
 }
 
-// One task's colour pass with TMA-staged rows.  Warp g of sub-block sb updates plane x0 + g
-// of units sb, sb + kStSub, ...; lane l the entry pair (2l, 2l+1).  Lane 0 of each sub-block's
-// first warp issues the copies kStAhead stages ahead.  False if a wait gave up (the copies
-// still in flight have then been waited for, boundedly).
+// One task's colour pass with TMA-staged rows.  Warp g of sub-block sb (compute warps
+// 0 .. kStSub * kStG - 1) updates plane x0 + g of units sb, sb + kStSub, ...; lane l the entry
+// pair (2l, 2l+1).  The last warp issues the copies: its lane sb fills sub-block sb's ring as
+// far as released stages allow.  False if a wait gave up (the copy lanes have then waited,
+// boundedly, for the copies still in flight).
 template <int MOVE, int DMI, bool HAS_K, int EI>
 __device__ __forceinline__ bool run_chunk_staged(const EnsParams& P, uint32_t rep, uint32_t ph, uint32_t ch,
                                                  StRing& R, volatile int* s_abort, v2& de, v2& dmx, v2& dmy,
                                                  v2& dmz) {
     const EnsDev& E = P.e[EI];
-    const EnsMaps& M = P.maps[EI];
     const CbGeom& G = E.g;
     const int colour = (int)(ph & 1u);
+    const uint32_t ny = (uint32_t)G.ny, nx = (uint32_t)G.nx, xs = G.row_stride_x;
+    const uint32_t x0c = ch * E.P;
+    const uint32_t np = min(x0c + E.P, nx) - x0c;
+    const uint32_t nunits = (np / (uint32_t)kStG) * E.st_nseg;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    bool ok = true;
+    if (warp == (uint32_t)(kStSub * kStG)) {   // the copy warp
+        if (lane >= (uint32_t)kStSub) return true;
+        const EnsMaps& M = P.maps[EI];
+        // the spins the copies read were published by st.release and acquired by this thread
+        // in the generic proxy: order them before this task's async-proxy (TMA) reads
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        uint32_t m = R.cons;   // copy lanes: stages issued so far
+#pragma unroll 1
+        for (uint32_t u = lane; u < nunits && ok; u += kStSub) {
+            const StUnit U = st_unit(E, x0c, u);
+            const uint32_t T = U.yb - U.ya + 2u;
+#pragma unroll 1
+            for (uint32_t t = 0; t < T; ++t) {
+                if (m >= (uint32_t)kStStages)
+                    ok = st_wait(P, R.empty + m % kStStages, ((m / kStStages) - 1u) & 1u, s_abort);
+                if (!ok) break;
+                st_issue(M, E, R, m, U, t, colour, rep);
+                ++m;
+            }
+        }
+        if (!ok) {
+            // the last kStStages stages issued may still write into the ring: let them land
+            for (uint32_t q = m > (uint32_t)kStStages ? m - kStStages : 0u; q < m; ++q)
+                for (uint32_t it = 0; it < (1u << 20); ++it)
+                    if (st_try(R.full + q % kStStages, (q / kStStages) & 1u)) break;
+        }
+        R.cons = m;
+        return ok;
+    }
     const uint32_t sweep = __ldcg(E.sweep_ctr + rep) + (ph >> 1);
     const float beta2 = (float)(__ldcg(E.beta_rep + rep) * 1.4426950408889634);
     float* __restrict__ sx = E.spins + (size_t)rep * 3 * E.N;
     float* __restrict__ sy = sx + E.N;
     float* __restrict__ sz = sy + E.N;
-    const uint32_t ny = (uint32_t)G.ny, nx = (uint32_t)G.nx, xs = G.row_stride_x;
     const uint32_t own = (uint32_t)colour * G.half;
-    const uint32_t x0c = ch * E.P;
-    const uint32_t np = min(x0c + E.P, nx) - x0c;
-    const uint32_t nunits = (np / (uint32_t)kStG) * E.st_nseg;
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t sb = warp / (uint32_t)kStG, g = warp - sb * (uint32_t)kStG;
-    const bool producer = g == 0 && lane == 0;
     const uint32_t j = 2u * lane;
-
-    // producer cursor: unit pu, step pt (of pT), stage number prod
-    uint32_t prod = R.cons, pu = sb, pt = 0, pT = 0;
-    StUnit PU{0, 0, 0};
-    if (pu < nunits) { PU = st_unit(E, x0c, pu); pT = PU.yb - PU.ya + 2u; }
-    bool ok = true;
-    // the spins the copies read were published by st.release and acquired by this thread in
-    // the generic proxy: order them before this task's async-proxy (TMA) reads
-    if (producer) asm volatile("fence.proxy.async.global;" ::: "memory");
-    // every stage of this task has been waited for once the loop ends normally
 #pragma unroll 1
     for (uint32_t u = sb; u < nunits && ok; u += kStSub) {
         const StUnit U = st_unit(E, x0c, u);
@@ -252,21 +271,7 @@ __device__ __forceinline__ bool run_chunk_staged(const EnsParams& P, uint32_t re
 #pragma unroll 1
         for (uint32_t t = 0; t < T; ++t) {
             const uint32_t n = R.cons;
-            if (producer) {
-                while (ok && pu < nunits && prod <= n + (uint32_t)kStAhead) {
-                    if (prod >= (uint32_t)kStStages)
-                        ok = st_wait(P, R.empty + prod % kStStages, ((prod / kStStages) - 1u) & 1u, s_abort);
-                    if (!ok) break;
-                    st_issue(M, E, R, prod, PU, pt, colour, rep);
-                    ++prod;
-                    if (++pt == pT) {
-                        pu += kStSub;
-                        pt = 0;
-                        if (pu < nunits) { PU = st_unit(E, x0c, pu); pT = PU.yb - PU.ya + 2u; }
-                    }
-                }
-            }
-            ok = ok && st_wait(P, R.full + n % kStStages, (n / kStStages) & 1u, s_abort);
+            ok = st_wait(P, R.full + n % kStStages, (n / kStStages) & 1u, s_abort);
             if (!ok) break;
             R.cons = n + 1u;
             if (t < 2) continue;
@@ -305,22 +310,15 @@ __device__ __forceinline__ bool run_chunk_staged(const EnsParams& P, uint32_t re
             }
         }
     }
-    if (!ok && producer) {
-        // copies issued but not waited for still write into the ring: let them land
-        for (uint32_t m = R.cons; m < prod; ++m) {
-            for (uint32_t it = 0; it < (1u << 20); ++it)
-                if (st_try(R.full + m % kStStages, (m / kStStages) & 1u)) break;
-        }
-    }
     return ok;
 }
 
 template <int MOVE, int DMI, bool HAS_K, bool STAGED>
-__global__ void __launch_bounds__(kEnsMaxThreads, 2) k_ensembles(const __grid_constant__ EnsParams P) {
+__global__ void __launch_bounds__(STAGED ? kStThreads : kEnsMaxThreads, 2) k_ensembles(const __grid_constant__ EnsParams P) {
     __shared__ uint32_t s_task[5];
     __shared__ int s_go, s_fin;
     __shared__ volatile int s_abort;
-    __shared__ float red[4][kEnsMaxThreads / 32];
+    __shared__ float red[4][(kStThreads + 31) / 32];
     extern __shared__ __align__(128) unsigned char st_raw[];
     const uint32_t nph = 2u * P.k;
     const uint32_t tpr = P.tasks_per_round;
@@ -328,7 +326,9 @@ __global__ void __launch_bounds__(kEnsMaxThreads, 2) k_ensembles(const __grid_co
     StRing ring{};
     if (STAGED) {
         unsigned char* base = st_raw + ((128u - (st_smem(st_raw) & 127u)) & 127u);
-        const uint32_t sb = (threadIdx.x >> 5) / (uint32_t)kStG;
+        // compute warps by sub-block; lane sb of the copy warp serves sub-block sb
+        const uint32_t w = threadIdx.x >> 5, l = threadIdx.x & 31u;
+        const uint32_t sb = w < (uint32_t)(kStSub * kStG) ? w / (uint32_t)kStG : (l < (uint32_t)kStSub ? l : 0u);
         float* stages = reinterpret_cast<float*>(base);
         uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStSub * kStStages * kStStageFloats * 4u);
         ring.stages = stages + sb * kStStages * kStStageFloats;
