@@ -20,6 +20,7 @@ CASES = {
     "sc4": (O.SC_CELL, (4, 4, 4)),
     "sc6": (O.SC_CELL, (6, 6, 6)),
     "sc8": (O.SC_CELL, (8, 8, 8)),
+    "sc16": (O.SC_CELL, (16, 16, 16)),
     "bcc3": (O.BCC_CELL, (3, 3, 3)),
     "hk3": (O.HYPER_KAGOME_CELL, (3, 3, 3)),
 }

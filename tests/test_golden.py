@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-NAMES = ["sc4", "sc6", "sc8", "bcc3", "hk3"]
+NAMES = ["sc4", "sc6", "sc8", "sc16", "bcc3", "hk3"]
 
 
 @pytest.mark.parametrize("name", NAMES)

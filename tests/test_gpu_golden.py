@@ -8,7 +8,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 HAM = dict(J=-1.0, J_prime=0.15, Dz=0.4, B=0.2, K=0.05, K_axis=(0.0, 0.6, 0.8))
-CELLS = {"sc4": ("SC", (4, 4, 4)), "sc6": ("SC", (6, 6, 6)), "sc8": ("SC", (8, 8, 8)),
+CELLS = {"sc4": ("SC", (4, 4, 4)), "sc6": ("SC", (6, 6, 6)), "sc8": ("SC", (8, 8, 8)), "sc16": ("SC", (16, 16, 16)),
          "bcc3": ("BCC", (3, 3, 3)), "hk3": ("HK", (3, 3, 3))}
 
 
