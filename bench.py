@@ -417,7 +417,11 @@ def run_gpu(args, w):
 
     # end to end through the C-ABI with host-owned FP64 spins (the reference's atomSpins):
     # every step uploads all replicas from pinned host memory, runs the round, downloads
-    # all replicas and the per-replica energies.
+    # all replicas and the per-replica energies.  The transfers are queued per replica
+    # (ising_spins_*_async): the upload of replica r starts once the previous step's download
+    # of r has landed in the host array, while other replicas still download, so the two
+    # directions of the link overlap; the run waits for every upload, and the timed region
+    # ends after the last downloads have landed.
     e2e = None
     if not args.no_e2e:
         L_ = _lib.load()
@@ -432,20 +436,26 @@ def run_gpu(args, w):
         def e2e_step():
             for (mm, b, _, _), hs in zip(members, host):
                 for r in range(len(b)):
-                    _lib.check(L_.ising_spins_set(mm.handle, r, dp(hs[r])), "set")
-            run(1)
+                    _lib.check(L_.ising_spins_set_async(mm.handle, r, dp(hs[r])), "set")
+            run(1)          # waits for the uploads
             for (mm, b, _, _), hs in zip(members, host):
                 for r in range(len(b)):
-                    _lib.check(L_.ising_spins_get(mm.handle, r, dp(hs[r])), "get")
+                    _lib.check(L_.ising_spins_get_async(mm.handle, r, dp(hs[r])), "get")
             return energies()
 
+        def e2e_wait():
+            for mm, _, _, _ in members:
+                _lib.check(L_.ising_spins_wait(mm.handle), "wait")
+
         e2e_step()
+        e2e_wait()
         barrier()
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(stream)
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             e2e_step()
+        e2e_wait()
         a1.record(stream)
         barrier()
         wall = time.perf_counter() - t0
@@ -454,7 +464,8 @@ def run_gpu(args, w):
         e2e = {"value": world * updates_per_step * e2e_steps / (e_ms / 1e3), "unit": "spin-updates/s",
                "h2d_bytes_per_step": sites * 3 * 8, "d2h_bytes_per_step": sites * 3 * 8 + n_rep * 32,
                "steps": e2e_steps,
-               "path": "ising_spins_set per replica -> one round -> ising_spins_get per replica + energies"}
+               "path": "ising_spins_set_async per replica -> one round -> ising_spins_get_async per replica "
+                       "+ energies; ising_spins_wait at the end"}
 
     cpu = cpu_fast = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -107,6 +107,17 @@ int ising_mesh_derivative_list(const ising_mesh* mesh, int64_t* out);
  * (ChainMesh_t%atomSpins, src/chainMesh.f90:20).  set rejects NaN or zero vectors. */
 int ising_spins_set(ising_mesh* mesh, int replica, const double* col_major_n3);
 int ising_spins_get(const ising_mesh* mesh, int replica, double* col_major_n3);
+/* Asynchronous forms (no reference counterpart): queue the transfer of one replica and return.
+ * Downloads and uploads run on two streams of their own, after the work already issued on the
+ * mesh, so opposite directions overlap; an upload of replica r waits for the last download of
+ * r (and vice versa), so one host array can be read back and sent again without a host wait.
+ * The host array must stay valid, and unmodified by the host, until ising_spins_wait returns;
+ * use pinned memory for overlap.  ising_spins_wait waits for every queued transfer and reports
+ * invalid uploaded spins (ISING_ERR_NAN); every other call on the mesh, or on a PT object or
+ * engine using it, waits for them first. */
+int ising_spins_get_async(ising_mesh* mesh, int replica, double* col_major_n3);
+int ising_spins_set_async(ising_mesh* mesh, int replica, const double* col_major_n3);
+int ising_spins_wait(ising_mesh* mesh);
 /* Uniform unit vectors on every replica from Philox(seed; site, 0, replica, ensemble|1).
  * The reference leaves PT spins uninitialised (src/chainMesh.f90:889-890). */
 int ising_spins_init_uniform(ising_mesh* mesh, uint64_t seed, uint32_t ensemble);

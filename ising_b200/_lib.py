@@ -88,6 +88,9 @@ _SIGS = {
     "ising_mesh_colouring": (_i, [_vp, _P(Params), _P(_i), _P(_i)]),
     "ising_spins_set": (_i, [_vp, _i, _P(_d)]),
     "ising_spins_get": (_i, [_vp, _i, _P(_d)]),
+    "ising_spins_set_async": (_i, [_vp, _i, _P(_d)]),
+    "ising_spins_get_async": (_i, [_vp, _i, _P(_d)]),
+    "ising_spins_wait": (_i, [_vp]),
     "ising_spins_init_uniform": (_i, [_vp, _u64, _u32]),
     "ising_params_reference": (_i, [_i, _d, _d, _d, _d, _d, _P(Params)]),
     "ising_local_energy": (_i, [_vp, _i, _i, _P(Params), _P(_d), _P(_d), _P(_d)]),

@@ -169,6 +169,21 @@ class ChainMesh:
         col = np.ascontiguousarray(s.T)
         _lib.call("ising_spins_set", self._h, replica, _dp(col))
 
+    def get_spins_async(self, host_ptr: int, replica: int = 0):
+        """Queue the download of one replica's atomSpins (3 x numAtoms FP64, column-major) to
+        the host address `host_ptr` (pinned memory for overlap, e.g. a pinned torch tensor's
+        data_ptr()); complete after wait_spins()."""
+        _lib.call("ising_spins_get_async", self._h, replica, C.cast(host_ptr, _P(C.c_double)))
+
+    def set_spins_async(self, host_ptr: int, replica: int = 0):
+        """Queue the upload of one replica from the host address `host_ptr` (same layout);
+        it starts after the last queued download of that replica."""
+        _lib.call("ising_spins_set_async", self._h, replica, C.cast(host_ptr, _P(C.c_double)))
+
+    def wait_spins(self):
+        """Wait for every queued transfer; raises on invalid uploaded spins."""
+        _lib.call("ising_spins_wait", self._h)
+
     @property
     def atomSpins(self) -> np.ndarray:
         return self.get_spins(0)

@@ -340,11 +340,16 @@ int enqueue_sweep(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_rep
     return enqueue_sweeps(m, plan, rep_first, n_rep, d_beta_rep, sweep_offset, 1, seed, ensemble, move, r, partials);
 }
 
-int check_replica(const ising_mesh* m, int replica) {
+int check_replica_only(const ising_mesh* m, int replica) {
     if (!m) return fail(ISING_ERR_ARG, "mesh is NULL");
     if (m->device < 0) return fail(ISING_ERR_ARG, "mesh was created without a device (device = -1)");
     if (replica < 0 || replica >= m->n_replicas) return fail(ISING_ERR_BOUNDS, "replica index out of range");
     return ISING_OK;
+}
+// the replica check of every synchronous entry point: also lets pending transfers land
+int check_replica(const ising_mesh* m, int replica) {
+    ISG_TRY(check_replica_only(m, replica));
+    return mesh_settle(m);
 }
 
 // energy + magnetisation of replicas [first, first+n) into d_out[n][4] (device)
@@ -454,11 +459,16 @@ extern "C" int ising_mesh_create(const float* frac, int nsub, int nx, int ny, in
     return ISING_OK;
 }
 
+namespace {
+void xfer_release(ising_mesh* m);   // asynchronous-transfer state (defined with ising_spins_*_async)
+}
+
 extern "C" int ising_mesh_destroy(ising_mesh* m) {
     if (!m) return ISING_OK;
     if (m->device < 0) { delete m; return ISING_OK; }
     DeviceGuard g(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
+    xfer_release(m);
     cudaFree(m->d_spins); cudaFree(m->d_sweep); cudaFree(m->d_scratch); cudaFree(m->d_status);
     cudaFree(m->d_staging); cudaFree(m->d_beta); cudaFree(m->d_winding_tmp); cudaFree(m->d_slots); cudaFree(m->d_slot_count);
     cudaFree(m->d_plaq);
@@ -488,6 +498,7 @@ extern "C" int ising_mesh_set_stream(ising_mesh* m, void* stream) {
     if (!m) return fail(ISING_ERR_ARG, "mesh is NULL");
     if (m->device < 0) return fail(ISING_ERR_ARG, "mesh was created without a device (device = -1)");
     DeviceGuard g(m->device);
+    ISG_TRY(mesh_settle(m));
     // order the switch: work already issued on the old stream completes first
     ISG_CUDA(cudaStreamSynchronize(m->stream));
     m->stream = stream ? static_cast<cudaStream_t>(stream) : m->own_stream;
@@ -590,6 +601,113 @@ extern "C" int ising_spins_get(const ising_mesh* mc, int replica, double* s) {
     ISG_CUDA(cudaMemcpyAsync(s, d, (size_t)3 * N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
     ISG_CUDA(cudaStreamSynchronize(m->stream));
     return ISING_OK;
+}
+
+namespace {
+
+// Asynchronous transfers of a mesh: downloads on one stream, uploads on another, one FP64
+// staging buffer per replica and, per replica, the events that order a download and an
+// upload of the same replica (they share the staging buffer and, typically, the host array).
+struct Xfer {
+    cudaStream_t d2h = nullptr, h2d = nullptr;
+    cudaEvent_t main_ready = nullptr;        // the mesh stream's work issued before a transfer
+    std::vector<double*> stage;
+    std::vector<cudaEvent_t> got, put;       // download / upload of replica r complete
+    bool pending = false;
+};
+
+void xfer_release(ising_mesh* m) {
+    Xfer* x = static_cast<Xfer*>(m->xfer);
+    if (!x) return;
+    if (x->d2h) { cudaStreamSynchronize(x->d2h); cudaStreamDestroy(x->d2h); }
+    if (x->h2d) { cudaStreamSynchronize(x->h2d); cudaStreamDestroy(x->h2d); }
+    if (x->main_ready) cudaEventDestroy(x->main_ready);
+    for (double* d : x->stage) cudaFree(d);
+    for (cudaEvent_t e : x->got) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : x->put) if (e) cudaEventDestroy(e);
+    delete x;
+    m->xfer = nullptr;
+}
+
+int xfer_state(ising_mesh* m, Xfer** out) {
+    if (!m->xfer) {
+        std::unique_ptr<Xfer> x(new Xfer());
+        const int R = m->n_replicas;
+        x->stage.assign(R, nullptr);
+        x->got.assign(R, nullptr);
+        x->put.assign(R, nullptr);
+        m->xfer = x.release();
+        Xfer* y = static_cast<Xfer*>(m->xfer);
+        auto bail = [&](cudaError_t e, const char* what) { xfer_release(m); return cuda_fail(e, what); };
+        cudaError_t e;
+        if ((e = cudaStreamCreateWithFlags(&y->d2h, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+        if ((e = cudaStreamCreateWithFlags(&y->h2d, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+        if ((e = cudaEventCreateWithFlags(&y->main_ready, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
+        for (int r = 0; r < R; ++r)
+            if ((e = cudaEventCreateWithFlags(&y->got[r], cudaEventDisableTiming)) != cudaSuccess ||
+                (e = cudaEventCreateWithFlags(&y->put[r], cudaEventDisableTiming)) != cudaSuccess)
+                return bail(e, "event");
+    }
+    *out = static_cast<Xfer*>(m->xfer);
+    return ISING_OK;
+}
+
+}  // namespace
+
+int isg::mesh_settle(const ising_mesh* mc) {
+    ising_mesh* m = const_cast<ising_mesh*>(mc);
+    Xfer* x = m ? static_cast<Xfer*>(m->xfer) : nullptr;
+    if (!x || !x->pending) return ISING_OK;
+    DeviceGuard g(m->device);
+    x->pending = false;
+    ISG_CUDA(cudaStreamSynchronize(x->d2h));
+    ISG_CUDA(cudaStreamSynchronize(x->h2d));
+    return check_status(m);   // an upload of non-finite or zero spins set the status word
+}
+
+extern "C" int ising_spins_get_async(ising_mesh* m, int replica, double* s) {
+    ISG_TRY(check_replica_only(m, replica));
+    if (!s) return fail(ISING_ERR_ARG, "spins array is NULL");
+    DeviceGuard g(m->device);
+    Xfer* x;
+    ISG_TRY(xfer_state(m, &x));
+    const int64_t N = m->lat.natoms;
+    if (!x->stage[replica]) ISG_TRY(dev_alloc(&x->stage[replica], (size_t)3 * N));
+    // after the work already issued on the mesh's stream and any upload of this replica
+    ISG_CUDA(cudaEventRecord(x->main_ready, m->stream));
+    ISG_CUDA(cudaStreamWaitEvent(x->d2h, x->main_ready, 0));
+    ISG_CUDA(cudaStreamWaitEvent(x->d2h, x->put[replica], 0));
+    x->pending = true;
+    ISG_TRY(launch_spins_to_f64(m->d_spins + (int64_t)replica * 3 * N, x->stage[replica], N, m->layout, x->d2h));
+    ISG_CUDA(cudaMemcpyAsync(s, x->stage[replica], (size_t)3 * N * sizeof(double), cudaMemcpyDeviceToHost, x->d2h));
+    ISG_CUDA(cudaEventRecord(x->got[replica], x->d2h));
+    return ISING_OK;
+}
+
+extern "C" int ising_spins_set_async(ising_mesh* m, int replica, const double* s) {
+    ISG_TRY(check_replica_only(m, replica));
+    if (!s) return fail(ISING_ERR_ARG, "spins array is NULL");
+    DeviceGuard g(m->device);
+    Xfer* x;
+    ISG_TRY(xfer_state(m, &x));
+    const int64_t N = m->lat.natoms;
+    if (!x->stage[replica]) ISG_TRY(dev_alloc(&x->stage[replica], (size_t)3 * N));
+    // after the work already issued on the mesh's stream and any download of this replica
+    // (which reads the same staging buffer and may fill the host array read here)
+    ISG_CUDA(cudaEventRecord(x->main_ready, m->stream));
+    ISG_CUDA(cudaStreamWaitEvent(x->h2d, x->main_ready, 0));
+    ISG_CUDA(cudaStreamWaitEvent(x->h2d, x->got[replica], 0));
+    x->pending = true;
+    ISG_CUDA(cudaMemcpyAsync(x->stage[replica], s, (size_t)3 * N * sizeof(double), cudaMemcpyHostToDevice, x->h2d));
+    ISG_TRY(launch_spins_from_f64(x->stage[replica], m->d_spins + (int64_t)replica * 3 * N, N, m->layout, m->d_status,
+                                  x->h2d));
+    ISG_CUDA(cudaEventRecord(x->put[replica], x->h2d));
+    return ISING_OK;
+}
+
+extern "C" int ising_spins_wait(ising_mesh* m) {
+    if (!m) return fail(ISING_ERR_ARG, "mesh is NULL");
+    return mesh_settle(m);
 }
 
 extern "C" int ising_spins_init_uniform(ising_mesh* m, uint64_t seed, uint32_t ensemble) {
@@ -872,6 +990,7 @@ void pt_free(ising_pt* pt) {
 
 int pt_resync_enqueue(ising_pt* pt) {
     ising_mesh* m = pt->mesh;
+    ISG_TRY(mesh_settle(m));
     ISG_TRY(enqueue_energy(m, pt->p, 0, pt->n, pt->d_energy_out, pt->d_energy_tmp));
     ISG_CUDA(cudaMemcpyAsync(pt->d_acc, pt->d_energy_out, (size_t)pt->n * 4 * sizeof(double),
                              cudaMemcpyDeviceToDevice, m->stream));
@@ -882,6 +1001,7 @@ int pt_resync_enqueue(ising_pt* pt) {
 // fold the per-block partial sums into the FP64 accumulators, exchange, advance counters.
 int pt_enqueue_round(ising_pt* pt, int k) {
     ising_mesh* m = pt->mesh;
+    ISG_TRY(mesh_settle(m));
     const int n = pt->n;
     const int move = pt->opt.move;
     if (!pt->opt.record)
@@ -919,6 +1039,7 @@ extern "C" int ising_pt_create(ising_mesh* m, int n, const double* betas, const 
     if (!out) return fail(ISING_ERR_ARG, "out is NULL");
     *out = nullptr;
     if (!m || !betas || !opt) return fail(ISING_ERR_ARG, "NULL argument");
+    ISG_TRY(mesh_settle(m));
     ISG_TRY(check_replica(m, 0));
     ISG_TRY(validate_params(p));
     if (n < 1 || n > m->n_replicas) return fail(ISING_ERR_ARG, "n_temps must be in 1..n_replicas");
@@ -985,6 +1106,7 @@ extern "C" int ising_pt_run(ising_pt* pt, int k, int rounds) {
     if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
     if (k < 1 || rounds < 0) return fail(ISING_ERR_ARG, "sweeps_per_swap must be >= 1 and rounds >= 0");
     ising_mesh* m = pt->mesh;
+    ISG_TRY(mesh_settle(m));
     DeviceGuard g(m->device);
     if (pt->graph_k != k) {
         if (pt->graph) { cudaGraphExecDestroy(pt->graph); pt->graph = nullptr; }
@@ -1011,6 +1133,7 @@ extern "C" int ising_pt_relax(ising_pt* pt, int n_sweeps) {
     if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
     if (n_sweeps < 0) return fail(ISING_ERR_ARG, "n_sweeps must be >= 0");
     ising_mesh* m = pt->mesh;
+    ISG_TRY(mesh_settle(m));
     DeviceGuard g(m->device);
     ISG_TRY(enqueue_sweeps(m, pt->plan, 0, pt->n, pt->d_beta_rep, 0u, n_sweeps, pt->opt.seed, pt->opt.ensemble,
                            pt->opt.move, pt->opt.r, pt->d_partials));
@@ -1098,6 +1221,7 @@ namespace {
 
 int patch_setup(ising_pt* pt, int colour, int offx, int offy, int offz, int slots, PatchStep* P, int* n_slots) {
     ising_mesh* m = pt->mesh;
+    ISG_TRY(mesh_settle(m));
     const Lattice& L = m->lat;
     if (!pt->plan.sc || L.nsub != 1) return fail(ISING_ERR_UNSUPPORTED, "the patch move needs a simple-cubic mesh with shell-1 couplings");
     if (L.nx % 8 || L.ny % 8 || L.nz % 8) return fail(ISING_ERR_ARG, "the patch move needs nx, ny, nz divisible by 8");
@@ -1117,6 +1241,7 @@ int patch_setup(ising_pt* pt, int colour, int offx, int offy, int offz, int slot
 
 int patch_workspace(ising_pt* pt, int batch) {
     ising_mesh* m = pt->mesh;
+    ISG_TRY(mesh_settle(m));
     const int64_t windows = (int64_t)pt->n * (m->lat.nx / 8) * (m->lat.ny / 8) * (m->lat.nz / 8);
     if (pt->pw_batch >= batch && pt->pw_windows >= windows) return ISING_OK;
     cudaFree(pt->pw_win); cudaFree(pt->pw_winp); cudaFree(pt->pw_prop); cudaFree(pt->pw_lqf); cudaFree(pt->pw_dE);
@@ -1176,6 +1301,7 @@ extern "C" int ising_pt_patch_count(const ising_pt* pt, int slots, int64_t* n_wi
 extern "C" int ising_pt_patch_step(ising_pt* pt, ising_net* net, int colour, int offx, int offy, int offz, int slots) {
     if (!pt || !net) return fail(ISING_ERR_ARG, "NULL argument");
     ising_mesh* m = pt->mesh;
+    ISG_TRY(mesh_settle(m));
     if (net_device(net) != m->device) return fail(ISING_ERR_ARG, "network and mesh are on different devices");
     DeviceGuard g(m->device);
     PatchStep P;
@@ -1207,6 +1333,7 @@ extern "C" int ising_pt_patch_samples(ising_pt* pt, int colour, int offx, int of
     if (!pt || !d_windows || !d_targets) return fail(ISING_ERR_ARG, "NULL argument");
     if (n_local < 0) return fail(ISING_ERR_ARG, "n_local must be >= 0");
     ising_mesh* m = pt->mesh;
+    ISG_TRY(mesh_settle(m));
     DeviceGuard g(m->device);
     PatchStep P;
     int ns = 0;
@@ -1571,6 +1698,7 @@ int ens_check(ising_ensembles* s) {
 }
 
 int ens_run(ising_ensembles* s, int k, int rounds) {
+    for (auto& h : s->ens) ISG_TRY(mesh_settle(h.mesh));   // the engine's stream reads the meshes' spins
     ISG_TRY(ens_build_table(s, k));
     const int64_t tpr = (int64_t)s->table.size();
     const int max_r = (int)std::max<int64_t>(1, ((int64_t)1 << 31) / std::max<int64_t>(tpr, 1) - 1);
@@ -1846,6 +1974,7 @@ extern "C" int ising_ensembles_swap_stats(const ising_ensembles* s, int e, uint6
 extern "C" int ising_ensembles_resync(ising_ensembles* s) {
     if (!s) return fail(ISING_ERR_ARG, "engine is NULL");
     DeviceGuard g(s->device);
+    for (auto& h : s->ens) ISG_TRY(mesh_settle(h.mesh));
     ISG_TRY(ens_resync_enqueue(s));
     ISG_CUDA(cudaStreamSynchronize(s->stream));
     return ISING_OK;

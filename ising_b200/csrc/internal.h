@@ -107,11 +107,16 @@ struct ising_mesh {
     int* d_plaq = nullptr;               // winding plaquette offsets (4 x {dx,dy,sub})
     int sclx = 10, scly = 10;            // fine-grid scale factors (makeChainMesh defaults)
     void* sky = nullptr;                 // skyrmion-counting workspace, made on first use
+    void* xfer = nullptr;                // asynchronous spin transfers (streams, per-replica staging)
 };
 
 namespace isg {
 // Frees the skyrmion-counting workspace of a mesh (called by ising_mesh_destroy).
 void skyrmion_release(ising_mesh* m);
+// Waits for the mesh's asynchronous spin transfers (ising_spins_*_async) still in flight and
+// reports invalid uploaded spins; a no-op when none are.  Every entry point that reads or
+// writes a mesh's spins calls it first.
+int mesh_settle(const ising_mesh* m);
 }  // namespace isg
 
 namespace isg {

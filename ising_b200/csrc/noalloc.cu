@@ -59,6 +59,7 @@ extern "C" int ising_total_energy_noalloc(const ising_mesh* mc, int replica, con
     if (!e) return fail(ISING_ERR_ARG, "e is NULL");
     int st = check_params(p);
     if (st != ISING_OK) return st;
+    if ((st = mesh_settle(m)) != ISING_OK) return st;   // asynchronous spin transfers land first
     const int nb = energy_blocks_for(m->lat.natoms);
     if (nb > kNoAllocMaxBlocks)
         return fail(ISING_ERR_ARG, "replica too large: the allocation-free energy accepts at most 16777216 atoms "

@@ -529,7 +529,7 @@ int check_mesh(const ising_mesh* m, int replica, int z1) {
         return fail(ISING_ERR_ARG, "fine grid below 5 x 5 (Gaussian_filter_2d reads 5 cells back)");
     if ((int64_t)m->lat.ny * m->scly > 65535 || (int64_t)m->lat.nx * m->sclx * m->lat.ny * m->scly > (int64_t)1 << 31)
         return fail(ISING_ERR_ARG, "fine grid too large (y extent above 65535 or more than 2^31 cells)");
-    return ISING_OK;
+    return mesh_settle(m);   // asynchronous spin transfers land first
 }
 
 // slice z1 of one replica -> fine density in w->d_dens

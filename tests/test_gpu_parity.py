@@ -274,6 +274,74 @@ def test_error_paths(ib, cuda_ok):
     assert e.value.status == 3
 
 
+def test_async_spin_transfers(ib, cuda_ok):
+    """Queued downloads and uploads equal the synchronous ones; an upload after a download of
+    the same replica and host array waits for it; later calls wait for queued transfers;
+    invalid uploads are reported by the wait."""
+    import torch
+    L, R = 8, 3
+    pm = ib.ChainMesh.simple_cubic(L, n_replicas=R)
+    pm.init_uniform(11, 2)
+    N = pm.numAtoms
+    ref = [pm.get_spins(r).copy() for r in range(R)]
+    host = [torch.empty(3 * N, dtype=torch.float64, pin_memory=True) for _ in range(R)]
+    for r in range(R):
+        pm.get_spins_async(host[r].data_ptr(), r)
+    pm.wait_spins()
+    for r in range(R):
+        np.testing.assert_array_equal(host[r].numpy().reshape(3, N).T, ref[r])
+    # download and upload again from the same host arrays without a host wait: a round trip
+    new = _random_spins(N, 5)
+    pm.set_spins(new, 1)
+    for r in range(R):
+        pm.get_spins_async(host[r].data_ptr(), r)
+    for r in range(R):
+        pm.set_spins_async(host[r].data_ptr(), (r + 1) % R)     # rotate replicas r -> r+1
+    got = [pm.get_spins(r) for r in range(R)]                   # waits for the queued transfers
+    want = [ref[0], new, ref[2]]
+    for r in range(R):
+        np.testing.assert_array_equal(got[(r + 1) % R], want[r])
+    # an upload followed by a download of the same replica sees the upload
+    h2 = torch.from_numpy(np.ascontiguousarray(ref[2].T).reshape(-1)).pin_memory()
+    pm.set_spins_async(h2.data_ptr(), 0)
+    pm.get_spins_async(host[0].data_ptr(), 0)
+    pm.wait_spins()
+    np.testing.assert_array_equal(host[0].numpy().reshape(3, N).T, ref[2])
+    # an invalid upload is reported by the wait
+    bad = h2.clone().pin_memory()
+    bad[7] = float("nan")
+    pm.set_spins_async(bad.data_ptr(), 2)
+    with pytest.raises(ib.IsingError) as e:
+        pm.wait_spins()
+    assert e.value.status == 2
+
+
+def test_async_uploads_feed_the_engine(ib, cuda_ok):
+    """An engine run after queued uploads (no explicit wait) sweeps the uploaded spins: the
+    result equals the run after synchronous uploads."""
+    import torch
+    spec_p = ib.params(J=-1.0, Dz=0.5, B=0.2, dmi="bulk", include_Jp=False)
+    betas = 1.0 / ib.temperature_ladder(0.3, 1.5, 2)
+    out = []
+    for use_async in (False, True):
+        m = ib.ChainMesh.simple_cubic(8, n_replicas=2)
+        m.init_uniform(3, 9)
+        s = [_random_spins(m.numAtoms, 40 + r) for r in range(2)]
+        if use_async:
+            hs = [torch.from_numpy(np.ascontiguousarray(v.T).reshape(-1)).pin_memory() for v in s]
+            for r in range(2):
+                m.set_spins_async(hs[r].data_ptr(), r)
+        else:
+            for r in range(2):
+                m.set_spins(s[r], r)
+        eng = ib.Ensembles([(m, betas, spec_p, 9)], seed=21)
+        eng.run(2, 2)
+        out.append([m.get_spins(r) for r in range(2)])
+        eng.close()
+    for r in range(2):
+        np.testing.assert_array_equal(out[0][r], out[1][r])
+
+
 def test_empty_and_null_inputs(ib, cuda_ok):
     """Empty batches are no-ops; NULL buffers and out-of-range replicas are argument errors."""
     from ising_b200 import _lib
