@@ -470,9 +470,11 @@ def run_gpu(args, w):
     cpu = cpu_fast = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = host_cores()
-        rate, sample = cpu_reference_rate(w, 2, 1, threads, L_sample=min(max(L for L, _, _, _ in spec), 64))
+        # one replica of the workload's largest lattice (C3: L=128, about a second of CPU work)
+        L_cpu = max(L for L, _, _, _ in spec)
+        rate, sample = cpu_reference_rate(w, 2, 1, threads, L_sample=L_cpu)
         cpu = {"value": rate, "unit": "spin-updates/s", "cores": threads, "kind": "port", "sample": sample}
-        rate, sample = cpu_fast_rate(w, threads)
+        rate, sample = cpu_fast_rate(w, threads, L=L_cpu)
         cpu_fast = {"value": rate, "unit": "spin-updates/s", "cores": threads, "kind": "optimised port",
                     "sample": sample}
 
