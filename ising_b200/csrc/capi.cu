@@ -1900,6 +1900,8 @@ extern "C" int ising_ensembles_autotune(ising_ensembles* s, int k, int rounds_pe
         // replica groups of ~64 MB (one L2-resident group per round); slower so far, kept as a candidate
         cand.push_back({t, 8192, ISING_ENS_ORDER_GROUPS, 64000000, 0.0, ISING_ENS_LOADER_REGISTERS});
     }
+    if (max_lanes <= 64)      // two-warp blocks (8 per SM, the same 16 warps) with small tasks
+        for (int c : {2048, 4096}) cand.push_back({64, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_REGISTERS});
     if (ens_staged_fits(s))   // groups of 4, 8 and 16 x-planes per task at nz = 128
         for (int c : {16384, 32768, 65536}) cand.push_back({256, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_STAGED});
     cudaEvent_t e0, e1;
