@@ -335,7 +335,8 @@ def run_gpu(args, w):
         if args.schedule:   # threads,chunk_pairs,loader: a fixed schedule instead of the autotuner
             bt, cp, ld = (int(v) for v in args.schedule.split(","))
             eng.set_schedule(block_threads=bt, chunk_pairs=cp, loader=ld)
-        trials = eng.autotune(k, 2) if not (args.no_autotune or args.schedule) else []
+        # 4 rounds per candidate: near-tied schedules are told apart by more than timer noise
+        trials = eng.autotune(k, 4) if not (args.no_autotune or args.schedule) else []
         eng.run(k, max(args.warmup, 1))
         run = lambda n: eng.run(k, n)
         energies = lambda: [eng.energies(i) for i in range(len(members))]
