@@ -114,7 +114,8 @@ int ising_spins_get(const ising_mesh* mesh, int replica, double* col_major_n3);
  * The host array must stay valid, and unmodified by the host, until ising_spins_wait returns;
  * use pinned memory for overlap.  ising_spins_wait waits for every queued transfer and reports
  * invalid uploaded spins (ISING_ERR_NAN); every other call on the mesh, or on a PT object or
- * engine using it, waits for them first. */
+ * engine using it, waits for them first.  The first queued transfer of a replica allocates a
+ * device staging buffer of 24 bytes per site for it, kept until the mesh is destroyed. */
 int ising_spins_get_async(ising_mesh* mesh, int replica, double* col_major_n3);
 int ising_spins_set_async(ising_mesh* mesh, int replica, const double* col_major_n3);
 int ising_spins_wait(ising_mesh* mesh);
