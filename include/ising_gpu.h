@@ -314,6 +314,9 @@ typedef struct {
 #define ISING_ENS_ORDER_PHASE 0   /* queue by colour pass: every ensemble's pass p, then p+1 */
 #define ISING_ENS_ORDER_GROUPS 1  /* replica groups of ~group_bytes run a whole round in turn
                                      (the group's spins stay resident in L2) */
+#define ISING_ENS_ORDER_WAVE 2    /* colour passes as a wavefront: pass p visits chunk
+                                     (p + i) mod nch at step 3p + i, so consecutive passes
+                                     follow each other through the lattice */
 
 typedef struct {
     uint64_t seed;

@@ -67,7 +67,7 @@ class EnsSchedule(C.Structure):
                 ("group_bytes", C.c_int64), ("ms_per_round", C.c_double), ("loader", C.c_int)]
 
 
-ENS_ORDER_PHASE, ENS_ORDER_GROUPS = 0, 1
+ENS_ORDER_PHASE, ENS_ORDER_GROUPS, ENS_ORDER_WAVE = 0, 1, 2
 ENS_LOADER_REGISTERS, ENS_LOADER_STAGED = 0, 1
 
 _P = C.POINTER

@@ -583,6 +583,9 @@ class ParallelTempering:
         return out[:, : n.value, :]
 
 
+_ORDER_NAMES = {0: "phase", 1: "groups", 2: "wave"}
+
+
 class Ensembles:
     """Many PT ensembles (parameter slots of src/PT.f90:147-176) advanced together by one
     persistent kernel per launch.  `members` is a sequence of (mesh, betas, params,
@@ -637,7 +640,7 @@ class Ensembles:
         c, g, t = EnsSchedule(), C.c_int(), C.c_int64()
         _lib.call("ising_ensembles_get_schedule", self._h, C.byref(c), C.byref(g), C.byref(t))
         return {"block_threads": c.block_threads, "chunk_pairs": c.chunk_pairs,
-                "order": "groups" if c.order == ENS_ORDER_GROUPS else "phase", "group_bytes": c.group_bytes,
+                "order": _ORDER_NAMES.get(c.order, str(c.order)), "group_bytes": c.group_bytes,
                 "loader": "staged" if c.loader == 1 else "registers",
                 "ms_per_round": c.ms_per_round, "grid_blocks": g.value, "tasks_per_pass": t.value}
 
@@ -647,7 +650,7 @@ class Ensembles:
         n = C.c_int()
         _lib.call("ising_ensembles_autotune", self._h, sweeps_per_swap, rounds_per_trial, trials, 64, C.byref(n))
         return [{"block_threads": t.block_threads, "chunk_pairs": t.chunk_pairs,
-                 "order": "groups" if t.order == ENS_ORDER_GROUPS else "phase", "group_bytes": t.group_bytes,
+                 "order": _ORDER_NAMES.get(t.order, str(t.order)), "group_bytes": t.group_bytes,
                  "loader": "staged" if t.loader == 1 else "registers",
                  "ms_per_round": t.ms_per_round} for t in trials[: n.value]]
 

@@ -1484,8 +1484,8 @@ int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) 
     if (c.block_threads < 64 || c.block_threads > kEnsMaxThreads || c.block_threads % 32)
         return fail(ISING_ERR_ARG, "block_threads must be 64..256 in whole warps");
     if (c.chunk_pairs < 1) return fail(ISING_ERR_ARG, "chunk_pairs must be >= 1");
-    if (c.order != ISING_ENS_ORDER_PHASE && c.order != ISING_ENS_ORDER_GROUPS)
-        return fail(ISING_ERR_ARG, "order must be ISING_ENS_ORDER_PHASE or ISING_ENS_ORDER_GROUPS");
+    if (c.order != ISING_ENS_ORDER_PHASE && c.order != ISING_ENS_ORDER_GROUPS && c.order != ISING_ENS_ORDER_WAVE)
+        return fail(ISING_ERR_ARG, "order must be ISING_ENS_ORDER_PHASE, _GROUPS or _WAVE");
     if (c.order == ISING_ENS_ORDER_GROUPS && c.group_bytes < 1) return fail(ISING_ERR_ARG, "group_bytes must be >= 1");
     if (c.loader != ISING_ENS_LOADER_REGISTERS && c.loader != ISING_ENS_LOADER_STAGED)
         return fail(ISING_ERR_ARG, "loader must be ISING_ENS_LOADER_REGISTERS or ISING_ENS_LOADER_STAGED");
@@ -1567,14 +1567,35 @@ int ens_build_table(ising_ensembles* s, int k) {
         groups.push_back({b, units.size()});
     }
     s->table.clear();
-    for (const auto& g : groups)
-        for (int ph = 0; ph < 2 * k; ++ph)
-            for (size_t u = g.first; u < g.second; ++u) {
-                const EnsHost& h = s->ens[units[u].e];
-                for (uint32_t ch = 0; ch < h.nch; ++ch)
-                    s->table.push_back(make_uint2(((uint32_t)units[u].e << 24) | (uint32_t)units[u].r,
-                                                  ((uint32_t)ph << 16) | ch));
-            }
+    if (s->sched.order == ISING_ENS_ORDER_WAVE) {
+        // wave key 3 ph + ((ch - ph) mod nch): each task's dependencies (the previous pass on
+        // chunks ch-1, ch, ch+1, cyclic) have strictly smaller keys, so ordering by key (ties
+        // by replica, then chunk) keeps every task after the tasks it waits for
+        struct Keyed { uint64_t key; uint2 task; };
+        std::vector<Keyed> all;
+        for (size_t u = 0; u < units.size(); ++u) {
+            const EnsHost& h = s->ens[units[u].e];
+            for (int ph = 0; ph < 2 * k; ++ph)
+                for (uint32_t ch = 0; ch < h.nch; ++ch) {
+                    const uint64_t w = 3ull * (uint64_t)ph + (uint64_t)((ch + h.nch - (uint32_t)ph % h.nch) % h.nch);
+                    all.push_back({(w << 40) | ((uint64_t)u << 16) | ch,
+                                   make_uint2(((uint32_t)units[u].e << 24) | (uint32_t)units[u].r,
+                                              ((uint32_t)ph << 16) | ch)});
+                }
+        }
+        std::sort(all.begin(), all.end(), [](const Keyed& a, const Keyed& b) { return a.key < b.key; });
+        s->table.reserve(all.size());
+        for (const auto& t : all) s->table.push_back(t.task);
+    } else {
+        for (const auto& g : groups)
+            for (int ph = 0; ph < 2 * k; ++ph)
+                for (size_t u = g.first; u < g.second; ++u) {
+                    const EnsHost& h = s->ens[units[u].e];
+                    for (uint32_t ch = 0; ch < h.nch; ++ch)
+                        s->table.push_back(make_uint2(((uint32_t)units[u].e << 24) | (uint32_t)units[u].r,
+                                                      ((uint32_t)ph << 16) | ch));
+                }
+    }
     if (s->table.size() >= (1u << 30)) return fail(ISING_ERR_ARG, "task table too large");
     ISG_CUDA(cudaStreamSynchronize(s->stream));
     if (s->table.size() > s->table_cap) {
