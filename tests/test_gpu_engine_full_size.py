@@ -90,3 +90,36 @@ def test_engine_equals_pt_path_at_c4_size(ib, cuda_ok):
                                           err_msg=f"ensemble {i} replica {r}")
         pt.close()
     eng.close()
+
+
+@pytest.mark.parametrize("sched", [dict(block_threads=128, chunk_pairs=8192, loader=0),
+                                   dict(block_threads=256, chunk_pairs=16384, loader=1)],
+                         ids=["registers", "staged"])
+def test_engine_long_run_at_c3_size(ib, cuda_ok, sched):
+    """300 rounds (3000 sweeps) of the C3 workload in 3 launches: no wait gives up, the spins
+    stay unit vectors, every slice charge stays an integer, and the running accumulators,
+    summed from 3000 sweeps of FP32 dE, stay within 1e-6 per site of recomputed energies."""
+    pp = ib.params(J=-1.0, Dz=0.7, B=0.3, K=0.05, dmi="bulk", include_Jp=False)
+    betas = 1.0 / ib.temperature_ladder(0.1, 1.5, R)
+    m = ib.ChainMesh.simple_cubic(L, n_replicas=R)
+    m.init_uniform(SEED, 0)
+    eng = ib.Ensembles([(m, betas, pp, 0)], seed=SEED)
+    eng.set_schedule(**sched)
+    for _ in range(3):
+        eng.run(K_SWEEPS, 100)
+    N = m.numAtoms
+    for r in (0, R // 2, R - 1):
+        s = m.get_spins(r)
+        assert np.max(np.abs(np.linalg.norm(s, axis=1) - 1.0)) < 1e-6
+        q = ib.winding_all_slices(m, r)
+        assert np.allclose(q, np.round(q), atol=1e-6)
+    perm = eng.permutation(0)
+    assert sorted(perm) == list(range(R))
+    e_run, m_run = eng.energies(0)
+    eng.resync()
+    e_new, m_new = eng.energies(0)
+    assert np.max(np.abs(e_run - e_new)) / N < 1e-6
+    assert np.max(np.abs(m_run - m_new)) / N < 1e-6
+    att, acc = eng.swap_stats(0)
+    assert np.all(att > 0) and np.all(acc <= att)
+    eng.close()
