@@ -114,7 +114,10 @@ class ClockSampler:
         self.proc = None
         self.kind = None
         self.t0 = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # the raw samples (the line carries their summary): $BENCH_CLOCKS_DIR or the temp dir
+        import tempfile
+        self.path = os.path.join(os.environ.get("BENCH_CLOCKS_DIR") or tempfile.gettempdir(),
+                                 f"ising_bench_clocks_{os.getpid()}.csv")
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
