@@ -284,6 +284,45 @@ def run_reference(args, w):
 
 
 # ---------------------------------------------------------------- GPU arm
+def link_rates(torch, host, stream):
+    """Host<->device copy rates over the given pinned host arrays (lists of 1-D FP64 tensors):
+    all of them to the device, all back, and both directions at once on two streams."""
+    flat = [t for hs in host for t in hs]
+    dev = [torch.empty_like(t, device="cuda") for t in flat]
+    nbytes = sum(t.numel() * 8 for t in flat)
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(fn):
+        best = float("inf")
+        for _ in range(3):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            for st in (up, down):
+                stream.wait_stream(st)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+    def h2d():
+        with torch.cuda.stream(up):
+            for d, h in zip(dev, flat):
+                d.copy_(h, non_blocking=True)
+
+    def d2h():
+        with torch.cuda.stream(down):
+            for d, h in zip(dev, flat):
+                h.copy_(d, non_blocking=True)
+
+    t_up, t_down = timed(h2d), timed(d2h)
+    t_both = timed(lambda: (h2d(), d2h()))
+    del dev
+    return {"h2d_gbs": nbytes / t_up / 1e6, "d2h_gbs": nbytes / t_down / 1e6,
+            "bidir_gbs_each": nbytes / t_both / 1e6, "bidir_ms": t_both}
+
+
 def ensembles_of(args, w):
     """[(L, replicas, D, B)] of the workload."""
     if "ensembles" in w:
@@ -470,6 +509,14 @@ def run_gpu(args, w):
                "steps": e2e_steps,
                "path": "ising_spins_set_async per replica -> one round -> ising_spins_get_async per replica "
                        "+ energies; ising_spins_wait at the end"}
+        # the link's own rates on the same pinned arrays (one bulk copy per direction, device
+        # buffers of the same size): the floor of a step that does not overlap the round with
+        # the copies is (both directions at once) + (the round)
+        link = link_rates(torch, host, stream)
+        floor_ms = link["bidir_ms"] + ms / args.steps
+        e2e["link"] = {k: v for k, v in link.items() if k != "bidir_ms"}
+        e2e["floor_ms_per_step"] = floor_ms
+        e2e["frac_of_floor"] = floor_ms / (e_ms / e2e_steps)
 
     cpu = cpu_fast = None
     if rank == 0 and world == 1 and not args.no_cpu:
