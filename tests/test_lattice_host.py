@@ -37,6 +37,34 @@ def test_lattice_tables_match_oracle(oracle, ib, name, kind, dims):
     assert np.allclose(pm.a_vec, v[0]) and np.allclose(pm.b_vec, v[1]) and np.allclose(pm.c_vec, v[2])
 
 
+def _random_cases(n=12, seed=20261204):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        kind = ["SC", "BCC", "HK"][i % 3]
+        hi = 5 if kind == "HK" else 8            # the hyper-kagome cell holds 12 atoms
+        dims = tuple(int(v) for v in rng.integers(3, hi, size=3))
+        shells = int(rng.integers(1, 3))
+        out.append((f"{kind.lower()}_{dims[0]}{dims[1]}{dims[2]}_s{shells}", kind, dims, shells))
+    return out
+
+
+@pytest.mark.parametrize("name,kind,dims,shells", _random_cases(), ids=[c[0] for c in _random_cases()])
+def test_lattice_tables_match_oracle_on_random_shapes(oracle, ib, name, kind, dims, shells):
+    """Seeded random shapes (3-7 cells per side, odd and even, non-cubic) and shell counts:
+    the same element-by-element comparison as above."""
+    frac, (a, b, c, ab, bc, ca) = _cell(oracle, kind)
+    om = oracle.Mesh(frac, *dims, a, b, c, ab, bc, ca, n_shells=shells)
+    pm = ib.ChainMesh(*dims, frac, a, b, c, ab, bc, ca, numShells=shells, device=-1)
+    assert pm.numAtoms == om.natoms
+    assert np.array_equal(pm.positions(), om.positions())
+    for atom in range(om.natoms):
+        for s in range(shells):
+            assert np.array_equal(pm.neighbours(atom, s), om.shell(atom, s)), (atom, s)
+        assert np.array_equal(pm.neighbours(atom, -1), om.neighbor_list(atom)), atom
+    assert np.array_equal(pm.derivative_list(), om.derivative_table())
+
+
 def test_non_orthogonal_cell_sets(oracle, ib):
     # monoclinic cell with an inexact lattice constant: neighbour SETS must agree
     frac = np.array([[0.0, 0.0, 0.0], [0.5, 0.5, 0.0]], np.float32)
