@@ -91,6 +91,46 @@ def test_total_energy_parity(oracle, ib, cuda_ok, kind, dims):
         assert np.allclose(m[0], s.sum(axis=0), atol=1e-9 * om.natoms)
 
 
+def _random_energy_cases(n=8, seed=4242):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        kind = ["SC", "BCC", "HK", "SC"][i % 4]
+        hi = 5 if kind == "HK" else 8
+        dims = tuple(int(v) for v in rng.integers(3, hi, size=3))
+        ax = rng.normal(size=3)
+        ax /= np.linalg.norm(ax)
+        h = dict(J=float(rng.choice([-1.0, 1.0]) * rng.uniform(0.5, 1.5)), Jp=float(rng.uniform(-0.3, 0.3)),
+                 Dz=float(rng.uniform(0.0, 1.0)), B=float(rng.uniform(-0.5, 0.5)), K=float(rng.uniform(0.0, 0.2)),
+                 Kax=tuple(float(v) for v in ax), bulk=bool(i % 2))
+        out.append((kind, dims, h))
+    return out
+
+
+@pytest.mark.parametrize("case", range(8))
+def test_energy_parity_on_random_shapes_and_hamiltonians(oracle, ib, cuda_ok, case):
+    """Seeded random meshes (SC, BCC, hyper-kagome; 3-7 cells per side, odd sizes taking the
+    general-colouring path) and random Hamiltonians: per-site energies of 200 random proposals
+    and the canonical total energy equal the oracle's within 1e-6 of the energy scale."""
+    kind, dims, h = _random_energy_cases()[case]
+    om, pm = _pair(oracle, ib, kind, dims)
+    s = _random_spins(om.natoms, 100 + case)
+    om.set_spins(s)
+    pm.set_spins(s)
+    op, pp = _both_params(oracle, ib, **h)
+    rng = np.random.default_rng(case)
+    atoms = rng.choice(om.natoms, size=min(om.natoms, 200), replace=False)
+    sp = _random_spins(len(atoms), 300 + case)
+    go, gn = ib.local_energy_batch(pm, atoms, sp, pp)
+    z1, z2 = len(om.shell(0, 0)), len(om.shell(0, 1))
+    scale = abs(h["J"]) * z1 + h["Dz"] * z1 + abs(h["Jp"]) * z2 + abs(h["B"]) + h["K"]
+    for k, a in enumerate(atoms):
+        o, n = om.local_energy(int(a), op, sp[k])
+        assert abs(go[k] - o) <= 1e-6 * scale and abs(gn[k] - n) <= 1e-6 * scale, (a, go[k], o, gn[k], n)
+    e, _m = ib.observables(pm, pp)
+    assert abs(e[0] - om.canonical_energy(op)) <= 1e-6 * om.natoms * scale
+
+
 def test_init_uniform_matches_oracle(oracle, ib, cuda_ok):
     om, pm = _pair(oracle, ib, "SC", (6, 6, 6), n_replicas=3)
     pm.init_uniform(0x15196, ensemble=5)
