@@ -237,6 +237,26 @@ REPLAYS = [("SC", (8, 8, 8), dict(J=-1.0, Dz=0.3, B=0.1, bulk=True), 0, 0.0, 1.5
            ("HK", (3, 3, 3), dict(J=-1.0, Dz=0.3, B=0.1, bulk=False), 1, 0.2, 1.0)]
 
 
+def _random_replays(n=6, seed=777):
+    """Seeded random replay cases: cell, shape (odd sizes take the general colouring),
+    Hamiltonian, move, ball radius and beta."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        kind = ["SC", "BCC", "SC", "HK", "SC", "BCC"][i]
+        hi = 5 if kind == "HK" else 9
+        dims = tuple(int(v) for v in rng.integers(3, hi, size=3))
+        h = dict(J=-float(rng.uniform(0.5, 1.5)), Jp=float(rng.uniform(0.0, 0.2)) if i % 3 == 0 else 0.0,
+                 Dz=float(rng.uniform(0.1, 0.8)), B=float(rng.uniform(0.0, 0.4)), K=float(rng.uniform(0.0, 0.1)),
+                 bulk=bool(i % 2))
+        move = int(i % 2)
+        out.append((kind, dims, h, move, 0.25 if move else 0.0, float(rng.uniform(0.5, 3.0))))
+    return out
+
+
+REPLAYS = REPLAYS + _random_replays()
+
+
 @pytest.mark.parametrize("case", range(len(REPLAYS)))
 def test_sweep_replay(oracle, ib, cuda_ok, case):
     """One GPU sweep against the oracle's colour passes with the same Philox keys and the
