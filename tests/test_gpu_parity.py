@@ -376,6 +376,50 @@ def test_async_spin_transfers(ib, cuda_ok):
     assert e.value.status == 2
 
 
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_async_transfers_follow_program_order_per_replica(ib, cuda_ok, seed):
+    """Random sequences of queued downloads and uploads (one pinned host array per replica),
+    waits, host edits after a wait and synchronous reads leave the device spins and every
+    host array exactly as executing the calls one by one would."""
+    import torch
+    R, L = 4, 8
+    pm = ib.ChainMesh.simple_cubic(L, n_replicas=R)
+    pm.init_uniform(seed, 1)
+    N = pm.numAtoms
+    rng = np.random.default_rng(seed)
+    dev = [pm.get_spins(r).copy() for r in range(R)]                  # model of the device
+    host_t = [torch.zeros(3 * N, dtype=torch.float64).pin_memory() for _ in range(R)]
+    host = [np.zeros((N, 3)) for _ in range(R)]                        # model of the host arrays
+    view = lambda r: host_t[r].numpy().reshape(3, N).T
+    for r in range(R):                     # every host array starts as a copy of its replica
+        pm.get_spins_async(host_t[r].data_ptr(), r)
+        host[r] = dev[r].copy()
+    pm.wait_spins()
+    for _ in range(60):
+        op = rng.choice(["get", "set", "wait", "sync_get"], p=[0.4, 0.35, 0.15, 0.1])
+        r = int(rng.integers(R))
+        if op == "get":
+            pm.get_spins_async(host_t[r].data_ptr(), r)
+            host[r] = dev[r].copy()
+        elif op == "set":
+            pm.set_spins_async(host_t[r].data_ptr(), r)
+            dev[r] = host[r].copy()
+        elif op == "wait":
+            pm.wait_spins()
+            for q in range(R):
+                np.testing.assert_array_equal(view(q), host[q])
+            q = int(rng.integers(R))                                  # the host edits an array
+            new = _random_spins(N, int(rng.integers(1 << 30)))
+            view(q)[:] = new
+            host[q] = new
+        else:
+            np.testing.assert_array_equal(pm.get_spins(r), dev[r])   # waits for the queue
+    pm.wait_spins()
+    for r in range(R):
+        np.testing.assert_array_equal(view(r), host[r])
+        np.testing.assert_array_equal(pm.get_spins(r), dev[r])
+
+
 def test_async_uploads_feed_the_engine(ib, cuda_ok):
     """An engine run after queued uploads (no explicit wait) sweeps the uploaded spins: the
     result equals the run after synchronous uploads."""
