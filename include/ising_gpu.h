@@ -331,10 +331,18 @@ typedef struct {
 #define ISING_ENS_LOADER_STAGED 1      /* rows staged in shared memory by TMA copies (every ensemble
                                           with nz = 128 and nx % 4 == 0; whole groups of 4 x-planes
                                           per task; 256-thread blocks) */
+#define ISING_ENS_LOADER_FUSED 2       /* both colour passes of a sweep in one pass over memory:
+                                          a task updates one sweep of a chunk of x-planes (one
+                                          thread row per plane plus a halo plane on either side;
+                                          block_threads 128..512 and >= nz) and a y-segment
+                                          (chunk_pairs / chunk width / (nz/4) rows), reading one
+                                          spin buffer and writing a second one the engine
+                                          allocates; sweeps_per_swap must be even.  Bit-identical
+                                          to the other loaders. */
 
 /* One schedule: block size, target site pairs per task, queue order, group size, loader. */
 typedef struct {
-    int block_threads;        /* 64..256, whole warps */
+    int block_threads;        /* 64..256 (fused loader 128..512), whole warps */
     int chunk_pairs;          /* site pairs of one colour per task (whole x-planes) */
     int order;                /* ISING_ENS_ORDER_* */
     int64_t group_bytes;      /* ISING_ENS_ORDER_GROUPS: spin bytes per replica group */
@@ -364,6 +372,11 @@ int ising_ensembles_energies(const ising_ensembles* s, int ensemble_index, doubl
 int ising_ensembles_swap_stats(const ising_ensembles* s, int ensemble_index, uint64_t* attempts,
                                uint64_t* accepts);
 int ising_ensembles_resync(ising_ensembles* s);
+/* Recompute every replica's FP64 energy and magnetisation accumulators from its spins after
+ * each `every` rounds of ising_ensembles_run, counted from this call (0: never); the option
+ * resync_every of ising_ensembles_create, re-armed.  No reference counterpart: the reference
+ * recomputes TotalHeisenbergEnergy at every exchange (src/PT.f90:251-254). */
+int ising_ensembles_set_resync(ising_ensembles* s, int every);
 /* Test hook for the bounded waits: in the next run, rounds >= 1 of ensemble_index wait for
  * a flag that nothing sets, so that run returns ISING_ERR_TIMEOUT after wait_timeout_ms;
  * the engine then resynchronises its accumulators and stays usable. */

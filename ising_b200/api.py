@@ -584,6 +584,7 @@ class ParallelTempering:
 
 
 _ORDER_NAMES = {0: "phase", 1: "groups", 2: "wave"}
+_LOADER_NAMES = {0: "registers", 1: "staged", 2: "fused"}
 
 
 class Ensembles:
@@ -632,7 +633,9 @@ class Ensembles:
     def set_schedule(self, block_threads: int = 256, chunk_pairs: int = 4096, order: int = ENS_ORDER_PHASE,
                      group_bytes: int = 48_000_000, loader: int = 0):
         """loader 0: neighbours loaded per thread; 1: rows staged in shared memory by TMA
-        (nz = 128 and nx % 4 == 0 in every ensemble, 256-thread blocks)."""
+        (nz = 128 and nx % 4 == 0 in every ensemble, 256-thread blocks); 2: both colour passes
+        of a sweep fused into one pass over ping-pong buffers (128..512-thread blocks of at
+        least nz threads; even sweeps_per_swap)."""
         c = EnsSchedule(block_threads, chunk_pairs, order, group_bytes, 0.0, loader)
         _lib.call("ising_ensembles_set_schedule", self._h, C.byref(c))
 
@@ -641,7 +644,7 @@ class Ensembles:
         _lib.call("ising_ensembles_get_schedule", self._h, C.byref(c), C.byref(g), C.byref(t))
         return {"block_threads": c.block_threads, "chunk_pairs": c.chunk_pairs,
                 "order": _ORDER_NAMES.get(c.order, str(c.order)), "group_bytes": c.group_bytes,
-                "loader": "staged" if c.loader == 1 else "registers",
+                "loader": _LOADER_NAMES.get(c.loader, str(c.loader)),
                 "ms_per_round": c.ms_per_round, "grid_blocks": g.value, "tasks_per_pass": t.value}
 
     def autotune(self, sweeps_per_swap: int, rounds_per_trial: int = 1):
@@ -651,7 +654,7 @@ class Ensembles:
         _lib.call("ising_ensembles_autotune", self._h, sweeps_per_swap, rounds_per_trial, trials, 64, C.byref(n))
         return [{"block_threads": t.block_threads, "chunk_pairs": t.chunk_pairs,
                  "order": _ORDER_NAMES.get(t.order, str(t.order)), "group_bytes": t.group_bytes,
-                 "loader": "staged" if t.loader == 1 else "registers",
+                 "loader": _LOADER_NAMES.get(t.loader, str(t.loader)),
                  "ms_per_round": t.ms_per_round} for t in trials[: n.value]]
 
     def permutation(self, e: int) -> np.ndarray:
@@ -675,6 +678,11 @@ class Ensembles:
 
     def resync(self):
         _lib.call("ising_ensembles_resync", self._h)
+
+    def set_resync(self, every: int):
+        """FP64 recomputation of the accumulators after each `every` rounds of run(),
+        counted from this call (0: never)."""
+        _lib.call("ising_ensembles_set_resync", self._h, every)
 
     def inject_stall(self, e: int):
         """Test hook: the next run's rounds >= 1 of ensemble e wait for a flag nothing sets."""

@@ -1411,8 +1411,10 @@ struct EnsHost {
     uint32_t* d_round = nullptr;
     double* d_energy_tmp = nullptr;
     double* d_energy_out = nullptr;
-    uint32_t P = 1, nch = 1;        // x-planes per chunk, chunks per replica
+    uint32_t P = 1, nch = 1;        // x-planes per chunk, tasks per replica and colour pass (sweep when fused)
     size_t part_off = 0, done_off = 0;
+    float* d_spins_b = nullptr;     // fused loader: second spin buffer of replicas 0..n-1
+    uint32_t fnch = 1, fnseg = 1, fnp = 0;   // fused loader: chunks, y-segments, thread rows per block
 };
 
 // sync words, zeroed before every launch: head, abort, where, (pad), ready[kMaxEnsembles],
@@ -1433,6 +1435,7 @@ struct ising_ensembles {
     bool has_k = false;
     ising_ensembles_schedule_t sched{256, 4096, ISING_ENS_ORDER_PHASE, 48000000, 0.0};
     int grid = 0;
+    size_t fu_smem = 0;             // fused loader: dynamic shared memory per block
     std::vector<uint2> table;
     int table_k = -1;
     uint2* d_table = nullptr;
@@ -1456,6 +1459,7 @@ void ens_free(ising_ensembles* s) {
     for (auto& h : s->ens) {
         cudaFree(h.d_beta_t); cudaFree(h.d_beta_rep); cudaFree(h.d_t2r); cudaFree(h.d_r2t); cudaFree(h.d_acc);
         cudaFree(h.d_stats); cudaFree(h.d_round); cudaFree(h.d_energy_tmp); cudaFree(h.d_energy_out);
+        cudaFree(h.d_spins_b);
     }
     cudaFree(s->d_table); cudaFree(s->d_partials); cudaFree(s->d_sync); cudaFree(s->d_status);
     if (s->h_words) cudaFreeHost(s->h_words);
@@ -1481,22 +1485,53 @@ bool ens_staged_fits(const ising_ensembles* s) {
 
 // Chunking, grid and buffers for schedule `c`.
 int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) {
-    if (c.block_threads < 64 || c.block_threads > kEnsMaxThreads || c.block_threads % 32)
+    const bool fused = c.loader == ISING_ENS_LOADER_FUSED;
+    if (fused) {
+        if (c.block_threads < 128 || c.block_threads > kFuMaxThreads || c.block_threads % 32)
+            return fail(ISING_ERR_ARG, "the fused loader runs 128..512-thread blocks in whole warps");
+    } else if (c.block_threads < 64 || c.block_threads > kEnsMaxThreads || c.block_threads % 32) {
         return fail(ISING_ERR_ARG, "block_threads must be 64..256 in whole warps");
+    }
     if (c.chunk_pairs < 1) return fail(ISING_ERR_ARG, "chunk_pairs must be >= 1");
     if (c.order != ISING_ENS_ORDER_PHASE && c.order != ISING_ENS_ORDER_GROUPS && c.order != ISING_ENS_ORDER_WAVE)
         return fail(ISING_ERR_ARG, "order must be ISING_ENS_ORDER_PHASE, _GROUPS or _WAVE");
     if (c.order == ISING_ENS_ORDER_GROUPS && c.group_bytes < 1) return fail(ISING_ERR_ARG, "group_bytes must be >= 1");
-    if (c.loader != ISING_ENS_LOADER_REGISTERS && c.loader != ISING_ENS_LOADER_STAGED)
-        return fail(ISING_ERR_ARG, "loader must be ISING_ENS_LOADER_REGISTERS or ISING_ENS_LOADER_STAGED");
+    if (c.loader != ISING_ENS_LOADER_REGISTERS && c.loader != ISING_ENS_LOADER_STAGED && !fused)
+        return fail(ISING_ERR_ARG, "loader must be ISING_ENS_LOADER_REGISTERS, _STAGED or _FUSED");
+    if (fused && c.order != ISING_ENS_ORDER_PHASE) return fail(ISING_ERR_ARG, "the fused loader queues in phase order");
     const bool staged = c.loader == ISING_ENS_LOADER_STAGED;
     if (staged) {
         if (c.block_threads != kStSub * kStG * 32) return fail(ISING_ERR_ARG, "the staged loader runs 256-thread blocks");
         if (!ens_staged_fits(s)) return fail(ISING_ERR_ARG, "the staged loader needs nz = 128 and nx % 4 == 0 in every ensemble");
     }
-    size_t part = 0, done = 0;
+    size_t part = 0, done = 0, fu_smem = 0;
     for (auto& h : s->ens) {
         const Lattice& L = h.mesh->lat;
+        if (fused) {
+            // one thread row per x-plane of a chunk plus two halo planes; chunks of at least
+            // two planes and y-segments of at least two rows keep every task's reads inside
+            // its 3 x 3 neighbourhood of units
+            const uint32_t G = (uint32_t)L.nz / 4u, rows = (uint32_t)c.block_threads / G;
+            if (rows < 4) return fail(ISING_ERR_ARG, "the fused loader needs block_threads >= nz of every ensemble");
+            const uint32_t pm = std::min<uint32_t>(rows - 2u, (uint32_t)L.nx);
+            const uint32_t nch = ((uint32_t)L.nx + pm - 1u) / pm;
+            const uint32_t widest = ((uint32_t)L.nx + nch - 1u) / nch;
+            const double yl = std::max(2.0, (double)c.chunk_pairs / ((double)widest * G));
+            long nseg = std::lround((double)L.ny / yl);
+            nseg = std::max(1L, std::min(nseg, (long)L.ny / 2));
+            if ((uint64_t)nch * (uint64_t)nseg >= 65536u) return fail(ISING_ERR_ARG, "too many fused units per replica");
+            h.fnch = nch;
+            h.fnseg = (uint32_t)nseg;
+            h.fnp = widest + 2u;
+            h.P = widest;
+            h.nch = nch * (uint32_t)nseg;
+            fu_smem = std::max(fu_smem, (size_t)(3u * (h.fnp + 2u) + 3u * h.fnp) * 3u * ((uint32_t)L.nz / 2u) * 4u);
+            h.part_off = part;
+            h.done_off = done;
+            part += (size_t)h.n * h.nch * 4;
+            done += (size_t)h.n * h.nch;
+            continue;
+        }
         const int lanes = L.nz / 4;   // W / 2
         if (lanes > c.block_threads) return fail(ISING_ERR_ARG, "block_threads smaller than nz / 4 of an ensemble");
         const double plane_pairs = (double)L.ny * lanes;
@@ -1510,12 +1545,18 @@ int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) 
         part += (size_t)h.n * h.nch * 4;
         done += (size_t)h.n * h.nch;
     }
+    if (fu_smem > 227u * 1024u) return fail(ISING_ERR_ARG, "fused loader: rows of the chunk exceed shared memory");
+    const int loader = fused ? 2 : (staged ? 1 : 0);
     int per_sm = 0;
-    ISG_TRY(ensembles_blocks_per_sm(s->move, s->dmi, s->has_k, staged, c.block_threads, &per_sm));
+    ISG_TRY(ensembles_blocks_per_sm(s->move, s->dmi, s->has_k, loader, c.block_threads, fu_smem, &per_sm));
     if (per_sm < 1) return fail(ISING_ERR_CUDA, "persistent engine kernel cannot be resident");
     int sms = 0;
     ISG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
     ISG_CUDA(cudaStreamSynchronize(s->stream));
+    if (fused)
+        for (auto& h : s->ens)
+            if (!h.d_spins_b) ISG_TRY(dev_alloc(&h.d_spins_b, (size_t)3 * (size_t)h.mesh->lat.natoms * (size_t)h.n));
+    s->fu_smem = fu_smem;
     if (part > s->partials_cap) {
         cudaFree(s->d_partials);
         s->d_partials = nullptr;
@@ -1567,7 +1608,17 @@ int ens_build_table(ising_ensembles* s, int k) {
         groups.push_back({b, units.size()});
     }
     s->table.clear();
-    if (s->sched.order == ISING_ENS_ORDER_WAVE) {
+    if (s->sched.loader == ISING_ENS_LOADER_FUSED) {
+        // one task per (replica, sweep, unit), sweep by sweep: a task only waits for the
+        // previous sweep
+        for (int sw = 0; sw < k; ++sw)
+            for (size_t u = 0; u < units.size(); ++u) {
+                const EnsHost& h = s->ens[units[u].e];
+                for (uint32_t ch = 0; ch < h.nch; ++ch)
+                    s->table.push_back(make_uint2(((uint32_t)units[u].e << 24) | (uint32_t)units[u].r,
+                                                  ((uint32_t)sw << 16) | ch));
+            }
+    } else if (s->sched.order == ISING_ENS_ORDER_WAVE) {
         // wave key 3 ph + ((ch - ph) mod nch): each task's dependencies (the previous pass on
         // chunks ch-1, ch, ch+1, cyclic) have strictly smaller keys, so ordering by key (ties
         // by replica, then chunk) keeps every task after the tasks it waits for
@@ -1640,6 +1691,12 @@ void ens_params(const ising_ensembles* s, int k, int rounds, int stall, EnsParam
             d.st_nseg = std::min<uint32_t>((uint32_t)L.ny, groups % 2 ? 2u : 1u);
             d.st_seg_len = ((uint32_t)L.ny + d.st_nseg - 1) / d.st_nseg;
         }
+        if (s->sched.loader == ISING_ENS_LOADER_FUSED) {
+            d.spins_b = h.d_spins_b;
+            d.fnch = h.fnch;
+            d.fnseg = h.fnseg;
+            d.fnp = h.fnp;
+        }
         d.n_rep = h.n;
         d.beta_rep = h.d_beta_rep;
         d.sweep_ctr = h.mesh->d_sweep;
@@ -1679,7 +1736,9 @@ int ens_enqueue_launch(ising_ensembles* s, int k, int rounds, int stall) {
                 return fail(ISING_ERR_CUDA, "cuTensorMapEncodeTiled (staged loader) failed");
         }
     ISG_CUDA(cudaMemsetAsync(s->d_sync, 0, s->sync_words * sizeof(uint32_t), s->stream));
-    return launch_ensembles(P, s->move, s->dmi, s->has_k, staged, s->sched.block_threads, s->grid, s->stream);
+    const int loader = s->sched.loader == ISING_ENS_LOADER_FUSED ? 2 : (staged ? 1 : 0);
+    return launch_ensembles(P, s->move, s->dmi, s->has_k, loader, s->sched.block_threads, s->grid, s->fu_smem,
+                            s->stream);
 }
 
 int ens_resync_enqueue(ising_ensembles* s) {
@@ -1719,6 +1778,9 @@ int ens_check(ising_ensembles* s) {
 }
 
 int ens_run(ising_ensembles* s, int k, int rounds) {
+    // the fused loader alternates two buffers sweep by sweep: an even round ends in the mesh's own
+    if (s->sched.loader == ISING_ENS_LOADER_FUSED && k % 2)
+        return fail(ISING_ERR_ARG, "the fused loader needs an even number of sweeps per round");
     for (auto& h : s->ens) ISG_TRY(mesh_settle(h.mesh));   // the engine's stream reads the meshes' spins
     ISG_TRY(ens_build_table(s, k));
     const int64_t tpr = (int64_t)s->table.size();
@@ -1928,6 +1990,11 @@ extern "C" int ising_ensembles_autotune(ising_ensembles* s, int k, int rounds_pe
         for (int c : {2048, 4096}) cand.push_back({64, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_REGISTERS});
     if (ens_staged_fits(s))   // groups of 4, 8 and 16 x-planes per task at nz = 128
         for (int c : {16384, 32768, 65536}) cand.push_back({256, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_STAGED});
+    if (k % 2 == 0)           // one pass per sweep: chunk widths by block size, y-segments by chunk_pairs
+        for (int t : {256, 384, 512})
+            if (t >= 4 * max_lanes)
+                for (int c : {16384, 65536, 1 << 30})
+                    cand.push_back({t, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_FUSED});
     cudaEvent_t e0, e1;
     ISG_CUDA(cudaEventCreate(&e0));
     ISG_CUDA(cudaEventCreate(&e1));
@@ -2003,6 +2070,14 @@ extern "C" int ising_ensembles_resync(ising_ensembles* s) {
     for (auto& h : s->ens) ISG_TRY(mesh_settle(h.mesh));
     ISG_TRY(ens_resync_enqueue(s));
     ISG_CUDA(cudaStreamSynchronize(s->stream));
+    return ISING_OK;
+}
+
+extern "C" int ising_ensembles_set_resync(ising_ensembles* s, int every) {
+    if (!s) return fail(ISING_ERR_ARG, "engine is NULL");
+    if (every < 0) return fail(ISING_ERR_ARG, "resync interval must be >= 0");
+    s->opt.resync_every = every;
+    s->rounds_done = 0;
     return ISING_OK;
 }
 

@@ -7,42 +7,48 @@
 
 namespace isg {
 
-static const void* ens_kernel(int move, int dmi, bool hk, bool staged) {
+static const void* ens_kernel(int move, int dmi, bool hk, int loader) {
     // kind 0 (no DMI) runs the bulk form with D = 0: h gains 0 * (...) terms only
     if (dmi == 0) dmi = 1;
-    return move == 0 ? ensembles_kernel_uniform(dmi, hk, staged) : ensembles_kernel_ball(dmi, hk, staged);
+    return move == 0 ? ensembles_kernel_uniform(dmi, hk, loader) : ensembles_kernel_ball(dmi, hk, loader);
 }
 
-// The staged kernels' shared-memory limit is a per-device attribute.  It is raised where a
-// schedule is applied (ensembles_blocks_per_sm, on the engine's device and outside any
-// stream capture), before the first launch of that schedule.
-static int ens_smem_attr(const void* fn, bool staged) {
-    if (staged) ISG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStSmemBytes));
+// Dynamic shared memory of a launch: the staged ring, or the fused kernel's row slots.
+static size_t ens_smem(int loader, size_t fused_smem) {
+    return loader == 1 ? (size_t)kStSmemBytes : (loader == 2 ? fused_smem : 0);
+}
+
+// The staged and fused kernels' shared-memory limit is a per-device attribute.  It is raised
+// where a schedule is applied (ensembles_blocks_per_sm, on the engine's device and outside
+// any stream capture), before the first launch of that schedule.
+static int ens_smem_attr(const void* fn, int loader, size_t smem) {
+    if (loader != 0) ISG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     return ISING_OK;
 }
 
-int ensembles_blocks_per_sm(int move, int dmi, bool has_k, bool staged, int threads, int* out) {
-    const void* fn = ens_kernel(move, dmi, has_k, staged);
-    const int st = ens_smem_attr(fn, staged);
+static int ens_threads(int loader, int threads) { return loader == 1 ? kStThreads : threads; }
+
+int ensembles_blocks_per_sm(int move, int dmi, bool has_k, int loader, int threads, size_t smem, int* out) {
+    const void* fn = ens_kernel(move, dmi, has_k, loader);
+    const size_t sb = ens_smem(loader, smem);
+    const int st = ens_smem_attr(fn, loader, sb);
     if (st != ISING_OK) return st;
     int n = 0;
-    ISG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, staged ? kStThreads : threads,
-                                                           staged ? (size_t)kStSmemBytes : 0));
+    ISG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, ens_threads(loader, threads), sb));
     *out = n;
     return ISING_OK;
 }
 
-int launch_ensembles(const EnsParams& P, int move, int dmi, bool has_k, bool staged, int threads, int grid,
-                     cudaStream_t s) {
-    if (threads < 32 || threads > kEnsMaxThreads || threads % 32)
-        return fail(ISING_ERR_ARG, "block size must be 32..256, whole warps");
-    if (staged && threads != kStSub * kStG * 32) return fail(ISING_ERR_ARG, "the staged loader runs 256-thread blocks");
+int launch_ensembles(const EnsParams& P, int move, int dmi, bool has_k, int loader, int threads, int grid,
+                     size_t smem, cudaStream_t s) {
+    const int maxt = loader == 2 ? kFuMaxThreads : kEnsMaxThreads;
+    if (threads < 32 || threads > maxt || threads % 32) return fail(ISING_ERR_ARG, "block size out of range for the loader");
+    if (loader == 1 && threads != kStSub * kStG * 32) return fail(ISING_ERR_ARG, "the staged loader runs 256-thread blocks");
     if (P.n_ens < 1 || P.n_ens > kMaxEnsembles) return fail(ISING_ERR_ARG, "1..16 ensembles per engine");
-    const void* fn = ens_kernel(move, dmi, has_k, staged);
+    const void* fn = ens_kernel(move, dmi, has_k, loader);
     void* args[] = {const_cast<EnsParams*>(&P)};
     // staged: the schedule's 256 compute threads plus the copy warp
-    ISG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(staged ? kStThreads : threads), args,
-                              staged ? (size_t)kStSmemBytes : 0, s));
+    ISG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(ens_threads(loader, threads)), args, ens_smem(loader, smem), s));
     return ISING_OK;
 }
 

@@ -30,6 +30,9 @@ struct EnsDev {
     uint32_t nseg, seg_len;      // y-segments per plane in a task, rows per segment
     FastDiv divSeg;              // by nseg
     uint32_t st_nseg, st_seg_len;   // staged loader: y-segments per group of kStG planes, rows per segment
+    float* spins_b;              // fused loader: the second spin buffer (same layout as spins)
+    uint32_t fnch, fnseg;        // fused loader: chunks of x-planes, y-segments (nch = fnch * fnseg units)
+    uint32_t fnp;                // fused loader: thread rows per block (widest chunk + 2 halo planes)
     int n_rep;                   // replicas 0..n_rep-1 (= temperature slots)
     double* beta_rep;
     uint32_t* sweep_ctr;         // the mesh's per-replica sweep counters
@@ -59,6 +62,10 @@ constexpr uint32_t kStOwnFloats = 3u * kStG * 64u;         // [3][kStG][64]
 constexpr uint32_t kStStageFloats = kStNxtFloats + kStOwnFloats;
 constexpr uint32_t kStSmemBytes = kStSub * kStStages * kStStageFloats * 4u + 2u * kStSub * kStStages * 8u + 128u;
 
+// Fused loader (schedule loader 2): one pass per sweep over ping-pong buffers, a block of up to
+// kFuMaxThreads threads holding one thread row per x-plane of a chunk plus two halo planes.
+constexpr int kFuMaxThreads = 512;
+
 // Tensor maps of one ensemble's spins, dims (entry, y, x, colour, 3 replica + component):
 // next = box {64, 1, kStG+2, 1, 3}, own = {64, 1, kStG, 1, 3}, ctr = {64, 1, kStG, 1, 1},
 // halo = {64, 1, 1, 1, 1} (ctr and halo serve plane groups whose x-halo wraps around).
@@ -86,13 +93,14 @@ struct EnsParams {
 };
 static_assert(sizeof(EnsParams) < 32000, "kernel parameter block too large");
 
-int launch_ensembles(const EnsParams& P, int move, int dmi, bool has_k, bool staged, int threads, int grid,
-                     cudaStream_t s);
+// loader: 0 registers, 1 staged, 2 fused (smem = dynamic shared memory of the fused kernel)
+int launch_ensembles(const EnsParams& P, int move, int dmi, bool has_k, int loader, int threads, int grid,
+                     size_t smem, cudaStream_t s);
 // kernel instantiations, one translation unit per move kind (dmi in 1..3: 1 bulk,
 // 2 interfacial about z, 3 tabulated per bond direction)
-const void* ensembles_kernel_uniform(int dmi, bool has_k, bool staged);
-const void* ensembles_kernel_ball(int dmi, bool has_k, bool staged);
-int ensembles_blocks_per_sm(int move, int dmi, bool has_k, bool staged, int threads, int* out);
+const void* ensembles_kernel_uniform(int dmi, bool has_k, int loader);
+const void* ensembles_kernel_ball(int dmi, bool has_k, int loader);
+int ensembles_blocks_per_sm(int move, int dmi, bool has_k, int loader, int threads, size_t smem, int* out);
 // the staged loader's tensor maps for one ensemble (spins of n_rep replicas of an
 // nx x ny x 128 colour-separated mesh); false if the driver refuses one
 bool ensembles_encode_maps(float* spins, int nx, int ny, int n_rep, EnsMaps* m);

@@ -112,16 +112,16 @@ __device__ __forceinline__ void propose2(const float2* s, uint4 ra, uint4 rb, fl
 
 // Update of one site pair from its loaded neighbourhood: own pair s at entries (j, j+1) of
 // packed row `row` (parity p), the other colour's pairs px, mx (x +- 1), py, my (y +- 1) and
-// oz (same row) at entries (j, j+1), and the edge entry (ex, ey, ez) of that row.  The pair
-// is written back at own_off when either site accepts.
+// oz (same row) at entries (j, j+1), and the edge entry (ex, ey, ez) of that row.  Returns
+// the pair after the Metropolis decisions (rejected sites bit-identical to s); `any` tells
+// whether either site accepted.  dE and dM of accepted moves are added to the running sums
+// when `count` is set (a recomputed halo pair is not counted).
 template <int MOVE, int DMI, bool HAS_K>
-__device__ __forceinline__ void pair_compute(const CbGeom& P, const uint32_t* rk, int* status,
-                                             float* __restrict__ sx, float* __restrict__ sy,
-                                             float* __restrict__ sz, uint32_t own_off, uint32_t row,
-                                             uint32_t j, uint32_t p, const v23& s, const v23& px, const v23& mx,
-                                             const v23& py, const v23& my, const v23& oz, float ex, float ey,
-                                             float ez, uint32_t sweep, uint32_t rep, float beta2,
-                                             v2& de, v2& dmx, v2& dmy, v2& dmz) {
+__device__ __forceinline__ v23 pair_new(const CbGeom& P, const uint32_t* rk, int* status, uint32_t row,
+                                        uint32_t j, uint32_t p, const v23& s, const v23& px, const v23& mx,
+                                        const v23& py, const v23& my, const v23& oz, float ex, float ey,
+                                        float ez, uint32_t sweep, uint32_t rep, float beta2, bool count,
+                                        v2& de, v2& dmx, v2& dmy, v2& dmz, bool& any) {
     const CbGeom& a = P;
     const HamDev& H = P.ham;
     v23 zp, zm;
@@ -186,20 +186,36 @@ __device__ __forceinline__ void pair_compute(const CbGeom& P, const uint32_t* rk
                       V(-0.99999994f));
     const bool acc0 = (dE.x <= 0.f) || (u3.x < ax_ex2(t.x));
     const bool acc1 = (dE.y <= 0.f) || (u3.y < ax_ex2(t.y));
-    const v2 m = make_float2(acc0 ? 1.f : 0.f, acc1 ? 1.f : 0.f);
-    de = fma2(m, dE, de);
-    dmx = fma2(m, d.x, dmx);
-    dmy = fma2(m, d.y, dmy);
-    dmz = fma2(m, d.z, dmz);
-    // S + m (S' - S) keeps rejected sites bit-identical (m = 0) and takes S' exactly (m = 1)
-    const v2 nx_ = make_float2(acc0 ? sp.x.x : s.x.x, acc1 ? sp.x.y : s.x.y);
-    const v2 ny_ = make_float2(acc0 ? sp.y.x : s.y.x, acc1 ? sp.y.y : s.y.y);
-    const v2 nz_ = make_float2(acc0 ? sp.z.x : s.z.x, acc1 ? sp.z.y : s.z.y);
-    if (acc0 | acc1) {
-        const uint32_t o = own_off;
-        *reinterpret_cast<v2*>(sx + o) = nx_;
-        *reinterpret_cast<v2*>(sy + o) = ny_;
-        *reinterpret_cast<v2*>(sz + o) = nz_;
+    if (count) {
+        const v2 m = make_float2(acc0 ? 1.f : 0.f, acc1 ? 1.f : 0.f);
+        de = fma2(m, dE, de);
+        dmx = fma2(m, d.x, dmx);
+        dmy = fma2(m, d.y, dmy);
+        dmz = fma2(m, d.z, dmz);
+    }
+    // rejected sites keep s bit for bit, accepted ones take S' exactly
+    any = acc0 | acc1;
+    return {make_float2(acc0 ? sp.x.x : s.x.x, acc1 ? sp.x.y : s.x.y),
+            make_float2(acc0 ? sp.y.x : s.y.x, acc1 ? sp.y.y : s.y.y),
+            make_float2(acc0 ? sp.z.x : s.z.x, acc1 ? sp.z.y : s.z.y)};
+}
+
+// pair_new, with the pair written back at own_off when either site accepts.
+template <int MOVE, int DMI, bool HAS_K>
+__device__ __forceinline__ void pair_compute(const CbGeom& P, const uint32_t* rk, int* status,
+                                             float* __restrict__ sx, float* __restrict__ sy,
+                                             float* __restrict__ sz, uint32_t own_off, uint32_t row,
+                                             uint32_t j, uint32_t p, const v23& s, const v23& px, const v23& mx,
+                                             const v23& py, const v23& my, const v23& oz, float ex, float ey,
+                                             float ez, uint32_t sweep, uint32_t rep, float beta2,
+                                             v2& de, v2& dmx, v2& dmy, v2& dmz) {
+    bool any;
+    const v23 n = pair_new<MOVE, DMI, HAS_K>(P, rk, status, row, j, p, s, px, mx, py, my, oz, ex, ey, ez, sweep,
+                                             rep, beta2, true, de, dmx, dmy, dmz, any);
+    if (any) {
+        *reinterpret_cast<v2*>(sx + own_off) = n.x;
+        *reinterpret_cast<v2*>(sy + own_off) = n.y;
+        *reinterpret_cast<v2*>(sz + own_off) = n.z;
     }
 }
 

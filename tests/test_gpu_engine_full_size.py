@@ -1,6 +1,6 @@
 """The persistent engine at the full C3 and C4 sizes.  C3 (SC L=128 x 16 PT replicas, bulk
 D=0.7, B=0.3, K=0.05, ball move r=0.2), on the schedules the autotuner chooses between: after
-3 rounds of 10 sweeps its spins, exchange permutation and swap counts are bit-equal to the
+3 rounds of 10 sweeps (every loader, the fused one with and without y-segments) its spins, exchange permutation and swap counts are bit-equal to the
 per-pass PT path (itself replayed against the oracle) from the same seed; the spins stay unit
 vectors, every z-slice's winding number is an integer, and the running FP64 accumulators
 agree with energies recomputed from the spins within 1e-6 per site.  C4 (12 uneven
@@ -15,8 +15,10 @@ L, R, K_SWEEPS, ROUNDS, SEED = 128, 16, 10, 3, 0x15196
 
 
 @pytest.mark.parametrize("sched", [dict(block_threads=128, chunk_pairs=8192, loader=0),
-                                   dict(block_threads=256, chunk_pairs=16384, loader=1)],
-                         ids=["registers", "staged"])
+                                   dict(block_threads=256, chunk_pairs=16384, loader=1),
+                                   dict(block_threads=512, chunk_pairs=1 << 30, loader=2),
+                                   dict(block_threads=256, chunk_pairs=16384, loader=2)],
+                         ids=["registers", "staged", "fused", "fused-segments"])
 def test_engine_equals_pt_path_at_c3_size(ib, cuda_ok, sched):
     pp = ib.params(J=-1.0, Dz=0.7, B=0.3, K=0.05, dmi="bulk", include_Jp=False)
     betas = 1.0 / ib.temperature_ladder(0.1, 1.5, R)
@@ -58,7 +60,10 @@ C4_R = {16: 16, 24: 16, 32: 32, 48: 32, 64: 48, 96: 64}
 C4_DB = [(0.3, 0.1), (0.3, 0.3), (0.5, 0.1), (0.5, 0.3), (0.7, 0.1), (0.7, 0.3)]
 
 
-def test_engine_equals_pt_path_at_c4_size(ib, cuda_ok):
+@pytest.mark.parametrize("sched", [dict(block_threads=128, chunk_pairs=32768, loader=0),
+                                   dict(block_threads=384, chunk_pairs=1 << 30, loader=2)],
+                         ids=["registers", "fused"])
+def test_engine_equals_pt_path_at_c4_size(ib, cuda_ok, sched):
     spec, refs, emeshes, rmeshes = [], [], [], []
     for i, L in enumerate(C4_L):
         n = C4_R[L]
@@ -74,7 +79,7 @@ def test_engine_equals_pt_path_at_c4_size(ib, cuda_ok):
         spec.append((em, betas, p, i))
         refs.append((rm, betas, p, i))
     eng = ib.Ensembles(spec, seed=SEED)
-    eng.set_schedule(block_threads=128, chunk_pairs=32768, loader=0)
+    eng.set_schedule(**sched)
     eng.run(K_SWEEPS, 2)
     for i, (rm, betas, p, ens) in enumerate(refs):
         pt = ib.ParallelTempering(rm, betas, p, seed=SEED, ensemble=ens)
@@ -93,8 +98,10 @@ def test_engine_equals_pt_path_at_c4_size(ib, cuda_ok):
 
 
 @pytest.mark.parametrize("sched", [dict(block_threads=128, chunk_pairs=8192, loader=0),
-                                   dict(block_threads=256, chunk_pairs=16384, loader=1)],
-                         ids=["registers", "staged"])
+                                   dict(block_threads=256, chunk_pairs=16384, loader=1),
+                                   dict(block_threads=512, chunk_pairs=1 << 30, loader=2),
+                                   dict(block_threads=256, chunk_pairs=16384, loader=2)],
+                         ids=["registers", "staged", "fused", "fused-segments"])
 def test_engine_long_run_at_c3_size(ib, cuda_ok, sched):
     """300 rounds (3000 sweeps) of the C3 workload in 3 launches: no wait gives up, the spins
     stay unit vectors, every slice charge stays an integer, and the running accumulators,

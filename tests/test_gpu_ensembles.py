@@ -227,3 +227,116 @@ def test_engine_rejects_bad_input(ib, cuda_ok):
         eng.set_schedule(block_threads=48)
     with pytest.raises(ib.IsingError):
         eng.run(0, 1)
+
+
+# The fused loader (both colour passes in one pass over ping-pong buffers) must reproduce the
+# per-pass PT path bit for bit: chunks of 2 planes (many halo planes), chunks narrower than
+# the mesh with uneven widths, whole meshes (halo planes are the chunk's own), y-segments of
+# 2 rows and whole columns.
+FUSED_SCHEDS = [
+    {"block_threads": 128, "chunk_pairs": 16, "order": 0, "loader": 2},
+    {"block_threads": 128, "chunk_pairs": 1 << 30, "order": 0, "loader": 2},
+    {"block_threads": 256, "chunk_pairs": 64, "order": 0, "loader": 2},
+    {"block_threads": 512, "chunk_pairs": 1 << 30, "order": 0, "loader": 2},
+]
+
+
+@pytest.mark.parametrize("sched", FUSED_SCHEDS)
+@pytest.mark.parametrize("move", [1, 0])
+def test_fused_loader_matches_single_ensemble_pt(ib, cuda_ok, sched, move):
+    eng, em, rm, refs = _engine_and_refs(ib, MEMBERS, k=2, rounds=4, move=move, sched=sched)
+    assert eng.schedule()["loader"] == "fused"
+    _assert_same(MEMBERS, eng, em, rm, refs)
+
+
+FUSED_WIDE = [((12, 6, 128), 3, 0.5, 0.3, 0.05, 51), ((4, 4, 128), 2, 0.7, 0.1, 0.0, 52),
+              ((10, 8, 96), 4, 0.3, 0.2, 0.0, 53)]
+
+
+@pytest.mark.parametrize("threads,chunk", [(128, 64), (256, 1 << 30), (384, 512), (512, 1 << 30)])
+def test_fused_loader_nz128_and_nz96(ib, cuda_ok, threads, chunk):
+    sched = {"block_threads": threads, "chunk_pairs": chunk, "order": 0, "loader": 2}
+    eng, em, rm, refs = _engine_and_refs(ib, FUSED_WIDE, k=4, rounds=3, sched=sched)
+    _assert_same(FUSED_WIDE, eng, em, rm, refs)
+
+
+def test_fused_loader_random_pairs_anisotropy_and_repeated_runs(ib, cuda_ok):
+    members = [(8, 4, 0.3, 0.1, 0.05, 61), (12, 5, 0.7, 0.3, 0.05, 62), (16, 3, 0.5, 0.2, 0.0, 63)]
+    sched = {"block_threads": 256, "chunk_pairs": 32, "order": 0, "loader": 2}
+    eng, em, rm, refs = _engine_and_refs(ib, members, k=2, rounds=2, scheme=1, sched=sched)
+    eng.run(4, 2)            # a second run with another round length continues the same chain
+    for pt in refs:
+        pt.run(4, 2)
+    _assert_same(members, eng, em, rm, refs)
+
+
+def test_fused_loader_mixed_dmi_forms(ib, cuda_ok):
+    """Bulk and interfacial ensembles together run the tabulated-D kernel."""
+    members = [(8, 4, 0.5, 0.2, 0.0, 71), (12, 4, 0.5, 0.2, 0.0, 72)]
+    emeshes, rmeshes, spec = [], [], []
+    for (L, n, D, B, K, ens), dmi in zip(members, ("bulk", "interfacial")):
+        em, rmm = ib.ChainMesh.simple_cubic(L, n_replicas=n), ib.ChainMesh.simple_cubic(L, n_replicas=n)
+        em.init_uniform(SEED, ens)
+        rmm.init_uniform(SEED, ens)
+        emeshes.append(em)
+        rmeshes.append(rmm)
+        spec.append((em, _betas(ib, n), _p(ib, D, B, K, dmi), ens))
+    eng = ib.Ensembles(spec, seed=SEED)
+    eng.set_schedule(block_threads=128, chunk_pairs=16, loader=2)
+    eng.run(2, 3)
+    refs = []
+    for (L, n, D, B, K, ens), dmi, rmm in zip(members, ("bulk", "interfacial"), rmeshes):
+        pt = ib.ParallelTempering(rmm, _betas(ib, n), _p(ib, D, B, K, dmi), seed=SEED, ensemble=ens)
+        pt.run(2, 3)
+        refs.append(pt)
+    _assert_same(members, eng, emeshes, rmeshes, refs)
+
+
+def test_fused_loader_rejects_odd_rounds_and_small_blocks(ib, cuda_ok):
+    m = ib.ChainMesh.simple_cubic(8, ny=8, nz=128, n_replicas=2)
+    m.init_uniform(SEED, 81)
+    eng = ib.Ensembles([(m, _betas(ib, 2), _p(ib, 0.3, 0.1), 81)], seed=SEED)
+    with pytest.raises(ib.IsingError):
+        eng.set_schedule(block_threads=96, chunk_pairs=4096, loader=2)     # fewer than nz threads
+    eng.set_schedule(block_threads=128, chunk_pairs=4096, loader=2)
+    with pytest.raises(ib.IsingError):
+        eng.run(3, 1)                                                     # odd sweeps per round
+    eng.run(2, 1)
+
+
+def test_fused_loader_timeout_and_recovery(ib, cuda_ok):
+    spec = []
+    for L, n, D, B, K, ens in MEMBERS[:2]:
+        m = ib.ChainMesh.simple_cubic(L, n_replicas=n)
+        m.init_uniform(SEED, ens)
+        spec.append((m, _betas(ib, n), _p(ib, D, B), ens))
+    eng = ib.Ensembles(spec, seed=SEED, wait_timeout_ms=50)
+    eng.set_schedule(block_threads=128, chunk_pairs=16, loader=2)
+    eng.inject_stall(1)
+    with pytest.raises(ib.IsingError) as ei:
+        eng.run(2, 3)
+    assert ei.value.status == 4          # ISING_ERR_TIMEOUT
+    eng.run(2, 2)
+    for i in range(2):
+        e_run, _ = eng.energies(i)
+        assert np.all(np.isfinite(e_run))
+        eng.resync()
+        e_new, _ = eng.energies(i)
+        assert np.max(np.abs(e_run - e_new)) / spec[i][0].numAtoms < 1e-5
+
+
+def test_set_resync_rearms_the_fp64_recomputation(ib, cuda_ok):
+    spec = []
+    for L, n, D, B, K, ens in MEMBERS[:2]:
+        m = ib.ChainMesh.simple_cubic(L, n_replicas=n)
+        m.init_uniform(SEED, ens)
+        spec.append((m, _betas(ib, n), _p(ib, D, B), ens))
+    eng = ib.Ensembles(spec, seed=SEED)
+    eng.set_resync(3)
+    eng.run(2, 6)               # ends on a resync: the accumulators equal a fresh recomputation
+    e_run = [eng.energies(i)[0] for i in range(2)]
+    eng.resync()
+    for i in range(2):
+        np.testing.assert_array_equal(e_run[i], eng.energies(i)[0])
+    with pytest.raises(ib.IsingError):
+        eng.set_resync(-1)
