@@ -154,10 +154,12 @@ __global__ void __launch_bounds__(64) k_patch_accept(PatchStep P, int64_t w0, co
     const float ls = fminf(kLogSigMax, fmaxf(kLogSigMin, o[3])) + logf(sc_);
     V3 e1, e2;
     pframe(sp, e1, e2);
+    // geodesic distance from both the cosine and the sine (the component of s normal to s'):
+    // acos of a cosine near 1 would lose most bits of a small angle
     const float cth = fminf(1.f, fmaxf(-1.f, vdot(sp, s)));
-    const float th = acosf(cth);
     const V3 vv = vaxpy(-cth, sp, s);
     const float nv = sqrtf(vdot(vv, vv));
+    const float th = atan2f(nv, cth);
     const float sc = nv > 1e-12f ? th / nv : 0.f;
     const V3 mu = vscale(sc_ * P.drift, v3(o[0], o[1], o[2]));
     const float r1 = sc * vdot(vv, e1) - vdot(mu, e1), r2 = sc * vdot(vv, e2) - vdot(mu, e2);

@@ -1,6 +1,6 @@
-"""Every symbol that the Fortran module in INTEGRATION.md binds (bind(C, name="...")) is
-declared in include/ising_gpu.h and exported by the built library, so the documented
-interfaces name real entry points."""
+"""Every symbol that the Fortran module include/ising_gpu.f90 binds (bind(C, name="...")) is
+declared in include/ising_gpu.h with the same number of arguments and exported by the built
+library, so the module's interfaces name real entry points."""
 import ctypes
 import os
 import re
@@ -11,12 +11,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_fortran_bindings_name_real_entry_points():
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    doc = open(os.path.join(ROOT, "include", "ising_gpu.f90")).read()
     names = sorted(set(re.findall(r'bind\(C,\s*name="([A-Za-z0-9_]+)"\)', doc)))
     assert len(names) >= 20
     header = open(os.path.join(ROOT, "include", "ising_gpu.h")).read()
     missing_decl = [n for n in names if not re.search(r"\b" + n + r"\s*\(", header)]
-    assert not missing_decl, f"bound in INTEGRATION.md but not declared in the header: {missing_decl}"
+    assert not missing_decl, f"bound in the Fortran module but not declared in the header: {missing_decl}"
     so = os.path.join(ROOT, "ising_b200", "libisinggpu.so")
     if not os.path.exists(so):
         pytest.skip("libisinggpu.so not built")
@@ -33,7 +33,7 @@ def _c_arg_count(header, name):
 
 
 def test_fortran_bindings_take_as_many_arguments_as_the_c_prototypes():
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    doc = open(os.path.join(ROOT, "include", "ising_gpu.f90")).read()
     joined = re.sub(r"&\s*\n\s*", " ", doc)          # Fortran continuation lines
     header = open(os.path.join(ROOT, "include", "ising_gpu.h")).read()
     found = re.findall(r'function\s+\w+\(([^)]*)\)\s*bind\(C,\s*name="([A-Za-z0-9_]+)"\)', joined)
