@@ -613,6 +613,17 @@ class Ensembles:
             mesh._depend(self)
         _LIVE["eng"].add(self)
 
+    @classmethod
+    def for_rank(cls, members, rank: int, world: int, sweeps: int = 1, **kw):
+        """The share of `members` that one rank of a multi-GPU job runs: whole ensembles,
+        balanced by sites x temperatures x sweeps (``sharding.partition_ensembles``), as an
+        engine of its own with no collective between ranks (the parameter slots of
+        src/PT.f90:147-176 never exchange data).  Returns (engine or None when the rank gets
+        no ensemble, indices into `members`)."""
+        from .sharding import members_for_rank
+        idx, mine = members_for_rank(members, rank, world, sweeps)
+        return (cls(mine, **kw) if mine else None), idx
+
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
             _lib.load().ising_ensembles_destroy(self._h)

@@ -60,3 +60,17 @@ def partition_ensembles(costs: Sequence[float], size: int) -> List[List[int]]:
 
 def ensemble_cost(L: int, replicas: int, sweeps: int, n_sub: int = 1) -> float:
     return float(L ** 3 * n_sub * replicas * sweeps)
+
+
+def members_for_rank(members, rank: int, world: int, sweeps: int = 1):
+    """(indices, members) that ``partition_ensembles`` places on `rank` of `world`.
+
+    `members` is the engine's list of (mesh, betas, params, ensemble_id); the cost of an
+    ensemble is its sites x temperatures x sweeps.  The ensemble ids stay those of the full
+    list, so an ensemble's chain (keyed by seed and id) is the same on any placement."""
+    if not 0 <= rank < world:
+        raise ValueError("rank must be in 0..world-1")
+    costs = [float(m.numAtoms) * len(b) * sweeps for m, b, _, _ in members]
+    mine = partition_ensembles(costs, world)[rank]
+    return mine, [members[i] for i in mine]
+
