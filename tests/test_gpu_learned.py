@@ -276,3 +276,88 @@ def test_trained_network_gains_over_the_untrained_proposal(ib, cuda_ok):
     e1, acc1 = esjd(net, 0.25)
     assert 0.1 < acc0 < 0.5 and 0.1 < acc1 < 0.5, (acc0, acc1)
     assert e1 > 1.5 * e0, (e0, e1)
+
+
+def test_learned_only_chains_sample_the_boltzmann_distribution(ib, cuda_ok):
+    """Stationarity of the learned move by itself.  16 replicas of SC L=8 with the C5
+    Hamiltonian (bulk D=0.5, B=0.25) at T=1 are equilibrated by 2000 plain sweeps on two twin
+    meshes (bit-identical states).  Then one mesh continues with plain single-spin sweeps only
+    and the other moves ONLY by learned patch proposals (all eight colour classes per step,
+    random offsets), with a network trained so that its mean rotations are non-zero and its
+    spreads site-dependent, at drift 0.5: the proposal is strongly asymmetric, so the forward
+    and reverse densities, the exponential map's Jacobian and the |omega| < pi rejection all
+    enter the acceptance.  If the MH ratio is exact, the learned chains stay in the Boltzmann
+    distribution the plain chains sample: the per-replica averages of E/N, |M|/N, Q, and the
+    per-replica C_v and chi agree (paired over replicas, which share their starting state)
+    within 3 standard errors."""
+    import torch
+    torch.manual_seed(0)
+    R, L, beta = 16, 8, 1.0
+    N = L ** 3
+    p = ib.params(J=-1.0, Dz=0.5, B=0.25, dmi="bulk", include_Jp=False)
+    meshes, pts = [], []
+    for _ in range(2):
+        m = ib.ChainMesh.simple_cubic(L, n_replicas=R)
+        m.init_uniform(0xB41, 0)
+        meshes.append(m)
+        pts.append(ib.ParallelTempering(m, np.full(R, beta), p, seed=0xB41, ensemble=0))
+    for pt in pts:
+        pt.relax(2000)
+    for r in range(R):
+        np.testing.assert_array_equal(meshes[0].get_spins(r), meshes[1].get_spins(r))
+    plain, learned = pts
+    # a trained network: windows of the equilibrated states, targets from local equilibration
+    net = ib.ProposalNet(max_batch=64, seed=13)
+    rng = np.random.default_rng(3)
+    ws, ts = [], []
+    for i in range(24):
+        w, t = learned.patch_samples(int(rng.integers(0, 8)), tuple(int(v) for v in rng.integers(0, 8, 3)), n_local=20)
+        ws.append(w)
+        ts.append(t)
+    W, T = torch.cat(ws), torch.cat(ts)
+    for step in range(200):
+        j = torch.randint(0, W.shape[0], (64,), device=W.device)
+        net.train_step(W[j], T[j], lr=2e-3)
+    out = net.forward(W[:64]).float()
+    assert out[..., :3].abs().mean().item() > 1e-2          # non-zero mean rotations
+    learned.patch_tune_scale(net, target=0.3, iters=10, seed=4, drift=0.5)
+    # the tuning steps moved the learned arm only; both arms now run n_meas steps
+    n_meas = 2500
+    q = C.c_double()
+
+    def sample(pt, mesh, with_q):
+        e, mv = pt.energies()
+        qs = []
+        if with_q:
+            for r in range(R):
+                ib._lib.call("ising_winding_number", mesh.handle, r, L // 2, C.byref(q))
+                qs.append(q.value)
+        return e / N, np.linalg.norm(mv, axis=1) / N, qs
+
+    series = {0: ([], [], []), 1: ([], [], [])}
+    p0, a0 = learned.patch_stats()
+    for it in range(n_meas):
+        plain.relax(1)
+        for c in range(8):
+            learned.patch_step(net, c, tuple(int(v) for v in rng.integers(0, 8, 3)))
+        for arm, (pt, mesh) in enumerate(((plain, meshes[0]), (learned, meshes[1]))):
+            e, mm, qs = sample(pt, mesh, it % 5 == 4)
+            series[arm][0].append(e)
+            series[arm][1].append(mm)
+            if qs:
+                series[arm][2].append(qs)
+    p1, a1 = learned.patch_stats()
+    acc = float((a1 - a0).sum() / max(int((p1 - p0).sum()), 1))
+    assert 0.05 < acc < 0.8, acc
+    stats = {}
+    for arm in (0, 1):
+        E, M, Q = (np.array(x).T for x in series[arm])             # [replica][sample]
+        stats[arm] = {"E": E.mean(1), "M": M.mean(1), "Q": Q.mean(1),
+                      "C_v": beta * beta * N * E.var(1), "chi": beta * N * M.var(1)}
+    z = {}
+    for k in ("E", "M", "Q", "C_v", "chi"):
+        d = stats[1][k] - stats[0][k]
+        se = d.std(ddof=1) / np.sqrt(R)
+        z[k] = abs(d.mean()) / se if se > 0 else 0.0
+    print("learned-only vs plain-only:", {k: round(v, 2) for k, v in z.items()}, "acceptance", round(acc, 3))
+    assert max(z.values()) < 3.0, z
