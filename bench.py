@@ -2,22 +2,28 @@
 """Benchmark of the Heisenberg Metropolis / parallel-tempering hot path on B200.
 
 One step = one parallel-tempering round of the workload: `sweeps_per_swap` colour-class
-sweeps of every replica of every ensemble, then each ensemble's replica exchange.  The
-whole timed region is one launch of the persistent multi-ensemble kernel (ising_ensembles_*,
-replayed from a CUDA graph); its schedule is picked by the library's autotuner during
-warm-up.  `--engine pt` times the per-colour-pass launch path (ising_pt_*) instead.
-metric: spin-updates/s = attempted single-site updates (N per replica per sweep) / s.
+sweeps of every replica of every ensemble, then each ensemble's replica exchange, run by the
+persistent multi-ensemble kernel (ising_ensembles_*, replayed from a CUDA graph) with its
+schedule picked by the library's autotuner during warm-up; the FP64 recomputation of the
+energy / magnetisation accumulators runs inside the timed region every `--resync-every`
+rounds (default 10 rounds = 100 sweeps).  `--engine pt` times the per-colour-pass launch path
+(ising_pt_*) instead.  metric: spin-updates/s = attempted single-site updates (N per replica
+per sweep) / s.
 
-Default workload (N=1): simple cubic L=128, 16 replicas, T geometric 0.1-1.5, J=1
-(ferromagnetic, passed as J=-1 in the reference sign convention), bulk DMI D=0.7,
-B=0.3 along z, K=0.05 along z, ball move r=0.2, swaps every 10 sweeps.  Spin state is
-384 MiB (> 126 MB L2), so no L2 flush is needed between steps.  Workload c4: 12 ensembles
-L in {16,24,32,48,64,96} (two each), (D,B) on the grid {0.3,0.5,0.7} x {0.1,0.3},
-16-64 replicas each, T geometric 0.1-2.0 (148,160,512 sites, 1.78 GB of spins).
+Default workload (N=1), the configuration the metric "spin-updates/s and Q-ESS/s, learned vs
+plain" is quoted on: simple cubic L=96, 48 replicas, T geometric 0.1-1.5, J=1 (ferromagnetic,
+passed as J=-1 in the reference sign convention), bulk DMI D=0.5, B=0.25 along z, K=0, ball
+move r=0.2, swaps every 10 sweeps.  Spin state 486 MiB (> 126 MB L2), so no L2 flush is needed
+between steps.  The line also carries `fp64_error` (accumulator drift and snapshot errors of E,
+|M| and Q against the FP64 oracle) and `q_ess` (learned patch proposal against plain
+Metropolis: tau_int and effective samples per second of Q and E, observables per slot).
+Workloads c3 (L=128 x 16) and c4 (12 ensembles L in {16,24,32,48,64,96}, 16-64 replicas each,
+148,160,512 sites) are --workload options.
 
-Under torchrun each rank runs its own copy of the workload on its GPU (independent
-ensembles, weak scaling, no collective on the data path); the timed region is bracketed
-by barriers and the max over ranks is reported.
+Under torchrun a single-ensemble workload runs one copy per rank (independent ensembles, weak
+scaling); c4's ensembles are split across ranks by whole ensembles (strong scaling).  No
+collective on the data path; the timed region is bracketed by barriers and the max over ranks
+is reported.
 
 --impl reference times the reference algorithm on the host cores instead: the CPU
 restatement of Metropolis_mcs (src/energyMin.f90:234-374) with all host threads.
@@ -330,6 +336,52 @@ def ensembles_of(args, w):
     return [(args.L or w["L"], args.replicas or w["R"], w["D"], w["B"])]
 
 
+def fp64_errors(ib, O, eng, members, w, k):
+    """Error of the reported observables against FP64: (1) the drift of the running FP64
+    accumulators (sums of FP32 dE, dM) over 9 rounds since the last resync, against the device
+    recomputation; (2) on the downloaded spins of the coldest and the hottest slot of the
+    first ensemble, the device E, |M| and winding numbers against the FP64 oracle."""
+    import numpy as np
+    eng.run(k, 9)
+    acc = [eng.energies(i) for i in range(len(members))]
+    eng.resync()
+    fresh = [eng.energies(i) for i in range(len(members))]
+    drift_e = max(float(np.max(np.abs(a[0] - f[0]))) / m.numAtoms for a, f, (m, *_) in zip(acc, fresh, members))
+    drift_m = max(float(np.max(np.abs(a[1] - f[1]))) / m.numAtoms for a, f, (m, *_) in zip(acc, fresh, members))
+    m, betas, _, _ = members[0]
+    L = m.numCellsX
+    N = m.numAtoms
+    perm = eng.permutation(0)
+    if "ensembles" in w:
+        D0, B0 = w["ensembles"][0][2]
+    else:
+        D0, B0 = w["D"], w["B"]
+    op = O.Params(J=w["J"], Dz=D0, B=B0, K=w["K"], dmi_bulk=True)
+    E_dev, M_dev = fresh[0]
+    snaps = []
+    for t in (0, len(betas) - 1):
+        r = int(perm[t])
+        s = m.get_spins(r)
+        om = O.Mesh.sc(L)
+        om.set_spins(s)
+        e_o = om.canonical_energy(op)
+        mo = float(np.linalg.norm(s.sum(axis=0))) / N
+        md = float(np.linalg.norm(M_dev[r])) / N
+        q_dev = ib.winding_all_slices(m, r)
+        q_o = np.array([om.winding_number(z) for z in range(1, L + 1)])
+        snaps.append({"slot": t, "T": float(1.0 / betas[t]),
+                      "E_per_site": {"device": float(E_dev[r]) / N, "oracle": e_o / N,
+                                     "abs_err": abs(float(E_dev[r]) - e_o) / N},
+                      "absM": {"device": md, "oracle": mo, "abs_err": abs(md - mo)},
+                      "Q_sum": {"device": float(q_dev.sum()), "oracle": float(q_o.sum()),
+                                "max_abs_err_per_slice": float(np.max(np.abs(q_dev - q_o))),
+                                "rounded_equal": bool(round(q_dev.sum()) == round(q_o.sum()))}})
+    return {"accumulator_drift_per_site_after_90_sweeps": {"E": drift_e, "M": drift_m},
+            "snapshots_vs_fp64_oracle": snaps,
+            "note": "device E: FP64 sums of FP32 terms; Q: FP64 Berg-Luscher per slice; C_v and chi derive from "
+                    "the recorded E and |M|, whose errors are those above"}
+
+
 def run_gpu(args, w):
     import numpy as np
     import torch
@@ -347,15 +399,26 @@ def run_gpu(args, w):
     k = w["k"]
     move = _lib.MOVE_BALL if w["move"] == "ball" else _lib.MOVE_UNIFORM
     spec = ensembles_of(args, w)
+    # multi-ensemble workloads are split across ranks by whole ensembles (the parameter slots
+    # of src/PT.f90:147-176 never exchange data): strong scaling; a single ensemble runs as
+    # one independent copy per rank (distinct Philox ensemble ids): weak scaling
+    split = world > 1 and len(spec) > 1
+    if split:
+        from ising_b200.sharding import partition_ensembles
+        mine = partition_ensembles([float(L ** 3 * R) for L, R, _, _ in spec], world)[rank]
+    else:
+        mine = list(range(len(spec)))
     members = []
-    for i, (L, R, D, B) in enumerate(spec):
-        ens_id = rank * len(spec) + i            # distinct Philox streams per rank and ensemble
+    for i in mine:
+        L, R, D, B = spec[i]
+        ens_id = i if split else rank * len(spec) + i
         m = ib.ChainMesh.simple_cubic(L, n_replicas=R, device=dev)
         m.set_stream(stream.cuda_stream)
         m.init_uniform(0x15196, ensemble=ens_id)
         p = ib.params(J=w["J"], Dz=D, B=B, K=w["K"], dmi="bulk")
         members.append((m, 1.0 / ib.temperature_ladder(w["tmin"], w["tmax"], R), p, ens_id))
-    sites = sum(L ** 3 * R for L, R, _, _ in spec)
+    sites = sum(spec[i][0] ** 3 * spec[i][1] for i in mine)
+    sites_job = sum(L ** 3 * R for L, R, _, _ in spec) if split else world * sites
     updates_per_step = sites * k
 
     def barrier():
@@ -371,26 +434,35 @@ def run_gpu(args, w):
         return float(t.item())
 
     sched_info = {}
+    eng = None
+    n_chunks = 1
     if args.engine == "ensembles":
-        eng = ib.Ensembles(members, seed=0x15196, move=move, r=w["r"])
-        eng.set_stream(stream.cuda_stream)
-        if args.schedule:   # threads,chunk_pairs,loader: a fixed schedule instead of the autotuner
-            bt, cp, ld = (int(v) for v in args.schedule.split(","))
-            eng.set_schedule(block_threads=bt, chunk_pairs=cp, loader=ld)
-        # 4 rounds per candidate: near-tied schedules are told apart by more than timer noise
-        trials = eng.autotune(k, 4) if not (args.no_autotune or args.schedule) else []
-        eng.run(k, max(args.warmup, 1))
-        run = lambda n: eng.run(k, n)
+        eng = ib.Ensembles(members, seed=0x15196, move=move, r=w["r"]) if members else None
+        if eng:
+            eng.set_stream(stream.cuda_stream)
+            if args.schedule:   # threads,chunk_pairs,loader: a fixed schedule instead of the autotuner
+                bt, cp, ld = (int(v) for v in args.schedule.split(","))
+                eng.set_schedule(block_threads=bt, chunk_pairs=cp, loader=ld)
+            # 4 rounds per candidate: near-tied schedules are told apart by more than timer noise
+            trials = eng.autotune(k, 4) if not (args.no_autotune or args.schedule) else []
+            eng.run(k, max(args.warmup, 1))
+            # the periodic FP64 resync that bounds the accumulators' drift runs inside the
+            # timed region, every resync_every rounds counted from here
+            eng.set_resync(args.resync_every)
+            sched_info = eng.schedule()
+            sched_info["autotune_trials"] = len(trials)
+            if trials:
+                best = min(trials, key=lambda t: t["ms_per_round"])
+                worst = max(trials, key=lambda t: t["ms_per_round"])
+                sched_info["autotune_spread_ms"] = [best["ms_per_round"], worst["ms_per_round"]]
+        run = (lambda n: eng.run(k, n)) if eng else (lambda n: None)
         energies = lambda: [eng.energies(i) for i in range(len(members))]
-        sched_info = eng.schedule()
-        sched_info["autotune_trials"] = len(trials)
-        if trials:
-            best = min(trials, key=lambda t: t["ms_per_round"])
-            worst = max(trials, key=lambda t: t["ms_per_round"])
-            sched_info["autotune_spread_ms"] = [best["ms_per_round"], worst["ms_per_round"]]
-        kernel_name = "k_ensembles"
-        launches_timed = 1                       # one persistent launch (plus a memset node)
-        closers = [eng]
+        kernel_name = "k_ensembles_fused" if sched_info.get("loader") == "fused" else "k_ensembles"
+        # one persistent launch per resync interval (plus a memset node), then the resync's
+        # energy reduction (energy pass + block fold) and its copy into the accumulators
+        n_chunks = -(-args.steps // args.resync_every) if args.resync_every else 1
+        launches_timed = n_chunks + (args.steps // args.resync_every) * 2 if args.resync_every else 1
+        closers = [eng] if eng else []
     else:
         if len(members) != 1:
             raise SystemExit("--engine pt runs single-ensemble workloads only")
@@ -419,14 +491,15 @@ def run_gpu(args, w):
     ms_local = ev0.elapsed_time(ev1)
     ms = max_over_ranks(ms_local)
     clk = clocks.stop()
-    value = world * updates_per_step * args.steps / (ms / 1e3)
+    value = sites_job * k * args.steps / (ms / 1e3)
 
-    # dominant kernel: with the engine the timed region is one launch of k_ensembles, so its
-    # launch duration is the event time of the region; with --engine pt the colour-pass
-    # kernel is timed alone over relax sweeps (colour-pass launches plus one fold/advance)
+    # dominant kernel: with the engine the timed region is the persistent launches (one per
+    # resync interval) and the resyncs (one energy pass each, well under 1 % of the region),
+    # so the region's duration stands for the launches' duration; with --engine pt the
+    # colour-pass kernel is timed alone over relax sweeps
     if args.engine == "ensembles":
-        launch_ms = ms_local
-        bytes_per_launch = BYTES_PER_UPDATE * updates_per_step * args.steps
+        launch_ms = ms_local / max(n_chunks, 1)
+        bytes_per_launch = BYTES_PER_UPDATE * updates_per_step * args.steps / max(n_chunks, 1)
     else:
         n_relax = max(4, min(40, args.steps * k // 2))
         launches = pt.schedule(n_relax)[1]
@@ -447,7 +520,7 @@ def run_gpu(args, w):
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
-    achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
+    achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else 0.0
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     if os.path.exists(tfile):
@@ -466,7 +539,7 @@ def run_gpu(args, w):
     # directions of the link overlap; the run waits for every upload, and the timed region
     # ends after the last downloads have landed.
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and members:
         L_ = _lib.load()
         host = [[torch.empty(3 * mm.numAtoms, dtype=torch.float64, pin_memory=True) for _ in range(len(b))]
                 for mm, b, _, _ in members]
@@ -504,7 +577,7 @@ def run_gpu(args, w):
         wall = time.perf_counter() - t0
         e_ms = max_over_ranks(max(a0.elapsed_time(a1), wall * 1e3))
         n_rep = sum(len(b) for _, b, _, _ in members)
-        e2e = {"value": world * updates_per_step * e2e_steps / (e_ms / 1e3), "unit": "spin-updates/s",
+        e2e = {"value": sites_job * k * e2e_steps / (e_ms / 1e3), "unit": "spin-updates/s",
                "h2d_bytes_per_step": sites * 3 * 8, "d2h_bytes_per_step": sites * 3 * 8 + n_rep * 32,
                "steps": e2e_steps,
                "path": "ising_spins_set_async per replica -> one round -> ising_spins_get_async per replica "
@@ -514,14 +587,21 @@ def run_gpu(args, w):
         # the copies is (both directions at once) + (the round)
         link = link_rates(torch, host, stream)
         floor_ms = link["bidir_ms"] + ms / args.steps
-        e2e["link"] = {k: v for k, v in link.items() if k != "bidir_ms"}
+        e2e["link"] = {k_: v for k_, v in link.items() if k_ != "bidir_ms"}
         e2e["floor_ms_per_step"] = floor_ms
         e2e["frac_of_floor"] = floor_ms / (e_ms / e2e_steps)
+        del host
+
+    errors = None
+    if rank == 0 and world == 1 and eng is not None and not args.no_cpu:
+        from oracle import oracle as O
+        O.build()
+        errors = fp64_errors(ib, O, eng, members, w, k)
 
     cpu = cpu_fast = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = host_cores()
-        # one replica of the workload's largest lattice (C3: L=128, about a second of CPU work)
+        # one replica of the workload's largest lattice (about a second of CPU work)
         L_cpu = max(L for L, _, _, _ in spec)
         rate, sample = cpu_reference_rate(w, 2, 1, threads, L_sample=L_cpu)
         cpu = {"value": rate, "unit": "spin-updates/s", "cores": threads, "kind": "port", "sample": sample}
@@ -529,16 +609,26 @@ def run_gpu(args, w):
         cpu_fast = {"value": rate, "unit": "spin-updates/s", "cores": threads, "kind": "optimised port",
                     "sample": sample}
 
+    for c in closers:
+        c.close()
+    for mm, *_ in members:
+        mm.close()
+    q_ess = training = None
+    if rank == 0 and world == 1 and args.workload == "c5" and not args.no_learned:
+        q_ess, training = learned_vs_plain(args, w)
+
     if rank == 0:
         line = {
             "metric": "spin-updates/s", "value": value, "unit": "spin-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "strong" if split else "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (uniform random initial spins from Philox, seed 0x15196)",
             "config": {"workload": args.workload, "desc": w["desc"], "ensembles": len(spec),
                        "lattices": sorted({L for L, _, _, _ in spec}), "replicas": sum(R for _, R, _, _ in spec),
-                       "sweeps_per_step": k, "sites": sites, "engine": args.engine,
-                       "parallelism": f"replicas x{world} (independent ensembles)",
+                       "sweeps_per_step": k, "sites": sites_job, "engine": args.engine,
+                       "resync_every_rounds": args.resync_every if args.engine == "ensembles" else None,
+                       "parallelism": (f"whole ensembles over {world} ranks" if split
+                                       else f"replicas x{world} (independent ensembles)"),
                        "l2": "state larger than L2 (no flush)" if sites * 12 > 126e6 else "state fits L2; no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
@@ -551,12 +641,12 @@ def run_gpu(args, w):
             "cpu_fastest": cpu_fast,
             "gpu_launches": launches_timed,
             "schedule": sched_info,
+            "fp64_error": errors,
         }
+        if q_ess is not None:
+            line["q_ess"] = q_ess
+            line["training"] = training
         print(json.dumps(line), flush=True)
-    for c in closers:
-        c.close()
-    for mm, *_ in members:
-        mm.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -808,12 +898,58 @@ def run_patch_probe(args, w):
 
 
 # ---------------------------------------------------------------- C5: learned vs plain
-def run_c5(args, w):
+def _jackknife_var_obs(x, beta, N, kind, n_blocks=20):
+    """Blocked jackknife error of C_v = beta^2 N var(e) (kind 'cv', x = E/N) or
+    chi = beta N var(|m|) (kind 'chi', x = |M|/N) over one time series."""
+    import numpy as np
+    x = np.asarray(x, dtype=np.float64)
+    f = (beta * beta * N) if kind == "cv" else (beta * N)
+    nb = min(n_blocks, len(x) // 2)
+    if nb < 2:
+        return f * x.var(), 0.0
+    b = len(x) // nb
+    x = x[: nb * b]
+    full = f * x.var()
+    reps = np.array([f * np.delete(x.reshape(nb, b), i, axis=0).ravel().var() for i in range(nb)])
+    return full, float(np.sqrt((nb - 1) / nb * ((reps - reps.mean()) ** 2).sum()))
+
+
+def compare_arms(a, b, betas, N):
+    """Per temperature slot: E/N, |M|/N, Q, C_v, chi of two recorded series [slot][sample][E,|M|,Qmid,Qmean]
+    (E total) with binning (mean) and blocked jackknife (C_v, chi) errors; counts of slots
+    within 2 combined standard errors.  A slot whose Q is frozen in both series agrees only
+    when the two frozen values are equal."""
+    import numpy as np
+    from ising_b200 import analysis as A
+    R = a.shape[0]
+    per = {k: [] for k in ("E", "absM", "Q", "C_v", "chi")}
+    for t in range(R):
+        for name, col in (("E", 0), ("absM", 1), ("Q", 3)):
+            xa, xb = a[t, :, col], b[t, :, col]
+            if col == 0:
+                xa, xb = xa / N, xb / N
+            err = float(np.hypot(A.binning_error(xa), A.binning_error(xb)))
+            d = float(abs(xa.mean() - xb.mean()))
+            per[name].append(d <= 2 * err + 1e-12)
+        for name, col, kind in (("C_v", 0, "cv"), ("chi", 1, "chi")):
+            xa, xb = a[t, :, col], b[t, :, col]
+            if col == 0:
+                xa, xb = xa / N, xb / N
+            va, ea = _jackknife_var_obs(xa, betas[t], N, kind)
+            vb, eb = _jackknife_var_obs(xb, betas[t], N, kind)
+            per[name].append(abs(va - vb) <= 2 * float(np.hypot(ea, eb)) + 1e-12)
+    within = {k: int(sum(v)) for k, v in per.items()}
+    return within, {k: [t for t in range(R) if not v[t]] for k, v in per.items()}
+
+
+def learned_vs_plain(args, w):
     """Learned patch proposal against plain Metropolis on the C5 ensemble (SC L=96, 48 PT
-    replicas): train the network on PT windows, then run both samplers from the same
-    equilibrated chain with the same exchange schedule (one exchange per sweep) and compare
-    the topological charge's integrated autocorrelation time and effective samples per
-    second, and the observables per temperature slot (within 2 binning standard errors)."""
+    replicas, one exchange per sweep): thermalise one chain with plain sweeps, train the
+    network on its windows, tune the patch step scales; then copy the state into a second
+    mesh and run the two samplers as independent chains from that common state, in
+    alternating segments: the plain arm (plain sweeps) and the learned arm (a plain sweep
+    then one colour class of patch moves per step).  Reports tau_int and effective samples
+    per second of Q and E per arm, and the per-slot agreement of E, |M|, Q, C_v and chi."""
     import numpy as np
     import torch
 
@@ -821,17 +957,21 @@ def run_c5(args, w):
     from ising_b200 import _lib
     from ising_b200 import analysis as A
 
-    L, R, k = w["L"], w["R"], 1
+    L, R = w["L"], w["R"]
     N = L ** 3
     n_plain, n_learned = args.c5_plain, args.c5_learned
     stream = torch.cuda.current_stream()
-    mesh = ib.ChainMesh.simple_cubic(L, n_replicas=R)
-    mesh.set_stream(stream.cuda_stream)
-    mesh.init_uniform(0x15196, ensemble=0)
     p = ib.params(J=w["J"], Dz=w["D"], B=w["B"], K=w["K"], dmi="bulk", include_Jp=False)
     betas = 1.0 / ib.temperature_ladder(w["tmin"], w["tmax"], R)
-    pt = ib.ParallelTempering(mesh, betas, p, seed=0x15196, ensemble=0, move=_lib.MOVE_BALL, r=w["r"],
-                              record=True, record_capacity=2 * n_plain + n_learned + 8)
+    meshes, pts = [], []
+    for arm in range(2):
+        m = ib.ChainMesh.simple_cubic(L, n_replicas=R)
+        m.set_stream(stream.cuda_stream)
+        m.init_uniform(0x15196, ensemble=arm)
+        meshes.append(m)
+        pts.append(ib.ParallelTempering(m, betas, p, seed=0x15196 + arm, ensemble=arm, move=_lib.MOVE_BALL,
+                                        r=w["r"], record=True, record_capacity=max(n_plain, n_learned) + 8))
+    plain, learned = pts
 
     def timed(fn):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -843,35 +983,31 @@ def run_c5(args, w):
         torch.cuda.synchronize()
         return max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3) / 1e3
 
-    pt.relax(args.c5_therm)
-    # kernel-level plain throughput (sweeps without exchange or recording)
-    t_relax = timed(lambda: pt.relax(40))
-    value = 40 * R * N / t_relax
+    t_therm = timed(lambda: plain.relax(args.c5_therm))
     rng = np.random.default_rng(7)
     net = ib.ProposalNet(max_batch=args.c5_batch, seed=1)
 
     def jump_stats(steps=8):
-        """per slot: acceptance and squared spin displacement per site per proposal (ESJD)
-        over `steps` patch steps at the current step scales"""
-        p0, a0 = pt.patch_stats()
-        j0 = pt.patch_jump()
+        """per slot: acceptance and squared spin displacement per site per proposal (ESJD)"""
+        p0, a0 = plain.patch_stats()
+        j0 = plain.patch_jump()
         for i in range(steps):
-            pt.patch_step(net, i % 8, tuple(int(v) for v in rng.integers(0, 8, 3)))
-        p1, a1 = pt.patch_stats()
-        j1 = pt.patch_jump()
+            plain.patch_step(net, i % 8, tuple(int(v) for v in rng.integers(0, 8, 3)))
+        p1, a1 = plain.patch_stats()
+        j1 = plain.patch_jump()
         n = np.maximum(p1 - p0, 1).astype(float)
         return (a1 - a0) / n, (j1 - j0) / n / 64.0
 
     # the network as initialised (mu ~ 0, sigma = 0.3 everywhere) with its own tuned step scale
-    scale_untrained = pt.patch_tune_scale(net, target=0.25, iters=args.c5_tune, seed=1, drift=1.0)
+    plain.patch_tune_scale(net, target=0.25, iters=args.c5_tune, seed=1, drift=1.0)
     acc_untrained, esjd_untrained = jump_stats()
     # training set: windows of plain-PT states, targets from local equilibration of the patch
     ws, ts = [], []
     n_have = 0
     while n_have < args.c5_train:
-        pt.relax(20)
-        wi, ti = pt.patch_samples(int(rng.integers(0, 8)), tuple(int(v) for v in rng.integers(0, 8, 3)),
-                                  n_local=args.c5_nlocal)
+        plain.relax(20)
+        wi, ti = plain.patch_samples(int(rng.integers(0, 8)), tuple(int(v) for v in rng.integers(0, 8, 3)),
+                                     n_local=args.c5_nlocal)
         ws.append(wi)
         ts.append(ti)
         n_have += wi.shape[0]
@@ -889,107 +1025,115 @@ def run_c5(args, w):
                 losses.append(net.train_step(W[j], T[j], lr=1e-3))
 
     t_train = timed(train)
+    del W, T
     # the trained network at three drift weights, each with its own tuned step scale; the
-    # measurement run uses the one with the largest mean ESJD
+    # learned arm uses the one with the largest mean ESJD
     trained = {}
     for lam in (0.0, 0.25, 1.0):
-        sc = pt.patch_tune_scale(net, target=0.25, iters=args.c5_tune, seed=2, drift=lam)
+        sc = plain.patch_tune_scale(net, target=0.25, iters=args.c5_tune, seed=2, drift=lam)
         acc, ej = jump_stats()
         trained[lam] = (sc, acc, ej)
     best_lam = max(trained, key=lambda l: float(np.mean(trained[l][2])))
     scale_trained, acc_trained, esjd_trained = trained[best_lam]
-    pt.patch_set_scale(scale_trained, best_lam)
-    # measurement: plain, then learned (1:1 alternation), from the same chain
-    c0 = pt.series().shape[1]
-    t_plain = timed(lambda: pt.run(k, n_plain))
-    c1 = pt.series().shape[1]
+    learned.patch_set_scale(scale_trained, best_lam)
+    plain.relax(200)
+    # the common starting state: slot t of the plain chain -> replica t of the learned mesh
+    t2r = plain.permutation()
+    for t in range(R):
+        meshes[1].set_spins(meshes[0].get_spins(int(t2r[t])), t)
+    learned.resync()
+    # alternating segments; both arms record every sweep
+    seg = max(1, min(500, n_plain, n_learned))
+    t_plain = t_learned = 0.0
+    done_p = done_l = 0
+    step = [0]
 
-    def learned_run():
-        for i in range(n_learned):
-            pt.run(k, 1)
-            pt.patch_step(net, i % 8, tuple(int(v) for v in rng.integers(0, 8, 3)), slots=args.c5_slots)
+    def learned_steps(n):
+        for _ in range(n):
+            learned.run(1, 1)
+            learned.patch_step(net, step[0] % 8, tuple(int(v) for v in rng.integers(0, 8, 3)), slots=args.c5_slots)
+            step[0] += 1
 
-    t_learned = timed(learned_run)
-    c2 = pt.series().shape[1]
-    # a second plain segment after the learned one: the first starts closer to thermalisation,
-    # so drift could inflate its tau; the plain arm is the segment with the larger Q-ESS
-    t_plain2 = timed(lambda: pt.run(k, n_plain))
-    ser = pt.series()
-    sp, sl, sp2 = ser[:, c0:c1], ser[:, c1:c2], ser[:, c2:]
+    while done_p < n_plain or done_l < n_learned:
+        if done_p < n_plain:
+            n = min(seg, n_plain - done_p)
+            t_plain += timed(lambda: plain.run(1, n))
+            done_p += n
+        if done_l < n_learned:
+            n = min(seg, n_learned - done_l)
+            t_learned += timed(lambda: learned_steps(n))
+            done_l += n
+    sp, sl = plain.series(), learned.series()
+    # the samplers' own cost per step, without the per-sweep recording of E, |M| and the
+    # winding numbers (measurement overhead shared by both arms): relax sweeps record nothing
+    c_plain = timed(lambda: plain.relax(100)) / 100
+    c_patch = timed(lambda: [plain.patch_step(net, i % 8, tuple(int(v) for v in rng.integers(0, 8, 3)),
+                                              slots=args.c5_slots) for i in range(40)]) / 40
 
-    def arm(x, secs):
+    def arm(x, secs, cost):
         out = []
         for t in range(R):
             q, e = x[t, :, 3], x[t, :, 0]
             tq, te = A.tau_int(q), A.tau_int(e)
             out.append({"tau_Q": tq, "tau_E": te, "ess_Q_per_s": len(q) / (2 * tq) / secs,
-                        "ess_E_per_s": len(e) / (2 * te) / secs, "q_var": float(np.var(q))})
+                        "ess_E_per_s": len(e) / (2 * te) / secs, "ess_Q_per_sampler_s": 1.0 / (2 * tq * cost),
+                        "q_var": float(np.var(q))})
         return out
 
-    ap1, al, ap2 = arm(sp, t_plain), arm(sl, t_learned), arm(sp2, t_plain2)
-    # Q-ESS over the slots where Q fluctuates in every segment (a frozen Q has no defined tau)
-    live = [t for t in range(R) if ap1[t]["q_var"] > 1e-12 and al[t]["q_var"] > 1e-12 and ap2[t]["q_var"] > 1e-12]
-    q1 = float(np.mean([ap1[t]["ess_Q_per_s"] for t in live])) if live else 0.0
-    q2 = float(np.mean([ap2[t]["ess_Q_per_s"] for t in live])) if live else 0.0
-    ap = ap2 if q2 > q1 else ap1
-    plain_segment = "after" if q2 > q1 else "before"
-    within = {}
-    for name, col in (("E", 0), ("absM", 1), ("Q", 3)):
-        ok = 0
-        for t in range(R):
-            a, b = (sp2 if plain_segment == "after" else sp)[t, :, col], sl[t, :, col]
-            err = np.hypot(A.binning_error(a), A.binning_error(b))
-            ok += int(abs(a.mean() - b.mean()) <= 2 * err + 1e-12)
-        within[name] = ok
+    ap, al = arm(sp, t_plain, c_plain), arm(sl, t_learned, c_plain + c_patch)
+    live = [t for t in range(R) if ap[t]["q_var"] > 1e-12 and al[t]["q_var"] > 1e-12]
     qp = float(np.mean([ap[t]["ess_Q_per_s"] for t in live])) if live else 0.0
     ql = float(np.mean([al[t]["ess_Q_per_s"] for t in live])) if live else 0.0
-    # per-slot ratios: the mean of ESS/s over slots is dominated by the slots with the shortest tau
+    qp_s = float(np.mean([ap[t]["ess_Q_per_sampler_s"] for t in live])) if live else 0.0
+    ql_s = float(np.mean([al[t]["ess_Q_per_sampler_s"] for t in live])) if live else 0.0
     ratios = [al[t]["ess_Q_per_s"] / ap[t]["ess_Q_per_s"] for t in live if ap[t]["ess_Q_per_s"] > 0]
-    per_slot = {"ratios": [round(r, 3) for r in ratios],
-                "median": float(np.median(ratios)) if ratios else None,
-                "geometric_mean": float(np.exp(np.mean(np.log(ratios)))) if ratios else None,
-                "slots_learned_better": sum(1 for r in ratios if r > 1.0)}
-    # a windowed tau estimate means something only for chains much longer than tau (N >= 50 tau)
+    within, outside = compare_arms(sp, sl, betas, N)
     reliable = {"plain": sum(1 for t in live if n_plain >= 50 * ap[t]["tau_Q"]),
                 "learned": sum(1 for t in live if n_learned >= 50 * al[t]["tau_Q"]), "of": len(live)}
-    line = {
-        "metric": "spin-updates/s", "value": value, "unit": "spin-updates/s", "n_gpus": 1, "steps": n_plain,
-        "warmup": args.c5_therm, "ms_per_step": 1e3 * t_plain / n_plain, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (uniform random initial spins from Philox, seed 0x15196)",
-        "config": {"workload": "c5", "desc": w["desc"], "L": L, "replicas": R, "exchange_every": 1,
-                   "patch_slots": args.c5_slots or R, "train_windows": int(W.shape[0]), "epochs": args.c5_epochs},
-        "q_ess": {"metric": "Q-ESS/s (mean over the temperature slots where Q fluctuates in both runs)",
-                  "slots_used": live, "plain": qp, "learned": ql,
-                  "learned_over_plain": ql / qp if qp > 0 else None,
-                  "learned_over_plain_per_slot": per_slot,
-                  "plain_segments": {"before_learned": q1, "after_learned": q2, "used": plain_segment,
-                                     "tau_Q_before": [round(ap1[t]["tau_Q"], 2) for t in live],
-                                     "tau_Q_after": [round(ap2[t]["tau_Q"], 2) for t in live]},
-                  "plain_sweeps": n_plain, "learned_steps": n_learned,
-                  "slots_with_N_ge_50_tauQ": reliable,
-                  "s_per_step": {"plain": t_plain / n_plain, "learned": t_learned / n_learned},
-                  "plain_s": t_plain, "learned_s": t_learned,
-                  "tau_Q_plain": [round(x["tau_Q"], 2) for x in ap], "tau_Q_learned": [round(x["tau_Q"], 2) for x in al],
-                  "E_ess_per_s": {"plain": float(np.mean([x["ess_E_per_s"] for x in ap])),
-                                  "learned": float(np.mean([x["ess_E_per_s"] for x in al]))},
-                  "slots_within_2sigma": within, "slots": R},
-        "training": {"seconds": t_train, "steps": len(losses), "loss_first": losses[0] if losses else None,
-                     "loss_last": losses[-1] if losses else None,
-                     "untrained": {"step_scale": [round(float(x), 4) for x in scale_untrained],
-                                   "acceptance": [round(float(x), 4) for x in acc_untrained],
-                                   "esjd_per_site": [float("%.3g" % x) for x in esjd_untrained]},
-                     "trained": {str(l): {"step_scale": [round(float(x), 4) for x in v[0]],
-                                          "acceptance": [round(float(x), 4) for x in v[1]],
-                                          "esjd_per_site": [float("%.3g" % x) for x in v[2]],
-                                          "esjd_mean": float(np.mean(v[2]))} for l, v in trained.items()},
-                     "drift_used": best_lam, "n_local": args.c5_nlocal,
-                     "esjd_trained_over_untrained_mean": float(np.mean(esjd_trained) / max(np.mean(esjd_untrained), 1e-30))},
-        "roofline": None, "e2e": None, "cpu_baseline": None, "gpu_launches": None,
+    q_ess = {
+        "metric": "Q-ESS/s (mean over the temperature slots where Q fluctuates in both arms)",
+        "plain": qp, "learned": ql, "learned_over_plain": ql / qp if qp > 0 else None,
+        "per_sampler_second": {"plain": qp_s, "learned": ql_s, "learned_over_plain": ql_s / qp_s if qp_s > 0 else None,
+                               "plain_sweep_s": c_plain, "patch_step_s": c_patch,
+                               "note": "cost per step without the per-sweep recording of E, |M| and Q"},
+        "learned_over_plain_per_slot": {"median": float(np.median(ratios)) if ratios else None,
+                                        "slots_learned_better": sum(1 for r in ratios if r > 1.0),
+                                        "of": len(ratios)},
+        "slots_used": live, "slots_with_N_ge_50_tauQ": reliable,
+        "plain_sweeps": n_plain, "learned_steps": n_learned, "plain_s": t_plain, "learned_s": t_learned,
+        "tau_Q_plain": [round(x["tau_Q"], 2) for x in ap], "tau_Q_learned": [round(x["tau_Q"], 2) for x in al],
+        "E_ess_per_s": {"plain": float(np.mean([x["ess_E_per_s"] for x in ap])),
+                        "learned": float(np.mean([x["ess_E_per_s"] for x in al]))},
+        "observables_within_2sigma": {"slots": R, **within, "outside": outside,
+                                      "design": "two independent chains from one thermalised state, "
+                                                "binning errors (means) and blocked jackknife (C_v, chi)"},
+        "exchange_every": 1, "thermalisation_sweeps": args.c5_therm, "thermalisation_s": t_therm,
     }
-    print(json.dumps(line), flush=True)
+    training = {"seconds": t_train, "steps": len(losses), "windows": args.c5_train, "epochs": args.c5_epochs,
+                "loss_first": losses[0] if losses else None, "loss_last": losses[-1] if losses else None,
+                "untrained": {"acceptance_mean": float(np.mean(acc_untrained)),
+                              "esjd_mean": float(np.mean(esjd_untrained))},
+                "trained": {str(l): {"acceptance_mean": float(np.mean(v[1])), "esjd_mean": float(np.mean(v[2]))}
+                            for l, v in trained.items()},
+                "drift_used": best_lam, "n_local": args.c5_nlocal,
+                "esjd_trained_over_untrained_mean": float(np.mean(esjd_trained) / max(np.mean(esjd_untrained), 1e-30))}
     net.close()
-    pt.close()
-    mesh.close()
+    for q in pts:
+        q.close()
+    for m in meshes:
+        m.close()
+    return q_ess, training
+
+
+def run_c5(args, w):
+    """--learned: the learned-vs-plain comparison on its own, as one JSON line."""
+    q_ess, training = learned_vs_plain(args, w)
+    line = {"metric": "Q-ESS/s", "value": q_ess["learned"], "unit": "effective Q samples/s", "n_gpus": 1,
+            "higher_is_better": True, "vs_baseline": None, "dtype": "f32 (network bf16)",
+            "data": "synthetic (uniform random initial spins from Philox, seed 0x15196)",
+            "config": {"workload": "c5", "desc": w["desc"], "L": w["L"], "replicas": w["R"]},
+            "q_ess": q_ess, "training": training}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -998,7 +1142,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c5", choices=sorted(WORKLOADS))
     ap.add_argument("--L", type=int, default=0, help="override lattice size (profiling)")
     ap.add_argument("--replicas", type=int, default=0, help="override replica count (profiling)")
     ap.add_argument("--engine", default="ensembles", choices=["ensembles", "pt"])
@@ -1023,6 +1167,9 @@ def main():
     ap.add_argument("--c5-batch", type=int, default=8192)
     ap.add_argument("--c5-slots", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="c5: skip the learned-vs-plain q_ess block")
+    ap.add_argument("--resync-every", type=int, default=10,
+                    help="engine rounds between FP64 accumulator resyncs inside the timed region (0 = none)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
