@@ -59,6 +59,18 @@ WORKLOADS = {
                            [(0.3, 0.1), (0.3, 0.3), (0.5, 0.1), (0.5, 0.3), (0.7, 0.1), (0.7, 0.3)][i % 6])
                           for i, L in enumerate([16, 16, 24, 24, 32, 32, 48, 48, 64, 64, 96, 96])]),
 }
+# the reference's own crystals (src/unit_cells.f90): BCC as bin/PT runs it (shell 1 only, J' = 0,
+# src/PT.f90:145,229-230) and hyper-kagome as bin/ISING does (src/ISING.f90:105), both with the
+# default interfacial DMI of calculateHeisenbergEnergy; run by the per-pass PT path on the
+# octant storage order (the persistent engine covers simple cubic)
+WORKLOADS["bcc"] = dict(cell="bcc", L=96, R=16, tmin=0.1, tmax=2.0, J=-1.0, D=0.5, B=0.2, K=0.0, move="ball", r=0.2,
+                        k=10, dmi="interfacial",
+                        desc="BCC 96^3 cells (2 atoms) x 16 PT replicas, T 0.1-2.0, J=1, interfacial D=0.5, B=0.2 z, "
+                             "shell 1")
+WORKLOADS["hk"] = dict(cell="hk", L=48, R=16, tmin=0.1, tmax=2.0, J=-1.0, D=0.3, B=0.1, K=0.0, move="ball", r=0.2,
+                       k=10, dmi="interfacial",
+                       desc="hyper-kagome 48^3 cells (12 atoms) x 16 PT replicas, T 0.1-2.0, J=1, interfacial D=0.3, "
+                            "B=0.1 z, shell 1")
 WORKLOADS["stats"] = dict(L=96, nz=96, scale=10, J=-1.0, D=0.5, B=0.25, K=0.0, move="ball", r=0.2, tmin=0.1,
                           desc="chainMesh_statistics on SC L=96 (96 slices): winding per slice, magnetisation and "
                                "the 60 x 20 skyrmion search on the middle slice's 960 x 960 interpolated density")
@@ -216,6 +228,10 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- reference (CPU) arm
+def oracle_cell(O, w):
+    return {"bcc": O.BCC_CELL, "hk": O.HYPER_KAGOME_CELL}.get(w.get("cell"), O.SC_CELL)
+
+
 def cpu_reference_rate(w, steps, warmup, threads, L_sample=None):
     """Throughput of the CPU restatement of Metropolis_mcs on the host cores: one sweep of
     one replica per step (numAtoms trials), the reference's parallel structure (OpenMP over
@@ -223,9 +239,10 @@ def cpu_reference_rate(w, steps, warmup, threads, L_sample=None):
     from oracle import oracle as O
     O.build()
     L = L_sample or w["L"]
-    m = O.Mesh.sc(L)
+    frac, (a, b, c, ab, bc, ca) = oracle_cell(O, w)
+    m = O.Mesh(frac, L, L, L, a, b, c, ab, bc, ca)
     m.init_uniform(0x15196)
-    p = O.Params(J=w["J"], Dz=w["D"], B=w["B"], K=w["K"], dmi_bulk=True)
+    p = O.Params(J=w["J"], Dz=w["D"], B=w["B"], K=w["K"], dmi_bulk=w.get("dmi", "bulk") == "bulk")
     beta = 1.0 / w["tmin"]
     for _ in range(warmup):
         m.metropolis_mcs_omp(beta, 1, p, w["r"], n_threads=threads, time_seed=1)
@@ -234,7 +251,8 @@ def cpu_reference_rate(w, steps, warmup, threads, L_sample=None):
         m.metropolis_mcs_omp(beta, 1, p, w["r"], n_threads=threads, time_seed=1)
     dt = time.perf_counter() - t0
     rate = steps * m.natoms / dt
-    return rate, f"{steps} sweep(s) of one SC L={L} replica ({m.natoms} trials each), {threads} threads"
+    return rate, (f"{steps} sweep(s) of one {w.get('cell', 'sc').upper()} L={L} replica ({m.natoms} trials each), "
+                  f"{threads} threads")
 
 
 def cpu_fast_rate(w, threads, L=64, sweeps=4):
@@ -279,7 +297,7 @@ def run_reference(args, w):
     line = {
         "metric": "spin-updates/s", "value": rate, "unit": "spin-updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * (w["L"] ** 3) / rate, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * (w["L"] ** 3) * cell_atoms(w) / rate, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "desc": w["desc"], "sample": "one replica per step"},
         "cpu_baseline": {"value": rate, "unit": "spin-updates/s", "cores": threads, "kind": "port",
@@ -327,6 +345,21 @@ def link_rates(torch, host, stream):
     del dev
     return {"h2d_gbs": nbytes / t_up / 1e6, "d2h_gbs": nbytes / t_down / 1e6,
             "bidir_gbs_each": nbytes / t_both / 1e6, "bidir_ms": t_both}
+
+
+def cell_atoms(w):
+    return {"bcc": 2, "hk": 12}.get(w.get("cell"), 1)
+
+
+def make_mesh(ib, w, L, R, dev):
+    """The workload's mesh: simple cubic, or the reference's BCC / hyper-kagome cell."""
+    if w.get("cell") == "bcc":
+        a, b, c, ab, bc, ca, f = ib.bcc_unit_cell()
+    elif w.get("cell") == "hk":
+        a, b, c, ab, bc, ca, f = ib.hyper_kagome_unit_cell()
+    else:
+        return ib.ChainMesh.simple_cubic(L, n_replicas=R, device=dev)
+    return ib.ChainMesh(L, L, L, f, a, b, c, ab, bc, ca, n_replicas=R, device=dev)
 
 
 def ensembles_of(args, w):
@@ -412,12 +445,12 @@ def run_gpu(args, w):
     for i in mine:
         L, R, D, B = spec[i]
         ens_id = i if split else rank * len(spec) + i
-        m = ib.ChainMesh.simple_cubic(L, n_replicas=R, device=dev)
+        m = make_mesh(ib, w, L, R, dev)
         m.set_stream(stream.cuda_stream)
         m.init_uniform(0x15196, ensemble=ens_id)
-        p = ib.params(J=w["J"], Dz=D, B=B, K=w["K"], dmi="bulk")
+        p = ib.params(J=w["J"], Dz=D, B=B, K=w["K"], dmi=w.get("dmi", "bulk"))
         members.append((m, 1.0 / ib.temperature_ladder(w["tmin"], w["tmax"], R), p, ens_id))
-    sites = sum(spec[i][0] ** 3 * spec[i][1] for i in mine)
+    sites = sum(spec[i][0] ** 3 * spec[i][1] for i in mine) * cell_atoms(w)
     sites_job = sum(L ** 3 * R for L, R, _, _ in spec) if split else world * sites
     updates_per_step = sites * k
 
@@ -436,7 +469,8 @@ def run_gpu(args, w):
     sched_info = {}
     eng = None
     n_chunks = 1
-    if args.engine == "ensembles":
+    engine = "pt" if w.get("cell") else args.engine      # the engine runs simple cubic only
+    if engine == "ensembles":
         eng = ib.Ensembles(members, seed=0x15196, move=move, r=w["r"]) if members else None
         if eng:
             eng.set_stream(stream.cuda_stream)
@@ -473,7 +507,8 @@ def run_gpu(args, w):
         energies = lambda: [pt.energies()]
         group, per_round, kern_id = pt.schedule(k)
         sched_info = {"l2_group_replicas": group, "colour_pass_launches_per_round": per_round,
-                      "kernel": {0: "stencil", 1: "k_cb_sweep", 2: "k_cb_tma"}[kern_id]}
+                      "kernel": {0: "k_octant_colour" if m.layout == "octant" else "k_general_colour",
+                                 1: "k_cb_sweep", 2: "k_cb_tma"}[kern_id], "layout": m.layout}
         kernel_name = sched_info["kernel"]
         launches_timed = args.steps * (per_round + 3)   # colour passes + fold + exchange + advance
         closers = [pt]
@@ -497,7 +532,7 @@ def run_gpu(args, w):
     # resync interval) and the resyncs (one energy pass each, well under 1 % of the region),
     # so the region's duration stands for the launches' duration; with --engine pt the
     # colour-pass kernel is timed alone over relax sweeps
-    if args.engine == "ensembles":
+    if engine == "ensembles":
         launch_ms = ms_local / max(n_chunks, 1)
         bytes_per_launch = BYTES_PER_UPDATE * updates_per_step * args.steps / max(n_chunks, 1)
     else:
@@ -605,9 +640,10 @@ def run_gpu(args, w):
         L_cpu = max(L for L, _, _, _ in spec)
         rate, sample = cpu_reference_rate(w, 2, 1, threads, L_sample=L_cpu)
         cpu = {"value": rate, "unit": "spin-updates/s", "cores": threads, "kind": "port", "sample": sample}
-        rate, sample = cpu_fast_rate(w, threads, L=L_cpu)
-        cpu_fast = {"value": rate, "unit": "spin-updates/s", "cores": threads, "kind": "optimised port",
-                    "sample": sample}
+        if not w.get("cell"):     # the fast CPU form is the simple-cubic checkerboard
+            rate, sample = cpu_fast_rate(w, threads, L=L_cpu)
+            cpu_fast = {"value": rate, "unit": "spin-updates/s", "cores": threads, "kind": "optimised port",
+                        "sample": sample}
 
     for c in closers:
         c.close()
@@ -625,8 +661,8 @@ def run_gpu(args, w):
             "data": "synthetic (uniform random initial spins from Philox, seed 0x15196)",
             "config": {"workload": args.workload, "desc": w["desc"], "ensembles": len(spec),
                        "lattices": sorted({L for L, _, _, _ in spec}), "replicas": sum(R for _, R, _, _ in spec),
-                       "sweeps_per_step": k, "sites": sites_job, "engine": args.engine,
-                       "resync_every_rounds": args.resync_every if args.engine == "ensembles" else None,
+                       "sweeps_per_step": k, "sites": sites_job, "engine": engine,
+                       "resync_every_rounds": args.resync_every if engine == "ensembles" else None,
                        "parallelism": (f"whole ensembles over {world} ranks" if split
                                        else f"replicas x{world} (independent ensembles)"),
                        "l2": "state larger than L2 (no flush)" if sites * 12 > 126e6 else "state fits L2; no flush"},

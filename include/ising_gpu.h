@@ -70,7 +70,10 @@ typedef struct {
     int n_shells;            /* neighbour shells built (default 2) */
     int n_replicas;          /* replica spin buffers held on the device */
     int shell_size[2];       /* entries per atom in shells 1 and 2 (sublattice 0) */
-    int checkerboard;        /* 1 if the SC 2-colour fast path applies (even nx, ny; nz % 4 == 0) */
+    int checkerboard;        /* storage order of the spins on the device: 1 the SC 2-colour fast path
+                                (even nx, ny; nz % 4 == 0); 2 the octant order of other crystals
+                                with even extents (colour classes = cell octant x sublattice
+                                group, each one contiguous range); 0 the reference atom order */
     double a_vec[3], b_vec[3], c_vec[3];
 } ising_mesh_info;
 
@@ -150,8 +153,11 @@ int ising_params_reference(int which, double J, double J_prime, double Dz, doubl
                            double B, ising_params* p);
 
 /* Colour class of every atom as the sweep uses it for the Hamiltonian p: the checkerboard
- * (x+y+z)&1 on simple-cubic meshes with even nx, ny, nz % 4 == 0 and no J', a verified greedy
- * colouring of the active shells otherwise.  No reference counterpart: Metropolis_mcs draws random parity cells
+ * (x+y+z)&1 on simple-cubic meshes with even nx, ny, nz % 4 == 0 and no J'; on other crystals
+ * with even extents whose shells 1-2 never join one sublattice at an all-even non-zero cell
+ * offset (BCC and hyper-kagome, src/unit_cells.f90:7-77), class octant * groups + group of the
+ * cell octant (x&1, y&1, z&1) and a sublattice group (sublattices bonded at an all-even offset
+ * get different groups); a verified greedy colouring of the active shells otherwise.  No reference counterpart: Metropolis_mcs draws random parity cells
  * instead (src/energyMin.f90:288-316). */
 int ising_mesh_colouring(ising_mesh* mesh, const ising_params* p, int* colour_of, int* n_colours);
 
@@ -187,7 +193,8 @@ int ising_observables(const ising_mesh* mesh, const ising_params* p, double* e, 
 
 /* Replaces Metropolis_mcs(chainMesh, beta, numMCSSweeps, J, J', Dz, Dz', B, r, lockArray,
  * demag) (src/energyMin.f90:234-374).  A sweep visits every atom once through colour
- * classes (checkerboard on even simple-cubic meshes, greedy colouring otherwise) with
+ * classes (checkerboard on even simple-cubic meshes, octant classes on other crystals with
+ * even extents, greedy colouring otherwise) with
  * Philox keyed by (seed, ensemble 0, replica, sweep, atom); the per-replica sweep counter
  * lives in the handle so successive calls continue the stream.  r > 0 selects the ball
  * move of radius r, r <= 0 the uniform move.  lockArray has no counterpart (no locks). */

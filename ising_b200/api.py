@@ -118,7 +118,8 @@ class ChainMesh:
         self.numCellsX, self.numCellsY, self.numCellsZ = info.nx, info.ny, info.nz
         self.n_sub = info.n_sub
         self.n_replicas = info.n_replicas
-        self.checkerboard = bool(info.checkerboard)
+        self.checkerboard = info.checkerboard == 1
+        self.layout = {0: "reference", 1: "checkerboard", 2: "octant"}.get(info.checkerboard, str(info.checkerboard))
         self.a_vec = np.array(info.a_vec[:])
         self.b_vec = np.array(info.b_vec[:])
         self.c_vec = np.array(info.c_vec[:])

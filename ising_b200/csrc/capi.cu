@@ -198,14 +198,36 @@ int sc_dmi(const ising_mesh* m, const ising_params& p, HamDev* h, int* kind) {
     return ISING_OK;
 }
 
+// Colour classes of a mesh that is not on the checkerboard path: the octant classes
+// (octant o, sublattice group g) as class o * groups + g for octant-layout meshes, else a
+// greedy colouring of the active shells' bonds.
+int host_colouring(ising_mesh* m, bool shell2, Colouring& c) {
+    if (!c.host_colour.empty()) return ISING_OK;
+    const Lattice& L = m->lat;
+    if (m->layout.cb == 2) {
+        const int ng = (int)m->oct_rank0.size() - 1;
+        c.host_colour.resize(L.natoms);
+        for (int64_t at = 0; at < L.natoms; ++at) {
+            int ix, iy, iz, sb;
+            L.cell_of(at, &ix, &iy, &iz, &sb);
+            const int rk = m->layout.srank[sb];
+            int g = 0;
+            while (rk >= m->oct_rank0[g + 1]) ++g;
+            c.host_colour[at] = (((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1)) * ng + g;
+        }
+        c.ncol = 8 * ng;
+        return ISING_OK;
+    }
+    int ncol = 0;
+    ISG_TRY(greedy_colouring(L, shell2, &c.host_colour, &ncol));
+    c.ncol = ncol;
+    return ISING_OK;
+}
+
 int ensure_colouring(ising_mesh* m, bool shell2, Colouring** out) {
     Colouring& c = m->colour[shell2 ? 1 : 0];
     if (c.d_sites) { *out = &c; return ISING_OK; }
-    if (c.host_colour.empty()) {
-        int ncol = 0;
-        ISG_TRY(greedy_colouring(m->lat, shell2, &c.host_colour, &ncol));
-        c.ncol = ncol;
-    }
+    ISG_TRY(host_colouring(m, shell2, c));
     c.class_start.assign(c.ncol + 1, 0);
     for (int v : c.host_colour) c.class_start[v + 1]++;
     for (int k = 0; k < c.ncol; ++k) c.class_start[k + 1] += c.class_start[k];
@@ -235,7 +257,7 @@ struct SweepPlan {
 int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots, int* count) {
     plan->ham = make_ham(p);
     const bool sh2 = uses_shell2(m->lat, p);
-    if (m->layout.cb && !sh2) {
+    if (m->layout.cb == 1 && !sh2) {
         plan->sc = true;
         ISG_TRY(sc_dmi(m, p, &plan->ham, &plan->dmi_kind));
         const Lattice& Lt = m->lat;
@@ -253,8 +275,14 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
     ISG_TRY(upload_stencil(m, p, false, slots, count));
     ISG_TRY(ensure_colouring(m, sh2, &plan->col));
     int tot = 0;
-    for (int k = 0; k < plan->col->ncol; ++k)
-        tot += general_slots_for(plan->col->class_start[k + 1] - plan->col->class_start[k]);
+    if (m->layout.cb == 2) {
+        const int ng = (int)m->oct_rank0.size() - 1;
+        for (int k = 0; k < 8 * ng; ++k)
+            tot += octant_slots_for(m->layout.q8 * (m->oct_rank0[k % ng + 1] - m->oct_rank0[k % ng]));
+    } else {
+        for (int k = 0; k < plan->col->ncol; ++k)
+            tot += general_slots_for(plan->col->class_start[k + 1] - plan->col->class_start[k]);
+    }
     plan->slots_per_rep = tot;
     return ISING_OK;
 }
@@ -321,6 +349,20 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
     g.seed = seed; g.ensemble = ensemble; g.move = move; g.r = (float)r;
     g.ham = plan.ham; g.st = StencilDev{plan.d_slots, plan.d_count, L.nsub}; g.layout = m->layout;
     g.partials = partials; g.slots_per_rep = plan.slots_per_rep; g.status = m->d_status;
+    if (m->layout.cb == 2) {   // octant classes: contiguous storage ranges
+        const int ng = (int)m->oct_rank0.size() - 1;
+        for (int sw = 0; sw < n_sweeps; ++sw) {
+            g.sweep_offset = sw0 + (uint32_t)sw;
+            int slot = 0;
+            for (int k = 0; k < 8 * ng; ++k) {
+                const int gi = k % ng, r0 = m->oct_rank0[gi], nr = m->oct_rank0[gi + 1] - r0;
+                g.slot_base = slot;
+                ISG_TRY(launch_octant_colour(g, k / ng, r0, nr, m->stream));
+                slot += octant_slots_for(m->layout.q8 * nr);
+            }
+        }
+        return ISING_OK;
+    }
     for (int sw = 0; sw < n_sweeps; ++sw) {
         g.sweep_offset = sw0 + (uint32_t)sw;
         int slot = 0;
@@ -411,6 +453,25 @@ extern "C" int ising_mesh_create(const float* frac, int nsub, int nx, int ny, in
     {
         const Lattice& L = m->lat;
         m->layout = Layout{m->checkerboard && L.nz % 4 == 0 ? 1 : 0, L.nx, L.ny, L.nz, L.nsub, L.natoms / 2};
+        std::vector<int> grp;
+        int ng = 0;
+        // other crystals: octant order when the octant colouring applies (ranks grouped by
+        // sublattice group, so each colour class is one contiguous range)
+        if (!m->checkerboard && octant_groups(L, &grp, &ng)) {
+            m->layout.cb = 2;
+            m->layout.q8 = L.ncells / 8;
+            int next = 0;
+            m->oct_rank0.assign(1, 0);
+            for (int g = 0; g < ng; ++g) {
+                for (int sb = 0; sb < L.nsub; ++sb)
+                    if (grp[sb] == g) {
+                        m->layout.srank[sb] = (uint8_t)next;
+                        m->layout.sofr[next] = (uint8_t)sb;
+                        ++next;
+                    }
+                m->oct_rank0.push_back(next);
+            }
+        }
     }
     if (device == -1) {  // lattice tables only
         m->device = -1;
@@ -540,7 +601,7 @@ extern "C" int ising_mesh_colouring(ising_mesh* m, const ising_params* p, int* c
     ISG_TRY(validate_params(p));
     const Lattice& L = m->lat;
     const bool sh2 = uses_shell2(L, *p);
-    if (m->layout.cb && !sh2) {
+    if (m->layout.cb == 1 && !sh2) {
         for (int64_t a = 0; a < L.natoms; ++a) {
             int ix, iy, iz, s;
             L.cell_of(a, &ix, &iy, &iz, &s);
@@ -550,11 +611,7 @@ extern "C" int ising_mesh_colouring(ising_mesh* m, const ising_params* p, int* c
         return ISING_OK;
     }
     Colouring& c = m->colour[sh2 ? 1 : 0];
-    if (c.host_colour.empty()) {
-        int ncol = 0;
-        ISG_TRY(greedy_colouring(L, sh2, &c.host_colour, &ncol));
-        c.ncol = ncol;
-    }
+    ISG_TRY(host_colouring(m, sh2, c));
     std::memcpy(colour_of, c.host_colour.data(), L.natoms * sizeof(int));
     *n_colours = c.ncol;
     return ISING_OK;
@@ -1845,7 +1902,7 @@ extern "C" int ising_ensembles_create(int n, const ising_ensemble_desc* desc, co
             if (desc[f].mesh == d.mesh) return fail(ISING_ERR_ARG, "each ensemble needs its own mesh");
         ISG_TRY(validate_params(&d.params));
         const Lattice& L = d.mesh->lat;
-        if (!d.mesh->layout.cb || uses_shell2(L, d.params))
+        if (d.mesh->layout.cb != 1 || uses_shell2(L, d.params))
             return fail(ISING_ERR_UNSUPPORTED, "the batched engine needs colour-separated simple-cubic meshes "
                                                "(even nx, ny; nz % 4 == 0) and shell-1 couplings");
         if (L.nx > 65535 || L.natoms >= (int64_t)1 << 31) return fail(ISING_ERR_ARG, "mesh too large for the engine");

@@ -119,14 +119,28 @@ struct StencilDev {
 // cb = 1 (simple-cubic meshes with even extents): colour-separated -- the sites with
 // (x+y+z)&1 == 0 first, then colour 1; inside a colour, row order (x, y) with the packed
 // z index z>>1, so a colour pass reads and writes whole sectors of its own colour.
+// cb = 2 (other crystals with even extents whose couplings never join two sites of one
+// sublattice at an all-even non-zero cell offset): octant order -- blocks (octant,
+// sublattice rank) of q8 = cells/8 sites, octant = (x&1, y&1, z&1), inside a block the
+// packed cell ((x>>1, y>>1), z>>1).  A colour class (octant, sublattice group) is then one
+// contiguous range (the sublattices of a group have consecutive ranks), and the neighbours
+// of consecutive sites through one stencil slot are consecutive as well.
 struct Layout {
     int cb;
     int nx, ny, nz, nsub;
-    int64_t half;   // sites per colour (cb = 1)
+    int64_t half;             // sites per colour (cb = 1)
+    int64_t q8;               // cells per octant (cb = 2)
+    uint8_t srank[kMaxSub];   // cb = 2: storage rank of each sublattice
+    uint8_t sofr[kMaxSub];    // cb = 2: sublattice of each rank
 };
 
 __host__ __device__ __forceinline__ int64_t sidx(const Layout& L, int ix, int iy, int iz, int sub) {
     if (!L.cb) return (((int64_t)ix * L.ny + iy) * L.nz + iz) * L.nsub + sub;
+    if (L.cb == 2) {
+        const int oct = ((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1);
+        const int64_t packed = ((int64_t)(ix >> 1) * (L.ny >> 1) + (iy >> 1)) * (L.nz >> 1) + (iz >> 1);
+        return ((int64_t)oct * L.nsub + L.srank[sub]) * L.q8 + packed;
+    }
     const int c = (ix + iy + iz) & 1;
     return c * L.half + ((int64_t)ix * L.ny + iy) * (L.nz >> 1) + (iz >> 1);
 }
@@ -134,10 +148,12 @@ __host__ __device__ __forceinline__ int64_t sidx(const Layout& L, int ix, int iy
 // storage index of a reference-order atom index
 __host__ __device__ __forceinline__ int64_t sidx_atom(const Layout& L, int64_t atom) {
     if (!L.cb) return atom;
-    const int iz = (int)(atom % L.nz);
-    const int64_t row = atom / L.nz;
+    const int sub = (int)(atom % L.nsub);
+    const int64_t cell = atom / L.nsub;
+    const int iz = (int)(cell % L.nz);
+    const int64_t row = cell / L.nz;
     const int iy = (int)(row % L.ny), ix = (int)(row / L.ny);
-    return sidx(L, ix, iy, iz, 0);
+    return sidx(L, ix, iy, iz, sub);
 }
 
 // Per-replica running accumulators: E, Mx, My, Mz.

@@ -66,6 +66,11 @@ int greedy_colouring(const Lattice& L, bool use_shell2, std::vector<int>* colour
 // extents, so the 2-colour checkerboard fast path applies.
 bool is_checkerboard_sc(const Lattice& L);
 
+// Sublattice groups of the octant colouring (class = cell octant x sublattice group) of a
+// general crystal; false when the octant colouring does not apply (odd extents, or a bond of
+// shells 1-2 between two sites of one sublattice at an all-even non-zero cell offset).
+bool octant_groups(const Lattice& L, std::vector<int>* group, int* ngroups);
+
 // ---------------------------------------------------------------- device-side handle
 struct Colouring {
     int ncol = 0;
@@ -100,6 +105,7 @@ struct ising_mesh {
     double* d_winding_tmp = nullptr;     // per-slice winding results
     bool checkerboard = false;
     isg::Layout layout{};                // storage order of the spin planes
+    std::vector<int> oct_rank0;          // octant layout: first storage rank of each sublattice group (+ end)
     isg::Colouring colour[2];            // [0]: shell 1 bonds, [1]: shells 1+2
     // cached device stencils keyed by the Hamiltonian that filled their weights
     isg::Slot* d_slots = nullptr;
@@ -176,6 +182,10 @@ struct GeneralLaunch {
     int* status;
 };
 int launch_general_colour(const GeneralLaunch& a, cudaStream_t s);
+// One class (octant, sublattice group) of an octant-layout mesh: sites of storage ranks
+// [rank0, rank0 + nrank) of that octant (a.sites and a.n_sites unused).
+int launch_octant_colour(const GeneralLaunch& a, int octant, int rank0, int nrank, cudaStream_t s);
+int octant_slots_for(int64_t n_sites);
 int general_slots_for(int n_sites);
 
 struct ReduceLaunch {

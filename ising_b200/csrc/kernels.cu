@@ -69,6 +69,34 @@ __device__ __forceinline__ f3 stencil_field(const float* sx, const float* sy, co
     return h;
 }
 
+// Metropolis update of one site (ix, iy, iz, sub), reference atom index `at`, with the local
+// field of its stencil; accepted moves add to the running sums.
+template <int MOVE>
+__device__ __forceinline__ void general_site(const GeneralLaunch& a, const Slot* sl, const int* cnt, float* sx,
+                                             float* sy, float* sz, int64_t at, int ix, int iy, int iz, int sub,
+                                             uint32_t sweep, int rep, float beta, float& de, float& dmx, float& dmy,
+                                             float& dmz) {
+    const HamDev& H = a.ham;
+    f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.layout);
+    h.z -= H.Bz;
+    const int64_t si = sidx(a.layout, ix, iy, iz, sub);
+    const f3 s = {sx[si], sy[si], sz[si]};
+    const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)at, sweep, (uint32_t)rep, (a.ensemble << 8) | kTagSweep),
+                                    philox_key(a.seed));
+    const f3 sp = propose<MOVE>(s, u01(r4.x), u01(r4.y), u01(r4.z), a.r);
+    float dE = (sp.x - s.x) * h.x + (sp.y - s.y) * h.y + (sp.z - s.z) * h.z;
+    if (H.K != 0.f) {
+        const float e1 = sp.x * H.kx + sp.y * H.ky + sp.z * H.kz;
+        const float e0 = s.x * H.kx + s.y * H.ky + s.z * H.kz;
+        dE -= H.K * (e1 * e1 - e0 * e0);
+    }
+    if (!(dE == dE)) atomicOr(a.status, kStatNan);
+    if ((dE <= 0.f) || (u01(r4.w) < __expf(-beta * dE))) {
+        sx[si] = sp.x; sy[si] = sp.y; sz[si] = sp.z;
+        de += dE; dmx += sp.x - s.x; dmy += sp.y - s.y; dmz += sp.z - s.z;
+    }
+}
+
 template <int MOVE>
 __global__ void __launch_bounds__(kGenThreads) k_general_colour(GeneralLaunch a) {
     extern __shared__ unsigned char smem_raw[];
@@ -85,7 +113,6 @@ __global__ void __launch_bounds__(kGenThreads) k_general_colour(GeneralLaunch a)
     float* __restrict__ sz = sy + N;
     const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
     const float beta = (float)a.beta_rep[rep];
-    const HamDev& H = a.ham;
     float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
     const int base = blockIdx.x * blockDim.x * kGenSitesPerThread;
     for (int it = 0; it < kGenSitesPerThread; ++it) {
@@ -94,25 +121,7 @@ __global__ void __launch_bounds__(kGenThreads) k_general_colour(GeneralLaunch a)
         const int64_t at = a.sites[t];
         int ix, iy, iz, sub;
         decode_atom(at, a.nsub, a.ny, a.nz, &ix, &iy, &iz, &sub);
-        f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.layout);
-        h.z -= H.Bz;
-        const int64_t si = sidx(a.layout, ix, iy, iz, sub);
-        const f3 s = {sx[si], sy[si], sz[si]};
-        const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)at, sweep, (uint32_t)rep,
-                                                   (a.ensemble << 8) | kTagSweep),
-                                        philox_key(a.seed));
-        const f3 sp = propose<MOVE>(s, u01(r4.x), u01(r4.y), u01(r4.z), a.r);
-        float dE = (sp.x - s.x) * h.x + (sp.y - s.y) * h.y + (sp.z - s.z) * h.z;
-        if (H.K != 0.f) {
-            const float e1 = sp.x * H.kx + sp.y * H.ky + sp.z * H.kz;
-            const float e0 = s.x * H.kx + s.y * H.ky + s.z * H.kz;
-            dE -= H.K * (e1 * e1 - e0 * e0);
-        }
-        if (!(dE == dE)) atomicOr(a.status, kStatNan);
-        if ((dE <= 0.f) || (u01(r4.w) < __expf(-beta * dE))) {
-            sx[si] = sp.x; sy[si] = sp.y; sz[si] = sp.z;
-            de += dE; dmx += sp.x - s.x; dmy += sp.y - s.y; dmz += sp.z - s.z;
-        }
+        general_site<MOVE>(a, sl, cnt, sx, sy, sz, at, ix, iy, iz, sub, sweep, rep, beta, de, dmx, dmy, dmz);
     }
     if (a.partials) {
         __shared__ double tot[4];
@@ -122,6 +131,72 @@ __global__ void __launch_bounds__(kGenThreads) k_general_colour(GeneralLaunch a)
             p[0] += tot[0]; p[1] += tot[1]; p[2] += tot[2]; p[3] += tot[3];
         }
     }
+}
+
+// One class of the octant colouring: thread t of the class updates the site of storage rank
+// rank0 + t / q8 at packed cell t % q8 of the octant, so the own reads and writes of a warp
+// are consecutive and so are its reads through each stencil slot (the packed cells of a
+// neighbour octant move in step).  Same arithmetic and Philox keys as k_general_colour.
+template <int MOVE>
+__global__ void __launch_bounds__(kGenThreads) k_octant_colour(GeneralLaunch a, int oct, int rank0, int nrank) {
+    extern __shared__ unsigned char smem_raw[];
+    Slot* sl = reinterpret_cast<Slot*>(smem_raw);
+    int* cnt = reinterpret_cast<int*>(sl + a.st.nsub * kMaxSlots);
+    for (int q = threadIdx.x; q < a.st.nsub * kMaxSlots; q += blockDim.x) sl[q] = a.st.slots[q];
+    for (int q = threadIdx.x; q < a.st.nsub; q += blockDim.x) cnt[q] = a.st.count[q];
+    __syncthreads();
+    const int rl = blockIdx.y;
+    const int rep = a.rep_first + rl;
+    const int64_t N = a.natoms;
+    float* __restrict__ sx = a.spins + (int64_t)rl * 3 * N;
+    float* __restrict__ sy = sx + N;
+    float* __restrict__ sz = sy + N;
+    const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
+    const float beta = (float)a.beta_rep[rep];
+    const Layout& L = a.layout;
+    const int64_t q8 = L.q8, n = q8 * nrank;
+    const int hy = a.ny >> 1, hz = a.nz >> 1;
+    const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
+    float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
+    const int64_t base = (int64_t)blockIdx.x * blockDim.x * kGenSitesPerThread;
+    for (int it = 0; it < kGenSitesPerThread; ++it) {
+        const int64_t t = base + it * blockDim.x + threadIdx.x;
+        if (t >= n) break;
+        const int rk = rank0 + (int)(t / q8);
+        const int64_t pc = t - (int64_t)(rk - rank0) * q8;
+        const int Z = (int)(pc % hz);
+        const int64_t r = pc / hz;
+        const int Y = (int)(r % hy), X = (int)(r / hy);
+        const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z + oz, sub = L.sofr[rk];
+        const int64_t at = (((int64_t)ix * a.ny + iy) * a.nz + iz) * a.nsub + sub;
+        general_site<MOVE>(a, sl, cnt, sx, sy, sz, at, ix, iy, iz, sub, sweep, rep, beta, de, dmx, dmy, dmz);
+    }
+    if (a.partials) {
+        __shared__ double tot[4];
+        block_sum4<double>(de, dmx, dmy, dmz, tot);
+        if (threadIdx.x == 0) {
+            double* p = a.partials + ((int64_t)rep * a.slots_per_rep + a.slot_base + blockIdx.x) * 4;
+            p[0] += tot[0]; p[1] += tot[1]; p[2] += tot[2]; p[3] += tot[3];
+        }
+    }
+}
+
+int octant_slots_for(int64_t n_sites) {
+    const int64_t per = (int64_t)kGenThreads * kGenSitesPerThread;
+    return (int)((n_sites + per - 1) / per);
+}
+
+int launch_octant_colour(const GeneralLaunch& a, int oct, int rank0, int nrank, cudaStream_t s) {
+    const int64_t n = a.layout.q8 * nrank;
+    if (n <= 0) return ISING_OK;
+    if (oct < 0 || oct > 7 || rank0 < 0 || nrank < 1 || rank0 + nrank > a.nsub)
+        return fail(ISING_ERR_ARG, "octant class out of range");
+    dim3 g(octant_slots_for(n), a.n_rep), b(kGenThreads);
+    size_t sm = (size_t)a.st.nsub * kMaxSlots * sizeof(Slot) + kMaxSub * sizeof(int);
+    if (a.move == 0) k_octant_colour<0><<<g, b, sm, s>>>(a, oct, rank0, nrank);
+    else k_octant_colour<1><<<g, b, sm, s>>>(a, oct, rank0, nrank);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
 }
 
 int launch_general_colour(const GeneralLaunch& a, cudaStream_t s) {

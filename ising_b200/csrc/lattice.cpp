@@ -330,6 +330,43 @@ int greedy_colouring(const Lattice& L, bool use_shell2, std::vector<int>* colour
     return ISING_OK;
 }
 
+// Octant colouring of a general crystal: class (cell octant (x&1, y&1, z&1), sublattice
+// group).  Valid when every extent is even (periodic wraps keep parities) and no bond of
+// shells 1-2 joins two sites of one sublattice at an all-even non-zero cell offset; two
+// sublattices joined by a bond at an all-even offset (including 0) go to different groups
+// (greedy colouring of that small graph).  A bond of a site to itself, which the reference's
+// shell search puts into shell 2 of BCC cells, does not constrain the colouring: the update
+// reads the site's own old value there, as a sequential sweep does.
+bool octant_groups(const Lattice& L, std::vector<int>* group, int* ngroups) {
+    if ((L.nx & 1) || (L.ny & 1) || (L.nz & 1) || L.nsub > kMaxSub || L.nsub < 1) return false;
+    std::vector<std::vector<char>> conflict(L.nsub, std::vector<char>(L.nsub, 0));
+    for (int sh = 0; sh < 2; ++sh)
+        for (int s = 0; s < L.nsub; ++s)
+            for (const NbrSlot& q : L.shell[sh][s]) {
+                if ((q.dx & 1) || (q.dy & 1) || (q.dz & 1)) continue;   // different octant
+                if (q.sub == s) {
+                    if (q.dx || q.dy || q.dz) return false;
+                    continue;
+                }
+                conflict[s][q.sub] = conflict[q.sub][s] = 1;
+            }
+    group->assign(L.nsub, -1);
+    int ng = 0;
+    for (int s = 0; s < L.nsub; ++s) {
+        int g = 0;
+        for (;; ++g) {
+            bool ok = true;
+            for (int t = 0; t < s; ++t)
+                if ((*group)[t] == g && conflict[s][t]) { ok = false; break; }
+            if (ok) break;
+        }
+        (*group)[s] = g;
+        ng = std::max(ng, g + 1);
+    }
+    *ngroups = ng;
+    return true;
+}
+
 bool is_checkerboard_sc(const Lattice& L) {
     if (L.nsub != 1) return false;
     if ((L.nx & 1) || (L.ny & 1) || (L.nz & 1)) return false;

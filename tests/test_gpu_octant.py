@@ -1,0 +1,83 @@
+"""The octant storage order and colour classes of general crystals (BCC and hyper-kagome meshes
+with even extents, the reference's own lattices: src/PT.f90:145, src/ISING.f90:105) against
+the FP64 oracle: spins round-trip through the layout, per-site and total energies and winding
+numbers equal the oracle's, and sweeps replay the oracle's colour passes (same Philox keys,
+the product's colour classes) decision for decision, with J' on (BCC's shell 2 holds each
+site itself, which the octant classes accept) and off, both moves, over several sweeps."""
+import numpy as np
+import pytest
+
+from test_gpu_parity import _both_params, _pair, _random_spins
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("BCC", (6, 6, 4), dict(J=-1.0, Dz=0.4, B=0.1, bulk=True), 1, 0.2, 1.5),
+    ("BCC", (4, 6, 8), dict(J=-1.0, Jp=0.2, Dz=0.3, B=0.2, K=0.05, bulk=False), 0, 0.0, 2.0),
+    ("HK", (4, 4, 4), dict(J=-1.0, Dz=0.3, B=0.1, bulk=False), 1, 0.25, 1.0),
+    ("HK", (4, 6, 4), dict(J=1.0, Jp=0.1, Dz=0.2, B=0.3, bulk=True), 0, 0.0, 3.0),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_octant_layout_energies_and_winding(oracle, ib, cuda_ok, case):
+    kind, dims, h, _, _, _ = CASES[case]
+    om, pm = _pair(oracle, ib, kind, dims, n_replicas=2)
+    assert pm.layout == "octant"
+    s = _random_spins(om.natoms, 300 + case)
+    om.set_spins(s)
+    pm.set_spins(s, 1)
+    np.testing.assert_array_equal(pm.get_spins(1), s)
+    op, pp = _both_params(oracle, ib, **h)
+    rng = np.random.default_rng(case)
+    atoms = rng.choice(om.natoms, size=min(300, om.natoms), replace=False)
+    sp = _random_spins(len(atoms), 900 + case)
+    go, gn = ib.local_energy_batch(pm, atoms, sp, pp, replica=1)
+    for k, a in enumerate(atoms):
+        o, n = om.local_energy(int(a), op, sp[k])
+        scale = 1.0 + abs(o)
+        assert abs(go[k] - o) < 1e-6 * scale * 10 and abs(gn[k] - n) < 1e-6 * scale * 10, (a, go[k], o)
+    e, _ = ib.observables(pm, pp)
+    assert abs(e[1] - om.canonical_energy(op)) < 1e-6 * om.natoms
+    q = ib.winding_all_slices(pm, 1)
+    for z in range(1, dims[2] + 1):
+        assert abs(q[z - 1] - om.winding_number(z)) < 1e-9
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_octant_sweeps_replay_the_oracle(oracle, ib, cuda_ok, case):
+    kind, dims, h, move, r, beta = CASES[case]
+    om, pm = _pair(oracle, ib, kind, dims)
+    s = _random_spins(om.natoms, 500 + case)
+    om.set_spins(s)
+    pm.set_spins(s)
+    op, pp = _both_params(oracle, ib, **h)
+    col, ncol = pm.colouring(pp)
+    assert ncol % 8 == 0
+    seed = 0x0C7A + case
+    key = oracle.SweepKey(seed=seed, ensemble=0, replica=0, move=move, r=r, philox_rounds=10)
+    n_sweeps = 3
+    ib.metropolis_mcs(pm, beta, n_sweeps, 0, 0, 0, 0, 0, r if move == 1 else 0.0, seed=seed, p=pp)
+    for sw in range(n_sweeps):
+        for c in range(ncol):
+            om.colour_pass(col, c, sw, beta, op, key)
+    diff = np.abs(pm.get_spins(0) - om.spins).max(axis=1)
+    # FP32 against FP64: a decision flips only where ln u + beta dE is within rounding of 0,
+    # and a flipped site changes its neighbours' later decisions
+    assert (diff > 2e-4).sum() <= max(3, om.natoms // 400), int((diff > 2e-4).sum())
+
+
+def test_octant_pt_accumulators_track_recomputed_energies(oracle, ib, cuda_ok):
+    om, pm = _pair(oracle, ib, "BCC", (8, 8, 6), n_replicas=4)
+    pm.init_uniform(5)
+    op, pp = _both_params(oracle, ib, J=-1.0, Dz=0.5, B=0.2, bulk=True)
+    pt = ib.ParallelTempering(pm, 1.0 / ib.temperature_ladder(0.2, 2.0, 4), pp, seed=3, move=ib._lib.MOVE_BALL)
+    pt.run(5, 6)
+    e_run, m_run = pt.energies()
+    pt.resync()
+    e_new, m_new = pt.energies()
+    assert np.max(np.abs(e_run - e_new)) < 1e-5 * pm.numAtoms
+    assert np.max(np.abs(m_run - m_new)) < 1e-5 * pm.numAtoms
+    for r in range(4):
+        om.set_spins(pm.get_spins(r))
+        assert abs(e_new[r] - om.canonical_energy(op)) < 1e-6 * pm.numAtoms

@@ -78,20 +78,40 @@ def test_non_orthogonal_cell_sets(oracle, ib):
 
 
 def test_colouring_is_independent(oracle, ib):
-    for kind, dims in (("SC", (6, 6, 6)), ("SC", (5, 5, 5)), ("BCC", (4, 4, 4)), ("HK", (4, 4, 4))):
+    """Every colour class is an independent set of the active shells' bonds (a bond of a site
+    to itself, which the reference's shell search gives BCC cells in shell 2, excepted).  Even
+    BCC and hyper-kagome meshes take the octant classes: class = octant * groups + group with
+    octant = (x&1, y&1, z&1) of the cell; odd meshes a greedy colouring."""
+    cases = (("SC", (6, 6, 6)), ("SC", (5, 5, 5)), ("BCC", (4, 4, 4)), ("BCC", (6, 4, 8)), ("BCC", (3, 4, 3)),
+             ("HK", (4, 4, 4)), ("HK", (4, 6, 4)), ("HK", (3, 3, 3)))
+    for kind, dims in cases:
         frac, (a, b, c, ab, bc, ca) = _cell(oracle, kind)
         pm = ib.ChainMesh(*dims, frac, a, b, c, ab, bc, ca, device=-1)
+        even = all(d % 2 == 0 for d in dims)
+        assert pm.layout == ("checkerboard" if kind == "SC" and dims[2] % 4 == 0 and even
+                             else "octant" if kind != "SC" and even else "reference"), (kind, dims, pm.layout)
         for Jp in (0.0, 0.2):
             col, n = pm.colouring(ib.params(J=-1.0, J_prime=Jp))
             shells = (0, 1) if Jp else (0,)
             for atom in range(pm.numAtoms):
                 for s in shells:
                     nb = pm.neighbours(atom, s)
-                    assert np.all(col[nb] != col[atom])
+                    nb = nb[nb != atom]
+                    assert np.all(col[nb] != col[atom]), (kind, dims, Jp, atom)
             if kind == "SC" and dims[0] % 4 == 0 and Jp == 0.0:
                 assert n == 2 and pm.checkerboard
-            deg = sum(len(pm.neighbours(0, s)) for s in shells)
-            assert n <= deg + 1  # greedy bound
+            if pm.layout == "octant":
+                assert n % 8 == 0
+                nsub = len(frac)
+                for atom in range(0, pm.numAtoms, 7):
+                    cell, sub = divmod(atom, nsub)
+                    iz = cell % dims[2]
+                    iy = (cell // dims[2]) % dims[1]
+                    ix = cell // (dims[1] * dims[2])
+                    assert col[atom] // (n // 8) == ((ix & 1) << 2 | (iy & 1) << 1 | (iz & 1))
+            else:
+                deg = sum(len(pm.neighbours(0, s)) for s in shells)
+                assert n <= deg + 1  # greedy bound
 
 
 def test_mesh_argument_errors(ib):
