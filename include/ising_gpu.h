@@ -182,7 +182,9 @@ int ising_total_energy(const ising_mesh* mesh, int replica, const ising_params* 
  * front -- can still evaluate energies.  Replicas are limited to 16,777,216 atoms (larger
  * ones return ISING_ERR_ARG).  All calls on a device share that array: calls that overlap
  * on the GPU race, so issue them one after another.  The first call on a device looks up
- * the array's address; make it before any stream capture.  No counterpart in the reference. */
+ * the array's address; make it before any stream capture.  The address is kept until the
+ * process exits, so do not call this again on a device after cudaDeviceReset on it.  No
+ * counterpart in the reference. */
 int ising_total_energy_noalloc(const ising_mesh* mesh, int replica, const ising_params* p, double* e);
 /* Energy and magnetisation vector of every replica in one pass: e[R], m[R*3]. */
 int ising_observables(const ising_mesh* mesh, const ising_params* p, double* e, double* m);

@@ -137,33 +137,11 @@ bool uses_shell2(const Lattice& L, const ising_params& p) {
 // Fill the device stencil of `m` for the given Hamiltonian.  legacy: the legacy list with
 // (J, D); otherwise shell 1 with (J, D) and shell 2 with J' when active.
 int upload_stencil(ising_mesh* m, const ising_params& p, bool legacy, Slot* dst_slots, int* dst_count) {
-    const Lattice& L = m->lat;
+    // one stencil builder for every path (the allocation-free energy entry point fills the
+    // same tables into its own host memory)
     std::vector<Slot> slots((size_t)kMaxSub * kMaxSlots);
     std::vector<int> cnt(kMaxSub, 0);
-    for (int s = 0; s < L.nsub; ++s) {
-        int c = 0;
-        auto add = [&](const NbrSlot& q, float w, bool dmi) -> int {
-            if (c >= kMaxSlots) return fail(ISING_ERR_ARG, "stencil exceeds 128 slots");
-            Slot e{};
-            e.dx = (int8_t)q.dx; e.dy = (int8_t)q.dy; e.dz = (int8_t)q.dz; e.sub = (uint8_t)q.sub;
-            e.w = w;
-            if (dmi && p.Dz != 0.0) {
-                double D[3];
-                bond_dmi(L, p, q.r, D);
-                e.Dx = (float)D[0]; e.Dy = (float)D[1]; e.Dz = (float)D[2];
-            }
-            slots[(size_t)s * kMaxSlots + c++] = e;
-            return ISING_OK;
-        };
-        if (legacy) {
-            for (const auto& q : L.legacy[s]) ISG_TRY(add(q, (float)p.J, true));
-        } else {
-            for (const auto& q : L.shell[0][s]) ISG_TRY(add(q, (float)p.J, true));
-            if (uses_shell2(L, p))
-                for (const auto& q : L.shell[1][s]) ISG_TRY(add(q, (float)p.J_prime, false));
-        }
-        cnt[s] = c;
-    }
+    ISG_TRY(fill_query_stencil_host(m, p, legacy, slots.data(), cnt.data()));
     ISG_CUDA(cudaMemcpyAsync(dst_slots, slots.data(), slots.size() * sizeof(Slot), cudaMemcpyHostToDevice, m->stream));
     ISG_CUDA(cudaMemcpyAsync(dst_count, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice, m->stream));
     // the host vectors die at return: make the copies complete first

@@ -15,7 +15,9 @@
 // on the array; issue them one after another.
 //
 // The first call on a device resolves the array's device address with cudaGetSymbolAddress
-// (with that device current); make that first call before any stream capture begins.
+// (with that device current); make that first call before any stream capture begins.  The
+// address is kept for the life of the process: a cudaDeviceReset unloads the module and makes
+// it stale, so this entry point must not be used on a device after that device was reset.
 #include <mutex>
 
 #include "internal.h"
