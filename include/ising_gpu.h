@@ -36,7 +36,7 @@ extern "C" {
 #define ISING_ERR_NAN 2          /* NaN in spins or proposals (src/energyMin.f90:330-331) */
 #define ISING_ERR_BOUNDS 3       /* index out of range (e.g. Z_index, rsp:334) */
 #define ISING_ERR_TIMEOUT 4      /* a bounded device-side wait gave up */
-#define ISING_ERR_UNSUPPORTED 5  /* e.g. demag=.true. (out of scope) */
+#define ISING_ERR_UNSUPPORTED 5  /* e.g. demag=.true. in parallel tempering */
 #define ISING_ERR_CUDA 6         /* CUDA runtime error or no usable device */
 #define ISING_ERR_ALLOC 7        /* device or host allocation failed */
 #define ISING_ERR_LATTICE 8      /* derivative list incomplete ("Unable to locate atoms",
@@ -143,7 +143,11 @@ typedef struct {
     int dmi_mode;        /* ISING_DMI_INTERFACIAL or ISING_DMI_BULK */
     double dmi_axis[3];  /* interfacial axis; all zero selects c_vec/|c_vec| (:114) */
     int legacy_neighbours; /* 1: sum over the legacy NeighborList (TotalHeisenbergEnergy) */
-    int demag;           /* must be 0: demag=.true. returns ISING_ERR_UNSUPPORTED */
+    int demag;           /* 1: the demagnetising field enters as -mu_0 S.H in the local energy and
+                            the sweeps, -1/2 mu_0 S.H in the total energy (mu_0 of
+                            src/constants.f90:15); parallel tempering and the batched engine
+                            return ISING_ERR_UNSUPPORTED for it (the reference's drivers run with
+                            demag = .false., src/PT.f90:29, src/ISING.f90:46) */
 } ising_params;
 
 /* Fills p with the conventions of one reference routine:
@@ -175,6 +179,14 @@ int ising_local_energy_batch(const ising_mesh* mesh, int replica, int n, const i
 /* Replaces TotalHeisenbergEnergy(chainMesh, J, J', Dz, Dz', B, lockArray, totalEnergy,
  * demag) (src/energyMin.f90:499-528): FP32 terms, FP64 block sums. */
 int ising_total_energy(const ising_mesh* mesh, int replica, const ising_params* p, double* e);
+/* Replaces calculate_demagnetisation_field(chainMesh, outputArray)
+ * (src/reciprocalSpaceProcesses.f90:202-281): the demagnetising field of one replica's spins at
+ * every atom, H[3 * numAtoms] column-major as outputArray(numAtoms, 3), FP64.  Cloud-in-cell
+ * deposit onto the cell centres (27 neighbouring cells), forward transform, H(k) = -(k.M/k^2) k
+ * with k = 0 and the bins beyond pi/a, pi/b, pi/c removed, backward transform / (N L M), and the
+ * same weights back to the atoms.  Metropolis sweeps with demag recompute it at the start and
+ * every int(pi sqrt(5) / (2 r)) sweeps (src/energyMin.f90:258-259, 363-366). */
+int ising_demag_field(const ising_mesh* mesh, int replica, double* H);
 /* Same result as ising_total_energy, but allocates no device memory: the per-block partial
  * sums live in a fixed array inside the library (128 KiB per device, held until exit), so
  * callers that cannot call cudaMalloc -- loops that must not stall other streams, work

@@ -298,6 +298,14 @@ def calculate_winding_number2(mesh: ChainMesh, Z_index: int, replica: int = 0) -
     return q.value
 
 
+def demag_field(mesh: ChainMesh, replica: int = 0) -> np.ndarray:
+    """calculate_demagnetisation_field (src/reciprocalSpaceProcesses.f90:202-281): the
+    demagnetising field at every atom, (numAtoms, 3) FP64."""
+    out = np.empty((3, mesh.numAtoms))
+    _lib.call("ising_demag_field", mesh.handle, replica, _dp(out))
+    return out.T
+
+
 def winding_all_slices(mesh: ChainMesh, replica: int = 0) -> np.ndarray:
     out = np.empty(mesh.numCellsZ)
     _lib.call("ising_winding_all_slices", mesh.handle, replica, _dp(out))

@@ -92,7 +92,6 @@ int check_status(ising_mesh* m) {
 
 int validate_params(const ising_params* p) {
     if (!p) return fail(ISING_ERR_ARG, "params is NULL");
-    if (p->demag) return fail(ISING_ERR_UNSUPPORTED, "demag=.true. is out of scope (demagnetising field not built)");
     const double v[] = {p->J, p->J_prime, p->Dz, p->Dz_prime, p->B, p->K, p->zeeman_factor};
     for (double x : v) if (!std::isfinite(x)) return fail(ISING_ERR_NAN, "non-finite Hamiltonian parameter");
     if (p->dmi_mode != ISING_DMI_INTERFACIAL && p->dmi_mode != ISING_DMI_BULK)
@@ -229,13 +228,14 @@ struct SweepPlan {
     int slots_per_rep = 0;
     Slot* d_slots = nullptr;   // general path: stencil buffers this plan reads
     int* d_count = nullptr;
+    const float* demag = nullptr;   // general path: demagnetising field of the swept replica
 };
 
 // Fills plan for Hamiltonian p; the general path uploads its stencil into (slots, count).
 int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots, int* count) {
     plan->ham = make_ham(p);
     const bool sh2 = uses_shell2(m->lat, p);
-    if (m->layout.cb == 1 && !sh2) {
+    if (m->layout.cb == 1 && !sh2 && !p.demag) {
         plan->sc = true;
         ISG_TRY(sc_dmi(m, p, &plan->ham, &plan->dmi_kind));
         const Lattice& Lt = m->lat;
@@ -327,6 +327,7 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
     g.seed = seed; g.ensemble = ensemble; g.move = move; g.r = (float)r;
     g.ham = plan.ham; g.st = StencilDev{plan.d_slots, plan.d_count, L.nsub}; g.layout = m->layout;
     g.partials = partials; g.slots_per_rep = plan.slots_per_rep; g.status = m->d_status;
+    g.demag = plan.demag; g.mu0 = (float)kMu0;
     if (m->layout.cb == 2) {   // octant classes: contiguous storage ranges
         const int ng = (int)m->oct_rank0.size() - 1;
         for (int sw = 0; sw < n_sweeps; ++sw) {
@@ -512,6 +513,7 @@ extern "C" int ising_mesh_destroy(ising_mesh* m) {
     cudaFree(m->d_staging); cudaFree(m->d_beta); cudaFree(m->d_winding_tmp); cudaFree(m->d_slots); cudaFree(m->d_slot_count);
     cudaFree(m->d_plaq);
     isg::skyrmion_release(m);
+    isg::demag_release(m);
     for (auto& c : m->colour) cudaFree(c.d_sites);
     if (m->h_pinned) cudaFreeHost(m->h_pinned);
     if (m->own_stream) cudaStreamDestroy(m->own_stream);
@@ -793,6 +795,7 @@ extern "C" int ising_local_energy_batch(const ising_mesh* mc, int replica, int n
     // scratch layout: atoms (n int64 as doubles), sprop (3n), old (n), new (n)
     const int chunk = kScratchDoubles / 6;
     ISG_TRY(upload_query_stencil(m, *p, false));
+    if (p->demag) ISG_TRY(demag_enqueue(m, replica, true, false));
     for (int off = 0; off < n; off += chunk) {
         const int k = std::min(chunk, n - off);
         int64_t* d_atoms = reinterpret_cast<int64_t*>(m->d_scratch);
@@ -806,6 +809,7 @@ extern "C" int ising_local_energy_batch(const ising_mesh* mc, int replica, int n
         a.spins = m->d_spins + (int64_t)replica * 3 * m->lat.natoms;
         a.natoms = m->lat.natoms; a.nx = m->lat.nx; a.ny = m->lat.ny; a.nz = m->lat.nz; a.nsub = m->lat.nsub;
         a.ham = make_ham(*p); a.st = stencil_of(m); a.layout = m->layout; a.atoms = d_atoms; a.sprop = d_sp; a.old_e = d_old; a.new_e = d_new; a.n = k;
+        a.demag_H = p->demag ? demag_field64(m) : nullptr;
         ISG_TRY(launch_local_energy(a, m->stream));
         ISG_CUDA(cudaMemcpyAsync(m->h_pinned + 4 * k, d_old, 2 * k * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
         ISG_CUDA(cudaStreamSynchronize(m->stream));
@@ -842,6 +846,13 @@ extern "C" int ising_observables(const ising_mesh* mc, const ising_params* p, do
     }
     cudaFree(d_tmp);
     if (st != ISING_OK) return st;
+    if (p->demag)   // -1/2 mu_0 S.H with the field of the current spins (src/energyMin.f90:223-226, 511)
+        for (int r = 0; r < R; ++r) {
+            double dot = 0.0;
+            ISG_TRY(demag_enqueue(m, r, true, false));
+            ISG_TRY(demag_dot(m, r, &dot));
+            h[4 * r] += -0.5 * kMu0 * dot;
+        }
     for (int r = 0; r < R; ++r) {
         if (e) e[r] = h[4 * r];
         if (mv) for (int k = 0; k < 3; ++k) mv[3 * r + k] = h[4 * r + 1 + k];
@@ -867,7 +878,26 @@ extern "C" int ising_total_energy(const ising_mesh* mc, int replica, const ising
     }
     cudaFree(d_tmp);
     if (st != ISING_OK) return st;
+    if (p->demag) {   // -1/2 mu_0 S.H with the field of the current spins (src/energyMin.f90:223-226, 511)
+        double dot = 0.0;
+        ISG_TRY(demag_enqueue(m, replica, true, false));
+        ISG_TRY(demag_dot(m, replica, &dot));
+        h[0] += -0.5 * kMu0 * dot;
+    }
     *e = h[0];
+    return ISING_OK;
+}
+
+extern "C" int ising_demag_field(const ising_mesh* mc, int replica, double* H) {
+    ising_mesh* m = const_cast<ising_mesh*>(mc);
+    ISG_TRY(check_replica(m, replica));
+    if (!H) return fail(ISING_ERR_ARG, "H is NULL");
+    DeviceGuard g(m->device);
+    ISG_TRY(mesh_settle(m));
+    ISG_TRY(demag_enqueue(m, replica, true, false));
+    ISG_CUDA(cudaMemcpyAsync(H, demag_field64(m), 3 * (size_t)m->lat.natoms * sizeof(double), cudaMemcpyDeviceToHost,
+                             m->stream));
+    ISG_CUDA(cudaStreamSynchronize(m->stream));
     return ISING_OK;
 }
 
@@ -885,7 +915,22 @@ extern "C" int ising_metropolis_mcs(ising_mesh* m, int replica, double beta, int
     const int move = r > 0.0 ? 1 : 0;
     m->h_pinned[0] = beta;
     ISG_CUDA(cudaMemcpyAsync(m->d_beta + replica, m->h_pinned, sizeof(double), cudaMemcpyHostToDevice, m->stream));
-    ISG_TRY(enqueue_sweeps(m, plan, replica, 1, m->d_beta, 0u, n_sweeps, seed, 0u, move, r, nullptr));
+    if (p->demag) {
+        // the field is computed at the start and after every demag_update_interval =
+        // int(pi sqrt(5) / (2 r)) sweeps (src/energyMin.f90:258-259, 363-366); the uniform move
+        // (r <= 0) keeps the field of the start
+        const double pi_f = (double)3.14159265358979323846f;
+        const int every = move ? std::max(1, (int)(pi_f * std::sqrt(5.0) / (2.0 * r))) : n_sweeps;
+        plan.demag = demag_field32(m);
+        for (int sw0 = 0; sw0 < n_sweeps; sw0 += every) {
+            ISG_TRY(demag_enqueue(m, replica, false, true));
+            plan.demag = demag_field32(m);
+            ISG_TRY(enqueue_sweeps(m, plan, replica, 1, m->d_beta, (uint32_t)sw0, std::min(every, n_sweeps - sw0), seed,
+                                   0u, move, r, nullptr));
+        }
+    } else {
+        ISG_TRY(enqueue_sweeps(m, plan, replica, 1, m->d_beta, 0u, n_sweeps, seed, 0u, move, r, nullptr));
+    }
     ISG_TRY(launch_advance(m->d_sweep + replica, 1, (uint32_t)n_sweeps, m->stream));
     m->h_sweep[replica] += (uint32_t)n_sweeps;
     return check_status(m);
@@ -1077,6 +1122,8 @@ extern "C" int ising_pt_create(ising_mesh* m, int n, const double* betas, const 
     ISG_TRY(mesh_settle(m));
     ISG_TRY(check_replica(m, 0));
     ISG_TRY(validate_params(p));
+    if (p->demag)   // the reference's drivers run with demag = .false. (src/PT.f90:29, src/ISING.f90:46)
+        return fail(ISING_ERR_UNSUPPORTED, "parallel tempering runs without the demagnetising field");
     if (n < 1 || n > m->n_replicas) return fail(ISING_ERR_ARG, "n_temps must be in 1..n_replicas");
     for (int t = 0; t < n; ++t) if (!std::isfinite(betas[t])) return fail(ISING_ERR_NAN, "non-finite beta");
     if (opt->move != ISING_MOVE_UNIFORM && opt->move != ISING_MOVE_BALL) return fail(ISING_ERR_ARG, "bad move");
@@ -1879,6 +1926,7 @@ extern "C" int ising_ensembles_create(int n, const ising_ensemble_desc* desc, co
         for (int f = 0; f < e; ++f)
             if (desc[f].mesh == d.mesh) return fail(ISING_ERR_ARG, "each ensemble needs its own mesh");
         ISG_TRY(validate_params(&d.params));
+        if (d.params.demag) return fail(ISING_ERR_UNSUPPORTED, "the batched engine runs without the demagnetising field");
         const Lattice& L = d.mesh->lat;
         if (d.mesh->layout.cb != 1 || uses_shell2(L, d.params))
             return fail(ISING_ERR_UNSUPPORTED, "the batched engine needs colour-separated simple-cubic meshes "

@@ -114,11 +114,22 @@ struct ising_mesh {
     int sclx = 10, scly = 10;            // fine-grid scale factors (makeChainMesh defaults)
     void* sky = nullptr;                 // skyrmion-counting workspace, made on first use
     void* xfer = nullptr;                // asynchronous spin transfers (streams, per-replica staging)
+    void* demag = nullptr;               // demagnetising-field workspace, made on first use
 };
 
 namespace isg {
 // Frees the skyrmion-counting workspace of a mesh (called by ising_mesh_destroy).
 void skyrmion_release(ising_mesh* m);
+// Demagnetising field (calculate_demagnetisation_field, src/reciprocalSpaceProcesses.f90:202-281)
+// of one replica, enqueued on the mesh's stream: FP64 per atom in reference order
+// (demag_field64, [3][natoms]) and/or FP32 in the storage order of the spins (demag_field32).
+int demag_enqueue(ising_mesh* m, int replica, bool want64, bool want32);
+const double* demag_field64(const ising_mesh* m);
+const float* demag_field32(const ising_mesh* m);
+// sum over atoms of S . H (FP64) for the field last computed into demag_field64 (synchronous)
+int demag_dot(ising_mesh* m, int replica, double* out);
+void demag_release(ising_mesh* m);
+constexpr double kMu0 = 1.25663706127e-6;   // mu_0 of src/constants.f90:15
 // Waits for the mesh's asynchronous spin transfers (ising_spins_*_async) still in flight and
 // reports invalid uploaded spins; a no-op when none are.  Every entry point that reads or
 // writes a mesh's spins calls it first.
@@ -180,6 +191,8 @@ struct GeneralLaunch {
     int slots_per_rep;
     int slot_base;         // class offset into the slot range
     int* status;
+    const float* demag;    // demagnetising field of the (single) replica in storage order, or null
+    float mu0;             // its factor in the local field: h -= mu0 H
 };
 int launch_general_colour(const GeneralLaunch& a, cudaStream_t s);
 // One class (octant, sublattice group) of an octant-layout mesh: sites of storage ranks
@@ -232,6 +245,7 @@ struct LocalLaunch {
     double* old_e;
     double* new_e;
     int n;
+    const double* demag_H; // demagnetising field per atom, reference order [3][natoms], or null
 };
 int launch_local_energy(const LocalLaunch& a, cudaStream_t s);
 

@@ -80,6 +80,12 @@ __device__ __forceinline__ void general_site(const GeneralLaunch& a, const Slot*
     f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.layout);
     h.z -= H.Bz;
     const int64_t si = sidx(a.layout, ix, iy, iz, sub);
+    if (a.demag) {   // -mu_0 S.H of calculateHeisenbergEnergy (src/energyMin.f90:163-167)
+        const int64_t N = a.natoms;
+        h.x = fmaf(-a.mu0, a.demag[si], h.x);
+        h.y = fmaf(-a.mu0, a.demag[N + si], h.y);
+        h.z = fmaf(-a.mu0, a.demag[2 * N + si], h.z);
+    }
     const f3 s = {sx[si], sy[si], sz[si]};
     const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)at, sweep, (uint32_t)rep, (a.ensemble << 8) | kTagSweep),
                                     philox_key(a.seed));
@@ -378,6 +384,12 @@ __global__ void k_local_energy(LocalLaunch a) {
         const float q1 = sp.x * a.ham.kx + sp.y * a.ham.ky + sp.z * a.ham.kz;
         e0 -= a.ham.K * q0 * q0;
         e1 -= a.ham.K * q1 * q1;
+    }
+    if (a.demag_H) {   // -mu_0 S.H in FP64 (src/energyMin.f90:163-167)
+        const double hx = a.demag_H[at], hy = a.demag_H[N + at], hz = a.demag_H[2 * N + at];
+        a.old_e[t] = (double)e0 - kMu0 * ((double)s.x * hx + (double)s.y * hy + (double)s.z * hz);
+        a.new_e[t] = (double)e1 - kMu0 * (a.sprop[3 * t] * hx + a.sprop[3 * t + 1] * hy + a.sprop[3 * t + 2] * hz);
+        return;
     }
     a.old_e[t] = (double)e0;
     a.new_e[t] = (double)e1;

@@ -151,9 +151,9 @@ __device__ __forceinline__ void tframe(F3 s, F3& e1, F3& e2) {
 // log_s(t) in the frame of s; returns the angle
 __device__ __forceinline__ float tlog(F3 s, F3 t, float& w1, float& w2) {
     const float c = fminf(1.f, fmaxf(-1.f, dot3(s, t)));
-    const float th = acosf(c);
     const F3 v = axpy3(-c, s, t);
     const float nv = sqrtf(dot3(v, v));
+    const float th = atan2f(nv, c);   // small angles keep their bits (acos of c near 1 would not)
     F3 e1, e2;
     tframe(s, e1, e2);
     const float sc = nv > 1e-12f ? th / nv : 0.f;
@@ -180,7 +180,10 @@ __global__ void k_nll(const float* __restrict__ win, const float* __restrict__ t
         F3 e1, e2;
         tframe(s, e1, e2);
         const F3 mu = f3(out[r * 4], out[r * 4 + 1], out[r * 4 + 2]);
-        const float ls = out[r * 4 + 3];
+        // log sigma clamped to the range the proposal uses (a target that did not move would
+        // otherwise drive log sigma to -infinity and the loss to NaN); no gradient outside it
+        const float lraw = out[r * 4 + 3];
+        const float ls = fminf(kLogSigMax, fmaxf(kLogSigMin, lraw));
         const float r1 = w1 - dot3(mu, e1), r2 = w2 - dot3(mu, e2);
         const float is2 = expf(-2.f * ls);
         const float q = r1 * r1 + r2 * r2;
@@ -188,7 +191,7 @@ __global__ void k_nll(const float* __restrict__ win, const float* __restrict__ t
         // d/dmu = -(r1 e1 + r2 e2) / sigma^2 ; d/dlog sigma = -q / sigma^2 + 2
         const F3 g = scale3(-is2 * inv_n, axpy3(r1, e1, scale3(r2, e2)));
         dout[r * 4] = g.x; dout[r * 4 + 1] = g.y; dout[r * 4 + 2] = g.z;
-        dout[r * 4 + 3] = (-q * is2 + 2.f) * inv_n;
+        dout[r * 4 + 3] = (lraw > kLogSigMin && lraw < kLogSigMax) ? (-q * is2 + 2.f) * inv_n : 0.f;
     }
     l = warp_sum(l);
     if ((threadIdx.x & 31) == 0 && l != 0.0) atomicAdd(loss_acc, l);

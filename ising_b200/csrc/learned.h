@@ -11,6 +11,9 @@ struct ising_net;
 
 namespace isg {
 
+// range of log sigma in the proposal and in the training loss
+constexpr float kLogSigMin = -6.f, kLogSigMax = 1.5f;
+
 // C/O[M x N] = epilogue(A[M x K] * B[N x K]^T + bias)
 struct GemmArgs {
     const __nv_bfloat16* A;

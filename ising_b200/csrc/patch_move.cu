@@ -34,7 +34,6 @@ __device__ __forceinline__ void pframe(V3 s, V3& e1, V3& e2) {
 // log(|w| / sin|w|)
 __device__ __forceinline__ float log_jac(float th) { return th > 1e-3f ? logf(th / sinf(th)) : th * th * (1.f / 6.f); }
 
-constexpr float kLogSigMin = -6.f, kLogSigMax = 1.5f;
 
 template <typename T>
 __device__ __forceinline__ T block_sum64(T v, T* sm) {   // 64 threads

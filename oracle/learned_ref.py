@@ -182,7 +182,7 @@ def loss(p: dict, windows, targets, round_bf16=False):
     s = patch_spins(windows)
     om, _ = log_map(s, torch.as_tensor(targets, dtype=F64))
     r = om - tangent_mean(out, s)
-    ls = out[..., 3]
+    ls = out[..., 3].clamp(-6.0, 1.5)        # the proposal's log sigma range (no gradient outside)
     return (0.5 * (r * r).sum(-1) * torch.exp(-2.0 * ls) + 2.0 * ls).mean()
 
 
