@@ -16,7 +16,9 @@
 //
 // Per step a thread loads one colour-0 and one colour-1 pair row (both one step ahead) and
 // stores two; the x-neighbour rows of both colours come from the neighbouring thread rows
-// through shared memory (three rotating row slots, one barrier per step).  DRAM moves 12 B
+// through shared memory (three rotating row slots).  One named barrier per step, split: a
+// thread arrives once its new colour-0 row is in shared memory, draws the Philox numbers of its
+// colour-1 pair (which need no neighbour data) and then waits for the others' rows.  DRAM moves 12 B
 // read + 12 B written per site and sweep plus the halo planes' rows, against 36 B for two
 // passes.
 //
@@ -114,6 +116,9 @@ __device__ __forceinline__ void run_fused(const EnsParams& P, uint32_t rep, uint
     __syncthreads();
 #pragma unroll 1
     for (uint32_t t = 0; t < T; ++t) {
+        const uint32_t ym = dn(yc);
+        const uint32_t p1 = (x + ym + 1u) & 1u;
+        v23 Wn{};
         if (active) {
             // colour 0 at row yc against the old colour-1 rows
             const float* kc = ksm + s0 * kslab;
@@ -121,44 +126,49 @@ __device__ __forceinline__ void run_fused(const EnsParams& P, uint32_t rep, uint
             const uint32_t je = p0 ? (j + 2u == W ? 0u : j + 2u) : (j == 0u ? W - 1u : j - 1u);
             const bool inrow = t >= 1u && t <= Y;
             bool any;
-            const v23 Wn = pair_new<MOVE, DMI, HAS_K>(
+            Wn = pair_new<MOVE, DMI, HAS_K>(
                 G, P.rk, P.status, x * ny + yc, j, p0, Wo, sm_get(kc + rowf, W, j), sm_get(kc - rowf, W, j), Kn,
                 sm_get(ksm + s2 * kslab, W, j), sm_get(kc, W, j), kc[je], kc[W + je], kc[2u * W + je], sweep, rep,
                 beta2, inrow && !halo, de, dmx, dmy, dmz, any);
             sm_put(wsm + s0 * wslab, W, j, Wn);
             if (!halo && inrow) st3(out, N, x * xs + yc * W + j, Wn);
-            if (!halo && t >= 2u) {
-                // colour 1 at row yc - 1: its colour-0 neighbours are rows yc-2 .. yc of this
-                // plane and row yc - 1 of planes x +- 1 (written last step)
-                const uint32_t ym = dn(yc);
-                const float* wc = wsm + s2 * wslab;
-                const uint32_t p1 = (x + ym + 1u) & 1u;
-                const uint32_t je1 = p1 ? (j + 2u == W ? 0u : j + 2u) : (j == 0u ? W - 1u : j - 1u);
-                const v23 Kw = pair_new<MOVE, DMI, HAS_K>(
-                    G, P.rk, P.status, x * ny + ym, j, p1, sm_get(ksm + s2 * kslab, W, j), sm_get(wc + rowf, W, j),
-                    sm_get(wc - rowf, W, j), Wn, sm_get(wsm + s1 * wslab, W, j), sm_get(wc, W, j), wc[je1],
-                    wc[W + je1], wc[2u * W + je1], sweep, rep, beta2, true, de, dmx, dmy, dmz, any);
-                st3(out, N, half + x * xs + ym * W + j, Kw);
-            }
             // the next step's colour-1 rows: row yc + 1 of this plane and of the outside plane
             sm_put(ksm + s1 * kslab, W, j, Kn);
             if (halo) sm_put(osm + s1 * kslab, W, j, pfO);
+            // registers of the next step, and the loads of the step after it
+            Kn = pfK;
+            Wo = pfW;
+            if (t + 2u < T) {
+                const uint32_t y2 = up(up(yc));
+                pfW = ldW(x, y2);
+                pfK = ldK(x, up(y2));
+                if (halo) pfO = ldK(xo, y2);
+            }
         }
-        __syncthreads();
+        // the new colour-0 rows are published at arrive; the colour-1 pair's Philox draws,
+        // which need none of them, fill the wait
+        asm volatile("bar.arrive 1, %0;" ::"r"(blockDim.x) : "memory");
+        const bool c1 = active && !halo && t >= 2u;
+        uint4 ra = make_uint4(0u, 0u, 0u, 0u), rb = ra;
+        if (c1) pair_draws(G, P.rk, x * ny + ym, j, p1, sweep, rep, ra, rb);
+        asm volatile("bar.sync 1, %0;" ::"r"(blockDim.x) : "memory");
+        if (c1) {
+            // colour 1 at row yc - 1: its colour-0 neighbours are rows yc-2 .. yc of this plane
+            // and row yc - 1 of planes x +- 1 (written last step)
+            const float* wc = wsm + s2 * wslab;
+            const uint32_t je1 = p1 ? (j + 2u == W ? 0u : j + 2u) : (j == 0u ? W - 1u : j - 1u);
+            bool any;
+            const v23 Kw = pair_new_drawn<MOVE, DMI, HAS_K>(
+                G, P.status, p1, sm_get(ksm + s2 * kslab, W, j), sm_get(wc + rowf, W, j), sm_get(wc - rowf, W, j),
+                Wn, sm_get(wsm + s1 * wslab, W, j), sm_get(wc, W, j), wc[je1], wc[W + je1], wc[2u * W + je1], ra, rb,
+                beta2, true, de, dmx, dmy, dmz, any);
+            st3(out, N, half + x * xs + ym * W + j, Kw);
+        }
         {
             const uint32_t r = s0;
             s0 = s1; s1 = s2; s2 = r;
         }
-        if (active) {
-            Kn = pfK;
-            Wo = pfW;
-            yc = up(yc);
-            if (t + 2u < T) {
-                pfW = ldW(x, up(yc));
-                pfK = ldK(x, up(up(yc)));
-                if (halo) pfO = ldK(xo, up(yc));
-            }
-        }
+        yc = up(yc);
     }
 }
 

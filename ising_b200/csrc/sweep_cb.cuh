@@ -110,18 +110,29 @@ __device__ __forceinline__ void propose2(const float2* s, uint4 ra, uint4 rb, fl
     sp[0] = vx; sp[1] = vy; sp[2] = vz;
 }
 
+// The two Philox draws of the site pair (j, j+1) of packed row `row` (parity p): counters
+// (reference atom index, sweep, replica, ensemble << 8 | sweep tag).
+__device__ __forceinline__ void pair_draws(const CbGeom& P, const uint32_t* rk, uint32_t row, uint32_t j,
+                                           uint32_t p, uint32_t sweep, uint32_t rep, uint4& ra, uint4& rb) {
+    const uint32_t i0 = row * (uint32_t)P.nz + 2u * j + p;   // reference atom index of site .x
+    const uint32_t cw = (P.ensemble << 8) | kTagSweep;
+    ra = philox_rk(make_uint4(i0, sweep, rep, cw), rk);
+    rb = philox_rk(make_uint4(i0 + 2u, sweep, rep, cw), rk);
+}
+
 // Update of one site pair from its loaded neighbourhood: own pair s at entries (j, j+1) of
 // packed row `row` (parity p), the other colour's pairs px, mx (x +- 1), py, my (y +- 1) and
 // oz (same row) at entries (j, j+1), and the edge entry (ex, ey, ez) of that row.  Returns
 // the pair after the Metropolis decisions (rejected sites bit-identical to s); `any` tells
 // whether either site accepted.  dE and dM of accepted moves are added to the running sums
 // when `count` is set (a recomputed halo pair is not counted).
+// pair_new_drawn takes the pair's Philox draws (pair_draws); pair_new draws them itself.
 template <int MOVE, int DMI, bool HAS_K>
-__device__ __forceinline__ v23 pair_new(const CbGeom& P, const uint32_t* rk, int* status, uint32_t row,
-                                        uint32_t j, uint32_t p, const v23& s, const v23& px, const v23& mx,
-                                        const v23& py, const v23& my, const v23& oz, float ex, float ey,
-                                        float ez, uint32_t sweep, uint32_t rep, float beta2, bool count,
-                                        v2& de, v2& dmx, v2& dmy, v2& dmz, bool& any) {
+__device__ __forceinline__ v23 pair_new_drawn(const CbGeom& P, int* status, uint32_t p, const v23& s,
+                                              const v23& px, const v23& mx, const v23& py, const v23& my,
+                                              const v23& oz, float ex, float ey, float ez, const uint4& ra,
+                                              const uint4& rb, float beta2, bool count, v2& de, v2& dmx, v2& dmy,
+                                              v2& dmz, bool& any) {
     const CbGeom& a = P;
     const HamDev& H = P.ham;
     v23 zp, zm;
@@ -160,11 +171,7 @@ __device__ __forceinline__ v23 pair_new(const CbGeom& P, const uint32_t* rk, int
     }
     h.z = sub(h.z, V(H.Bz));
 
-    // Philox draws (one per site) and the packed proposals
-    const uint32_t i0 = row * (uint32_t)a.nz + 2u * j + p;   // reference atom index of site .x
-    const uint32_t cw = (a.ensemble << 8) | kTagSweep;
-    const uint4 ra = philox_rk(make_uint4(i0, sweep, rep, cw), rk);
-    const uint4 rb = philox_rk(make_uint4(i0 + 2u, sweep, rep, cw), rk);
+    // packed proposals from the draws
     v23 sp;
     {
         const float2 sv[3] = {s.x, s.y, s.z};
@@ -198,6 +205,18 @@ __device__ __forceinline__ v23 pair_new(const CbGeom& P, const uint32_t* rk, int
     return {make_float2(acc0 ? sp.x.x : s.x.x, acc1 ? sp.x.y : s.x.y),
             make_float2(acc0 ? sp.y.x : s.y.x, acc1 ? sp.y.y : s.y.y),
             make_float2(acc0 ? sp.z.x : s.z.x, acc1 ? sp.z.y : s.z.y)};
+}
+
+template <int MOVE, int DMI, bool HAS_K>
+__device__ __forceinline__ v23 pair_new(const CbGeom& P, const uint32_t* rk, int* status, uint32_t row,
+                                        uint32_t j, uint32_t p, const v23& s, const v23& px, const v23& mx,
+                                        const v23& py, const v23& my, const v23& oz, float ex, float ey,
+                                        float ez, uint32_t sweep, uint32_t rep, float beta2, bool count,
+                                        v2& de, v2& dmx, v2& dmy, v2& dmz, bool& any) {
+    uint4 ra, rb;
+    pair_draws(P, rk, row, j, p, sweep, rep, ra, rb);
+    return pair_new_drawn<MOVE, DMI, HAS_K>(P, status, p, s, px, mx, py, my, oz, ex, ey, ez, ra, rb, beta2, count,
+                                            de, dmx, dmy, dmz, any);
 }
 
 // pair_new, with the pair written back at own_off when either site accepts.
