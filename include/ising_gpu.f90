@@ -128,6 +128,12 @@ module ising_gpu
       type(ising_params), intent(in) :: p
       real(c_double), intent(out) :: e
     end function
+    integer(c_int) function ising_demag_field(mesh, replica, h) bind(C, name="ising_demag_field")
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: mesh
+      integer(c_int), value :: replica
+      real(c_double), intent(out) :: h(*)           ! outputArray(numAtoms, 3), column-major
+    end function
     integer(c_int) function ising_winding_number(mesh, replica, z_index, q) bind(C, name="ising_winding_number")
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: mesh
