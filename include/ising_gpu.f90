@@ -134,6 +134,12 @@ module ising_gpu
       integer(c_int), value :: replica
       real(c_double), intent(out) :: h(*)           ! outputArray(numAtoms, 3), column-major
     end function
+    integer(c_int) function ising_write_demag_csv(mesh, replica, path) bind(C, name="ising_write_demag_csv")
+      import :: c_int, c_char, c_ptr
+      type(c_ptr), value :: mesh
+      integer(c_int), value :: replica
+      character(kind=c_char), intent(in) :: path(*)  ! NUL-terminated
+    end function
     integer(c_int) function ising_winding_number(mesh, replica, z_index, q) bind(C, name="ising_winding_number")
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: mesh

@@ -187,6 +187,10 @@ int ising_total_energy(const ising_mesh* mesh, int replica, const ising_params* 
  * same weights back to the atoms.  Metropolis sweeps with demag recompute it at the start and
  * every int(pi sqrt(5) / (2 r)) sweeps (src/energyMin.f90:258-259, 363-366). */
 int ising_demag_field(const ising_mesh* mesh, int replica, double* H);
+/* Replaces write_demagnetisation_field_to_file(chainMesh, demag_field, filepath)
+ * (src/energyMin.f90:559-583) for the field of one replica's current spins: header
+ * x,y,z,fx,fy,fz, one record per atom, every value F8.4. */
+int ising_write_demag_csv(const ising_mesh* mesh, int replica, const char* path);
 /* Same result as ising_total_energy, but allocates no device memory: the per-block partial
  * sums live in a fixed array inside the library (128 KiB per device, held until exit), so
  * callers that cannot call cudaMalloc -- loops that must not stall other streams, work

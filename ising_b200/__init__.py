@@ -10,7 +10,7 @@ from ._lib import IsingError, Params, load
 from .api import (ChainMesh, Ensembles, ParallelTempering, ProposalNet, bcc_unit_cell, calculate_heisenberg_energy,
                   calculate_skyrmion_number, calculate_winding_density_interpolated, calculate_winding_number2,
                   calculate_winding_number_density, chain_mesh_statistics, chain_mesh_statistics_full,
-                  compute_skyrmion_distribution, demag_field, frame_filename, gaussian_filter_2d, interpolation_scale,
+                  compute_skyrmion_distribution, demag_field, write_demagnetisation_field_to_file, frame_filename, gaussian_filter_2d, interpolation_scale,
                   set_interpolation_scale, write_frame_info, write_winding_number_density_interpolated,
                   skyrmion_number_from_density,
                   hyper_kagome_unit_cell, local_energy_batch, make_chain_mesh, metropolis_mcs, observables,
@@ -20,7 +20,7 @@ from .api import (ChainMesh, Ensembles, ParallelTempering, ProposalNet, bcc_unit
 
 __all__ = ["ChainMesh", "Ensembles", "ParallelTempering", "ProposalNet", "IsingError", "Params", "load", "bcc_unit_cell",
            "calculate_skyrmion_number", "calculate_winding_density_interpolated", "chain_mesh_statistics_full",
-           "compute_skyrmion_distribution", "demag_field", "frame_filename", "gaussian_filter_2d", "interpolation_scale",
+           "compute_skyrmion_distribution", "demag_field", "write_demagnetisation_field_to_file", "frame_filename", "gaussian_filter_2d", "interpolation_scale",
            "set_interpolation_scale", "write_frame_info", "write_winding_number_density_interpolated",
            "skyrmion_number_from_density",
            "calculate_heisenberg_energy", "calculate_winding_number2", "calculate_winding_number_density",

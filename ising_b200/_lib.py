@@ -136,6 +136,7 @@ _SIGS = {
     "ising_ensembles_inject_stall": (_i, [_vp, _i]),
     "ising_ensembles_set_resync": (_i, [_vp, _i]),
     "ising_demag_field": (_i, [_vp, _i, _P(_d)]),
+    "ising_write_demag_csv": (_i, [_vp, _i, C.c_char_p]),
     "ising_conv3_bf16": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _i, _vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "ising_bf16_gemm": (_i, [_vp, _i, _vp, _i, _i, _i, _i, _P(C.c_float), _P(C.c_float), _i, _vp, _i, _i, _vp]),
     "ising_net_create": (_i, [_i, _i, _u64, _P(_vp)]),

@@ -306,6 +306,12 @@ def demag_field(mesh: ChainMesh, replica: int = 0) -> np.ndarray:
     return out.T
 
 
+def write_demagnetisation_field_to_file(mesh: ChainMesh, filepath: str, replica: int = 0):
+    """write_demagnetisation_field_to_file (src/energyMin.f90:559-583) of the field of the
+    replica's current spins."""
+    _lib.call("ising_write_demag_csv", mesh.handle, replica, filepath.encode())
+
+
 def winding_all_slices(mesh: ChainMesh, replica: int = 0) -> np.ndarray:
     out = np.empty(mesh.numCellsZ)
     _lib.call("ising_winding_all_slices", mesh.handle, replica, _dp(out))

@@ -37,6 +37,15 @@ std::string F0(double x, int d) {
     return out;
 }
 
+// Fw.d appended to o: right-justified in w characters (the zero before the point written, as
+// it is whenever the field has room), w asterisks when the number does not fit
+void Fw_app(std::string& o, double x, int w, int d) {
+    char buf[512];
+    const int n = std::snprintf(buf, sizeof buf, "%*.*f", w, d, x);
+    if (n > w || std::isnan(x) || std::isinf(x)) { o.append((size_t)w, '*'); return; }
+    o.append(buf, (size_t)n);
+}
+
 std::string I0m(long v, int m) {
     char buf[64];
     if (v < 0) std::snprintf(buf, sizeof buf, "-%0*ld", m, -v);
@@ -236,6 +245,31 @@ extern "C" int ising_write_winding_density_csv(const ising_mesh* m, int replica,
     });
     parts.insert(parts.begin(), std::string("x,y,z,Winding_Density\n"));
     parts.push_back("\n");
+    return write_parts(path, parts, false);
+}
+
+// write_demagnetisation_field_to_file (src/energyMin.f90:559-583): header x,y,z,fx,fy,fz, one
+// record per atom with the single-precision position makeChainMesh stores and the field
+// components, each F8.4.
+extern "C" int ising_write_demag_csv(const ising_mesh* m, int replica, const char* path) {
+    if (!m || !path) return fail(ISING_ERR_ARG, "NULL argument");
+    const Lattice& L = m->lat;
+    const int64_t N = L.natoms;
+    std::vector<double> H((size_t)(3 * N));
+    int st = ising_demag_field(m, replica, H.data());
+    if (st != ISING_OK) return st;
+    std::vector<std::string> parts = format_records(N, 6 * 9, [&](int64_t a, std::string& o) {
+        float p[3];
+        L.position(a, p);
+        fmt::Fw_app(o, (double)p[0], 8, 4); o += ',';
+        fmt::Fw_app(o, (double)p[1], 8, 4); o += ',';
+        fmt::Fw_app(o, (double)p[2], 8, 4); o += ',';
+        fmt::Fw_app(o, H[(size_t)a], 8, 4); o += ',';
+        fmt::Fw_app(o, H[(size_t)(N + a)], 8, 4); o += ',';
+        fmt::Fw_app(o, H[(size_t)(2 * N + a)], 8, 4);
+        o += '\n';
+    });
+    parts.insert(parts.begin(), std::string("x,y,z,fx,fy,fz\n"));
     return write_parts(path, parts, false);
 }
 

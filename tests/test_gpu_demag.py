@@ -63,3 +63,23 @@ def test_metropolis_with_demag_and_pt_refusal(oracle, ib, cuda_ok):
     with pytest.raises(ib.IsingError) as e:
         ib.ParallelTempering(pm, [1.0, 2.0], pd)
     assert e.value.status == 5           # ISING_ERR_UNSUPPORTED
+
+
+def test_demag_csv_bytes(oracle, ib, cuda_ok, tmp_path):
+    """write_demagnetisation_field_to_file: header and one F8.4 record per atom (position as
+    stored in single precision, field components), asterisks where a value does not fit."""
+    om, pm = _pair(oracle, ib, "BCC", (4, 4, 4))
+    s = _random_spins(om.natoms, 74)
+    pm.set_spins(s)
+    path = tmp_path / "demag.csv"
+    ib.write_demagnetisation_field_to_file(pm, str(path))
+    H = ib.demag_field(pm, 0)
+    pos = om.positions().astype(np.float64)
+
+    def f84(v):
+        t = "%8.4f" % v
+        return "*" * 8 if len(t) > 8 else t
+    lines = ["x,y,z,fx,fy,fz"]
+    for i in range(om.natoms):
+        lines.append(",".join(f84(v) for v in (pos[i, 0], pos[i, 1], pos[i, 2], H[i, 0], H[i, 1], H[i, 2])))
+    assert path.read_text() == "\n".join(lines) + "\n"
