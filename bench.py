@@ -954,12 +954,15 @@ def compare_arms(a, b, betas, N):
     """Per temperature slot: E/N, |M|/N, Q, C_v, chi of two recorded series [slot][sample][E,|M|,Qmid,Qmean]
     (E total) with binning (mean) and blocked jackknife (C_v, chi) errors; counts of slots
     within 2 combined standard errors.  A slot whose Q is frozen in both series agrees only
-    when the two frozen values are equal."""
+    when the two frozen values are equal.  A slot counts as resolved for an observable when both
+    series are at least 50 tau_int long (tau of E for C_v, of |M| for chi)."""
     import numpy as np
     from ising_b200 import analysis as A
     R = a.shape[0]
     per = {k: [] for k in ("E", "absM", "Q", "C_v", "chi")}
+    resolved = {k: [] for k in per}
     for t in range(R):
+        taus = {}
         for name, col in (("E", 0), ("absM", 1), ("Q", 3)):
             xa, xb = a[t, :, col], b[t, :, col]
             if col == 0:
@@ -967,6 +970,9 @@ def compare_arms(a, b, betas, N):
             err = float(np.hypot(A.binning_error(xa), A.binning_error(xb)))
             d = float(abs(xa.mean() - xb.mean()))
             per[name].append(d <= 2 * err + 1e-12)
+            # an error bar means something only for series much longer than their tau_int
+            taus[name] = max(A.tau_int(xa), A.tau_int(xb))
+            resolved[name].append(min(len(xa), len(xb)) >= 50 * taus[name])
         for name, col, kind in (("C_v", 0, "cv"), ("chi", 1, "chi")):
             xa, xb = a[t, :, col], b[t, :, col]
             if col == 0:
@@ -974,8 +980,12 @@ def compare_arms(a, b, betas, N):
             va, ea = _jackknife_var_obs(xa, betas[t], N, kind)
             vb, eb = _jackknife_var_obs(xb, betas[t], N, kind)
             per[name].append(abs(va - vb) <= 2 * float(np.hypot(ea, eb)) + 1e-12)
+            resolved[name].append(resolved["E" if col == 0 else "absM"][-1])
     within = {k: int(sum(v)) for k, v in per.items()}
-    return within, {k: [t for t in range(R) if not v[t]] for k, v in per.items()}
+    res = {k: {"resolved_slots": int(sum(resolved[k])),
+               "within_2sigma_of_resolved": int(sum(1 for t in range(R) if resolved[k][t] and per[k][t]))}
+           for k in per}
+    return within, {k: [t for t in range(R) if not v[t]] for k, v in per.items()}, res
 
 
 def learned_vs_plain(args, w):
@@ -1123,7 +1133,7 @@ def learned_vs_plain(args, w):
     qp_s = float(np.mean([ap[t]["ess_Q_per_sampler_s"] for t in live])) if live else 0.0
     ql_s = float(np.mean([al[t]["ess_Q_per_sampler_s"] for t in live])) if live else 0.0
     ratios = [al[t]["ess_Q_per_s"] / ap[t]["ess_Q_per_s"] for t in live if ap[t]["ess_Q_per_s"] > 0]
-    within, outside = compare_arms(sp, sl, betas, N)
+    within, outside, resolved = compare_arms(sp, sl, betas, N)
     reliable = {"plain": sum(1 for t in live if n_plain >= 50 * ap[t]["tau_Q"]),
                 "learned": sum(1 for t in live if n_learned >= 50 * al[t]["tau_Q"]), "of": len(live)}
     q_ess = {
@@ -1141,6 +1151,7 @@ def learned_vs_plain(args, w):
         "E_ess_per_s": {"plain": float(np.mean([x["ess_E_per_s"] for x in ap])),
                         "learned": float(np.mean([x["ess_E_per_s"] for x in al]))},
         "observables_within_2sigma": {"slots": R, **within, "outside": outside,
+                                      "resolved": resolved,
                                       "design": "two independent chains from one thermalised state, "
                                                 "binning errors (means) and blocked jackknife (C_v, chi)"},
         "exchange_every": 1, "thermalisation_sweeps": args.c5_therm, "thermalisation_s": t_therm,
