@@ -16,9 +16,9 @@
 //
 // Per step a thread loads one colour-0 and one colour-1 pair row (both one step ahead) and
 // stores two; the x-neighbour rows of both colours come from the neighbouring thread rows
-// through shared memory (three rotating row slots).  One named barrier per step, split: a
-// thread arrives once its new colour-0 row is in shared memory, draws the Philox numbers of its
-// colour-1 pair (which need no neighbour data) and then waits for the others' rows.  DRAM moves 12 B
+// through shared memory (three rotating row slots).  One mbarrier phase per step: a thread
+// arrives once its new colour-0 row is in shared memory, draws the Philox numbers of its
+// colour-1 pair (which need no neighbour data) and then waits, boundedly, for the others' rows.  DRAM moves 12 B
 // read + 12 B written per site and sweep plus the halo planes' rows, against 36 B for two
 // passes.
 //
@@ -59,7 +59,8 @@ __host__ __device__ __forceinline__ uint32_t fused_smem_floats(uint32_t np, uint
 // replica `rep`.
 template <int MOVE, int DMI, bool HAS_K, int EI>
 __device__ __forceinline__ void run_fused(const EnsParams& P, uint32_t rep, uint32_t sw, uint32_t u, float* sm,
-                                          v2& de, v2& dmx, v2& dmy, v2& dmz) {
+                                          uint64_t* bar, uint32_t& bphase, volatile int* s_abort, v2& de, v2& dmx,
+                                          v2& dmy, v2& dmz) {
     const EnsDev& E = P.e[EI];
     const CbGeom& G = E.g;
     const uint32_t nx = (uint32_t)G.nx, ny = (uint32_t)G.ny, W = G.W, xs = G.row_stride_x, half = G.half, N = E.N;
@@ -145,13 +146,17 @@ __device__ __forceinline__ void run_fused(const EnsParams& P, uint32_t rep, uint
                 if (halo) pfO = ldK(xo, y2);
             }
         }
-        // the new colour-0 rows are published at arrive; the colour-1 pair's Philox draws,
-        // which need none of them, fill the wait
-        asm volatile("bar.arrive 1, %0;" ::"r"(blockDim.x) : "memory");
+        // the new rows are published by the arrival on the step's mbarrier phase (release); the
+        // colour-1 pair's Philox draws, which need none of them, fill the time until every
+        // thread has arrived.  The wait is bounded (st_wait): one that gives up raises the
+        // block's and the engine's abort flags, and every thread then leaves the march.
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(st_smem(bar)) : "memory");
         const bool c1 = active && !halo && t >= 2u;
         uint4 ra = make_uint4(0u, 0u, 0u, 0u), rb = ra;
         if (c1) pair_draws(G, P.rk, x * ny + ym, j, p1, sweep, rep, ra, rb);
-        asm volatile("bar.sync 1, %0;" ::"r"(blockDim.x) : "memory");
+        const bool ok = st_wait(P, bar, bphase & 1u, s_abort);
+        ++bphase;
+        if (!ok) break;
         if (c1) {
             // colour 1 at row yc - 1: its colour-0 neighbours are rows yc-2 .. yc of this plane
             // and row yc - 1 of planes x +- 1 (written last step)
@@ -177,10 +182,19 @@ __global__ void __launch_bounds__(kFuMaxThreads, 1) k_ensembles_fused(const __gr
     __shared__ uint32_t s_task[5];
     __shared__ int s_go, s_fin;
     __shared__ float red[4][kFuMaxThreads / 32];
+    __shared__ __align__(8) uint64_t fu_bar;   // one phase per y-step, all threads arrive
+    __shared__ volatile int fu_abort;
     extern __shared__ __align__(16) float fu_sm[];
     const uint32_t k = P.k;
     const uint32_t tpr = P.tasks_per_round;
     const uint32_t total = tpr * P.rounds;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(st_smem(&fu_bar)), "r"(blockDim.x));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        fu_abort = 0;
+    }
+    __syncthreads();
+    uint32_t bphase = 0;   // steps completed on fu_bar (the same count in every thread)
     uint32_t next = 0;
     if (threadIdx.x == 0) next = atomicAdd(P.head, 1u);
     for (;;) {
@@ -226,7 +240,7 @@ __global__ void __launch_bounds__(kFuMaxThreads, 1) k_ensembles_fused(const __gr
         }
         v2 de = V(0.f), dmx = V(0.f), dmy = V(0.f), dmz = V(0.f);
         switch (e) {
-#define ISG_EC(i) case i: run_fused<MOVE, DMI, HAS_K, i>(P, rep, sw, u, fu_sm, de, dmx, dmy, dmz); break;
+#define ISG_EC(i) case i: run_fused<MOVE, DMI, HAS_K, i>(P, rep, sw, u, fu_sm, &fu_bar, bphase, &fu_abort, de, dmx, dmy, dmz); break;
             ISG_EC(0) ISG_EC(1) ISG_EC(2) ISG_EC(3) ISG_EC(4) ISG_EC(5) ISG_EC(6) ISG_EC(7)
             ISG_EC(8) ISG_EC(9) ISG_EC(10) ISG_EC(11) ISG_EC(12) ISG_EC(13) ISG_EC(14) ISG_EC(15)
 #undef ISG_EC
@@ -247,6 +261,7 @@ __global__ void __launch_bounds__(kFuMaxThreads, 1) k_ensembles_fused(const __gr
             }
         }
         __syncthreads();
+        if (fu_abort) break;   // a step's wait gave up: the unit is incomplete
         if (threadIdx.x == 0) {
             __threadfence();
             st_release(E.done + (size_t)rep * E.nch + u, phi + 1u);
