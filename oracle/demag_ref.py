@@ -13,7 +13,7 @@ Follows src/reciprocalSpaceProcesses.f90 (rsp):
 - calculate_demagnetisation_field (rsp:202-281): H(k) = -(k.M / k^2) k with
   k = 2 pi (wx/N) ar + 2 pi (wy/L) br + 2 pi (wz/M) cr (wy, wz folded to the signed range,
   wx in 0..N/2), the k = 0 bin zero, and every bin with |k_x| > pi/a, |k_y| > pi/b or
-  |k_z| > pi/c set to zero; backward complex-to-real transforms divided by N L M;
+  |k_z| > pi/c set to zero (a, b, c the lattice constants as given); backward complex-to-real transforms divided by N L M;
 - interpolate_fft_to_atoms (rsp:128-176): the same weights carry the grid field back to the
   atoms.
 The constant pi is the reference's default-real literal (src/constants.f90), i.e. pi rounded
@@ -70,7 +70,11 @@ def cic_pairs(mesh):
 def demag_field(mesh, spins):
     """H per atom [natoms, 3] of spins [natoms, 3] (calculate_demagnetisation_field)."""
     nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
-    a, b, c = (float(np.linalg.norm(x)) for x in mesh.vectors()[:3])
+    # the cut-off takes the lattice constants as given (chainMesh%a, %b, %c,
+    # src/chainMesh.f90:792-794), not the lengths of the Bravais vectors, which differ in the
+    # last bits (sin of the single-precision right angle is not 1); on a Nyquist plane
+    # |k_i| equals pi/a_i to rounding, so the choice decides whether that plane is cut
+    a, b, c = mesh.a, mesh.b, mesh.c
     ar, br, cr = mesh.vectors()[3:]
     cell, atom, w = cic_pairs(mesh)
     ncell = nx * ny * nz

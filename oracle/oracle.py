@@ -166,6 +166,7 @@ class Mesh:
         L = lib()
         frac = np.ascontiguousarray(frac, dtype=np.float32)
         self.nx, self.ny, self.nz = nx, ny, nz
+        self.a, self.b, self.c = float(a), float(b), float(c)   # chainMesh%a, %b, %c
         self.nsub = frac.shape[0]
         self.n_shells = n_shells if n_shells > 0 else 2
         self._h = L.ora_mesh_create(frac.ctypes.data_as(C.POINTER(C.c_float)), self.nsub,
