@@ -961,6 +961,7 @@ def compare_arms(a, b, betas, N):
     R = a.shape[0]
     per = {k: [] for k in ("E", "absM", "Q", "C_v", "chi")}
     resolved = {k: [] for k in per}
+    detail = {k: [] for k in ("E", "absM", "Q")}   # [slot, mean a, mean b, 2-sigma bar, tau a, tau b]
     for t in range(R):
         taus = {}
         for name, col in (("E", 0), ("absM", 1), ("Q", 3)):
@@ -971,8 +972,12 @@ def compare_arms(a, b, betas, N):
             d = float(abs(xa.mean() - xb.mean()))
             per[name].append(d <= 2 * err + 1e-12)
             # an error bar means something only for series much longer than their tau_int
-            taus[name] = max(A.tau_int(xa), A.tau_int(xb))
+            ta, tb = A.tau_int(xa), A.tau_int(xb)
+            taus[name] = max(ta, tb)
             resolved[name].append(min(len(xa), len(xb)) >= 50 * taus[name])
+            if not per[name][-1]:
+                detail[name].append([t, float(f"{xa.mean():.6g}"), float(f"{xb.mean():.6g}"),
+                                     float(f"{2 * err:.3g}"), round(float(ta), 1), round(float(tb), 1)])
         for name, col, kind in (("C_v", 0, "cv"), ("chi", 1, "chi")):
             xa, xb = a[t, :, col], b[t, :, col]
             if col == 0:
@@ -985,6 +990,8 @@ def compare_arms(a, b, betas, N):
     res = {k: {"resolved_slots": int(sum(resolved[k])),
                "within_2sigma_of_resolved": int(sum(1 for t in range(R) if resolved[k][t] and per[k][t]))}
            for k in per}
+    for k in ("E", "absM", "Q"):
+        res[k]["detail_outside"] = detail[k]
     return within, {k: [t for t in range(R) if not v[t]] for k, v in per.items()}, res
 
 
@@ -1110,6 +1117,13 @@ def learned_vs_plain(args, w):
             t_learned += timed(lambda: learned_steps(n))
             done_l += n
     sp, sl = plain.series(), learned.series()
+    # the running FP64 accumulators of both arms against a device recomputation of E and M
+    acc_check = {}
+    for name, q, m in (("plain", plain, meshes[0]), ("learned", learned, meshes[1])):
+        e_run, m_run = q.energies()
+        e_dev, m_dev = ib.observables(m, p)
+        acc_check[name] = {"max_abs_dE_per_site": float(np.max(np.abs(e_run - e_dev)) / N),
+                           "max_abs_dM_per_site": float(np.max(np.abs(m_run - m_dev)) / N)}
     # the samplers' own cost per step, without the per-sweep recording of E, |M| and the
     # winding numbers (measurement overhead shared by both arms): relax sweeps record nothing
     c_plain = timed(lambda: plain.relax(100)) / 100
@@ -1155,6 +1169,7 @@ def learned_vs_plain(args, w):
                                       "design": "two independent chains from one thermalised state, "
                                                 "binning errors (means) and blocked jackknife (C_v, chi)"},
         "exchange_every": 1, "thermalisation_sweeps": args.c5_therm, "thermalisation_s": t_therm,
+        "accumulators_vs_recomputed": acc_check,
     }
     training = {"seconds": t_train, "steps": len(losses), "windows": args.c5_train, "epochs": args.c5_epochs,
                 "loss_first": losses[0] if losses else None, "loss_last": losses[-1] if losses else None,

@@ -192,3 +192,29 @@ def test_interpolated_density_csv_bytes(oracle, ib, cuda_ok, tmp_path):
                 out.append(",".join(oracle.fmt_F0(float(v), 8) for v in (*pos, dens[j - 1, k - 1])) + "\n\n")
     out.append("\n")
     assert path.read_text() == "".join(out)
+
+
+@pytest.mark.parametrize("name", ["stereographic", "bloch3"])
+def test_counting_on_known_textures(oracle, ib, cuda_ok, name):
+    """Textures of known winding number (the reference's own stereographic test skyrmion,
+    src/ISING.f90:131-137, Q = -1; three Bloch skyrmions, Q = +3): the device's winding number
+    rounds to Q, its fine density integrates to Q, and its counts equal the independent
+    restatement of the counting stage written from the Fortran text (oracle/skyrmion_count_ref)
+    on the same fine density."""
+    import sys, os
+    sys.path.insert(0, os.path.dirname(__file__))
+    from test_oracle_skyrmion import known_texture
+    from oracle import skyrmion_count_ref as S
+    om, q = known_texture(oracle, name)
+    L = om.nx
+    pm = ib.ChainMesh.simple_cubic(L, L, 4)
+    pm.set_spins(om.spins.copy())
+    ib.set_interpolation_scale(pm, 2, 2)
+    z = 2
+    assert round(ib.calculate_winding_number2(pm, z)) == q
+    dens = ib.calculate_winding_density_interpolated(pm, z)
+    assert abs(dens.sum() - q) < 1e-6
+    for thr, sigma in ((0.5, 1.0), (0.1, 1.0), (0.1, 0.5), (0.01, 1e-5)):
+        want, _ = S.skyrmion_number(dens, L, L, thr, 1, sigma)
+        assert ib.calculate_skyrmion_number(pm, z, thr, 1, sigma) == want, (thr, sigma)
+    pm.close()

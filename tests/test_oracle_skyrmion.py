@@ -99,3 +99,60 @@ def test_skyrmion_distribution_on_hand_case(oracle):
     assert st == 0 and w == [1, 0]
     st, _ = oracle.skyrmion_distribution(d, 10, 10, 1.0, 1, 0.9, 0.1, 60)
     assert st == 5
+
+
+def _bloch_texture(L, nz, R, centres):
+    """z-uniform Bloch skyrmions of radius R (theta = pi (1 - r/R) inside, core down) on a
+    uniform background: total winding number +1 per skyrmion."""
+    x, y = np.meshgrid(np.arange(L, dtype=np.float64), np.arange(L, dtype=np.float64), indexing="ij")
+    theta, phi = np.zeros((L, L)), np.zeros((L, L))
+    for cx, cy in centres:
+        dx = (x - cx + L / 2) % L - L / 2
+        dy = (y - cy + L / 2) % L - L / 2
+        r = np.hypot(dx, dy)
+        inside = r < R
+        theta = np.where(inside, np.pi * (1.0 - r / R), theta)
+        phi = np.where(inside, np.arctan2(dy, dx) + np.pi / 2, phi)
+    s = np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), -np.cos(theta)], axis=-1)
+    return np.repeat(s[:, :, None, :], nz, axis=2).reshape(-1, 3)
+
+
+KNOWN_TEXTURES = {
+    # the reference's own test skyrmion (src/ISING.f90:131-137: centre mid-mesh, R_s = a,
+    # chi = 3.12/2, N = 1; src/LLG.f90:28-73): winding number -1
+    "stereographic": (24, -1),
+    # three Bloch skyrmions of radius L/6: winding number +3
+    "bloch3": (24, 3),
+}
+
+
+def known_texture(oracle, name):
+    L, q = KNOWN_TEXTURES[name]
+    om = oracle.Mesh.sc(L, L, 4)
+    if name == "stereographic":
+        om.init_skyrmion(L / 2, L / 2, 1.0, 1.56, 1)
+    else:
+        om.set_spins(_bloch_texture(L, 4, L / 6, [(L / 4, L / 4), (3 * L / 4, L / 3), (L / 2, 3 * L / 4)]))
+    return om, q
+
+
+@pytest.mark.parametrize("name", sorted(KNOWN_TEXTURES))
+def test_counting_on_known_textures_matches_second_restatement(oracle, name):
+    """The C oracle's count equals an independent restatement written from the Fortran text on
+    textures of known winding number.  The counts are the reference's, not the number of
+    skyrmions: the last loop adds one per CELL of a matching region, and regions of a filtered
+    density rarely integrate to within 0.05 of 1."""
+    from oracle import skyrmion_count_ref as S
+    om, q = known_texture(oracle, name)
+    L = om.nx
+    z = 2
+    assert round(om.winding_number(z)) == q
+    dens = oracle.winding_density_interpolated(om, z, 1, 1)
+    assert abs(dens.sum() - q) < 1e-6
+    seen = set()
+    for thr in (0.5, 0.1, 0.01):
+        for sigma in (1.0, 0.5, 1e-5):
+            want, accs = S.skyrmion_number(dens, L, L, thr, 1, sigma)
+            assert oracle.skyrmion_number(dens, L, L, thr, 1, sigma) == (0, want), (thr, sigma)
+            seen.add(want)
+    assert seen - {0} or name == "stereographic"   # the Bloch texture reaches the per-cell count
