@@ -229,6 +229,7 @@ struct SweepPlan {
     Slot* d_slots = nullptr;   // general path: stencil buffers this plan reads
     int* d_count = nullptr;
     const float* demag = nullptr;   // general path: demagnetising field of the swept replica
+    int oct_maxcnt = 0;        // octant layout: k_octant_fast's table width (0: k_octant_colour)
 };
 
 // Fills plan for Hamiltonian p; the general path uploads its stencil into (slots, count).
@@ -257,6 +258,31 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
         const int ng = (int)m->oct_rank0.size() - 1;
         for (int k = 0; k < 8 * ng; ++k)
             tot += octant_slots_for(m->layout.q8 * (m->oct_rank0[k % ng + 1] - m->oct_rank0[k % ng]));
+        // the per-class stencil of k_octant_fast: every packed offset floor((o + d) / 2),
+        // o in {0, 1}, must lie within one period of its axis
+        std::vector<Slot> hs((size_t)kMaxSub * kMaxSlots);
+        std::vector<int> hc(kMaxSub, 0);
+        ISG_TRY(fill_query_stencil_host(m, p, false, hs.data(), hc.data()));
+        const Lattice& Lt = m->lat;
+        const int half[3] = {Lt.nx / 2, Lt.ny / 2, Lt.nz / 2};
+        int maxcnt = 0;
+        bool fits = true;
+        for (int sub = 0; sub < Lt.nsub; ++sub) {
+            maxcnt = std::max(maxcnt, hc[sub]);
+            for (int q = 0; q < hc[sub]; ++q) {
+                const Slot& e = hs[(size_t)sub * kMaxSlots + q];
+                const int d[3] = {e.dx, e.dy, e.dz};
+                for (int ax = 0; ax < 3; ++ax)
+                    for (int o = 0; o < 2; ++o) {
+                        const int t = o + d[ax];
+                        const int ex = (t - (t & 1)) / 2;
+                        if (ex < -half[ax] || ex > half[ax]) fits = false;
+                    }
+            }
+        }
+        plan->oct_maxcnt = fits ? std::max(maxcnt, 1) : 0;
+        // replicas per L2 group: a group runs all its sweeps before the next group starts
+        plan->group = std::max(1, (int)(kL2GroupBytes / (12.0 * (double)Lt.natoms)));
     } else {
         for (int k = 0; k < plan->col->ncol; ++k)
             tot += general_slots_for(plan->col->class_start[k + 1] - plan->col->class_start[k]);
@@ -329,15 +355,24 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
     g.partials = partials; g.slots_per_rep = plan.slots_per_rep; g.status = m->d_status;
     g.demag = plan.demag; g.mu0 = (float)kMu0;
     if (m->layout.cb == 2) {   // octant classes: contiguous storage ranges
+        // replicas are independent: each L2-sized group of replicas runs all its sweeps
+        // (every class, in order) before the next group starts, so a group's spins stay in L2
         const int ng = (int)m->oct_rank0.size() - 1;
-        for (int sw = 0; sw < n_sweeps; ++sw) {
-            g.sweep_offset = sw0 + (uint32_t)sw;
-            int slot = 0;
-            for (int k = 0; k < 8 * ng; ++k) {
-                const int gi = k % ng, r0 = m->oct_rank0[gi], nr = m->oct_rank0[gi + 1] - r0;
-                g.slot_base = slot;
-                ISG_TRY(launch_octant_colour(g, k / ng, r0, nr, m->stream));
-                slot += octant_slots_for(m->layout.q8 * nr);
+        g.oct_maxcnt = plan.oct_maxcnt;
+        const int G = std::max(1, plan.group);
+        for (int gr = 0; gr < n_rep; gr += G) {
+            g.rep_first = rep_first + gr;
+            g.n_rep = std::min(G, n_rep - gr);
+            g.spins = m->d_spins + (int64_t)g.rep_first * 3 * L.natoms;
+            for (int sw = 0; sw < n_sweeps; ++sw) {
+                g.sweep_offset = sw0 + (uint32_t)sw;
+                int slot = 0;
+                for (int k = 0; k < 8 * ng; ++k) {
+                    const int gi = k % ng, r0 = m->oct_rank0[gi], nr = m->oct_rank0[gi + 1] - r0;
+                    g.slot_base = slot;
+                    ISG_TRY(launch_octant_colour(g, k / ng, r0, nr, m->stream));
+                    slot += octant_slots_for(m->layout.q8 * nr);
+                }
             }
         }
         return ISING_OK;
@@ -1092,9 +1127,12 @@ int pt_enqueue_round(ising_pt* pt, int k) {
                               pt->opt.r, pt->d_partials));
         {
             ISG_TRY(launch_fold_partials(pt->d_partials, pt->plan.slots_per_rep, n, pt->d_acc, m->stream));
+            // FP64, as the reference computes arc_winding: in FP32 a nearly antiparallel
+            // neighbour pair rounds 1 + s_i.s_j to <= 0, and the normalisation sqrt of the
+            // Berg-Luscher term is NaN (seen in hot replicas every few hundred sweeps)
             WindingLaunch w{};
             w.spins = m->d_spins; w.natoms = m->lat.natoms; w.nx = m->lat.nx; w.ny = m->lat.ny; w.nz = m->lat.nz;
-            w.nsub = m->lat.nsub; w.n_rep = n; w.plaq = m->d_plaq; w.layout = m->layout; w.out = pt->d_q; w.fp64 = 0;
+            w.nsub = m->lat.nsub; w.n_rep = n; w.plaq = m->d_plaq; w.layout = m->layout; w.out = pt->d_q; w.fp64 = 1;
             ISG_TRY(launch_winding(w, m->stream));
             RecordLaunch rl{};
             rl.acc = pt->d_acc; rl.q = pt->d_q; rl.t2r = pt->d_t2r; rl.nz = m->lat.nz; rl.n_rep = n;

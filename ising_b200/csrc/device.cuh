@@ -88,6 +88,29 @@ __device__ __forceinline__ f3 propose(f3 s, float u0, float u1, float u2, float 
 }
 #endif  // __CUDACC__
 
+// Unsigned 32-bit division by an invariant divisor (Granlund & Montgomery, PLDI'94, round-up
+// method): q = (t + ((n - t) >> 1)) >> (l - 1) with t = mulhi(m, n).
+struct FastDiv {
+    uint32_t d, m;
+    int l;
+};
+inline FastDiv make_div(uint32_t d) {
+    FastDiv f;
+    f.d = d;
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    f.l = l;
+    f.m = (uint32_t)((((1ull << l) - d) << 32) / d + 1);
+    return f;
+}
+#if defined(__CUDACC__)
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
+    if (f.l == 0) return n;   // d == 1
+    const uint32_t t = __umulhi(f.m, n);
+    return (t + ((n - t) >> 1)) >> (f.l - 1);
+}
+#endif  // __CUDACC__
+
 // ---------------------------------------------------------------- kernel-facing structs
 // FP32 Hamiltonian as the kernels consume it.
 struct HamDev {

@@ -72,14 +72,11 @@ __device__ __forceinline__ f3 stencil_field(const float* sx, const float* sy, co
 // Metropolis update of one site (ix, iy, iz, sub), reference atom index `at`, with the local
 // field of its stencil; accepted moves add to the running sums.
 template <int MOVE>
-__device__ __forceinline__ void general_site(const GeneralLaunch& a, const Slot* sl, const int* cnt, float* sx,
-                                             float* sy, float* sz, int64_t at, int ix, int iy, int iz, int sub,
-                                             uint32_t sweep, int rep, float beta, float& de, float& dmx, float& dmy,
-                                             float& dmz) {
+__device__ __forceinline__ void site_update(const GeneralLaunch& a, f3 h, int64_t si, int64_t at, float* sx,
+                                            float* sy, float* sz, uint32_t sweep, int rep, float beta, float& de,
+                                            float& dmx, float& dmy, float& dmz) {
     const HamDev& H = a.ham;
-    f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.layout);
     h.z -= H.Bz;
-    const int64_t si = sidx(a.layout, ix, iy, iz, sub);
     if (a.demag) {   // -mu_0 S.H of calculateHeisenbergEnergy (src/energyMin.f90:163-167)
         const int64_t N = a.natoms;
         h.x = fmaf(-a.mu0, a.demag[si], h.x);
@@ -101,6 +98,15 @@ __device__ __forceinline__ void general_site(const GeneralLaunch& a, const Slot*
         sx[si] = sp.x; sy[si] = sp.y; sz[si] = sp.z;
         de += dE; dmx += sp.x - s.x; dmy += sp.y - s.y; dmz += sp.z - s.z;
     }
+}
+
+template <int MOVE>
+__device__ __forceinline__ void general_site(const GeneralLaunch& a, const Slot* sl, const int* cnt, float* sx,
+                                             float* sy, float* sz, int64_t at, int ix, int iy, int iz, int sub,
+                                             uint32_t sweep, int rep, float beta, float& de, float& dmx, float& dmy,
+                                             float& dmz) {
+    const f3 h = stencil_field(sx, sy, sz, sl + sub * kMaxSlots, cnt[sub], ix, iy, iz, a.layout);
+    site_update<MOVE>(a, h, sidx(a.layout, ix, iy, iz, sub), at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
 }
 
 template <int MOVE>
@@ -187,6 +193,115 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_colour(GeneralLaunch a, 
     }
 }
 
+// The same class with the stencil resolved per class: a neighbour of the site at packed cell
+// (X, Y, Z) of octant o through cell offset d lies in octant (o + d) & 1 per axis, at packed
+// cell X + floor((o_x + d_x) / 2) (and so on) of its sublattice's plane, so per (rank, slot)
+// the plane base and three packed offsets are fixed for the whole class.  The block resolves
+// them into shared memory once; a site then needs three compare-and-wrap steps and one
+// multiply-add chain per neighbour instead of the cell-coordinate modulo and octant decode
+// of sidx.  Every packed offset is within one period (the launcher checks), the summation
+// order is the stencil's, and the update is the one of k_octant_colour, bit for bit.
+struct __align__(16) OctSlot {
+    int plane;               // (octant * nsub + storage rank) * q8 of the neighbour
+    int8_t ex, ey, ez, pad;  // packed-cell offsets
+    float w, Dx, Dy, Dz;
+    float pad2[2];           // 32 bytes: two 16-byte shared-memory loads
+};
+struct OctDims {
+    FastDiv q8, hz, hy;
+    int hx, hyi, hzi;
+};
+
+template <int MOVE>
+__global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, OctDims od, int oct, int rank0,
+                                                              int nrank) {
+    extern __shared__ __align__(16) unsigned char oct_smem[];
+    const int mc = a.oct_maxcnt;
+    OctSlot* tab = reinterpret_cast<OctSlot*>(oct_smem);
+    int* s_cnt = reinterpret_cast<int*>(tab + nrank * mc);
+    int* s_sub = s_cnt + nrank;
+    __shared__ int s_srank[kMaxSub], s_sofr[kMaxSub];
+    const Layout& L = a.layout;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < kMaxSub; ++k) { s_srank[k] = L.srank[k]; s_sofr[k] = L.sofr[k]; }
+    }
+    __syncthreads();
+    const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
+    const int q8 = (int)L.q8;
+    for (int e = threadIdx.x; e < nrank * mc; e += blockDim.x) {
+        const int lr = e / mc, q = e - lr * mc;
+        const int sub = s_sofr[rank0 + lr];
+        OctSlot o{};
+        if (q < a.st.count[sub]) {
+            const Slot sl = a.st.slots[sub * kMaxSlots + q];
+            const int tx = ox + sl.dx, ty = oy + sl.dy, tz = oz + sl.dz;
+            const int o2 = ((tx & 1) << 2) | ((ty & 1) << 1) | (tz & 1);
+            o.plane = (o2 * a.nsub + s_srank[sl.sub]) * q8;
+            o.ex = (int8_t)(tx >> 1); o.ey = (int8_t)(ty >> 1); o.ez = (int8_t)(tz >> 1);
+            o.w = sl.w; o.Dx = sl.Dx; o.Dy = sl.Dy; o.Dz = sl.Dz;
+        }
+        tab[e] = o;
+    }
+    for (int lr = threadIdx.x; lr < nrank; lr += blockDim.x) {
+        s_sub[lr] = s_sofr[rank0 + lr];
+        s_cnt[lr] = a.st.count[s_sub[lr]];
+    }
+    __syncthreads();
+    const int rl = blockIdx.y;
+    const int rep = a.rep_first + rl;
+    const int64_t N = a.natoms;
+    float* __restrict__ sx = a.spins + (int64_t)rl * 3 * N;
+    float* __restrict__ sy = sx + N;
+    float* __restrict__ sz = sy + N;
+    const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
+    const float beta = (float)a.beta_rep[rep];
+    const uint32_t n = (uint32_t)q8 * (uint32_t)nrank;
+    const int hx = od.hx, hy = od.hyi, hz = od.hzi;
+    const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
+    float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
+    const uint32_t base = blockIdx.x * (uint32_t)(blockDim.x * kGenSitesPerThread);
+    for (int it = 0; it < kGenSitesPerThread; ++it) {
+        const uint32_t t = base + it * blockDim.x + threadIdx.x;
+        if (t >= n) break;
+        const uint32_t lr = fdiv(t, od.q8);
+        const uint32_t pc = t - lr * (uint32_t)q8;
+        const uint32_t r = fdiv(pc, od.hz);
+        const int Z = (int)(pc - r * (uint32_t)hz);
+        const uint32_t Xu = fdiv(r, od.hy);
+        const int Y = (int)(r - Xu * (uint32_t)hy), X = (int)Xu;
+        const int sub = s_sub[lr];
+        const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z + oz;
+        const uint32_t at = ((uint32_t)(ix * a.ny + iy) * (uint32_t)a.nz + (uint32_t)iz) * (uint32_t)a.nsub + sub;
+        const OctSlot* ts = tab + lr * mc;
+        f3 h = {0.f, 0.f, 0.f};
+        const int cn = s_cnt[lr];
+        for (int q = 0; q < cn; ++q) {
+            const OctSlot o = ts[q];
+            int jx = X + o.ex, jy = Y + o.ey, jz = Z + o.ez;
+            jx += jx < 0 ? hx : 0; jx -= jx >= hx ? hx : 0;
+            jy += jy < 0 ? hy : 0; jy -= jy >= hy ? hy : 0;
+            jz += jz < 0 ? hz : 0; jz -= jz >= hz ? hz : 0;
+            const uint32_t j = (uint32_t)o.plane + (uint32_t)((jx * hy + jy) * hz + jz);
+            const f3 sj = {sx[j], sy[j], sz[j]};
+            const f3 c = cross(sj, mk(o.Dx, o.Dy, o.Dz));
+            h.x += fmaf(o.w, sj.x, c.x);
+            h.y += fmaf(o.w, sj.y, c.y);
+            h.z += fmaf(o.w, sj.z, c.z);
+        }
+        site_update<MOVE>(a, h, (int64_t)(class_base + t), (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
+                          dmz);
+    }
+    if (a.partials) {
+        __shared__ double tot[4];
+        block_sum4<double>(de, dmx, dmy, dmz, tot);
+        if (threadIdx.x == 0) {
+            double* p = a.partials + ((int64_t)rep * a.slots_per_rep + a.slot_base + blockIdx.x) * 4;
+            p[0] += tot[0]; p[1] += tot[1]; p[2] += tot[2]; p[3] += tot[3];
+        }
+    }
+}
+
 int octant_slots_for(int64_t n_sites) {
     const int64_t per = (int64_t)kGenThreads * kGenSitesPerThread;
     return (int)((n_sites + per - 1) / per);
@@ -198,6 +313,18 @@ int launch_octant_colour(const GeneralLaunch& a, int oct, int rank0, int nrank, 
     if (oct < 0 || oct > 7 || rank0 < 0 || nrank < 1 || rank0 + nrank > a.nsub)
         return fail(ISING_ERR_ARG, "octant class out of range");
     dim3 g(octant_slots_for(n), a.n_rep), b(kGenThreads);
+    if (a.oct_maxcnt > 0) {
+        OctDims od;
+        od.q8 = make_div((uint32_t)a.layout.q8);
+        od.hx = a.nx / 2; od.hyi = a.ny / 2; od.hzi = a.nz / 2;
+        od.hz = make_div((uint32_t)od.hzi);
+        od.hy = make_div((uint32_t)od.hyi);
+        const size_t sm = (size_t)nrank * a.oct_maxcnt * sizeof(OctSlot) + 2 * (size_t)nrank * sizeof(int);
+        if (a.move == 0) k_octant_fast<0><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
+        else k_octant_fast<1><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
+        ISG_CUDA(cudaGetLastError());
+        return ISING_OK;
+    }
     size_t sm = (size_t)a.st.nsub * kMaxSlots * sizeof(Slot) + kMaxSub * sizeof(int);
     if (a.move == 0) k_octant_colour<0><<<g, b, sm, s>>>(a, oct, rank0, nrank);
     else k_octant_colour<1><<<g, b, sm, s>>>(a, oct, rank0, nrank);

@@ -10,8 +10,9 @@ Follows src/reciprocalSpaceProcesses.f90 (rsp):
 - calculate_skyrmion_number (rsp:627-812) after its interpolation step: mask |d| > q max|d|;
   a cell starts a region when it is masked, unvisited and a local maximum of |d| against its 8
   neighbours taken modulo the COARSE cell counts (rsp:711-712); the region grows by a stack
-  flood fill over masked, unvisited, downhill neighbours (add_neighbors_to_stack, rsp:582-625,
-  periodic on the fine grid, downhill = |d(i,j)| >= |d(n)| - 1e-10); the final loop runs over
+  flood fill over masked, unvisited, downhill neighbours (add_neighbors_to_stack, rsp:582-625:
+  a neighbour index below 1 becomes the COARSE count and one above the coarse count becomes 1,
+  rsp:596-607; downhill = |d(i,j)| >= |d(n)| - 1e-10); the final loop runs over
   CELLS and adds nint(sign(acc)) for every cell of an unmerged region whose |acc| is within 0.05
   of particle_number (rsp:764-773), and marks pairs of neighbouring regions (coarse modulo
   again) merged when their sum is.
@@ -64,7 +65,9 @@ def skyrmion_number(dens, ncx, ncy, q_threshold, particle_number, sigma):
             def push(ci, cj):
                 for di in (-1, 0, 1):
                     for dj in (-1, 0, 1):
-                        x, y = (ci + di) % n, (cj + dj) % l
+                        x, y = ci + di, cj + dj            # 0-based form of the coarse wrap
+                        x = ncx - 1 if x < 0 else (0 if x > ncx - 1 else x)
+                        y = ncy - 1 if y < 0 else (0 if y > ncy - 1 else y)
                         if in_stack[x, y]:
                             continue
                         if not visited[x, y] and mask[x, y] and ad[ci, cj] >= ad[x, y] - 1e-10:
