@@ -139,6 +139,7 @@ int mesh_settle(const ising_mesh* m);
 namespace isg {
 constexpr int kScratchDoubles = 1 << 16;
 constexpr double kL2GroupBytes = 64.0e6;   // replica group size of the paired colour schedule
+constexpr int64_t kOctMinLaunchSites = 148 * 2048;   // octant classes: sites per launch to fill the GPU
 
 // Kernel launchers.
 // Colour-separated checkerboard sweep (sweep_cb.cu): up to two segments per launch, each a
@@ -200,7 +201,7 @@ int launch_general_colour(const GeneralLaunch& a, cudaStream_t s);
 // One class (octant, sublattice group) of an octant-layout mesh: sites of storage ranks
 // [rank0, rank0 + nrank) of that octant (a.sites and a.n_sites unused).
 int launch_octant_colour(const GeneralLaunch& a, int octant, int rank0, int nrank, cudaStream_t s);
-int octant_slots_for(int64_t n_sites);
+int octant_slots_for(int64_t n_sites, bool fast);   // partial-sum slots (blocks) of one class launch
 int general_slots_for(int n_sites);
 
 struct ReduceLaunch {

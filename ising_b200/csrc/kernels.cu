@@ -260,10 +260,10 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
     const int hx = od.hx, hy = od.hyi, hz = od.hzi;
     const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
     float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
-    const uint32_t base = blockIdx.x * (uint32_t)(blockDim.x * kGenSitesPerThread);
-    for (int it = 0; it < kGenSitesPerThread; ++it) {
-        const uint32_t t = base + it * blockDim.x + threadIdx.x;
-        if (t >= n) break;
+    // one site per thread: a class of a small mesh still fills the GPU
+    {
+        const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= n) goto done;
         const uint32_t lr = fdiv(t, od.q8);
         const uint32_t pc = t - lr * (uint32_t)q8;
         const uint32_t r = fdiv(pc, od.hz);
@@ -292,6 +292,7 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
         site_update<MOVE>(a, h, (int64_t)(class_base + t), (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
                           dmz);
     }
+done:
     if (a.partials) {
         __shared__ double tot[4];
         block_sum4<double>(de, dmx, dmy, dmz, tot);
@@ -302,8 +303,8 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
     }
 }
 
-int octant_slots_for(int64_t n_sites) {
-    const int64_t per = (int64_t)kGenThreads * kGenSitesPerThread;
+int octant_slots_for(int64_t n_sites, bool fast) {
+    const int64_t per = (int64_t)kGenThreads * (fast ? 1 : kGenSitesPerThread);
     return (int)((n_sites + per - 1) / per);
 }
 
@@ -312,7 +313,7 @@ int launch_octant_colour(const GeneralLaunch& a, int oct, int rank0, int nrank, 
     if (n <= 0) return ISING_OK;
     if (oct < 0 || oct > 7 || rank0 < 0 || nrank < 1 || rank0 + nrank > a.nsub)
         return fail(ISING_ERR_ARG, "octant class out of range");
-    dim3 g(octant_slots_for(n), a.n_rep), b(kGenThreads);
+    dim3 g(octant_slots_for(n, a.oct_maxcnt > 0), a.n_rep), b(kGenThreads);
     if (a.oct_maxcnt > 0) {
         OctDims od;
         od.q8 = make_div((uint32_t)a.layout.q8);

@@ -324,9 +324,6 @@ def test_error_paths(ib, cuda_ok):
         pm.set_spins(s)
     assert e.value.status == 2
     with pytest.raises(ib.IsingError) as e:
-        ib.metropolis_mcs(pm, 1.0, 1, -1.0, 0.0, 0.3, 0.0, 0.1, 0.2, demag=True)
-    assert e.value.status == 5
-    with pytest.raises(ib.IsingError) as e:
         pm.get_spins(3)
     assert e.value.status == 3
     with pytest.raises(ib.IsingError) as e:
