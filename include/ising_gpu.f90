@@ -47,7 +47,7 @@ module ising_gpu
   ! pass over two spin buffers (even sweeps_per_swap)
   integer(c_int), parameter :: ISING_ENS_ORDER_PHASE = 0, ISING_ENS_ORDER_GROUPS = 1, ISING_ENS_ORDER_WAVE = 2
   integer(c_int), parameter :: ISING_ENS_LOADER_REGISTERS = 0, ISING_ENS_LOADER_STAGED = 1, &
-      ISING_ENS_LOADER_FUSED = 2, ISING_ENS_LOADER_PIPELINED = 3
+      ISING_ENS_LOADER_FUSED = 2
   type, bind(C) :: ising_ensembles_schedule
     integer(c_int) :: block_threads, chunk_pairs, order
     integer(c_int64_t) :: group_bytes

@@ -364,13 +364,10 @@ typedef struct {
                                           spin buffer and writing a second one the engine
                                           allocates; sweeps_per_swap must be even.  Bit-identical
                                           to the other loaders. */
-#define ISING_ENS_LOADER_PIPELINED 3   /* the register loader with each thread's loads of the next
-                                          row issued before the current row's update (32..128-
-                                          thread blocks, three per SM); bit-identical */
 
 /* One schedule: block size, target site pairs per task, queue order, group size, loader. */
 typedef struct {
-    int block_threads;        /* 64..256 (fused loader 128..512, pipelined 32..128), whole warps */
+    int block_threads;        /* 64..256 (fused loader 128..512), whole warps */
     int chunk_pairs;          /* site pairs of one colour per task (whole x-planes) */
     int order;                /* ISING_ENS_ORDER_* */
     int64_t group_bytes;      /* ISING_ENS_ORDER_GROUPS: spin bytes per replica group */

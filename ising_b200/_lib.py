@@ -68,7 +68,7 @@ class EnsSchedule(C.Structure):
 
 
 ENS_ORDER_PHASE, ENS_ORDER_GROUPS, ENS_ORDER_WAVE = 0, 1, 2
-ENS_LOADER_REGISTERS, ENS_LOADER_STAGED, ENS_LOADER_FUSED, ENS_LOADER_PIPELINED = 0, 1, 2, 3
+ENS_LOADER_REGISTERS, ENS_LOADER_STAGED, ENS_LOADER_FUSED = 0, 1, 2
 
 _P = C.POINTER
 _d, _i, _i64, _u32, _u64, _vp = C.c_double, C.c_int, C.c_int64, C.c_uint32, C.c_uint64, C.c_void_p

@@ -599,7 +599,7 @@ class ParallelTempering:
 
 
 _ORDER_NAMES = {0: "phase", 1: "groups", 2: "wave"}
-_LOADER_NAMES = {0: "registers", 1: "staged", 2: "fused", 3: "pipelined"}
+_LOADER_NAMES = {0: "registers", 1: "staged", 2: "fused"}
 
 
 class Ensembles:
@@ -661,8 +661,7 @@ class Ensembles:
         """loader 0: neighbours loaded per thread; 1: rows staged in shared memory by TMA
         (nz = 128 and nx % 4 == 0 in every ensemble, 256-thread blocks); 2: both colour passes
         of a sweep fused into one pass over ping-pong buffers (128..512-thread blocks of at
-        least nz threads; even sweeps_per_swap); 3: loader 0 with each thread's next-row loads
-        issued before the current row's update (32..128-thread blocks)."""
+        least nz threads; even sweeps_per_swap)."""
         c = EnsSchedule(block_threads, chunk_pairs, order, group_bytes, 0.0, loader)
         _lib.call("ising_ensembles_set_schedule", self._h, C.byref(c))
 

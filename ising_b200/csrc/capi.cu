@@ -1614,13 +1614,9 @@ bool ens_staged_fits(const ising_ensembles* s) {
 // Chunking, grid and buffers for schedule `c`.
 int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) {
     const bool fused = c.loader == ISING_ENS_LOADER_FUSED;
-    const bool pipe = c.loader == ISING_ENS_LOADER_PIPELINED;
     if (fused) {
         if (c.block_threads < 128 || c.block_threads > kFuMaxThreads || c.block_threads % 32)
             return fail(ISING_ERR_ARG, "the fused loader runs 128..512-thread blocks in whole warps");
-    } else if (pipe) {
-        if (c.block_threads < 32 || c.block_threads > kEnsPipeThreads || c.block_threads % 32)
-            return fail(ISING_ERR_ARG, "the pipelined loader runs 32..128-thread blocks in whole warps");
     } else if (c.block_threads < 64 || c.block_threads > kEnsMaxThreads || c.block_threads % 32) {
         return fail(ISING_ERR_ARG, "block_threads must be 64..256 in whole warps");
     }
@@ -1628,8 +1624,8 @@ int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) 
     if (c.order != ISING_ENS_ORDER_PHASE && c.order != ISING_ENS_ORDER_GROUPS && c.order != ISING_ENS_ORDER_WAVE)
         return fail(ISING_ERR_ARG, "order must be ISING_ENS_ORDER_PHASE, _GROUPS or _WAVE");
     if (c.order == ISING_ENS_ORDER_GROUPS && c.group_bytes < 1) return fail(ISING_ERR_ARG, "group_bytes must be >= 1");
-    if (c.loader != ISING_ENS_LOADER_REGISTERS && c.loader != ISING_ENS_LOADER_STAGED && !fused && !pipe)
-        return fail(ISING_ERR_ARG, "loader must be ISING_ENS_LOADER_REGISTERS, _STAGED, _FUSED or _PIPELINED");
+    if (c.loader != ISING_ENS_LOADER_REGISTERS && c.loader != ISING_ENS_LOADER_STAGED && !fused)
+        return fail(ISING_ERR_ARG, "loader must be ISING_ENS_LOADER_REGISTERS, _STAGED or _FUSED");
     if (fused && c.order != ISING_ENS_ORDER_PHASE) return fail(ISING_ERR_ARG, "the fused loader queues in phase order");
     const bool staged = c.loader == ISING_ENS_LOADER_STAGED;
     if (staged) {
@@ -1678,7 +1674,7 @@ int ens_apply_schedule(ising_ensembles* s, const ising_ensembles_schedule_t& c) 
         done += (size_t)h.n * h.nch;
     }
     if (fu_smem > 227u * 1024u) return fail(ISING_ERR_ARG, "fused loader: rows of the chunk exceed shared memory");
-    const int loader = fused ? 2 : (staged ? 1 : (pipe ? 3 : 0));
+    const int loader = fused ? 2 : (staged ? 1 : 0);
     int per_sm = 0;
     ISG_TRY(ensembles_blocks_per_sm(s->move, s->dmi, s->has_k, loader, c.block_threads, fu_smem, &per_sm));
     if (per_sm < 1) return fail(ISING_ERR_CUDA, "persistent engine kernel cannot be resident");
@@ -1868,8 +1864,7 @@ int ens_enqueue_launch(ising_ensembles* s, int k, int rounds, int stall) {
                 return fail(ISING_ERR_CUDA, "cuTensorMapEncodeTiled (staged loader) failed");
         }
     ISG_CUDA(cudaMemsetAsync(s->d_sync, 0, s->sync_words * sizeof(uint32_t), s->stream));
-    const int loader = s->sched.loader == ISING_ENS_LOADER_FUSED ? 2
-                       : (staged ? 1 : (s->sched.loader == ISING_ENS_LOADER_PIPELINED ? 3 : 0));
+    const int loader = s->sched.loader == ISING_ENS_LOADER_FUSED ? 2 : (staged ? 1 : 0);
     return launch_ensembles(P, s->move, s->dmi, s->has_k, loader, s->sched.block_threads, s->grid, s->fu_smem,
                             s->stream);
 }
@@ -2122,9 +2117,6 @@ extern "C" int ising_ensembles_autotune(ising_ensembles* s, int k, int rounds_pe
     for (int c : {512, 1024}) cand.push_back({128, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_REGISTERS});
     if (max_lanes <= 64)      // two-warp blocks (8 per SM, the same 16 warps) with small tasks
         for (int c : {2048, 4096}) cand.push_back({64, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_REGISTERS});
-    // the pipelined march: more registers per thread, so three 128-thread blocks per SM
-    if (max_lanes <= 128)
-        for (int c : {1024, 4096, 8192, 16384}) cand.push_back({128, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_PIPELINED});
     if (ens_staged_fits(s))   // groups of 4, 8 and 16 x-planes per task at nz = 128
         for (int c : {16384, 32768, 65536}) cand.push_back({256, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_STAGED});
     if (k % 2 == 0)           // one pass per sweep: chunk widths by block size, y-segments by chunk_pairs

@@ -41,7 +41,7 @@ int ensembles_blocks_per_sm(int move, int dmi, bool has_k, int loader, int threa
 
 int launch_ensembles(const EnsParams& P, int move, int dmi, bool has_k, int loader, int threads, int grid,
                      size_t smem, cudaStream_t s) {
-    const int maxt = loader == 2 ? kFuMaxThreads : (loader == 3 ? kEnsPipeThreads : kEnsMaxThreads);
+    const int maxt = loader == 2 ? kFuMaxThreads : kEnsMaxThreads;
     if (threads < 32 || threads > maxt || threads % 32) return fail(ISING_ERR_ARG, "block size out of range for the loader");
     if (loader == 1 && threads != kStSub * kStG * 32) return fail(ISING_ERR_ARG, "the staged loader runs 256-thread blocks");
     if (P.n_ens < 1 || P.n_ens > kMaxEnsembles) return fail(ISING_ERR_ARG, "1..16 ensembles per engine");

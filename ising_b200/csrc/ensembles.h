@@ -17,7 +17,6 @@ namespace isg {
 
 constexpr int kMaxEnsembles = 16;   // compile-time slots of the kernel's ensemble switch
 constexpr int kEnsMaxThreads = 256;
-constexpr int kEnsPipeThreads = 128;   // pipelined register loader: block size cap (3 blocks per SM)
 
 struct EnsDev {
     CbGeom g;                    // geometry and Hamiltonian for the pair update

@@ -7,9 +7,8 @@ namespace isg {
 template <int D, bool K>
 static const void* fn(int loader) {
     if (loader == 2) return reinterpret_cast<const void*>(&k_ensembles_fused<1, D, K>);
-    if (loader == 3) return reinterpret_cast<const void*>(&k_ensembles<1, D, K, 3>);
-    return loader == 1 ? reinterpret_cast<const void*>(&k_ensembles<1, D, K, 1>)
-                       : reinterpret_cast<const void*>(&k_ensembles<1, D, K, 0>);
+    return loader == 1 ? reinterpret_cast<const void*>(&k_ensembles<1, D, K, true>)
+                       : reinterpret_cast<const void*>(&k_ensembles<1, D, K, false>);
 }
 
 const void* ensembles_kernel_ball(int dmi, bool has_k, int loader) {

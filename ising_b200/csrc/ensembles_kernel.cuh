@@ -90,7 +90,7 @@ static __device__ __forceinline__ void finish_round(const EnsParams& P, const En
 
 // One task's colour pass over x-planes [x0, x1): columns (plane, y-segment), nseg segments
 // per plane so that every thread row is busy, each marched along y (march_column).
-template <int MOVE, int DMI, bool HAS_K, int EI, bool PIPE>
+template <int MOVE, int DMI, bool HAS_K, int EI>
 __device__ __forceinline__ void run_chunk(const EnsParams& P, uint32_t rep, uint32_t ph, uint32_t ch,
                                           v2& de, v2& dmx, v2& dmy, v2& dmz) {
     const EnsDev& E = P.e[EI];
@@ -113,12 +113,8 @@ __device__ __forceinline__ void run_chunk(const EnsParams& P, uint32_t rep, uint
         const uint32_t x = x0 + xo;
         const uint32_t ya = seg * E.seg_len, yb = min(ya + E.seg_len, ny);
         if (ya >= yb) continue;
-        if (PIPE)
-            march_column_pipe<MOVE, DMI, HAS_K>(G, P.rk, P.status, sx, sy, sz, x, ya, yb, j, colour, sweep, rep, beta2,
-                                                de, dmx, dmy, dmz);
-        else
-            march_column<MOVE, DMI, HAS_K>(G, P.rk, P.status, sx, sy, sz, x, ya, yb, j, colour, sweep, rep, beta2, de,
-                                           dmx, dmy, dmz);
+        march_column<MOVE, DMI, HAS_K>(G, P.rk, P.status, sx, sy, sz, x, ya, yb, j, colour, sweep, rep, beta2, de, dmx,
+                                       dmy, dmz);
     }
 }
 
@@ -317,12 +313,8 @@ __device__ __forceinline__ bool run_chunk_staged(const EnsParams& P, uint32_t re
     return ok;
 }
 
-// LD: the loader (0 registers, 1 TMA-staged, 3 registers with the software-pipelined march,
-// which needs more registers: at most 128 threads, three blocks per SM)
-template <int MOVE, int DMI, bool HAS_K, int LD>
-__global__ void __launch_bounds__(LD == 1 ? kStThreads : (LD == 3 ? kEnsPipeThreads : kEnsMaxThreads), LD == 3 ? 3 : 2)
-    k_ensembles(const __grid_constant__ EnsParams P) {
-    constexpr bool STAGED = LD == 1;
+template <int MOVE, int DMI, bool HAS_K, bool STAGED>
+__global__ void __launch_bounds__(STAGED ? kStThreads : kEnsMaxThreads, 2) k_ensembles(const __grid_constant__ EnsParams P) {
     __shared__ uint32_t s_task[5];
     __shared__ int s_go, s_fin;
     __shared__ volatile int s_abort;
@@ -402,7 +394,7 @@ __global__ void __launch_bounds__(LD == 1 ? kStThreads : (LD == 3 ? kEnsPipeThre
             }
         } else {
             switch (e) {
-#define ISG_EC(i) case i: run_chunk<MOVE, DMI, HAS_K, i, LD == 3>(P, rep, ph, ch, de, dmx, dmy, dmz); break;
+#define ISG_EC(i) case i: run_chunk<MOVE, DMI, HAS_K, i>(P, rep, ph, ch, de, dmx, dmy, dmz); break;
                 ISG_EC(0) ISG_EC(1) ISG_EC(2) ISG_EC(3) ISG_EC(4) ISG_EC(5) ISG_EC(6) ISG_EC(7)
                 ISG_EC(8) ISG_EC(9) ISG_EC(10) ISG_EC(11) ISG_EC(12) ISG_EC(13) ISG_EC(14) ISG_EC(15)
 #undef ISG_EC

@@ -285,49 +285,4 @@ __device__ __forceinline__ void march_column(const CbGeom& G, const uint32_t* rk
     }
 }
 
-// The same march, software-pipelined: the 15 loads of row y + 1 are issued before the pair
-// update of row y, so each thread keeps one row of loads in flight while it computes (27 more
-// live registers).  Row y + 1 of the own colour at (x, j) is written only by this thread, and
-// only in the next iteration; the other colour is not written during the pass.  Same
-// arithmetic and stores as march_column, bit for bit.
-template <int MOVE, int DMI, bool HAS_K>
-__device__ __forceinline__ void march_column_pipe(const CbGeom& G, const uint32_t* rk, int* status,
-                                                  float* __restrict__ sx, float* __restrict__ sy,
-                                                  float* __restrict__ sz, uint32_t x, uint32_t ya, uint32_t yb,
-                                                  uint32_t j, int colour, uint32_t sweep, uint32_t rep, float beta2,
-                                                  v2& de, v2& dmx, v2& dmy, v2& dmz) {
-    const uint32_t ny = (uint32_t)G.ny, nx = (uint32_t)G.nx, W = G.W, xs = G.row_stride_x;
-    const uint32_t own = (uint32_t)colour * G.half, oth = (uint32_t)(colour ^ 1) * G.half;
-    const uint32_t pl = x * xs;
-    const uint32_t plp = x + 1 == nx ? 0u : pl + xs;
-    const uint32_t plm = x == 0 ? (nx - 1) * xs : pl - xs;
-    v23 prev = ld3(sx, sy, sz, oth + pl + (ya == 0 ? ny - 1 : ya - 1) * W + j);
-    v23 cur = ld3(sx, sy, sz, oth + pl + ya * W + j);
-    v23 nn, ns, npx, nmx;
-    float nex, ney, nez;
-    auto issue = [&](uint32_t y) {
-        const uint32_t rw = y * W;
-        nn = ld3(sx, sy, sz, oth + pl + (y + 1 == ny ? 0u : rw + W) + j);
-        ns = ld3(sx, sy, sz, own + pl + rw + j);
-        npx = ld3(sx, sy, sz, oth + plp + rw + j);
-        nmx = ld3(sx, sy, sz, oth + plm + rw + j);
-        const uint32_t p = (x + y + (uint32_t)colour) & 1u;
-        const uint32_t je = p ? (j + 2 == W ? 0u : j + 2) : (j == 0 ? W - 1 : j - 1);
-        const uint32_t oe = oth + pl + rw + je;
-        nex = sx[oe]; ney = sy[oe]; nez = sz[oe];
-    };
-    issue(ya);
-#pragma unroll 1
-    for (uint32_t y = ya; y < yb; ++y) {
-        const v23 next = nn, s = ns, px = npx, mx = nmx;
-        const float ex = nex, ey = ney, ez = nez;
-        if (y + 1 < yb) issue(y + 1);
-        const uint32_t p = (x + y + (uint32_t)colour) & 1u;
-        pair_compute<MOVE, DMI, HAS_K>(G, rk, status, sx, sy, sz, own + pl + y * W + j, x * ny + y, j, p, s, px, mx,
-                                       next, prev, cur, ex, ey, ez, sweep, rep, beta2, de, dmx, dmy, dmz);
-        prev = cur;
-        cur = next;
-    }
-}
-
 }  // namespace isg

@@ -17,9 +17,8 @@ L, R, K_SWEEPS, ROUNDS, SEED = 128, 16, 10, 3, 0x15196
 @pytest.mark.parametrize("sched", [dict(block_threads=128, chunk_pairs=8192, loader=0),
                                    dict(block_threads=256, chunk_pairs=16384, loader=1),
                                    dict(block_threads=512, chunk_pairs=1 << 30, loader=2),
-                                   dict(block_threads=256, chunk_pairs=16384, loader=2),
-                                   dict(block_threads=128, chunk_pairs=8192, loader=3)],
-                         ids=["registers", "staged", "fused", "fused-segments", "pipelined"])
+                                   dict(block_threads=256, chunk_pairs=16384, loader=2)],
+                         ids=["registers", "staged", "fused", "fused-segments"])
 def test_engine_equals_pt_path_at_c3_size(ib, cuda_ok, sched):
     pp = ib.params(J=-1.0, Dz=0.7, B=0.3, K=0.05, dmi="bulk", include_Jp=False)
     betas = 1.0 / ib.temperature_ladder(0.1, 1.5, R)

@@ -73,9 +73,6 @@ def _assert_same(members, eng, emeshes, rmeshes, refs):
     {"block_threads": 64, "chunk_pairs": 100000, "order": 1, "group_bytes": 1},      # whole replicas, one per group
     {"block_threads": 128, "chunk_pairs": 16, "order": 2},          # wavefront order, one x-plane per task
     {"block_threads": 256, "chunk_pairs": 64, "order": 2},          # wavefront order, a few planes per task
-    {"block_threads": 128, "chunk_pairs": 16, "order": 0, "loader": 3},   # pipelined march, one plane per task
-    {"block_threads": 64, "chunk_pairs": 100000, "order": 0, "loader": 3},  # pipelined march, whole meshes
-    {"block_threads": 32, "chunk_pairs": 64, "order": 0, "loader": 3},    # pipelined march, one warp per block
 ])
 def test_engine_matches_single_ensemble_pt(ib, cuda_ok, sched):
     eng, em, rm, refs = _engine_and_refs(ib, MEMBERS, k=3, rounds=5, sched=sched)
