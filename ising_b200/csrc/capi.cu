@@ -1274,14 +1274,17 @@ extern "C" int ising_pt_schedule(const ising_pt* pt, int k, int* group, int* lau
     if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
     if (k < 1) return fail(ISING_ERR_ARG, "sweeps_per_swap must be >= 1");
     const SweepPlan& P = pt->plan;
-    int grp = P.sc ? P.group : pt->n;
+    const bool oct = !P.sc && pt->mesh->layout.cb == 2;
+    int grp = (P.sc || oct) ? std::min(P.group, pt->n) : pt->n;
     int G = (pt->n + grp - 1) / grp;
     int L = 0;
     if (P.sc) L = G > 1 ? G * k + 1 : 2 * k;
+    else if (oct) L = G * k * 8 * ((int)pt->mesh->oct_rank0.size() - 1);
     else L = k * P.col->ncol;
     if (group) *group = grp;
     if (launches) *launches = L;
-    if (kernel) *kernel = P.sc ? (P.tma ? 2 : 1) : 0;
+    // 0 k_general_colour / k_octant_colour, 1 k_cb_sweep, 2 k_cb_tma, 3 k_octant_fast
+    if (kernel) *kernel = P.sc ? (P.tma ? 2 : 1) : (oct && P.oct_maxcnt > 0 ? 3 : 0);
     return ISING_OK;
 }
 
