@@ -502,14 +502,15 @@ def run_gpu(args, w):
             raise SystemExit("--engine pt runs single-ensemble workloads only")
         m, betas, p, ens_id = members[0]
         pt = ib.ParallelTempering(m, betas, p, seed=0x15196, ensemble=ens_id, move=move, r=w["r"],
-                                  l2_group=args.l2_group)
+                                  l2_group=args.l2_group, sweep_kernel=args.sweep_kernel)
         pt.run(k, max(args.warmup, 1))
         run = lambda n: pt.run(k, n)
         energies = lambda: [pt.energies()]
         group, per_round, kern_id = pt.schedule(k)
         sched_info = {"l2_group_replicas": group, "colour_pass_launches_per_round": per_round,
                       "kernel": {0: "k_octant_colour" if m.layout == "octant" else "k_general_colour",
-                                 1: "k_cb_sweep", 2: "k_cb_tma", 3: "k_octant_fast"}[kern_id], "layout": m.layout}
+                                 1: "k_cb_sweep", 2: "k_cb_tma", 3: "k_octant_fast",
+                                 4: "k_octant_engine"}[kern_id], "layout": m.layout}
         kernel_name = sched_info["kernel"]
         launches_timed = args.steps * (per_round + 3)   # colour passes + fold + exchange + advance
         closers = [pt]
@@ -1213,6 +1214,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--schedule", default="", help="engine schedule 'threads,chunk_pairs,loader' (no autotuner)")
     ap.add_argument("--l2-group", type=int, default=0, help="--engine pt: replicas per sweep group (0 = auto)")
+    ap.add_argument("--sweep-kernel", type=int, default=0,
+                    help="--engine pt: 0 auto; checkerboard 1 register / 2 TMA; octant 1 one launch per class")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--learned", action="store_true", help="c5: learned patch proposal vs plain Metropolis")
     ap.add_argument("--patch-probe", action="store_true", help="time learned patch steps (C5 Hamiltonian)")

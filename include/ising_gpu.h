@@ -283,7 +283,9 @@ typedef struct {
     int record_capacity;      /* sweeps to keep per replica when record = 1 */
     int l2_group;             /* replicas per group of the L2-paired sweep schedule, or of the
                                  octant schedule (every sweep of a group, then the next; 0 = auto) */
-    int sweep_kernel;         /* checkerboard meshes: 0 auto, 1 register kernel, 2 TMA-staged kernel */
+    int sweep_kernel;         /* checkerboard meshes: 0 auto, 1 register kernel, 2 TMA-staged kernel;
+                                 octant meshes: 0 auto (one persistent launch per round), 1 one
+                                 launch per colour class */
 } ising_pt_options;
 
 /* Replaces the PT state of src/PT.f90:193-204 (TemperatureMeshArray, TemperatureArray):
@@ -302,7 +304,7 @@ int ising_pt_relax(ising_pt* pt, int n_sweeps);
 /* Launch schedule of a round: replicas per L2 group, colour-pass launches per round of
  * sweeps_per_swap sweeps, and which colour-pass kernel runs (1 register, 2 TMA-staged,
  * 0 the stencil kernel of the greedy or octant colouring, 3 the octant kernel with the
- * stencil resolved per class).  No reference counterpart. */
+ * stencil resolved per class, 4 the persistent octant engine).  No reference counterpart. */
 int ising_pt_schedule(const ising_pt* pt, int sweeps_per_swap, int* l2_group, int* pass_launches,
                       int* kernel);
 /* temperature slot -> replica (TemperatureMeshArray(i, :), src/PT.f90:58) */

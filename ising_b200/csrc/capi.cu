@@ -230,6 +230,9 @@ struct SweepPlan {
     int* d_count = nullptr;
     const float* demag = nullptr;   // general path: demagnetising field of the swept replica
     int oct_maxcnt = 0;        // octant layout: k_octant_fast's table width (0: k_octant_colour)
+    bool oct_engine = false;   // octant layout: every sweep of a call in one persistent launch
+    int oct_reach = 1;         // its dependency reach in packed x-planes
+    int oct_grid = 0;          // its persistent blocks
 };
 
 // Fills plan for Hamiltonian p; the general path uploads its stencil into (slots, count).
@@ -263,7 +266,7 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
         ISG_TRY(fill_query_stencil_host(m, p, false, hs.data(), hc.data()));
         const Lattice& Lt = m->lat;
         const int half[3] = {Lt.nx / 2, Lt.ny / 2, Lt.nz / 2};
-        int maxcnt = 0;
+        int maxcnt = 0, reach = 0;
         bool fits = true;
         for (int sub = 0; sub < Lt.nsub; ++sub) {
             maxcnt = std::max(maxcnt, hc[sub]);
@@ -275,10 +278,19 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
                         const int t = o + d[ax];
                         const int ex = (t - (t & 1)) / 2;
                         if (ex < -half[ax] || ex > half[ax]) fits = false;
+                        if (ax == 0) reach = std::max(reach, std::abs(ex));
                     }
             }
         }
         plan->oct_maxcnt = fits ? std::max(maxcnt, 1) : 0;
+        // the persistent engine: one partial slot per (replica, packed x-plane)
+        if (plan->oct_maxcnt > 0) {
+            plan->oct_engine = true;
+            plan->oct_reach = std::max(reach, 1);
+            ISG_TRY(octant_engine_grid(&plan->oct_grid));
+            if (!m->d_oct_sync)
+                ISG_TRY(dev_alloc(&m->d_oct_sync, (size_t)m->n_replicas * (size_t)(Lt.nx / 2) + 2));
+        }
         int min_class = INT32_MAX;
         for (int k = 0; k < 8 * ng; ++k) {
             const int64_t n = m->layout.q8 * (m->oct_rank0[k % ng + 1] - m->oct_rank0[k % ng]);
@@ -291,6 +303,7 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
         const int g_l2 = std::max(1, (int)(kL2GroupBytes / (12.0 * (double)Lt.natoms)));
         const int g_fill = (int)((kOctMinLaunchSites + min_class - 1) / std::max(min_class, 1));
         plan->group = std::max(g_l2, g_fill);
+        if (plan->oct_engine) tot = std::max(tot, Lt.nx / 2);
     } else {
         for (int k = 0; k < plan->col->ncol; ++k)
             tot += general_slots_for(plan->col->class_start[k + 1] - plan->col->class_start[k]);
@@ -362,6 +375,24 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
     g.ham = plan.ham; g.st = StencilDev{plan.d_slots, plan.d_count, L.nsub}; g.layout = m->layout;
     g.partials = partials; g.slots_per_rep = plan.slots_per_rep; g.status = m->d_status;
     g.demag = plan.demag; g.mu0 = (float)kMu0;
+    if (m->layout.cb == 2 && plan.oct_engine) {   // every sweep of the call in one launch
+        OctEngineLaunch e{};
+        const int hx = L.nx / 2;
+        e.head = m->d_oct_sync;
+        e.abort = m->d_oct_sync + 1;
+        e.done = m->d_oct_sync + 2;
+        e.n_sweeps = n_sweeps;
+        e.ng = (int)m->oct_rank0.size() - 1;
+        e.reach = plan.oct_reach;
+        for (int k = 0; k <= kMaxSub; ++k) e.rank0[k] = k <= e.ng ? m->oct_rank0[k] : m->oct_rank0[e.ng];
+        e.wait_ns = 2000000000ull;
+        e.grid = plan.oct_grid;
+        g.oct_maxcnt = plan.oct_maxcnt;
+        g.sweep_offset = sw0;
+        g.slot_base = 0;
+        ISG_CUDA(cudaMemsetAsync(m->d_oct_sync, 0, ((size_t)n_rep * hx + 2) * sizeof(uint32_t), m->stream));
+        return launch_octant_engine(g, e, m->stream);
+    }
     if (m->layout.cb == 2) {   // octant classes: contiguous storage ranges
         // replicas are independent: each L2-sized group of replicas runs all its sweeps
         // (every class, in order) before the next group starts, so a group's spins stay in L2
@@ -554,7 +585,7 @@ extern "C" int ising_mesh_destroy(ising_mesh* m) {
     xfer_release(m);
     cudaFree(m->d_spins); cudaFree(m->d_sweep); cudaFree(m->d_scratch); cudaFree(m->d_status);
     cudaFree(m->d_staging); cudaFree(m->d_beta); cudaFree(m->d_winding_tmp); cudaFree(m->d_slots); cudaFree(m->d_slot_count);
-    cudaFree(m->d_plaq);
+    cudaFree(m->d_plaq); cudaFree(m->d_oct_sync);
     isg::skyrmion_release(m);
     isg::demag_release(m);
     for (auto& c : m->colour) cudaFree(c.d_sites);
@@ -1188,6 +1219,7 @@ extern "C" int ising_pt_create(ising_mesh* m, int n, const double* betas, const 
     if (opt->l2_group < 0) return bail(fail(ISING_ERR_ARG, "l2_group must be >= 0"));
     if (opt->l2_group > 0) pt->plan.group = opt->l2_group;
     if (opt->sweep_kernel < 0 || opt->sweep_kernel > 2) return bail(fail(ISING_ERR_ARG, "sweep_kernel must be 0, 1 or 2"));
+    if (opt->sweep_kernel == 1 && m->layout.cb == 2) pt->plan.oct_engine = false;   // one launch per class
     if (opt->sweep_kernel == 2) {
         const Lattice& Lt = m->lat;
         if (!pt->plan.sc || !cb_tma_supported(Lt.nx, Lt.ny, Lt.nz))
@@ -1279,12 +1311,14 @@ extern "C" int ising_pt_schedule(const ising_pt* pt, int k, int* group, int* lau
     int G = (pt->n + grp - 1) / grp;
     int L = 0;
     if (P.sc) L = G > 1 ? G * k + 1 : 2 * k;
+    else if (oct && P.oct_engine) { L = 1; grp = pt->n; }
     else if (oct) L = G * k * 8 * ((int)pt->mesh->oct_rank0.size() - 1);
     else L = k * P.col->ncol;
     if (group) *group = grp;
     if (launches) *launches = L;
-    // 0 k_general_colour / k_octant_colour, 1 k_cb_sweep, 2 k_cb_tma, 3 k_octant_fast
-    if (kernel) *kernel = P.sc ? (P.tma ? 2 : 1) : (oct && P.oct_maxcnt > 0 ? 3 : 0);
+    // 0 k_general_colour / k_octant_colour, 1 k_cb_sweep, 2 k_cb_tma, 3 k_octant_fast,
+    // 4 k_octant_engine
+    if (kernel) *kernel = P.sc ? (P.tma ? 2 : 1) : (oct ? (P.oct_engine ? 4 : (P.oct_maxcnt > 0 ? 3 : 0)) : 0);
     return ISING_OK;
 }
 

@@ -115,6 +115,7 @@ struct ising_mesh {
     void* sky = nullptr;                 // skyrmion-counting workspace, made on first use
     void* xfer = nullptr;                // asynchronous spin transfers (streams, per-replica staging)
     void* demag = nullptr;               // demagnetising-field workspace, made on first use
+    uint32_t* d_oct_sync = nullptr;      // octant engine: [n_replicas][nx/2] counters + head + abort
 };
 
 namespace isg {
@@ -202,6 +203,21 @@ int launch_general_colour(const GeneralLaunch& a, cudaStream_t s);
 // [rank0, rank0 + nrank) of that octant (a.sites and a.n_sites unused).
 int launch_octant_colour(const GeneralLaunch& a, int octant, int rank0, int nrank, cudaStream_t s);
 int octant_slots_for(int64_t n_sites, bool fast);   // partial-sum slots (blocks) of one class launch
+// The octant sweeps of a PT round as ONE persistent launch: tasks (sweep, class, replica,
+// packed x-plane) in phase-major queue order, each waiting (bounded) until the planes within
+// `reach` of its own have finished the previous phase.  Partial sums: one slot per (replica,
+// plane), so slots_per_rep >= hx.
+struct OctEngineLaunch {
+    uint32_t* done;          // [n_rep][hx] phases completed in this launch (zeroed before it)
+    uint32_t* head;          // task queue head (zeroed before it)
+    uint32_t* abort;         // raised by a wait that gives up (zeroed before it)
+    int n_sweeps, ng, reach; // sweeps, sublattice groups (classes = 8 ng), dependency reach in planes
+    int rank0[kMaxSub + 1];  // first storage rank of each group, and the end
+    uint64_t wait_ns;        // bound of every wait
+    int grid;                // persistent blocks
+};
+int launch_octant_engine(const GeneralLaunch& a, const OctEngineLaunch& e, cudaStream_t s);
+int octant_engine_grid(int* blocks);
 int general_slots_for(int n_sites);
 
 struct ReduceLaunch {

@@ -208,7 +208,7 @@ struct __align__(16) OctSlot {
     float pad2[2];           // 32 bytes: two 16-byte shared-memory loads
 };
 struct OctDims {
-    FastDiv q8, hz, hy;
+    FastDiv q8, hz, hy, hyz;
     int hx, hyi, hzi;
 };
 
@@ -301,6 +301,217 @@ done:
             p[0] += tot[0]; p[1] += tot[1]; p[2] += tot[2]; p[3] += tot[3];
         }
     }
+}
+
+// ---- persistent octant engine ----------------------------------------------------------
+// All sweeps of a PT round over the octant classes in ONE launch.  A task is (phase, replica,
+// packed x-plane u), phase = sweep * classes + class; tasks are taken from an atomic queue in
+// phase-major order, so every task a block waits for sits earlier in the queue and is held by a
+// running block (no co-residency is assumed).  A task of phase p on plane u waits until the
+// planes u - reach .. u + reach of its replica have finished phase p - 1: its neighbours lie
+// in those planes, and the previous phase's readers of plane u lie there too.  It then
+// updates every site of the class in plane u (all Y, Z, every rank of the class) exactly as
+// k_octant_fast does, adds its block sums to the (replica, plane) partial slot and releases
+// the plane's counter.  Ordering: thread 0 acquires the counters (ld.acquire.gpu), every
+// thread acquires them again before its loads (so its SM's L1 holds no stale line), and the
+// release follows __syncthreads + __threadfence.  Every wait is bounded (%globaltimer and a
+// poll count); one that gives up sets kStatTimeout and raises the abort word, which stops
+// every block at its next task.
+__device__ __forceinline__ uint32_t oe_ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void oe_st_release(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t oe_now() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// thread 0: wait until *p >= target; false when aborted or past the bound (then aborts)
+__device__ __forceinline__ bool oe_wait_ge(const OctEngineLaunch& e, int* status, const uint32_t* p, uint32_t target) {
+    if (oe_ld_acquire(p) >= target) return true;
+    const uint64_t t0 = oe_now();
+    const uint64_t max_polls = e.wait_ns / 32u + 1024u;
+    uint32_t ns = 32;
+    for (uint64_t it = 0; it < max_polls; ++it) {
+        __nanosleep(ns);
+        if (ns < 512) ns <<= 1;
+        if (oe_ld_acquire(p) >= target) return true;
+        if (*(volatile const uint32_t*)e.abort) return false;
+        if (oe_now() - t0 > e.wait_ns) break;
+    }
+    atomicOr(status, kStatTimeout);
+    atomicExch(e.abort, 1u);
+    __threadfence();
+    return false;
+}
+
+template <int MOVE>
+__global__ void __launch_bounds__(kGenThreads, 4) k_octant_engine(GeneralLaunch a, OctDims od, OctEngineLaunch e) {
+    extern __shared__ __align__(16) unsigned char oe_smem[];
+    const int mc = a.oct_maxcnt;
+    OctSlot* tab = reinterpret_cast<OctSlot*>(oe_smem);   // [ranks of the class][mc]
+    __shared__ int s_srank[kMaxSub], s_sofr[kMaxSub], s_rank0[kMaxSub + 1], s_sub[kMaxSub], s_cnt[kMaxSub];
+    __shared__ uint32_t s_task[3];
+    __shared__ int s_go;
+    __shared__ double tot[4];
+    const Layout& L = a.layout;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < kMaxSub; ++k) { s_srank[k] = L.srank[k]; s_sofr[k] = L.sofr[k]; s_rank0[k] = e.rank0[k]; }
+        s_rank0[kMaxSub] = e.rank0[kMaxSub];
+    }
+    __syncthreads();
+    const int hx = od.hx, hy = od.hyi, hz = od.hzi;
+    const uint32_t hyz = (uint32_t)hy * (uint32_t)hz;
+    const int q8 = (int)L.q8;
+    const int ncls = 8 * e.ng;
+    const uint32_t per_phase = (uint32_t)a.n_rep * (uint32_t)hx;
+    const uint32_t total = per_phase * (uint32_t)ncls * (uint32_t)e.n_sweeps;
+    const int64_t N = a.natoms;
+    int cached = -1;
+    uint32_t next = 0;
+    if (threadIdx.x == 0) next = atomicAdd(e.head, 1u);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            int go = 0;
+            const uint32_t id = next;
+            if (id < total && !*(volatile const uint32_t*)e.abort) {
+                const uint32_t ph = id / per_phase, rem = id - ph * per_phase;
+                const uint32_t r = rem / (uint32_t)hx, u = rem - r * (uint32_t)hx;
+                go = 1;
+                if (ph > 0) {
+                    const uint32_t* d = e.done + r * (uint32_t)hx;
+                    for (int k = -e.reach; k <= e.reach && go; ++k) {
+                        int uu = ((int)u + k) % hx;
+                        uu += uu < 0 ? hx : 0;
+                        go = oe_wait_ge(e, a.status, d + uu, ph);
+                    }
+                }
+                s_task[0] = ph; s_task[1] = r; s_task[2] = u;
+            }
+            s_go = go;
+        }
+        __syncthreads();
+        if (!s_go) break;
+        if (threadIdx.x == 0) next = atomicAdd(e.head, 1u);   // prefetch; used next iteration
+        const uint32_t ph = s_task[0], r = s_task[1], u = s_task[2];
+        if (threadIdx.x != 0 && ph > 0) {
+            const uint32_t* d = e.done + r * (uint32_t)hx;
+            for (int k = -e.reach; k <= e.reach; ++k) {
+                int uu = ((int)u + k) % hx;
+                uu += uu < 0 ? hx : 0;
+                oe_ld_acquire(d + uu);
+            }
+        }
+        const int sw = (int)(ph / (uint32_t)ncls), c = (int)ph - sw * ncls;
+        const int oct = c / e.ng, gi = c - oct * e.ng;
+        const int rank0 = s_rank0[gi], nrank = s_rank0[gi + 1] - rank0;
+        const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
+        if (c != cached) {   // the class's stencil, resolved as in k_octant_fast
+            for (int en = threadIdx.x; en < nrank * mc; en += blockDim.x) {
+                const int lr = en / mc, q = en - lr * mc;
+                const int sub = s_sofr[rank0 + lr];
+                OctSlot o{};
+                if (q < a.st.count[sub]) {
+                    const Slot sl = a.st.slots[sub * kMaxSlots + q];
+                    const int tx = ox + sl.dx, ty = oy + sl.dy, tz = oz + sl.dz;
+                    const int o2 = ((tx & 1) << 2) | ((ty & 1) << 1) | (tz & 1);
+                    o.plane = (o2 * a.nsub + s_srank[sl.sub]) * q8;
+                    o.ex = (int8_t)(tx >> 1); o.ey = (int8_t)(ty >> 1); o.ez = (int8_t)(tz >> 1);
+                    o.w = sl.w; o.Dx = sl.Dx; o.Dy = sl.Dy; o.Dz = sl.Dz;
+                }
+                tab[en] = o;
+            }
+            for (int lr = threadIdx.x; lr < nrank; lr += blockDim.x) {
+                s_sub[lr] = s_sofr[rank0 + lr];
+                s_cnt[lr] = a.st.count[s_sub[lr]];
+            }
+            cached = c;
+            __syncthreads();
+        }
+        const int rep = a.rep_first + (int)r;
+        float* __restrict__ sx = a.spins + (int64_t)r * 3 * N;
+        float* __restrict__ sy = sx + N;
+        float* __restrict__ sz = sy + N;
+        const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset + (uint32_t)sw;
+        const float beta = (float)a.beta_rep[rep];
+        const uint32_t nsite = (uint32_t)nrank * hyz;
+        const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
+        const int X = (int)u;
+        float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
+        for (uint32_t t = threadIdx.x; t < nsite; t += blockDim.x) {
+            const uint32_t lr = fdiv(t, od.hyz);
+            const uint32_t rem = t - lr * hyz;
+            const uint32_t Yu = fdiv(rem, od.hz);
+            const int Z = (int)(rem - Yu * (uint32_t)hz), Y = (int)Yu;
+            const int sub = s_sub[lr];
+            const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z + oz;
+            const uint32_t at = ((uint32_t)(ix * a.ny + iy) * (uint32_t)a.nz + (uint32_t)iz) * (uint32_t)a.nsub + sub;
+            const OctSlot* ts = tab + lr * mc;
+            f3 h = {0.f, 0.f, 0.f};
+            const int cn = s_cnt[lr];
+            for (int q = 0; q < cn; ++q) {
+                const OctSlot o = ts[q];
+                int jx = X + o.ex, jy = Y + o.ey, jz = Z + o.ez;
+                jx += jx < 0 ? hx : 0; jx -= jx >= hx ? hx : 0;
+                jy += jy < 0 ? hy : 0; jy -= jy >= hy ? hy : 0;
+                jz += jz < 0 ? hz : 0; jz -= jz >= hz ? hz : 0;
+                const uint32_t j = (uint32_t)o.plane + (uint32_t)((jx * hy + jy) * hz + jz);
+                const f3 sj = {sx[j], sy[j], sz[j]};
+                const f3 cr = cross(sj, mk(o.Dx, o.Dy, o.Dz));
+                h.x += fmaf(o.w, sj.x, cr.x);
+                h.y += fmaf(o.w, sj.y, cr.y);
+                h.z += fmaf(o.w, sj.z, cr.z);
+            }
+            const uint32_t si = class_base + lr * (uint32_t)q8 + (uint32_t)X * hyz + rem;
+            site_update<MOVE>(a, h, (int64_t)si, (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+        }
+        if (a.partials) {
+            block_sum4<double>(de, dmx, dmy, dmz, tot);
+            if (threadIdx.x == 0) {
+                double* pp = a.partials + ((int64_t)rep * a.slots_per_rep + u) * 4;
+                __stcg(pp, __ldcg(pp) + tot[0]); __stcg(pp + 1, __ldcg(pp + 1) + tot[1]);
+                __stcg(pp + 2, __ldcg(pp + 2) + tot[2]); __stcg(pp + 3, __ldcg(pp + 3) + tot[3]);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            oe_st_release(e.done + r * (uint32_t)hx + u, ph + 1u);
+        }
+    }
+}
+
+int octant_engine_grid(int* blocks) {
+    int dev = 0, sms = 0, per = 0;
+    ISG_CUDA(cudaGetDevice(&dev));
+    ISG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    ISG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_octant_engine<1>, kGenThreads,
+                                                           (size_t)kMaxSub * 16 * sizeof(OctSlot)));
+    *blocks = sms * std::max(per, 1);
+    return ISING_OK;
+}
+
+int launch_octant_engine(const GeneralLaunch& a, const OctEngineLaunch& e, cudaStream_t s) {
+    if (a.oct_maxcnt < 1 || e.ng < 1 || e.n_sweeps < 1 || e.grid < 1) return fail(ISING_ERR_ARG, "octant engine setup");
+    int maxr = 0;
+    for (int g = 0; g < e.ng; ++g) maxr = std::max(maxr, e.rank0[g + 1] - e.rank0[g]);
+    OctDims od;
+    od.q8 = make_div((uint32_t)a.layout.q8);
+    od.hx = a.nx / 2; od.hyi = a.ny / 2; od.hzi = a.nz / 2;
+    od.hz = make_div((uint32_t)od.hzi);
+    od.hy = make_div((uint32_t)od.hyi);
+    od.hyz = make_div((uint32_t)(od.hyi * od.hzi));
+    const size_t sm = (size_t)maxr * a.oct_maxcnt * sizeof(OctSlot);
+    if (sm > 48u * 1024u) return fail(ISING_ERR_ARG, "octant engine: class stencil table exceeds 48 KB");
+    if (a.move == 0) k_octant_engine<0><<<e.grid, kGenThreads, sm, s>>>(a, od, e);
+    else k_octant_engine<1><<<e.grid, kGenThreads, sm, s>>>(a, od, e);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
 }
 
 int octant_slots_for(int64_t n_sites, bool fast) {

@@ -81,3 +81,37 @@ def test_octant_pt_accumulators_track_recomputed_energies(oracle, ib, cuda_ok):
     for r in range(4):
         om.set_spins(pm.get_spins(r))
         assert abs(e_new[r] - om.canonical_energy(op)) < 1e-6 * pm.numAtoms
+
+
+@pytest.mark.parametrize("kind,dims,shell2", [("BCC", (8, 6, 4), False), ("BCC", (6, 4, 8), True),
+                                              ("HK", (4, 6, 4), False), ("HK", (8, 4, 6), True)])
+@pytest.mark.parametrize("move", [0, 1])
+def test_octant_engine_equals_one_launch_per_class(oracle, ib, cuda_ok, kind, dims, shell2, move):
+    """The persistent octant engine (every sweep of a round in one launch, tasks per packed
+    x-plane with bounded dependency waits) against one launch per colour class: spins,
+    exchange permutation and swap counts bit-equal after several rounds of PT, accumulators
+    within FP32 rounding of each other (the partial sums are grouped differently)."""
+    runs = []
+    for sweep_kernel in (0, 1):
+        om, pm = _pair(oracle, ib, kind, dims, n_replicas=6)
+        assert pm.layout == "octant"
+        pm.init_uniform(77, 0)
+        kw = dict(J=-1.0, Dz=0.4, B=0.15, bulk=False)
+        if shell2:
+            kw["Jp"] = 0.2
+        op, pp = _both_params(oracle, ib, **kw)
+        pt = ib.ParallelTempering(pm, 1.0 / ib.temperature_ladder(0.3, 2.5, 6), pp, seed=11, move=move,
+                                  r=0.3, sweep_kernel=sweep_kernel)
+        assert pt.schedule(4)[2] == (4 if sweep_kernel == 0 else 3)
+        pt.run(4, 5)
+        e, m = pt.energies()
+        runs.append(([pm.get_spins(r) for r in range(6)], pt.permutation(), pt.swap_stats(), e, m, pm.numAtoms))
+        pt.close()
+    (s0, p0, st0, e0, m0, n), (s1, p1, st1, e1, m1, _) = runs
+    for r in range(6):
+        np.testing.assert_array_equal(s0[r], s1[r])
+    np.testing.assert_array_equal(p0, p1)
+    np.testing.assert_array_equal(st0[0], st1[0])
+    np.testing.assert_array_equal(st0[1], st1[1])
+    np.testing.assert_allclose(e0, e1, rtol=0, atol=1e-6 * n)
+    np.testing.assert_allclose(m0, m1, rtol=0, atol=1e-6 * n)
