@@ -2154,6 +2154,12 @@ extern "C" int ising_ensembles_autotune(ising_ensembles* s, int k, int rounds_pe
     for (int c : {512, 1024}) cand.push_back({128, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_REGISTERS});
     if (max_lanes <= 64)      // two-warp blocks (8 per SM, the same 16 warps) with small tasks
         for (int c : {2048, 4096}) cand.push_back({64, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_REGISTERS});
+    // rows of W/2 = 24 lanes (nz = 96, as in C5) leave 8 of 128 threads idle; 96-thread blocks
+    // hold exactly four rows
+    bool rows24 = true;
+    for (auto& h : s->ens) rows24 = rows24 && h.mesh->lat.nz / 4 == 24;
+    if (rows24)
+        for (int c : {512, 1024, 2048, 4096}) cand.push_back({96, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_REGISTERS});
     if (ens_staged_fits(s))   // groups of 4, 8 and 16 x-planes per task at nz = 128
         for (int c : {16384, 32768, 65536}) cand.push_back({256, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_STAGED});
     if (k % 2 == 0)           // one pass per sweep: chunk widths by block size, y-segments by chunk_pairs
