@@ -301,6 +301,12 @@ int ising_pt_run(ising_pt* pt, int sweeps_per_swap, int rounds);
 /* n_sweeps sweeps of every replica at its current temperature without exchange: the
  * "relax each domain" loop of src/PT.f90:276-287. */
 int ising_pt_relax(ising_pt* pt, int n_sweeps);
+/* Test hook of the persistent octant engine (octant meshes, sweep_kernel 0): during the next
+ * ising_pt_run call every dependency wait of the first class change gives up after wait_ms
+ * milliseconds (a count nothing reaches); the call returns ISING_ERR_TIMEOUT, the context
+ * stays usable, and ising_pt_resync restores the running energies.  No reference
+ * counterpart. */
+int ising_pt_inject_stall(ising_pt* pt, int wait_ms);
 /* Launch schedule of a round: replicas per L2 group, colour-pass launches per round of
  * sweeps_per_swap sweeps, and which colour-pass kernel runs (1 register, 2 TMA-staged,
  * 0 the stencil kernel of the greedy or octant colouring, 3 the octant kernel with the

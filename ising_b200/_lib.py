@@ -120,6 +120,7 @@ _SIGS = {
     "ising_pt_permutation": (_i, [_vp, _P(_i)]),
     "ising_pt_energies": (_i, [_vp, _P(_d), _P(_d)]),
     "ising_pt_resync": (_i, [_vp]),
+    "ising_pt_inject_stall": (_i, [_vp, _i]),
     "ising_pt_swap_stats": (_i, [_vp, _P(_u64), _P(_u64)]),
     "ising_pt_series": (_i, [_vp, _P(_d), _P(_i)]),
     "ising_ensembles_create": (_i, [_i, _P(EnsembleDesc), _P(EnsemblesOptions), _P(_vp)]),

@@ -522,6 +522,10 @@ class ParallelTempering:
     def resync(self):
         _lib.call("ising_pt_resync", self._h)
 
+    def inject_stall(self, wait_ms: int = 200):
+        """Test hook (octant meshes): the next run's dependency waits give up after wait_ms."""
+        _lib.call("ising_pt_inject_stall", self._h, wait_ms)
+
     def swap_stats(self):
         att = np.zeros(max(self.n - 1, 1), dtype=np.uint64)
         acc = np.zeros(max(self.n - 1, 1), dtype=np.uint64)

@@ -233,6 +233,8 @@ struct SweepPlan {
     bool oct_engine = false;   // octant layout: every sweep of a call in one persistent launch
     int oct_reach = 1;         // its dependency reach in packed x-planes
     int oct_grid = 0;          // its persistent blocks
+    int oct_stall = 0;         // test hook (ising_pt_inject_stall): the next round's waits run out
+    uint64_t oct_wait_ns = 2000000000ull;   // bound of every wait of the engine
 };
 
 // Fills plan for Hamiltonian p; the general path uploads its stencil into (slots, count).
@@ -385,7 +387,8 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
         e.ng = (int)m->oct_rank0.size() - 1;
         e.reach = plan.oct_reach;
         for (int k = 0; k <= kMaxSub; ++k) e.rank0[k] = k <= e.ng ? m->oct_rank0[k] : m->oct_rank0[e.ng];
-        e.wait_ns = 2000000000ull;
+        e.wait_ns = plan.oct_wait_ns;
+        e.stall = plan.oct_stall;
         e.grid = plan.oct_grid;
         g.oct_maxcnt = plan.oct_maxcnt;
         g.sweep_offset = sw0;
@@ -1286,7 +1289,27 @@ extern "C" int ising_pt_run(ising_pt* pt, int k, int rounds) {
         ++pt->rounds_done;
         if (pt->opt.resync_every > 0 && pt->rounds_done % pt->opt.resync_every == 0) ISG_TRY(pt_resync_enqueue(pt));
     }
+    if (pt->plan.oct_stall) {   // an injected stall lasts one call: capture the plain round again
+        ISG_CUDA(cudaStreamSynchronize(m->stream));
+        pt->plan.oct_stall = 0;
+        pt->plan.oct_wait_ns = 2000000000ull;
+        if (pt->graph) { cudaGraphExecDestroy(pt->graph); pt->graph = nullptr; }
+        pt->graph_k = -1;
+    }
     return check_status(m);
+}
+
+extern "C" int ising_pt_inject_stall(ising_pt* pt, int wait_ms) {
+    if (!pt) return fail(ISING_ERR_ARG, "pt is NULL");
+    if (!pt->plan.oct_engine) return fail(ISING_ERR_ARG, "stall injection needs the persistent octant engine");
+    if (wait_ms < 1 || wait_ms > 60000) return fail(ISING_ERR_ARG, "wait_ms must be 1..60000");
+    DeviceGuard g(pt->mesh->device);
+    ISG_CUDA(cudaStreamSynchronize(pt->mesh->stream));
+    pt->plan.oct_stall = 1;
+    pt->plan.oct_wait_ns = (uint64_t)wait_ms * 1000000ull;
+    if (pt->graph) { cudaGraphExecDestroy(pt->graph); pt->graph = nullptr; }
+    pt->graph_k = -1;
+    return ISING_OK;
 }
 
 extern "C" int ising_pt_relax(ising_pt* pt, int n_sweeps) {

@@ -215,6 +215,7 @@ struct OctEngineLaunch {
     int rank0[kMaxSub + 1];  // first storage rank of each group, and the end
     uint64_t wait_ns;        // bound of every wait
     int grid;                // persistent blocks
+    int stall;               // test hook: the tasks of phase 1 wait for a count nothing reaches
 };
 int launch_octant_engine(const GeneralLaunch& a, const OctEngineLaunch& e, cudaStream_t s);
 int octant_engine_grid(int* blocks);

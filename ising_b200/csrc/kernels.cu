@@ -385,10 +385,11 @@ __global__ void __launch_bounds__(kGenThreads, 4) k_octant_engine(GeneralLaunch 
                 go = 1;
                 if (ph > 0) {
                     const uint32_t* d = e.done + r * (uint32_t)hx;
+                    const uint32_t target = (e.stall && ph == 1u) ? 0x40000000u : ph;
                     for (int k = -e.reach; k <= e.reach && go; ++k) {
                         int uu = ((int)u + k) % hx;
                         uu += uu < 0 ? hx : 0;
-                        go = oe_wait_ge(e, a.status, d + uu, ph);
+                        go = oe_wait_ge(e, a.status, d + uu, target);
                     }
                 }
                 s_task[0] = ph; s_task[1] = r; s_task[2] = u;

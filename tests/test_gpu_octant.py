@@ -115,3 +115,28 @@ def test_octant_engine_equals_one_launch_per_class(oracle, ib, cuda_ok, kind, di
     np.testing.assert_array_equal(st0[1], st1[1])
     np.testing.assert_allclose(e0, e1, rtol=0, atol=1e-6 * n)
     np.testing.assert_allclose(m0, m1, rtol=0, atol=1e-6 * n)
+
+
+def test_octant_engine_timeout_and_recovery(oracle, ib, cuda_ok):
+    """A dependency wait that runs out (the injected stall makes the first class change wait
+    for a count nothing reaches) ends the round with ISING_ERR_TIMEOUT after its bound; the
+    context stays usable, a resync restores the running energies, and later rounds run
+    normally (unit spins, accumulators equal to recomputed energies)."""
+    om, pm = _pair(oracle, ib, "BCC", (8, 6, 4), n_replicas=4)
+    pm.init_uniform(9, 0)
+    op, pp = _both_params(oracle, ib, J=-1.0, Dz=0.4, B=0.1, bulk=False)
+    pt = ib.ParallelTempering(pm, 1.0 / ib.temperature_ladder(0.3, 2.0, 4), pp, seed=5, move=1, r=0.3)
+    pt.run(2, 1)
+    pt.inject_stall(150)
+    with pytest.raises(ib.IsingError) as e:
+        pt.run(2, 1)
+    assert e.value.status == 4
+    pt.resync()
+    pt.run(2, 3)
+    e_run, _ = pt.energies()
+    e_dev, _ = ib.observables(pm, pp)
+    assert np.max(np.abs(e_run - e_dev)) < 1e-5 * pm.numAtoms
+    for r in range(4):
+        s = pm.get_spins(r)
+        assert np.max(np.abs(np.linalg.norm(s, axis=1) - 1.0)) < 1e-5
+    pt.close()
