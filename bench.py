@@ -1215,7 +1215,7 @@ def main():
     ap.add_argument("--schedule", default="", help="engine schedule 'threads,chunk_pairs,loader' (no autotuner)")
     ap.add_argument("--l2-group", type=int, default=0, help="--engine pt: replicas per sweep group (0 = auto)")
     ap.add_argument("--sweep-kernel", type=int, default=0,
-                    help="--engine pt: 0 auto; checkerboard 1 register / 2 TMA; octant 1 one launch per class")
+                    help="--engine pt: 0 auto; checkerboard 1 register / 2 TMA; octant 3 persistent engine")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--learned", action="store_true", help="c5: learned patch proposal vs plain Metropolis")
     ap.add_argument("--patch-probe", action="store_true", help="time learned patch steps (C5 Hamiltonian)")

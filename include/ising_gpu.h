@@ -284,8 +284,8 @@ typedef struct {
     int l2_group;             /* replicas per group of the L2-paired sweep schedule, or of the
                                  octant schedule (every sweep of a group, then the next; 0 = auto) */
     int sweep_kernel;         /* checkerboard meshes: 0 auto, 1 register kernel, 2 TMA-staged kernel;
-                                 octant meshes: 0 auto (one persistent launch per round), 1 one
-                                 launch per colour class */
+                                 octant meshes: 0 or 1 one launch per colour class, 3 one
+                                 persistent launch per round (bit-identical) */
 } ising_pt_options;
 
 /* Replaces the PT state of src/PT.f90:193-204 (TemperatureMeshArray, TemperatureArray):
@@ -301,7 +301,7 @@ int ising_pt_run(ising_pt* pt, int sweeps_per_swap, int rounds);
 /* n_sweeps sweeps of every replica at its current temperature without exchange: the
  * "relax each domain" loop of src/PT.f90:276-287. */
 int ising_pt_relax(ising_pt* pt, int n_sweeps);
-/* Test hook of the persistent octant engine (octant meshes, sweep_kernel 0): during the next
+/* Test hook of the persistent octant engine (octant meshes, sweep_kernel 3): during the next
  * ising_pt_run call every dependency wait of the first class change gives up after wait_ms
  * milliseconds (a count nothing reaches); the call returns ISING_ERR_TIMEOUT, the context
  * stays usable, and ising_pt_resync restores the running energies.  No reference

@@ -285,9 +285,9 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
             }
         }
         plan->oct_maxcnt = fits ? std::max(maxcnt, 1) : 0;
-        // the persistent engine: one partial slot per (replica, packed x-plane)
+        // the persistent engine (opt-in, sweep_kernel 3): one partial slot per (replica,
+        // packed x-plane); plan->oct_engine is set by the PT object that asks for it
         if (plan->oct_maxcnt > 0) {
-            plan->oct_engine = true;
             plan->oct_reach = std::max(reach, 1);
             ISG_TRY(octant_engine_grid(&plan->oct_grid));
             if (!m->d_oct_sync)
@@ -305,7 +305,7 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
         const int g_l2 = std::max(1, (int)(kL2GroupBytes / (12.0 * (double)Lt.natoms)));
         const int g_fill = (int)((kOctMinLaunchSites + min_class - 1) / std::max(min_class, 1));
         plan->group = std::max(g_l2, g_fill);
-        if (plan->oct_engine) tot = std::max(tot, Lt.nx / 2);
+        if (plan->oct_maxcnt > 0) tot = std::max(tot, Lt.nx / 2);
     } else {
         for (int k = 0; k < plan->col->ncol; ++k)
             tot += general_slots_for(plan->col->class_start[k + 1] - plan->col->class_start[k]);
@@ -1221,8 +1221,12 @@ extern "C" int ising_pt_create(ising_mesh* m, int n, const double* betas, const 
     if ((st = make_plan(m, *p, &pt->plan, pt->d_plan_slots, pt->d_plan_count)) != ISING_OK) return bail(st);
     if (opt->l2_group < 0) return bail(fail(ISING_ERR_ARG, "l2_group must be >= 0"));
     if (opt->l2_group > 0) pt->plan.group = opt->l2_group;
-    if (opt->sweep_kernel < 0 || opt->sweep_kernel > 2) return bail(fail(ISING_ERR_ARG, "sweep_kernel must be 0, 1 or 2"));
-    if (opt->sweep_kernel == 1 && m->layout.cb == 2) pt->plan.oct_engine = false;   // one launch per class
+    if (opt->sweep_kernel < 0 || opt->sweep_kernel > 3) return bail(fail(ISING_ERR_ARG, "sweep_kernel must be 0..3"));
+    if (opt->sweep_kernel == 3) {   // octant meshes: every sweep of a round in one persistent launch
+        if (m->layout.cb != 2 || pt->plan.oct_maxcnt < 1)
+            return bail(fail(ISING_ERR_ARG, "the persistent octant engine needs an octant-layout mesh"));
+        pt->plan.oct_engine = true;
+    }
     if (opt->sweep_kernel == 2) {
         const Lattice& Lt = m->lat;
         if (!pt->plan.sc || !cb_tma_supported(Lt.nx, Lt.ny, Lt.nz))
