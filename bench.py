@@ -1023,9 +1023,10 @@ def learned_vs_plain(args, w):
     for arm in range(2):
         m = ib.ChainMesh.simple_cubic(L, n_replicas=R)
         m.set_stream(stream.cuda_stream)
-        m.init_uniform(0x15196, ensemble=arm)
+        m.init_uniform(0x15196 + 1000 * args.c5_seed, ensemble=arm)
         meshes.append(m)
-        pts.append(ib.ParallelTempering(m, betas, p, seed=0x15196 + arm, ensemble=arm, move=_lib.MOVE_BALL,
+        pts.append(ib.ParallelTempering(m, betas, p, seed=0x15196 + arm + 1000 * args.c5_seed, ensemble=arm,
+                                        move=_lib.MOVE_BALL,
                                         r=w["r"], record=True, record_capacity=max(n_plain, n_learned) + 8))
     plain, learned = pts
 
@@ -1040,8 +1041,8 @@ def learned_vs_plain(args, w):
         return max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3) / 1e3
 
     t_therm = timed(lambda: plain.relax(args.c5_therm))
-    rng = np.random.default_rng(7)
-    net = ib.ProposalNet(max_batch=args.c5_batch, seed=1)
+    rng = np.random.default_rng(7 + args.c5_seed)
+    net = ib.ProposalNet(max_batch=args.c5_batch, seed=1 + args.c5_seed)
 
     def jump_stats(steps=8):
         """per slot: acceptance and squared spin displacement per site per proposal (ESJD)"""
@@ -1234,6 +1235,7 @@ def main():
     ap.add_argument("--c5-epochs", type=int, default=3)
     ap.add_argument("--c5-batch", type=int, default=8192)
     ap.add_argument("--c5-slots", type=int, default=0)
+    ap.add_argument("--c5-seed", type=int, default=0, help="c5 comparison: offset of every seed (independent repeats)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="c5: skip the learned-vs-plain q_ess block")
     ap.add_argument("--resync-every", type=int, default=10,
