@@ -74,6 +74,12 @@ WORKLOADS["hk"] = dict(cell="hk", L=48, R=16, tmin=0.1, tmax=2.0, J=-1.0, D=0.3,
 WORKLOADS["stats"] = dict(L=96, nz=96, scale=10, J=-1.0, D=0.5, B=0.25, K=0.0, move="ball", r=0.2, tmin=0.1,
                           desc="chainMesh_statistics on SC L=96 (96 slices): winding per slice, magnetisation and "
                                "the 60 x 20 skyrmion search on the middle slice's 960 x 960 interpolated density")
+WORKLOADS["setup"] = dict(cell="bcc", L=128, sample_L=48,
+                          desc="mesh set-up (makeChainMesh: positions, shells, neighbour and derivative lists, "
+                               "colouring, device state) of the reference's BCC cell at 128^3 cells (4,194,304 atoms)")
+WORKLOADS["demag"] = dict(cell="sc", L=64,
+                          desc="calculate_demagnetisation_field on SC 64^3 (262,144 atoms): CIC deposit, 3-D "
+                               "transforms, k-space projection, gather; FP64 field returned to the host")
 BYTES_PER_UPDATE = 24  # algorithmic: one FP32 x,y,z read and write per site per sweep
 
 
@@ -279,6 +285,23 @@ def cpu_fast_rate(w, threads, L=64, sweeps=4):
 def run_reference(args, w):
     rank, world, _ = dist_env()
     if rank != 0:
+        return
+    if args.workload in ("setup", "demag"):
+        if args.workload == "setup":
+            cpu = setup_cpu_baseline(w)
+        else:
+            import numpy as np
+            rng = np.random.default_rng(0x15196)
+            sp = rng.normal(size=(w["L"] ** 3, 3))
+            sp /= np.linalg.norm(sp, axis=1, keepdims=True)
+            cpu, _ = demag_cpu_baseline(w, sp.astype(np.float32).astype(np.float64))
+        line = {"metric": cpu["unit"], "value": cpu["value"], "unit": cpu["unit"], "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / cpu["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": args.workload, "desc": w["desc"]},
+                "cpu_baseline": cpu,
+                "e2e": {"value": cpu["value"], "unit": cpu["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return
     if args.workload == "stats":
         L, nz = args.L or w["L"], w["nz"]
@@ -738,6 +761,135 @@ def stats_cpu_baseline(w, L, nz, spins, n_sample=4):
                       f"calculate_skyrmion_number restatement on the {fx}x{fx} density ({t_pair*1e3:.1f} ms each, "
                       f"scaled to {pairs}) plus the {nz} slice winding numbers, magnetisation and one FFT "
                       f"interpolation ({t_fixed*1e3:.1f} ms); the reference redoes the interpolation per pair"}
+
+
+def _secondary_line(args, w, metric, unit, value, world, per_step_s, clocks, cpu, e2e, extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * per_step_s, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": w["desc"],
+                       "timer": "host wall clock around synchronous C-ABI calls"},
+            "roofline": None,
+            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"],
+                       "samples": clocks["samples"]},
+            "e2e": e2e, "cpu_baseline": cpu}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def setup_cpu_baseline(w):
+    """The oracle's restatement of makeChainMesh (src/chainMesh.f90:729-911: shells by a scan of
+    the 125 surrounding cells per atom, neighbour and derivative lists) on one host thread, on a
+    smaller mesh of the same cell, scaled by atom count (its cost is linear in the atoms)."""
+    from oracle import oracle as O
+    O.build()
+    frac, (a, b, c, ab, bc, ca) = O.BCC_CELL if w["cell"] == "bcc" else O.SC_CELL
+    Ls = w["sample_L"]
+    t0 = time.perf_counter()
+    m = O.Mesh(frac, Ls, Ls, Ls, a, b, c, ab, bc, ca)
+    dt = time.perf_counter() - t0
+    n_sample = m.natoms
+    del m
+    n_full = w["L"] ** 3 * len(frac)
+    t_full = dt * n_full / n_sample
+    return {"value": 1.0 / t_full, "unit": "mesh set-ups/s", "cores": 1, "kind": "port",
+            "sample": f"BCC {Ls}^3 ({n_sample} atoms) in {dt:.2f} s, scaled by atoms to {n_full}"}
+
+
+def run_setup(args, w):
+    """One step = ising_mesh_create + ising_mesh_destroy of the workload's mesh (one replica):
+    the lattice compiler (per-sublattice stencils from one scan at cell 0, octant colouring) and
+    the device state, against the oracle's per-atom restatement of makeChainMesh."""
+    import torch
+    import ising_b200 as ib
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    L = args.L or w["L"]
+    a, b, c, ab, bc, ca, f = ib.bcc_unit_cell()
+    for _ in range(max(args.warmup, 1)):
+        ib.ChainMesh(L, L, L, f, a, b, c, ab, bc, ca, n_replicas=1, device=local).close()
+    clk = ClockSampler(getattr(torch.cuda.get_device_properties(local), "pci_bus_id", None))
+    clk.start()
+    torch.cuda.synchronize()
+    clk.mark()
+    t0 = time.perf_counter()
+    natoms = 0
+    for _ in range(args.steps):
+        m = ib.ChainMesh(L, L, L, f, a, b, c, ab, bc, ca, n_replicas=1, device=local)
+        natoms = m.numAtoms
+        m.close()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / args.steps
+    clocks = clk.stop()
+    cpu = setup_cpu_baseline(w) if rank == 0 and world == 1 and not args.no_cpu else None
+    if rank == 0:
+        _secondary_line(args, w, "mesh set-ups/s", "mesh set-ups/s", 1.0 / dt, world, dt, clocks, cpu,
+                        {"value": 1.0 / dt, "unit": "mesh set-ups/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0, "path": "ising_mesh_create from the unit cell (host arrays in, "
+                                                           "device state out) + ising_mesh_destroy"},
+                        {"gpu_launches": args.steps * 2, "result": {"atoms": natoms}})
+
+
+def demag_cpu_baseline(w, spins):
+    """oracle/demag_ref.demag_field (numpy FP64, numpy's FFTs standing in for FFTW) on the same
+    mesh and spins, one host process."""
+    from oracle import oracle as O
+    from oracle import demag_ref as D
+    O.build()
+    L = w["L"]
+    om = O.Mesh.sc(L)
+    t0 = time.perf_counter()
+    H = D.demag_field(om, spins)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "demag fields/s", "cores": 1, "kind": "port",
+            "sample": f"one field of SC {L}^3 ({om.natoms} atoms) in {dt:.2f} s"}, H
+
+
+def run_demag(args, w):
+    """One step = one ising_demag_field call on a resident replica (the field returned to the host
+    in FP64); e2e adds the upload of the spins.  The result is checked against the oracle."""
+    import numpy as np
+    import torch
+    import ising_b200 as ib
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    L = args.L or w["L"]
+    mesh = ib.ChainMesh.simple_cubic(L, device=local)
+    rng = np.random.default_rng(0x15196)
+    spins = rng.normal(size=(mesh.numAtoms, 3))
+    spins /= np.linalg.norm(spins, axis=1, keepdims=True)
+    spins = spins.astype(np.float32).astype(np.float64)
+    mesh.set_spins(spins)
+    for _ in range(max(args.warmup, 1)):
+        H = ib.demag_field(mesh, 0)
+    clk = ClockSampler(getattr(torch.cuda.get_device_properties(local), "pci_bus_id", None))
+    clk.start()
+    torch.cuda.synchronize()
+    clk.mark()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        H = ib.demag_field(mesh, 0)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / args.steps
+    clocks = clk.stop()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        mesh.set_spins(spins)
+        H = ib.demag_field(mesh, 0)
+    e2e_dt = (time.perf_counter() - t0) / max(1, args.steps // 2)
+    cpu, err = None, None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu, Href = demag_cpu_baseline(w, spins)
+        err = float(np.max(np.abs(H - Href)))
+    mesh.close()
+    if rank == 0:
+        n = spins.shape[0]
+        _secondary_line(args, w, "demag fields/s", "demag fields/s", 1.0 / dt, world, dt, clocks, cpu,
+                        {"value": 1.0 / e2e_dt, "unit": "demag fields/s", "h2d_bytes_per_step": int(n * 24),
+                         "d2h_bytes_per_step": int(n * 24), "path": "ising_spins_set (host doubles) -> "
+                                                                   "ising_demag_field (host doubles)"},
+                        {"gpu_launches": args.steps * 9, "result": {"max_abs_err_vs_oracle": err,
+                                                                    "max_abs_field": float(np.abs(H).max())}})
 
 
 def run_stats(args, w):
@@ -1252,6 +1404,10 @@ def main():
         run_c1(args)
     elif args.workload == "stats":
         run_stats(args, w)
+    elif args.workload == "setup":
+        run_setup(args, w)
+    elif args.workload == "demag":
+        run_demag(args, w)
     else:
         run_gpu(args, w)
 
