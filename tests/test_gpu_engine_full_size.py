@@ -52,6 +52,36 @@ def test_engine_equals_pt_path_at_c3_size(ib, cuda_ok, sched):
     pt.close()
 
 
+@pytest.mark.parametrize("sched", [dict(block_threads=96, chunk_pairs=4096, loader=0),
+                                   dict(block_threads=384, chunk_pairs=1 << 30, loader=2)],
+                         ids=["registers-96", "fused-384"])
+def test_engine_equals_pt_path_at_c5_shape(ib, cuda_ok, sched):
+    """The default workload's mesh (SC L=96, nz = 96: rows of 24 lanes) on the schedules the
+    autotuner picks for it, 12 of its 48 replicas, 2 rounds of 10 sweeps: bit-equal to the
+    per-pass PT path."""
+    L5, R5 = 96, 12
+    pp = ib.params(J=-1.0, Dz=0.5, B=0.25, dmi="bulk", include_Jp=False)
+    betas = 1.0 / ib.temperature_ladder(0.1, 1.5, R5)
+    em = ib.ChainMesh.simple_cubic(L5, n_replicas=R5)
+    rm = ib.ChainMesh.simple_cubic(L5, n_replicas=R5)
+    em.init_uniform(SEED, 0)
+    rm.init_uniform(SEED, 0)
+    eng = ib.Ensembles([(em, betas, pp, 0)], seed=SEED, move=ib._lib.MOVE_BALL, r=0.2)
+    eng.set_schedule(**sched)
+    eng.run(K_SWEEPS, 2)
+    pt = ib.ParallelTempering(rm, betas, pp, seed=SEED, ensemble=0, move=ib._lib.MOVE_BALL, r=0.2)
+    pt.run(K_SWEEPS, 2)
+    np.testing.assert_array_equal(eng.permutation(0), pt.permutation())
+    for r in range(R5):
+        np.testing.assert_array_equal(em.get_spins(r), rm.get_spins(r), err_msg=f"replica {r}")
+    e_run, _ = eng.energies(0)
+    eng.resync()
+    e_new, _ = eng.energies(0)
+    assert np.max(np.abs(e_run - e_new)) / em.numAtoms < 1e-6
+    eng.close()
+    pt.close()
+
+
 # C4: 12 simple cubic ensembles, L in {16, 24, 32, 48, 64, 96} twice, 16-64 replicas each,
 # (D, B) cycling over {0.3, 0.5, 0.7} x {0.1, 0.3}, T 0.1-2.0, bulk DMI, B along z (416
 # replicas, 148,160,512 sites in one persistent launch)
