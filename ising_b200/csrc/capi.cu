@@ -2190,8 +2190,8 @@ extern "C" int ising_ensembles_autotune(ising_ensembles* s, int k, int rounds_pe
     if (ens_staged_fits(s))   // groups of 4, 8 and 16 x-planes per task at nz = 128
         for (int c : {16384, 32768, 65536}) cand.push_back({256, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_STAGED});
     if (k % 2 == 0)           // one pass per sweep: chunk widths by block size, y-segments by chunk_pairs
-        for (int t : {256, 384, 512})
-            if (t >= 4 * max_lanes)
+        for (int t : {256, 384, 480, 512})
+            if (t >= 4 * max_lanes && (t != 480 || rows24))   // 480 = 20 whole rows of 24 lanes
                 for (int c : {16384, 65536, 1 << 30})
                     cand.push_back({t, c, ISING_ENS_ORDER_PHASE, 0, 0.0, ISING_ENS_LOADER_FUSED});
     cudaEvent_t e0, e1;
