@@ -212,7 +212,25 @@ struct OctDims {
     int hx, hyi, hzi;
 };
 
-template <int MOVE>
+// block sums of the four running partials: FP32 within a warp (a warp's few sites), FP64
+// across warps
+__device__ __forceinline__ void block_sum4_fd(float v0, float v1, float v2, float v3, double* out /* smem 4 */) {
+    __shared__ double red[4][32];
+    v0 = warp_sum(v0); v1 = warp_sum(v1); v2 = warp_sum(v2); v3 = warp_sum(v3);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) { red[0][wid] = v0; red[1][wid] = v1; red[2][wid] = v2; red[3][wid] = v3; }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double t = 0.0;
+        for (int k = 0; k < nw; ++k) t += red[threadIdx.x][k];
+        out[threadIdx.x] = t;
+    }
+    __syncthreads();
+}
+
+// SPT sites per thread (consecutive blocks of blockDim.x sites), so that the block's set-up
+// and its reduction are shared by SPT x 256 sites where a launch has enough of them
+template <int MOVE, int SPT>
 __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, OctDims od, int oct, int rank0,
                                                               int nrank) {
     extern __shared__ __align__(16) unsigned char oct_smem[];
@@ -260,10 +278,10 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
     const int hx = od.hx, hy = od.hyi, hz = od.hzi;
     const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
     float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
-    // one site per thread: a class of a small mesh still fills the GPU
-    {
-        const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-        if (t >= n) goto done;
+#pragma unroll 1
+    for (int it = 0; it < SPT; ++it) {
+        const uint32_t t = (blockIdx.x * SPT + it) * blockDim.x + threadIdx.x;
+        if (t >= n) break;
         const uint32_t lr = fdiv(t, od.q8);
         const uint32_t pc = t - lr * (uint32_t)q8;
         const uint32_t r = fdiv(pc, od.hz);
@@ -292,10 +310,9 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
         site_update<MOVE>(a, h, (int64_t)(class_base + t), (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
                           dmz);
     }
-done:
     if (a.partials) {
         __shared__ double tot[4];
-        block_sum4<double>(de, dmx, dmy, dmz, tot);
+        block_sum4_fd(de, dmx, dmy, dmz, tot);
         if (threadIdx.x == 0) {
             double* p = a.partials + ((int64_t)rep * a.slots_per_rep + a.slot_base + blockIdx.x) * 4;
             p[0] += tot[0]; p[1] += tot[1]; p[2] += tot[2]; p[3] += tot[3];
@@ -527,14 +544,27 @@ int launch_octant_colour(const GeneralLaunch& a, int oct, int rank0, int nrank, 
         return fail(ISING_ERR_ARG, "octant class out of range");
     dim3 g(octant_slots_for(n, a.oct_maxcnt > 0), a.n_rep), b(kGenThreads);
     if (a.oct_maxcnt > 0) {
+        // sites per thread: as many as keep about two waves of blocks (6 resident per SM);
+        // fewer blocks than partial slots leave the last slots at zero
+        int sms = 148;
+        {
+            int dev = 0;
+            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        }
+        const int64_t per_launch = n * a.n_rep, want = 2LL * sms * 6 * kGenThreads;
+        const int spt = per_launch >= 4 * want ? 4 : (per_launch >= 2 * want ? 2 : 1);
+        g.x = (unsigned)((n + (int64_t)kGenThreads * spt - 1) / ((int64_t)kGenThreads * spt));
         OctDims od;
         od.q8 = make_div((uint32_t)a.layout.q8);
         od.hx = a.nx / 2; od.hyi = a.ny / 2; od.hzi = a.nz / 2;
         od.hz = make_div((uint32_t)od.hzi);
         od.hy = make_div((uint32_t)od.hyi);
         const size_t sm = (size_t)nrank * a.oct_maxcnt * sizeof(OctSlot) + 2 * (size_t)nrank * sizeof(int);
-        if (a.move == 0) k_octant_fast<0><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
-        else k_octant_fast<1><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
+#define ISG_OF(S)                                                                      \
+    if (a.move == 0) k_octant_fast<0, S><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);   \
+    else k_octant_fast<1, S><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
+        if (spt == 4) { ISG_OF(4) } else if (spt == 2) { ISG_OF(2) } else { ISG_OF(1) }
+#undef ISG_OF
         ISG_CUDA(cudaGetLastError());
         return ISING_OK;
     }
