@@ -293,18 +293,14 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
             if (!m->d_oct_sync)
                 ISG_TRY(dev_alloc(&m->d_oct_sync, (size_t)m->n_replicas * (size_t)(Lt.nx / 2) + 2));
         }
-        int min_class = INT32_MAX;
-        for (int k = 0; k < 8 * ng; ++k) {
-            const int64_t n = m->layout.q8 * (m->oct_rank0[k % ng + 1] - m->oct_rank0[k % ng]);
-            tot += octant_slots_for(n, plan->oct_maxcnt > 0);
-            min_class = (int)std::min<int64_t>(min_class, n);
-        }
-        // replicas per group: a group runs all its sweeps before the next group starts, so
-        // groups that fit L2 keep their spins there; but a class launch of a group must still
-        // fill the GPU, which wins over the L2 bound for meshes with small classes
-        const int g_l2 = std::max(1, (int)(kL2GroupBytes / (12.0 * (double)Lt.natoms)));
-        const int g_fill = (int)((kOctMinLaunchSites + min_class - 1) / std::max(min_class, 1));
-        plan->group = std::max(g_l2, g_fill);
+        for (int k = 0; k < 8 * ng; ++k)
+            tot += octant_slots_for(m->layout.q8 * (m->oct_rank0[k % ng + 1] - m->oct_rank0[k % ng]),
+                                    plan->oct_maxcnt > 0);
+        // every replica in each class launch: L2-sized replica groups (a group running all its
+        // sweeps before the next) measured no faster on BCC 96^3 x 16 and much slower on
+        // hyper-kagome, whose classes are small; large launches let a thread take several sites
+        // (ising_pt_options.l2_group still sets a group size)
+        plan->group = INT32_MAX;
         if (plan->oct_maxcnt > 0) tot = std::max(tot, Lt.nx / 2);
     } else {
         for (int k = 0; k < plan->col->ncol; ++k)

@@ -140,7 +140,6 @@ int mesh_settle(const ising_mesh* m);
 namespace isg {
 constexpr int kScratchDoubles = 1 << 16;
 constexpr double kL2GroupBytes = 64.0e6;   // replica group size of the paired colour schedule
-constexpr int64_t kOctMinLaunchSites = 148 * 2048;   // octant classes: sites per launch to fill the GPU
 
 // Kernel launchers.
 // Colour-separated checkerboard sweep (sweep_cb.cu): up to two segments per launch, each a
