@@ -230,7 +230,6 @@ struct SweepPlan {
     int* d_count = nullptr;
     const float* demag = nullptr;   // general path: demagnetising field of the swept replica
     int oct_maxcnt = 0;        // octant layout: k_octant_fast's table width (0: k_octant_colour)
-    bool oct_unit = false;     // every neighbour offset within one packed cell (interior split)
     bool oct_engine = false;   // octant layout: every sweep of a call in one persistent launch
     int oct_reach = 1;         // its dependency reach in packed x-planes
     int oct_grid = 0;          // its persistent blocks
@@ -269,7 +268,7 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
         ISG_TRY(fill_query_stencil_host(m, p, false, hs.data(), hc.data()));
         const Lattice& Lt = m->lat;
         const int half[3] = {Lt.nx / 2, Lt.ny / 2, Lt.nz / 2};
-        int maxcnt = 0, reach = 0, reach_any = 0;
+        int maxcnt = 0, reach = 0;
         bool fits = true;
         for (int sub = 0; sub < Lt.nsub; ++sub) {
             maxcnt = std::max(maxcnt, hc[sub]);
@@ -282,12 +281,10 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
                         const int ex = (t - (t & 1)) / 2;
                         if (ex < -half[ax] || ex > half[ax]) fits = false;
                         if (ax == 0) reach = std::max(reach, std::abs(ex));
-                        reach_any = std::max(reach_any, std::abs(ex));
                     }
             }
         }
         plan->oct_maxcnt = fits ? std::max(maxcnt, 1) : 0;
-        plan->oct_unit = reach_any <= 1;
         // the persistent engine (opt-in, sweep_kernel 3): one partial slot per (replica,
         // packed x-plane); plan->oct_engine is set by the PT object that asks for it
         if (plan->oct_maxcnt > 0) {
@@ -400,7 +397,6 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
         // (every class, in order) before the next group starts, so a group's spins stay in L2
         const int ng = (int)m->oct_rank0.size() - 1;
         g.oct_maxcnt = plan.oct_maxcnt;
-        g.oct_unit = plan.oct_unit ? 1 : 0;
         const int G = std::max(1, plan.group);
         for (int gr = 0; gr < n_rep; gr += G) {
             g.rep_first = rep_first + gr;

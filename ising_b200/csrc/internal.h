@@ -196,7 +196,6 @@ struct GeneralLaunch {
     float mu0;             // its factor in the local field: h -= mu0 H
     int oct_maxcnt;        // octant layout: largest stencil of a sublattice when every neighbour's
                            // packed offset needs at most one periodic wrap (k_octant_fast), else 0
-    int oct_unit;          // every neighbour's packed offset is -1, 0 or +1 on every axis
 };
 int launch_general_colour(const GeneralLaunch& a, cudaStream_t s);
 // One class (octant, sublattice group) of an octant-layout mesh: sites of storage ranks

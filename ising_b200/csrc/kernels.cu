@@ -205,19 +205,11 @@ struct __align__(16) OctSlot {
     int plane;               // (octant * nsub + storage rank) * q8 of the neighbour
     int8_t ex, ey, ez, pad;  // packed-cell offsets
     float w, Dx, Dy, Dz;
-    int koff;                // plane + ex hyz + ey hz + ez: the neighbour of an interior site
-    int pad2;                // 32 bytes: two 16-byte shared-memory loads
+    float pad2[2];           // 32 bytes: two 16-byte shared-memory loads
 };
 struct OctDims {
     FastDiv q8, hz, hy, hyz;
     int hx, hyi, hzi;
-    // interior / boundary split of a class (k_octant_fast): the interior box X, Y, Z in
-    // [1, h - 2] needs no periodic wrap for any neighbour (offsets within one cell), the
-    // boundary shell is enumerated as planes X = 0, hx-1, then rows Y = 0, hy-1, then Z = 0, hz-1
-    int ix, iy, iz;                  // interior extents (h - 2, at least 0)
-    uint32_t n_in, n_bd;             // interior and boundary sites per rank
-    FastDiv d_in, d_iyz, d_iz;       // by n_in, iy * iz, iz
-    FastDiv d_bd, d_bxz, d_bxy, d_biy;   // by n_bd, ix * hz, ix * iy, iy
 };
 
 // block sums of the four running partials: FP32 within a warp (a warp's few sites), FP64
@@ -240,7 +232,7 @@ __device__ __forceinline__ void block_sum4_fd(float v0, float v1, float v2, floa
 // and its reduction are shared by SPT x 256 sites where a launch has enough of them
 template <int MOVE, int SPT>
 __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, OctDims od, int oct, int rank0,
-                                                              int nrank, int n_in_blocks) {
+                                                              int nrank) {
     extern __shared__ __align__(16) unsigned char oct_smem[];
     const int mc = a.oct_maxcnt;
     OctSlot* tab = reinterpret_cast<OctSlot*>(oct_smem);
@@ -266,7 +258,6 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
             o.plane = (o2 * a.nsub + s_srank[sl.sub]) * q8;
             o.ex = (int8_t)(tx >> 1); o.ey = (int8_t)(ty >> 1); o.ez = (int8_t)(tz >> 1);
             o.w = sl.w; o.Dx = sl.Dx; o.Dy = sl.Dy; o.Dz = sl.Dz;
-            o.koff = o.plane + (int)o.ex * od.hyi * od.hzi + (int)o.ey * od.hzi + (int)o.ez;
         }
         tab[e] = o;
     }
@@ -283,95 +274,41 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
     float* __restrict__ sz = sy + N;
     const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
     const float beta = (float)a.beta_rep[rep];
+    const uint32_t n = (uint32_t)q8 * (uint32_t)nrank;
     const int hx = od.hx, hy = od.hyi, hz = od.hzi;
-    const uint32_t hyz = (uint32_t)hy * (uint32_t)hz;
     const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
-    // blocks [0, n_in_blocks) take the interior box, the rest the boundary shell (or, with
-    // od.n_in = 0, every site in storage order)
-    const bool inner = (int)blockIdx.x < n_in_blocks;
-    const uint32_t b = inner ? blockIdx.x : blockIdx.x - (uint32_t)n_in_blocks;
-    const uint32_t n = (inner ? od.n_in : od.n_bd) * (uint32_t)nrank;
     float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
 #pragma unroll 1
     for (int it = 0; it < SPT; ++it) {
-        const uint32_t t = (b * SPT + it) * blockDim.x + threadIdx.x;
+        const uint32_t t = (blockIdx.x * SPT + it) * blockDim.x + threadIdx.x;
         if (t >= n) break;
-        uint32_t lr;
-        int X, Y, Z;
-        if (inner) {
-            lr = fdiv(t, od.d_in);
-            const uint32_t r = t - lr * od.n_in;
-            const uint32_t xq = fdiv(r, od.d_iyz);
-            const uint32_t r2 = r - xq * (uint32_t)(od.iy * od.iz);
-            const uint32_t yq = fdiv(r2, od.d_iz);
-            X = (int)xq + 1; Y = (int)yq + 1; Z = (int)(r2 - yq * (uint32_t)od.iz) + 1;
-        } else if (od.n_in == 0) {   // no split: storage order
-            lr = fdiv(t, od.q8);
-            const uint32_t pc0 = t - lr * (uint32_t)q8;
-            const uint32_t r = fdiv(pc0, od.hz);
-            Z = (int)(pc0 - r * (uint32_t)hz);
-            const uint32_t Xu = fdiv(r, od.hy);
-            Y = (int)(r - Xu * (uint32_t)hy); X = (int)Xu;
-        } else {
-            lr = fdiv(t, od.d_bd);
-            uint32_t r = t - lr * od.n_bd;
-            const uint32_t bxz = (uint32_t)od.ix * (uint32_t)hz, bxy = (uint32_t)od.ix * (uint32_t)od.iy;
-            if (r < 2u * hyz) {              // planes X = 0 and X = hx - 1
-                const uint32_t side = r >= hyz ? 1u : 0u;
-                r -= side * hyz;
-                X = side ? hx - 1 : 0;
-                const uint32_t yq = fdiv(r, od.hz);
-                Y = (int)yq; Z = (int)(r - yq * (uint32_t)hz);
-            } else if (r < 2u * hyz + 2u * bxz) {   // rows Y = 0 and Y = hy - 1 of the inner planes
-                r -= 2u * hyz;
-                const uint32_t side = r >= bxz ? 1u : 0u;
-                r -= side * bxz;
-                Y = side ? hy - 1 : 0;
-                const uint32_t xq = fdiv(r, od.hz);
-                X = (int)xq + 1; Z = (int)(r - xq * (uint32_t)hz);
-            } else {                          // Z = 0 and Z = hz - 1 of the inner rows
-                r -= 2u * hyz + 2u * bxz;
-                const uint32_t side = r >= bxy ? 1u : 0u;
-                r -= side * bxy;
-                Z = side ? hz - 1 : 0;
-                const uint32_t xq = fdiv(r, od.d_biy);
-                X = (int)xq + 1; Y = (int)(r - xq * (uint32_t)od.iy) + 1;
-            }
-        }
-        const uint32_t pc = (uint32_t)X * hyz + (uint32_t)(Y * hz + Z);
+        const uint32_t lr = fdiv(t, od.q8);
+        const uint32_t pc = t - lr * (uint32_t)q8;
+        const uint32_t r = fdiv(pc, od.hz);
+        const int Z = (int)(pc - r * (uint32_t)hz);
+        const uint32_t Xu = fdiv(r, od.hy);
+        const int Y = (int)(r - Xu * (uint32_t)hy), X = (int)Xu;
         const int sub = s_sub[lr];
         const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z + oz;
         const uint32_t at = ((uint32_t)(ix * a.ny + iy) * (uint32_t)a.nz + (uint32_t)iz) * (uint32_t)a.nsub + sub;
         const OctSlot* ts = tab + lr * mc;
         f3 h = {0.f, 0.f, 0.f};
         const int cn = s_cnt[lr];
-        if (inner) {   // every neighbour within the period: one add per neighbour
-            for (int q = 0; q < cn; ++q) {
-                const OctSlot o = ts[q];
-                const uint32_t j = pc + (uint32_t)o.koff;
-                const f3 sj = {sx[j], sy[j], sz[j]};
-                const f3 c = cross(sj, mk(o.Dx, o.Dy, o.Dz));
-                h.x += fmaf(o.w, sj.x, c.x);
-                h.y += fmaf(o.w, sj.y, c.y);
-                h.z += fmaf(o.w, sj.z, c.z);
-            }
-        } else {
-            for (int q = 0; q < cn; ++q) {
-                const OctSlot o = ts[q];
-                int jx = X + o.ex, jy = Y + o.ey, jz = Z + o.ez;
-                jx += jx < 0 ? hx : 0; jx -= jx >= hx ? hx : 0;
-                jy += jy < 0 ? hy : 0; jy -= jy >= hy ? hy : 0;
-                jz += jz < 0 ? hz : 0; jz -= jz >= hz ? hz : 0;
-                const uint32_t j = (uint32_t)o.plane + (uint32_t)((jx * hy + jy) * hz + jz);
-                const f3 sj = {sx[j], sy[j], sz[j]};
-                const f3 c = cross(sj, mk(o.Dx, o.Dy, o.Dz));
-                h.x += fmaf(o.w, sj.x, c.x);
-                h.y += fmaf(o.w, sj.y, c.y);
-                h.z += fmaf(o.w, sj.z, c.z);
-            }
+        for (int q = 0; q < cn; ++q) {
+            const OctSlot o = ts[q];
+            int jx = X + o.ex, jy = Y + o.ey, jz = Z + o.ez;
+            jx += jx < 0 ? hx : 0; jx -= jx >= hx ? hx : 0;
+            jy += jy < 0 ? hy : 0; jy -= jy >= hy ? hy : 0;
+            jz += jz < 0 ? hz : 0; jz -= jz >= hz ? hz : 0;
+            const uint32_t j = (uint32_t)o.plane + (uint32_t)((jx * hy + jy) * hz + jz);
+            const f3 sj = {sx[j], sy[j], sz[j]};
+            const f3 c = cross(sj, mk(o.Dx, o.Dy, o.Dz));
+            h.x += fmaf(o.w, sj.x, c.x);
+            h.y += fmaf(o.w, sj.y, c.y);
+            h.z += fmaf(o.w, sj.z, c.z);
         }
-        site_update<MOVE>(a, h, (int64_t)(class_base + lr * (uint32_t)q8 + pc), (int64_t)at, sx, sy, sz, sweep, rep,
-                          beta, de, dmx, dmy, dmz);
+        site_update<MOVE>(a, h, (int64_t)(class_base + t), (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
+                          dmz);
     }
     if (a.partials) {
         __shared__ double tot[4];
@@ -597,8 +534,7 @@ int launch_octant_engine(const GeneralLaunch& a, const OctEngineLaunch& e, cudaS
 
 int octant_slots_for(int64_t n_sites, bool fast) {
     const int64_t per = (int64_t)kGenThreads * (fast ? 1 : kGenSitesPerThread);
-    // k_octant_fast splits a class into an interior and a boundary part: one block more
-    return (int)((n_sites + per - 1) / per) + (fast ? 1 : 0);
+    return (int)((n_sites + per - 1) / per);
 }
 
 int launch_octant_colour(const GeneralLaunch& a, int oct, int rank0, int nrank, cudaStream_t s) {
@@ -617,33 +553,16 @@ int launch_octant_colour(const GeneralLaunch& a, int oct, int rank0, int nrank, 
         }
         const int64_t per_launch = n * a.n_rep, want = 2LL * sms * 6 * kGenThreads;
         const int spt = per_launch >= 4 * want ? 4 : (per_launch >= 2 * want ? 2 : 1);
-        OctDims od{};
+        g.x = (unsigned)((n + (int64_t)kGenThreads * spt - 1) / ((int64_t)kGenThreads * spt));
+        OctDims od;
         od.q8 = make_div((uint32_t)a.layout.q8);
         od.hx = a.nx / 2; od.hyi = a.ny / 2; od.hzi = a.nz / 2;
         od.hz = make_div((uint32_t)od.hzi);
         od.hy = make_div((uint32_t)od.hyi);
-        od.hyz = make_div((uint32_t)(od.hyi * od.hzi));
-        // the interior split needs every neighbour within one packed cell on every axis
-        if (a.oct_unit) {
-            od.ix = std::max(od.hx - 2, 0); od.iy = std::max(od.hyi - 2, 0); od.iz = std::max(od.hzi - 2, 0);
-        }
-        od.n_in = (uint32_t)(od.ix * od.iy * od.iz);
-        od.n_bd = (uint32_t)a.layout.q8 - od.n_in;
-        od.d_in = make_div(std::max(od.n_in, 1u));
-        od.d_iyz = make_div((uint32_t)std::max(od.iy * od.iz, 1));
-        od.d_iz = make_div((uint32_t)std::max(od.iz, 1));
-        od.d_bd = make_div(std::max(od.n_bd, 1u));
-        od.d_bxz = make_div((uint32_t)std::max(od.ix * od.hzi, 1));
-        od.d_bxy = make_div((uint32_t)std::max(od.ix * od.iy, 1));
-        od.d_biy = make_div((uint32_t)std::max(od.iy, 1));
-        const int64_t per_block = (int64_t)kGenThreads * spt;
-        const int n_in_blocks = (int)(((int64_t)od.n_in * nrank + per_block - 1) / per_block);
-        const int n_bd_blocks = (int)(((int64_t)od.n_bd * nrank + per_block - 1) / per_block);
-        g.x = (unsigned)(n_in_blocks + n_bd_blocks);   // <= octant_slots_for(n, true)
         const size_t sm = (size_t)nrank * a.oct_maxcnt * sizeof(OctSlot) + 2 * (size_t)nrank * sizeof(int);
-#define ISG_OF(S)                                                                                   \
-    if (a.move == 0) k_octant_fast<0, S><<<g, b, sm, s>>>(a, od, oct, rank0, nrank, n_in_blocks);   \
-    else k_octant_fast<1, S><<<g, b, sm, s>>>(a, od, oct, rank0, nrank, n_in_blocks);
+#define ISG_OF(S)                                                                      \
+    if (a.move == 0) k_octant_fast<0, S><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);   \
+    else k_octant_fast<1, S><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
         if (spt == 4) { ISG_OF(4) } else if (spt == 2) { ISG_OF(2) } else { ISG_OF(1) }
 #undef ISG_OF
         ISG_CUDA(cudaGetLastError());
