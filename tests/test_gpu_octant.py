@@ -141,3 +141,26 @@ def test_octant_engine_timeout_and_recovery(oracle, ib, cuda_ok):
         s = pm.get_spins(r)
         assert np.max(np.abs(np.linalg.norm(s, axis=1) - 1.0)) < 1e-5
     pt.close()
+
+
+def test_octant_engine_option_errors(oracle, ib, cuda_ok):
+    """The persistent octant engine is refused where it cannot run (a checkerboard mesh), and
+    the stall hook without the engine or with a bound outside 1..60000 ms is refused."""
+    sc = ib.ChainMesh.simple_cubic(8, n_replicas=2)
+    pp = ib.params(J=-1.0, Dz=0.3, B=0.1, dmi="bulk", include_Jp=False)
+    with pytest.raises(ib.IsingError) as e:
+        ib.ParallelTempering(sc, np.array([1.0, 0.5]), pp, seed=1, sweep_kernel=3)
+    assert e.value.status == 1
+    pt = ib.ParallelTempering(sc, np.array([1.0, 0.5]), pp, seed=1)
+    with pytest.raises(ib.IsingError):
+        pt.inject_stall(100)
+    pt.close()
+    om, pm = _pair(oracle, ib, "BCC", (4, 4, 4), n_replicas=2)
+    op, bp = _both_params(oracle, ib, J=-1.0, Dz=0.3, B=0.1)
+    pt = ib.ParallelTempering(pm, np.array([1.0, 0.5]), bp, seed=1, sweep_kernel=3)
+    for bad in (0, 60001):
+        with pytest.raises(ib.IsingError) as e:
+            pt.inject_stall(bad)
+        assert e.value.status == 1
+    pt.run(2, 1)
+    pt.close()
