@@ -73,7 +73,10 @@ typedef struct {
     int checkerboard;        /* storage order of the spins on the device: 1 the SC 2-colour fast path
                                 (even nx, ny; nz % 4 == 0); 2 the octant order of other crystals
                                 with even extents (colour classes = cell octant x sublattice
-                                group, each one contiguous range); 0 the reference atom order */
+                                group, each one contiguous range); 3 sublattice planes of
+                                two-sublattice crystals whose first shell joins only the two
+                                sublattices (BCC; the colour classes are the sublattices);
+                                0 the reference atom order */
     double a_vec[3], b_vec[3], c_vec[3];
 } ising_mesh_info;
 
@@ -157,7 +160,8 @@ int ising_params_reference(int which, double J, double J_prime, double Dz, doubl
                            double B, ising_params* p);
 
 /* Colour class of every atom as the sweep uses it for the Hamiltonian p: the checkerboard
- * (x+y+z)&1 on simple-cubic meshes with even nx, ny, nz % 4 == 0 and no J'; on other crystals
+ * (x+y+z)&1 on simple-cubic meshes with even nx, ny, nz % 4 == 0 and no J'; the sublattice on
+ * BCC meshes (layout 3) without J'; on other crystals
  * with even extents whose shells 1-2 never join one sublattice at an all-even non-zero cell
  * offset (BCC and hyper-kagome, src/unit_cells.f90:7-77), class octant * groups + group of the
  * cell octant (x&1, y&1, z&1) and a sublattice group (sublattices bonded at an all-even offset
@@ -211,8 +215,9 @@ int ising_observables(const ising_mesh* mesh, const ising_params* p, double* e, 
 
 /* Replaces Metropolis_mcs(chainMesh, beta, numMCSSweeps, J, J', Dz, Dz', B, r, lockArray,
  * demag) (src/energyMin.f90:234-374).  A sweep visits every atom once through colour
- * classes (checkerboard on even simple-cubic meshes, octant classes on other crystals with
- * even extents, greedy colouring otherwise) with
+ * classes (checkerboard on even simple-cubic meshes, the two sublattices on BCC meshes
+ * without J', octant classes on other crystals with even extents, greedy colouring
+ * otherwise) with
  * Philox keyed by (seed, ensemble 0, replica, sweep, atom); the per-replica sweep counter
  * lives in the handle so successive calls continue the stream.  r > 0 selects the ball
  * move of radius r, r <= 0 the uniform move.  lockArray has no counterpart (no locks). */
@@ -310,7 +315,8 @@ int ising_pt_inject_stall(ising_pt* pt, int wait_ms);
 /* Launch schedule of a round: replicas per L2 group, colour-pass launches per round of
  * sweeps_per_swap sweeps, and which colour-pass kernel runs (1 register, 2 TMA-staged,
  * 0 the stencil kernel of the greedy or octant colouring, 3 the octant kernel with the
- * stencil resolved per class, 4 the persistent octant engine).  No reference counterpart. */
+ * stencil resolved per class, 4 the persistent octant engine, 5 the sublattice classes of
+ * BCC meshes).  No reference counterpart. */
 int ising_pt_schedule(const ising_pt* pt, int sweeps_per_swap, int* l2_group, int* pass_launches,
                       int* kernel);
 /* temperature slot -> replica (TemperatureMeshArray(i, :), src/PT.f90:58) */

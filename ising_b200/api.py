@@ -119,7 +119,8 @@ class ChainMesh:
         self.n_sub = info.n_sub
         self.n_replicas = info.n_replicas
         self.checkerboard = info.checkerboard == 1
-        self.layout = {0: "reference", 1: "checkerboard", 2: "octant"}.get(info.checkerboard, str(info.checkerboard))
+        self.layout = {0: "reference", 1: "checkerboard", 2: "octant", 3: "sublattice"}.get(info.checkerboard,
+                                                                                            str(info.checkerboard))
         self.a_vec = np.array(info.a_vec[:])
         self.b_vec = np.array(info.b_vec[:])
         self.c_vec = np.array(info.c_vec[:])

@@ -195,6 +195,12 @@ int host_colouring(ising_mesh* m, bool shell2, Colouring& c) {
         c.ncol = 8 * ng;
         return ISING_OK;
     }
+    if (m->layout.cb == 3 && !shell2) {   // the two sublattices
+        c.host_colour.resize(L.natoms);
+        for (int64_t at = 0; at < L.natoms; ++at) c.host_colour[at] = (int)(at % 2);
+        c.ncol = 2;
+        return ISING_OK;
+    }
     int ncol = 0;
     ISG_TRY(greedy_colouring(L, shell2, &c.host_colour, &ncol));
     c.ncol = ncol;
@@ -233,6 +239,8 @@ struct SweepPlan {
     bool oct_engine = false;   // octant layout: every sweep of a call in one persistent launch
     int oct_reach = 1;         // its dependency reach in packed x-planes
     int oct_grid = 0;          // its persistent blocks
+    bool bip = false;          // layout 3 without J': the two sublattice classes (k_bip_sweep)
+    BipClass bipc[2] = {};     // their first-shell bonds
     int oct_stall = 0;         // test hook (ising_pt_inject_stall): the next round's waits run out
     uint64_t oct_wait_ns = 2000000000ull;   // bound of every wait of the engine
 };
@@ -259,6 +267,34 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
     ISG_TRY(upload_stencil(m, p, false, slots, count));
     ISG_TRY(ensure_colouring(m, sh2, &plan->col));
     int tot = 0;
+    if (m->layout.cb == 3 && !sh2 && !p.demag && m->lat.nz % 2 == 0 && m->lat.nz / 2 <= 256) {
+        // the first shell of each sublattice as bonds (a, b, c) to the other one
+        std::vector<Slot> hs((size_t)kMaxSub * kMaxSlots);
+        std::vector<int> hc(kMaxSub, 0);
+        ISG_TRY(fill_query_stencil_host(m, p, false, hs.data(), hc.data()));
+        bool ok = true;
+        for (int sb = 0; sb < 2 && ok; ++sb) {
+            BipClass& c = plan->bipc[sb];
+            for (int k = 0; k < 3; ++k) c.base[k] = m->bip_base[sb][k];
+            int seen = 0;
+            ok = hc[sb] == 8;
+            for (int q = 0; q < hc[sb] && ok; ++q) {
+                const Slot& e = hs[(size_t)sb * kMaxSlots + q];
+                const int aa = e.dx - c.base[0], bb = e.dy - c.base[1], cc = e.dz - c.base[2];
+                ok = e.sub == 1 - sb && aa >= 0 && aa <= 1 && bb >= 0 && bb <= 1 && cc >= 0 && cc <= 1;
+                if (!ok) break;
+                const int i = aa * 4 + bb * 2 + cc;
+                seen |= 1 << i;
+                c.w[i] = e.w; c.D[i][0] = e.Dx; c.D[i][1] = e.Dy; c.D[i][2] = e.Dz;
+            }
+            ok = ok && seen == 0xff;
+        }
+        if (ok) {
+            plan->bip = true;
+            plan->slots_per_rep = 2 * bip_slots_per_class();
+            return ISING_OK;
+        }
+    }
     if (m->layout.cb == 2) {
         const int ng = (int)m->oct_rank0.size() - 1;
         // the per-class stencil of k_octant_fast: every packed offset floor((o + d) / 2),
@@ -373,6 +409,16 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
     g.ham = plan.ham; g.st = StencilDev{plan.d_slots, plan.d_count, L.nsub}; g.layout = m->layout;
     g.partials = partials; g.slots_per_rep = plan.slots_per_rep; g.status = m->d_status;
     g.demag = plan.demag; g.mu0 = (float)kMu0;
+    if (m->layout.cb == 3 && plan.bip) {   // the two sublattice classes
+        for (int sw = 0; sw < n_sweeps; ++sw) {
+            g.sweep_offset = sw0 + (uint32_t)sw;
+            for (int sb = 0; sb < 2; ++sb) {
+                g.slot_base = sb * bip_slots_per_class();
+                ISG_TRY(launch_bip_sweep(g, plan.bipc[sb], sb, m->stream));
+            }
+        }
+        return ISING_OK;
+    }
     if (m->layout.cb == 2 && plan.oct_engine) {   // every sweep of the call in one launch
         OctEngineLaunch e{};
         const int hx = L.nx / 2;
@@ -507,9 +553,12 @@ extern "C" int ising_mesh_create(const float* frac, int nsub, int nx, int ny, in
         m->layout = Layout{m->checkerboard && L.nz % 4 == 0 ? 1 : 0, L.nx, L.ny, L.nz, L.nsub, L.natoms / 2};
         std::vector<int> grp;
         int ng = 0;
-        // other crystals: octant order when the octant colouring applies (ranks grouped by
-        // sublattice group, so each colour class is one contiguous range)
-        if (!m->checkerboard && octant_groups(L, &grp, &ng)) {
+        // two sublattices joined only to each other (BCC): sublattice planes; other crystals:
+        // octant order when the octant colouring applies (ranks grouped by sublattice group,
+        // so each colour class is one contiguous range)
+        if (!m->checkerboard && bipartite_pair(L, m->bip_base)) {
+            m->layout.cb = 3;
+        } else if (!m->checkerboard && octant_groups(L, &grp, &ng)) {
             m->layout.cb = 2;
             m->layout.q8 = L.ncells / 8;
             int next = 0;
@@ -1334,14 +1383,16 @@ extern "C" int ising_pt_schedule(const ising_pt* pt, int k, int* group, int* lau
     int G = (pt->n + grp - 1) / grp;
     int L = 0;
     if (P.sc) L = G > 1 ? G * k + 1 : 2 * k;
+    else if (P.bip) { L = 2 * k; grp = pt->n; }
     else if (oct && P.oct_engine) { L = 1; grp = pt->n; }
     else if (oct) L = G * k * 8 * ((int)pt->mesh->oct_rank0.size() - 1);
     else L = k * P.col->ncol;
     if (group) *group = grp;
     if (launches) *launches = L;
     // 0 k_general_colour / k_octant_colour, 1 k_cb_sweep, 2 k_cb_tma, 3 k_octant_fast,
-    // 4 k_octant_engine
-    if (kernel) *kernel = P.sc ? (P.tma ? 2 : 1) : (oct ? (P.oct_engine ? 4 : (P.oct_maxcnt > 0 ? 3 : 0)) : 0);
+    // 4 k_octant_engine, 5 k_bip_sweep
+    if (kernel)
+        *kernel = P.sc ? (P.tma ? 2 : 1) : P.bip ? 5 : (oct ? (P.oct_engine ? 4 : (P.oct_maxcnt > 0 ? 3 : 0)) : 0);
     return ISING_OK;
 }
 

@@ -148,6 +148,10 @@ struct StencilDev {
 // packed cell ((x>>1, y>>1), z>>1).  A colour class (octant, sublattice group) is then one
 // contiguous range (the sublattices of a group have consecutive ranks), and the neighbours
 // of consecutive sites through one stencil slot are consecutive as well.
+// cb = 3 (two-sublattice crystals whose first shell only joins the two sublattices, the
+// reference's BCC cell): sublattice planes -- all sites of sublattice 0 in (x, y, z) order,
+// then sublattice 1, so each sublattice is a colour class of the first shell and a row of one
+// sublattice reads consecutive z-sites of the other.
 struct Layout {
     int cb;
     int nx, ny, nz, nsub;
@@ -164,6 +168,7 @@ __host__ __device__ __forceinline__ int64_t sidx(const Layout& L, int ix, int iy
         const int64_t packed = ((int64_t)(ix >> 1) * (L.ny >> 1) + (iy >> 1)) * (L.nz >> 1) + (iz >> 1);
         return ((int64_t)oct * L.nsub + L.srank[sub]) * L.q8 + packed;
     }
+    if (L.cb == 3) return (((int64_t)sub * L.nx + ix) * L.ny + iy) * L.nz + iz;   // sublattice planes
     const int c = (ix + iy + iz) & 1;
     return c * L.half + ((int64_t)ix * L.ny + iy) * (L.nz >> 1) + (iz >> 1);
 }

@@ -70,6 +70,9 @@ bool is_checkerboard_sc(const Lattice& L);
 // general crystal; false when the octant colouring does not apply (odd extents, or a bond of
 // shells 1-2 between two sites of one sublattice at an all-even non-zero cell offset).
 bool octant_groups(const Lattice& L, std::vector<int>* group, int* ngroups);
+// two sublattices joined only to each other by the first shell, 8 neighbours in cells
+// base + {0,1}^3 (layout 3); base[s] per sublattice
+bool bipartite_pair(const Lattice& L, int base[2][3]);
 
 // ---------------------------------------------------------------- device-side handle
 struct Colouring {
@@ -116,6 +119,7 @@ struct ising_mesh {
     void* xfer = nullptr;                // asynchronous spin transfers (streams, per-replica staging)
     void* demag = nullptr;               // demagnetising-field workspace, made on first use
     uint32_t* d_oct_sync = nullptr;      // octant engine: [n_replicas][nx/2] counters + head + abort
+    int bip_base[2][3] = {{0, 0, 0}, {0, 0, 0}};   // layout 3: first-shell cell offsets per sublattice
 };
 
 namespace isg {
@@ -217,6 +221,15 @@ struct OctEngineLaunch {
     int stall;               // test hook: the tasks of phase 1 wait for a count nothing reaches
 };
 int launch_octant_engine(const GeneralLaunch& a, const OctEngineLaunch& e, cudaStream_t s);
+// One sublattice class of a layout-3 mesh (BCC without J'): the first shell of sublattice
+// `sub` as 8 bonds to the other sublattice's cells base + (a, b, c), a, b, c in {0, 1}.
+struct BipClass {
+    int base[3];
+    float w[8];              // bond (a, b, c) at index a * 4 + b * 2 + c
+    float D[8][3];
+};
+int launch_bip_sweep(const GeneralLaunch& a, const BipClass& c, int sub, cudaStream_t s);
+int bip_slots_per_class();   // partial-sum slots (blocks) of one class launch
 int octant_engine_grid(int* blocks);
 int general_slots_for(int n_sites);
 

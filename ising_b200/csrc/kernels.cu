@@ -532,6 +532,104 @@ int launch_octant_engine(const GeneralLaunch& a, const OctEngineLaunch& e, cudaS
     return ISING_OK;
 }
 
+// ---- sublattice classes of layout 3 (BCC without J') ------------------------------------
+// A thread owns the sites z = j, j + 1 (j even) of one row (x, y) of sublattice `sub` and
+// loops over rows.  Their 8 first-shell neighbours lie in the 4 rows (x + bx + a, y + by + b),
+// a, b in {0, 1}, of the other sublattice, at z + bz + c, c in {0, 1}: per row one aligned
+// pair (z = j, j + 1) and one edge value (j - 1 for bz = -1, j + 2 for bz = 0), so the two
+// sites share their loads -- 6 component loads per row, 27 per pair of sites, with no
+// per-neighbour index arithmetic.  The local field sums the bonds in (a, b, c) order with the
+// stencil's expression, and each site is then updated by site_update (Philox keys of the
+// reference atom index).
+constexpr int kBipBlocksPerSM = 6;
+int bip_slots_per_class() { return 148 * kBipBlocksPerSM; }
+
+template <int MOVE>
+__global__ void __launch_bounds__(kGenThreads) k_bip_sweep(GeneralLaunch a, BipClass bc, int sub, uint32_t rb,
+                                                            FastDiv div_ny) {
+    const int rl = blockIdx.y;
+    const int rep = a.rep_first + rl;
+    const int64_t N = a.natoms;
+    float* __restrict__ sx = a.spins + (int64_t)rl * 3 * N;
+    float* __restrict__ sy = sx + N;
+    float* __restrict__ sz = sy + N;
+    const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
+    const float beta = (float)a.beta_rep[rep];
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const uint32_t lanes = (uint32_t)nz >> 1;
+    const uint32_t tx = threadIdx.x % lanes, ty = threadIdx.x / lanes;
+    const int j = 2 * (int)tx;
+    const int oth = 1 - sub;
+    const uint32_t rows = (uint32_t)nx * (uint32_t)ny;
+    const uint32_t step = gridDim.x * rb;
+    const int jm = j == 0 ? nz - 1 : j - 1, jp = j + 2 == nz ? 0 : j + 2;
+    const int je = bc.base[2] < 0 ? jm : jp;
+    float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
+#pragma unroll 1
+    for (uint32_t row = ty < rb ? blockIdx.x * rb + ty : rows; row < rows; row += step) {
+        const int ix = (int)fdiv(row, div_ny), iy = (int)row - ix * ny;
+        f3 h0 = {0.f, 0.f, 0.f}, h1 = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int aa = 0; aa < 2; ++aa) {
+            int jx = ix + bc.base[0] + aa;
+            jx += jx < 0 ? nx : 0; jx -= jx >= nx ? nx : 0;
+#pragma unroll
+            for (int bb = 0; bb < 2; ++bb) {
+                int jy = iy + bc.base[1] + bb;
+                jy += jy < 0 ? ny : 0; jy -= jy >= ny ? ny : 0;
+                const int64_t rbase = (((int64_t)oth * nx + jx) * ny + jy) * nz;
+                const float2 px = *reinterpret_cast<const float2*>(sx + rbase + j);
+                const float2 py = *reinterpret_cast<const float2*>(sy + rbase + j);
+                const float2 pz = *reinterpret_cast<const float2*>(sz + rbase + j);
+                const f3 e = {sx[rbase + je], sy[rbase + je], sz[rbase + je]};
+                const f3 lo = {px.x, py.x, pz.x}, hi = {px.y, py.y, pz.y};
+                // neighbours c = 0, 1 of site j (n0*) and of site j + 1 (n1*)
+                const f3 n00 = bc.base[2] < 0 ? e : lo, n01 = bc.base[2] < 0 ? lo : hi;
+                const f3 n10 = bc.base[2] < 0 ? lo : hi, n11 = bc.base[2] < 0 ? hi : e;
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) {
+                    const int q = aa * 4 + bb * 2 + cc;
+                    const f3 D = mk(bc.D[q][0], bc.D[q][1], bc.D[q][2]);
+                    const float w = bc.w[q];
+                    const f3 s0 = cc ? n01 : n00, s1 = cc ? n11 : n10;
+                    const f3 c0 = cross(s0, D), c1 = cross(s1, D);
+                    h0.x += fmaf(w, s0.x, c0.x); h0.y += fmaf(w, s0.y, c0.y); h0.z += fmaf(w, s0.z, c0.z);
+                    h1.x += fmaf(w, s1.x, c1.x); h1.y += fmaf(w, s1.y, c1.y); h1.z += fmaf(w, s1.z, c1.z);
+                }
+            }
+        }
+        const int64_t own = (((int64_t)sub * nx + ix) * ny + iy) * nz + j;
+        const int64_t at = (((int64_t)ix * ny + iy) * nz + j) * 2 + sub;
+        site_update<MOVE>(a, h0, own, at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+        site_update<MOVE>(a, h1, own + 1, at + 2, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+    }
+    if (a.partials) {
+        __shared__ double tot[4];
+        block_sum4_fd(de, dmx, dmy, dmz, tot);
+        if (threadIdx.x == 0) {
+            double* p = a.partials + ((int64_t)rep * a.slots_per_rep + a.slot_base + blockIdx.x) * 4;
+            p[0] += tot[0]; p[1] += tot[1]; p[2] += tot[2]; p[3] += tot[3];
+        }
+    }
+}
+
+int launch_bip_sweep(const GeneralLaunch& a, const BipClass& c, int sub, cudaStream_t s) {
+    if (a.n_rep <= 0) return ISING_OK;
+    if (a.nsub != 2 || sub < 0 || sub > 1 || a.nz % 2 || a.nz / 2 > kGenThreads || a.layout.cb != 3)
+        return fail(ISING_ERR_ARG, "sublattice-class sweep needs layout 3 and an even nz <= 512");
+    const uint32_t lanes = (uint32_t)(a.nz / 2), rb = std::max(1u, (uint32_t)kGenThreads / lanes);
+    const uint32_t rows = (uint32_t)(a.nx * a.ny);
+    int zb = (bip_slots_per_class() + a.n_rep - 1) / a.n_rep;
+    zb = std::min<int>(zb, (int)((rows + rb - 1) / rb));
+    zb = std::max(1, std::min(zb, bip_slots_per_class()));
+    dim3 g(zb, a.n_rep), b(kGenThreads);
+    const FastDiv dny = make_div((uint32_t)a.ny);
+    if (a.move == 0) k_bip_sweep<0><<<g, b, 0, s>>>(a, c, sub, rb, dny);
+    else k_bip_sweep<1><<<g, b, 0, s>>>(a, c, sub, rb, dny);
+    ISG_CUDA(cudaGetLastError());
+    return ISING_OK;
+}
+
 int octant_slots_for(int64_t n_sites, bool fast) {
     const int64_t per = (int64_t)kGenThreads * (fast ? 1 : kGenSitesPerThread);
     return (int)((n_sites + per - 1) / per);

@@ -330,6 +330,35 @@ int greedy_colouring(const Lattice& L, bool use_shell2, std::vector<int>* colour
     return ISING_OK;
 }
 
+// Sublattice-plane order (layout 3): two sublattices whose first shell joins each site to
+// exactly the 8 sites of the other sublattice in the cells base + {0,1}^3 (the reference's BCC
+// cell: base (-1,-1,-1) for the corner atom, (0,0,0) for the body centre).  Each sublattice
+// is then a colour class of the first shell.  base[s][axis] receives the offsets.
+bool bipartite_pair(const Lattice& L, int base[2][3]) {
+    if (L.nsub != 2) return false;
+    for (int s = 0; s < 2; ++s) {
+        const auto& sh = L.shell[0][s];
+        if (sh.size() != 8) return false;
+        int lo[3] = {1 << 20, 1 << 20, 1 << 20};
+        for (const auto& q : sh) {
+            if (q.sub != 1 - s) return false;
+            lo[0] = std::min(lo[0], q.dx); lo[1] = std::min(lo[1], q.dy); lo[2] = std::min(lo[2], q.dz);
+        }
+        int seen = 0;
+        for (const auto& q : sh) {
+            const int a = q.dx - lo[0], b = q.dy - lo[1], c = q.dz - lo[2];
+            if (a < 0 || a > 1 || b < 0 || b > 1 || c < 0 || c > 1) return false;
+            seen |= 1 << (a * 4 + b * 2 + c);
+        }
+        if (seen != 0xff) return false;
+        for (int k = 0; k < 3; ++k) {
+            if (lo[k] < -1 || lo[k] > 0) return false;
+            base[s][k] = lo[k];
+        }
+    }
+    return true;
+}
+
 // Octant colouring of a general crystal: class (cell octant (x&1, y&1, z&1), sublattice
 // group).  Valid when every extent is even (periodic wraps keep parities) and no bond of
 // shells 1-2 joins two sites of one sublattice at an all-even non-zero cell offset; two

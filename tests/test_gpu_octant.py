@@ -1,9 +1,11 @@
-"""The octant storage order and colour classes of general crystals (BCC and hyper-kagome meshes
-with even extents, the reference's own lattices: src/PT.f90:145, src/ISING.f90:105) against
-the FP64 oracle: spins round-trip through the layout, per-site and total energies and winding
-numbers equal the oracle's, and sweeps replay the oracle's colour passes (same Philox keys,
-the product's colour classes) decision for decision, with J' on (BCC's shell 2 holds each
-site itself, which the octant classes accept) and off, both moves, over several sweeps."""
+"""The storage orders and colour classes of the reference's own lattices (src/PT.f90:145,
+src/ISING.f90:105) against the FP64 oracle: BCC in sublattice planes (layout 3; without J'
+the two sublattices are the classes and run on the sublattice-class kernel, with J' a greedy
+colouring runs on the stencil kernel), hyper-kagome with even extents in octant order.  Spins
+round-trip through the layout, per-site and total energies and winding numbers equal the
+oracle's, and sweeps replay the oracle's colour passes (same Philox keys, the product's colour
+classes) decision for decision, with J' on (BCC's shell 2 holds each site itself, which the
+classes accept) and off, both moves, over several sweeps."""
 import numpy as np
 import pytest
 
@@ -11,8 +13,11 @@ from test_gpu_parity import _both_params, _pair, _random_spins
 
 pytestmark = pytest.mark.gpu
 
+LAYOUT = {"BCC": "sublattice", "HK": "octant"}
 CASES = [
     ("BCC", (6, 6, 4), dict(J=-1.0, Dz=0.4, B=0.1, bulk=True), 1, 0.2, 1.5),
+    ("BCC", (5, 6, 8), dict(J=-1.0, Dz=0.5, B=0.2, bulk=False), 1, 0.3, 1.2),
+    ("BCC", (4, 4, 6), dict(J=1.0, Dz=0.3, B=-0.2, K=0.1, bulk=False), 0, 0.0, 2.5),
     ("BCC", (4, 6, 8), dict(J=-1.0, Jp=0.2, Dz=0.3, B=0.2, K=0.05, bulk=False), 0, 0.0, 2.0),
     ("HK", (4, 4, 4), dict(J=-1.0, Dz=0.3, B=0.1, bulk=False), 1, 0.25, 1.0),
     ("HK", (4, 6, 4), dict(J=1.0, Jp=0.1, Dz=0.2, B=0.3, bulk=True), 0, 0.0, 3.0),
@@ -23,7 +28,7 @@ CASES = [
 def test_octant_layout_energies_and_winding(oracle, ib, cuda_ok, case):
     kind, dims, h, _, _, _ = CASES[case]
     om, pm = _pair(oracle, ib, kind, dims, n_replicas=2)
-    assert pm.layout == "octant"
+    assert pm.layout == LAYOUT[kind]
     s = _random_spins(om.natoms, 300 + case)
     om.set_spins(s)
     pm.set_spins(s, 1)
@@ -53,7 +58,10 @@ def test_octant_sweeps_replay_the_oracle(oracle, ib, cuda_ok, case):
     pm.set_spins(s)
     op, pp = _both_params(oracle, ib, **h)
     col, ncol = pm.colouring(pp)
-    assert ncol % 8 == 0
+    if pm.layout == "octant":
+        assert ncol % 8 == 0
+    elif "Jp" not in h:   # the two sublattices
+        assert ncol == 2 and np.array_equal(col, np.arange(om.natoms) % 2)
     seed = 0x0C7A + case
     key = oracle.SweepKey(seed=seed, ensemble=0, replica=0, move=move, r=r, philox_rounds=10)
     n_sweeps = 3
@@ -72,6 +80,7 @@ def test_octant_pt_accumulators_track_recomputed_energies(oracle, ib, cuda_ok):
     pm.init_uniform(5)
     op, pp = _both_params(oracle, ib, J=-1.0, Dz=0.5, B=0.2, bulk=True)
     pt = ib.ParallelTempering(pm, 1.0 / ib.temperature_ladder(0.2, 2.0, 4), pp, seed=3, move=ib._lib.MOVE_BALL)
+    assert pt.schedule(5)[2] == 5          # the sublattice-class kernel
     pt.run(5, 6)
     e_run, m_run = pt.energies()
     pt.resync()
@@ -83,7 +92,7 @@ def test_octant_pt_accumulators_track_recomputed_energies(oracle, ib, cuda_ok):
         assert abs(e_new[r] - om.canonical_energy(op)) < 1e-6 * pm.numAtoms
 
 
-@pytest.mark.parametrize("kind,dims,shell2", [("BCC", (8, 6, 4), False), ("BCC", (6, 4, 8), True),
+@pytest.mark.parametrize("kind,dims,shell2", [("HK", (6, 4, 4), False), ("HK", (4, 4, 6), True),
                                               ("HK", (4, 6, 4), False), ("HK", (8, 4, 6), True)])
 @pytest.mark.parametrize("move", [0, 1])
 def test_octant_engine_equals_one_launch_per_class(oracle, ib, cuda_ok, kind, dims, shell2, move):
@@ -122,7 +131,7 @@ def test_octant_engine_timeout_and_recovery(oracle, ib, cuda_ok):
     for a count nothing reaches) ends the round with ISING_ERR_TIMEOUT after its bound; the
     context stays usable, a resync restores the running energies, and later rounds run
     normally (unit spins, accumulators equal to recomputed energies)."""
-    om, pm = _pair(oracle, ib, "BCC", (8, 6, 4), n_replicas=4)
+    om, pm = _pair(oracle, ib, "HK", (4, 6, 4), n_replicas=4)
     pm.init_uniform(9, 0)
     op, pp = _both_params(oracle, ib, J=-1.0, Dz=0.4, B=0.1, bulk=False)
     pt = ib.ParallelTempering(pm, 1.0 / ib.temperature_ladder(0.3, 2.0, 4), pp, seed=5, move=1, r=0.3,
@@ -155,7 +164,7 @@ def test_octant_engine_option_errors(oracle, ib, cuda_ok):
     with pytest.raises(ib.IsingError):
         pt.inject_stall(100)
     pt.close()
-    om, pm = _pair(oracle, ib, "BCC", (4, 4, 4), n_replicas=2)
+    om, pm = _pair(oracle, ib, "HK", (4, 4, 4), n_replicas=2)
     op, bp = _both_params(oracle, ib, J=-1.0, Dz=0.3, B=0.1)
     pt = ib.ParallelTempering(pm, np.array([1.0, 0.5]), bp, seed=1, sweep_kernel=3)
     for bad in (0, 60001):

@@ -79,17 +79,20 @@ def test_non_orthogonal_cell_sets(oracle, ib):
 
 def test_colouring_is_independent(oracle, ib):
     """Every colour class is an independent set of the active shells' bonds (a bond of a site
-    to itself, which the reference's shell search gives BCC cells in shell 2, excepted).  Even
-    BCC and hyper-kagome meshes take the octant classes: class = octant * groups + group with
-    octant = (x&1, y&1, z&1) of the cell; odd meshes a greedy colouring."""
+    to itself, which the reference's shell search gives BCC cells in shell 2, excepted).  BCC
+    meshes of at least 4 cells per axis take sublattice planes, whose classes without J' are
+    the two sublattices; even hyper-kagome meshes the octant classes: class = octant * groups
+    + group with octant = (x&1, y&1, z&1) of the cell; other meshes a greedy colouring."""
     cases = (("SC", (6, 6, 6)), ("SC", (5, 5, 5)), ("BCC", (4, 4, 4)), ("BCC", (6, 4, 8)), ("BCC", (3, 4, 3)),
-             ("HK", (4, 4, 4)), ("HK", (4, 6, 4)), ("HK", (3, 3, 3)))
+             ("BCC", (5, 6, 7)), ("HK", (4, 4, 4)), ("HK", (4, 6, 4)), ("HK", (3, 3, 3)))
     for kind, dims in cases:
         frac, (a, b, c, ab, bc, ca) = _cell(oracle, kind)
         pm = ib.ChainMesh(*dims, frac, a, b, c, ab, bc, ca, device=-1)
         even = all(d % 2 == 0 for d in dims)
-        assert pm.layout == ("checkerboard" if kind == "SC" and dims[2] % 4 == 0 and even
-                             else "octant" if kind != "SC" and even else "reference"), (kind, dims, pm.layout)
+        want = ("checkerboard" if kind == "SC" and dims[2] % 4 == 0 and even
+                else "sublattice" if kind == "BCC" and min(dims) >= 4
+                else "octant" if kind == "HK" and even else "reference")
+        assert pm.layout == want, (kind, dims, pm.layout)
         for Jp in (0.0, 0.2):
             col, n = pm.colouring(ib.params(J=-1.0, J_prime=Jp))
             shells = (0, 1) if Jp else (0,)
@@ -100,7 +103,9 @@ def test_colouring_is_independent(oracle, ib):
                     assert np.all(col[nb] != col[atom]), (kind, dims, Jp, atom)
             if kind == "SC" and dims[0] % 4 == 0 and Jp == 0.0:
                 assert n == 2 and pm.checkerboard
-            if pm.layout == "octant":
+            if pm.layout == "sublattice" and Jp == 0.0:
+                assert n == 2 and np.array_equal(col, np.arange(pm.numAtoms) % 2)
+            elif pm.layout == "octant":
                 assert n % 8 == 0
                 nsub = len(frac)
                 for atom in range(0, pm.numAtoms, 7):
