@@ -62,7 +62,7 @@ WORKLOADS = {
 # the reference's own crystals (src/unit_cells.f90): BCC as bin/PT runs it (shell 1 only, J' = 0,
 # src/PT.f90:145,229-230) and hyper-kagome as bin/ISING does (src/ISING.f90:105), both with the
 # default interfacial DMI of calculateHeisenbergEnergy; run by the per-pass PT path on the
-# octant storage order (the persistent engine covers simple cubic)
+# sublattice planes (BCC) and octant order (hyper-kagome) (the persistent engine covers simple cubic)
 WORKLOADS["bcc"] = dict(cell="bcc", L=96, R=16, tmin=0.1, tmax=2.0, J=-1.0, D=0.5, B=0.2, K=0.0, move="ball", r=0.2,
                         k=10, dmi="interfacial",
                         desc="BCC 96^3 cells (2 atoms) x 16 PT replicas, T 0.1-2.0, J=1, interfacial D=0.5, B=0.2 z, "
