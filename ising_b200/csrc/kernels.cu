@@ -544,9 +544,11 @@ int launch_octant_engine(const GeneralLaunch& a, const OctEngineLaunch& e, cudaS
 constexpr int kBipBlocksPerSM = 6;
 int bip_slots_per_class() { return 148 * kBipBlocksPerSM; }
 
+struct BipRow { f3 lo, hi, e; };   // z-sites j, j + 1 and the edge value of one row
+
 template <int MOVE>
 __global__ void __launch_bounds__(kGenThreads) k_bip_sweep(GeneralLaunch a, BipClass bc, int sub, uint32_t rb,
-                                                            FastDiv div_ny) {
+                                                            uint32_t nseg, FastDiv div_seg) {
     const int rl = blockIdx.y;
     const int rep = a.rep_first + rl;
     const int64_t N = a.natoms;
@@ -560,48 +562,63 @@ __global__ void __launch_bounds__(kGenThreads) k_bip_sweep(GeneralLaunch a, BipC
     const uint32_t tx = threadIdx.x % lanes, ty = threadIdx.x / lanes;
     const int j = 2 * (int)tx;
     const int oth = 1 - sub;
-    const uint32_t rows = (uint32_t)nx * (uint32_t)ny;
-    const uint32_t step = gridDim.x * rb;
-    const int jm = j == 0 ? nz - 1 : j - 1, jp = j + 2 == nz ? 0 : j + 2;
-    const int je = bc.base[2] < 0 ? jm : jp;
-    float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
-#pragma unroll 1
-    for (uint32_t row = ty < rb ? blockIdx.x * rb + ty : rows; row < rows; row += step) {
-        const int ix = (int)fdiv(row, div_ny), iy = (int)row - ix * ny;
-        f3 h0 = {0.f, 0.f, 0.f}, h1 = {0.f, 0.f, 0.f};
+    const uint32_t units = (uint32_t)nx * nseg;
+    const int je = bc.base[2] < 0 ? (j == 0 ? nz - 1 : j - 1) : (j + 2 == nz ? 0 : j + 2);
+    auto load_row = [&](int jx, int jy) {
+        const int64_t rbase = (((int64_t)oth * nx + jx) * ny + jy) * nz;
+        const float2 px = *reinterpret_cast<const float2*>(sx + rbase + j);
+        const float2 py = *reinterpret_cast<const float2*>(sy + rbase + j);
+        const float2 pz = *reinterpret_cast<const float2*>(sz + rbase + j);
+        BipRow r;
+        r.lo = {px.x, py.x, pz.x};
+        r.hi = {px.y, py.y, pz.y};
+        r.e = {sx[rbase + je], sy[rbase + je], sz[rbase + je]};
+        return r;
+    };
+    // bonds (a, b, c = 0, 1) of one neighbour row to the sites j (h0) and j + 1 (h1)
+    auto add_row = [&](const BipRow& r, int q0, f3& h0, f3& h1) {
+        const f3 n00 = bc.base[2] < 0 ? r.e : r.lo, n01 = bc.base[2] < 0 ? r.lo : r.hi;
+        const f3 n10 = bc.base[2] < 0 ? r.lo : r.hi, n11 = bc.base[2] < 0 ? r.hi : r.e;
 #pragma unroll
-        for (int aa = 0; aa < 2; ++aa) {
-            int jx = ix + bc.base[0] + aa;
-            jx += jx < 0 ? nx : 0; jx -= jx >= nx ? nx : 0;
-#pragma unroll
-            for (int bb = 0; bb < 2; ++bb) {
-                int jy = iy + bc.base[1] + bb;
-                jy += jy < 0 ? ny : 0; jy -= jy >= ny ? ny : 0;
-                const int64_t rbase = (((int64_t)oth * nx + jx) * ny + jy) * nz;
-                const float2 px = *reinterpret_cast<const float2*>(sx + rbase + j);
-                const float2 py = *reinterpret_cast<const float2*>(sy + rbase + j);
-                const float2 pz = *reinterpret_cast<const float2*>(sz + rbase + j);
-                const f3 e = {sx[rbase + je], sy[rbase + je], sz[rbase + je]};
-                const f3 lo = {px.x, py.x, pz.x}, hi = {px.y, py.y, pz.y};
-                // neighbours c = 0, 1 of site j (n0*) and of site j + 1 (n1*)
-                const f3 n00 = bc.base[2] < 0 ? e : lo, n01 = bc.base[2] < 0 ? lo : hi;
-                const f3 n10 = bc.base[2] < 0 ? lo : hi, n11 = bc.base[2] < 0 ? hi : e;
-#pragma unroll
-                for (int cc = 0; cc < 2; ++cc) {
-                    const int q = aa * 4 + bb * 2 + cc;
-                    const f3 D = mk(bc.D[q][0], bc.D[q][1], bc.D[q][2]);
-                    const float w = bc.w[q];
-                    const f3 s0 = cc ? n01 : n00, s1 = cc ? n11 : n10;
-                    const f3 c0 = cross(s0, D), c1 = cross(s1, D);
-                    h0.x += fmaf(w, s0.x, c0.x); h0.y += fmaf(w, s0.y, c0.y); h0.z += fmaf(w, s0.z, c0.z);
-                    h1.x += fmaf(w, s1.x, c1.x); h1.y += fmaf(w, s1.y, c1.y); h1.z += fmaf(w, s1.z, c1.z);
-                }
-            }
+        for (int cc = 0; cc < 2; ++cc) {
+            const int q = q0 + cc;
+            const f3 D = mk(bc.D[q][0], bc.D[q][1], bc.D[q][2]);
+            const float w = bc.w[q];
+            const f3 s0 = cc ? n01 : n00, s1 = cc ? n11 : n10;
+            const f3 c0 = cross(s0, D), c1 = cross(s1, D);
+            h0.x += fmaf(w, s0.x, c0.x); h0.y += fmaf(w, s0.y, c0.y); h0.z += fmaf(w, s0.z, c0.z);
+            h1.x += fmaf(w, s1.x, c1.x); h1.y += fmaf(w, s1.y, c1.y); h1.z += fmaf(w, s1.z, c1.z);
         }
-        const int64_t own = (((int64_t)sub * nx + ix) * ny + iy) * nz + j;
-        const int64_t at = (((int64_t)ix * ny + iy) * nz + j) * 2 + sub;
-        site_update<MOVE>(a, h0, own, at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
-        site_update<MOVE>(a, h1, own + 1, at + 2, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+    };
+    float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
+    // a thread marches the column (x, j) of one y-segment; the row of the other sublattice at
+    // y + by + 1 read for step y is the row at (y + 1) + by of the next step
+#pragma unroll 1
+    for (uint32_t u = ty < rb ? blockIdx.x * rb + ty : units; u < units; u += gridDim.x * rb) {
+        const uint32_t ix = fdiv(u, div_seg), sg = u - ix * nseg;
+        const int ya = (int)(sg * (uint32_t)ny / nseg), yb = (int)((sg + 1u) * (uint32_t)ny / nseg);
+        int jx0 = (int)ix + bc.base[0], jx1 = jx0 + 1;
+        jx0 += jx0 < 0 ? nx : 0; jx0 -= jx0 >= nx ? nx : 0;
+        jx1 += jx1 < 0 ? nx : 0; jx1 -= jx1 >= nx ? nx : 0;
+        int jy = ya + bc.base[1];
+        jy += jy < 0 ? ny : 0; jy -= jy >= ny ? ny : 0;
+        BipRow p0 = load_row(jx0, jy), p1 = load_row(jx1, jy);
+#pragma unroll 1
+        for (int iy = ya; iy < yb; ++iy) {
+            jy = jy + 1 == ny ? 0 : jy + 1;
+            const BipRow c0 = load_row(jx0, jy), c1 = load_row(jx1, jy);
+            f3 h0 = {0.f, 0.f, 0.f}, h1 = {0.f, 0.f, 0.f};
+            add_row(p0, 0, h0, h1);   // (a, b) = (0, 0)
+            add_row(c0, 2, h0, h1);   // (0, 1)
+            add_row(p1, 4, h0, h1);   // (1, 0)
+            add_row(c1, 6, h0, h1);   // (1, 1)
+            p0 = c0;
+            p1 = c1;
+            const int64_t own = (((int64_t)sub * nx + ix) * ny + iy) * nz + j;
+            const int64_t at = (((int64_t)ix * ny + iy) * nz + j) * 2 + sub;
+            site_update<MOVE>(a, h0, own, at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+            site_update<MOVE>(a, h1, own + 1, at + 2, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+        }
     }
     if (a.partials) {
         __shared__ double tot[4];
@@ -618,14 +635,18 @@ int launch_bip_sweep(const GeneralLaunch& a, const BipClass& c, int sub, cudaStr
     if (a.nsub != 2 || sub < 0 || sub > 1 || a.nz % 2 || a.nz / 2 > kGenThreads || a.layout.cb != 3)
         return fail(ISING_ERR_ARG, "sublattice-class sweep needs layout 3 and an even nz <= 512");
     const uint32_t lanes = (uint32_t)(a.nz / 2), rb = std::max(1u, (uint32_t)kGenThreads / lanes);
-    const uint32_t rows = (uint32_t)(a.nx * a.ny);
-    int zb = (bip_slots_per_class() + a.n_rep - 1) / a.n_rep;
-    zb = std::min<int>(zb, (int)((rows + rb - 1) / rb));
+    // y-segments per x-column: enough column units for about two blocks of work per resident
+    // block slot, every segment at least two rows long
+    const int64_t want_units = 2LL * bip_slots_per_class() * rb;
+    int64_t nseg = (want_units + (int64_t)a.nx * a.n_rep - 1) / ((int64_t)a.nx * a.n_rep);
+    nseg = std::max<int64_t>(1, std::min<int64_t>(nseg, a.ny / 2));
+    const uint32_t units = (uint32_t)(a.nx * nseg);
+    int zb = (int)((units + rb - 1) / rb);
     zb = std::max(1, std::min(zb, bip_slots_per_class()));
     dim3 g(zb, a.n_rep), b(kGenThreads);
-    const FastDiv dny = make_div((uint32_t)a.ny);
-    if (a.move == 0) k_bip_sweep<0><<<g, b, 0, s>>>(a, c, sub, rb, dny);
-    else k_bip_sweep<1><<<g, b, 0, s>>>(a, c, sub, rb, dny);
+    const FastDiv dseg = make_div((uint32_t)nseg);
+    if (a.move == 0) k_bip_sweep<0><<<g, b, 0, s>>>(a, c, sub, rb, (uint32_t)nseg, dseg);
+    else k_bip_sweep<1><<<g, b, 0, s>>>(a, c, sub, rb, (uint32_t)nseg, dseg);
     ISG_CUDA(cudaGetLastError());
     return ISING_OK;
 }
