@@ -575,19 +575,27 @@ __global__ void __launch_bounds__(kGenThreads) k_bip_sweep(GeneralLaunch a, BipC
         r.e = {sx[rbase + je], sy[rbase + je], sz[rbase + je]};
         return r;
     };
-    // bonds (a, b, c = 0, 1) of one neighbour row to the sites j (h0) and j + 1 (h1)
-    auto add_row = [&](const BipRow& r, int q0, f3& h0, f3& h1) {
+    // bonds (a, b, c = 0, 1) of one neighbour row to the sites j and j + 1, both sites in the
+    // lanes of packed FP32x2 fields (hx, hy, hz): h += w S + S x D per bond
+    auto add_row = [&](const BipRow& r, int q0, float2& hx, float2& hy, float2& hz) {
         const f3 n00 = bc.base[2] < 0 ? r.e : r.lo, n01 = bc.base[2] < 0 ? r.lo : r.hi;
         const f3 n10 = bc.base[2] < 0 ? r.lo : r.hi, n11 = bc.base[2] < 0 ? r.hi : r.e;
 #pragma unroll
         for (int cc = 0; cc < 2; ++cc) {
             const int q = q0 + cc;
-            const f3 D = mk(bc.D[q][0], bc.D[q][1], bc.D[q][2]);
-            const float w = bc.w[q];
             const f3 s0 = cc ? n01 : n00, s1 = cc ? n11 : n10;
-            const f3 c0 = cross(s0, D), c1 = cross(s1, D);
-            h0.x += fmaf(w, s0.x, c0.x); h0.y += fmaf(w, s0.y, c0.y); h0.z += fmaf(w, s0.z, c0.z);
-            h1.x += fmaf(w, s1.x, c1.x); h1.y += fmaf(w, s1.y, c1.y); h1.z += fmaf(w, s1.z, c1.z);
+            const float2 sx_ = make_float2(s0.x, s1.x), sy_ = make_float2(s0.y, s1.y), sz_ = make_float2(s0.z, s1.z);
+            const float2 w = make_float2(bc.w[q], bc.w[q]);
+            const float2 Dx = make_float2(bc.D[q][0], bc.D[q][0]), Dy = make_float2(bc.D[q][1], bc.D[q][1]);
+            const float2 Dz = make_float2(bc.D[q][2], bc.D[q][2]);
+            const float2 nDx = make_float2(-bc.D[q][0], -bc.D[q][0]), nDy = make_float2(-bc.D[q][1], -bc.D[q][1]);
+            const float2 nDz = make_float2(-bc.D[q][2], -bc.D[q][2]);
+            const float2 cx = __ffma2_rn(sy_, Dz, __fmul2_rn(sz_, nDy));
+            const float2 cy = __ffma2_rn(sz_, Dx, __fmul2_rn(sx_, nDz));
+            const float2 cz = __ffma2_rn(sx_, Dy, __fmul2_rn(sy_, nDx));
+            hx = __fadd2_rn(hx, __ffma2_rn(w, sx_, cx));
+            hy = __fadd2_rn(hy, __ffma2_rn(w, sy_, cy));
+            hz = __fadd2_rn(hz, __ffma2_rn(w, sz_, cz));
         }
     };
     float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
@@ -607,11 +615,12 @@ __global__ void __launch_bounds__(kGenThreads) k_bip_sweep(GeneralLaunch a, BipC
         for (int iy = ya; iy < yb; ++iy) {
             jy = jy + 1 == ny ? 0 : jy + 1;
             const BipRow c0 = load_row(jx0, jy), c1 = load_row(jx1, jy);
-            f3 h0 = {0.f, 0.f, 0.f}, h1 = {0.f, 0.f, 0.f};
-            add_row(p0, 0, h0, h1);   // (a, b) = (0, 0)
-            add_row(c0, 2, h0, h1);   // (0, 1)
-            add_row(p1, 4, h0, h1);   // (1, 0)
-            add_row(c1, 6, h0, h1);   // (1, 1)
+            float2 hx = make_float2(0.f, 0.f), hy = hx, hz = hx;
+            add_row(p0, 0, hx, hy, hz);   // (a, b) = (0, 0)
+            add_row(c0, 2, hx, hy, hz);   // (0, 1)
+            add_row(p1, 4, hx, hy, hz);   // (1, 0)
+            add_row(c1, 6, hx, hy, hz);   // (1, 1)
+            const f3 h0 = {hx.x, hy.x, hz.x}, h1 = {hx.y, hy.y, hz.y};
             p0 = c0;
             p1 = c1;
             const int64_t own = (((int64_t)sub * nx + ix) * ny + iy) * nz + j;
