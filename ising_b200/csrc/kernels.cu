@@ -210,6 +210,7 @@ struct __align__(16) OctSlot {
 struct OctDims {
     FastDiv q8, hz, hy, hyz;
     int hx, hyi, hzi;
+    FastDiv q8h;             // by q8 / 2 (site pairs of k_octant_pair)
 };
 
 // block sums of the four running partials: FP32 within a warp (a warp's few sites), FP64
@@ -309,6 +310,114 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
         }
         site_update<MOVE>(a, h, (int64_t)(class_base + t), (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
                           dmz);
+    }
+    if (a.partials) {
+        __shared__ double tot[4];
+        block_sum4_fd(de, dmx, dmy, dmz, tot);
+        if (threadIdx.x == 0) {
+            double* p = a.partials + ((int64_t)rep * a.slots_per_rep + a.slot_base + blockIdx.x) * 4;
+            p[0] += tot[0]; p[1] += tot[1]; p[2] += tot[2]; p[3] += tot[3];
+        }
+    }
+}
+
+// The same class, one pair of sites per thread: packed cells Z0 and Z0 + 1 (Z0 even, nz % 4 ==
+// 0, so a pair never straddles a row) of one row.  The pair shares the row decode and, per
+// stencil slot, the x/y wrap and the row base; a slot with no packed z offset reads both
+// neighbours as one aligned pair per component.  Each site's field is summed in slot order
+// with the stencil's expression, so the update equals k_octant_fast's bit for bit.
+template <int MOVE>
+__global__ void __launch_bounds__(kGenThreads) k_octant_pair(GeneralLaunch a, OctDims od, int oct, int rank0,
+                                                              int nrank) {
+    extern __shared__ __align__(16) unsigned char oct_smem[];
+    const int mc = a.oct_maxcnt;
+    OctSlot* tab = reinterpret_cast<OctSlot*>(oct_smem);
+    int* s_cnt = reinterpret_cast<int*>(tab + nrank * mc);
+    int* s_sub = s_cnt + nrank;
+    __shared__ int s_srank[kMaxSub], s_sofr[kMaxSub];
+    const Layout& L = a.layout;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < kMaxSub; ++k) { s_srank[k] = L.srank[k]; s_sofr[k] = L.sofr[k]; }
+    }
+    __syncthreads();
+    const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
+    const int q8 = (int)L.q8;
+    for (int e = threadIdx.x; e < nrank * mc; e += blockDim.x) {
+        const int lr = e / mc, q = e - lr * mc;
+        const int sub = s_sofr[rank0 + lr];
+        OctSlot o{};
+        if (q < a.st.count[sub]) {
+            const Slot sl = a.st.slots[sub * kMaxSlots + q];
+            const int tx = ox + sl.dx, ty = oy + sl.dy, tz = oz + sl.dz;
+            const int o2 = ((tx & 1) << 2) | ((ty & 1) << 1) | (tz & 1);
+            o.plane = (o2 * a.nsub + s_srank[sl.sub]) * q8;
+            o.ex = (int8_t)(tx >> 1); o.ey = (int8_t)(ty >> 1); o.ez = (int8_t)(tz >> 1);
+            o.w = sl.w; o.Dx = sl.Dx; o.Dy = sl.Dy; o.Dz = sl.Dz;
+        }
+        tab[e] = o;
+    }
+    for (int lr = threadIdx.x; lr < nrank; lr += blockDim.x) {
+        s_sub[lr] = s_sofr[rank0 + lr];
+        s_cnt[lr] = a.st.count[s_sub[lr]];
+    }
+    __syncthreads();
+    const int rl = blockIdx.y;
+    const int rep = a.rep_first + rl;
+    const int64_t N = a.natoms;
+    float* __restrict__ sx = a.spins + (int64_t)rl * 3 * N;
+    float* __restrict__ sy = sx + N;
+    float* __restrict__ sz = sy + N;
+    const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
+    const float beta = (float)a.beta_rep[rep];
+    const int hx = od.hx, hy = od.hyi, hz = od.hzi;
+    const uint32_t half8 = (uint32_t)q8 >> 1;
+    const uint32_t npair = half8 * (uint32_t)nrank;
+    const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
+    float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
+    const uint32_t tp = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tp < npair) {
+        const uint32_t lr = fdiv(tp, od.q8h);
+        const uint32_t pc0 = 2u * (tp - lr * half8);
+        const uint32_t r = fdiv(pc0, od.hz);
+        const int Z0 = (int)(pc0 - r * (uint32_t)hz);
+        const uint32_t Xu = fdiv(r, od.hy);
+        const int Y = (int)(r - Xu * (uint32_t)hy), X = (int)Xu;
+        const int sub = s_sub[lr];
+        const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z0 + oz;
+        const uint32_t at0 = ((uint32_t)(ix * a.ny + iy) * (uint32_t)a.nz + (uint32_t)iz) * (uint32_t)a.nsub + sub;
+        const uint32_t at1 = at0 + 2u * (uint32_t)a.nsub;   // cell z + 2
+        const OctSlot* ts = tab + lr * mc;
+        f3 h0 = {0.f, 0.f, 0.f}, h1 = {0.f, 0.f, 0.f};
+        const int cn = s_cnt[lr];
+        for (int q = 0; q < cn; ++q) {
+            const OctSlot o = ts[q];
+            int jx = X + o.ex, jy = Y + o.ey;
+            jx += jx < 0 ? hx : 0; jx -= jx >= hx ? hx : 0;
+            jy += jy < 0 ? hy : 0; jy -= jy >= hy ? hy : 0;
+            const uint32_t rb = (uint32_t)o.plane + (uint32_t)((jx * hy + jy) * hz);
+            f3 s0, s1;
+            if (o.ez == 0) {   // both neighbours at Z0, Z0 + 1: one aligned pair per component
+                const float2 px = *reinterpret_cast<const float2*>(sx + rb + Z0);
+                const float2 py = *reinterpret_cast<const float2*>(sy + rb + Z0);
+                const float2 pz = *reinterpret_cast<const float2*>(sz + rb + Z0);
+                s0 = {px.x, py.x, pz.x};
+                s1 = {px.y, py.y, pz.y};
+            } else {
+                int jz0 = Z0 + o.ez, jz1 = Z0 + 1 + o.ez;
+                jz0 += jz0 < 0 ? hz : 0; jz0 -= jz0 >= hz ? hz : 0;
+                jz1 += jz1 < 0 ? hz : 0; jz1 -= jz1 >= hz ? hz : 0;
+                s0 = {sx[rb + jz0], sy[rb + jz0], sz[rb + jz0]};
+                s1 = {sx[rb + jz1], sy[rb + jz1], sz[rb + jz1]};
+            }
+            const f3 D = mk(o.Dx, o.Dy, o.Dz);
+            const f3 c0 = cross(s0, D), c1 = cross(s1, D);
+            h0.x += fmaf(o.w, s0.x, c0.x); h0.y += fmaf(o.w, s0.y, c0.y); h0.z += fmaf(o.w, s0.z, c0.z);
+            h1.x += fmaf(o.w, s1.x, c1.x); h1.y += fmaf(o.w, s1.y, c1.y); h1.z += fmaf(o.w, s1.z, c1.z);
+        }
+        const uint32_t si0 = class_base + lr * (uint32_t)q8 + pc0;
+        site_update<MOVE>(a, h0, (int64_t)si0, (int64_t)at0, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+        site_update<MOVE>(a, h1, (int64_t)si0 + 1, (int64_t)at1, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
     }
     if (a.partials) {
         __shared__ double tot[4];
@@ -688,6 +797,14 @@ int launch_octant_colour(const GeneralLaunch& a, int oct, int rank0, int nrank, 
         od.hz = make_div((uint32_t)od.hzi);
         od.hy = make_div((uint32_t)od.hyi);
         const size_t sm = (size_t)nrank * a.oct_maxcnt * sizeof(OctSlot) + 2 * (size_t)nrank * sizeof(int);
+        if (od.hzi % 2 == 0) {   // site pairs along packed z
+            od.q8h = make_div((uint32_t)(a.layout.q8 / 2));
+            g.x = (unsigned)((n / 2 + kGenThreads - 1) / kGenThreads);   // <= octant_slots_for(n, true)
+            if (a.move == 0) k_octant_pair<0><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
+            else k_octant_pair<1><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
+            ISG_CUDA(cudaGetLastError());
+            return ISING_OK;
+        }
 #define ISG_OF(S)                                                                      \
     if (a.move == 0) k_octant_fast<0, S><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);   \
     else k_octant_fast<1, S><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
