@@ -533,7 +533,8 @@ def run_gpu(args, w):
         sched_info = {"l2_group_replicas": group, "colour_pass_launches_per_round": per_round,
                       "kernel": {0: "k_octant_colour" if m.layout == "octant" else "k_general_colour",
                                  1: "k_cb_sweep", 2: "k_cb_tma", 3: "k_octant_fast",
-                                 4: "k_octant_engine", 5: "k_bip_sweep"}[kern_id], "layout": m.layout}
+                                 4: "k_octant_engine", 5: "k_bip_sweep", 6: "k_octant_pair"}[kern_id],
+                      "layout": m.layout}
         kernel_name = sched_info["kernel"]
         launches_timed = args.steps * (per_round + 3)   # colour passes + fold + exchange + advance
         closers = [pt]

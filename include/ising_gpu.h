@@ -316,7 +316,8 @@ int ising_pt_inject_stall(ising_pt* pt, int wait_ms);
  * sweeps_per_swap sweeps, and which colour-pass kernel runs (1 register, 2 TMA-staged,
  * 0 the stencil kernel of the greedy or octant colouring, 3 the octant kernel with the
  * stencil resolved per class, 4 the persistent octant engine, 5 the sublattice classes of
- * BCC meshes).  No reference counterpart. */
+ * BCC meshes, 6 the octant kernel with a pair of sites per thread).  No reference
+ * counterpart. */
 int ising_pt_schedule(const ising_pt* pt, int sweeps_per_swap, int* l2_group, int* pass_launches,
                       int* kernel);
 /* temperature slot -> replica (TemperatureMeshArray(i, :), src/PT.f90:58) */

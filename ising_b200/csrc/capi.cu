@@ -1390,9 +1390,10 @@ extern "C" int ising_pt_schedule(const ising_pt* pt, int k, int* group, int* lau
     if (group) *group = grp;
     if (launches) *launches = L;
     // 0 k_general_colour / k_octant_colour, 1 k_cb_sweep, 2 k_cb_tma, 3 k_octant_fast,
-    // 4 k_octant_engine, 5 k_bip_sweep
+    // 4 k_octant_engine, 5 k_bip_sweep, 6 k_octant_pair
+    const int fast = pt->mesh->lat.nz % 4 == 0 ? 6 : 3;
     if (kernel)
-        *kernel = P.sc ? (P.tma ? 2 : 1) : P.bip ? 5 : (oct ? (P.oct_engine ? 4 : (P.oct_maxcnt > 0 ? 3 : 0)) : 0);
+        *kernel = P.sc ? (P.tma ? 2 : 1) : P.bip ? 5 : (oct ? (P.oct_engine ? 4 : (P.oct_maxcnt > 0 ? fast : 0)) : 0);
     return ISING_OK;
 }
 
