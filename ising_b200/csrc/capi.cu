@@ -175,24 +175,27 @@ int sc_dmi(const ising_mesh* m, const ising_params& p, HamDev* h, int* kind) {
     return ISING_OK;
 }
 
-// Colour classes of a mesh that is not on the checkerboard path: the octant classes
-// (octant o, sublattice group g) as class o * groups + g for octant-layout meshes, else a
-// greedy colouring of the active shells' bonds.
+// Colour classes of a mesh that is not on the checkerboard path.  Octant-layout meshes: the
+// octant classes (octant o, sublattice group g) as class o * groups + g, or, without J' where
+// the mesh has shell-1 classes, those classes (every octant of each); else a greedy colouring
+// of the active shells' bonds.
 int host_colouring(ising_mesh* m, bool shell2, Colouring& c) {
     if (!c.host_colour.empty()) return ISING_OK;
     const Lattice& L = m->lat;
     if (m->layout.cb == 2) {
-        const int ng = (int)m->oct_rank0.size() - 1;
+        const bool by_class = !shell2 && !m->oct_class0.empty();
+        const std::vector<int>& r0 = by_class ? m->oct_class0 : m->oct_rank0;
+        const int ng = (int)r0.size() - 1;
         c.host_colour.resize(L.natoms);
         for (int64_t at = 0; at < L.natoms; ++at) {
             int ix, iy, iz, sb;
             L.cell_of(at, &ix, &iy, &iz, &sb);
             const int rk = m->layout.srank[sb];
             int g = 0;
-            while (rk >= m->oct_rank0[g + 1]) ++g;
-            c.host_colour[at] = (((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1)) * ng + g;
+            while (rk >= r0[g + 1]) ++g;
+            c.host_colour[at] = by_class ? g : (((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1)) * ng + g;
         }
-        c.ncol = 8 * ng;
+        c.ncol = by_class ? ng : 8 * ng;
         return ISING_OK;
     }
     if (m->layout.cb == 3 && !shell2) {   // the two sublattices
@@ -237,6 +240,7 @@ struct SweepPlan {
     const float* demag = nullptr;   // general path: demagnetising field of the swept replica
     int oct_maxcnt = 0;        // octant layout: k_octant_fast's table width (0: k_octant_colour)
     bool oct_engine = false;   // octant layout: every sweep of a call in one persistent launch
+    bool oct_by_class = false; // octant layout: the classes are the mesh's shell-1 classes
     int oct_reach = 1;         // its dependency reach in packed x-planes
     int oct_grid = 0;          // its persistent blocks
     bool bip = false;          // layout 3 without J': the two sublattice classes (k_bip_sweep)
@@ -329,9 +333,17 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
             if (!m->d_oct_sync)
                 ISG_TRY(dev_alloc(&m->d_oct_sync, (size_t)m->n_replicas * (size_t)(Lt.nx / 2) + 2));
         }
-        for (int k = 0; k < 8 * ng; ++k)
-            tot += octant_slots_for(m->layout.q8 * (m->oct_rank0[k % ng + 1] - m->oct_rank0[k % ng]),
-                                    plan->oct_maxcnt > 0);
+        // without J' on a mesh with shell-1 classes: one class (all 8 octants) after another
+        plan->oct_by_class = !sh2 && !m->oct_class0.empty();
+        if (plan->oct_by_class) {
+            for (size_t k = 0; k + 1 < m->oct_class0.size(); ++k)
+                tot += octant_class_slots(m->layout.q8, m->oct_class0[k + 1] - m->oct_class0[k], 8,
+                                          plan->oct_maxcnt > 0);
+        } else {
+            for (int k = 0; k < 8 * ng; ++k)
+                tot += octant_slots_for(m->layout.q8 * (m->oct_rank0[k % ng + 1] - m->oct_rank0[k % ng]),
+                                        plan->oct_maxcnt > 0);
+        }
         // every replica in each class launch: L2-sized replica groups (a group running all its
         // sweeps before the next) measured no faster on BCC 96^3 x 16 and much slower on
         // hyper-kagome, whose classes are small; large launches let a thread take several sites
@@ -426,9 +438,11 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
         e.abort = m->d_oct_sync + 1;
         e.done = m->d_oct_sync + 2;
         e.n_sweeps = n_sweeps;
-        e.ng = (int)m->oct_rank0.size() - 1;
+        const std::vector<int>& r0 = plan.oct_by_class ? m->oct_class0 : m->oct_rank0;
+        e.ng = (int)r0.size() - 1;
+        e.class_major = plan.oct_by_class ? 1 : 0;
         e.reach = plan.oct_reach;
-        for (int k = 0; k <= kMaxSub; ++k) e.rank0[k] = k <= e.ng ? m->oct_rank0[k] : m->oct_rank0[e.ng];
+        for (int k = 0; k <= kMaxSub; ++k) e.rank0[k] = k <= e.ng ? r0[k] : r0[e.ng];
         e.wait_ns = plan.oct_wait_ns;
         e.stall = plan.oct_stall;
         e.grid = plan.oct_grid;
@@ -451,10 +465,19 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
             for (int sw = 0; sw < n_sweeps; ++sw) {
                 g.sweep_offset = sw0 + (uint32_t)sw;
                 int slot = 0;
+                if (plan.oct_by_class) {
+                    for (size_t k = 0; k + 1 < m->oct_class0.size(); ++k) {
+                        const int r0 = m->oct_class0[k], nr = m->oct_class0[k + 1] - r0;
+                        g.slot_base = slot;
+                        ISG_TRY(launch_octant_colour(g, 0, 8, r0, nr, m->stream));
+                        slot += octant_class_slots(m->layout.q8, nr, 8, plan.oct_maxcnt > 0);
+                    }
+                    continue;
+                }
                 for (int k = 0; k < 8 * ng; ++k) {
                     const int gi = k % ng, r0 = m->oct_rank0[gi], nr = m->oct_rank0[gi + 1] - r0;
                     g.slot_base = slot;
-                    ISG_TRY(launch_octant_colour(g, k / ng, r0, nr, m->stream));
+                    ISG_TRY(launch_octant_colour(g, k / ng, 1, r0, nr, m->stream));
                     slot += octant_slots_for(m->layout.q8 * nr, plan.oct_maxcnt > 0);
                 }
             }
@@ -551,19 +574,21 @@ extern "C" int ising_mesh_create(const float* frac, int nsub, int nx, int ny, in
     {
         const Lattice& L = m->lat;
         m->layout = Layout{m->checkerboard && L.nz % 4 == 0 ? 1 : 0, L.nx, L.ny, L.nz, L.nsub, L.natoms / 2};
-        std::vector<int> grp;
+        std::vector<int> grp, cls;
         int ng = 0;
         // two sublattices joined only to each other (BCC): sublattice planes; other crystals:
         // octant order when the octant colouring applies (ranks grouped by sublattice group,
         // so each colour class is one contiguous range)
         if (!m->checkerboard && bipartite_pair(L, m->bip_base)) {
             m->layout.cb = 3;
-        } else if (!m->checkerboard && octant_groups(L, &grp, &ng)) {
+        } else if (!m->checkerboard && octant_groups(L, &grp, &ng, &cls)) {
             m->layout.cb = 2;
             m->layout.q8 = L.ncells / 8;
             int next = 0;
             m->oct_rank0.assign(1, 0);
+            m->oct_class0.clear();
             for (int g = 0; g < ng; ++g) {
+                if (!cls.empty() && (g == 0 || cls[g] != cls[g - 1])) m->oct_class0.push_back(next);
                 for (int sb = 0; sb < L.nsub; ++sb)
                     if (grp[sb] == g) {
                         m->layout.srank[sb] = (uint8_t)next;
@@ -572,6 +597,7 @@ extern "C" int ising_mesh_create(const float* frac, int nsub, int nx, int ny, in
                     }
                 m->oct_rank0.push_back(next);
             }
+            if (!cls.empty()) m->oct_class0.push_back(next);
         }
     }
     if (device == -1) {  // lattice tables only
@@ -1385,7 +1411,11 @@ extern "C" int ising_pt_schedule(const ising_pt* pt, int k, int* group, int* lau
     if (P.sc) L = G > 1 ? G * k + 1 : 2 * k;
     else if (P.bip) { L = 2 * k; grp = pt->n; }
     else if (oct && P.oct_engine) { L = 1; grp = pt->n; }
-    else if (oct) L = G * k * 8 * ((int)pt->mesh->oct_rank0.size() - 1);
+    else if (oct && P.oct_by_class) {
+        const std::vector<int>& c0 = pt->mesh->oct_class0;
+        for (size_t c = 0; c + 1 < c0.size(); ++c) L += octant_class_launches(c0[c + 1] - c0[c], P.oct_maxcnt, 8);
+        L *= G * k;
+    } else if (oct) L = G * k * 8 * ((int)pt->mesh->oct_rank0.size() - 1);
     else L = k * P.col->ncol;
     if (group) *group = grp;
     if (launches) *launches = L;

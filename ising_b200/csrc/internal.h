@@ -69,7 +69,10 @@ bool is_checkerboard_sc(const Lattice& L);
 // Sublattice groups of the octant colouring (class = cell octant x sublattice group) of a
 // general crystal; false when the octant colouring does not apply (odd extents, or a bond of
 // shells 1-2 between two sites of one sublattice at an all-even non-zero cell offset).
-bool octant_groups(const Lattice& L, std::vector<int>* group, int* ngroups);
+// class_of_group: each group's shell-1 class (groups of a class are consecutive; a class is
+// free of shell-1 bonds in all 8 octants), or empty when shell 1 does not allow them.
+bool octant_groups(const Lattice& L, std::vector<int>* group, int* ngroups,
+                   std::vector<int>* class_of_group = nullptr);
 // two sublattices joined only to each other by the first shell, 8 neighbours in cells
 // base + {0,1}^3 (layout 3); base[s] per sublattice
 bool bipartite_pair(const Lattice& L, int base[2][3]);
@@ -120,6 +123,9 @@ struct ising_mesh {
     void* demag = nullptr;               // demagnetising-field workspace, made on first use
     uint32_t* d_oct_sync = nullptr;      // octant engine: [n_replicas][nx/2] counters + head + abort
     int bip_base[2][3] = {{0, 0, 0}, {0, 0, 0}};   // layout 3: first-shell cell offsets per sublattice
+    std::vector<int> oct_class0;         // octant layout: first storage rank of each shell-1 class
+                                         // (+ end), empty when there are none; without J' a sweep
+                                         // is one class (all 8 octants) after another
 };
 
 namespace isg {
@@ -204,7 +210,12 @@ struct GeneralLaunch {
 int launch_general_colour(const GeneralLaunch& a, cudaStream_t s);
 // One class (octant, sublattice group) of an octant-layout mesh: sites of storage ranks
 // [rank0, rank0 + nrank) of that octant (a.sites and a.n_sites unused).
-int launch_octant_colour(const GeneralLaunch& a, int octant, int rank0, int nrank, cudaStream_t s);
+// octants oct0 .. oct0 + noct - 1 of storage ranks rank0 .. rank0 + nrank - 1 (a set of sites
+// with no bond among them): one launch, or one per octant where the stencil table of all of
+// them does not fit; partial slots from a.slot_base, octant_class_slots of them at most
+int launch_octant_colour(const GeneralLaunch& a, int oct0, int noct, int rank0, int nrank, cudaStream_t s);
+int octant_class_slots(int64_t q8, int nrank, int noct, bool fast);
+int octant_class_launches(int nrank, int maxcnt, int noct);   // launches of such a set
 int octant_slots_for(int64_t n_sites, bool fast);   // partial-sum slots (blocks) of one class launch
 // The octant sweeps of a PT round as ONE persistent launch: tasks (sweep, class, replica,
 // packed x-plane) in phase-major queue order, each waiting (bounded) until the planes within
@@ -216,6 +227,8 @@ struct OctEngineLaunch {
     uint32_t* abort;         // raised by a wait that gives up (zeroed before it)
     int n_sweeps, ng, reach; // sweeps, sublattice groups (classes = 8 ng), dependency reach in planes
     int rank0[kMaxSub + 1];  // first storage rank of each group, and the end
+    int class_major;         // 1: the groups are shell-1 classes, class c = g * 8 + octant
+                             // (else octant * ng + g)
     uint64_t wait_ns;        // bound of every wait
     int grid;                // persistent blocks
     int stall;               // test hook: the tasks of phase 1 wait for a count nothing reaches

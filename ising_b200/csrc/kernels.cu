@@ -211,7 +211,33 @@ struct OctDims {
     FastDiv q8, hz, hy, hyz;
     int hx, hyi, hzi;
     FastDiv q8h;             // by q8 / 2 (site pairs of k_octant_pair)
+    FastDiv per_oct;         // by the work items (sites or pairs) of one octant of the launch
 };
+
+// The stencil table of a launch over octants oct0 .. oct0 + noct - 1 and storage ranks
+// rank0 .. rank0 + nrank - 1: entry ((octant - oct0) * nrank + rank) * mc + slot.
+__device__ __forceinline__ void octant_table(const GeneralLaunch& a, OctSlot* tab, int mc, int oct0, int noct,
+                                             int rank0, int nrank, const int* s_srank, const int* s_sofr) {
+    const int q8 = (int)a.layout.q8;
+    const int per = nrank * mc;
+    for (int e = threadIdx.x; e < noct * per; e += blockDim.x) {
+        const int lo = e / per, rem = e - lo * per;
+        const int lr = rem / mc, q = rem - lr * mc;
+        const int oct = oct0 + lo;
+        const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
+        const int sub = s_sofr[rank0 + lr];
+        OctSlot o{};
+        if (q < a.st.count[sub]) {
+            const Slot sl = a.st.slots[sub * kMaxSlots + q];
+            const int tx = ox + sl.dx, ty = oy + sl.dy, tz = oz + sl.dz;
+            const int o2 = ((tx & 1) << 2) | ((ty & 1) << 1) | (tz & 1);
+            o.plane = (o2 * a.nsub + s_srank[sl.sub]) * q8;
+            o.ex = (int8_t)(tx >> 1); o.ey = (int8_t)(ty >> 1); o.ez = (int8_t)(tz >> 1);
+            o.w = sl.w; o.Dx = sl.Dx; o.Dy = sl.Dy; o.Dz = sl.Dz;
+        }
+        tab[e] = o;
+    }
+}
 
 // block sums of the four running partials: FP32 within a warp (a warp's few sites), FP64
 // across warps
@@ -232,12 +258,12 @@ __device__ __forceinline__ void block_sum4_fd(float v0, float v1, float v2, floa
 // SPT sites per thread (consecutive blocks of blockDim.x sites), so that the block's set-up
 // and its reduction are shared by SPT x 256 sites where a launch has enough of them
 template <int MOVE, int SPT>
-__global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, OctDims od, int oct, int rank0,
-                                                              int nrank) {
+__global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, OctDims od, int oct0, int noct,
+                                                              int rank0, int nrank) {
     extern __shared__ __align__(16) unsigned char oct_smem[];
     const int mc = a.oct_maxcnt;
     OctSlot* tab = reinterpret_cast<OctSlot*>(oct_smem);
-    int* s_cnt = reinterpret_cast<int*>(tab + nrank * mc);
+    int* s_cnt = reinterpret_cast<int*>(tab + noct * nrank * mc);
     int* s_sub = s_cnt + nrank;
     __shared__ int s_srank[kMaxSub], s_sofr[kMaxSub];
     const Layout& L = a.layout;
@@ -246,22 +272,8 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
         for (int k = 0; k < kMaxSub; ++k) { s_srank[k] = L.srank[k]; s_sofr[k] = L.sofr[k]; }
     }
     __syncthreads();
-    const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
     const int q8 = (int)L.q8;
-    for (int e = threadIdx.x; e < nrank * mc; e += blockDim.x) {
-        const int lr = e / mc, q = e - lr * mc;
-        const int sub = s_sofr[rank0 + lr];
-        OctSlot o{};
-        if (q < a.st.count[sub]) {
-            const Slot sl = a.st.slots[sub * kMaxSlots + q];
-            const int tx = ox + sl.dx, ty = oy + sl.dy, tz = oz + sl.dz;
-            const int o2 = ((tx & 1) << 2) | ((ty & 1) << 1) | (tz & 1);
-            o.plane = (o2 * a.nsub + s_srank[sl.sub]) * q8;
-            o.ex = (int8_t)(tx >> 1); o.ey = (int8_t)(ty >> 1); o.ez = (int8_t)(tz >> 1);
-            o.w = sl.w; o.Dx = sl.Dx; o.Dy = sl.Dy; o.Dz = sl.Dz;
-        }
-        tab[e] = o;
-    }
+    octant_table(a, tab, mc, oct0, noct, rank0, nrank, s_srank, s_sofr);
     for (int lr = threadIdx.x; lr < nrank; lr += blockDim.x) {
         s_sub[lr] = s_sofr[rank0 + lr];
         s_cnt[lr] = a.st.count[s_sub[lr]];
@@ -275,16 +287,20 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
     float* __restrict__ sz = sy + N;
     const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
     const float beta = (float)a.beta_rep[rep];
-    const uint32_t n = (uint32_t)q8 * (uint32_t)nrank;
+    const uint32_t n = (uint32_t)q8 * (uint32_t)nrank;   // sites of one octant
+    const uint32_t ntot = n * (uint32_t)noct;
     const int hx = od.hx, hy = od.hyi, hz = od.hzi;
-    const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
     float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
 #pragma unroll 1
     for (int it = 0; it < SPT; ++it) {
         const uint32_t t = (blockIdx.x * SPT + it) * blockDim.x + threadIdx.x;
-        if (t >= n) break;
-        const uint32_t lr = fdiv(t, od.q8);
-        const uint32_t pc = t - lr * (uint32_t)q8;
+        if (t >= ntot) break;
+        const uint32_t lo = fdiv(t, od.per_oct);
+        const uint32_t tt = t - lo * n;
+        const int oct = oct0 + (int)lo;
+        const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
+        const uint32_t lr = fdiv(tt, od.q8);
+        const uint32_t pc = tt - lr * (uint32_t)q8;
         const uint32_t r = fdiv(pc, od.hz);
         const int Z = (int)(pc - r * (uint32_t)hz);
         const uint32_t Xu = fdiv(r, od.hy);
@@ -292,7 +308,7 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
         const int sub = s_sub[lr];
         const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z + oz;
         const uint32_t at = ((uint32_t)(ix * a.ny + iy) * (uint32_t)a.nz + (uint32_t)iz) * (uint32_t)a.nsub + sub;
-        const OctSlot* ts = tab + lr * mc;
+        const OctSlot* ts = tab + (lo * (uint32_t)nrank + lr) * mc;
         f3 h = {0.f, 0.f, 0.f};
         const int cn = s_cnt[lr];
         for (int q = 0; q < cn; ++q) {
@@ -308,7 +324,8 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
             h.y += fmaf(o.w, sj.y, c.y);
             h.z += fmaf(o.w, sj.z, c.z);
         }
-        site_update<MOVE>(a, h, (int64_t)(class_base + t), (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
+        const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
+        site_update<MOVE>(a, h, (int64_t)(class_base + tt), (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
                           dmz);
     }
     if (a.partials) {
@@ -327,12 +344,12 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
 // neighbours as one aligned pair per component.  Each site's field is summed in slot order
 // with the stencil's expression, so the update equals k_octant_fast's bit for bit.
 template <int MOVE>
-__global__ void __launch_bounds__(kGenThreads) k_octant_pair(GeneralLaunch a, OctDims od, int oct, int rank0,
-                                                              int nrank) {
+__global__ void __launch_bounds__(kGenThreads) k_octant_pair(GeneralLaunch a, OctDims od, int oct0, int noct,
+                                                              int rank0, int nrank) {
     extern __shared__ __align__(16) unsigned char oct_smem[];
     const int mc = a.oct_maxcnt;
     OctSlot* tab = reinterpret_cast<OctSlot*>(oct_smem);
-    int* s_cnt = reinterpret_cast<int*>(tab + nrank * mc);
+    int* s_cnt = reinterpret_cast<int*>(tab + noct * nrank * mc);
     int* s_sub = s_cnt + nrank;
     __shared__ int s_srank[kMaxSub], s_sofr[kMaxSub];
     const Layout& L = a.layout;
@@ -341,22 +358,8 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_pair(GeneralLaunch a, Oc
         for (int k = 0; k < kMaxSub; ++k) { s_srank[k] = L.srank[k]; s_sofr[k] = L.sofr[k]; }
     }
     __syncthreads();
-    const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
     const int q8 = (int)L.q8;
-    for (int e = threadIdx.x; e < nrank * mc; e += blockDim.x) {
-        const int lr = e / mc, q = e - lr * mc;
-        const int sub = s_sofr[rank0 + lr];
-        OctSlot o{};
-        if (q < a.st.count[sub]) {
-            const Slot sl = a.st.slots[sub * kMaxSlots + q];
-            const int tx = ox + sl.dx, ty = oy + sl.dy, tz = oz + sl.dz;
-            const int o2 = ((tx & 1) << 2) | ((ty & 1) << 1) | (tz & 1);
-            o.plane = (o2 * a.nsub + s_srank[sl.sub]) * q8;
-            o.ex = (int8_t)(tx >> 1); o.ey = (int8_t)(ty >> 1); o.ez = (int8_t)(tz >> 1);
-            o.w = sl.w; o.Dx = sl.Dx; o.Dy = sl.Dy; o.Dz = sl.Dz;
-        }
-        tab[e] = o;
-    }
+    octant_table(a, tab, mc, oct0, noct, rank0, nrank, s_srank, s_sofr);
     for (int lr = threadIdx.x; lr < nrank; lr += blockDim.x) {
         s_sub[lr] = s_sofr[rank0 + lr];
         s_cnt[lr] = a.st.count[s_sub[lr]];
@@ -372,13 +375,16 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_pair(GeneralLaunch a, Oc
     const float beta = (float)a.beta_rep[rep];
     const int hx = od.hx, hy = od.hyi, hz = od.hzi;
     const uint32_t half8 = (uint32_t)q8 >> 1;
-    const uint32_t npair = half8 * (uint32_t)nrank;
-    const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
+    const uint32_t npair = half8 * (uint32_t)nrank;   // pairs of one octant
     float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
     const uint32_t tp = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tp < npair) {
-        const uint32_t lr = fdiv(tp, od.q8h);
-        const uint32_t pc0 = 2u * (tp - lr * half8);
+    if (tp < npair * (uint32_t)noct) {
+        const uint32_t lo = fdiv(tp, od.per_oct);
+        const uint32_t tq = tp - lo * npair;
+        const int oct = oct0 + (int)lo;
+        const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
+        const uint32_t lr = fdiv(tq, od.q8h);
+        const uint32_t pc0 = 2u * (tq - lr * half8);
         const uint32_t r = fdiv(pc0, od.hz);
         const int Z0 = (int)(pc0 - r * (uint32_t)hz);
         const uint32_t Xu = fdiv(r, od.hy);
@@ -387,7 +393,7 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_pair(GeneralLaunch a, Oc
         const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z0 + oz;
         const uint32_t at0 = ((uint32_t)(ix * a.ny + iy) * (uint32_t)a.nz + (uint32_t)iz) * (uint32_t)a.nsub + sub;
         const uint32_t at1 = at0 + 2u * (uint32_t)a.nsub;   // cell z + 2
-        const OctSlot* ts = tab + lr * mc;
+        const OctSlot* ts = tab + (lo * (uint32_t)nrank + lr) * mc;
         f3 h0 = {0.f, 0.f, 0.f}, h1 = {0.f, 0.f, 0.f};
         const int cn = s_cnt[lr];
         for (int q = 0; q < cn; ++q) {
@@ -415,6 +421,7 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_pair(GeneralLaunch a, Oc
             h0.x += fmaf(o.w, s0.x, c0.x); h0.y += fmaf(o.w, s0.y, c0.y); h0.z += fmaf(o.w, s0.z, c0.z);
             h1.x += fmaf(o.w, s1.x, c1.x); h1.y += fmaf(o.w, s1.y, c1.y); h1.z += fmaf(o.w, s1.z, c1.z);
         }
+        const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
         const uint32_t si0 = class_base + lr * (uint32_t)q8 + pc0;
         site_update<MOVE>(a, h0, (int64_t)si0, (int64_t)at0, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
         site_update<MOVE>(a, h1, (int64_t)si0 + 1, (int64_t)at1, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
@@ -535,24 +542,12 @@ __global__ void __launch_bounds__(kGenThreads, 4) k_octant_engine(GeneralLaunch 
             }
         }
         const int sw = (int)(ph / (uint32_t)ncls), c = (int)ph - sw * ncls;
-        const int oct = c / e.ng, gi = c - oct * e.ng;
+        // classes o * ng + g, or, for shell-1 classes (class-major), g * 8 + o
+        const int oct = e.class_major ? (c & 7) : c / e.ng, gi = e.class_major ? (c >> 3) : c - oct * e.ng;
         const int rank0 = s_rank0[gi], nrank = s_rank0[gi + 1] - rank0;
         const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
         if (c != cached) {   // the class's stencil, resolved as in k_octant_fast
-            for (int en = threadIdx.x; en < nrank * mc; en += blockDim.x) {
-                const int lr = en / mc, q = en - lr * mc;
-                const int sub = s_sofr[rank0 + lr];
-                OctSlot o{};
-                if (q < a.st.count[sub]) {
-                    const Slot sl = a.st.slots[sub * kMaxSlots + q];
-                    const int tx = ox + sl.dx, ty = oy + sl.dy, tz = oz + sl.dz;
-                    const int o2 = ((tx & 1) << 2) | ((ty & 1) << 1) | (tz & 1);
-                    o.plane = (o2 * a.nsub + s_srank[sl.sub]) * q8;
-                    o.ex = (int8_t)(tx >> 1); o.ey = (int8_t)(ty >> 1); o.ez = (int8_t)(tz >> 1);
-                    o.w = sl.w; o.Dx = sl.Dx; o.Dy = sl.Dy; o.Dz = sl.Dz;
-                }
-                tab[en] = o;
-            }
+            octant_table(a, tab, mc, oct, 1, rank0, nrank, s_srank, s_sofr);
             for (int lr = threadIdx.x; lr < nrank; lr += blockDim.x) {
                 s_sub[lr] = s_sofr[rank0 + lr];
                 s_cnt[lr] = a.st.count[s_sub[lr]];
@@ -774,11 +769,31 @@ int octant_slots_for(int64_t n_sites, bool fast) {
     return (int)((n_sites + per - 1) / per);
 }
 
-int launch_octant_colour(const GeneralLaunch& a, int oct, int rank0, int nrank, cudaStream_t s) {
-    const int64_t n = a.layout.q8 * nrank;
+int octant_class_slots(int64_t q8, int nrank, int noct, bool fast) {
+    return noct * octant_slots_for(q8 * nrank, fast);
+}
+
+int octant_class_launches(int nrank, int maxcnt, int noct) {
+    const size_t sm = (size_t)noct * nrank * maxcnt * sizeof(OctSlot) + 2 * (size_t)nrank * sizeof(int);
+    return (noct > 1 && (maxcnt < 1 || sm > 48u * 1024u)) ? noct : 1;
+}
+
+int launch_octant_colour(const GeneralLaunch& a, int oct0, int noct, int rank0, int nrank, cudaStream_t s) {
+    const int64_t n = a.layout.q8 * nrank;   // sites of one octant
     if (n <= 0) return ISING_OK;
-    if (oct < 0 || oct > 7 || rank0 < 0 || nrank < 1 || rank0 + nrank > a.nsub)
+    if (oct0 < 0 || noct < 1 || oct0 + noct > 8 || rank0 < 0 || nrank < 1 || rank0 + nrank > a.nsub)
         return fail(ISING_ERR_ARG, "octant class out of range");
+    const size_t tab = (size_t)nrank * a.oct_maxcnt * sizeof(OctSlot);
+    if (octant_class_launches(nrank, a.oct_maxcnt, noct) > 1) {
+        // one launch per octant, in octant order (the sites of the set are independent)
+        GeneralLaunch b = a;
+        for (int o = 0; o < noct; ++o) {
+            const int rc = launch_octant_colour(b, oct0 + o, 1, rank0, nrank, s);
+            if (rc != ISING_OK) return rc;
+            b.slot_base += octant_slots_for(n, a.oct_maxcnt > 0);
+        }
+        return ISING_OK;
+    }
     dim3 g(octant_slots_for(n, a.oct_maxcnt > 0), a.n_rep), b(kGenThreads);
     if (a.oct_maxcnt > 0) {
         // sites per thread: as many as keep about two waves of blocks (6 resident per SM);
@@ -788,34 +803,38 @@ int launch_octant_colour(const GeneralLaunch& a, int oct, int rank0, int nrank, 
             int dev = 0;
             if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         }
-        const int64_t per_launch = n * a.n_rep, want = 2LL * sms * 6 * kGenThreads;
+        const int64_t ntot = n * noct;
+        const int64_t per_launch = ntot * a.n_rep, want = 2LL * sms * 6 * kGenThreads;
         const int spt = per_launch >= 4 * want ? 4 : (per_launch >= 2 * want ? 2 : 1);
-        g.x = (unsigned)((n + (int64_t)kGenThreads * spt - 1) / ((int64_t)kGenThreads * spt));
+        g.x = (unsigned)((ntot + (int64_t)kGenThreads * spt - 1) / ((int64_t)kGenThreads * spt));
         OctDims od;
         od.q8 = make_div((uint32_t)a.layout.q8);
         od.hx = a.nx / 2; od.hyi = a.ny / 2; od.hzi = a.nz / 2;
         od.hz = make_div((uint32_t)od.hzi);
         od.hy = make_div((uint32_t)od.hyi);
-        const size_t sm = (size_t)nrank * a.oct_maxcnt * sizeof(OctSlot) + 2 * (size_t)nrank * sizeof(int);
+        const size_t sm = (size_t)noct * tab + 2 * (size_t)nrank * sizeof(int);
         if (od.hzi % 2 == 0) {   // site pairs along packed z
             od.q8h = make_div((uint32_t)(a.layout.q8 / 2));
-            g.x = (unsigned)((n / 2 + kGenThreads - 1) / kGenThreads);   // <= octant_slots_for(n, true)
-            if (a.move == 0) k_octant_pair<0><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
-            else k_octant_pair<1><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
+            od.per_oct = make_div((uint32_t)(n / 2));
+            // <= octant_class_slots(q8, nrank, noct, true) blocks
+            g.x = (unsigned)((ntot / 2 + kGenThreads - 1) / kGenThreads);
+            if (a.move == 0) k_octant_pair<0><<<g, b, sm, s>>>(a, od, oct0, noct, rank0, nrank);
+            else k_octant_pair<1><<<g, b, sm, s>>>(a, od, oct0, noct, rank0, nrank);
             ISG_CUDA(cudaGetLastError());
             return ISING_OK;
         }
-#define ISG_OF(S)                                                                      \
-    if (a.move == 0) k_octant_fast<0, S><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);   \
-    else k_octant_fast<1, S><<<g, b, sm, s>>>(a, od, oct, rank0, nrank);
+        od.per_oct = make_div((uint32_t)n);
+#define ISG_OF(S)                                                                                \
+    if (a.move == 0) k_octant_fast<0, S><<<g, b, sm, s>>>(a, od, oct0, noct, rank0, nrank);      \
+    else k_octant_fast<1, S><<<g, b, sm, s>>>(a, od, oct0, noct, rank0, nrank);
         if (spt == 4) { ISG_OF(4) } else if (spt == 2) { ISG_OF(2) } else { ISG_OF(1) }
 #undef ISG_OF
         ISG_CUDA(cudaGetLastError());
         return ISING_OK;
     }
     size_t sm = (size_t)a.st.nsub * kMaxSlots * sizeof(Slot) + kMaxSub * sizeof(int);
-    if (a.move == 0) k_octant_colour<0><<<g, b, sm, s>>>(a, oct, rank0, nrank);
-    else k_octant_colour<1><<<g, b, sm, s>>>(a, oct, rank0, nrank);
+    if (a.move == 0) k_octant_colour<0><<<g, b, sm, s>>>(a, oct0, rank0, nrank);
+    else k_octant_colour<1><<<g, b, sm, s>>>(a, oct0, rank0, nrank);
     ISG_CUDA(cudaGetLastError());
     return ISING_OK;
 }

@@ -366,11 +366,67 @@ bool bipartite_pair(const Lattice& L, int base[2][3]) {
 // (greedy colouring of that small graph).  A bond of a site to itself, which the reference's
 // shell search puts into shell 2 of BCC cells, does not constrain the colouring: the update
 // reads the site's own old value there, as a sequential sweep does.
-bool octant_groups(const Lattice& L, std::vector<int>* group, int* ngroups) {
+//
+// Shell-1 classes: when shell 1 joins no sublattice to itself at a non-zero offset, a fewest-
+// colour colouring of the sublattices by shell-1 bonds at ANY offset gives classes whose sites never
+// bond through shell 1, in every octant at once.  The groups are then numbered class by class
+// (each class coloured by the octant rule on its own), so a class is a run of consecutive
+// groups; this is kept only when it needs no more groups than the plain octant colouring.
+// class_of_group[g] is group g's shell-1 class, or empty when there are no such classes.
+namespace {
+int greedy_groups(int n, const std::vector<std::vector<char>>& conflict, const std::vector<int>& order,
+                  std::vector<int>* colour, int first) {
+    int top = first;
+    for (int s : order) {
+        int g = first;
+        for (;; ++g) {
+            bool ok = true;
+            for (int t = 0; t < n; ++t)
+                if ((*colour)[t] == g && conflict[s][t]) { ok = false; break; }
+            if (ok) break;
+        }
+        (*colour)[s] = g;
+        top = std::max(top, g + 1);
+    }
+    return top;
+}
+
+// colour the n nodes with k colours by backtracking (a bounded search; false when it finds
+// none within the bound)
+bool colour_k(int n, const std::vector<std::vector<char>>& conflict, int k, std::vector<int>* colour) {
+    colour->assign(n, -1);
+    long budget = 1L << 20;
+    std::vector<int> next(n, 0);
+    int i = 0;
+    while (i >= 0 && i < n) {
+        if (--budget < 0) return false;
+        int c = next[i];
+        for (; c < k; ++c) {
+            bool ok = true;
+            for (int t = 0; t < i; ++t)
+                if ((*colour)[t] == c && conflict[i][t]) { ok = false; break; }
+            if (ok) break;
+        }
+        if (c < k) {
+            (*colour)[i] = c;
+            next[i] = c + 1;
+            ++i;
+            if (i < n) next[i] = 0;
+        } else {
+            (*colour)[i] = -1;
+            --i;
+        }
+    }
+    return i == n;
+}
+}  // namespace
+
+bool octant_groups(const Lattice& L, std::vector<int>* group, int* ngroups, std::vector<int>* class_of_group) {
     if ((L.nx & 1) || (L.ny & 1) || (L.nz & 1) || L.nsub > kMaxSub || L.nsub < 1) return false;
-    std::vector<std::vector<char>> conflict(L.nsub, std::vector<char>(L.nsub, 0));
+    const int n = L.nsub;
+    std::vector<std::vector<char>> conflict(n, std::vector<char>(n, 0));
     for (int sh = 0; sh < 2; ++sh)
-        for (int s = 0; s < L.nsub; ++s)
+        for (int s = 0; s < n; ++s)
             for (const NbrSlot& q : L.shell[sh][s]) {
                 if ((q.dx & 1) || (q.dy & 1) || (q.dz & 1)) continue;   // different octant
                 if (q.sub == s) {
@@ -379,20 +435,41 @@ bool octant_groups(const Lattice& L, std::vector<int>* group, int* ngroups) {
                 }
                 conflict[s][q.sub] = conflict[q.sub][s] = 1;
             }
-    group->assign(L.nsub, -1);
-    int ng = 0;
-    for (int s = 0; s < L.nsub; ++s) {
-        int g = 0;
-        for (;; ++g) {
-            bool ok = true;
-            for (int t = 0; t < s; ++t)
-                if ((*group)[t] == g && conflict[s][t]) { ok = false; break; }
-            if (ok) break;
-        }
-        (*group)[s] = g;
-        ng = std::max(ng, g + 1);
-    }
+    std::vector<int> all(n);
+    for (int s = 0; s < n; ++s) all[s] = s;
+    group->assign(n, -1);
+    const int ng = greedy_groups(n, conflict, all, group, 0);
     *ngroups = ng;
+    if (class_of_group) class_of_group->clear();
+    bool merge = class_of_group != nullptr;
+    std::vector<std::vector<char>> bond1(n, std::vector<char>(n, 0));
+    for (int s = 0; s < n && merge; ++s)
+        for (const NbrSlot& q : L.shell[0][s]) {
+            if (q.sub == s) {
+                if (q.dx || q.dy || q.dz) { merge = false; break; }
+                continue;
+            }
+            bond1[s][q.sub] = bond1[q.sub][s] = 1;
+        }
+    if (!merge) return true;
+    std::vector<int> cls(n, -1), fewer;
+    int nc = greedy_groups(n, bond1, all, &cls, 0);
+    for (int k = 1; k < nc; ++k)   // fewer classes than the greedy colouring, where there are
+        if (colour_k(n, bond1, k, &fewer)) { cls = fewer; nc = k; break; }
+    std::vector<int> g2(n, -1), of;
+    int next = 0;
+    for (int k = 0; k < nc; ++k) {
+        std::vector<int> members;
+        for (int s = 0; s < n; ++s)
+            if (cls[s] == k) members.push_back(s);
+        const int top = greedy_groups(n, conflict, members, &g2, next);
+        for (int g = next; g < top; ++g) of.push_back(k);
+        next = top;
+    }
+    if (next > ng) return true;   // the plain octant colouring has fewer groups
+    *group = g2;
+    *ngroups = next;
+    *class_of_group = of;
     return true;
 }
 

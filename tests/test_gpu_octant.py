@@ -59,7 +59,7 @@ def test_octant_sweeps_replay_the_oracle(oracle, ib, cuda_ok, case):
     op, pp = _both_params(oracle, ib, **h)
     col, ncol = pm.colouring(pp)
     if pm.layout == "octant":
-        assert ncol % 8 == 0
+        assert ncol % 8 == 0 if "Jp" in h else ncol == 3   # without J': the shell-1 classes
     elif "Jp" not in h:   # the two sublattices
         assert ncol == 2 and np.array_equal(col, np.arange(om.natoms) % 2)
     seed = 0x0C7A + case

@@ -81,8 +81,9 @@ def test_colouring_is_independent(oracle, ib):
     """Every colour class is an independent set of the active shells' bonds (a bond of a site
     to itself, which the reference's shell search gives BCC cells in shell 2, excepted).  BCC
     meshes of at least 4 cells per axis take sublattice planes, whose classes without J' are
-    the two sublattices; even hyper-kagome meshes the octant classes: class = octant * groups
-    + group with octant = (x&1, y&1, z&1) of the cell; other meshes a greedy colouring."""
+    the two sublattices; even hyper-kagome meshes the octant classes with J': class = octant *
+    groups + group with octant = (x&1, y&1, z&1) of the cell, and without J' its three shell-1
+    classes (4 of the 12 sublattices each, in every octant); other meshes a greedy colouring."""
     cases = (("SC", (6, 6, 6)), ("SC", (5, 5, 5)), ("BCC", (4, 4, 4)), ("BCC", (6, 4, 8)), ("BCC", (3, 4, 3)),
              ("BCC", (5, 6, 7)), ("HK", (4, 4, 4)), ("HK", (4, 6, 4)), ("HK", (3, 3, 3)))
     for kind, dims in cases:
@@ -105,6 +106,11 @@ def test_colouring_is_independent(oracle, ib):
                 assert n == 2 and pm.checkerboard
             if pm.layout == "sublattice" and Jp == 0.0:
                 assert n == 2 and np.array_equal(col, np.arange(pm.numAtoms) % 2)
+            elif pm.layout == "octant" and Jp == 0.0:
+                assert n == 3
+                nsub = len(frac)
+                subs = [sorted(set(np.flatnonzero(col == k) % nsub)) for k in range(3)]
+                assert sorted(len(x) for x in subs) == [4, 4, 4] and sorted(sum(subs, [])) == list(range(nsub))
             elif pm.layout == "octant":
                 assert n % 8 == 0
                 nsub = len(frac)
