@@ -71,6 +71,11 @@ WORKLOADS["hk"] = dict(cell="hk", L=48, R=16, tmin=0.1, tmax=2.0, J=-1.0, D=0.3,
                        k=10, dmi="interfacial",
                        desc="hyper-kagome 48^3 cells (12 atoms) x 16 PT replicas, T 0.1-2.0, J=1, interfacial D=0.3, "
                             "B=0.1 z, shell 1")
+# bin/ISING takes J' from its command line (src/ISING.f90:50-58): hyper-kagome with shell 2 on
+WORKLOADS["hkjp"] = dict(cell="hk", L=48, R=16, tmin=0.1, tmax=2.0, J=-1.0, Jp=0.1, D=0.3, B=0.1, K=0.0,
+                         move="ball", r=0.2, k=10, dmi="interfacial",
+                         desc="hyper-kagome 48^3 cells (12 atoms) x 16 PT replicas, T 0.1-2.0, J=1, J'=0.1 "
+                              "(shells 1-2), interfacial D=0.3, B=0.1 z")
 WORKLOADS["stats"] = dict(L=96, nz=96, scale=10, J=-1.0, D=0.5, B=0.25, K=0.0, move="ball", r=0.2, tmin=0.1,
                           desc="chainMesh_statistics on SC L=96 (96 slices): winding per slice, magnetisation and "
                                "the 60 x 20 skyrmion search on the middle slice's 960 x 960 interpolated density")
@@ -248,7 +253,8 @@ def cpu_reference_rate(w, steps, warmup, threads, L_sample=None):
     frac, (a, b, c, ab, bc, ca) = oracle_cell(O, w)
     m = O.Mesh(frac, L, L, L, a, b, c, ab, bc, ca)
     m.init_uniform(0x15196)
-    p = O.Params(J=w["J"], Dz=w["D"], B=w["B"], K=w["K"], dmi_bulk=w.get("dmi", "bulk") == "bulk")
+    p = O.Params(J=w["J"], J_prime=w.get("Jp", 0.0), Dz=w["D"], B=w["B"], K=w["K"],
+                 dmi_bulk=w.get("dmi", "bulk") == "bulk")
     beta = 1.0 / w["tmin"]
     for _ in range(warmup):
         m.metropolis_mcs_omp(beta, 1, p, w["r"], n_threads=threads, time_seed=1)
@@ -471,7 +477,7 @@ def run_gpu(args, w):
         m = make_mesh(ib, w, L, R, dev)
         m.set_stream(stream.cuda_stream)
         m.init_uniform(0x15196, ensemble=ens_id)
-        p = ib.params(J=w["J"], Dz=D, B=B, K=w["K"], dmi=w.get("dmi", "bulk"))
+        p = ib.params(J=w["J"], J_prime=w.get("Jp", 0.0), Dz=D, B=B, K=w["K"], dmi=w.get("dmi", "bulk"))
         members.append((m, 1.0 / ib.temperature_ladder(w["tmin"], w["tmax"], R), p, ens_id))
     sites = sum(spec[i][0] ** 3 * spec[i][1] for i in mine) * cell_atoms(w)
     sites_job = sum(L ** 3 * R for L, R, _, _ in spec) if split else world * sites
@@ -587,6 +593,10 @@ def run_gpu(args, w):
     if os.path.exists(tfile):
         try:
             for t in json.load(open(tfile)).get("kernels", []):
+                # an entry with "only" holds for those workloads alone (the traffic of a class
+                # pass depends on the stencil)
+                if t.get("only") and args.workload not in t["only"]:
+                    continue
                 if t.get("kernel") == kernel_name and t.get("bytes_per_update"):
                     traffic = t["bytes_per_update"] * bytes_per_launch / BYTES_PER_UPDATE
         except Exception:

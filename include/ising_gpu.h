@@ -72,10 +72,9 @@ typedef struct {
     int shell_size[2];       /* entries per atom in shells 1 and 2 (sublattice 0) */
     int checkerboard;        /* storage order of the spins on the device: 1 the SC 2-colour fast path
                                 (even nx, ny; nz % 4 == 0); 2 the octant order of other crystals
-                                with even extents (colour classes = cell octant x sublattice
-                                group, each one contiguous range; without J', where shell 1
-                                allows it, runs of groups free of shell-1 bonds in all 8
-                                octants); 3 sublattice planes of
+                                with even extents (blocks of cells/8 sites per cell octant
+                                and sublattice; each colour class is a set of blocks); 3
+                                sublattice planes of
                                 two-sublattice crystals whose first shell joins only the two
                                 sublattices (BCC; the colour classes are the sublattices);
                                 0 the reference atom order */
@@ -165,12 +164,13 @@ int ising_params_reference(int which, double J, double J_prime, double Dz, doubl
  * (x+y+z)&1 on simple-cubic meshes with even nx, ny, nz % 4 == 0 and no J'; the sublattice on
  * BCC meshes (layout 3) without J'; on other crystals
  * with even extents whose shells 1-2 never join one sublattice at an all-even non-zero cell
- * offset (BCC and hyper-kagome, src/unit_cells.f90:7-77), class octant * groups + group of the
- * cell octant (x&1, y&1, z&1) and a sublattice group (sublattices bonded at an all-even offset
- * get different groups), or without J', where shell 1 joins no sublattice to itself, the fewest
- * classes of sublattices free of shell-1 bonds at any offset (every octant of each; 3 on
- * hyper-kagome); a verified greedy colouring of the active shells otherwise.  No reference counterpart: Metropolis_mcs draws random parity cells
- * instead (src/energyMin.f90:288-316). */
+ * offset (BCC and hyper-kagome, src/unit_cells.f90:7-77), classes of whole blocks (cell octant
+ * (x&1, y&1, z&1), sublattice) with no bond of the active shells among them: the fewer of the
+ * octant x sublattice-group classes (without J', where shell 1 joins no sublattice to itself,
+ * the fewest sublattice sets free of shell-1 bonds at any offset, every octant of each: 3 on
+ * hyper-kagome) and a DSatur colouring of the blocks (15 on hyper-kagome with J'); a verified
+ * greedy colouring of the active shells otherwise.  No reference counterpart: Metropolis_mcs
+ * draws random parity cells instead (src/energyMin.f90:288-316). */
 int ising_mesh_colouring(ising_mesh* mesh, const ising_params* p, int* colour_of, int* n_colours);
 
 /* ---------------------------------------------------------------- energies */

@@ -175,27 +175,51 @@ int sc_dmi(const ising_mesh* m, const ising_params& p, HamDev* h, int* kind) {
     return ISING_OK;
 }
 
-// Colour classes of a mesh that is not on the checkerboard path.  Octant-layout meshes: the
-// octant classes (octant o, sublattice group g) as class o * groups + g, or, without J' where
-// the mesh has shell-1 classes, those classes (every octant of each); else a greedy colouring
-// of the active shells' bonds.
+// Colour classes of a mesh that is not on the checkerboard path.  Octant-layout meshes: sets
+// of blocks (cell octant, sublattice), the fewer of (1) the octant classes (octant o,
+// sublattice group g) as class o * groups + g, or without J', where the mesh has them, its
+// shell-1 classes (every octant of each), and (2) a DSatur colouring of the block graph of the
+// active shells; else a greedy colouring of the active shells' bonds.
 int host_colouring(ising_mesh* m, bool shell2, Colouring& c) {
     if (!c.host_colour.empty()) return ISING_OK;
     const Lattice& L = m->lat;
     if (m->layout.cb == 2) {
-        const bool by_class = !shell2 && !m->oct_class0.empty();
-        const std::vector<int>& r0 = by_class ? m->oct_class0 : m->oct_rank0;
-        const int ng = (int)r0.size() - 1;
+        auto code = [&](int o, int rank) { return (uint8_t)((o << 4) | rank); };
+        std::vector<std::vector<uint8_t>> cls;
+        if (!shell2 && !m->oct_class0.empty()) {
+            for (size_t k = 0; k + 1 < m->oct_class0.size(); ++k) {
+                cls.emplace_back();
+                for (int o = 0; o < 8; ++o)
+                    for (int r = m->oct_class0[k]; r < m->oct_class0[k + 1]; ++r) cls.back().push_back(code(o, r));
+            }
+        } else {
+            const int ng = (int)m->oct_rank0.size() - 1;
+            for (int k = 0; k < 8 * ng; ++k) {
+                cls.emplace_back();
+                for (int r = m->oct_rank0[k % ng]; r < m->oct_rank0[k % ng + 1]; ++r) cls.back().push_back(code(k / ng, r));
+            }
+        }
+        std::vector<std::vector<int>> ds;
+        if (octant_block_classes(L, shell2, &ds) && ds.size() < cls.size()) {
+            cls.clear();
+            for (const auto& k : ds) {
+                cls.emplace_back();
+                for (int v : k) cls.back().push_back(code(v / L.nsub, m->layout.srank[v % L.nsub]));
+                std::sort(cls.back().begin(), cls.back().end());
+            }
+        }
+        std::vector<int> of_block(128, -1);
+        for (size_t k = 0; k < cls.size(); ++k)
+            for (uint8_t b : cls[k]) of_block[b] = (int)k;
         c.host_colour.resize(L.natoms);
         for (int64_t at = 0; at < L.natoms; ++at) {
             int ix, iy, iz, sb;
             L.cell_of(at, &ix, &iy, &iz, &sb);
-            const int rk = m->layout.srank[sb];
-            int g = 0;
-            while (rk >= r0[g + 1]) ++g;
-            c.host_colour[at] = by_class ? g : (((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1)) * ng + g;
+            const int o = ((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1);
+            c.host_colour[at] = of_block[code(o, m->layout.srank[sb])];
         }
-        c.ncol = by_class ? ng : 8 * ng;
+        c.ncol = (int)cls.size();
+        c.oct_blocks = std::move(cls);
         return ISING_OK;
     }
     if (m->layout.cb == 3 && !shell2) {   // the two sublattices
@@ -240,7 +264,6 @@ struct SweepPlan {
     const float* demag = nullptr;   // general path: demagnetising field of the swept replica
     int oct_maxcnt = 0;        // octant layout: k_octant_fast's table width (0: k_octant_colour)
     bool oct_engine = false;   // octant layout: every sweep of a call in one persistent launch
-    bool oct_by_class = false; // octant layout: the classes are the mesh's shell-1 classes
     int oct_reach = 1;         // its dependency reach in packed x-planes
     int oct_grid = 0;          // its persistent blocks
     bool bip = false;          // layout 3 without J': the two sublattice classes (k_bip_sweep)
@@ -300,7 +323,6 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
         }
     }
     if (m->layout.cb == 2) {
-        const int ng = (int)m->oct_rank0.size() - 1;
         // the per-class stencil of k_octant_fast: every packed offset floor((o + d) / 2),
         // o in {0, 1}, must lie within one period of its axis
         std::vector<Slot> hs((size_t)kMaxSub * kMaxSlots);
@@ -333,17 +355,9 @@ int make_plan(ising_mesh* m, const ising_params& p, SweepPlan* plan, Slot* slots
             if (!m->d_oct_sync)
                 ISG_TRY(dev_alloc(&m->d_oct_sync, (size_t)m->n_replicas * (size_t)(Lt.nx / 2) + 2));
         }
-        // without J' on a mesh with shell-1 classes: one class (all 8 octants) after another
-        plan->oct_by_class = !sh2 && !m->oct_class0.empty();
-        if (plan->oct_by_class) {
-            for (size_t k = 0; k + 1 < m->oct_class0.size(); ++k)
-                tot += octant_class_slots(m->layout.q8, m->oct_class0[k + 1] - m->oct_class0[k], 8,
-                                          plan->oct_maxcnt > 0);
-        } else {
-            for (int k = 0; k < 8 * ng; ++k)
-                tot += octant_slots_for(m->layout.q8 * (m->oct_rank0[k % ng + 1] - m->oct_rank0[k % ng]),
-                                        plan->oct_maxcnt > 0);
-        }
+        // the classes are lists of blocks (octant, storage rank), host_colouring's
+        for (const auto& k : plan->col->oct_blocks)
+            tot += octant_class_slots(m->layout.q8, (int)k.size(), plan->oct_maxcnt);
         // every replica in each class launch: L2-sized replica groups (a group running all its
         // sweeps before the next) measured no faster on BCC 96^3 x 16 and much slower on
         // hyper-kagome, whose classes are small; large launches let a thread take several sites
@@ -438,11 +452,17 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
         e.abort = m->d_oct_sync + 1;
         e.done = m->d_oct_sync + 2;
         e.n_sweeps = n_sweeps;
-        const std::vector<int>& r0 = plan.oct_by_class ? m->oct_class0 : m->oct_rank0;
-        e.ng = (int)r0.size() - 1;
-        e.class_major = plan.oct_by_class ? 1 : 0;
+        const auto& cls = plan.col->oct_blocks;
+        e.ncls = (int)cls.size();
+        e.maxnb = 0;
+        int nb = 0;
+        for (int c = 0; c < e.ncls; ++c) {
+            e.start[c] = (uint8_t)nb;
+            for (uint8_t b : cls[c]) e.code[nb++] = b;
+            e.maxnb = std::max(e.maxnb, (int)cls[c].size());
+        }
+        e.start[e.ncls] = (uint8_t)nb;
         e.reach = plan.oct_reach;
-        for (int k = 0; k <= kMaxSub; ++k) e.rank0[k] = k <= e.ng ? r0[k] : r0[e.ng];
         e.wait_ns = plan.oct_wait_ns;
         e.stall = plan.oct_stall;
         e.grid = plan.oct_grid;
@@ -452,11 +472,11 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
         ISG_CUDA(cudaMemsetAsync(m->d_oct_sync, 0, ((size_t)n_rep * hx + 2) * sizeof(uint32_t), m->stream));
         return launch_octant_engine(g, e, m->stream);
     }
-    if (m->layout.cb == 2) {   // octant classes: contiguous storage ranges
+    if (m->layout.cb == 2) {   // octant classes: lists of blocks (octant, storage rank)
         // replicas are independent: each L2-sized group of replicas runs all its sweeps
         // (every class, in order) before the next group starts, so a group's spins stay in L2
-        const int ng = (int)m->oct_rank0.size() - 1;
         g.oct_maxcnt = plan.oct_maxcnt;
+        const auto& cls = plan.col->oct_blocks;
         const int G = std::max(1, plan.group);
         for (int gr = 0; gr < n_rep; gr += G) {
             g.rep_first = rep_first + gr;
@@ -465,20 +485,13 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
             for (int sw = 0; sw < n_sweeps; ++sw) {
                 g.sweep_offset = sw0 + (uint32_t)sw;
                 int slot = 0;
-                if (plan.oct_by_class) {
-                    for (size_t k = 0; k + 1 < m->oct_class0.size(); ++k) {
-                        const int r0 = m->oct_class0[k], nr = m->oct_class0[k + 1] - r0;
-                        g.slot_base = slot;
-                        ISG_TRY(launch_octant_colour(g, 0, 8, r0, nr, m->stream));
-                        slot += octant_class_slots(m->layout.q8, nr, 8, plan.oct_maxcnt > 0);
-                    }
-                    continue;
-                }
-                for (int k = 0; k < 8 * ng; ++k) {
-                    const int gi = k % ng, r0 = m->oct_rank0[gi], nr = m->oct_rank0[gi + 1] - r0;
+                for (const auto& k : cls) {
+                    OctBlocks bl{};
+                    bl.n = (int)k.size();
+                    for (int i = 0; i < bl.n; ++i) bl.code[i] = k[i];
                     g.slot_base = slot;
-                    ISG_TRY(launch_octant_colour(g, k / ng, 1, r0, nr, m->stream));
-                    slot += octant_slots_for(m->layout.q8 * nr, plan.oct_maxcnt > 0);
+                    ISG_TRY(launch_octant_class(g, bl, m->stream));
+                    slot += octant_class_slots(m->layout.q8, bl.n, plan.oct_maxcnt);
                 }
             }
         }
@@ -1411,11 +1424,10 @@ extern "C" int ising_pt_schedule(const ising_pt* pt, int k, int* group, int* lau
     if (P.sc) L = G > 1 ? G * k + 1 : 2 * k;
     else if (P.bip) { L = 2 * k; grp = pt->n; }
     else if (oct && P.oct_engine) { L = 1; grp = pt->n; }
-    else if (oct && P.oct_by_class) {
-        const std::vector<int>& c0 = pt->mesh->oct_class0;
-        for (size_t c = 0; c + 1 < c0.size(); ++c) L += octant_class_launches(c0[c + 1] - c0[c], P.oct_maxcnt, 8);
+    else if (oct) {
+        for (const auto& c : P.col->oct_blocks) L += octant_class_launches((int)c.size(), P.oct_maxcnt);
         L *= G * k;
-    } else if (oct) L = G * k * 8 * ((int)pt->mesh->oct_rank0.size() - 1);
+    }
     else L = k * P.col->ncol;
     if (group) *group = grp;
     if (launches) *launches = L;

@@ -73,6 +73,9 @@ bool is_checkerboard_sc(const Lattice& L);
 // free of shell-1 bonds in all 8 octants), or empty when shell 1 does not allow them.
 bool octant_groups(const Lattice& L, std::vector<int>* group, int* ngroups,
                    std::vector<int>* class_of_group = nullptr);
+// classes of the octant blocks (octant o, sublattice s) for the active shells, each as the
+// ascending list of o * nsub + s (a DSatur colouring of the block graph)
+bool octant_block_classes(const Lattice& L, bool shell2, std::vector<std::vector<int>>* out);
 // two sublattices joined only to each other by the first shell, 8 neighbours in cells
 // base + {0,1}^3 (layout 3); base[s] per sublattice
 bool bipartite_pair(const Lattice& L, int base[2][3]);
@@ -83,6 +86,9 @@ struct Colouring {
     std::vector<int> host_colour;
     std::vector<int> class_start;   // ncol + 1
     int* d_sites = nullptr;         // atoms grouped by class
+    // octant layout: the blocks (octant, storage rank) of each class as octant << 4 | rank,
+    // ascending (storage order)
+    std::vector<std::vector<uint8_t>> oct_blocks;
 };
 
 struct DeviceStencil {
@@ -210,12 +216,18 @@ struct GeneralLaunch {
 int launch_general_colour(const GeneralLaunch& a, cudaStream_t s);
 // One class (octant, sublattice group) of an octant-layout mesh: sites of storage ranks
 // [rank0, rank0 + nrank) of that octant (a.sites and a.n_sites unused).
-// octants oct0 .. oct0 + noct - 1 of storage ranks rank0 .. rank0 + nrank - 1 (a set of sites
-// with no bond among them): one launch, or one per octant where the stencil table of all of
-// them does not fit; partial slots from a.slot_base, octant_class_slots of them at most
-int launch_octant_colour(const GeneralLaunch& a, int oct0, int noct, int rank0, int nrank, cudaStream_t s);
-int octant_class_slots(int64_t q8, int nrank, int noct, bool fast);
-int octant_class_launches(int nrank, int maxcnt, int noct);   // launches of such a set
+// One colour class of an octant-layout mesh as a list of blocks (cell octant o, storage rank
+// r), each code o << 4 | r; the blocks' sites share no bond.
+constexpr int kMaxOctBlocks = 8 * kMaxSub;
+struct OctBlocks {
+    int n;
+    uint8_t code[kMaxOctBlocks];
+};
+// the class in one launch, or in runs of blocks whose stencils fit 48 KB of shared memory;
+// partial slots from a.slot_base, octant_class_slots of them
+int launch_octant_class(const GeneralLaunch& a, const OctBlocks& b, cudaStream_t s);
+int octant_class_slots(int64_t q8, int nblocks, int maxcnt);
+int octant_class_launches(int nblocks, int maxcnt);
 int octant_slots_for(int64_t n_sites, bool fast);   // partial-sum slots (blocks) of one class launch
 // The octant sweeps of a PT round as ONE persistent launch: tasks (sweep, class, replica,
 // packed x-plane) in phase-major queue order, each waiting (bounded) until the planes within
@@ -225,10 +237,10 @@ struct OctEngineLaunch {
     uint32_t* done;          // [n_rep][hx] phases completed in this launch (zeroed before it)
     uint32_t* head;          // task queue head (zeroed before it)
     uint32_t* abort;         // raised by a wait that gives up (zeroed before it)
-    int n_sweeps, ng, reach; // sweeps, sublattice groups (classes = 8 ng), dependency reach in planes
-    int rank0[kMaxSub + 1];  // first storage rank of each group, and the end
-    int class_major;         // 1: the groups are shell-1 classes, class c = g * 8 + octant
-                             // (else octant * ng + g)
+    int n_sweeps, reach;     // sweeps, dependency reach in packed x-planes
+    int ncls, maxnb;         // classes per sweep, most blocks in a class
+    uint8_t code[kMaxOctBlocks];        // the blocks of every class, class after class
+    uint8_t start[kMaxOctBlocks + 1];   // class c: code[start[c] .. start[c + 1])
     uint64_t wait_ns;        // bound of every wait
     int grid;                // persistent blocks
     int stall;               // test hook: the tasks of phase 1 wait for a count nothing reaches

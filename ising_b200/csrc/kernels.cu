@@ -211,31 +211,53 @@ struct OctDims {
     FastDiv q8, hz, hy, hyz;
     int hx, hyi, hzi;
     FastDiv q8h;             // by q8 / 2 (site pairs of k_octant_pair)
-    FastDiv per_oct;         // by the work items (sites or pairs) of one octant of the launch
 };
 
-// The stencil table of a launch over octants oct0 .. oct0 + noct - 1 and storage ranks
-// rank0 .. rank0 + nrank - 1: entry ((octant - oct0) * nrank + rank) * mc + slot.
-__device__ __forceinline__ void octant_table(const GeneralLaunch& a, OctSlot* tab, int mc, int oct0, int noct,
-                                             int rank0, int nrank, const int* s_srank, const int* s_sofr) {
+// Per launch the block stencils of a list of octant blocks (octant << 4 | storage rank):
+// table entry b * mc + slot, and per block its sublattice, slot count, octant and storage base.
+// The kernels take the launch structs as __grid_constant__ parameters, so the block list and
+// the layout tables are indexed in the parameter space (no per-thread copy).
+struct OctBlockSmem {
+    OctSlot* tab;
+    int *sub, *cnt, *oct;
+    uint32_t* base;
+};
+__device__ __forceinline__ OctBlockSmem octant_smem(unsigned char* raw, int nb, int mc) {
+    OctBlockSmem m;
+    m.tab = reinterpret_cast<OctSlot*>(raw);
+    m.sub = reinterpret_cast<int*>(m.tab + nb * mc);
+    m.cnt = m.sub + nb;
+    m.oct = m.cnt + nb;
+    m.base = reinterpret_cast<uint32_t*>(m.oct + nb);
+    return m;
+}
+size_t octant_smem_bytes(int nb, int mc) { return (size_t)nb * mc * sizeof(OctSlot) + 4 * (size_t)nb * sizeof(int); }
+
+__device__ __forceinline__ void octant_table(const GeneralLaunch& a, const OctBlockSmem& m, int mc, const uint8_t* code,
+                                             int nb) {
     const int q8 = (int)a.layout.q8;
-    const int per = nrank * mc;
-    for (int e = threadIdx.x; e < noct * per; e += blockDim.x) {
-        const int lo = e / per, rem = e - lo * per;
-        const int lr = rem / mc, q = rem - lr * mc;
-        const int oct = oct0 + lo;
+    for (int e = threadIdx.x; e < nb * mc; e += blockDim.x) {
+        const int b = e / mc, q = e - b * mc;
+        const int oct = code[b] >> 4;
         const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
-        const int sub = s_sofr[rank0 + lr];
+        const int sub = a.layout.sofr[code[b] & 15];
         OctSlot o{};
         if (q < a.st.count[sub]) {
             const Slot sl = a.st.slots[sub * kMaxSlots + q];
             const int tx = ox + sl.dx, ty = oy + sl.dy, tz = oz + sl.dz;
             const int o2 = ((tx & 1) << 2) | ((ty & 1) << 1) | (tz & 1);
-            o.plane = (o2 * a.nsub + s_srank[sl.sub]) * q8;
+            o.plane = (o2 * a.nsub + a.layout.srank[sl.sub]) * q8;
             o.ex = (int8_t)(tx >> 1); o.ey = (int8_t)(ty >> 1); o.ez = (int8_t)(tz >> 1);
             o.w = sl.w; o.Dx = sl.Dx; o.Dy = sl.Dy; o.Dz = sl.Dz;
         }
-        tab[e] = o;
+        m.tab[e] = o;
+    }
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        const int oct = code[b] >> 4, rank = code[b] & 15;
+        m.sub[b] = a.layout.sofr[rank];
+        m.cnt[b] = a.st.count[m.sub[b]];
+        m.oct[b] = oct;
+        m.base[b] = (uint32_t)((oct * a.nsub + rank) * q8);
     }
 }
 
@@ -255,29 +277,17 @@ __device__ __forceinline__ void block_sum4_fd(float v0, float v1, float v2, floa
     __syncthreads();
 }
 
-// SPT sites per thread (consecutive blocks of blockDim.x sites), so that the block's set-up
-// and its reduction are shared by SPT x 256 sites where a launch has enough of them
+// A class given as a list of octant blocks (the blocks of one class share no bond, so they
+// are updated at once): thread t takes site t % q8 of block t / q8, SPT sites per thread
+// (consecutive runs of blockDim.x sites), so that the block's set-up and its reduction are
+// shared by SPT x 256 sites where a launch has enough of them
 template <int MOVE, int SPT>
-__global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, OctDims od, int oct0, int noct,
-                                                              int rank0, int nrank) {
+__global__ void __launch_bounds__(kGenThreads) k_octant_fast(const __grid_constant__ GeneralLaunch a, OctDims od,
+                                                              const __grid_constant__ OctBlocks bl) {
     extern __shared__ __align__(16) unsigned char oct_smem[];
-    const int mc = a.oct_maxcnt;
-    OctSlot* tab = reinterpret_cast<OctSlot*>(oct_smem);
-    int* s_cnt = reinterpret_cast<int*>(tab + noct * nrank * mc);
-    int* s_sub = s_cnt + nrank;
-    __shared__ int s_srank[kMaxSub], s_sofr[kMaxSub];
-    const Layout& L = a.layout;
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < kMaxSub; ++k) { s_srank[k] = L.srank[k]; s_sofr[k] = L.sofr[k]; }
-    }
-    __syncthreads();
-    const int q8 = (int)L.q8;
-    octant_table(a, tab, mc, oct0, noct, rank0, nrank, s_srank, s_sofr);
-    for (int lr = threadIdx.x; lr < nrank; lr += blockDim.x) {
-        s_sub[lr] = s_sofr[rank0 + lr];
-        s_cnt[lr] = a.st.count[s_sub[lr]];
-    }
+    const int mc = a.oct_maxcnt, nb = bl.n;
+    const OctBlockSmem m = octant_smem(oct_smem, nb, mc);
+    octant_table(a, m, mc, bl.code, nb);
     __syncthreads();
     const int rl = blockIdx.y;
     const int rep = a.rep_first + rl;
@@ -287,30 +297,26 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
     float* __restrict__ sz = sy + N;
     const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
     const float beta = (float)a.beta_rep[rep];
-    const uint32_t n = (uint32_t)q8 * (uint32_t)nrank;   // sites of one octant
-    const uint32_t ntot = n * (uint32_t)noct;
+    const int q8 = (int)a.layout.q8;
+    const uint32_t ntot = (uint32_t)q8 * (uint32_t)nb;
     const int hx = od.hx, hy = od.hyi, hz = od.hzi;
     float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
 #pragma unroll 1
     for (int it = 0; it < SPT; ++it) {
         const uint32_t t = (blockIdx.x * SPT + it) * blockDim.x + threadIdx.x;
         if (t >= ntot) break;
-        const uint32_t lo = fdiv(t, od.per_oct);
-        const uint32_t tt = t - lo * n;
-        const int oct = oct0 + (int)lo;
-        const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
-        const uint32_t lr = fdiv(tt, od.q8);
-        const uint32_t pc = tt - lr * (uint32_t)q8;
+        const uint32_t b = fdiv(t, od.q8);
+        const uint32_t pc = t - b * (uint32_t)q8;
         const uint32_t r = fdiv(pc, od.hz);
         const int Z = (int)(pc - r * (uint32_t)hz);
         const uint32_t Xu = fdiv(r, od.hy);
         const int Y = (int)(r - Xu * (uint32_t)hy), X = (int)Xu;
-        const int sub = s_sub[lr];
-        const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z + oz;
+        const int oct = m.oct[b], sub = m.sub[b];
+        const int ix = 2 * X + ((oct >> 2) & 1), iy = 2 * Y + ((oct >> 1) & 1), iz = 2 * Z + (oct & 1);
         const uint32_t at = ((uint32_t)(ix * a.ny + iy) * (uint32_t)a.nz + (uint32_t)iz) * (uint32_t)a.nsub + sub;
-        const OctSlot* ts = tab + (lo * (uint32_t)nrank + lr) * mc;
+        const OctSlot* ts = m.tab + b * mc;
         f3 h = {0.f, 0.f, 0.f};
-        const int cn = s_cnt[lr];
+        const int cn = m.cnt[b];
         for (int q = 0; q < cn; ++q) {
             const OctSlot o = ts[q];
             int jx = X + o.ex, jy = Y + o.ey, jz = Z + o.ez;
@@ -324,8 +330,7 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
             h.y += fmaf(o.w, sj.y, c.y);
             h.z += fmaf(o.w, sj.z, c.z);
         }
-        const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
-        site_update<MOVE>(a, h, (int64_t)(class_base + tt), (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
+        site_update<MOVE>(a, h, (int64_t)(m.base[b] + pc), (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
                           dmz);
     }
     if (a.partials) {
@@ -343,27 +348,13 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(GeneralLaunch a, Oc
 // stencil slot, the x/y wrap and the row base; a slot with no packed z offset reads both
 // neighbours as one aligned pair per component.  Each site's field is summed in slot order
 // with the stencil's expression, so the update equals k_octant_fast's bit for bit.
-template <int MOVE>
-__global__ void __launch_bounds__(kGenThreads) k_octant_pair(GeneralLaunch a, OctDims od, int oct0, int noct,
-                                                              int rank0, int nrank) {
+template <int MOVE, int PPT>
+__global__ void __launch_bounds__(kGenThreads, 5) k_octant_pair(const __grid_constant__ GeneralLaunch a, OctDims od,
+                                                                 const __grid_constant__ OctBlocks bl) {
     extern __shared__ __align__(16) unsigned char oct_smem[];
-    const int mc = a.oct_maxcnt;
-    OctSlot* tab = reinterpret_cast<OctSlot*>(oct_smem);
-    int* s_cnt = reinterpret_cast<int*>(tab + noct * nrank * mc);
-    int* s_sub = s_cnt + nrank;
-    __shared__ int s_srank[kMaxSub], s_sofr[kMaxSub];
-    const Layout& L = a.layout;
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < kMaxSub; ++k) { s_srank[k] = L.srank[k]; s_sofr[k] = L.sofr[k]; }
-    }
-    __syncthreads();
-    const int q8 = (int)L.q8;
-    octant_table(a, tab, mc, oct0, noct, rank0, nrank, s_srank, s_sofr);
-    for (int lr = threadIdx.x; lr < nrank; lr += blockDim.x) {
-        s_sub[lr] = s_sofr[rank0 + lr];
-        s_cnt[lr] = a.st.count[s_sub[lr]];
-    }
+    const int mc = a.oct_maxcnt, nb = bl.n;
+    const OctBlockSmem m = octant_smem(oct_smem, nb, mc);
+    octant_table(a, m, mc, bl.code, nb);
     __syncthreads();
     const int rl = blockIdx.y;
     const int rep = a.rep_first + rl;
@@ -374,28 +365,26 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_pair(GeneralLaunch a, Oc
     const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset;
     const float beta = (float)a.beta_rep[rep];
     const int hx = od.hx, hy = od.hyi, hz = od.hzi;
-    const uint32_t half8 = (uint32_t)q8 >> 1;
-    const uint32_t npair = half8 * (uint32_t)nrank;   // pairs of one octant
+    const uint32_t half8 = (uint32_t)a.layout.q8 >> 1;
+    const uint32_t npair = half8 * (uint32_t)nb;
     float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
-    const uint32_t tp = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tp < npair * (uint32_t)noct) {
-        const uint32_t lo = fdiv(tp, od.per_oct);
-        const uint32_t tq = tp - lo * npair;
-        const int oct = oct0 + (int)lo;
-        const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
-        const uint32_t lr = fdiv(tq, od.q8h);
-        const uint32_t pc0 = 2u * (tq - lr * half8);
+#pragma unroll 1
+    for (int it = 0; it < PPT; ++it) {
+        const uint32_t tp = (blockIdx.x * PPT + it) * blockDim.x + threadIdx.x;
+        if (tp >= npair) break;
+        const uint32_t b = fdiv(tp, od.q8h);
+        const uint32_t pc0 = 2u * (tp - b * half8);
         const uint32_t r = fdiv(pc0, od.hz);
         const int Z0 = (int)(pc0 - r * (uint32_t)hz);
         const uint32_t Xu = fdiv(r, od.hy);
         const int Y = (int)(r - Xu * (uint32_t)hy), X = (int)Xu;
-        const int sub = s_sub[lr];
-        const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z0 + oz;
+        const int oct = m.oct[b], sub = m.sub[b];
+        const int ix = 2 * X + ((oct >> 2) & 1), iy = 2 * Y + ((oct >> 1) & 1), iz = 2 * Z0 + (oct & 1);
         const uint32_t at0 = ((uint32_t)(ix * a.ny + iy) * (uint32_t)a.nz + (uint32_t)iz) * (uint32_t)a.nsub + sub;
         const uint32_t at1 = at0 + 2u * (uint32_t)a.nsub;   // cell z + 2
-        const OctSlot* ts = tab + (lo * (uint32_t)nrank + lr) * mc;
+        const OctSlot* ts = m.tab + b * mc;
         f3 h0 = {0.f, 0.f, 0.f}, h1 = {0.f, 0.f, 0.f};
-        const int cn = s_cnt[lr];
+        const int cn = m.cnt[b];
         for (int q = 0; q < cn; ++q) {
             const OctSlot o = ts[q];
             int jx = X + o.ex, jy = Y + o.ey;
@@ -421,8 +410,7 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_pair(GeneralLaunch a, Oc
             h0.x += fmaf(o.w, s0.x, c0.x); h0.y += fmaf(o.w, s0.y, c0.y); h0.z += fmaf(o.w, s0.z, c0.z);
             h1.x += fmaf(o.w, s1.x, c1.x); h1.y += fmaf(o.w, s1.y, c1.y); h1.z += fmaf(o.w, s1.z, c1.z);
         }
-        const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
-        const uint32_t si0 = class_base + lr * (uint32_t)q8 + pc0;
+        const uint32_t si0 = m.base[b] + pc0;
         site_update<MOVE>(a, h0, (int64_t)si0, (int64_t)at0, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
         site_update<MOVE>(a, h1, (int64_t)si0 + 1, (int64_t)at1, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
     }
@@ -483,25 +471,17 @@ __device__ __forceinline__ bool oe_wait_ge(const OctEngineLaunch& e, int* status
 }
 
 template <int MOVE>
-__global__ void __launch_bounds__(kGenThreads, 4) k_octant_engine(GeneralLaunch a, OctDims od, OctEngineLaunch e) {
+__global__ void __launch_bounds__(kGenThreads, 4) k_octant_engine(const __grid_constant__ GeneralLaunch a, OctDims od,
+                                                                    const __grid_constant__ OctEngineLaunch e) {
     extern __shared__ __align__(16) unsigned char oe_smem[];
     const int mc = a.oct_maxcnt;
-    OctSlot* tab = reinterpret_cast<OctSlot*>(oe_smem);   // [ranks of the class][mc]
-    __shared__ int s_srank[kMaxSub], s_sofr[kMaxSub], s_rank0[kMaxSub + 1], s_sub[kMaxSub], s_cnt[kMaxSub];
+    const OctBlockSmem m = octant_smem(oe_smem, e.maxnb, mc);   // the current class's blocks
     __shared__ uint32_t s_task[3];
     __shared__ int s_go;
     __shared__ double tot[4];
-    const Layout& L = a.layout;
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < kMaxSub; ++k) { s_srank[k] = L.srank[k]; s_sofr[k] = L.sofr[k]; s_rank0[k] = e.rank0[k]; }
-        s_rank0[kMaxSub] = e.rank0[kMaxSub];
-    }
-    __syncthreads();
     const int hx = od.hx, hy = od.hyi, hz = od.hzi;
     const uint32_t hyz = (uint32_t)hy * (uint32_t)hz;
-    const int q8 = (int)L.q8;
-    const int ncls = 8 * e.ng;
+    const int ncls = e.ncls;
     const uint32_t per_phase = (uint32_t)a.n_rep * (uint32_t)hx;
     const uint32_t total = per_phase * (uint32_t)ncls * (uint32_t)e.n_sweeps;
     const int64_t N = a.natoms;
@@ -542,16 +522,9 @@ __global__ void __launch_bounds__(kGenThreads, 4) k_octant_engine(GeneralLaunch 
             }
         }
         const int sw = (int)(ph / (uint32_t)ncls), c = (int)ph - sw * ncls;
-        // classes o * ng + g, or, for shell-1 classes (class-major), g * 8 + o
-        const int oct = e.class_major ? (c & 7) : c / e.ng, gi = e.class_major ? (c >> 3) : c - oct * e.ng;
-        const int rank0 = s_rank0[gi], nrank = s_rank0[gi + 1] - rank0;
-        const int ox = (oct >> 2) & 1, oy = (oct >> 1) & 1, oz = oct & 1;
+        const int nb = e.start[c + 1] - e.start[c];
         if (c != cached) {   // the class's stencil, resolved as in k_octant_fast
-            octant_table(a, tab, mc, oct, 1, rank0, nrank, s_srank, s_sofr);
-            for (int lr = threadIdx.x; lr < nrank; lr += blockDim.x) {
-                s_sub[lr] = s_sofr[rank0 + lr];
-                s_cnt[lr] = a.st.count[s_sub[lr]];
-            }
+            octant_table(a, m, mc, e.code + e.start[c], nb);
             cached = c;
             __syncthreads();
         }
@@ -561,21 +534,20 @@ __global__ void __launch_bounds__(kGenThreads, 4) k_octant_engine(GeneralLaunch 
         float* __restrict__ sz = sy + N;
         const uint32_t sweep = a.sweep_ctr[rep] + a.sweep_offset + (uint32_t)sw;
         const float beta = (float)a.beta_rep[rep];
-        const uint32_t nsite = (uint32_t)nrank * hyz;
-        const uint32_t class_base = (uint32_t)((oct * a.nsub + rank0) * q8);
+        const uint32_t nsite = (uint32_t)nb * hyz;
         const int X = (int)u;
         float de = 0.f, dmx = 0.f, dmy = 0.f, dmz = 0.f;
         for (uint32_t t = threadIdx.x; t < nsite; t += blockDim.x) {
-            const uint32_t lr = fdiv(t, od.hyz);
-            const uint32_t rem = t - lr * hyz;
+            const uint32_t b = fdiv(t, od.hyz);
+            const uint32_t rem = t - b * hyz;
             const uint32_t Yu = fdiv(rem, od.hz);
             const int Z = (int)(rem - Yu * (uint32_t)hz), Y = (int)Yu;
-            const int sub = s_sub[lr];
-            const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z + oz;
+            const int oct = m.oct[b], sub = m.sub[b];
+            const int ix = 2 * X + ((oct >> 2) & 1), iy = 2 * Y + ((oct >> 1) & 1), iz = 2 * Z + (oct & 1);
             const uint32_t at = ((uint32_t)(ix * a.ny + iy) * (uint32_t)a.nz + (uint32_t)iz) * (uint32_t)a.nsub + sub;
-            const OctSlot* ts = tab + lr * mc;
+            const OctSlot* ts = m.tab + b * mc;
             f3 h = {0.f, 0.f, 0.f};
-            const int cn = s_cnt[lr];
+            const int cn = m.cnt[b];
             for (int q = 0; q < cn; ++q) {
                 const OctSlot o = ts[q];
                 int jx = X + o.ex, jy = Y + o.ey, jz = Z + o.ez;
@@ -589,7 +561,7 @@ __global__ void __launch_bounds__(kGenThreads, 4) k_octant_engine(GeneralLaunch 
                 h.y += fmaf(o.w, sj.y, cr.y);
                 h.z += fmaf(o.w, sj.z, cr.z);
             }
-            const uint32_t si = class_base + lr * (uint32_t)q8 + (uint32_t)X * hyz + rem;
+            const uint32_t si = m.base[b] + (uint32_t)X * hyz + rem;
             site_update<MOVE>(a, h, (int64_t)si, (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
         }
         if (a.partials) {
@@ -619,16 +591,18 @@ int octant_engine_grid(int* blocks) {
 }
 
 int launch_octant_engine(const GeneralLaunch& a, const OctEngineLaunch& e, cudaStream_t s) {
-    if (a.oct_maxcnt < 1 || e.ng < 1 || e.n_sweeps < 1 || e.grid < 1) return fail(ISING_ERR_ARG, "octant engine setup");
-    int maxr = 0;
-    for (int g = 0; g < e.ng; ++g) maxr = std::max(maxr, e.rank0[g + 1] - e.rank0[g]);
+    if (a.oct_maxcnt < 1 || e.ncls < 1 || e.n_sweeps < 1 || e.grid < 1 || e.maxnb < 1 || e.maxnb > kMaxOctBlocks)
+        return fail(ISING_ERR_ARG, "octant engine setup");
+    for (int c = 0; c < e.ncls; ++c)
+        if (e.start[c + 1] <= e.start[c] || e.start[c + 1] - e.start[c] > e.maxnb)
+            return fail(ISING_ERR_ARG, "octant engine: class list");
     OctDims od;
     od.q8 = make_div((uint32_t)a.layout.q8);
     od.hx = a.nx / 2; od.hyi = a.ny / 2; od.hzi = a.nz / 2;
     od.hz = make_div((uint32_t)od.hzi);
     od.hy = make_div((uint32_t)od.hyi);
     od.hyz = make_div((uint32_t)(od.hyi * od.hzi));
-    const size_t sm = (size_t)maxr * a.oct_maxcnt * sizeof(OctSlot);
+    const size_t sm = octant_smem_bytes(e.maxnb, a.oct_maxcnt);
     if (sm > 48u * 1024u) return fail(ISING_ERR_ARG, "octant engine: class stencil table exceeds 48 KB");
     if (a.move == 0) k_octant_engine<0><<<e.grid, kGenThreads, sm, s>>>(a, od, e);
     else k_octant_engine<1><<<e.grid, kGenThreads, sm, s>>>(a, od, e);
@@ -769,72 +743,88 @@ int octant_slots_for(int64_t n_sites, bool fast) {
     return (int)((n_sites + per - 1) / per);
 }
 
-int octant_class_slots(int64_t q8, int nrank, int noct, bool fast) {
-    return noct * octant_slots_for(q8 * nrank, fast);
+// blocks of one class launch: as many as keep the block stencils within 48 KB of shared memory
+static int octant_chunk(int maxcnt) {
+    if (maxcnt < 1) return 1;   // k_octant_colour: one launch per block
+    const int fit = (int)((48u * 1024u) / octant_smem_bytes(1, maxcnt));
+    return std::max(1, std::min(kMaxOctBlocks, fit));
 }
 
-int octant_class_launches(int nrank, int maxcnt, int noct) {
-    const size_t sm = (size_t)noct * nrank * maxcnt * sizeof(OctSlot) + 2 * (size_t)nrank * sizeof(int);
-    return (noct > 1 && (maxcnt < 1 || sm > 48u * 1024u)) ? noct : 1;
+int octant_class_launches(int nblocks, int maxcnt) {
+    const int c = octant_chunk(maxcnt);
+    return (nblocks + c - 1) / c;
 }
 
-int launch_octant_colour(const GeneralLaunch& a, int oct0, int noct, int rank0, int nrank, cudaStream_t s) {
-    const int64_t n = a.layout.q8 * nrank;   // sites of one octant
-    if (n <= 0) return ISING_OK;
-    if (oct0 < 0 || noct < 1 || oct0 + noct > 8 || rank0 < 0 || nrank < 1 || rank0 + nrank > a.nsub)
-        return fail(ISING_ERR_ARG, "octant class out of range");
-    const size_t tab = (size_t)nrank * a.oct_maxcnt * sizeof(OctSlot);
-    if (octant_class_launches(nrank, a.oct_maxcnt, noct) > 1) {
-        // one launch per octant, in octant order (the sites of the set are independent)
-        GeneralLaunch b = a;
-        for (int o = 0; o < noct; ++o) {
-            const int rc = launch_octant_colour(b, oct0 + o, 1, rank0, nrank, s);
+int octant_class_slots(int64_t q8, int nblocks, int maxcnt) {
+    const int c = octant_chunk(maxcnt);
+    int tot = 0;
+    for (int b0 = 0; b0 < nblocks; b0 += c) tot += octant_slots_for(q8 * std::min(c, nblocks - b0), maxcnt > 0);
+    return tot;
+}
+
+int launch_octant_class(const GeneralLaunch& a, const OctBlocks& bl, cudaStream_t s) {
+    if (bl.n < 1 || bl.n > kMaxOctBlocks) return fail(ISING_ERR_ARG, "octant class: 1 to 128 blocks");
+    for (int k = 0; k < bl.n; ++k)
+        if ((bl.code[k] & 15) >= a.nsub) return fail(ISING_ERR_ARG, "octant class block out of range");
+    const int64_t q8 = a.layout.q8;
+    const int chunk = octant_chunk(a.oct_maxcnt);
+    if (bl.n > chunk) {   // consecutive runs of blocks, one launch each (the class's sites are independent)
+        GeneralLaunch g = a;
+        for (int b0 = 0; b0 < bl.n; b0 += chunk) {
+            OctBlocks part{};
+            part.n = std::min(chunk, bl.n - b0);
+            for (int k = 0; k < part.n; ++k) part.code[k] = bl.code[b0 + k];
+            const int rc = launch_octant_class(g, part, s);
             if (rc != ISING_OK) return rc;
-            b.slot_base += octant_slots_for(n, a.oct_maxcnt > 0);
+            g.slot_base += octant_slots_for(q8 * part.n, a.oct_maxcnt > 0);
         }
         return ISING_OK;
     }
-    dim3 g(octant_slots_for(n, a.oct_maxcnt > 0), a.n_rep), b(kGenThreads);
-    if (a.oct_maxcnt > 0) {
-        // sites per thread: as many as keep about two waves of blocks (6 resident per SM);
-        // fewer blocks than partial slots leave the last slots at zero
-        int sms = 148;
-        {
-            int dev = 0;
-            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        }
-        const int64_t ntot = n * noct;
-        const int64_t per_launch = ntot * a.n_rep, want = 2LL * sms * 6 * kGenThreads;
-        const int spt = per_launch >= 4 * want ? 4 : (per_launch >= 2 * want ? 2 : 1);
-        g.x = (unsigned)((ntot + (int64_t)kGenThreads * spt - 1) / ((int64_t)kGenThreads * spt));
-        OctDims od;
-        od.q8 = make_div((uint32_t)a.layout.q8);
-        od.hx = a.nx / 2; od.hyi = a.ny / 2; od.hzi = a.nz / 2;
-        od.hz = make_div((uint32_t)od.hzi);
-        od.hy = make_div((uint32_t)od.hyi);
-        const size_t sm = (size_t)noct * tab + 2 * (size_t)nrank * sizeof(int);
-        if (od.hzi % 2 == 0) {   // site pairs along packed z
-            od.q8h = make_div((uint32_t)(a.layout.q8 / 2));
-            od.per_oct = make_div((uint32_t)(n / 2));
-            // <= octant_class_slots(q8, nrank, noct, true) blocks
-            g.x = (unsigned)((ntot / 2 + kGenThreads - 1) / kGenThreads);
-            if (a.move == 0) k_octant_pair<0><<<g, b, sm, s>>>(a, od, oct0, noct, rank0, nrank);
-            else k_octant_pair<1><<<g, b, sm, s>>>(a, od, oct0, noct, rank0, nrank);
-            ISG_CUDA(cudaGetLastError());
-            return ISING_OK;
-        }
-        od.per_oct = make_div((uint32_t)n);
-#define ISG_OF(S)                                                                                \
-    if (a.move == 0) k_octant_fast<0, S><<<g, b, sm, s>>>(a, od, oct0, noct, rank0, nrank);      \
-    else k_octant_fast<1, S><<<g, b, sm, s>>>(a, od, oct0, noct, rank0, nrank);
-        if (spt == 4) { ISG_OF(4) } else if (spt == 2) { ISG_OF(2) } else { ISG_OF(1) }
-#undef ISG_OF
+    dim3 b(kGenThreads);
+    if (a.oct_maxcnt < 1) {   // a single block: the cell-coordinate stencil
+        dim3 g(octant_slots_for(q8, false), a.n_rep);
+        const size_t sm = (size_t)a.st.nsub * kMaxSlots * sizeof(Slot) + kMaxSub * sizeof(int);
+        const int oct = bl.code[0] >> 4, rank = bl.code[0] & 15;
+        if (a.move == 0) k_octant_colour<0><<<g, b, sm, s>>>(a, oct, rank, 1);
+        else k_octant_colour<1><<<g, b, sm, s>>>(a, oct, rank, 1);
         ISG_CUDA(cudaGetLastError());
         return ISING_OK;
     }
-    size_t sm = (size_t)a.st.nsub * kMaxSlots * sizeof(Slot) + kMaxSub * sizeof(int);
-    if (a.move == 0) k_octant_colour<0><<<g, b, sm, s>>>(a, oct0, rank0, nrank);
-    else k_octant_colour<1><<<g, b, sm, s>>>(a, oct0, rank0, nrank);
+    // sites (pairs) per thread: as many as keep about two waves of blocks (6 resident per SM);
+    // fewer blocks than partial slots leave the last slots at zero
+    int sms = 148;
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const int64_t ntot = q8 * bl.n;
+    const int64_t per_launch = ntot * a.n_rep, want = 2LL * sms * 6 * kGenThreads;
+    OctDims od;
+    od.q8 = make_div((uint32_t)q8);
+    od.hx = a.nx / 2; od.hyi = a.ny / 2; od.hzi = a.nz / 2;
+    od.hz = make_div((uint32_t)od.hzi);
+    od.hy = make_div((uint32_t)od.hyi);
+    const size_t sm = octant_smem_bytes(bl.n, a.oct_maxcnt);
+    if (od.hzi % 2 == 0) {   // site pairs along packed z (q8 is even)
+        od.q8h = make_div((uint32_t)(q8 / 2));
+        const int ppt = per_launch / 2 >= 4 * want ? 4 : (per_launch / 2 >= 2 * want ? 2 : 1);
+        // <= octant_slots_for(ntot, true) blocks
+        dim3 g((unsigned)((ntot / 2 + (int64_t)kGenThreads * ppt - 1) / ((int64_t)kGenThreads * ppt)), a.n_rep);
+#define ISG_OP(P)                                                          \
+    if (a.move == 0) k_octant_pair<0, P><<<g, b, sm, s>>>(a, od, bl);      \
+    else k_octant_pair<1, P><<<g, b, sm, s>>>(a, od, bl);
+        if (ppt == 4) { ISG_OP(4) } else if (ppt == 2) { ISG_OP(2) } else { ISG_OP(1) }
+#undef ISG_OP
+        ISG_CUDA(cudaGetLastError());
+        return ISING_OK;
+    }
+    const int spt = per_launch >= 4 * want ? 4 : (per_launch >= 2 * want ? 2 : 1);
+    dim3 g((unsigned)((ntot + (int64_t)kGenThreads * spt - 1) / ((int64_t)kGenThreads * spt)), a.n_rep);
+#define ISG_OF(S)                                                          \
+    if (a.move == 0) k_octant_fast<0, S><<<g, b, sm, s>>>(a, od, bl);      \
+    else k_octant_fast<1, S><<<g, b, sm, s>>>(a, od, bl);
+    if (spt == 4) { ISG_OF(4) } else if (spt == 2) { ISG_OF(2) } else { ISG_OF(1) }
+#undef ISG_OF
     ISG_CUDA(cudaGetLastError());
     return ISING_OK;
 }

@@ -473,6 +473,56 @@ bool octant_groups(const Lattice& L, std::vector<int>* group, int* ngroups, std:
     return true;
 }
 
+// Colour classes of the octant blocks (cell octant o, sublattice s) of an octant-layout
+// crystal: block (o, s) reaches block (o', t) through a bond of the active shells from s to t
+// at cell offset d when o' = (o + d) & 1 per axis (every extent is even), and two blocks so
+// joined get different classes; a bond of a site to itself does not count.  DSatur (Brelaz,
+// CACM 22(4), 1979): the next block coloured is the uncoloured one with the most distinct
+// colours among its neighbours, ties broken by degree and then by the lower index, and it
+// takes the lowest colour free there.  out[k] = the blocks of class k as o * nsub + s,
+// ascending; false when a block reaches itself (the octant colouring does not apply).
+bool octant_block_classes(const Lattice& L, bool shell2, std::vector<std::vector<int>>* out) {
+    const int ns = L.nsub, n = 8 * ns;
+    std::vector<std::vector<char>> adj(n, std::vector<char>(n, 0));
+    for (int o = 0; o < 8; ++o) {
+        const int ox = (o >> 2) & 1, oy = (o >> 1) & 1, oz = o & 1;
+        for (int sh = 0; sh < (shell2 ? 2 : 1); ++sh)
+            for (int s = 0; s < ns; ++s)
+                for (const NbrSlot& q : L.shell[sh][s]) {
+                    if (q.sub == s && !q.dx && !q.dy && !q.dz) continue;   // the site itself
+                    const int o2 = (((ox + q.dx) & 1) << 2) | (((oy + q.dy) & 1) << 1) | ((oz + q.dz) & 1);
+                    const int u = o * ns + s, v = o2 * ns + q.sub;
+                    if (u == v) return false;
+                    adj[u][v] = adj[v][u] = 1;
+                }
+    }
+    std::vector<int> deg(n, 0), col(n, -1);
+    for (int u = 0; u < n; ++u)
+        for (int v = 0; v < n; ++v) deg[u] += adj[u][v];
+    int ncol = 0;
+    for (int step = 0; step < n; ++step) {
+        int best = -1, bsat = -1;
+        for (int v = 0; v < n; ++v) {
+            if (col[v] >= 0) continue;
+            std::vector<char> seen(ncol + 1, 0);
+            int sat = 0;
+            for (int w = 0; w < n; ++w)
+                if (adj[v][w] && col[w] >= 0 && !seen[col[w]]) { seen[col[w]] = 1; ++sat; }
+            if (sat > bsat || (sat == bsat && deg[v] > deg[best])) { best = v; bsat = sat; }
+        }
+        std::vector<char> used(ncol + 1, 0);
+        for (int w = 0; w < n; ++w)
+            if (adj[best][w] && col[w] >= 0) used[col[w]] = 1;
+        int c = 0;
+        while (used[c]) ++c;
+        col[best] = c;
+        ncol = std::max(ncol, c + 1);
+    }
+    out->assign(ncol, {});
+    for (int v = 0; v < n; ++v) (*out)[col[v]].push_back(v);
+    return true;
+}
+
 bool is_checkerboard_sc(const Lattice& L) {
     if (L.nsub != 1) return false;
     if ((L.nx & 1) || (L.ny & 1) || (L.nz & 1)) return false;

@@ -58,8 +58,8 @@ def test_octant_sweeps_replay_the_oracle(oracle, ib, cuda_ok, case):
     pm.set_spins(s)
     op, pp = _both_params(oracle, ib, **h)
     col, ncol = pm.colouring(pp)
-    if pm.layout == "octant":
-        assert ncol % 8 == 0 if "Jp" in h else ncol == 3   # without J': the shell-1 classes
+    if pm.layout == "octant":   # classes of octant blocks: 3 shell-1 classes, or 15 with J'
+        assert ncol == (15 if "Jp" in h else 3)
     elif "Jp" not in h:   # the two sublattices
         assert ncol == 2 and np.array_equal(col, np.arange(om.natoms) % 2)
     seed = 0x0C7A + case

@@ -81,9 +81,10 @@ def test_colouring_is_independent(oracle, ib):
     """Every colour class is an independent set of the active shells' bonds (a bond of a site
     to itself, which the reference's shell search gives BCC cells in shell 2, excepted).  BCC
     meshes of at least 4 cells per axis take sublattice planes, whose classes without J' are
-    the two sublattices; even hyper-kagome meshes the octant classes with J': class = octant *
-    groups + group with octant = (x&1, y&1, z&1) of the cell, and without J' its three shell-1
-    classes (4 of the 12 sublattices each, in every octant); other meshes a greedy colouring."""
+    the two sublattices; even hyper-kagome meshes classes of whole octant blocks (cell octant
+    (x&1, y&1, z&1), sublattice): without J' its three shell-1 classes (4 of the 12 sublattices
+    each, in every octant), with J' the 15 classes of a DSatur colouring of the 96 blocks (72
+    octant x sublattice-group classes before); other meshes a greedy colouring."""
     cases = (("SC", (6, 6, 6)), ("SC", (5, 5, 5)), ("BCC", (4, 4, 4)), ("BCC", (6, 4, 8)), ("BCC", (3, 4, 3)),
              ("BCC", (5, 6, 7)), ("HK", (4, 4, 4)), ("HK", (4, 6, 4)), ("HK", (3, 3, 3)))
     for kind, dims in cases:
@@ -112,14 +113,17 @@ def test_colouring_is_independent(oracle, ib):
                 subs = [sorted(set(np.flatnonzero(col == k) % nsub)) for k in range(3)]
                 assert sorted(len(x) for x in subs) == [4, 4, 4] and sorted(sum(subs, [])) == list(range(nsub))
             elif pm.layout == "octant":
-                assert n % 8 == 0
+                assert n == 15
                 nsub = len(frac)
-                for atom in range(0, pm.numAtoms, 7):
+                of_block = {}
+                for atom in range(pm.numAtoms):   # the colour is a function of the block
                     cell, sub = divmod(atom, nsub)
                     iz = cell % dims[2]
                     iy = (cell // dims[2]) % dims[1]
                     ix = cell // (dims[1] * dims[2])
-                    assert col[atom] // (n // 8) == ((ix & 1) << 2 | (iy & 1) << 1 | (iz & 1))
+                    blk = ((ix & 1) << 2 | (iy & 1) << 1 | (iz & 1), sub)
+                    assert of_block.setdefault(blk, col[atom]) == col[atom]
+                assert len(of_block) == 8 * nsub
             else:
                 deg = sum(len(pm.neighbours(0, s)) for s in shells)
                 assert n <= deg + 1  # greedy bound
