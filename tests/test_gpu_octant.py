@@ -21,6 +21,10 @@ CASES = [
     ("BCC", (4, 6, 8), dict(J=-1.0, Jp=0.2, Dz=0.3, B=0.2, K=0.05, bulk=False), 0, 0.0, 2.0),
     ("HK", (4, 4, 4), dict(J=-1.0, Dz=0.3, B=0.1, bulk=False), 1, 0.25, 1.0),
     ("HK", (4, 6, 4), dict(J=1.0, Jp=0.1, Dz=0.2, B=0.3, bulk=True), 0, 0.0, 3.0),
+    # 15 block classes with J' on the pair kernel (nz % 4 == 0) and on the one-site kernel
+    ("HK", (8, 8, 8), dict(J=-1.0, Jp=0.1, Dz=0.3, B=0.1, bulk=False), 1, 0.2, 1.5),
+    ("HK", (4, 4, 6), dict(J=-1.0, Jp=-0.2, Dz=0.4, B=0.2, bulk=False), 1, 0.3, 2.0),
+    ("HK", (6, 4, 6), dict(J=-1.0, Dz=0.4, B=0.2, bulk=False), 0, 0.0, 1.2),
 ]
 
 
