@@ -432,6 +432,7 @@ int enqueue_sweeps(ising_mesh* m, const SweepPlan& plan, int rep_first, int n_re
     g.natoms = L.natoms; g.nx = L.nx; g.ny = L.ny; g.nz = L.nz; g.nsub = L.nsub;
     g.n_rep = n_rep; g.rep_first = rep_first; g.beta_rep = d_beta_rep; g.sweep_ctr = m->d_sweep;
     g.seed = seed; g.ensemble = ensemble; g.move = move; g.r = (float)r;
+    philox_round_keys(seed, g.rk);
     g.ham = plan.ham; g.st = StencilDev{plan.d_slots, plan.d_count, L.nsub}; g.layout = m->layout;
     g.partials = partials; g.slots_per_rep = plan.slots_per_rep; g.status = m->d_status;
     g.demag = plan.demag; g.mu0 = (float)kMu0;
@@ -2002,8 +2003,7 @@ void ens_params(const ising_ensembles* s, int k, int rounds, int stall, EnsParam
     P->scheme = s->opt.scheme;
     P->stall_ens = stall;
     P->seed = s->opt.seed;
-    uint32_t k0 = (uint32_t)s->opt.seed, k1 = (uint32_t)(s->opt.seed >> 32);
-    for (int i = 0; i < 10; ++i) { P->rk[2 * i] = k0; P->rk[2 * i + 1] = k1; k0 += kPhiloxW0; k1 += kPhiloxW1; }
+    philox_round_keys(s->opt.seed, P->rk);
 }
 
 int ens_enqueue_launch(ising_ensembles* s, int k, int rounds, int stall) {

@@ -44,9 +44,28 @@ __device__ __forceinline__ float u01(uint32_t x) {
     return __uint_as_float((x >> 9) | 0x3f800000u) - 0.99999994f;
 }
 
+// Philox4x32-10 with the ten round keys precomputed (philox_round_keys) and taken from the
+// kernel parameters: each round is two 32x32->64 products and two three-input XORs, the
+// round keys constant-bank operands.  Same values as philox4x32<10>(c, philox_key(seed)).
+__device__ __forceinline__ uint4 philox_rk(uint4 c, const uint32_t* rk) {
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+        const uint64_t p0 = (uint64_t)kPhiloxM0 * c.x;
+        const uint64_t p1 = (uint64_t)kPhiloxM1 * c.z;
+        c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ rk[2 * i], (uint32_t)p1,
+                       (uint32_t)(p0 >> 32) ^ c.w ^ rk[2 * i + 1], (uint32_t)p0);
+    }
+    return c;
+}
+
 #endif  // __CUDACC__
 __host__ __device__ __forceinline__ uint2 philox_key(uint64_t seed) {
     return make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+}
+// rk[2i], rk[2i+1] = the key of round i: key + i * (W0, W1)
+inline void philox_round_keys(uint64_t seed, uint32_t* rk) {
+    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    for (int i = 0; i < 10; ++i) { rk[2 * i] = k0; rk[2 * i + 1] = k1; k0 += kPhiloxW0; k1 += kPhiloxW1; }
 }
 
 // ---------------------------------------------------------------- small vector helpers

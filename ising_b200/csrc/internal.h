@@ -196,6 +196,7 @@ struct GeneralLaunch {
     const uint32_t* sweep_ctr;
     uint32_t sweep_offset;
     uint64_t seed;
+    uint32_t rk[20];         // Philox round keys of seed (philox_round_keys)
     uint32_t ensemble;
     int move;
     float r;

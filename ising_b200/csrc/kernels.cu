@@ -70,8 +70,13 @@ __device__ __forceinline__ f3 stencil_field(const float* sx, const float* sy, co
 }
 
 // Metropolis update of one site (ix, iy, iz, sub), reference atom index `at`, with the local
-// field of its stencil; accepted moves add to the running sums.
-template <int MOVE>
+// field of its stencil; accepted moves add to the running sums.  RK: Philox with the launch's
+// precomputed round keys (constant-bank operands; BCC 96^3 x 16 5.56e10 -> 6.44e10
+// updates/s); false: the key schedule computed in registers, for loops that run several
+// updates per thread, where the compiler keeps the 20 round keys in registers instead
+// (hyper-kagome's 4 pairs per thread: 6.12e10 -> 5.07e10 with round keys at 48 registers).
+// Both give the same numbers.
+template <int MOVE, bool RK = true>
 __device__ __forceinline__ void site_update(const GeneralLaunch& a, f3 h, int64_t si, int64_t at, float* sx,
                                             float* sy, float* sz, uint32_t sweep, int rep, float beta, float& de,
                                             float& dmx, float& dmy, float& dmz) {
@@ -84,8 +89,8 @@ __device__ __forceinline__ void site_update(const GeneralLaunch& a, f3 h, int64_
         h.z = fmaf(-a.mu0, a.demag[2 * N + si], h.z);
     }
     const f3 s = {sx[si], sy[si], sz[si]};
-    const uint4 r4 = philox4x32<10>(make_uint4((uint32_t)at, sweep, (uint32_t)rep, (a.ensemble << 8) | kTagSweep),
-                                    philox_key(a.seed));
+    const uint4 c4 = make_uint4((uint32_t)at, sweep, (uint32_t)rep, (a.ensemble << 8) | kTagSweep);
+    const uint4 r4 = RK ? philox_rk(c4, a.rk) : philox4x32<10>(c4, philox_key(a.seed));
     const f3 sp = propose<MOVE>(s, u01(r4.x), u01(r4.y), u01(r4.z), a.r);
     float dE = (sp.x - s.x) * h.x + (sp.y - s.y) * h.y + (sp.z - s.z) * h.z;
     if (H.K != 0.f) {
@@ -411,8 +416,9 @@ __global__ void __launch_bounds__(kGenThreads, 5) k_octant_pair(const __grid_con
             h1.x += fmaf(o.w, s1.x, c1.x); h1.y += fmaf(o.w, s1.y, c1.y); h1.z += fmaf(o.w, s1.z, c1.z);
         }
         const uint32_t si0 = m.base[b] + pc0;
-        site_update<MOVE>(a, h0, (int64_t)si0, (int64_t)at0, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
-        site_update<MOVE>(a, h1, (int64_t)si0 + 1, (int64_t)at1, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+        site_update<MOVE, PPT == 1>(a, h0, (int64_t)si0, (int64_t)at0, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+        site_update<MOVE, PPT == 1>(a, h1, (int64_t)si0 + 1, (int64_t)at1, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
+                                    dmz);
     }
     if (a.partials) {
         __shared__ double tot[4];

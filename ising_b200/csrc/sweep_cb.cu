@@ -103,8 +103,7 @@ int launch_cb_sweep(const CbLaunch& a, int move, int dmi, cudaStream_t s) {
     P.g.ensemble = a.ensemble;
     P.g.r = a.r;
     {
-        uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
-        for (int i = 0; i < 10; ++i) { P.rk[2 * i] = k0; P.rk[2 * i + 1] = k1; k0 += kPhiloxW0; k1 += kPhiloxW1; }
+        philox_round_keys(a.seed, P.rk);
     }
     // block = (W/2 pair lanes) x (rows per block); about ISG_CB_BLOCKS_PER_SM resident blocks
     // per SM across the launch, at least one per replica

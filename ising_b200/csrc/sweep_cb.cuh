@@ -45,18 +45,6 @@ struct CbGeom {
     float r;                // ball-step radius
 };
 
-// Philox4x32-10 with the round keys taken from the kernel parameters.
-__device__ __forceinline__ uint4 philox_rk(uint4 c, const uint32_t* rk) {
-#pragma unroll
-    for (int i = 0; i < 10; ++i) {
-        const uint64_t p0 = (uint64_t)kPhiloxM0 * c.x;
-        const uint64_t p1 = (uint64_t)kPhiloxM1 * c.z;
-        c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ rk[2 * i], (uint32_t)p1,
-                       (uint32_t)(p0 >> 32) ^ c.w ^ rk[2 * i + 1], (uint32_t)p0);
-    }
-    return c;
-}
-
 // Trial spins for a pair of sites with packed arithmetic; the MUFU approximations stay scalar.
 template <int MOVE>
 __device__ __forceinline__ void propose2(const float2* s, uint4 ra, uint4 rb, float r, float2* sp) {

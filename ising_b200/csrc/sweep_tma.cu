@@ -94,17 +94,6 @@ struct TmaParams {
     uint32_t rk[20];     // Philox round keys
 };
 
-__device__ __forceinline__ uint4 philox_rk(uint4 c, const uint32_t* rk) {
-#pragma unroll
-    for (int i = 0; i < 10; ++i) {
-        const uint64_t p0 = (uint64_t)kPhiloxM0 * c.x;
-        const uint64_t p1 = (uint64_t)kPhiloxM1 * c.z;
-        c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ rk[2 * i], (uint32_t)p1,
-                       (uint32_t)(p0 >> 32) ^ c.w ^ rk[2 * i + 1], (uint32_t)p0);
-    }
-    return c;
-}
-
 template <int MOVE>
 __device__ __forceinline__ v23 propose2(const v23& s, uint4 ra, uint4 rb, float r) {
     const v2 u0 = u01x2(ra.x, rb.x), u1 = u01x2(ra.y, rb.y);
@@ -389,8 +378,7 @@ int launch_cb_tma(const CbLaunch& a, int move, int dmi, cudaStream_t s) {
     P.nchunk = ((uint32_t)a.nx + XC - 1) / XC;
     P.half = (uint32_t)(a.natoms / 2);
     {
-        uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
-        for (int i = 0; i < 10; ++i) { P.rk[2 * i] = k0; P.rk[2 * i + 1] = k1; k0 += kPhiloxW0; k1 += kPhiloxW1; }
+        philox_round_keys(a.seed, P.rk);
     }
     const size_t sm = sizeof(float) * ((size_t)kOthStages * 3 * (RS + 2) * P.W + (size_t)kOwnStages * 3 * RS * P.W);
     // whole warps only: the block reduction shuffles with a full mask
