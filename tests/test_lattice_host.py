@@ -12,7 +12,13 @@ CASES = [
 ]
 
 
+FCC_CELL = (np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]], np.float32),
+            (1.0, 1.0, 1.0, 90.0, 90.0, 90.0))
+
+
 def _cell(oracle, kind):
+    if kind == "FCC":   # not one of the reference's cells: a 4-sublattice check of the colourings
+        return FCC_CELL
     if kind == "SC":
         return oracle.SC_CELL
     if kind == "BCC":
@@ -84,16 +90,20 @@ def test_colouring_is_independent(oracle, ib):
     the two sublattices; even hyper-kagome meshes classes of whole octant blocks (cell octant
     (x&1, y&1, z&1), sublattice): without J' its three shell-1 classes (4 of the 12 sublattices
     each, in every octant), with J' the 15 classes of a DSatur colouring of the 96 blocks (72
-    octant x sublattice-group classes before); other meshes a greedy colouring."""
+    octant x sublattice-group classes before); other meshes a greedy colouring.  An FCC cell
+    (4 sublattices, not a reference cell) with even extents takes octant order too: without J'
+    its 4 sublattices are the classes, with J' 10 block classes."""
     cases = (("SC", (6, 6, 6)), ("SC", (5, 5, 5)), ("BCC", (4, 4, 4)), ("BCC", (6, 4, 8)), ("BCC", (3, 4, 3)),
-             ("BCC", (5, 6, 7)), ("HK", (4, 4, 4)), ("HK", (4, 6, 4)), ("HK", (3, 3, 3)))
+             ("BCC", (5, 6, 7)), ("HK", (4, 4, 4)), ("HK", (4, 6, 4)), ("HK", (3, 3, 3)),
+             ("FCC", (4, 4, 4)), ("FCC", (6, 4, 6)), ("FCC", (5, 5, 5)))
+    n_classes = {("HK", False): 3, ("HK", True): 15, ("FCC", False): 4, ("FCC", True): 10}
     for kind, dims in cases:
         frac, (a, b, c, ab, bc, ca) = _cell(oracle, kind)
         pm = ib.ChainMesh(*dims, frac, a, b, c, ab, bc, ca, device=-1)
         even = all(d % 2 == 0 for d in dims)
         want = ("checkerboard" if kind == "SC" and dims[2] % 4 == 0 and even
                 else "sublattice" if kind == "BCC" and min(dims) >= 4
-                else "octant" if kind == "HK" and even else "reference")
+                else "octant" if kind in ("HK", "FCC") and even else "reference")
         assert pm.layout == want, (kind, dims, pm.layout)
         for Jp in (0.0, 0.2):
             col, n = pm.colouring(ib.params(J=-1.0, J_prime=Jp))
@@ -107,13 +117,15 @@ def test_colouring_is_independent(oracle, ib):
                 assert n == 2 and pm.checkerboard
             if pm.layout == "sublattice" and Jp == 0.0:
                 assert n == 2 and np.array_equal(col, np.arange(pm.numAtoms) % 2)
-            elif pm.layout == "octant" and Jp == 0.0:
-                assert n == 3
+            elif pm.layout == "octant" and Jp == 0.0:   # whole sublattices, every octant
+                assert n == n_classes[(kind, False)]
                 nsub = len(frac)
-                subs = [sorted(set(np.flatnonzero(col == k) % nsub)) for k in range(3)]
-                assert sorted(len(x) for x in subs) == [4, 4, 4] and sorted(sum(subs, [])) == list(range(nsub))
+                subs = [sorted(set(np.flatnonzero(col == k) % nsub)) for k in range(n)]
+                assert sorted(sum(subs, [])) == list(range(nsub))
+                if kind == "HK":
+                    assert sorted(len(x) for x in subs) == [4, 4, 4]
             elif pm.layout == "octant":
-                assert n == 15
+                assert n == n_classes[(kind, True)]
                 nsub = len(frac)
                 of_block = {}
                 for atom in range(pm.numAtoms):   # the colour is a function of the block
