@@ -95,7 +95,7 @@ template <int MOVE>
 __device__ __forceinline__ f3 propose(f3 s, float u0, float u1, float u2, float r) {
     const float cz = fmaf(2.0f, u0, -1.0f);                       // exact
     const float st = ax_sqrt(fmaf(-cz, cz, 1.0f));
-    const float ph = 6.28318531f * (u1 - 0.5f);                    // azimuth in (-pi, pi)
+    const float ph = fmaf(6.28318531f, u1, -3.14159265f);          // azimuth in (-pi, pi), as propose2
     f3 v = {st * ax_cos(ph), st * ax_sin(ph), cz};
     if (MOVE == 1) {
         const float rho = r * ax_ex2(0.33333334f * ax_lg2(u2));   // r * cbrt(u2)
@@ -128,6 +128,41 @@ __device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
     const uint32_t t = __umulhi(f.m, n);
     return (t + ((n - t) >> 1)) >> (f.l - 1);
 }
+#endif  // __CUDACC__
+
+#if defined(__CUDACC__)
+// Trial spins for a pair of sites with packed arithmetic; the MUFU approximations stay scalar.
+template <int MOVE>
+__device__ __forceinline__ void propose2(const float2* s, uint4 ra, uint4 rb, float r, float2* sp) {
+    const float2 one = make_float2(1.f, 1.f);
+    const float2 u0 = __fadd2_rn(make_float2(__uint_as_float((ra.x >> 9) | 0x3f800000u),
+                                             __uint_as_float((rb.x >> 9) | 0x3f800000u)), make_float2(-0.99999994f, -0.99999994f));
+    const float2 u1 = __fadd2_rn(make_float2(__uint_as_float((ra.y >> 9) | 0x3f800000u),
+                                             __uint_as_float((rb.y >> 9) | 0x3f800000u)), make_float2(-0.99999994f, -0.99999994f));
+    const float2 cz = __ffma2_rn(make_float2(2.f, 2.f), u0, make_float2(-1.f, -1.f));
+    const float2 q = __ffma2_rn(make_float2(-cz.x, -cz.y), cz, one);
+    const float2 ph = __ffma2_rn(make_float2(6.28318531f, 6.28318531f), u1, make_float2(-3.14159265f, -3.14159265f));
+    const float2 st = make_float2(ax_sqrt(q.x), ax_sqrt(q.y));
+    float2 vx = __fmul2_rn(st, make_float2(ax_cos(ph.x), ax_cos(ph.y)));
+    float2 vy = __fmul2_rn(st, make_float2(ax_sin(ph.x), ax_sin(ph.y)));
+    float2 vz = cz;
+    if (MOVE == 1) {
+        const float2 u2 = __fadd2_rn(make_float2(__uint_as_float((ra.z >> 9) | 0x3f800000u),
+                                                 __uint_as_float((rb.z >> 9) | 0x3f800000u)), make_float2(-0.99999994f, -0.99999994f));
+        const float2 lg = __fmul2_rn(make_float2(ax_lg2(u2.x), ax_lg2(u2.y)), make_float2(0.33333334f, 0.33333334f));
+        const float2 rho = __fmul2_rn(make_float2(r, r), make_float2(ax_ex2(lg.x), ax_ex2(lg.y)));
+        vx = __ffma2_rn(rho, vx, s[0]);
+        vy = __ffma2_rn(rho, vy, s[1]);
+        vz = __ffma2_rn(rho, vz, s[2]);
+        const float2 n2 = __ffma2_rn(vx, vx, __ffma2_rn(vy, vy, __fmul2_rn(vz, vz)));
+        const float2 rn = make_float2(ax_rsqrt(n2.x), ax_rsqrt(n2.y));
+        vx = __fmul2_rn(vx, rn);
+        vy = __fmul2_rn(vy, rn);
+        vz = __fmul2_rn(vz, rn);
+    }
+    sp[0] = vx; sp[1] = vy; sp[2] = vz;
+}
+
 #endif  // __CUDACC__
 
 // ---------------------------------------------------------------- kernel-facing structs

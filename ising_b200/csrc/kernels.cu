@@ -92,17 +92,71 @@ __device__ __forceinline__ void site_update(const GeneralLaunch& a, f3 h, int64_
     const uint4 c4 = make_uint4((uint32_t)at, sweep, (uint32_t)rep, (a.ensemble << 8) | kTagSweep);
     const uint4 r4 = RK ? philox_rk(c4, a.rk) : philox4x32<10>(c4, philox_key(a.seed));
     const f3 sp = propose<MOVE>(s, u01(r4.x), u01(r4.y), u01(r4.z), a.r);
-    float dE = (sp.x - s.x) * h.x + (sp.y - s.y) * h.y + (sp.z - s.z) * h.z;
+    // every operation rounded as written, so that a lane of site_update_pair gives the same
+    const float dx = __fsub_rn(sp.x, s.x), dy = __fsub_rn(sp.y, s.y), dz = __fsub_rn(sp.z, s.z);
+    float dE = fmaf(dx, h.x, fmaf(dy, h.y, __fmul_rn(dz, h.z)));
     if (H.K != 0.f) {
-        const float e1 = sp.x * H.kx + sp.y * H.ky + sp.z * H.kz;
-        const float e0 = s.x * H.kx + s.y * H.ky + s.z * H.kz;
-        dE -= H.K * (e1 * e1 - e0 * e0);
+        const float e1 = fmaf(sp.x, H.kx, fmaf(sp.y, H.ky, __fmul_rn(sp.z, H.kz)));
+        const float e0 = fmaf(s.x, H.kx, fmaf(s.y, H.ky, __fmul_rn(s.z, H.kz)));
+        dE = fmaf(-H.K, __fmul_rn(__fsub_rn(e1, e0), __fadd_rn(e1, e0)), dE);
     }
     if (!(dE == dE)) atomicOr(a.status, kStatNan);
     if ((dE <= 0.f) || (u01(r4.w) < __expf(-beta * dE))) {
         sx[si] = sp.x; sy[si] = sp.y; sz[si] = sp.z;
-        de += dE; dmx += sp.x - s.x; dmy += sp.y - s.y; dmz += sp.z - s.z;
+        de += dE; dmx += dx; dmy += dy; dmz += dz;
     }
+}
+
+// The update of the site pair (si, si + 1) of one row (si even; reference atoms at0, at1)
+// with its two fields in the lanes of packed FP32x2 (hx, hy, hz): the pair's spins are read as
+// one aligned pair per component, the proposals (propose2), energy changes and anisotropy run
+// in packed arithmetic, the decisions per lane.  Each lane performs site_update's operations
+// in the same order and rounding, so the pair equals two site_update calls bit for bit.
+template <int MOVE, bool RK = true>
+__device__ __forceinline__ void site_update_pair(const GeneralLaunch& a, float2 hx, float2 hy, float2 hz, int64_t si,
+                                                 uint32_t at0, uint32_t at1, float* sx, float* sy, float* sz,
+                                                 uint32_t sweep, int rep, float beta, float& de, float& dmx, float& dmy,
+                                                 float& dmz) {
+    const HamDev& H = a.ham;
+    hz = __fadd2_rn(hz, make_float2(-H.Bz, -H.Bz));
+    if (a.demag) {   // -mu_0 S.H of calculateHeisenbergEnergy (src/energyMin.f90:163-167)
+        const int64_t N = a.natoms;
+        const float2 nm = make_float2(-a.mu0, -a.mu0);
+        hx = __ffma2_rn(nm, *reinterpret_cast<const float2*>(a.demag + si), hx);
+        hy = __ffma2_rn(nm, *reinterpret_cast<const float2*>(a.demag + N + si), hy);
+        hz = __ffma2_rn(nm, *reinterpret_cast<const float2*>(a.demag + 2 * N + si), hz);
+    }
+    float2 s[3] = {*reinterpret_cast<const float2*>(sx + si), *reinterpret_cast<const float2*>(sy + si),
+                   *reinterpret_cast<const float2*>(sz + si)};
+    const uint32_t cw = (a.ensemble << 8) | kTagSweep;
+    const uint4 ca = make_uint4(at0, sweep, (uint32_t)rep, cw), cb = make_uint4(at1, sweep, (uint32_t)rep, cw);
+    const uint4 ra = RK ? philox_rk(ca, a.rk) : philox4x32<10>(ca, philox_key(a.seed));
+    const uint4 rb = RK ? philox_rk(cb, a.rk) : philox4x32<10>(cb, philox_key(a.seed));
+    float2 sp[3];
+    propose2<MOVE>(s, ra, rb, a.r, sp);
+    const float2 m1 = make_float2(-1.f, -1.f);
+    const float2 dx = __ffma2_rn(s[0], m1, sp[0]), dy = __ffma2_rn(s[1], m1, sp[1]), dz = __ffma2_rn(s[2], m1, sp[2]);
+    float2 dE = __ffma2_rn(dx, hx, __ffma2_rn(dy, hy, __fmul2_rn(dz, hz)));
+    if (H.K != 0.f) {
+        const float2 kx = make_float2(H.kx, H.kx), ky = make_float2(H.ky, H.ky), kz = make_float2(H.kz, H.kz);
+        const float2 e1 = __ffma2_rn(sp[0], kx, __ffma2_rn(sp[1], ky, __fmul2_rn(sp[2], kz)));
+        const float2 e0 = __ffma2_rn(s[0], kx, __ffma2_rn(s[1], ky, __fmul2_rn(s[2], kz)));
+        dE = __ffma2_rn(make_float2(-H.K, -H.K), __fmul2_rn(__ffma2_rn(e0, m1, e1), __fadd2_rn(e1, e0)), dE);
+    }
+    if (!(dE.x == dE.x) || !(dE.y == dE.y)) atomicOr(a.status, kStatNan);
+    const bool acc0 = (dE.x <= 0.f) || (u01(ra.w) < __expf(-beta * dE.x));
+    const bool acc1 = (dE.y <= 0.f) || (u01(rb.w) < __expf(-beta * dE.y));
+    if (acc0 && acc1) {
+        *reinterpret_cast<float2*>(sx + si) = sp[0];
+        *reinterpret_cast<float2*>(sy + si) = sp[1];
+        *reinterpret_cast<float2*>(sz + si) = sp[2];
+    } else if (acc0) {
+        sx[si] = sp[0].x; sy[si] = sp[1].x; sz[si] = sp[2].x;
+    } else if (acc1) {
+        sx[si + 1] = sp[0].y; sy[si + 1] = sp[1].y; sz[si + 1] = sp[2].y;
+    }
+    if (acc0) { de += dE.x; dmx += dx.x; dmy += dy.x; dmz += dz.x; }
+    if (acc1) { de += dE.y; dmx += dx.y; dmy += dy.y; dmz += dz.y; }
 }
 
 template <int MOVE>
@@ -416,9 +470,8 @@ __global__ void __launch_bounds__(kGenThreads, 5) k_octant_pair(const __grid_con
             h1.x += fmaf(o.w, s1.x, c1.x); h1.y += fmaf(o.w, s1.y, c1.y); h1.z += fmaf(o.w, s1.z, c1.z);
         }
         const uint32_t si0 = m.base[b] + pc0;
-        site_update<MOVE, PPT == 1>(a, h0, (int64_t)si0, (int64_t)at0, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
-        site_update<MOVE, PPT == 1>(a, h1, (int64_t)si0 + 1, (int64_t)at1, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
-                                    dmz);
+        site_update_pair<MOVE, PPT == 1>(a, make_float2(h0.x, h1.x), make_float2(h0.y, h1.y), make_float2(h0.z, h1.z),
+                                         (int64_t)si0, at0, at1, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
     }
     if (a.partials) {
         __shared__ double tot[4];
@@ -631,7 +684,7 @@ int bip_slots_per_class() { return 148 * kBipBlocksPerSM; }
 struct BipRow { f3 lo, hi, e; };   // z-sites j, j + 1 and the edge value of one row
 
 template <int MOVE>
-__global__ void __launch_bounds__(kGenThreads) k_bip_sweep(GeneralLaunch a, BipClass bc, int sub, uint32_t rb,
+__global__ void __launch_bounds__(kGenThreads, 3) k_bip_sweep(GeneralLaunch a, BipClass bc, int sub, uint32_t rb,
                                                             uint32_t nseg, FastDiv div_seg) {
     const int rl = blockIdx.y;
     const int rep = a.rep_first + rl;
@@ -704,13 +757,11 @@ __global__ void __launch_bounds__(kGenThreads) k_bip_sweep(GeneralLaunch a, BipC
             add_row(c0, 2, hx, hy, hz);   // (0, 1)
             add_row(p1, 4, hx, hy, hz);   // (1, 0)
             add_row(c1, 6, hx, hy, hz);   // (1, 1)
-            const f3 h0 = {hx.x, hy.x, hz.x}, h1 = {hx.y, hy.y, hz.y};
             p0 = c0;
             p1 = c1;
             const int64_t own = (((int64_t)sub * nx + ix) * ny + iy) * nz + j;
-            const int64_t at = (((int64_t)ix * ny + iy) * nz + j) * 2 + sub;
-            site_update<MOVE>(a, h0, own, at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
-            site_update<MOVE>(a, h1, own + 1, at + 2, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+            const uint32_t at = (uint32_t)((((int64_t)ix * ny + iy) * nz + j) * 2 + sub);
+            site_update_pair<MOVE>(a, hx, hy, hz, own, at, at + 2u, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
         }
     }
     if (a.partials) {

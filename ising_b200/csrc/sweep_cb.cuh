@@ -45,38 +45,6 @@ struct CbGeom {
     float r;                // ball-step radius
 };
 
-// Trial spins for a pair of sites with packed arithmetic; the MUFU approximations stay scalar.
-template <int MOVE>
-__device__ __forceinline__ void propose2(const float2* s, uint4 ra, uint4 rb, float r, float2* sp) {
-    const float2 one = make_float2(1.f, 1.f);
-    const float2 u0 = __fadd2_rn(make_float2(__uint_as_float((ra.x >> 9) | 0x3f800000u),
-                                             __uint_as_float((rb.x >> 9) | 0x3f800000u)), make_float2(-0.99999994f, -0.99999994f));
-    const float2 u1 = __fadd2_rn(make_float2(__uint_as_float((ra.y >> 9) | 0x3f800000u),
-                                             __uint_as_float((rb.y >> 9) | 0x3f800000u)), make_float2(-0.99999994f, -0.99999994f));
-    const float2 cz = __ffma2_rn(make_float2(2.f, 2.f), u0, make_float2(-1.f, -1.f));
-    const float2 q = __ffma2_rn(make_float2(-cz.x, -cz.y), cz, one);
-    const float2 ph = __ffma2_rn(make_float2(6.28318531f, 6.28318531f), u1, make_float2(-3.14159265f, -3.14159265f));
-    const float2 st = make_float2(ax_sqrt(q.x), ax_sqrt(q.y));
-    float2 vx = __fmul2_rn(st, make_float2(ax_cos(ph.x), ax_cos(ph.y)));
-    float2 vy = __fmul2_rn(st, make_float2(ax_sin(ph.x), ax_sin(ph.y)));
-    float2 vz = cz;
-    if (MOVE == 1) {
-        const float2 u2 = __fadd2_rn(make_float2(__uint_as_float((ra.z >> 9) | 0x3f800000u),
-                                                 __uint_as_float((rb.z >> 9) | 0x3f800000u)), make_float2(-0.99999994f, -0.99999994f));
-        const float2 lg = __fmul2_rn(make_float2(ax_lg2(u2.x), ax_lg2(u2.y)), make_float2(0.33333334f, 0.33333334f));
-        const float2 rho = __fmul2_rn(make_float2(r, r), make_float2(ax_ex2(lg.x), ax_ex2(lg.y)));
-        vx = __ffma2_rn(rho, vx, s[0]);
-        vy = __ffma2_rn(rho, vy, s[1]);
-        vz = __ffma2_rn(rho, vz, s[2]);
-        const float2 n2 = __ffma2_rn(vx, vx, __ffma2_rn(vy, vy, __fmul2_rn(vz, vz)));
-        const float2 rn = make_float2(ax_rsqrt(n2.x), ax_rsqrt(n2.y));
-        vx = __fmul2_rn(vx, rn);
-        vy = __fmul2_rn(vy, rn);
-        vz = __fmul2_rn(vz, rn);
-    }
-    sp[0] = vx; sp[1] = vy; sp[2] = vz;
-}
-
 // The two Philox draws of the site pair (j, j+1) of packed row `row` (parity p): counters
 // (reference atom index, sweep, replica, ensemble << 8 | sweep tag).
 __device__ __forceinline__ void pair_draws(const CbGeom& P, const uint32_t* rk, uint32_t row, uint32_t j,
