@@ -320,6 +320,18 @@ __device__ __forceinline__ void octant_table(const GeneralLaunch& a, const OctBl
     }
 }
 
+// One bond's term of a site's local field, h += w S_j + S_j x D, every operation rounded as
+// written; k_octant_pair computes the same terms for its two sites in the lanes of FP32x2, so
+// the octant kernels agree bit for bit.
+__device__ __forceinline__ void bond_term(f3& h, const f3& sj, const OctSlot& o) {
+    const float cx = fmaf(sj.y, o.Dz, __fmul_rn(sj.z, -o.Dy));
+    const float cy = fmaf(sj.z, o.Dx, __fmul_rn(sj.x, -o.Dz));
+    const float cz = fmaf(sj.x, o.Dy, __fmul_rn(sj.y, -o.Dx));
+    h.x = __fadd_rn(h.x, fmaf(o.w, sj.x, cx));
+    h.y = __fadd_rn(h.y, fmaf(o.w, sj.y, cy));
+    h.z = __fadd_rn(h.z, fmaf(o.w, sj.z, cz));
+}
+
 // block sums of the four running partials: FP32 within a warp (a warp's few sites), FP64
 // across warps
 __device__ __forceinline__ void block_sum4_fd(float v0, float v1, float v2, float v3, double* out /* smem 4 */) {
@@ -384,10 +396,7 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(const __grid_consta
             jz += jz < 0 ? hz : 0; jz -= jz >= hz ? hz : 0;
             const uint32_t j = (uint32_t)o.plane + (uint32_t)((jx * hy + jy) * hz + jz);
             const f3 sj = {sx[j], sy[j], sz[j]};
-            const f3 c = cross(sj, mk(o.Dx, o.Dy, o.Dz));
-            h.x += fmaf(o.w, sj.x, c.x);
-            h.y += fmaf(o.w, sj.y, c.y);
-            h.z += fmaf(o.w, sj.z, c.z);
+            bond_term(h, sj, o);
         }
         site_update<MOVE>(a, h, (int64_t)(m.base[b] + pc), (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy,
                           dmz);
@@ -406,7 +415,7 @@ __global__ void __launch_bounds__(kGenThreads) k_octant_fast(const __grid_consta
 // 0, so a pair never straddles a row) of one row.  The pair shares the row decode and, per
 // stencil slot, the x/y wrap and the row base; a slot with no packed z offset reads both
 // neighbours as one aligned pair per component.  Each site's field is summed in slot order
-// with the stencil's expression, so the update equals k_octant_fast's bit for bit.
+// with bond_term's operations in FP32x2 lanes, so the update equals k_octant_fast's bit for bit.
 template <int MOVE, int PPT>
 __global__ void __launch_bounds__(kGenThreads, 5) k_octant_pair(const __grid_constant__ GeneralLaunch a, OctDims od,
                                                                  const __grid_constant__ OctBlocks bl) {
@@ -442,7 +451,7 @@ __global__ void __launch_bounds__(kGenThreads, 5) k_octant_pair(const __grid_con
         const uint32_t at0 = ((uint32_t)(ix * a.ny + iy) * (uint32_t)a.nz + (uint32_t)iz) * (uint32_t)a.nsub + sub;
         const uint32_t at1 = at0 + 2u * (uint32_t)a.nsub;   // cell z + 2
         const OctSlot* ts = m.tab + b * mc;
-        f3 h0 = {0.f, 0.f, 0.f}, h1 = {0.f, 0.f, 0.f};
+        float2 hx2 = make_float2(0.f, 0.f), hy2 = hx2, hz2 = hx2;   // the two sites' fields
         const int cn = m.cnt[b];
         for (int q = 0; q < cn; ++q) {
             const OctSlot o = ts[q];
@@ -464,14 +473,19 @@ __global__ void __launch_bounds__(kGenThreads, 5) k_octant_pair(const __grid_con
                 s0 = {sx[rb + jz0], sy[rb + jz0], sz[rb + jz0]};
                 s1 = {sx[rb + jz1], sy[rb + jz1], sz[rb + jz1]};
             }
-            const f3 D = mk(o.Dx, o.Dy, o.Dz);
-            const f3 c0 = cross(s0, D), c1 = cross(s1, D);
-            h0.x += fmaf(o.w, s0.x, c0.x); h0.y += fmaf(o.w, s0.y, c0.y); h0.z += fmaf(o.w, s0.z, c0.z);
-            h1.x += fmaf(o.w, s1.x, c1.x); h1.y += fmaf(o.w, s1.y, c1.y); h1.z += fmaf(o.w, s1.z, c1.z);
+            // bond_term for both sites in the lanes of FP32x2
+            const float2 PX = make_float2(s0.x, s1.x), PY = make_float2(s0.y, s1.y), PZ = make_float2(s0.z, s1.z);
+            const float2 w2 = make_float2(o.w, o.w);
+            const float2 cx = __ffma2_rn(PY, make_float2(o.Dz, o.Dz), __fmul2_rn(PZ, make_float2(-o.Dy, -o.Dy)));
+            const float2 cy = __ffma2_rn(PZ, make_float2(o.Dx, o.Dx), __fmul2_rn(PX, make_float2(-o.Dz, -o.Dz)));
+            const float2 cz = __ffma2_rn(PX, make_float2(o.Dy, o.Dy), __fmul2_rn(PY, make_float2(-o.Dx, -o.Dx)));
+            hx2 = __fadd2_rn(hx2, __ffma2_rn(w2, PX, cx));
+            hy2 = __fadd2_rn(hy2, __ffma2_rn(w2, PY, cy));
+            hz2 = __fadd2_rn(hz2, __ffma2_rn(w2, PZ, cz));
         }
         const uint32_t si0 = m.base[b] + pc0;
-        site_update_pair<MOVE, PPT == 1>(a, make_float2(h0.x, h1.x), make_float2(h0.y, h1.y), make_float2(h0.z, h1.z),
-                                         (int64_t)si0, at0, at1, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
+        site_update_pair<MOVE, PPT == 1>(a, hx2, hy2, hz2, (int64_t)si0, at0, at1, sx, sy, sz, sweep, rep, beta, de, dmx,
+                                         dmy, dmz);
     }
     if (a.partials) {
         __shared__ double tot[4];
@@ -615,10 +629,7 @@ __global__ void __launch_bounds__(kGenThreads, 4) k_octant_engine(const __grid_c
                 jz += jz < 0 ? hz : 0; jz -= jz >= hz ? hz : 0;
                 const uint32_t j = (uint32_t)o.plane + (uint32_t)((jx * hy + jy) * hz + jz);
                 const f3 sj = {sx[j], sy[j], sz[j]};
-                const f3 cr = cross(sj, mk(o.Dx, o.Dy, o.Dz));
-                h.x += fmaf(o.w, sj.x, cr.x);
-                h.y += fmaf(o.w, sj.y, cr.y);
-                h.z += fmaf(o.w, sj.z, cr.z);
+                bond_term(h, sj, o);
             }
             const uint32_t si = m.base[b] + (uint32_t)X * hyz + rem;
             site_update<MOVE>(a, h, (int64_t)si, (int64_t)at, sx, sy, sz, sweep, rep, beta, de, dmx, dmy, dmz);
