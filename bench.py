@@ -561,8 +561,9 @@ def run_gpu(args, w):
     value = sites_job * k * args.steps / (ms / 1e3)
 
     # dominant kernel: with the engine the timed region is the persistent launches (one per
-    # resync interval) and the resyncs (one energy pass each, well under 1 % of the region),
-    # so the region's duration stands for the launches' duration; with --engine pt the
+    # resync interval) and the resyncs (one FP64 energy pass each, about 1-1.4 ms per 10
+    # rounds of C5: 2-3 % of the region), so the region's duration stands for the launches'
+    # duration (the roofline fraction is a little low by that); with --engine pt the
     # colour-pass kernel is timed alone over relax sweeps
     if engine == "ensembles":
         launch_ms = ms_local / max(n_chunks, 1)
