@@ -177,3 +177,32 @@ def test_octant_engine_option_errors(oracle, ib, cuda_ok):
         assert e.value.status == 1
     pt.run(2, 1)
     pt.close()
+
+
+FCC = (np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]], np.float32), (1.0, 1.0, 1.0, 90.0, 90.0, 90.0))
+
+
+@pytest.mark.parametrize("Jp,ncol,dims", [(0.0, 4, (4, 4, 8)), (0.2, 10, (6, 4, 4)), (0.2, 10, (4, 4, 6))])
+def test_fcc_block_classes_replay_the_oracle(oracle, ib, cuda_ok, Jp, ncol, dims):
+    """A cell that is not one of the reference's (FCC, 4 sublattices) on the octant layout:
+    without J' its sublattices are the classes, with J' 10 DSatur classes of whole blocks, on
+    the pair kernel (nz % 4 == 0) and the one-site kernel; sweeps replay the oracle's colour
+    passes as for the reference cells."""
+    frac, (a, b, c, ab, bc, ca) = FCC
+    om = oracle.Mesh(frac, *dims, a, b, c, ab, bc, ca)
+    pm = ib.ChainMesh(*dims, frac, a, b, c, ab, bc, ca)
+    assert pm.layout == "octant"
+    s = _random_spins(om.natoms, 77)
+    om.set_spins(s)
+    pm.set_spins(s)
+    op, pp = _both_params(oracle, ib, J=-1.0, Jp=Jp, Dz=0.3, B=0.1, bulk=False)
+    col, n = pm.colouring(pp)
+    assert n == ncol
+    seed, r, beta = 0xFCC, 0.25, 1.2
+    key = oracle.SweepKey(seed=seed, ensemble=0, replica=0, move=1, r=r, philox_rounds=10)
+    ib.metropolis_mcs(pm, beta, 3, 0, 0, 0, 0, 0, r, seed=seed, p=pp)
+    for sw in range(3):
+        for k in range(n):
+            om.colour_pass(col, k, sw, beta, op, key)
+    diff = np.abs(pm.get_spins(0) - om.spins).max(axis=1)
+    assert (diff > 2e-4).sum() <= max(3, om.natoms // 400), int((diff > 2e-4).sum())
